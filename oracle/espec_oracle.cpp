@@ -1,0 +1,1160 @@
+// espec_oracle.cpp -- CPU FP64 restatement of eSPec's propagation path.
+//
+// TEST INFRASTRUCTURE ONLY (see espec_oracle.h).  Each function cites the
+// Fortran routine of the reference (path:line under the reference's src/)
+// whose arithmetic it follows.  Index arithmetic is 0-based here; the
+// Fortran is 1-based.
+#include "espec_oracle.h"
+
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <vector>
+#include <atomic>
+#include <thread>
+
+typedef std::complex<double> cd;
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+
+// Fortran DO with a REAL*8 control variable: trip count max(0, INT((m2-m1+m3)/m3))
+// (used by pspofft.f:110, psodfft.f:154, plnz.f:109).
+extern "C" int orc_do_count(double a, double b, double c) {
+  double t = (b - a + c) / c;
+  if (!(t > 0.0)) return 0;
+  return (int)t;  // INT truncates toward zero
+}
+
+// fcorrel.f:60-65  plain left-to-right real dot product
+extern "C" double orc_fcorrel(int n, const double* a, const double* b) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s = s + a[i] * b[i];
+  return s;
+}
+
+// ecnorm.f:59-65  2-norm
+extern "C" double orc_ecnorm(int n, const double* a) {
+  double s = 0.0;
+  for (int i = 0; i < n; ++i) s = s + a[i] * a[i];
+  return std::sqrt(s);
+}
+
+// ---------------------------------------------------------------------------
+// FFT.  The reference uses Singleton's 1968 mixed-radix FFT (fft3d.f:1-606),
+// one call per variable of a column-major multi-dimensional array.  Any
+// exact DFT is arithmetically equivalent up to rounding; this is a recursive
+// mixed-radix Cooley-Tukey with per-length cached twiddle tables.  isn > 0
+// selects exp(+2 pi i jk/n), isn < 0 exp(-2 pi i jk/n); unnormalised.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct TwiddleTable {
+  std::vector<cd> w;  // w[j] = exp(+2 pi i j / n)
+};
+
+const TwiddleTable& twiddles(int n) {
+  static std::mutex mu;
+  static std::map<int, TwiddleTable*> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = cache.find(n);
+  if (it != cache.end()) return *it->second;
+  TwiddleTable* t = new TwiddleTable;
+  t->w.resize(n);
+  for (int j = 0; j < n; ++j) {
+    // reduce to the first octant-free form: angle = 2 pi j / n exactly rounded once
+    long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)j /
+                    (long double)n;
+    t->w[j] = cd((double)cosl(a), (double)sinl(a));
+  }
+  cache[n] = t;
+  return *t;
+}
+
+int pick_radix(int n) {
+  if (n % 4 == 0 && n != 8) return 4;
+  if (n % 2 == 0) return 2;
+  if (n % 3 == 0) return 3;
+  if (n % 5 == 0) return 5;
+  for (int p = 7; p * p <= n; p += 2)
+    if (n % p == 0) return p;
+  return n;
+}
+
+// out[k] = sum_j in[j*stride] * W^(sign*j*k*tstep), W = exp(2 pi i / tn)
+void fft_rec(const cd* in, int stride, cd* out, int n, const cd* tab, int tn,
+             int tstep, int sign, cd* tmp) {
+  if (n == 1) {
+    out[0] = in[0];
+    return;
+  }
+  const int r = pick_radix(n);
+  const int m = n / r;
+  for (int q = 0; q < r; ++q)
+    fft_rec(in + q * stride, stride * r, out + q * m, m, tab, tn, tstep * r, sign, tmp);
+  // combine: X[k + m s] = sum_q W_n^{q(k + m s)} Y_q[k]
+  auto wn = [&](long long e) -> cd {  // W_n^e with sign
+    long long idx = (e * tstep) % tn;
+    if (idx < 0) idx += tn;
+    cd w = tab[idx];
+    return sign > 0 ? w : std::conj(w);
+  };
+  for (int k = 0; k < m; ++k) {
+    cd y[64];
+    std::vector<cd> yv;
+    cd* yy = y;
+    if (r > 64) {
+      yv.resize(r);
+      yy = yv.data();
+    }
+    for (int q = 0; q < r; ++q) yy[q] = out[q * m + k] * (q == 0 ? cd(1, 0) : wn((long long)q * k));
+    if (r == 2) {
+      tmp[k] = yy[0] + yy[1];
+      tmp[k + m] = yy[0] - yy[1];
+    } else if (r == 4) {
+      cd a0 = yy[0] + yy[2], a1 = yy[0] - yy[2];
+      cd b0 = yy[1] + yy[3], b1 = yy[1] - yy[3];
+      cd jb1 = sign > 0 ? cd(-b1.imag(), b1.real()) : cd(b1.imag(), -b1.real());
+      tmp[k] = a0 + b0;
+      tmp[k + m] = a1 + jb1;
+      tmp[k + 2 * m] = a0 - b0;
+      tmp[k + 3 * m] = a1 - jb1;
+    } else {
+      for (int s = 0; s < r; ++s) {
+        cd acc(0, 0);
+        for (int q = 0; q < r; ++q) {
+          long long e = ((long long)q * s * m) % n;  // W_n^{q m s} = W_r^{q s}
+          acc += yy[q] * (e == 0 ? cd(1, 0) : wn(e));
+        }
+        tmp[k + s * m] = acc;
+      }
+    }
+  }
+  for (int i = 0; i < n; ++i) out[i] = tmp[i];
+}
+
+void dft_line(cd* x, int n, int sign) {
+  const TwiddleTable& t = twiddles(n);
+  std::vector<cd> in(x, x + n), tmp(n);
+  fft_rec(in.data(), 1, x, n, t.w.data(), n, 1, sign, tmp.data());
+}
+
+}  // namespace
+
+// Singleton interface: ntot values, variable of length n, nspan = n * (stride)
+extern "C" void orc_fft(double* re, double* im, int ntot, int n, int nspan, int isn) {
+  if (n < 2) return;
+  const int stride = nspan / n;
+  const int sign = isn >= 0 ? +1 : -1;
+  std::vector<cd> line(n);
+  for (int base = 0; base < ntot; base += nspan) {
+    for (int off = 0; off < stride; ++off) {
+      for (int j = 0; j < n; ++j) {
+        int idx = base + off + j * stride;
+        line[j] = cd(re[idx], im[idx]);
+      }
+      dft_line(line.data(), n, sign);
+      for (int j = 0; j < n; ++j) {
+        int idx = base + off + j * stride;
+        re[idx] = line[j].real();
+        im[idx] = line[j].imag();
+      }
+    }
+  }
+}
+
+static void fft_all_axes(int ndim, const int* np, int n, double* re, double* im, int isn) {
+  int nf = 1;
+  for (int i = 0; i < ndim; ++i) {  // spofft.f:142-146
+    nf *= np[i];
+    orc_fft(re, im, n, np[i], nf, isn);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dkeft.f:64-137  DIGT kinetic table in FFT order.
+// ---------------------------------------------------------------------------
+static const double DIGT_TWOPI = 6.283185307;  // dkeft.f:38 (truncated literal)
+
+static void digt_axis(int np, double sh, double sm, double* t) {
+  // dkeft.f:69-79: P accumulated by repeated addition
+  const double dp = DIGT_TWOPI / (np * sh);
+  double p = 0.0;
+  for (int i = 0; i < np / 2; ++i) {
+    t[i] = p * p / (2.0 * sm);
+    p = p + dp;
+  }
+  p = -p;
+  for (int i = np / 2; i < np; ++i) {
+    t[i] = p * p / (2.0 * sm);
+    p = p + dp;
+  }
+}
+
+extern "C" void orc_digt(int ndim, const int* np, const double* sh, const double* sm,
+                         double* tc, double* b, int quirks) {
+  int n = 1;
+  for (int a = 0; a < ndim; ++a) n *= np[a];
+  *b = 1.0 / n;  // dkeft.f:66,82,106
+  if (ndim == 1) {
+    digt_axis(np[0], sh[0], sm[0], tc);
+    return;
+  }
+  if (quirks & ORC_Q_DIGT_ND) {
+    // literal 2D/3D loops of dkeft.f:80-137: only TC(1..NP1) is written
+    for (int i = 0; i < n; ++i) tc[i] = 0.0;
+    double dp[3];
+    for (int a = 0; a < ndim; ++a) dp[a] = DIGT_TWOPI / (np[a] * sh[a]);
+    if (ndim == 2) {
+      double p1 = 0, p2 = 0;
+      for (int j = 0; j < np[1] / 2; ++j) {
+        for (int i = 0; i < np[0] / 2; ++i) {
+          tc[i] = p1 * p1 / (2 * sm[0]) + p2 * p2 / (2 * sm[1]);
+          p1 = p1 + dp[0];
+        }
+        p2 = p2 + dp[1];
+      }
+      p1 = -(p1 + dp[0]);
+      p2 = -(p2 + dp[1]);
+      for (int j = np[1] / 2; j < np[1]; ++j) {
+        for (int i = np[0] / 2; i < np[0]; ++i) {
+          tc[i] = p1 * p1 / (2 * sm[0]) + p2 * p2 / (2 * sm[1]);
+          p1 = p1 + dp[0];
+        }
+        p2 = p2 + dp[1];
+      }
+    } else {
+      double p1 = 0, p2 = 0, p3 = 0;
+      for (int k = 0; k < np[2] / 2; ++k) {
+        for (int j = 0; j < np[1] / 2; ++j) {
+          for (int i = 0; i < np[0] / 2; ++i) {
+            tc[i] = p1 * p1 / (2 * sm[0]) + p2 * p2 / (2 * sm[1]) + p3 * p3 / (2 * sm[2]);
+            p1 = p1 + dp[0];
+          }
+          p2 = p2 + dp[1];
+        }
+        p3 = p3 + dp[2];
+      }
+      p1 = -(p1 + dp[0]);
+      p2 = -(p2 + dp[1]);
+      p3 = -(p3 + dp[2]);
+      // dkeft.f:127-137 loops J and I start at NP/2 (not NP/2+1)
+      for (int k = np[2] / 2; k < np[2]; ++k) {
+        for (int j = np[1] / 2 - 1; j < np[1]; ++j) {
+          for (int i = np[0] / 2 - 1; i < np[0]; ++i) {
+            tc[i] = p1 * p1 / (2 * sm[0]) + p2 * p2 / (2 * sm[1]) + p3 * p3 / (2 * sm[2]);
+            p1 = p1 + dp[0];
+          }
+          p2 = p2 + dp[1];
+        }
+        p3 = p3 + dp[2];
+      }
+    }
+    return;
+  }
+  // corrected N-D table: outer sum of the per-axis 1D tables
+  std::vector<double> t[3];
+  for (int a = 0; a < ndim; ++a) {
+    t[a].resize(np[a]);
+    digt_axis(np[a], sh[a], sm[a], t[a].data());
+  }
+  if (ndim == 2) {
+    for (int j = 0; j < np[1]; ++j)
+      for (int i = 0; i < np[0]; ++i) tc[i + np[0] * j] = t[0][i] + t[1][j];
+  } else {
+    for (int k = 0; k < np[2]; ++k)
+      for (int j = 0; j < np[1]; ++j)
+        for (int i = 0; i < np[0]; ++i)
+          tc[i + np[0] * (j + np[1] * k)] = t[0][i] + t[1][j] + t[2][k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// au1d.f:52-73, au2di.f:57-225, au3d.f:61-117: H_FD u with the 5-point
+// 4th-order stencil SHM*(1,-16,30,-16,1) per axis plus V u; values outside
+// the grid are zero.
+// ---------------------------------------------------------------------------
+extern "C" void orc_au(int ndim, const int* np, const double* shm, const double* vpot,
+                       const double* u, double* out) {
+  const int nx = np[0], ny = ndim > 1 ? np[1] : 1, nz = ndim > 2 ? np[2] : 1;
+  double sht = 0.0;
+  for (int a = 0; a < ndim; ++a) sht += shm[a];
+  const long sx = 1, sy = nx, sz = (long)nx * ny;
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i) {
+        const long c = i + sy * j + sz * k;
+        double s = (30.0 * sht + vpot[c]) * u[c];
+        const int idx[3] = {i, j, k};
+        const int len[3] = {nx, ny, nz};
+        const long str[3] = {sx, sy, sz};
+        for (int a = 0; a < ndim; ++a) {
+          const double h = shm[a];
+          if (idx[a] >= 2) s += h * u[c - 2 * str[a]];
+          if (idx[a] >= 1) s += -16.0 * h * u[c - str[a]];
+          if (idx[a] + 1 < len[a]) s += -16.0 * h * u[c + str[a]];
+          if (idx[a] + 2 < len[a]) s += h * u[c + 2 * str[a]];
+        }
+        out[c] = s;
+      }
+}
+
+// eigenerg.f:56-66  <u|H_FD|u>
+extern "C" double orc_eigenerg(int ndim, const int* np, const double* shm,
+                               const double* vpot, const double* u) {
+  int n = 1;
+  for (int a = 0; a < ndim; ++a) n *= np[a];
+  std::vector<double> w(n);
+  orc_au(ndim, np, shm, vpot, u, w.data());
+  return orc_fcorrel(n, u, w.data());
+}
+
+// eigenergfft.f:58-100  EFFT4 = sum V|psi|^2 + Re<psi|T_FFT|psi>
+extern "C" double orc_efft4(int ndim, const int* np, double b, const double* u,
+                            const double* v, const double* tc, const double* vpot) {
+  int n = 1;
+  for (int a = 0; a < ndim; ++a) n *= np[a];
+  const int nh = n / 2;
+  double su1 = 0, sv1 = 0;
+  for (int i = 0; i < n; ++i) {
+    su1 = su1 + u[i] * vpot[i] * u[i];
+    sv1 = sv1 + v[i] * vpot[i] * v[i];
+  }
+  std::vector<double> wu(n), wv(n);
+  for (int i = 0; i < nh; ++i) {
+    wu[i] = u[i + nh];
+    wv[i] = v[i + nh];
+    wu[i + nh] = u[i];
+    wv[i + nh] = v[i];
+  }
+  fft_all_axes(ndim, np, n, wu.data(), wv.data(), 1);
+  for (int i = 0; i < n; ++i) {
+    wu[i] = tc[i] * wu[i];
+    wv[i] = tc[i] * wv[i];
+  }
+  fft_all_axes(ndim, np, n, wu.data(), wv.data(), -1);
+  double su2 = 0, sv2 = 0;
+  for (int i = 0; i < nh; ++i) {
+    su2 = su2 + u[i] * b * wu[i + nh];
+    sv2 = sv2 + v[i] * b * wv[i + nh];
+    su2 = su2 + u[i + nh] * b * wu[i];
+    sv2 = sv2 + v[i + nh] * b * wv[i];
+  }
+  return su1 + su2 + sv1 + sv2;
+}
+
+// ---------------------------------------------------------------------------
+// spofft.f:64-200  PSPOFFTAUX: one split-operator step, in place.
+// ---------------------------------------------------------------------------
+extern "C" void orc_spo_step(int ndim, const int* np, double b, double cst1, double cst2,
+                             const double* tc, const double* vpot, const double* vabc,
+                             int absorb, int quirks, double* u, double* v) {
+  int n = 1;
+  for (int a = 0; a < ndim; ++a) n *= np[a];
+  const int nh = n / 2;
+  const bool voptic = absorb == ORC_ABS_VOPTIC;
+  const bool smooth = absorb == ORC_ABS_SMOOTHW;
+  // first V half-step with the half swap (spofft.f:66-81 / :120-133)
+  for (int i = 0; i < nh; ++i) {
+    double th1 = cst2 * vpot[i];
+    double c1 = std::cos(th1), s1 = std::sin(th1);
+    if (voptic) {
+      double e1 = std::exp(cst2 * vabc[i]);
+      c1 *= e1;
+      s1 *= e1;
+    }
+    double ua = c1 * u[i] + s1 * v[i];
+    double va = c1 * v[i] - s1 * u[i];
+    double th2 = cst2 * vpot[i + nh];
+    double c2 = std::cos(th2), s2 = std::sin(th2);
+    if (voptic) {
+      double e2 = std::exp(cst2 * vabc[i + nh]);
+      c2 *= e2;
+      s2 *= e2;
+    }
+    u[i] = c2 * u[i + nh] + s2 * v[i + nh];
+    v[i] = c2 * v[i + nh] - s2 * u[i + nh];
+    u[i + nh] = ua;
+    v[i + nh] = va;
+  }
+  fft_all_axes(ndim, np, n, u, v, 1);
+  // kinetic phase (spofft.f:148-154)
+  for (int i = 0; i < n; ++i) {
+    double th = cst1 * tc[i];
+    double c = std::cos(th), s = std::sin(th);
+    double un = c * u[i] + s * v[i];
+    if (quirks & ORC_Q_SPO_INPLACE) {
+      u[i] = un;
+      v[i] = c * v[i] - s * u[i];  // uses the updated U(I)
+    } else {
+      v[i] = c * v[i] - s * u[i];
+      u[i] = un;
+    }
+  }
+  fft_all_axes(ndim, np, n, u, v, -1);
+  // last V half-step with swap back and 1/N (spofft.f:103-118 / :162-191)
+  for (int i = 0; i < nh; ++i) {
+    double th1 = cst2 * vpot[i + nh];
+    double c1 = std::cos(th1), s1 = std::sin(th1);
+    if (voptic) {
+      double e1 = std::exp(cst2 * vabc[i + nh]);
+      c1 *= e1;
+      s1 *= e1;
+    }
+    double ua = c1 * b * u[i] + s1 * b * v[i];
+    double va = c1 * b * v[i] - s1 * b * u[i];
+    double th2 = cst2 * vpot[i];
+    double c2 = std::cos(th2), s2 = std::sin(th2);
+    if (voptic) {
+      double e2 = std::exp(cst2 * vabc[i]);
+      c2 *= e2;
+      s2 *= e2;
+    }
+    double un = c2 * b * u[i + nh] + s2 * b * v[i + nh];
+    double vn = c2 * b * v[i + nh] - s2 * b * u[i + nh];
+    if (smooth) {
+      u[i] = vabc[i] * un;
+      v[i] = vabc[i] * vn;
+      u[i + nh] = vabc[i + nh] * ua;
+      v[i + nh] = vabc[i + nh] * va;
+    } else {
+      u[i] = un;
+      v[i] = vn;
+      u[i + nh] = ua;
+      v[i + nh] = va;
+    }
+  }
+}
+
+// sodfft.f:64-126  PSODFFTAUX: psi+ = psi- - i cst H psi (T by FFT)
+static void sod_step(int ndim, const int* np, double b, double cst, const double* tc,
+                     const double* vpot, const double* vabc, int absorb, int quirks,
+                     double* u1, double* u2, double* v1, double* v2, double* wr, double* wi) {
+  int n = 1;
+  for (int a = 0; a < ndim; ++a) n *= np[a];
+  const int nh = n / 2;
+  if (absorb == ORC_ABS_VOPTIC) {
+    for (int i = 0; i < n; ++i) {
+      wr[i] = u1[i] + cst * vpot[i] * v2[i] + cst * vabc[i] * u2[i];
+      wi[i] = v1[i] - cst * vpot[i] * u2[i] + cst * vabc[i] * v2[i];
+      u1[i] = u2[i];
+      v1[i] = v2[i];
+    }
+  } else {
+    for (int i = 0; i < n; ++i) {
+      wr[i] = u1[i] + cst * vpot[i] * v2[i];
+      wi[i] = v1[i] - cst * vpot[i] * u2[i];
+      u1[i] = u2[i];
+      v1[i] = v2[i];
+    }
+  }
+  for (int i = 0; i < nh; ++i) {
+    double ua = u2[i], va = v2[i];
+    u2[i] = u2[i + nh];
+    v2[i] = v2[i + nh];
+    u2[i + nh] = ua;
+    v2[i + nh] = va;
+  }
+  fft_all_axes(ndim, np, n, u2, v2, 1);
+  for (int i = 0; i < n; ++i) {
+    u2[i] = tc[i] * u2[i];
+    v2[i] = tc[i] * v2[i];
+  }
+  fft_all_axes(ndim, np, n, u2, v2, -1);
+  // sodfft.f:108 tests TPABSOR(1:7) against the 8-character '.SMOOTHW', which
+  // never matches: the reference never applies the mask in this propagator.
+  const bool smooth = absorb == ORC_ABS_SMOOTHW && !(quirks & ORC_Q_SOD_SMOOTHW);
+  for (int i = 0; i < nh; ++i) {
+    double ua = wr[i + nh] + cst * b * v2[i];
+    double va = wi[i + nh] - cst * b * u2[i];
+    double ul = wr[i] + cst * b * v2[i + nh];
+    double vl = wi[i] - cst * b * u2[i + nh];
+    if (smooth) {
+      u2[i] = vabc[i] * ul;
+      v2[i] = vabc[i] * vl;
+      u2[i + nh] = vabc[i + nh] * ua;
+      v2[i + nh] = vabc[i + nh] * va;
+    } else {
+      u2[i] = ul;
+      v2[i] = vl;
+      u2[i + nh] = ua;
+      v2[i + nh] = va;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// absorb.f:62-195  ABSORBINGBC
+// ---------------------------------------------------------------------------
+extern "C" int orc_absorbingbc(int ndim, const int* np, int type, const double* al,
+                               const double* ar, const double* sh, const double* xi,
+                               const double* xf, const double* voi, double* vabc) {
+  if (ndim == 1) {
+    for (int i = 0; i < np[0]; ++i) {
+      double x1 = xi[0] + (i) * sh[0];  // XI(1) + (I - ONE)*SH(1)
+      double r;
+      switch (type) {
+        case ORC_ABC_SMOOTHW:  // absorb.f:66-79
+          if (x1 < al[0])
+            r = std::exp(voi[0] * std::pow(x1 - al[0], voi[1]) / (x1 + sh[0] - xi[0]));
+          else if (x1 > ar[0])
+            r = std::exp(-voi[0] * (x1 - ar[0]) / std::pow(xf[0] + sh[0] - x1, voi[1]));
+          else
+            r = 1.0;
+          break;
+        case ORC_ABC_SMRS:  // absorb.f:82-118 (active lines)
+          if (x1 < al[0])
+            r = 1.0 - voi[0] * (x1 - al[0]) * (x1 - al[0]);
+          else if (x1 > ar[0])
+            r = 1.0 - voi[0] * (x1 - ar[0]) * (x1 - ar[0]);
+          else
+            r = 1.0;
+          break;
+        case ORC_ABC_VOPTIC_LINEAR:  // absorb.f:120-130
+          if (x1 < al[0])
+            r = -voi[0] * (x1 - al[0]) / (x1 + sh[0] - xi[0]);
+          else if (x1 > ar[0])
+            r = voi[0] * (x1 - ar[0]) / (xf[0] + sh[0] - x1);
+          else
+            r = 0.0;
+          break;
+        case ORC_ABC_VOPTIC_POLIN:  // absorb.f:142-152
+          if (x1 < al[0])
+            r = voi[0] * std::pow(x1 - al[0], voi[1]);
+          else if (x1 > ar[0])
+            r = voi[0] * std::pow(x1 - ar[0], voi[1]);
+          else
+            r = 0.0;
+          break;
+        default:
+          return -1;
+      }
+      vabc[i] = r;
+    }
+    return 0;
+  }
+  if (ndim == 2 && type == ORC_ABC_SMOOTHW) {  // absorb.f:157-195
+    for (int j = 0; j < np[1]; ++j) {
+      double x2 = xi[1] + j * sh[1];
+      for (int i = 0; i < np[0]; ++i) {
+        double x1 = xi[0] + i * sh[0];
+        double r;
+        if (x1 < al[0])
+          r = std::exp(voi[0] * (x1 - al[0]) / (x1 + sh[0] - xi[0]));
+        else if (x2 < al[1])
+          r = std::exp(voi[1] * (x2 - al[1]) / (x2 + sh[1] - xi[1]));
+        else if (x1 > ar[0])
+          r = std::exp(-voi[0] * (x1 - ar[0]) / (xf[0] + sh[0] - x1));
+        else if (x2 > ar[1])
+          r = std::exp(-voi[1] * (x2 - ar[1]) / (xf[1] + sh[1] - x2));
+        else
+          r = 1.0;
+        vabc[i + np[0] * j] = r;
+      }
+    }
+    return 0;
+  }
+  return -1;  // absorb.f:196-205 STOP: not implemented in the reference
+}
+
+// ---------------------------------------------------------------------------
+// Propagator drivers
+// ---------------------------------------------------------------------------
+namespace {
+struct RowSink {
+  double* rows;
+  int cap;
+  int n = 0;
+  void put(double t, double e, double cr, double ci, double ct, double fn) {
+    if (rows && n < cap) {
+      double* r = rows + 6 * n;
+      r[0] = t;
+      r[1] = e;
+      r[2] = cr;
+      r[3] = ci;
+      r[4] = ct;
+      r[5] = fn;
+    }
+    ++n;
+  }
+};
+struct CSink {
+  double *re, *im;
+  int cap;
+  int n = 0;
+  void put(double cr, double ci) {
+    if (n < cap) {
+      re[n] = cr;
+      im[n] = ci;
+    }
+    ++n;
+  }
+};
+inline int npts(const orc_prop_t* p) {
+  int n = 1;
+  for (int a = 0; a < p->ndim; ++a) n *= p->np[a];
+  return n;
+}
+}  // namespace
+
+// pspofft.f:72-145  PSPOFFT
+extern "C" int orc_pspofft(const orc_prop_t* p, const double* vpot, const double* vabc,
+                           double* u1, double* v1, double* c_re, double* c_im, int c_cap,
+                           double* rows, int row_cap, int* nrows, int* info) {
+  const int n = npts(p);
+  RowSink rs{rows, row_cap};
+  CSink cs{c_re, c_im, c_cap};
+  *info = 0;
+  int mc = 0;
+  double t = p->ti;
+  const double cst1 = p->dt / ORC_SHFS, cst2 = p->dt / (2.0 * ORC_SHFS);
+  std::vector<double> u0(u1, u1 + n), v0(v1, v1 + n), tc(n);
+  double b;
+  orc_digt(p->ndim, p->np, p->sh, p->sm, tc.data(), &b, p->quirks);
+  auto corr = [&](double& cr, double& ci) {
+    cr = orc_fcorrel(n, u0.data(), u1) + orc_fcorrel(n, v0.data(), v1);
+    ci = orc_fcorrel(n, u0.data(), v1) - orc_fcorrel(n, v0.data(), u1);
+  };
+  auto normf = [&]() {
+    double fnr = orc_fcorrel(n, u1, u1) + orc_fcorrel(n, v1, v1);
+    double fni = orc_fcorrel(n, u1, v1) - orc_fcorrel(n, v1, u1);
+    return std::sqrt(fnr * fnr + fni * fni);
+  };
+  double cr, ci;
+  corr(cr, ci);
+  double ct = std::sqrt(cr * cr + ci * ci);
+  cs.put(cr, ci);
+  double et = orc_efft4(p->ndim, p->np, b, u1, v1, tc.data(), vpot);
+  const double e0 = et;
+  double fnt = normf();
+  const double f0 = fnt;
+  if (p->prtcrl != ORC_PRT_NONE) rs.put(t, et, cr, ci, ct, fnt);
+  const int nit = orc_do_count(p->ti + p->dt, p->tf + p->dt, p->dt);
+  t = p->ti + p->dt;
+  for (int it = 0; it < nit; ++it, t = t + p->dt) {
+    orc_spo_step(p->ndim, p->np, b, cst1, cst2, tc.data(), vpot, vabc, p->absorb, p->quirks,
+                 u1, v1);
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      corr(cr, ci);
+      cs.put(cr, ci);
+    }
+    if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+      corr(cr, ci);
+      ct = std::sqrt(cr * cr + ci * ci);
+      et = orc_efft4(p->ndim, p->np, b, u1, v1, tc.data(), vpot);
+      fnt = normf();
+      if (p->absorb != ORC_ABS_NONE) {  // pspofft.f:137-142
+        if (std::fabs((et - e0) / e0) * 100.0 > p->tol ||
+            std::fabs((fnt - f0) / f0) * 100.0 > p->tol)
+          *info = 1;
+      } else {
+        if (std::fabs((et - e0) / e0) * 100.0 > p->tol) *info = 1;
+      }
+      rs.put(t, et, cr, ci, ct, fnt);
+    }
+  }
+  if (nrows) *nrows = rs.n;
+  return cs.n;
+}
+
+// psodfft.f:77-206  PSODFFT
+extern "C" int orc_psodfft(const orc_prop_t* p, const double* vpot, const double* vabc,
+                           double* u1, double* v1, double* u2, double* v2, double* c_re,
+                           double* c_im, int c_cap, double* rows, int row_cap, int* nrows,
+                           int* info) {
+  const int n = npts(p);
+  RowSink rs{rows, row_cap};
+  CSink cs{c_re, c_im, c_cap};
+  *info = 0;
+  double t = p->ti;
+  const double cst = 2.0 * p->dt / ORC_SHFS;
+  std::vector<double> u0(u1, u1 + n), v0(v1, v1 + n), tc(n), wr(n), wi(n);
+  for (int i = 0; i < n; ++i) {
+    u2[i] = u0[i];
+    v2[i] = v0[i];
+  }
+  double b;
+  orc_digt(p->ndim, p->np, p->sh, p->sm, tc.data(), &b, p->quirks);
+  auto corr = [&](double& cr, double& ci) {
+    cr = orc_fcorrel(n, u0.data(), u2) + orc_fcorrel(n, v0.data(), v2);
+    ci = orc_fcorrel(n, u0.data(), v2) - orc_fcorrel(n, v0.data(), u2);
+  };
+  auto normf = [&]() {
+    double fnr = orc_fcorrel(n, u2, u2) + orc_fcorrel(n, v2, v2);
+    double fni = orc_fcorrel(n, u2, v2) - orc_fcorrel(n, v2, u2);
+    return std::sqrt(fnr * fnr + fni * fni);
+  };
+  auto drift = [&](double et, double e0, double fnt, double f0) {  // psodfft.f:178-183
+    if (p->absorb != ORC_ABS_NONE) {
+      if (std::fabs((et - e0) / e0) * 100.0 > p->tol) *info = 1;
+    } else {
+      if (std::fabs((et - e0) / e0) * 100.0 > p->tol ||
+          std::fabs((fnt - f0) / f0) * 100.0 > p->tol)
+        *info = 1;
+    }
+  };
+  double cr, ci;
+  corr(cr, ci);
+  double ct = std::sqrt(cr * cr + ci * ci);
+  cs.put(cr, ci);
+  double et = orc_efft4(p->ndim, p->np, b, u2, v2, tc.data(), vpot);
+  const double e0 = et;
+  double fnt = normf();
+  const double f0 = fnt;
+  if (p->prtcrl != ORC_PRT_NONE) rs.put(t, et, cr, ci, ct, fnt);
+  // start-up: two half-steps (psodfft.f:120-123)
+  sod_step(p->ndim, p->np, b, cst / 2.0, tc.data(), vpot, vabc, p->absorb, p->quirks, u1, u2,
+           v1, v2, wr.data(), wi.data());
+  sod_step(p->ndim, p->np, b, cst / 2.0, tc.data(), vpot, vabc, p->absorb, p->quirks, u1, u2,
+           v1, v2, wr.data(), wi.data());
+  int mc = 1;
+  t = p->ti + p->dt;
+  corr(cr, ci);
+  ct = std::sqrt(cr * cr + ci * ci);
+  if (mc == p->lc) {
+    mc = 0;
+    cs.put(cr, ci);
+  }
+  if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+    et = orc_efft4(p->ndim, p->np, b, u2, v2, tc.data(), vpot);
+    fnt = normf();
+    rs.put(t, et, cr, ci, ct, fnt);
+  }
+  for (int i = 0; i < n; ++i) {  // psodfft.f:149-152
+    u1[i] = u0[i];
+    v1[i] = v0[i];
+  }
+  const int nit = orc_do_count(p->ti + 2 * p->dt, p->tf + p->dt, p->dt);
+  t = p->ti + 2 * p->dt;
+  for (int it = 0; it < nit; ++it, t = t + p->dt) {
+    sod_step(p->ndim, p->np, b, cst, tc.data(), vpot, vabc, p->absorb, p->quirks, u1, u2, v1,
+             v2, wr.data(), wi.data());
+    mc = mc + 1;
+    if (mc == p->lc) {
+      corr(cr, ci);
+      mc = 0;
+      cs.put(cr, ci);
+    }
+    if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+      corr(cr, ci);
+      ct = std::sqrt(cr * cr + ci * ci);
+      et = orc_efft4(p->ndim, p->np, b, u2, v2, tc.data(), vpot);
+      fnt = normf();
+      drift(et, e0, fnt, f0);
+      rs.put(t, et, cr, ci, ct, fnt);
+    }
+  }
+  et = orc_efft4(p->ndim, p->np, b, u2, v2, tc.data(), vpot);
+  fnt = normf();
+  drift(et, e0, fnt, f0);
+  if (nrows) *nrows = rs.n;
+  return cs.n;
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric tridiagonal eigensolver (stands in for DSTEVX('V','A'),
+// dstevx.f).  Implicit-shift QL iteration with Wilkinson shifts on a copy of
+// (d, e), accumulating the rotations into Z.  Eigenvalues sorted ascending.
+// ---------------------------------------------------------------------------
+extern "C" int orc_tridiag_eig(int n, const double* d_in, const double* e_in, double* w,
+                               double* z) {
+  std::vector<double> d(d_in, d_in + n), e(n, 0.0);
+  for (int i = 0; i + 1 < n; ++i) e[i] = e_in[i];
+  for (int i = 0; i < n * n; ++i) z[i] = 0.0;
+  for (int i = 0; i < n; ++i) z[i + n * i] = 1.0;
+  for (int l = 0; l < n; ++l) {
+    int iter = 0;
+    for (;;) {
+      int m = l;
+      for (; m < n - 1; ++m) {
+        double dd = std::fabs(d[m]) + std::fabs(d[m + 1]);
+        if (std::fabs(e[m]) <= 1e-17 * dd) break;
+      }
+      if (m == l) break;
+      if (++iter > 60) return 1;
+      double g = (d[l + 1] - d[l]) / (2.0 * e[l]);
+      double r = std::hypot(g, 1.0);
+      g = d[m] - d[l] + e[l] / (g + (g >= 0 ? std::fabs(r) : -std::fabs(r)));
+      double s = 1.0, c = 1.0, pp = 0.0;
+      int i = m - 1;
+      bool underflow = false;
+      for (; i >= l; --i) {
+        double f = s * e[i], bb = c * e[i];
+        r = std::hypot(f, g);
+        e[i + 1] = r;
+        if (r == 0.0) {
+          d[i + 1] -= pp;
+          e[m] = 0.0;
+          underflow = true;
+          break;
+        }
+        s = f / r;
+        c = g / r;
+        g = d[i + 1] - pp;
+        r = (d[i] - g) * s + 2.0 * c * bb;
+        pp = s * r;
+        d[i + 1] = g + pp;
+        g = c * r - bb;
+        for (int k = 0; k < n; ++k) {  // rotate columns i, i+1 of Z
+          double zf = z[k + n * (i + 1)];
+          z[k + n * (i + 1)] = s * z[k + n * i] + c * zf;
+          z[k + n * i] = c * z[k + n * i] - s * zf;
+        }
+      }
+      if (underflow) continue;
+      d[l] -= pp;
+      e[l] = g;
+      e[m] = 0.0;
+    }
+  }
+  // sort ascending
+  std::vector<int> ord(n);
+  for (int i = 0; i < n; ++i) ord[i] = i;
+  for (int i = 0; i < n; ++i)
+    for (int j = i + 1; j < n; ++j)
+      if (d[ord[j]] < d[ord[i]]) std::swap(ord[i], ord[j]);
+  std::vector<double> zz(z, z + n * n);
+  for (int i = 0; i < n; ++i) {
+    w[i] = d[ord[i]];
+    for (int k = 0; k < n; ++k) z[k + n * i] = zz[k + n * ord[i]];
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// lnz.f:76-119 (LNZ) with reort.f:65-80 (REORT, classical Gram-Schmidt)
+// Builds mp Lanczos vectors of H from start vector s into L (n x mp,
+// column-major), alpha al[mp], beta bt[mp].  Returns false when the start
+// vector is zero (lnz.f:90 BT0.EQ.0 branch).
+// ---------------------------------------------------------------------------
+static bool lanczos(int ndim, const int* np, const double* shm, const double* vpot, int n,
+                    int mp, const double* s, double* L, double* al, double* bt) {
+  std::vector<double> work(s, s + n), vi(n, 0.0), v0(n), rv(mp);
+  for (long i = 0; i < (long)n * mp; ++i) L[i] = 0.0;
+  double bt0 = orc_ecnorm(n, work.data());
+  if (bt0 == 0.0) return false;
+  for (int it = 0; it < mp; ++it) {
+    for (int j = 0; j < n; ++j) {
+      v0[j] = vi[j];
+      vi[j] = work[j] / bt0;
+      L[j + (long)n * it] = vi[j];
+    }
+    orc_au(ndim, np, shm, vpot, vi.data(), work.data());
+    double sum1 = 0.0;
+    for (int j = 0; j < n; ++j) {
+      work[j] = work[j] - bt0 * v0[j];
+      sum1 = sum1 + vi[j] * work[j];
+    }
+    al[it] = sum1;
+    for (int j = 0; j < n; ++j) work[j] = work[j] - al[it] * vi[j];
+    const int m = it + 1;  // REORT against the it+1 stored vectors
+    for (int q = 0; q < m; ++q) {
+      double r = 0.0;
+      for (int j = 0; j < n; ++j) r = r + work[j] * L[j + (long)n * q];
+      rv[q] = r;
+    }
+    for (int q = 0; q < m; ++q)
+      for (int j = 0; j < n; ++j) work[j] = work[j] - rv[q] * L[j + (long)n * q];
+    bt[it] = orc_ecnorm(n, work.data());
+    bt0 = bt[it];
+  }
+  return true;
+}
+
+// sil.f:70-181 PLNZAUX: one short-iterative-Lanczos step, real and imaginary
+// parts propagated by separate Krylov bases.
+static int sil_step(const orc_prop_t* p, int mp, const double* vpot, const double* vabc,
+                    double cst, double* u, double* v) {
+  const int n = npts(p);
+  std::vector<double> L((size_t)n * mp), al(mp), bt(mp), w(mp), q((size_t)mp * mp);
+  std::vector<double> a(mp), c(mp), sn(mp), tmp(mp);
+  std::vector<double> ur(n, 0.0), ui(n, 0.0), vr(n, 0.0), vi(n, 0.0);
+  auto project = [&](const double* x, double* y) {  // y = Q^T L^T x
+    for (int k = 0; k < mp; ++k) tmp[k] = orc_fcorrel(n, L.data() + (size_t)n * k, x);
+    for (int i = 0; i < mp; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < mp; ++j) s = s + q[j + mp * i] * tmp[j];
+      y[i] = s;
+    }
+  };
+  auto expand = [&](const double* y, double* x) {  // x = L Q y
+    for (int j = 0; j < mp; ++j) {
+      double s = 0.0;
+      for (int i = 0; i < mp; ++i) s = s + q[j + mp * i] * y[i];
+      tmp[j] = s;
+    }
+    for (int k = 0; k < n; ++k) {
+      double s = 0.0;
+      for (int j = 0; j < mp; ++j) s = s + L[k + (size_t)n * j] * tmp[j];
+      x[k] = s;
+    }
+  };
+  // real part: e^{-iH dt} u = cos(H dt) u - i sin(H dt) u
+  if (lanczos(p->ndim, p->np, p->shm, vpot, n, mp, u, L.data(), al.data(), bt.data())) {
+    if (orc_tridiag_eig(mp, al.data(), bt.data(), w.data(), q.data())) return -1;
+    project(u, a.data());
+    for (int i = 0; i < mp; ++i) {
+      double e = w[i] * cst;
+      double cu = std::cos(e) * a[i];
+      sn[i] = -std::sin(e) * ((p->quirks & ORC_Q_SIL_INPLACE) ? cu : a[i]);
+      c[i] = cu;
+    }
+    expand(c.data(), ur.data());
+    expand(sn.data(), ui.data());
+  }
+  // imaginary part: e^{-iH dt} (i v) = sin(H dt) v + i cos(H dt) v
+  if (lanczos(p->ndim, p->np, p->shm, vpot, n, mp, v, L.data(), al.data(), bt.data())) {
+    if (orc_tridiag_eig(mp, al.data(), bt.data(), w.data(), q.data())) return -1;
+    project(v, a.data());
+    for (int i = 0; i < mp; ++i) {
+      double e = w[i] * cst;
+      sn[i] = std::sin(e) * a[i];
+      c[i] = std::cos(e) * a[i];
+    }
+    expand(c.data(), vi.data());
+    expand(sn.data(), vr.data());
+  }
+  if (p->absorb == ORC_ABS_SMOOTHW) {  // sil.f:171-175
+    for (int k = 0; k < n; ++k) {
+      u[k] = vabc[k] * (ur[k] + vr[k]);
+      v[k] = vabc[k] * (ui[k] + vi[k]);
+    }
+  } else {
+    for (int k = 0; k < n; ++k) {
+      u[k] = ur[k] + vr[k];
+      v[k] = ui[k] + vi[k];
+    }
+  }
+  return 0;
+}
+
+// plnz.f:71-151  PLNZ
+extern "C" int orc_plnz(const orc_prop_t* p, const double* vpot, const double* vabc,
+                        double* u, double* v, double* c_re, double* c_im, int c_cap,
+                        double* rows, int row_cap, int* nrows, int* info) {
+  const int n = npts(p);
+  RowSink rs{rows, row_cap};
+  CSink cs{c_re, c_im, c_cap};
+  *info = 0;
+  const double cst = p->dt / ORC_SHFS;
+  int mp = p->mp;
+  if (p->change && mp > p->lmtreort) mp = p->lmtreort;  // lnz.f:64-72 (MP aliased)
+  if (p->absorb == ORC_ABS_VOPTIC) return -1;           // real-symmetric Lanczos only
+  std::vector<double> u0(u, u + n), v0(v, v + n);
+  auto corr = [&](double& cr, double& ci) {
+    cr = orc_fcorrel(n, u0.data(), u) + orc_fcorrel(n, v0.data(), v);
+    ci = orc_fcorrel(n, u0.data(), v) - orc_fcorrel(n, v0.data(), u);
+  };
+  auto energy = [&]() {
+    return orc_eigenerg(p->ndim, p->np, p->shm, vpot, u) +
+           orc_eigenerg(p->ndim, p->np, p->shm, vpot, v);
+  };
+  double cr, ci;
+  corr(cr, ci);
+  double ct = cr * cr + ci * ci;  // plnz.f:86 prints |C|^2
+  cs.put(cr, ci);
+  double et = energy();
+  const double e0 = et;
+  double fnt = orc_fcorrel(n, u, u) + orc_fcorrel(n, v, v);
+  const double f0 = fnt;
+  if (p->prtcrl != ORC_PRT_NONE) rs.put(p->ti, et, cr, ci, ct, fnt);
+  int mc = 0;
+  const int nit = orc_do_count(p->ti + p->dt, p->tf + p->dt, p->dt);
+  double t = p->ti + p->dt;
+  for (int it = 0; it < nit; ++it, t = t + p->dt) {
+    if (sil_step(p, mp, vpot, vabc, cst, u, v)) return -1;  // sil.f:119-120 STOP
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      corr(cr, ci);
+      cs.put(cr, ci);
+    }
+    if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+      corr(cr, ci);
+      ct = cr * cr + ci * ci;
+      et = energy();
+      fnt = orc_fcorrel(n, u, u) + orc_fcorrel(n, v, v);
+      if (std::fabs((et - e0) / e0) * 100.0 > p->tol ||
+          std::fabs((fnt - f0) / f0) * 100.0 > p->tol)
+        *info = 1;
+      rs.put(t, et, cr, ci, ct, fnt);
+    }
+  }
+  et = energy();
+  fnt = orc_fcorrel(n, u, u) + orc_fcorrel(n, v, v);
+  if (std::fabs((et - e0) / e0) * 100.0 > p->tol || std::fabs((fnt - f0) / f0) * 100.0 > p->tol)
+    *info = 1;
+  if (nrows) *nrows = rs.n;
+  return cs.n;
+}
+
+// ---------------------------------------------------------------------------
+// Spectrum stage
+// ---------------------------------------------------------------------------
+
+// espec.f:1545-1576 (one correlation function, ND = 1): mirror C(-t) = C(t)*
+// onto 2^MF points; c_re/c_im hold the MC = 2^(MF-1) stored samples.
+extern "C" void orc_total_correlation(int mf, const double* c_re, const double* c_im,
+                                      double* u, double* v) {
+  const int mc = (1 << mf) / 2;
+  for (int i = 0; i < 2 * mc; ++i) u[i] = v[i] = 0.0;
+  for (int i = 1; i <= mc; ++i) {  // 1-based as in the Fortran
+    u[mc + i - 1] = u[mc + i - 1] + c_re[i - 1];
+    u[mc - i + 1] = u[mc + i - 1];
+    v[mc + i - 1] = v[mc + i - 1] + c_im[i - 1];
+    v[mc - i + 1] = -v[mc + i - 1];
+  }
+  u[0] = u[0] + c_re[mc - 1];
+  v[0] = v[0] + c_im[mc - 1];
+  v[0] = -v[0];
+}
+
+// hwhm.f:59-77  energy shift and exponential lifetime damping
+extern "C" void orc_hwhm(int mf, double dtf, double tf, double tal, double de, double* u,
+                         double* v) {
+  const int n = 1 << mf;
+  const double dem = -de * 1.5192676;
+  const double ta = tal * 1.5192676;
+  for (int i = 0; i < n; ++i) {
+    double t = -tf + (double)i * dtf;
+    double cs = std::cos(dem * t), sn = std::sin(dem * t);
+    double cstl = std::exp(-std::fabs(t) * ta);
+    double ui = u[i];
+    u[i] = cs * u[i] - sn * v[i];
+    v[i] = cs * v[i] + sn * ui;
+    u[i] = cstl * u[i];
+    v[i] = cstl * v[i];
+  }
+}
+
+// cfft.f:6-63  FFTNT: in-place radix-2 decimation-in-frequency DFT with
+// bit reversal; itype = -1 gives the inverse transform scaled by 1/N.
+extern "C" void orc_fftnt(double* x, double* y, int n, int m, int itype, int quirks) {
+  if (n == 1) return;
+  const double twopi = (quirks & ORC_Q_FFTNT_SP) ? (double)6.283185307179586476925287f
+                                                 : 6.283185307179586476925287;
+  if (itype == -1)
+    for (int i = 0; i < n; ++i) y[i] = -y[i];
+  const double pstep = twopi / n;
+  int n2 = n;
+  for (int k = 0; k < m; ++k) {
+    int n1 = n2;
+    n2 = n2 / 2;
+    int ie = n / n1, ia = 1;
+    for (int j = 1; j <= n2; ++j) {
+      double a = (ia - 1) * pstep;
+      double c = std::cos(a), s = std::sin(a);
+      ia = ia + ie;
+      for (int i = j; i <= n; i += n1) {
+        int l = i + n2;
+        double xt = x[i - 1] - x[l - 1];
+        x[i - 1] = x[i - 1] + x[l - 1];
+        double yt = y[i - 1] - y[l - 1];
+        y[i - 1] = y[i - 1] + y[l - 1];
+        x[l - 1] = c * xt + s * yt;
+        y[l - 1] = c * yt - s * xt;
+      }
+    }
+  }
+  int j = 1;
+  for (int i = 1; i <= n - 1; ++i) {
+    if (i < j) {
+      std::swap(x[j - 1], x[i - 1]);
+      std::swap(y[j - 1], y[i - 1]);
+    }
+    int k = n / 2;
+    while (k < j) {
+      j = j - k;
+      k = k / 2;
+    }
+    j = j + k;
+  }
+  if (itype == -1)
+    for (int i = 0; i < n; ++i) {
+      y[i] = -y[i] / n;
+      x[i] = x[i] / n;
+    }
+}
+
+// spectrumtd.f:58-109  window (.SG or none), half swap, inverse FFTNT.
+// en[i] receives the energy printed beside natural index i (without DE).
+extern "C" int orc_spectrumtd(int window_sg, int mf, double dtf, double tf, double wp,
+                              double de, double* u, double* v, double* en, int quirks) {
+  const int n = 1 << mf;
+  double enc = 1.0 / (n * dtf) * 1.519829846003e-1;
+  enc = enc * ORC_FATE;
+  double e = -n / 2.0 * enc;
+  (void)de;
+  if (window_sg) {
+    const double tmax = n * dtf;
+    const double taux = tmax * tmax / (std::log(1.0 / wp) * std::log(1.0 / wp));
+    for (int i = 0; i < n; ++i) {
+      double t = -tf + (double)i * dtf;
+      double cstl = std::exp(-t * t / taux);
+      u[i] = cstl * u[i];
+      v[i] = cstl * v[i];
+    }
+  }
+  for (int i = 0; i < n / 2; ++i) {
+    std::swap(u[i], u[n / 2 + i]);
+    std::swap(v[i], v[n / 2 + i]);
+  }
+  orc_fftnt(u, v, n, mf, -1, quirks);
+  for (int i = n / 2; i < n; ++i) {
+    en[i] = e;
+    e = e + enc;
+  }
+  for (int i = 0; i < n / 2; ++i) {
+    en[i] = e;
+    e = e + enc;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Batched 1D split-operator scan (CPU baseline): independent packets, each
+// propagated with the reference step (spofft.f:120-191) and C(t) of every
+// step (pspofft.f:115-123, LC = 1).  Packets are spread over nthreads host
+// threads through a shared packet counter.
+// ---------------------------------------------------------------------------
+extern "C" int orc_spo_batch(int npk, const int* off, const double* sh, const double* sm,
+                             const double* vpot, double* u, double* v, double dt_fs,
+                             int nsteps, int quirks, double* c_re, double* c_im,
+                             int nthreads) {
+  std::atomic<int> next{0};
+  auto worker = [&]() {
+    for (;;) {
+      const int k = next.fetch_add(1);
+      if (k >= npk) return;
+      const int n = off[k + 1] - off[k];
+      double* uk = u + off[k];
+      double* vk = v + off[k];
+      const double* vp = vpot + off[k];
+      std::vector<double> u0(uk, uk + n), v0(vk, vk + n), tc(n);
+      double b;
+      int np[3] = {n, 1, 1};
+      orc_digt(1, np, sh + k, sm + k, tc.data(), &b, 0);
+      const double cst1 = dt_fs / ORC_SHFS, cst2 = dt_fs / (2.0 * ORC_SHFS);
+      double* cr = c_re + (size_t)k * (nsteps + 1);
+      double* ci = c_im + (size_t)k * (nsteps + 1);
+      for (int s = 0; s <= nsteps; ++s) {
+        if (s > 0)
+          orc_spo_step(1, np, b, cst1, cst2, tc.data(), vp, nullptr, ORC_ABS_NONE, quirks, uk,
+                       vk);
+        cr[s] = orc_fcorrel(n, u0.data(), uk) + orc_fcorrel(n, v0.data(), vk);
+        ci[s] = orc_fcorrel(n, u0.data(), vk) - orc_fcorrel(n, v0.data(), uk);
+      }
+    }
+  };
+  if (nthreads < 1) nthreads = 1;
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nthreads; ++t) pool.emplace_back(worker);
+  worker();
+  for (auto& th : pool) th.join();
+  return 0;
+}

@@ -1,0 +1,321 @@
+#!/usr/bin/env python3
+"""Generate the golden fixtures that pin the CPU oracle to eSPec itself.
+
+Run in a container where the reference tree is mounted at /root/reference
+(the path can be overridden with ESPEC_REF).  The script only RUNS the shipped
+eSPec executable (espec_v07.x) as a black box on input decks, and reads the
+reference's own test fixtures (ttests/) as text; it never inspects the
+executable.  Outputs go to tests/golden/*.npz plus manifest.json.
+
+Cases:
+  test8       reference test 8 (.ONLYSPEC): C(t) from ttests/correl8.inp ->
+              HWHM -> SPECTRUMTD, compared with the executable's spectrum and
+              with ttests/results.test8 (the reference's committed golden).
+  test4       reference test 4 (.PSIL, N=201 from ttests/eigpot_test3.inp):
+              partial C(t) table and spectrum from the executable.
+  morse1d_*   1D Morse (N=1024 on [0.5, 8.0] bohr, mass 918 m_e, Gaussian at
+              1.8 bohr, sigma 0.2) at dt = 0.005 au for 2048 steps with .PFSOD,
+              .PFSPO and .PSIL, without absorber, with a .VOPTIC_POLIN CAP and
+              with a .SMOOTHW mask.
+  morse2d_*   2D coupled Morse on a 32x32 grid with .PSIL, .PFSPO and .PFSOD
+              (the last two pin the reference's 2D kinetic-table defect).
+"""
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+REF = os.environ.get("ESPEC_REF", "/root/reference")
+BIN = os.path.join(REF, "espec_v07.x")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+SHFS = 2.4188843243e-2
+AMU = 1836.152667539
+
+
+def run_deck(deck, files, timeout=600):
+    d = tempfile.mkdtemp(prefix="espec_golden_")
+    try:
+        with open(os.path.join(d, "input.spc"), "w") as f:
+            f.write(deck)
+        for name, src in files.items():
+            dst = os.path.join(d, name)
+            if isinstance(src, str) and os.path.exists(src):
+                os.symlink(src, dst)
+            else:
+                with open(dst, "w") as f:
+                    f.write(src)
+        r = subprocess.run([BIN], cwd=d, capture_output=True, text=True, timeout=timeout)
+        return r.stdout
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def _floats(line):
+    # Fortran prints '****' when a value overflows its edit descriptor
+    return [np.nan if "*" in x else float(x.replace("D", "E")) for x in line.split()]
+
+
+def parse_partial(out):
+    lines = out.splitlines()
+    for i, l in enumerate(lines):
+        if "Partial auto-correlation function:" in l:
+            break
+    else:
+        raise RuntimeError("no partial correlation table:\n" + out[-3000:])
+    rows = []
+    for l in lines[i + 4:]:
+        s = l.split()
+        if len(s) != 6:
+            if rows:
+                break
+            continue
+        try:
+            rows.append(_floats(l))
+        except ValueError:
+            rows.append([np.nan] * 6)
+    return np.array(rows)
+
+
+def parse_table(out, header, ncol):
+    lines = out.splitlines()
+    for i, l in enumerate(lines):
+        if l.strip() in (header if isinstance(header, tuple) else (header,)):
+            break
+    else:
+        raise RuntimeError("no table " + header)
+    rows = []
+    for l in lines[i + 1:]:
+        s = l.split()
+        if len(s) == ncol:
+            try:
+                rows.append(_floats(l))
+                continue
+            except ValueError:
+                pass
+        if rows:
+            break
+    return np.array(rows)
+
+
+def fmt(x):
+    return repr(float(x))
+
+
+def write_1d_file(x, psi, v):
+    s = ["# Eigenvector:"]
+    s += [f" {fmt(a)}   {fmt(b)}" for a, b in zip(x, psi)]
+    s += ["# Final potential values:"]
+    s += [f" {fmt(a)}   {fmt(b)}" for a, b in zip(x, v)]
+    return "\n".join(s) + "\n"
+
+
+def write_2d_file(x, y, psi, v):
+    # rows "y x value" with x fastest (rdpte.f reads (XI(I), I=ND,1,-1), V)
+    s = ["# Eigenvector:"]
+    for j, yy in enumerate(y):
+        for i, xx in enumerate(x):
+            s.append(f" {fmt(yy)}  {fmt(xx)}   {fmt(psi[j, i])}")
+    s.append("# Final potential values:")
+    for j, yy in enumerate(y):
+        for i, xx in enumerate(x):
+            s.append(f" {fmt(yy)}  {fmt(xx)}   {fmt(v[j, i])}")
+    return "\n".join(s) + "\n"
+
+
+DECK = """*** eSPec input file ***
+========================
+**MAIN
+*TITLE
+ golden fixture {title}
+*DIMENSION
+{dim}
+ {np}/
+*POTENTIAL
+.FILE
+wf_pot.inp
+*MASS
+ {mass}/
+*TPCALC
+.SPECTRUM
+.TD
+*INIEIGVC
+.GETR
+*CHANGE
+.YES
+*SHIFT_POTENTIAL
+.NO
+*PRTCRL
+.PARTIAL
+
+**TD
+*PROPAG
+{prop}
+ 0.0  {tf}  {dt}{mp}/
+*PRPGSTATE
+ 0/
+*TPTRANS
+.ONE
+*PRPTOL
+ 1D3/
+{absorb}
+**SPECTRUM
+*FOURIER
+ {mf}/
+*WINDOWING
+.SG
+ 1D-3/
+**END
+"""
+
+
+def morse1d_inputs():
+    n = 1024
+    x = 0.5 + np.arange(n) * (7.5 / 1023)
+    v = 0.17 * (1 - np.exp(-1.0 * (x - 1.4))) ** 2
+    psi = np.exp(-((x - 1.8) ** 2) / (2 * 0.2 ** 2))
+    psi = psi / np.sqrt(np.sum(psi ** 2))
+    # round-trip through the text the executable reads
+    x = np.array([float(fmt(a)) for a in x])
+    v = np.array([float(fmt(a)) for a in v])
+    psi = np.array([float(fmt(a)) for a in psi])
+    return x, psi, v
+
+
+def morse2d_inputs():
+    nx, ny = 32, 32
+    x = 1.0 + np.arange(nx) * (1.0 / (nx - 1))
+    y = 1.2 + np.arange(ny) * (1.2 / (ny - 1))
+    X, Y = np.meshgrid(x, y)  # [j, i]
+    v = (0.17 * (1 - np.exp(-1.0 * (X - 1.4))) ** 2 + 0.12 * (1 - np.exp(-1.2 * (Y - 1.8))) ** 2
+         + 0.01 * (X - 1.4) * (Y - 1.8))
+    psi = np.exp(-((X - 1.5) ** 2) / (2 * 0.1 ** 2) - ((Y - 1.8) ** 2) / (2 * 0.12 ** 2))
+    psi = psi / np.sqrt(np.sum(psi ** 2))
+    r = lambda a: np.vectorize(lambda t: float(fmt(t)))(a)
+    return r(x), r(y), r(psi), r(v)
+
+
+def case_morse1d(name, prop, absorb_block, absorb_meta):
+    x, psi, v = morse1d_inputs()
+    dt_fs = 0.005 * SHFS
+    nsteps = 2048
+    tf = nsteps * dt_fs
+    mass_amu = 918.0 / AMU
+    mp = "  10" if prop == ".PSIL" else ""
+    deck = DECK.format(title=name, dim=".1D", np="1024", mass=fmt(mass_amu), prop=prop,
+                       tf=fmt(tf), dt=fmt(dt_fs), mp=mp, absorb=absorb_block, mf=12)
+    out = run_deck(deck, {"wf_pot.inp": write_1d_file(x, psi, v)})
+    rows = parse_partial(out)
+    corr = parse_table(out, "*t/fs*       *C(t)r*       *C(t)i*", 3)
+    spec = parse_table(out, "*E (eV)*           *W*           *FFTr*          *FFTi*", 4)
+    meta = dict(kind="morse1d", prop=prop, np=[1024], dt_fs=dt_fs, tf_fs=tf, mass_amu=mass_amu,
+                mp=10, mf=12, window="SG", wp=1e-3, **absorb_meta)
+    # x, psi, v are regenerated by morse1d_inputs(); the energy axis of the
+    # spectrum overflows its F12.7 field at this dt, so only C(t) is kept.
+    arrays = dict(rows=rows)
+    if name in ("morse1d_sod", "morse1d_spo_voptic"):
+        # total C(t) table (espec.f:1545-1576).  Not kept for .PSIL: there the
+        # reference stores C(t) past the end of its LNZVC array and the table
+        # is corrupted before it is printed.
+        arrays["corr"] = corr
+    if name == "morse1d_sod":
+        arrays.update(x=x, psi=psi, v=v)
+    return meta, arrays
+
+
+def case_morse2d(name, prop):
+    x, y, psi, v = morse2d_inputs()
+    dt_fs = 0.005 * SHFS
+    nsteps = 512
+    tf = nsteps * dt_fs
+    m1, m2 = 918.0 / AMU, 1500.0 / AMU
+    mp = "  10" if prop == ".PSIL" else ""
+    deck = DECK.format(title=name, dim=".2D", np="32 32", mass=f"{fmt(m1)} {fmt(m2)}", prop=prop,
+                       tf=fmt(tf), dt=fmt(dt_fs), mp=mp, absorb="", mf=10)
+    out = run_deck(deck, {"wf_pot.inp": write_2d_file(x, y, psi, v)})
+    rows = parse_partial(out)
+    meta = dict(kind="morse2d", prop=prop, np=[32, 32], dt_fs=dt_fs, tf_fs=tf,
+                mass_amu=[m1, m2], mp=10, mf=10)
+    return meta, dict(x=x, y=y, psi=psi, v=v, rows=rows)
+
+
+def case_test4():
+    tt = os.path.join(REF, "ttests")
+    deck = open(os.path.join(tt, "input.test4")).read()
+    out = run_deck(deck, {"eigpot_test3.inp": os.path.join(tt, "eigpot_test3.inp")})
+    rows = parse_partial(out)
+    lines = open(os.path.join(tt, "eigpot_test3.inp")).read().splitlines()
+    data = [_floats(l) for l in lines if l.strip() and not l.startswith("#")]
+    data = np.array(data)
+    x, psi, v = data[:201, 0], data[:201, 1], data[201:402, 1]
+    golden_v04 = parse_partial(open(os.path.join(tt, "results.test4")).read())
+    meta = dict(kind="test4", prop=".PSIL", np=[201], mass_amu=7.49, ti_fs=0.0, tf_fs=250.0,
+                dt_fs=2e-3, mp=10, change=True, mf=12, hwhm=[0.087, 0.0, 0.12, 19.562],
+                shiftp=True, tol=3.0)
+    # the total C(t) and spectrum of this run are not kept: the reference
+    # stores C(t) past the end of its LNZVC array (MP+1 > LMTREORT) and the
+    # .PSIL path overwrites some of those samples before they are assembled
+    return meta, dict(x=x, psi=psi, v=v, rows=rows, rows_v04=golden_v04)
+
+
+def case_test8():
+    tt = os.path.join(REF, "ttests")
+    deck = open(os.path.join(tt, "input.test8")).read()
+    out = run_deck(deck, {"correl8.inp": os.path.join(tt, "correl8.inp")})
+    spec = parse_table(out, "*E (eV)*           *W*           *FFTr*          *FFTi*", 4)
+    cin = parse_table(open(os.path.join(tt, "correl8.inp")).read(),
+                      "*t/fs*       *C(t)r*       *C(t)i*", 3)
+    gold = parse_table(open(os.path.join(tt, "results.test8")).read(),
+                       ("*E/eV*           *W*           *FFTr*          *FFTi*",), 4)
+    meta = dict(kind="test8", mf=13, hwhm=[0.08, 0.0, 0.0, 0.0], window="NONE",
+                executable_equals_committed_golden=bool(np.array_equal(spec, gold)))
+    arrays = dict(cin=cin, spec_golden=gold)
+    if not np.array_equal(spec, gold):
+        arrays["spec"] = spec
+    return meta, arrays
+
+
+VOPTIC = """*ABSORBING
+.VOPTIC_POLIN
+ -0.02  2.0  0.0/
+ 1.6  2.2  0.0 0.0 0.0 0.0/
+"""
+SMOOTH = """*ABSORBING
+.SMOOTHW
+ 0.05  1.0  0.0/
+ 1.55  2.3  0.0 0.0 0.0 0.0/
+"""
+
+
+def main():
+    if not os.path.exists(BIN):
+        sys.exit("eSPec executable not found at " + BIN)
+    cases = {}
+    cases["test8"] = case_test8()
+    cases["test4"] = case_test4()
+    for prop, tag in [(".PFSOD", "sod"), (".PFSPO", "spo"), (".PSIL", "sil")]:
+        cases[f"morse1d_{tag}"] = case_morse1d(f"morse1d_{tag}", prop, "", {})
+    vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
+    smeta = dict(absorb="SMOOTHW", voi=[0.05, 1.0], al=1.55, ar=2.3)
+    for prop, tag in [(".PFSOD", "sod"), (".PFSPO", "spo")]:
+        cases[f"morse1d_{tag}_voptic"] = case_morse1d(f"morse1d_{tag}_voptic", prop, VOPTIC, vmeta)
+    for prop, tag in [(".PFSOD", "sod"), (".PFSPO", "spo"), (".PSIL", "sil")]:
+        cases[f"morse1d_{tag}_smooth"] = case_morse1d(f"morse1d_{tag}_smooth", prop, SMOOTH, smeta)
+    for prop, tag in [(".PSIL", "sil"), (".PFSPO", "spo"), (".PFSOD", "sod")]:
+        cases[f"morse2d_{tag}"] = case_morse2d(f"morse2d_{tag}", prop)
+    manifest = {}
+    for name, (meta, arrays) in cases.items():
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+        manifest[name] = meta
+        print(name, {k: getattr(a, "shape", None) for k, a in arrays.items()})
+    with open(os.path.join(OUT, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+    main()
