@@ -1,0 +1,280 @@
+#!/usr/bin/env python3
+"""Benchmark: batched 1D Morse scan, mixed precision, one persistent launch.
+
+Workload (one "step" = one full propagation of the batch): 4096 independent
+1D Morse packets with N ~ U{256,384,512,768,1024,1536,2048} on [0.5, 8] bohr,
+De ~ U[0.05,0.25] Eh, a ~ U[0.6,1.6] /bohr, re ~ U[1.0,2.5] bohr,
+m ~ U[900,30000] m_e, Gaussian packets, dt = 0.5 au, 8000 time steps, C(t)
+recorded every time step (seed 20261203).  Metric: grid-point time steps per
+second (Mgridpt*steps/s) over the whole job; packets/s reported beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision mixed|fp64] [--npk 4096] [--nsteps 8000]
+
+Multi-GPU (torchrun): packets are independent, each rank propagates its own
+batch (seed + rank) with no collective on the data path -> weak scaling.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Mgridpt*steps/s (batched 1D Morse scan, mixed precision, C(t) every step)"
+ALG_BYTES = {"mixed": 28.0, "fp64": 56.0}  # per grid point per time step
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--npk", type=int, default=4096)
+    ap.add_argument("--nsteps", type=int, default=8000)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--cpu-sample-steps", type=int, default=400)
+    ap.add_argument("--cpu-sample-packets", type=int, default=256)
+    return ap.parse_args()
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._th = None
+
+    def _run(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._th = threading.Thread(target=self._run, daemon=True)
+        self._th.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._th.join(timeout=10)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """CPU reference arm: the oracle port of spofft.f/pspofft.f on all host
+    cores, on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    from espec_b200 import workloads as W
+    from oracle import oracle as O
+
+    w = W.morse_scan(npk=args.cpu_sample_packets, nsteps=args.cpu_sample_steps)
+    cores = os.cpu_count() or 1
+    rates = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        O.spo_batch(w["off"], w["sh"], w["sm"], w["vpot"], w["psi"], np.zeros_like(w["psi"]),
+                    w["dt_fs"], w["nsteps"], nthreads=cores)
+        dt = time.perf_counter() - t0
+        if it >= args.warmup:
+            rates.append(w["off"][-1] * w["nsteps"] / dt / 1e6)
+    v = float(np.median(rates))
+    sample = (f"{w['npk']} packets x {w['nsteps']} time steps of the scan workload per step "
+              f"({int(w['off'][-1])} grid points)")
+    line = {"metric": METRIC, "value": v, "unit": "Mgridpt*steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "impl": "reference", "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "morse_scan_1d", "npk": args.npk, "nsteps": args.nsteps},
+            "cpu_baseline": {"value": v, "unit": "Mgridpt*steps/s", "cores": cores,
+                             "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "Mgridpt*steps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+            "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+
+
+def cpu_baseline(args):
+    from espec_b200 import workloads as W
+    from oracle import oracle as O
+
+    w = W.morse_scan(npk=args.cpu_sample_packets, nsteps=args.cpu_sample_steps)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    O.spo_batch(w["off"], w["sh"], w["sm"], w["vpot"], w["psi"], np.zeros_like(w["psi"]),
+                w["dt_fs"], w["nsteps"], nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": float(w["off"][-1] * w["nsteps"] / dt / 1e6), "unit": "Mgridpt*steps/s",
+            "cores": cores, "kind": "port",
+            "sample": f"{w['npk']} packets x {w['nsteps']} time steps of the scan workload"}
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_init(args)
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    import torch
+
+    import espec_b200 as E
+    from espec_b200 import workloads as W
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    w = W.morse_scan(npk=args.npk, nsteps=args.nsteps, seed=20261203 + rank)
+    pts_steps = float(w["off"][-1]) * w["nsteps"]
+    stream = torch.cuda.current_stream(dev)
+    sh = stream.cuda_stream
+    b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision=args.precision)
+    # inputs resident in HBM before timing
+    vpot_d = torch.from_numpy(w["vpot"]).to(dev)
+    psi_d = torch.from_numpy(w["psi"]).to(dev)
+    zero_d = torch.zeros_like(psi_d)
+    b.load(vpot_d, (psi_d, zero_d), stream=sh)
+    torch.cuda.synchronize()
+
+    def one_step():
+        b.load(vpot_d, (psi_d, zero_d), stream=sh)  # tables rebuilt from resident inputs
+        b.run(w["nsteps"], stream=sh)
+
+    for _ in range(args.warmup):
+        one_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            one_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+        torch.distributed.barrier()
+    value = pts_steps * world / (ms * 1e-3) / 1e6
+    launches = len(set(int(x) for x in w["n"])) + 1  # class kernels + set-up kernel
+
+    # roofline of the propagation kernels (algorithmic bytes per launch group)
+    peak, peak_kind = measured_peaks()
+    ev2 = torch.cuda.Event(enable_timing=True)
+    ev3 = torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
+    for _ in range(args.steps):
+        b.run(w["nsteps"], stream=sh)
+    ev3.record(stream)
+    torch.cuda.synchronize()
+    kms = ev2.elapsed_time(ev3) / args.steps
+    alg = ALG_BYTES[args.precision] * pts_steps
+    achieved = alg / (kms * 1e-3) / 1e9
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+            "kernel": "spo1d_kernel (7 size classes, concurrent streams)",
+            "kernel_ms": kms}
+
+    # end-to-end through the C-ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        vh, ph = w["vpot"], w["psi"]
+        c_host = None
+        t_e = []
+        for it in range(1 + min(args.steps, 3)):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            b.load(vh, ph)
+            b.run(w["nsteps"], stream=None)
+            c_host, _ = b.results()
+            t1 = time.perf_counter()
+            if it > 0:
+                t_e.append(t1 - t0)
+        h2d = w["vpot"].nbytes + 2 * w["psi"].nbytes
+        d2h = c_host.nbytes + 16 * int(w["off"][-1])
+        e2e = {"value": pts_steps * world / float(np.median(t_e)) / 1e6, "unit": "Mgridpt*steps/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "timing": "host wall clock around load+run+results (max over ranks not taken)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mgridpt*steps/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
+                "config": {"workload": "morse_scan_1d", "npk": args.npk, "nsteps": args.nsteps,
+                           "precision": args.precision, "parallelism": f"packets x {world} GPU",
+                           "l2": "tables and C(t) output exceed L2 (126 MB)",
+                           "packets_per_s": args.npk * world / (ms * 1e-3)},
+                "roofline": roof, "cpu_baseline": cpu_baseline(args) if world == 1 else None,
+                "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    b.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

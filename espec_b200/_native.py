@@ -1,0 +1,81 @@
+"""ctypes binding of libespecgpu.so (the C-ABI declared in include/espec_gpu.h).
+
+There is no CPU fallback: if the library or a CUDA device is missing every
+entry point raises EspecError.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libespecgpu.so")
+
+OK, EINVAL, ECUDA, ENOMEM = 0, -1, -2, -3
+FP64, MIXED = 0, 1
+ABS_NONE, ABS_VOPTIC, ABS_SMOOTHW = 0, 1, 2
+Q_SPO_INPLACE = 1
+MEM_HOST, MEM_DEVICE = 0, 1
+SHFS = 2.4188843243e-2
+
+# every symbol the header declares (checked by the CPU test suite)
+EXPORTS = [
+    "espec_last_error", "espec_version", "espec_device_ok",
+    "espec_spo_create", "espec_spo_load", "espec_spo_run", "espec_spo_results",
+    "espec_spo_device_c", "espec_spo_npoints", "espec_spo_destroy",
+]
+
+
+class EspecError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load():
+    """Load the in-tree library (building it first if sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        from . import build as _b
+        _b.build()
+    lib = C.CDLL(LIB_PATH)
+    d, i, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+    lib.espec_last_error.restype = C.c_char_p
+    lib.espec_version.restype = C.c_char_p
+    lib.espec_device_ok.restype = C.c_int
+    lib.espec_spo_create.argtypes = [C.POINTER(vp), C.c_int, i, d, d, C.c_double, C.c_int,
+                                     C.c_int, C.c_int]
+    lib.espec_spo_load.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]
+    lib.espec_spo_run.argtypes = [vp, C.c_int, vp]
+    lib.espec_spo_results.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]
+    lib.espec_spo_device_c.argtypes = [vp]
+    lib.espec_spo_device_c.restype = vp
+    lib.espec_spo_npoints.argtypes = [vp]
+    lib.espec_spo_destroy.argtypes = [vp]
+    lib.espec_spo_destroy.restype = None
+    _lib = lib
+    return lib
+
+
+def check(rc, what):
+    if rc != OK:
+        msg = load().espec_last_error().decode(errors="replace")
+        raise EspecError(f"{what} failed ({rc}): {msg}")
+
+
+def ptr(a):
+    """Address of a numpy array, a torch tensor or an int (device pointer)."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)

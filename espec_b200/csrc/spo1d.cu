@@ -1,0 +1,539 @@
+// spo1d.cu -- batched 1D split-operator plans: table set-up, launches and
+// the C-ABI entry points declared in include/espec_gpu.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "espec_gpu.h"
+#include "espec_internal.h"
+#include "spo1d.cuh"
+
+namespace espec {
+
+// ---------------------------------------------------------------------------
+// host-side index logic
+// ---------------------------------------------------------------------------
+// Frequency (FFT-order index) held at each final position of the DIF sequence
+// of plan PL: kappa_M(j) = R * kappa_{M/R}(j mod M/R) + j / (M/R).
+template <class PL>
+static std::vector<int> final_freq() {
+  std::vector<int> kap(PL::N);
+  for (int j = 0; j < PL::N; ++j) {
+    int f = 0, mult = 1, rem = j, M = PL::N;
+    // unroll the recursion from the outermost stage
+    std::vector<int> digits;
+    for (int s = 0; s < PL::S; ++s) {
+      const int R = PL::r[s];
+      const int m = M / R;
+      digits.push_back(rem / m);
+      rem = rem % m;
+      M = m;
+    }
+    // kappa = k'_0 + R_0 (k'_1 + R_1 (k'_2 + ...))
+    for (int s = 0; s < PL::S; ++s) {
+      f += digits[s] * mult;
+      mult *= PL::r[s];
+    }
+    kap[j] = f;
+  }
+  return kap;
+}
+
+// dkeft.f:64-79 (DIGT, 1D): TC(k) = p^2 / (2 m) in FFT order with the
+// reference's truncated 2 pi and p accumulated by repeated addition.
+static void digt_1d(int n, double sh, double sm, double* tc) {
+  const double twopi = 6.283185307;
+  const double dp = twopi / (n * sh);
+  double p = 0.0;
+  for (int i = 0; i < n / 2; ++i) {
+    tc[i] = p * p / (2.0 * sm);
+    p = p + dp;
+  }
+  p = -p;
+  for (int i = n / 2; i < n; ++i) {
+    tc[i] = p * p / (2.0 * sm);
+    p = p + dp;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// set-up kernel: FP64 phase generation with one argument reduction per value
+// ---------------------------------------------------------------------------
+struct SetupArgs {
+  const double* vpot;
+  const double* vabc;
+  const double2* psi0;
+  const double* tc;    // FFT order per packet
+  const int* kperm;    // per point: FFT index held at this final position
+  const int* pk_of;    // packet index of each point
+  const int* pk_off;   // first point of each packet
+  const double* kscale;  // per packet scale of the kinetic table
+  int npts;
+  double cst1, cst2;   // dt/SHFS, dt/(2 SHFS)
+  int absorb;          // ESPEC_ABS_*
+  int fp32;
+  // outputs (one of the two sets)
+  cpx<double>* g64;
+  cpx<double>* h64;
+  cpx<double>* hm64;
+  cpx<double>* k64;
+  cpx<double>* w64;
+  Tab<float>::phase_t* g32;
+  Tab<float>::phase_t* h32;
+  Tab<float>::phase_t* hm32;
+  Tab<float>::phase_t* k32;
+  cpx<float>* w32;
+  double* kq_c;
+  double* kq_s;
+};
+
+__device__ __forceinline__ Tab<float>::phase_t phase32(double phi, double a) {
+  RotF r = make_rotf(phi);
+  Tab<float>::phase_t o;
+  o.t = r.t;
+  o.s = r.s;
+  o.g = r.g;
+  o.a = (float)a;
+  return o;
+}
+
+__global__ void spo_setup_kernel(SetupArgs a) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.npts) return;
+  const int pk = a.pk_of[x];
+  const int base = a.pk_off[pk];
+  // x-space factors.  h = e^{-i cst2 V} (x e^{cst2 VABC} for .VOPTIC)
+  const double th = a.cst2 * a.vpot[x];
+  double hmag = 1.0, mask = 1.0;
+  if (a.absorb == ESPEC_ABS_VOPTIC) hmag = exp(a.cst2 * a.vabc[x]);
+  if (a.absorb == ESPEC_ABS_SMOOTHW) mask = a.vabc[x];
+  double sh, ch, s2, c2;
+  sincos(th, &sh, &ch);
+  sincos(2.0 * th, &s2, &c2);
+  const double gmag = hmag * hmag * mask;
+  const double2 p0 = a.psi0[x];
+  // w = conj(psi0) * mask * h
+  const double hr = ch * hmag * mask, hi = -sh * hmag * mask;
+  const double wr = p0.x * hr + p0.y * hi, wi = p0.x * hi - p0.y * hr;
+  // kinetic factor at this final position
+  const int f = x - base;
+  const int kidx = base + a.kperm[x];
+  const double tk = a.cst1 * a.tc[kidx];
+  double sk, ck;
+  sincos(tk, &sk, &ck);
+  const double ks = a.kscale[pk];
+  if (a.fp32) {
+    a.g32[x] = phase32(-2.0 * th, gmag);
+    a.h32[x] = phase32(-th, hmag);
+    a.hm32[x] = phase32(-th, hmag * mask);
+    a.k32[x] = phase32(-tk, ks);
+    a.w32[x] = mk((float)wr, (float)wi);
+  } else {
+    a.g64[x] = mk(c2 * gmag, -s2 * gmag);
+    a.h64[x] = mk(ch * hmag, -sh * hmag);
+    a.hm64[x] = mk(ch * hmag * mask, -sh * hmag * mask);
+    a.k64[x] = mk(ck * ks, -sk * ks);
+    a.w64[x] = mk(wr, wi);
+    if (a.kq_c) {
+      a.kq_c[x] = ck;
+      a.kq_s[x] = sk;
+    }
+  }
+  (void)f;
+}
+
+// ---------------------------------------------------------------------------
+// per-size-class dispatch
+// ---------------------------------------------------------------------------
+template <typename R, class PL, bool kCap, bool kQuirk>
+static cudaError_t launch_class(const SpoArgs<R>& a, int nblocks, cudaStream_t st) {
+  auto kern = spo1d_kernel<R, PL, kCap, kQuirk>;
+  const size_t smem = spo1d_smem_bytes<R, PL>();
+  static bool attr_set = false;  // per instantiation
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  kern<<<nblocks, PL::T, smem, st>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename R, class PL>
+static cudaError_t launch_any(const SpoArgs<R>& a, int nblocks, bool quirk, cudaStream_t st) {
+  if constexpr (sizeof(R) == 8) {
+    if (quirk) return launch_class<R, PL, false, true>(a, nblocks, st);
+  }
+  return launch_class<R, PL, false, false>(a, nblocks, st);
+}
+
+template <typename R>
+static cudaError_t launch_n(int n, const SpoArgs<R>& a, int nblocks, bool quirk, cudaStream_t st) {
+  switch (n) {
+    case 256: return launch_any<R, DefaultPlan<256>::type>(a, nblocks, quirk, st);
+    case 384: return launch_any<R, DefaultPlan<384>::type>(a, nblocks, quirk, st);
+    case 512: return launch_any<R, DefaultPlan<512>::type>(a, nblocks, quirk, st);
+    case 768: return launch_any<R, DefaultPlan<768>::type>(a, nblocks, quirk, st);
+    case 1024: return launch_any<R, DefaultPlan<1024>::type>(a, nblocks, quirk, st);
+    case 1536: return launch_any<R, DefaultPlan<1536>::type>(a, nblocks, quirk, st);
+    case 2048: return launch_any<R, DefaultPlan<2048>::type>(a, nblocks, quirk, st);
+    case 4096: return launch_any<R, DefaultPlan<4096>::type>(a, nblocks, quirk, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+
+static bool size_supported(int n) {
+  switch (n) {
+    case 256: case 384: case 512: case 768: case 1024: case 1536: case 2048: case 4096:
+      return true;
+    default:
+      return false;
+  }
+}
+
+template <class PL>
+static void fill_plan_info(int n, std::vector<int>& kap, int& n3) {
+  kap = final_freq<PL>();
+  n3 = PL::n3();
+  (void)n;
+}
+
+static void plan_info(int n, std::vector<int>& kap, int& n3) {
+  switch (n) {
+    case 256: fill_plan_info<DefaultPlan<256>::type>(n, kap, n3); break;
+    case 384: fill_plan_info<DefaultPlan<384>::type>(n, kap, n3); break;
+    case 512: fill_plan_info<DefaultPlan<512>::type>(n, kap, n3); break;
+    case 768: fill_plan_info<DefaultPlan<768>::type>(n, kap, n3); break;
+    case 1024: fill_plan_info<DefaultPlan<1024>::type>(n, kap, n3); break;
+    case 1536: fill_plan_info<DefaultPlan<1536>::type>(n, kap, n3); break;
+    case 2048: fill_plan_info<DefaultPlan<2048>::type>(n, kap, n3); break;
+    case 4096: fill_plan_info<DefaultPlan<4096>::type>(n, kap, n3); break;
+    default: break;
+  }
+}
+
+}  // namespace espec
+
+// ---------------------------------------------------------------------------
+// plan object behind the C-ABI
+// ---------------------------------------------------------------------------
+using namespace espec;
+
+struct espec_spo_plan {
+  int npk = 0, npts = 0, precision = 0, absorb = 0, quirks = 0;
+  double dt_fs = 0.0;
+  std::vector<int> n, off;
+  std::vector<double> sh, sm;
+  struct Class {
+    int n;
+    int count;
+    SpoPacket* d_pk;
+  };
+  std::vector<Class> classes;
+  std::vector<cudaStream_t> streams;
+  std::vector<cudaEvent_t> events;
+  cudaEvent_t ev_fork = nullptr;
+  // device buffers
+  double* d_vpot = nullptr;
+  double* d_vabc = nullptr;
+  double2* d_psi0 = nullptr;
+  double2* d_psi = nullptr;
+  double* d_tc = nullptr;
+  int* d_kperm = nullptr;
+  int* d_pk_of = nullptr;
+  int* d_pk_off = nullptr;
+  double* d_kscale = nullptr;
+  void* d_tab = nullptr;
+  size_t tab_bytes = 0;
+  double2* d_c = nullptr;
+  int c_cap_steps = -1;  // nsteps the C(t) buffer was sized for
+  double* d_kq_c = nullptr;
+  double* d_kq_s = nullptr;
+  bool loaded = false;
+  // tables (sub-pointers of d_tab)
+  SpoTables<double> t64{};
+  SpoTables<float> t32{};
+};
+
+static void plan_free(espec_spo_plan* p) {
+  for (auto& c : p->classes) cudaFree(c.d_pk);
+  for (auto s : p->streams) cudaStreamDestroy(s);
+  for (auto e : p->events) cudaEventDestroy(e);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  void* bufs[] = {p->d_vpot, p->d_vabc, p->d_psi0, p->d_psi, p->d_tc, p->d_kperm, p->d_pk_of,
+                  p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s};
+  for (void* b : bufs)
+    if (b) cudaFree(b);
+}
+
+#define ESPEC_CK(call)                                           \
+  do {                                                           \
+    cudaError_t e_ = (call);                                     \
+    if (e_ != cudaSuccess) return set_cuda_error(#call, e_);     \
+  } while (0)
+
+extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
+                                const double* sh, const double* sm, double dt_fs, int precision,
+                                int absorb, int quirks) {
+  if (!out || npk <= 0 || !npts || !sh || !sm) return set_error(ESPEC_EINVAL, "null argument");
+  if (precision != ESPEC_FP64 && precision != ESPEC_MIXED)
+    return set_error(ESPEC_EINVAL, "precision must be ESPEC_FP64 or ESPEC_MIXED");
+  if (precision == ESPEC_MIXED && (quirks & ESPEC_Q_SPO_INPLACE))
+    return set_error(ESPEC_EINVAL, "the reference-defect mode exists for FP64 only");
+  if (absorb < ESPEC_ABS_NONE || absorb > ESPEC_ABS_SMOOTHW)
+    return set_error(ESPEC_EINVAL, "unknown absorber type");
+  auto* p = new espec_spo_plan;
+  p->npk = npk;
+  p->precision = precision;
+  p->absorb = absorb;
+  p->quirks = quirks;
+  p->dt_fs = dt_fs;
+  p->n.assign(npts, npts + npk);
+  p->sh.assign(sh, sh + npk);
+  p->sm.assign(sm, sm + npk);
+  p->off.resize(npk + 1);
+  p->off[0] = 0;
+  for (int i = 0; i < npk; ++i) {
+    if (!size_supported(p->n[i])) {
+      delete p;
+      return set_error(ESPEC_EINVAL, "unsupported packet size (supported: 256, 384, 512, 768, "
+                                     "1024, 1536, 2048, 4096)");
+    }
+    p->off[i + 1] = p->off[i] + p->n[i];
+  }
+  p->npts = p->off[npk];
+  int rc = 0;
+  auto fail = [&](int code) {
+    plan_free(p);
+    delete p;
+    return code;
+  };
+  // size classes, largest first so that the longest CTAs start first
+  std::map<int, std::vector<SpoPacket>, std::greater<int>> cls;
+  for (int i = 0; i < npk; ++i) cls[p->n[i]].push_back(SpoPacket{p->off[i], 0});
+  for (auto& kv : cls) {
+    espec_spo_plan::Class c{kv.first, (int)kv.second.size(), nullptr};
+    if ((rc = ck(cudaMalloc(&c.d_pk, sizeof(SpoPacket) * c.count), "cudaMalloc"))) return fail(rc);
+    p->classes.push_back(c);
+    cudaStream_t s;
+    if ((rc = ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream"))) return fail(rc);
+    p->streams.push_back(s);
+    cudaEvent_t e;
+    if ((rc = ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event"))) return fail(rc);
+    p->events.push_back(e);
+  }
+  if ((rc = ck(cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming), "event")))
+    return fail(rc);
+  const size_t np = p->npts;
+  if ((rc = ck(cudaMalloc(&p->d_vpot, np * 8), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_vabc, np * 8), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_psi0, np * 16), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_psi, np * 16), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_tc, np * 8), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_kperm, np * 4), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_pk_of, np * 4), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_pk_off, npk * 4), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_kscale, npk * 8), "cudaMalloc"))) return fail(rc);
+  if (precision == ESPEC_FP64) {
+    p->tab_bytes = np * 16 * 5;
+  } else {
+    p->tab_bytes = np * (16 * 4 + 8);
+  }
+  if ((rc = ck(cudaMalloc(&p->d_tab, p->tab_bytes), "cudaMalloc"))) return fail(rc);
+  if (quirks & ESPEC_Q_SPO_INPLACE) {
+    if ((rc = ck(cudaMalloc(&p->d_kq_c, np * 8), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_kq_s, np * 8), "cudaMalloc"))) return fail(rc);
+  }
+  char* tb = (char*)p->d_tab;
+  if (precision == ESPEC_FP64) {
+    auto* c = (cpx<double>*)tb;
+    p->t64.g = c;
+    p->t64.h = c + np;
+    p->t64.hm = c + 2 * np;
+    p->t64.k = c + 3 * np;
+    p->t64.w = c + 4 * np;
+  } else {
+    auto* c = (Tab<float>::phase_t*)tb;
+    p->t32.g = c;
+    p->t32.h = c + np;
+    p->t32.hm = c + 2 * np;
+    p->t32.k = c + 3 * np;
+    p->t32.w = (cpx<float>*)(c + 4 * np);
+  }
+  // host-built index tables: DIGT, final-position frequencies, packet ids
+  std::vector<double> tc(np), kscale(npk);
+  std::vector<int> kperm(np), pk_of(np);
+  std::map<int, std::pair<std::vector<int>, int>> kap_cache;
+  for (int i = 0; i < npk; ++i) {
+    const int n = p->n[i];
+    digt_1d(n, p->sh[i], p->sm[i], tc.data() + p->off[i]);
+    auto it = kap_cache.find(n);
+    if (it == kap_cache.end()) {
+      std::vector<int> kap;
+      int n3 = 0;
+      plan_info(n, kap, n3);
+      it = kap_cache.emplace(n, std::make_pair(kap, n3)).first;
+    }
+    for (int j = 0; j < n; ++j) {
+      kperm[p->off[i] + j] = it->second.first[j];
+      pk_of[p->off[i] + j] = i;
+    }
+    // round trip gain: N, divided by 3 per unitary radix-3 stage of the FP32 form
+    double gain = n;
+    if (precision == ESPEC_MIXED)
+      for (int k = 0; k < it->second.second; ++k) gain /= 3.0;
+    kscale[i] = 1.0 / gain;
+  }
+  if ((rc = ck(cudaMemcpy(p->d_tc, tc.data(), np * 8, cudaMemcpyHostToDevice), "H2D"))) return fail(rc);
+  if ((rc = ck(cudaMemcpy(p->d_kperm, kperm.data(), np * 4, cudaMemcpyHostToDevice), "H2D")))
+    return fail(rc);
+  if ((rc = ck(cudaMemcpy(p->d_pk_of, pk_of.data(), np * 4, cudaMemcpyHostToDevice), "H2D")))
+    return fail(rc);
+  if ((rc = ck(cudaMemcpy(p->d_pk_off, p->off.data(), npk * 4, cudaMemcpyHostToDevice), "H2D")))
+    return fail(rc);
+  if ((rc = ck(cudaMemcpy(p->d_kscale, kscale.data(), npk * 8, cudaMemcpyHostToDevice), "H2D")))
+    return fail(rc);
+  *out = p;
+  return ESPEC_OK;
+}
+
+extern "C" void espec_spo_destroy(espec_spo_plan* p) {
+  if (!p) return;
+  plan_free(p);
+  delete p;
+}
+
+extern "C" int espec_spo_npoints(const espec_spo_plan* p) { return p ? p->npts : -1; }
+
+// set-up of all tables from state already in the plan's device buffers
+static int spo_build_tables(espec_spo_plan* p, cudaStream_t st) {
+  SetupArgs a{};
+  a.vpot = p->d_vpot;
+  a.vabc = p->d_vabc;
+  a.psi0 = p->d_psi0;
+  a.tc = p->d_tc;
+  a.kperm = p->d_kperm;
+  a.pk_of = p->d_pk_of;
+  a.pk_off = p->d_pk_off;
+  a.kscale = p->d_kscale;
+  a.npts = p->npts;
+  a.cst1 = p->dt_fs / ESPEC_SHFS;
+  a.cst2 = p->dt_fs / (2.0 * ESPEC_SHFS);
+  a.absorb = p->absorb;
+  a.fp32 = p->precision == ESPEC_MIXED;
+  a.g64 = const_cast<cpx<double>*>(p->t64.g);
+  a.h64 = const_cast<cpx<double>*>(p->t64.h);
+  a.hm64 = const_cast<cpx<double>*>(p->t64.hm);
+  a.k64 = const_cast<cpx<double>*>(p->t64.k);
+  a.w64 = const_cast<cpx<double>*>(p->t64.w);
+  a.g32 = const_cast<Tab<float>::phase_t*>(p->t32.g);
+  a.h32 = const_cast<Tab<float>::phase_t*>(p->t32.h);
+  a.hm32 = const_cast<Tab<float>::phase_t*>(p->t32.hm);
+  a.k32 = const_cast<Tab<float>::phase_t*>(p->t32.k);
+  a.w32 = const_cast<cpx<float>*>(p->t32.w);
+  a.kq_c = p->d_kq_c;
+  a.kq_s = p->d_kq_s;
+  const int bs = 256;
+  spo_setup_kernel<<<(p->npts + bs - 1) / bs, bs, 0, st>>>(a);
+  int rc = ck(cudaGetLastError(), "spo_setup_kernel");
+  if (rc) return rc;
+  p->loaded = true;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spo_load(espec_spo_plan* p, const double* vpot, const double* vabc,
+                              const double* psi_re, const double* psi_im, int where,
+                              void* stream) {
+  if (!p || !vpot || !psi_re) return set_error(ESPEC_EINVAL, "null argument");
+  if (p->absorb != ESPEC_ABS_NONE && !vabc) return set_error(ESPEC_EINVAL, "absorber table missing");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t np = p->npts;
+  const cudaMemcpyKind kind = where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  ESPEC_CK(cudaMemcpyAsync(p->d_vpot, vpot, np * 8, kind, st));
+  if (vabc) ESPEC_CK(cudaMemcpyAsync(p->d_vabc, vabc, np * 8, kind, st));
+  // interleave (re, im) into double2
+  ESPEC_CK(cudaMemcpy2DAsync(p->d_psi0, 16, psi_re, 8, 8, np, kind, st));
+  if (psi_im) {
+    ESPEC_CK(cudaMemcpy2DAsync((char*)p->d_psi0 + 8, 16, psi_im, 8, 8, np, kind, st));
+  } else {
+    ESPEC_CK(cudaMemset2DAsync((char*)p->d_psi0 + 8, 16, 0, 8, np, st));
+  }
+  return spo_build_tables(p, st);
+}
+
+extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spo_load has not been called");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->c_cap_steps != nsteps) {
+    if (p->d_c) cudaFree(p->d_c);
+    p->d_c = nullptr;
+    ESPEC_CK(cudaMalloc(&p->d_c, sizeof(double2) * (size_t)p->npk * (nsteps + 1)));
+    p->c_cap_steps = nsteps;
+    // packet descriptors carry the C(t) offsets
+    std::map<int, std::vector<SpoPacket>> cls;
+    for (int i = 0; i < p->npk; ++i)
+      cls[p->n[i]].push_back(SpoPacket{p->off[i], i * (nsteps + 1)});
+    for (auto& c : p->classes) {
+      auto& v = cls[c.n];
+      ESPEC_CK(cudaMemcpy(c.d_pk, v.data(), sizeof(SpoPacket) * v.size(), cudaMemcpyHostToDevice));
+    }
+  }
+  const bool quirk = (p->quirks & ESPEC_Q_SPO_INPLACE) != 0;
+  ESPEC_CK(cudaEventRecord(p->ev_fork, st));
+  for (size_t ci = 0; ci < p->classes.size(); ++ci) {
+    auto& c = p->classes[ci];
+    cudaStream_t cs = p->streams[ci];
+    ESPEC_CK(cudaStreamWaitEvent(cs, p->ev_fork, 0));
+    cudaError_t e;
+    if (p->precision == ESPEC_FP64) {
+      SpoArgs<double> a{};
+      a.tab = p->t64;
+      a.pk = c.d_pk;
+      a.psi0 = p->d_psi0;
+      a.psi_out = p->d_psi;
+      a.c_out = p->d_c;
+      a.kq_c = p->d_kq_c;
+      a.kq_s = p->d_kq_s;
+      a.kq_scale = 1.0 / c.n;
+      a.nsteps = nsteps;
+      e = launch_n<double>(c.n, a, c.count, quirk, cs);
+    } else {
+      SpoArgs<float> a{};
+      a.tab = p->t32;
+      a.pk = c.d_pk;
+      a.psi0 = p->d_psi0;
+      a.psi_out = p->d_psi;
+      a.c_out = p->d_c;
+      a.nsteps = nsteps;
+      e = launch_n<float>(c.n, a, c.count, false, cs);
+    }
+    if (e != cudaSuccess) return set_cuda_error("spo1d_kernel launch", e);
+    ESPEC_CK(cudaEventRecord(p->events[ci], cs));
+    ESPEC_CK(cudaStreamWaitEvent(st, p->events[ci], 0));
+  }
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spo_results(espec_spo_plan* p, double* c_re, double* c_im, double* psi_re,
+                                 double* psi_im, int where, void* stream) {
+  if (!p || p->c_cap_steps < 0) return set_error(ESPEC_EINVAL, "no results: run the plan first");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind = where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t nc = (size_t)p->npk * (p->c_cap_steps + 1);
+  if (c_re) ESPEC_CK(cudaMemcpy2DAsync(c_re, 8, p->d_c, 16, 8, nc, kind, st));
+  if (c_im) ESPEC_CK(cudaMemcpy2DAsync(c_im, 8, (char*)p->d_c + 8, 16, 8, nc, kind, st));
+  const size_t np = p->npts;
+  if (psi_re) ESPEC_CK(cudaMemcpy2DAsync(psi_re, 8, p->d_psi, 16, 8, np, kind, st));
+  if (psi_im) ESPEC_CK(cudaMemcpy2DAsync(psi_im, 8, (char*)p->d_psi + 8, 16, 8, np, kind, st));
+  if (where == ESPEC_MEM_HOST) ESPEC_CK(cudaStreamSynchronize(st));
+  return ESPEC_OK;
+}
+
+extern "C" const void* espec_spo_device_c(const espec_spo_plan* p) { return p ? p->d_c : nullptr; }

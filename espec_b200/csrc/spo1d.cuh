@@ -1,0 +1,430 @@
+// spo1d.cuh -- persistent batched 1D split-operator propagation (device side).
+//
+// One CTA owns one packet for the whole time loop; the wave function never
+// leaves registers/shared memory between steps.  Per step (Strang splitting
+// with the two V half-steps of consecutive steps merged, spofft.f:120-191):
+//
+//   phi <- g . phi            x space, g = e^{-i V dt} (x absorber)   [h at step 1]
+//   phi <- F^-1 K F phi       K = e^{-i T(k) dt} / N  (k space)
+//   C(t) = sum_j w_j phi_j    w = conj(psi0) . h      (FP64 accumulation)
+//
+// psi(t) = h . phi (x mask) is formed only once at the end.  The forward FFT
+// is a decimation-in-frequency Stockham sequence whose output stays in the
+// registers of the thread that computed the last butterflies; the inverse
+// runs the exact conjugate stages in reverse order, so each step needs
+// 2(S-1) shared-memory exchanges for S radix stages and no transposes.  The
+// half-swaps of spofft.f:120-133/178-191 (an fftshift before the forward and
+// after the inverse transform) cancel exactly and are not performed.
+#pragma once
+#include "cplx.cuh"
+
+namespace espec {
+
+// ---------------------------------------------------------------------------
+// radix plans: P points per thread, radices in execution order
+// ---------------------------------------------------------------------------
+template <int N_, int P_, int... Rs>
+struct Plan {
+  static constexpr int N = N_;
+  static constexpr int P = P_;
+  static constexpr int T = N_ / P_;
+  static constexpr int S = sizeof...(Rs);
+  static constexpr int r[S] = {Rs...};
+  static __host__ __device__ constexpr int M(int s) {
+    int m = N_;
+    for (int i = 0; i < s; ++i) m /= r[i];
+    return m;
+  }
+  // number of non-trivial twiddles held per thread (stages with M/R > 1)
+  static __host__ __device__ constexpr int tw_off(int s) {
+    int o = 0;
+    for (int i = 0; i < s; ++i)
+      if (M(i) / r[i] > 1) o += (P / r[i]) * (r[i] - 1);
+    return o;
+  }
+  static constexpr int NTW = tw_off(S) > 0 ? tw_off(S) : 1;
+  // number of unitary radix-3 factors (FP32 form keeps them unitary)
+  static __host__ __device__ constexpr int n3() {
+    int c = 0;
+    for (int i = 0; i < S; ++i)
+      if (r[i] % 3 == 0) ++c;
+    return c;
+  }
+};
+
+template <int N>
+struct DefaultPlan;
+template <> struct DefaultPlan<256>  { using type = Plan<256, 8, 8, 8, 4>; };
+template <> struct DefaultPlan<512>  { using type = Plan<512, 8, 8, 8, 8>; };
+template <> struct DefaultPlan<1024> { using type = Plan<1024, 8, 8, 8, 8, 2>; };
+template <> struct DefaultPlan<2048> { using type = Plan<2048, 8, 8, 8, 8, 4>; };
+template <> struct DefaultPlan<4096> { using type = Plan<4096, 16, 16, 16, 16>; };
+template <> struct DefaultPlan<384>  { using type = Plan<384, 12, 12, 4, 4, 2>; };
+template <> struct DefaultPlan<768>  { using type = Plan<768, 12, 12, 4, 4, 4>; };
+template <> struct DefaultPlan<1536> { using type = Plan<1536, 12, 12, 4, 4, 4, 2>; };
+
+// ---------------------------------------------------------------------------
+// per-precision table formats
+// ---------------------------------------------------------------------------
+template <typename R>
+struct Tab;
+template <>
+struct Tab<double> {
+  using rot_t = RotD;
+  using phase_t = cpx<double>;   // complex factor (rotation x magnitude)
+  using weight_t = cpx<double>;
+  static __device__ __forceinline__ cpx<double> apply(const phase_t& f, cpx<double> a) {
+    return mk(fma(a.x, f.x, -a.y * f.y), fma(a.x, f.y, a.y * f.x));
+  }
+};
+template <>
+struct Tab<float> {
+  using rot_t = RotF;
+  struct phase_t {
+    float t, s, g, a;  // lifting rotation, then real scale a
+  };
+  using weight_t = cpx<float>;
+  static __device__ __forceinline__ cpx<float> apply(const phase_t& f, cpx<float> v) {
+    RotF r;
+    r.t = f.t;
+    r.s = f.s;
+    r.g = f.g;
+    cpx<float> o = rot<false>(r, v);
+    return mk(o.x * f.a, o.y * f.a);
+  }
+};
+
+// pointers of one precision's tables (all per point, concatenated over packets)
+template <typename R>
+struct SpoTables {
+  const typename Tab<R>::phase_t* g;   // e^{-iV dt} (x absorber), x order
+  const typename Tab<R>::phase_t* h;   // e^{-iV dt/2}, x order (first step)
+  const typename Tab<R>::phase_t* hm;  // mask x e^{-iV dt/2}, x order (final psi)
+  const typename Tab<R>::phase_t* k;   // kinetic phase x scale, final FFT layout
+  const typename Tab<R>::weight_t* w;  // conj(psi0) x h (x mask), x order
+};
+
+struct SpoPacket {
+  int off;       // first point of the packet in the concatenated arrays
+  int c_off;     // first C(t) sample of the packet
+};
+
+template <typename R>
+struct SpoArgs {
+  SpoTables<R> tab;
+  const SpoPacket* pk;      // per CTA (packets of this size class)
+  const double2* psi0;      // initial psi (x order), FP64
+  double2* psi_out;         // psi(TF) (x order), FP64
+  double2* c_out;           // C(t) samples, nsteps+1 per packet
+  const double* kq_c;       // FP64 quirk form: cos(CST1*TC) per point (final layout)
+  const double* kq_s;       //                    sin(CST1*TC)
+  double kq_scale;          //                    1/N
+  int nsteps;
+};
+
+template <int T>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (T <= 32) {
+    __syncwarp();
+  } else {
+    __syncthreads();
+  }
+}
+
+template <typename R, class PL>
+struct SpoThread {
+  static constexpr int N = PL::N, P = PL::P, T = PL::T, S = PL::S;
+  using rot_t = typename Tab<R>::rot_t;
+
+  rot_t tw[PL::NTW];
+
+  static __device__ __forceinline__ int sidx(int i) { return i; }
+
+  __device__ void init_twiddles(int t) { init_stage<0>(t); }
+
+  template <int s>
+  __device__ __forceinline__ void init_stage(int t) {
+    if constexpr (s < S) {
+      constexpr int RR = PL::r[s];
+      constexpr int M = PL::M(s);
+      constexpr int m = M / RR;
+      constexpr int Q = P / RR;
+      if constexpr (m > 1) {
+        constexpr int o = PL::tw_off(s);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+          const int beta = t + T * q;
+          const int n1 = beta % m;
+#pragma unroll
+          for (int k = 1; k < RR; ++k) {
+            int j = (n1 * k) % M;
+            if (2 * j > M) j -= M;  // angle 2 pi j / M in (-pi, pi]
+            const double phi = 6.283185307179586476925287 * (double)j / (double)M;
+            if constexpr (sizeof(R) == 8) {
+              RotD r;
+              sincospi(2.0 * (double)j / (double)M, &r.s, &r.c);
+              tw[o + q * (RR - 1) + k - 1] = r;
+            } else {
+              tw[o + q * (RR - 1) + k - 1] = make_rotf(phi);
+            }
+          }
+        }
+      }
+      init_stage<s + 1>(t);
+    }
+  }
+
+  // forward stage s: butterflies then twiddles (DIF)
+  template <int s>
+  __device__ __forceinline__ void fwd_bfly(cpx<R>* v) const {
+    constexpr int RR = PL::r[s];
+    constexpr int m = PL::M(s) / RR;
+    constexpr int Q = P / RR;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      dft<R, RR, false>(v + q * RR);
+      if constexpr (m > 1) {
+        constexpr int o = PL::tw_off(s);
+#pragma unroll
+        for (int k = 1; k < RR; ++k)
+          v[q * RR + k] = rot<false>(tw[o + q * (RR - 1) + k - 1], v[q * RR + k]);
+      }
+    }
+  }
+
+  // inverse of stage s: conjugate twiddles then conjugate butterflies (DIT)
+  template <int s>
+  __device__ __forceinline__ void inv_bfly(cpx<R>* v) const {
+    constexpr int RR = PL::r[s];
+    constexpr int m = PL::M(s) / RR;
+    constexpr int Q = P / RR;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+      if constexpr (m > 1) {
+        constexpr int o = PL::tw_off(s);
+#pragma unroll
+        for (int k = 1; k < RR; ++k)
+          v[q * RR + k] = rot<true>(tw[o + q * (RR - 1) + k - 1], v[q * RR + k]);
+      }
+      dft<R, RR, true>(v + q * RR);
+    }
+  }
+
+  // positions of stage-s outputs held by thread t (slot q*R + k')
+  template <int s>
+  static __device__ __forceinline__ int out_pos(int t, int q, int k) {
+    constexpr int RR = PL::r[s];
+    constexpr int m = PL::M(s) / RR;
+    const int beta = t + T * q;
+    const int p = beta / m, n1 = beta % m;
+    return (p * RR + k) * m + n1;
+  }
+  // positions of stage-s inputs held by thread t (slot q*R + k)
+  template <int s>
+  static __device__ __forceinline__ int in_pos(int t, int q, int k) {
+    constexpr int RR = PL::r[s];
+    constexpr int M = PL::M(s);
+    constexpr int m = M / RR;
+    const int beta = t + T * q;
+    const int p = beta / m, n1 = beta % m;
+    return p * M + n1 + m * k;
+  }
+
+  // exchange after forward stage s (s < S-1): outputs of s -> inputs of s+1
+  template <int s>
+  static __device__ __forceinline__ void xchg_fwd(cpx<R>* v, cpx<R>* buf, int t) {
+    constexpr int R0 = PL::r[s], Q0 = P / R0;
+    constexpr int R1 = PL::r[s + 1], Q1 = P / R1;
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int k = 0; k < R0; ++k) buf[sidx(out_pos<s>(t, q, k))] = v[q * R0 + k];
+    group_sync<T>();
+#pragma unroll
+    for (int q = 0; q < Q1; ++q)
+#pragma unroll
+      for (int k = 0; k < R1; ++k) v[q * R1 + k] = buf[sidx(in_pos<s + 1>(t, q, k))];
+  }
+  // reverse exchange: inputs of s+1 -> outputs of s
+  template <int s>
+  static __device__ __forceinline__ void xchg_inv(cpx<R>* v, cpx<R>* buf, int t) {
+    constexpr int R0 = PL::r[s], Q0 = P / R0;
+    constexpr int R1 = PL::r[s + 1], Q1 = P / R1;
+#pragma unroll
+    for (int q = 0; q < Q1; ++q)
+#pragma unroll
+      for (int k = 0; k < R1; ++k) buf[sidx(in_pos<s + 1>(t, q, k))] = v[q * R1 + k];
+    group_sync<T>();
+#pragma unroll
+    for (int q = 0; q < Q0; ++q)
+#pragma unroll
+      for (int k = 0; k < R0; ++k) v[q * R0 + k] = buf[sidx(out_pos<s>(t, q, k))];
+  }
+
+  template <int s>
+  __device__ __forceinline__ void forward(cpx<R>* v, cpx<R>* b0, cpx<R>* b1, int t) const {
+    if constexpr (s < S) {
+      fwd_bfly<s>(v);
+      if constexpr (s + 1 < S) {
+        xchg_fwd<s>(v, (s & 1) ? b1 : b0, t);
+        forward<s + 1>(v, b0, b1, t);
+      }
+    }
+  }
+  template <int s>
+  __device__ __forceinline__ void inverse(cpx<R>* v, cpx<R>* b0, cpx<R>* b1, int t) const {
+    if constexpr (s >= 0) {
+      inv_bfly<s>(v);
+      if constexpr (s > 0) {
+        xchg_inv<s - 1>(v, (s & 1) ? b1 : b0, t);  // exchange of stage s-1 uses buffer (s-1+1)&1
+        inverse<s - 1>(v, b0, b1, t);
+      }
+    }
+  }
+
+  // final-layout position of slot j (for the k-space table)
+  static __device__ __forceinline__ int final_pos(int t, int j) {
+    constexpr int RR = PL::r[S - 1];
+    const int q = j / RR, k = j % RR;
+    return (t + T * q) * RR + k;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// the kernel: one CTA per packet of size N
+// ---------------------------------------------------------------------------
+template <typename R, class PL, bool kCap, bool kQuirk>
+__global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
+  constexpr int N = PL::N, P = PL::P, T = PL::T;
+  constexpr int NW = (T + 31) / 32;
+  using Th = SpoThread<R, PL>;
+  using TB = Tab<R>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  cpx<R>* b0 = reinterpret_cast<cpx<R>*>(smem_raw);
+  cpx<R>* b1 = b0 + N;
+  double2* cpart = reinterpret_cast<double2*>(b1 + N);  // [2][NW]
+
+  const int t = threadIdx.x;
+  const int lane = t & 31, warp = t >> 5;
+  const SpoPacket pk = a.pk[blockIdx.x];
+  const int base = pk.off;
+  double2* cout = a.c_out + pk.c_off;
+
+  Th th;
+  th.init_twiddles(t);
+
+  cpx<R> v[P];
+  typename TB::phase_t g[P], kk[P];
+  typename TB::weight_t w[P];
+  double c0r = 0.0;
+#pragma unroll
+  for (int j = 0; j < P; ++j) {
+    const int x = base + t + T * j;
+    const double2 p0 = a.psi0[x];
+    c0r += p0.x * p0.x + p0.y * p0.y;
+    v[j] = mk((R)p0.x, (R)p0.y);
+    g[j] = a.tab.g[x];
+    w[j] = a.tab.w[x];
+    if constexpr (!kQuirk) kk[j] = a.tab.k[base + Th::final_pos(t, j)];
+  }
+  // C(0) = <psi0|psi0>
+  {
+    double cr = c0r;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cr += __shfl_xor_sync(0xffffffffu, cr, o);
+    if (lane == 0) cpart[warp] = make_double2(cr, 0.0);
+    group_sync<T>();
+    if (t == 0) {
+      double sr = 0.0;
+      for (int i = 0; i < NW; ++i) sr += cpart[i].x;
+      cout[0] = make_double2(sr, 0.0);
+    }
+    group_sync<T>();
+  }
+
+  for (int step = 1; step <= a.nsteps; ++step) {
+    // x-space phase
+    if (step == 1) {
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = TB::apply(a.tab.h[base + t + T * j], v[j]);
+    } else {
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = TB::apply(g[j], v[j]);
+    }
+    th.template forward<0>(v, b0, b1, t);
+    // sum of the previous step's partial C(t): all partials are visible after
+    // the first exchange barrier of this step
+    if (T > 32 && t == 0 && step > 1) {
+      double sr = 0.0, si = 0.0;
+      const double2* cp = cpart + ((step - 1) & 1) * NW;
+      for (int i = 0; i < NW; ++i) {
+        sr += cp[i].x;
+        si += cp[i].y;
+      }
+      cout[step - 1] = make_double2(sr, si);
+    }
+    // kinetic phase
+    if constexpr (kQuirk) {
+      // spofft.f:148-154 as written: V(I) uses the already updated U(I)
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const int f = base + Th::final_pos(t, j);
+        const double c = a.kq_c[f], s = a.kq_s[f];
+        const double un = c * (double)v[j].x + s * (double)v[j].y;
+        const double vn = c * (double)v[j].y - s * un;
+        v[j] = mk((R)(un * a.kq_scale), (R)(vn * a.kq_scale));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = TB::apply(kk[j], v[j]);
+    }
+    th.template inverse<PL::S - 1>(v, b0, b1, t);
+    // partial C(t) = sum w phi in FP64
+    double cr = 0.0, ci = 0.0;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const double wx = (double)w[j].x, wy = (double)w[j].y;
+      const double vx = (double)v[j].x, vy = (double)v[j].y;
+      cr = fma(wx, vx, fma(-wy, vy, cr));
+      ci = fma(wx, vy, fma(wy, vx, ci));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      cr += __shfl_xor_sync(0xffffffffu, cr, o);
+      ci += __shfl_xor_sync(0xffffffffu, ci, o);
+    }
+    if constexpr (T <= 32) {
+      if (lane == 0) cout[step] = make_double2(cr, ci);
+    } else {
+      if (lane == 0) cpart[(step & 1) * NW + warp] = make_double2(cr, ci);
+    }
+  }
+  if constexpr (T > 32) {
+    group_sync<T>();
+    if (t == 0 && a.nsteps > 0) {
+      double sr = 0.0, si = 0.0;
+      const double2* cp = cpart + (a.nsteps & 1) * NW;
+      for (int i = 0; i < NW; ++i) {
+        sr += cp[i].x;
+        si += cp[i].y;
+      }
+      cout[a.nsteps] = make_double2(sr, si);
+    }
+  }
+  // psi(TF) = hm . phi
+  if (a.psi_out) {
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const int x = base + t + T * j;
+      cpx<R> o = (a.nsteps > 0) ? TB::apply(a.tab.hm[x], v[j]) : v[j];
+      a.psi_out[x] = make_double2((double)o.x, (double)o.y);
+    }
+  }
+}
+
+template <typename R, class PL>
+constexpr size_t spo1d_smem_bytes() {
+  return 2 * sizeof(cpx<R>) * PL::N + 2 * sizeof(double2) * ((PL::T + 31) / 32);
+}
+
+}  // namespace espec

@@ -1,0 +1,88 @@
+/*
+ * espec_gpu.h -- C-ABI of the B200 wave-packet propagator (libespecgpu.so).
+ *
+ * Two layers:
+ *   1. Fortran-callable drop-ins for eSPec's propagators (lower-case name
+ *      with trailing underscore, every argument by reference, one hidden
+ *      size_t length per CHARACTER*(*) argument appended in order).  They
+ *      take the same arguments as the reference routines and leave the same
+ *      outputs in the caller's arrays.
+ *   2. Plan-based batched entry points used by the drop-ins and by batched
+ *      scans (thousands of independent packets in one launch).
+ *
+ * All functions return ESPEC_OK (0) or a negative error code; the message of
+ * the last error of the calling thread is espec_last_error().  Nothing here
+ * aborts the process.  A library built without a usable GPU fails every call
+ * with ESPEC_ECUDA -- there is no CPU fallback.
+ */
+#ifndef ESPEC_GPU_H
+#define ESPEC_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* return codes */
+#define ESPEC_OK 0
+#define ESPEC_EINVAL (-1)   /* invalid argument / unsupported case          */
+#define ESPEC_ECUDA (-2)    /* CUDA runtime or launch error                 */
+#define ESPEC_ENOMEM (-3)   /* device allocation failed                     */
+
+/* arithmetic forms */
+#define ESPEC_FP64 0        /* plain FP64 form (parity form)                */
+#define ESPEC_MIXED 1       /* FP32 data, FP64 phases and C(t) accumulation */
+
+/* absorber kinds (absorb.f: .VOPTIC_* complex potentials, .SMOOTHW mask) */
+#define ESPEC_ABS_NONE 0
+#define ESPEC_ABS_VOPTIC 1
+#define ESPEC_ABS_SMOOTHW 2
+
+/* reproduce reference defects on request (FP64 form only) */
+#define ESPEC_Q_SPO_INPLACE 1   /* spofft.f:150-153 kinetic multiply            */
+
+/* memory space of user pointers */
+#define ESPEC_MEM_HOST 0
+#define ESPEC_MEM_DEVICE 1
+
+#define ESPEC_SHFS 2.4188843243e-2  /* fs per atomic unit of time (pspofft.f:76) */
+
+const char* espec_last_error(void);
+const char* espec_version(void);
+/* 1 when a CUDA device of compute capability 10.x is usable, else 0 */
+int espec_device_ok(void);
+
+/* ----------------------------------------------------------------------
+ * Batched 1D split-operator plans.
+ *
+ * Replaces the time loop of PSPOFFT (pspofft.f:110-145) with PSPOFFTAUX
+ * (spofft.f:3-203) for many independent 1D packets at once.  Packet k has
+ * npts[k] points (256, 384, 512, 768, 1024, 1536, 2048 or 4096), grid step
+ * sh[k] (bohr) and mass sm[k] (electron masses); all packets share dt_fs.
+ * Arrays passed to espec_spo_load are concatenated over packets in order.
+ * C(t) = <psi(0)|psi(t)> is produced for every step: nsteps+1 complex
+ * samples per packet, packet-major.
+ * ---------------------------------------------------------------------- */
+typedef struct espec_spo_plan espec_spo_plan;
+
+int espec_spo_create(espec_spo_plan** plan, int npk, const int* npts,
+                     const double* sh, const double* sm, double dt_fs,
+                     int precision, int absorb, int quirks);
+/* vabc: absorber table (complex-potential values for ESPEC_ABS_VOPTIC, mask
+ * for ESPEC_ABS_SMOOTHW), ignored for ESPEC_ABS_NONE; psi_im may be NULL. */
+int espec_spo_load(espec_spo_plan* plan, const double* vpot, const double* vabc,
+                   const double* psi_re, const double* psi_im, int where,
+                   void* stream);
+int espec_spo_run(espec_spo_plan* plan, int nsteps, void* stream);
+int espec_spo_results(espec_spo_plan* plan, double* c_re, double* c_im,
+                      double* psi_re, double* psi_im, int where, void* stream);
+/* device pointer of the C(t) buffer (double2, packet-major) */
+const void* espec_spo_device_c(const espec_spo_plan* plan);
+int espec_spo_npoints(const espec_spo_plan* plan);
+void espec_spo_destroy(espec_spo_plan* plan);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -52,94 +52,135 @@ extern "C" double orc_ecnorm(int n, const double* a) {
 // ---------------------------------------------------------------------------
 namespace {
 
-struct TwiddleTable {
-  std::vector<cd> w;  // w[j] = exp(+2 pi i j / n)
+// Plan of an iterative Stockham autosort FFT of length n: radices in
+// execution order and, per stage, the twiddles exp(+2 pi i j k / (l r)).
+struct FftPlan {
+  int n = 0;
+  std::vector<int> radix;
+  std::vector<std::vector<cd>> tw;  // per stage: tw[k*(r) + j]
 };
 
-const TwiddleTable& twiddles(int n) {
+std::vector<int> factorise(int n) {
+  std::vector<int> f;
+  while (n % 4 == 0) {
+    f.push_back(4);
+    n /= 4;
+  }
+  while (n % 2 == 0) {
+    f.push_back(2);
+    n /= 2;
+  }
+  for (int p = 3; n > 1; p += 2)
+    while (n % p == 0) {
+      f.push_back(p);
+      n /= p;
+    }
+  return f;
+}
+
+const FftPlan& fft_plan(int n) {
   static std::mutex mu;
-  static std::map<int, TwiddleTable*> cache;
+  static std::map<int, FftPlan*> cache;
   std::lock_guard<std::mutex> lk(mu);
   auto it = cache.find(n);
   if (it != cache.end()) return *it->second;
-  TwiddleTable* t = new TwiddleTable;
-  t->w.resize(n);
-  for (int j = 0; j < n; ++j) {
-    // reduce to the first octant-free form: angle = 2 pi j / n exactly rounded once
-    long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)j /
-                    (long double)n;
-    t->w[j] = cd((double)cosl(a), (double)sinl(a));
+  FftPlan* pl = new FftPlan;
+  pl->n = n;
+  pl->radix = factorise(n);
+  int l = 1;  // product of the radices already applied
+  for (int r : pl->radix) {
+    const int m = n / (l * r);
+    (void)m;
+    std::vector<cd> w((size_t)l * r);
+    for (int k = 0; k < l; ++k)
+      for (int j = 0; j < r; ++j) {
+        long double a = 2.0L * 3.141592653589793238462643383279502884L * (long double)(j * k) /
+                        (long double)(l * r);
+        w[(size_t)k * r + j] = cd((double)cosl(a), (double)sinl(a));
+      }
+    pl->tw.push_back(std::move(w));
+    l *= r;
   }
-  cache[n] = t;
-  return *t;
+  cache[n] = pl;
+  return *pl;
 }
 
-int pick_radix(int n) {
-  if (n % 4 == 0 && n != 8) return 4;
-  if (n % 2 == 0) return 2;
-  if (n % 3 == 0) return 3;
-  if (n % 5 == 0) return 5;
-  for (int p = 7; p * p <= n; p += 2)
-    if (n % p == 0) return p;
-  return n;
-}
-
-// out[k] = sum_j in[j*stride] * W^(sign*j*k*tstep), W = exp(2 pi i / tn)
-void fft_rec(const cd* in, int stride, cd* out, int n, const cd* tab, int tn,
-             int tstep, int sign, cd* tmp) {
-  if (n == 1) {
-    out[0] = in[0];
-    return;
+// one Stockham pass: x (length n, viewed as [r][m][l] with m = n/(l r)) ->
+// y viewed as [m][r][l]; sub-transforms of length l*r.
+void stockham_pass(const cd* x, cd* y, int n, int l, int r, const cd* tw, int sign) {
+  const int m = n / (l * r);
+  cd tmp[16];
+  std::vector<cd> big;
+  cd* t = tmp;
+  if (r > 16) {
+    big.resize(r);
+    t = big.data();
   }
-  const int r = pick_radix(n);
-  const int m = n / r;
-  for (int q = 0; q < r; ++q)
-    fft_rec(in + q * stride, stride * r, out + q * m, m, tab, tn, tstep * r, sign, tmp);
-  // combine: X[k + m s] = sum_q W_n^{q(k + m s)} Y_q[k]
-  auto wn = [&](long long e) -> cd {  // W_n^e with sign
-    long long idx = (e * tstep) % tn;
-    if (idx < 0) idx += tn;
-    cd w = tab[idx];
-    return sign > 0 ? w : std::conj(w);
-  };
-  for (int k = 0; k < m; ++k) {
-    cd y[64];
-    std::vector<cd> yv;
-    cd* yy = y;
-    if (r > 64) {
-      yv.resize(r);
-      yy = yv.data();
-    }
-    for (int q = 0; q < r; ++q) yy[q] = out[q * m + k] * (q == 0 ? cd(1, 0) : wn((long long)q * k));
-    if (r == 2) {
-      tmp[k] = yy[0] + yy[1];
-      tmp[k + m] = yy[0] - yy[1];
-    } else if (r == 4) {
-      cd a0 = yy[0] + yy[2], a1 = yy[0] - yy[2];
-      cd b0 = yy[1] + yy[3], b1 = yy[1] - yy[3];
-      cd jb1 = sign > 0 ? cd(-b1.imag(), b1.real()) : cd(b1.imag(), -b1.real());
-      tmp[k] = a0 + b0;
-      tmp[k + m] = a1 + jb1;
-      tmp[k + 2 * m] = a0 - b0;
-      tmp[k + 3 * m] = a1 - jb1;
-    } else {
-      for (int s = 0; s < r; ++s) {
-        cd acc(0, 0);
-        for (int q = 0; q < r; ++q) {
-          long long e = ((long long)q * s * m) % n;  // W_n^{q m s} = W_r^{q s}
-          acc += yy[q] * (e == 0 ? cd(1, 0) : wn(e));
+  for (int q = 0; q < m; ++q) {
+    for (int k = 0; k < l; ++k) {
+      // gather the r inputs of this butterfly, apply twiddles
+      for (int j = 0; j < r; ++j) {
+        cd v = x[(size_t)j * m * l + (size_t)q * l + k];
+        if (k && j) {
+          const cd w = tw[(size_t)k * r + j];
+          const double wi = sign > 0 ? w.imag() : -w.imag();
+          v = cd(v.real() * w.real() - v.imag() * wi, v.real() * wi + v.imag() * w.real());
         }
-        tmp[k + s * m] = acc;
+        t[j] = v;
+      }
+      cd* out = const_cast<cd*>(y) + (size_t)q * r * l + k;
+      if (r == 2) {
+        out[0] = t[0] + t[1];
+        out[l] = t[0] - t[1];
+      } else if (r == 4) {
+        cd a0 = t[0] + t[2], a1 = t[0] - t[2], b0 = t[1] + t[3], b1 = t[1] - t[3];
+        cd jb = sign > 0 ? cd(-b1.imag(), b1.real()) : cd(b1.imag(), -b1.real());
+        out[0] = a0 + b0;
+        out[l] = a1 + jb;
+        out[2 * l] = a0 - b0;
+        out[3 * l] = a1 - jb;
+      } else if (r == 3) {
+        const double h = 0.8660254037844386467637232;  // sqrt(3)/2
+        cd p = t[1] + t[2], mm = t[1] - t[2];
+        cd c = cd(t[0].real() - 0.5 * p.real(), t[0].imag() - 0.5 * p.imag());
+        cd u = cd(h * mm.real(), h * mm.imag());
+        cd iu = sign > 0 ? cd(-u.imag(), u.real()) : cd(u.imag(), -u.real());
+        out[0] = t[0] + p;
+        out[l] = c + iu;
+        out[2 * l] = c - iu;
+      } else {
+        // generic odd radix: W_r^{js} from the stage table (entry k = l/.. unused)
+        for (int s2 = 0; s2 < r; ++s2) {
+          double ar = 0.0, ai = 0.0;
+          for (int j = 0; j < r; ++j) {
+            const double ang = 6.283185307179586476925287 * (double)((j * s2) % r) / (double)r;
+            const double c = std::cos(ang), sn = sign > 0 ? std::sin(ang) : -std::sin(ang);
+            ar += t[j].real() * c - t[j].imag() * sn;
+            ai += t[j].real() * sn + t[j].imag() * c;
+          }
+          out[(size_t)s2 * l] = cd(ar, ai);
+        }
       }
     }
   }
-  for (int i = 0; i < n; ++i) out[i] = tmp[i];
 }
 
+// unnormalised DFT of x in place: sign > 0 -> exp(+2 pi i jk/n)
 void dft_line(cd* x, int n, int sign) {
-  const TwiddleTable& t = twiddles(n);
-  std::vector<cd> in(x, x + n), tmp(n);
-  fft_rec(in.data(), 1, x, n, t.w.data(), n, 1, sign, tmp.data());
+  const FftPlan& pl = fft_plan(n);
+  thread_local std::vector<cd> buf;
+  if ((int)buf.size() < n) buf.resize(n);
+  cd* a = x;
+  cd* b = buf.data();
+  int l = 1;
+  for (size_t s = 0; s < pl.radix.size(); ++s) {
+    const int r = pl.radix[s];
+    stockham_pass(a, b, n, l, r, pl.tw[s].data(), sign);
+    std::swap(a, b);
+    l *= r;
+  }
+  if (a != x)
+    for (int i = 0; i < n; ++i) x[i] = a[i];
 }
 
 }  // namespace
@@ -149,7 +190,8 @@ extern "C" void orc_fft(double* re, double* im, int ntot, int n, int nspan, int 
   if (n < 2) return;
   const int stride = nspan / n;
   const int sign = isn >= 0 ? +1 : -1;
-  std::vector<cd> line(n);
+  thread_local std::vector<cd> line;
+  if ((int)line.size() < n) line.resize(n);
   for (int base = 0; base < ntot; base += nspan) {
     for (int off = 0; off < stride; ++off) {
       for (int j = 0; j < n; ++j) {
@@ -360,7 +402,8 @@ extern "C" void orc_spo_step(int ndim, const int* np, double b, double cst1, dou
   // first V half-step with the half swap (spofft.f:66-81 / :120-133)
   for (int i = 0; i < nh; ++i) {
     double th1 = cst2 * vpot[i];
-    double c1 = std::cos(th1), s1 = std::sin(th1);
+    double c1, s1;
+    sincos(th1, &s1, &c1);
     if (voptic) {
       double e1 = std::exp(cst2 * vabc[i]);
       c1 *= e1;
@@ -369,7 +412,8 @@ extern "C" void orc_spo_step(int ndim, const int* np, double b, double cst1, dou
     double ua = c1 * u[i] + s1 * v[i];
     double va = c1 * v[i] - s1 * u[i];
     double th2 = cst2 * vpot[i + nh];
-    double c2 = std::cos(th2), s2 = std::sin(th2);
+    double c2, s2;
+    sincos(th2, &s2, &c2);
     if (voptic) {
       double e2 = std::exp(cst2 * vabc[i + nh]);
       c2 *= e2;
@@ -384,7 +428,8 @@ extern "C" void orc_spo_step(int ndim, const int* np, double b, double cst1, dou
   // kinetic phase (spofft.f:148-154)
   for (int i = 0; i < n; ++i) {
     double th = cst1 * tc[i];
-    double c = std::cos(th), s = std::sin(th);
+    double c, s;
+    sincos(th, &s, &c);
     double un = c * u[i] + s * v[i];
     if (quirks & ORC_Q_SPO_INPLACE) {
       u[i] = un;
@@ -398,7 +443,8 @@ extern "C" void orc_spo_step(int ndim, const int* np, double b, double cst1, dou
   // last V half-step with swap back and 1/N (spofft.f:103-118 / :162-191)
   for (int i = 0; i < nh; ++i) {
     double th1 = cst2 * vpot[i + nh];
-    double c1 = std::cos(th1), s1 = std::sin(th1);
+    double c1, s1;
+    sincos(th1, &s1, &c1);
     if (voptic) {
       double e1 = std::exp(cst2 * vabc[i + nh]);
       c1 *= e1;
@@ -407,7 +453,8 @@ extern "C" void orc_spo_step(int ndim, const int* np, double b, double cst1, dou
     double ua = c1 * b * u[i] + s1 * b * v[i];
     double va = c1 * b * v[i] - s1 * b * u[i];
     double th2 = cst2 * vpot[i];
-    double c2 = std::cos(th2), s2 = std::sin(th2);
+    double c2, s2;
+    sincos(th2, &s2, &c2);
     if (voptic) {
       double e2 = std::exp(cst2 * vabc[i]);
       c2 *= e2;

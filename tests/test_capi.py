@@ -1,0 +1,36 @@
+"""CPU-side checks of the C-ABI library: it loads and exports every symbol
+declared in include/espec_gpu.h.  No compute call is made."""
+import ctypes as C
+import os
+import re
+
+from espec_b200 import _native as N
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    src = open(os.path.join(ROOT, "include", "espec_gpu.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = re.findall(r"\b([a-z_][a-z0-9_]*)\s*\(", src)
+    keep = [n for n in names if n.startswith("espec_") or n.endswith("_")]
+    return sorted(set(keep))
+
+
+def test_library_loads_and_exports_declared_symbols():
+    lib = N.load()
+    declared = declared_symbols()
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(N.EXPORTS) <= set(declared)
+    assert lib.espec_version().startswith(b"espec_b200")
+
+
+def test_errors_are_reported_without_a_device_call():
+    lib = N.load()
+    h = C.c_void_p()
+    # invalid arguments are rejected on the host before any CUDA call
+    rc = lib.espec_spo_create(C.byref(h), 0, None, None, None, 0.0, 0, 0, 0)
+    assert rc == N.EINVAL
+    assert b"null" in lib.espec_last_error()
