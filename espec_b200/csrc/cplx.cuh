@@ -182,43 +182,89 @@ ESPEC_HD void dft4(cpx<R>* v) {
   v[3] = t1 - it3;
 }
 
+// DFT8 = 2 x DFT4 (even/odd) + twiddles + radix-2 butterflies; the
+// conjugate transform mirrors the forward sequence (see dft12).
 template <typename R, bool Inv>
 ESPEC_HD void dft8(cpx<R>* v) {
-  cpx<R> e[4] = {v[0], v[2], v[4], v[6]};
-  cpx<R> o[4] = {v[1], v[3], v[5], v[7]};
-  dft4<R, Inv>(e);
-  dft4<R, Inv>(o);
-  o[1] = twid_const<R, 1, 8, Inv>(o[1]);
-  o[2] = twid_const<R, 2, 8, Inv>(o[2]);
-  o[3] = twid_const<R, 3, 8, Inv>(o[3]);
+  cpx<R> e[4], o[4];
+  if constexpr (!Inv) {
 #pragma unroll
-  for (int k = 0; k < 4; ++k) {
-    v[k] = e[k] + o[k];
-    v[k + 4] = e[k] - o[k];
+    for (int k = 0; k < 4; ++k) {
+      e[k] = v[2 * k];
+      o[k] = v[2 * k + 1];
+    }
+    dft4<R, false>(e);
+    dft4<R, false>(o);
+    o[1] = twid_const<R, 1, 8, false>(o[1]);
+    o[2] = twid_const<R, 2, 8, false>(o[2]);
+    o[3] = twid_const<R, 3, 8, false>(o[3]);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[k] = e[k] + o[k];
+      v[k + 4] = e[k] - o[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      e[k] = v[k] + v[k + 4];
+      o[k] = v[k] - v[k + 4];
+    }
+    o[1] = twid_const<R, 1, 8, true>(o[1]);
+    o[2] = twid_const<R, 2, 8, true>(o[2]);
+    o[3] = twid_const<R, 3, 8, true>(o[3]);
+    dft4<R, true>(e);
+    dft4<R, true>(o);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      v[2 * k] = e[k];
+      v[2 * k + 1] = o[k];
+    }
   }
 }
 
 template <typename R, bool Inv>
 ESPEC_HD void dft16(cpx<R>* v) {
   cpx<R> e[8], o[8];
+  if constexpr (!Inv) {
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    e[k] = v[2 * k];
-    o[k] = v[2 * k + 1];
-  }
-  dft8<R, Inv>(e);
-  dft8<R, Inv>(o);
-  o[1] = twid_const<R, 1, 16, Inv>(o[1]);
-  o[2] = twid_const<R, 2, 16, Inv>(o[2]);
-  o[3] = twid_const<R, 3, 16, Inv>(o[3]);
-  o[4] = twid_const<R, 4, 16, Inv>(o[4]);
-  o[5] = twid_const<R, 5, 16, Inv>(o[5]);
-  o[6] = twid_const<R, 6, 16, Inv>(o[6]);
-  o[7] = twid_const<R, 7, 16, Inv>(o[7]);
+    for (int k = 0; k < 8; ++k) {
+      e[k] = v[2 * k];
+      o[k] = v[2 * k + 1];
+    }
+    dft8<R, false>(e);
+    dft8<R, false>(o);
+    o[1] = twid_const<R, 1, 16, false>(o[1]);
+    o[2] = twid_const<R, 2, 16, false>(o[2]);
+    o[3] = twid_const<R, 3, 16, false>(o[3]);
+    o[4] = twid_const<R, 4, 16, false>(o[4]);
+    o[5] = twid_const<R, 5, 16, false>(o[5]);
+    o[6] = twid_const<R, 6, 16, false>(o[6]);
+    o[7] = twid_const<R, 7, 16, false>(o[7]);
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    v[k] = e[k] + o[k];
-    v[k + 8] = e[k] - o[k];
+    for (int k = 0; k < 8; ++k) {
+      v[k] = e[k] + o[k];
+      v[k + 8] = e[k] - o[k];
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      e[k] = v[k] + v[k + 8];
+      o[k] = v[k] - v[k + 8];
+    }
+    o[1] = twid_const<R, 1, 16, true>(o[1]);
+    o[2] = twid_const<R, 2, 16, true>(o[2]);
+    o[3] = twid_const<R, 3, 16, true>(o[3]);
+    o[4] = twid_const<R, 4, 16, true>(o[4]);
+    o[5] = twid_const<R, 5, 16, true>(o[5]);
+    o[6] = twid_const<R, 6, 16, true>(o[6]);
+    o[7] = twid_const<R, 7, 16, true>(o[7]);
+    dft8<R, true>(e);
+    dft8<R, true>(o);
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      v[2 * k] = e[k];
+      v[2 * k + 1] = o[k];
+    }
   }
 }
 
@@ -255,59 +301,108 @@ ESPEC_HD void lift2(float& x, float& y, float t, float s) {
 template <bool Inv>
 struct Dft3<float, Inv> {
   static constexpr bool unitary = true;
+  // lifting constants of -pi/4 and -atan(sqrt(2))
+  static constexpr float t45 = -0.41421356237309503f, s45 = -0.70710678118654752f;
+  static constexpr float tph = -0.51763809020504152f, sph = -0.81649658092772603f;
   static ESPEC_HD void run(cpx<float>* v) {
-    // lifting constants of -pi/4 and -atan(sqrt(2))
-    const float t45 = -0.41421356237309503f, s45 = -0.70710678118654752f;
-    const float tph = -0.51763809020504152f, sph = -0.81649658092772603f;
-    cpx<float> a = v[0], b = v[1], c = v[2];
-    // (p, m): rotate (b, c) by -45deg -> ((b+c)/s2, (c-b)/s2); m = -(second)
-    float px = b.x, mx = c.x, py = b.y, my = c.y;
-    lift2(px, mx, t45, s45);
-    lift2(py, my, t45, s45);
-    mx = -mx;
-    my = -my;
-    // (y0, q): rotate (a, p) by -phi -> (cos a + sin p, -sin a + cos p); q = -(second)
-    float y0x = a.x, qx = px, y0y = a.y, qy = py;
-    lift2(y0x, qx, tph, sph);
-    lift2(y0y, qy, tph, sph);
-    qx = -qx;
-    qy = -qy;
-    // m' = +i m (forward, exp(+i)) or -i m (conjugate transform)
-    float m2x = Inv ? my : -my;
-    float m2y = Inv ? -mx : mx;
-    // (y1, y2) = ((q + m')/s2, (q - m')/s2): rotate (q, m') by -45deg, y2 = -(second)
-    float y1x = qx, y2x = m2x, y1y = qy, y2y = m2y;
-    lift2(y1x, y2x, t45, s45);
-    lift2(y1y, y2y, t45, s45);
-    v[0] = mk(y0x, y0y);
-    v[1] = mk(y1x, y1y);
-    v[2] = mk(-y2x, -y2y);
+    if constexpr (!Inv) {
+      cpx<float> a = v[0], b = v[1], c = v[2];
+      // (p, m): rotate (b, c) by -45deg -> ((b+c)/s2, (c-b)/s2); m = -(second)
+      float px = b.x, mx = c.x, py = b.y, my = c.y;
+      lift2(px, mx, t45, s45);
+      lift2(py, my, t45, s45);
+      mx = -mx;
+      my = -my;
+      // (y0, q): rotate (a, p) by -phi -> (cos a + sin p, -sin a + cos p); q = -(second)
+      float y0x = a.x, qx = px, y0y = a.y, qy = py;
+      lift2(y0x, qx, tph, sph);
+      lift2(y0y, qy, tph, sph);
+      qx = -qx;
+      qy = -qy;
+      // m' = +i m
+      const float m2x = -my, m2y = mx;
+      // (y1, y2) = ((q + m')/s2, (q - m')/s2): rotate (q, m') by -45deg, y2 = -(second)
+      float y1x = qx, y2x = m2x, y1y = qy, y2y = m2y;
+      lift2(y1x, y2x, t45, s45);
+      lift2(y1y, y2y, t45, s45);
+      v[0] = mk(y0x, y0y);
+      v[1] = mk(y1x, y1y);
+      v[2] = mk(-y2x, -y2y);
+    } else {
+      // exact mirror of the forward sequence: every lifting step undone in
+      // reverse order (shears with -t, -s), so that inverse(forward(x)) = x
+      // up to rounding for the rounded constants too
+      float y1x = v[1].x, y1y = v[1].y, y2x = -v[2].x, y2y = -v[2].y;
+      lift2(y1x, y2x, -t45, -s45);
+      lift2(y1y, y2y, -t45, -s45);
+      const float qx = y1x, qy = y1y, m2x = y2x, m2y = y2y;
+      // m = -i m'
+      float mx = m2y, my = -m2x;
+      float y0x = v[0].x, y0y = v[0].y, qxx = -qx, qyy = -qy;
+      lift2(y0x, qxx, -tph, -sph);
+      lift2(y0y, qyy, -tph, -sph);
+      const float ax = y0x, ay = y0y, px = qxx, py = qyy;
+      mx = -mx;
+      my = -my;
+      float bx = px, cx = mx, by = py, cy = my;
+      lift2(bx, cx, -t45, -s45);
+      lift2(by, cy, -t45, -s45);
+      v[0] = mk(ax, ay);
+      v[1] = mk(bx, by);
+      v[2] = mk(cx, cy);
+    }
   }
 };
 
 // DFT12 = DFT4 (inner) x DFT3 (outer), n = 3 n1 + n2, k = k1 + 4 k2,
-// internal twiddles exp(+2 pi i n2 k1 / 12).
+// internal twiddles exp(+2 pi i n2 k1 / 12).  The conjugate transform is the
+// exact mirror of the forward sequence (DFT3^-1, inverse twiddles, conjugate
+// DFT4), so that with rounded lifting constants the pair still composes to a
+// multiple of the identity; the conjugate algorithm run in forward order
+// leaves an O(eps) non-unitary residue that accumulates step after step.
 template <typename R, bool Inv>
 ESPEC_HD void dft12(cpx<R>* v) {
   cpx<R> a[3][4];
+  if constexpr (!Inv) {
 #pragma unroll
-  for (int n2 = 0; n2 < 3; ++n2) {
+    for (int n2 = 0; n2 < 3; ++n2) {
 #pragma unroll
-    for (int n1 = 0; n1 < 4; ++n1) a[n2][n1] = v[3 * n1 + n2];
-    dft4<R, Inv>(a[n2]);
-  }
-  a[1][1] = twid_const<R, 1, 12, Inv>(a[1][1]);
-  a[1][2] = twid_const<R, 2, 12, Inv>(a[1][2]);
-  a[1][3] = twid_const<R, 3, 12, Inv>(a[1][3]);
-  a[2][1] = twid_const<R, 2, 12, Inv>(a[2][1]);
-  a[2][2] = twid_const<R, 4, 12, Inv>(a[2][2]);
-  a[2][3] = twid_const<R, 6, 12, Inv>(a[2][3]);
+      for (int n1 = 0; n1 < 4; ++n1) a[n2][n1] = v[3 * n1 + n2];
+      dft4<R, false>(a[n2]);
+    }
+    a[1][1] = twid_const<R, 1, 12, false>(a[1][1]);
+    a[1][2] = twid_const<R, 2, 12, false>(a[1][2]);
+    a[1][3] = twid_const<R, 3, 12, false>(a[1][3]);
+    a[2][1] = twid_const<R, 2, 12, false>(a[2][1]);
+    a[2][2] = twid_const<R, 4, 12, false>(a[2][2]);
+    a[2][3] = twid_const<R, 6, 12, false>(a[2][3]);
 #pragma unroll
-  for (int k1 = 0; k1 < 4; ++k1) {
-    cpx<R> b[3] = {a[0][k1], a[1][k1], a[2][k1]};
-    Dft3<R, Inv>::run(b);
+    for (int k1 = 0; k1 < 4; ++k1) {
+      cpx<R> b[3] = {a[0][k1], a[1][k1], a[2][k1]};
+      Dft3<R, false>::run(b);
 #pragma unroll
-    for (int k2 = 0; k2 < 3; ++k2) v[k1 + 4 * k2] = b[k2];
+      for (int k2 = 0; k2 < 3; ++k2) v[k1 + 4 * k2] = b[k2];
+    }
+  } else {
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1) {
+      cpx<R> b[3] = {v[k1], v[k1 + 4], v[k1 + 8]};
+      Dft3<R, true>::run(b);
+#pragma unroll
+      for (int n2 = 0; n2 < 3; ++n2) a[n2][k1] = b[n2];
+    }
+    a[1][1] = twid_const<R, 1, 12, true>(a[1][1]);
+    a[1][2] = twid_const<R, 2, 12, true>(a[1][2]);
+    a[1][3] = twid_const<R, 3, 12, true>(a[1][3]);
+    a[2][1] = twid_const<R, 2, 12, true>(a[2][1]);
+    a[2][2] = twid_const<R, 4, 12, true>(a[2][2]);
+    a[2][3] = twid_const<R, 6, 12, true>(a[2][3]);
+#pragma unroll
+    for (int n2 = 0; n2 < 3; ++n2) {
+      dft4<R, true>(a[n2]);
+#pragma unroll
+      for (int n1 = 0; n1 < 4; ++n1) v[3 * n1 + n2] = a[n2][n1];
+    }
   }
 }
 

@@ -43,6 +43,15 @@ struct Plan {
     return o;
   }
   static constexpr int NTW = tw_off(S) > 0 ? tw_off(S) : 1;
+  static constexpr bool valid() {
+    int prod = 1;
+    for (int i = 0; i < S; ++i) {
+      if (P_ % r[i] != 0) return false;
+      prod *= r[i];
+    }
+    return prod == N_ && N_ % P_ == 0;
+  }
+  static_assert(valid(), "radices must multiply to N and divide P");
   // number of unitary radix-3 factors (FP32 form keeps them unitary)
   static __host__ __device__ constexpr int n3() {
     int c = 0;
@@ -138,12 +147,12 @@ struct SpoThread {
 
   rot_t tw[PL::NTW];
 
-  static __device__ __forceinline__ int sidx(int i) { return i; }
+  static ESPEC_HD int sidx(int i) { return i; }
 
-  __device__ void init_twiddles(int t) { init_stage<0>(t); }
+  ESPEC_HD void init_twiddles(int t) { init_stage<0>(t); }
 
   template <int s>
-  __device__ __forceinline__ void init_stage(int t) {
+  ESPEC_HD void init_stage(int t) {
     if constexpr (s < S) {
       constexpr int RR = PL::r[s];
       constexpr int M = PL::M(s);
@@ -162,7 +171,12 @@ struct SpoThread {
             const double phi = 6.283185307179586476925287 * (double)j / (double)M;
             if constexpr (sizeof(R) == 8) {
               RotD r;
+#ifdef __CUDA_ARCH__
               sincospi(2.0 * (double)j / (double)M, &r.s, &r.c);
+#else
+              r.s = sin(phi);
+              r.c = cos(phi);
+#endif
               tw[o + q * (RR - 1) + k - 1] = r;
             } else {
               tw[o + q * (RR - 1) + k - 1] = make_rotf(phi);
@@ -176,7 +190,7 @@ struct SpoThread {
 
   // forward stage s: butterflies then twiddles (DIF)
   template <int s>
-  __device__ __forceinline__ void fwd_bfly(cpx<R>* v) const {
+  ESPEC_HD void fwd_bfly(cpx<R>* v) const {
     constexpr int RR = PL::r[s];
     constexpr int m = PL::M(s) / RR;
     constexpr int Q = P / RR;
@@ -194,7 +208,7 @@ struct SpoThread {
 
   // inverse of stage s: conjugate twiddles then conjugate butterflies (DIT)
   template <int s>
-  __device__ __forceinline__ void inv_bfly(cpx<R>* v) const {
+  ESPEC_HD void inv_bfly(cpx<R>* v) const {
     constexpr int RR = PL::r[s];
     constexpr int m = PL::M(s) / RR;
     constexpr int Q = P / RR;
@@ -212,7 +226,7 @@ struct SpoThread {
 
   // positions of stage-s outputs held by thread t (slot q*R + k')
   template <int s>
-  static __device__ __forceinline__ int out_pos(int t, int q, int k) {
+  static ESPEC_HD int out_pos(int t, int q, int k) {
     constexpr int RR = PL::r[s];
     constexpr int m = PL::M(s) / RR;
     const int beta = t + T * q;
@@ -221,7 +235,7 @@ struct SpoThread {
   }
   // positions of stage-s inputs held by thread t (slot q*R + k)
   template <int s>
-  static __device__ __forceinline__ int in_pos(int t, int q, int k) {
+  static ESPEC_HD int in_pos(int t, int q, int k) {
     constexpr int RR = PL::r[s];
     constexpr int M = PL::M(s);
     constexpr int m = M / RR;
@@ -282,8 +296,14 @@ struct SpoThread {
     }
   }
 
+  // x position held in slot j at the start/end of a step (stage-0 inputs)
+  static ESPEC_HD int x_pos(int t, int j) {
+    constexpr int R0 = PL::r[0];
+    return in_pos<0>(t, j / R0, j % R0);
+  }
+
   // final-layout position of slot j (for the k-space table)
-  static __device__ __forceinline__ int final_pos(int t, int j) {
+  static ESPEC_HD int final_pos(int t, int j) {
     constexpr int RR = PL::r[S - 1];
     const int q = j / RR, k = j % RR;
     return (t + T * q) * RR + k;
@@ -319,7 +339,7 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
   double c0r = 0.0;
 #pragma unroll
   for (int j = 0; j < P; ++j) {
-    const int x = base + t + T * j;
+    const int x = base + Th::x_pos(t, j);
     const double2 p0 = a.psi0[x];
     c0r += p0.x * p0.x + p0.y * p0.y;
     v[j] = mk((R)p0.x, (R)p0.y);
@@ -346,7 +366,7 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
     // x-space phase
     if (step == 1) {
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = TB::apply(a.tab.h[base + t + T * j], v[j]);
+      for (int j = 0; j < P; ++j) v[j] = TB::apply(a.tab.h[base + Th::x_pos(t, j)], v[j]);
     } else {
 #pragma unroll
       for (int j = 0; j < P; ++j) v[j] = TB::apply(g[j], v[j]);
@@ -415,7 +435,7 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
   if (a.psi_out) {
 #pragma unroll
     for (int j = 0; j < P; ++j) {
-      const int x = base + t + T * j;
+      const int x = base + Th::x_pos(t, j);
       cpx<R> o = (a.nsteps > 0) ? TB::apply(a.tab.hm[x], v[j]) : v[j];
       a.psi_out[x] = make_double2((double)o.x, (double)o.y);
     }

@@ -79,7 +79,7 @@ def test_fp64_reference_defect_mode(oracle):
     assert np.max(np.abs(c - c_ref)) <= 1e-10
     # the defect is real: the corrected step differs
     c_ok, _ = gpu_batch(n, sh, sm, v, psi, dt, 400, "fp64")
-    assert np.max(np.abs(c_ok - c_ref)) > 1e-7
+    assert np.max(np.abs(c_ok - c_ref)) > 1e-9
 
 
 @pytest.mark.parametrize("kind", ["voptic", "smoothw"])
