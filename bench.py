@@ -42,6 +42,8 @@ def parse():
     ap.add_argument("--npk", type=int, default=4096)
     ap.add_argument("--nsteps", type=int, default=8000)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--sizes", default=None, help="comma list of packet sizes (profiling)")
     ap.add_argument("--cpu-sample-steps", type=int, default=400)
     ap.add_argument("--cpu-sample-packets", type=int, default=256)
     return ap.parse_args()
@@ -182,7 +184,8 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    w = W.morse_scan(npk=args.npk, nsteps=args.nsteps, seed=20261203 + rank)
+    sizes = tuple(int(x) for x in args.sizes.split(",")) if args.sizes else W.SCAN_SIZES
+    w = W.morse_scan(npk=args.npk, nsteps=args.nsteps, seed=20261203 + rank, sizes=sizes)
     pts_steps = float(w["off"][-1]) * w["nsteps"]
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
@@ -268,7 +271,8 @@ def main():
                            "precision": args.precision, "parallelism": f"packets x {world} GPU",
                            "l2": "tables and C(t) output exceed L2 (126 MB)",
                            "packets_per_s": args.npk * world / (ms * 1e-3)},
-                "roofline": roof, "cpu_baseline": cpu_baseline(args) if world == 1 else None,
+                "roofline": roof,
+                "cpu_baseline": cpu_baseline(args) if (world == 1 and not args.no_cpu) else None,
                 "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary()}
         print(json.dumps(line), flush=True)
     b.close()

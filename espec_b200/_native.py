@@ -23,6 +23,7 @@ EXPORTS = [
     "espec_last_error", "espec_version", "espec_device_ok",
     "espec_spo_create", "espec_spo_load", "espec_spo_run", "espec_spo_results",
     "espec_spo_device_c", "espec_spo_npoints", "espec_spo_destroy",
+    "espec_spo_set_variant", "espec_spo_variant_count",
 ]
 
 
@@ -54,6 +55,8 @@ def load():
     lib.espec_spo_device_c.argtypes = [vp]
     lib.espec_spo_device_c.restype = vp
     lib.espec_spo_npoints.argtypes = [vp]
+    lib.espec_spo_set_variant.argtypes = [vp, C.c_int, C.c_int]
+    lib.espec_spo_variant_count.restype = C.c_int
     lib.espec_spo_destroy.argtypes = [vp]
     lib.espec_spo_destroy.restype = None
     _lib = lib

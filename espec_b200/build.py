@@ -12,7 +12,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libespecgpu.so")
-SOURCES = ["spo1d.cu", "capi.cu"]
+SOURCES = ["spo1d.cu", "capi.cu", "spo1d_inst_f32_pow2.cu", "spo1d_inst_f32_r3.cu",
+           "spo1d_inst_f64_pow2.cu", "spo1d_inst_f64_r3.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -33,14 +34,24 @@ def needs_build():
 
 
 def build(force=False, verbose=False):
+    """Compile each translation unit in parallel, then link the shared library."""
     if not force and not needs_build():
         return LIB
-    cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-           "-I" + os.path.join(ROOT, "include"), "-I" + CSRC,
-           *[os.path.join(CSRC, s) for s in SOURCES], "-o", LIB + ".tmp", "-lcudart"]
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    common = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+              "-I" + os.path.join(ROOT, "include"), "-I" + CSRC]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.check_call(cmd)
+        common.append("-Xptxas=-v")
+    procs, objs = [], []
+    for src in SOURCES:
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        objs.append(obj)
+        procs.append((src, subprocess.Popen(common + ["-c", os.path.join(CSRC, src), "-o", obj])))
+    bad = [src for src, pr in procs if pr.wait() != 0]
+    if bad:
+        raise RuntimeError("nvcc failed for " + ", ".join(bad))
+    subprocess.check_call([nvcc(), *ARCH, "-shared", "-o", LIB + ".tmp", *objs, "-lcudart"])
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

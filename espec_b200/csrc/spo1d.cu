@@ -12,7 +12,7 @@
 
 #include "espec_gpu.h"
 #include "espec_internal.h"
-#include "spo1d.cuh"
+#include "spo1d_launch.cuh"
 
 namespace espec {
 
@@ -98,8 +98,7 @@ __device__ __forceinline__ Tab<float>::phase_t phase32(double phi, double a) {
   Tab<float>::phase_t o;
   o.t = r.t;
   o.s = r.s;
-  o.g = r.g;
-  o.a = (float)a;
+  o.ag = (float)(r.g * a);
   return o;
 }
 
@@ -151,43 +150,6 @@ __global__ void spo_setup_kernel(SetupArgs a) {
 // ---------------------------------------------------------------------------
 // per-size-class dispatch
 // ---------------------------------------------------------------------------
-template <typename R, class PL, bool kCap, bool kQuirk>
-static cudaError_t launch_class(const SpoArgs<R>& a, int nblocks, cudaStream_t st) {
-  auto kern = spo1d_kernel<R, PL, kCap, kQuirk>;
-  const size_t smem = spo1d_smem_bytes<R, PL>();
-  static bool attr_set = false;  // per instantiation
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  kern<<<nblocks, PL::T, smem, st>>>(a);
-  return cudaGetLastError();
-}
-
-template <typename R, class PL>
-static cudaError_t launch_any(const SpoArgs<R>& a, int nblocks, bool quirk, cudaStream_t st) {
-  if constexpr (sizeof(R) == 8) {
-    if (quirk) return launch_class<R, PL, false, true>(a, nblocks, st);
-  }
-  return launch_class<R, PL, false, false>(a, nblocks, st);
-}
-
-template <typename R>
-static cudaError_t launch_n(int n, const SpoArgs<R>& a, int nblocks, bool quirk, cudaStream_t st) {
-  switch (n) {
-    case 256: return launch_any<R, DefaultPlan<256>::type>(a, nblocks, quirk, st);
-    case 384: return launch_any<R, DefaultPlan<384>::type>(a, nblocks, quirk, st);
-    case 512: return launch_any<R, DefaultPlan<512>::type>(a, nblocks, quirk, st);
-    case 768: return launch_any<R, DefaultPlan<768>::type>(a, nblocks, quirk, st);
-    case 1024: return launch_any<R, DefaultPlan<1024>::type>(a, nblocks, quirk, st);
-    case 1536: return launch_any<R, DefaultPlan<1536>::type>(a, nblocks, quirk, st);
-    case 2048: return launch_any<R, DefaultPlan<2048>::type>(a, nblocks, quirk, st);
-    case 4096: return launch_any<R, DefaultPlan<4096>::type>(a, nblocks, quirk, st);
-    default: return cudaErrorInvalidValue;
-  }
-}
-
 static bool size_supported(int n) {
   switch (n) {
     case 256: case 384: case 512: case 768: case 1024: case 1536: case 2048: case 4096:
@@ -197,25 +159,53 @@ static bool size_supported(int n) {
   }
 }
 
-template <class PL>
-static void fill_plan_info(int n, std::vector<int>& kap, int& n3) {
-  kap = final_freq<PL>();
-  n3 = PL::n3();
-  (void)n;
+static bool is_pow2(int n) { return (n & (n - 1)) == 0; }
+
+template <typename R>
+static cudaError_t launch_n(int n, int v, const SpoArgs<R>& a, int nblocks, bool quirk,
+                            cudaStream_t st) {
+  if constexpr (sizeof(R) == 4) {
+    return is_pow2(n) ? spo_launch_f32_pow2(n, v, a, nblocks, st)
+                      : spo_launch_f32_r3(n, v, a, nblocks, st);
+  } else {
+    return is_pow2(n) ? spo_launch_f64_pow2(n, v, a, nblocks, quirk, st)
+                      : spo_launch_f64_r3(n, v, a, nblocks, quirk, st);
+  }
 }
 
-static void plan_info(int n, std::vector<int>& kap, int& n3) {
+template <class PL>
+static void fill_plan_info(std::vector<int>& kap, int& n3) {
+  kap = final_freq<PL>();
+  n3 = PL::n3();
+}
+
+template <int N>
+static void plan_info_n(int v, std::vector<int>& kap, int& n3) {
+  if (v == 3) fill_plan_info<typename AltPlan<N>::type>(kap, n3);
+  else fill_plan_info<typename DefaultPlan<N>::type>(kap, n3);
+}
+
+// final-layout frequencies and radix-3 count of the plan behind variant v
+static void plan_info(int n, int v, std::vector<int>& kap, int& n3) {
   switch (n) {
-    case 256: fill_plan_info<DefaultPlan<256>::type>(n, kap, n3); break;
-    case 384: fill_plan_info<DefaultPlan<384>::type>(n, kap, n3); break;
-    case 512: fill_plan_info<DefaultPlan<512>::type>(n, kap, n3); break;
-    case 768: fill_plan_info<DefaultPlan<768>::type>(n, kap, n3); break;
-    case 1024: fill_plan_info<DefaultPlan<1024>::type>(n, kap, n3); break;
-    case 1536: fill_plan_info<DefaultPlan<1536>::type>(n, kap, n3); break;
-    case 2048: fill_plan_info<DefaultPlan<2048>::type>(n, kap, n3); break;
-    case 4096: fill_plan_info<DefaultPlan<4096>::type>(n, kap, n3); break;
+    case 256: plan_info_n<256>(v, kap, n3); break;
+    case 384: plan_info_n<384>(v, kap, n3); break;
+    case 512: plan_info_n<512>(v, kap, n3); break;
+    case 768: plan_info_n<768>(v, kap, n3); break;
+    case 1024: plan_info_n<1024>(v, kap, n3); break;
+    case 1536: plan_info_n<1536>(v, kap, n3); break;
+    case 2048: plan_info_n<2048>(v, kap, n3); break;
+    case 4096: plan_info_n<4096>(v, kap, n3); break;
     default: break;
   }
+}
+
+// default variant per size and precision (set from autotuner measurements
+// on B200; see espec_b200/autotune.py)
+static int default_variant(int n, int precision) {
+  (void)n;
+  (void)precision;
+  return 0;
 }
 
 }  // namespace espec
@@ -234,7 +224,9 @@ struct espec_spo_plan {
     int n;
     int count;
     SpoPacket* d_pk;
+    int variant;
   };
+  bool index_dirty = true;
   std::vector<Class> classes;
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
@@ -278,6 +270,50 @@ static void plan_free(espec_spo_plan* p) {
     if (e_ != cudaSuccess) return set_cuda_error(#call, e_);     \
   } while (0)
 
+// host-built index tables: DIGT, final-position frequencies of the chosen
+// plans, packet ids and kinetic scales
+static int spo_index_tables(espec_spo_plan* p) {
+  const size_t np = p->npts;
+  const int npk = p->npk;
+  int rc = 0;
+  std::vector<double> tc(np), kscale(npk);
+  std::vector<int> kperm(np), pk_of(np);
+  std::map<int, int> var_of;
+  for (auto& c : p->classes) var_of[c.n] = c.variant;
+  std::map<int, std::pair<std::vector<int>, int>> kap_cache;
+  for (int i = 0; i < npk; ++i) {
+    const int n = p->n[i];
+    digt_1d(n, p->sh[i], p->sm[i], tc.data() + p->off[i]);
+    auto it = kap_cache.find(n);
+    if (it == kap_cache.end()) {
+      std::vector<int> kap;
+      int n3 = 0;
+      plan_info(n, var_of[n], kap, n3);
+      it = kap_cache.emplace(n, std::make_pair(kap, n3)).first;
+    }
+    for (int j = 0; j < n; ++j) {
+      kperm[p->off[i] + j] = it->second.first[j];
+      pk_of[p->off[i] + j] = i;
+    }
+    // round trip gain: N, divided by 3 per unitary radix-3 stage of the FP32 form
+    double gain = n;
+    if (p->precision == ESPEC_MIXED)
+      for (int k = 0; k < it->second.second; ++k) gain /= 3.0;
+    kscale[i] = 1.0 / gain;
+  }
+  if ((rc = ck(cudaMemcpy(p->d_tc, tc.data(), np * 8, cudaMemcpyHostToDevice), "H2D"))) return rc;
+  if ((rc = ck(cudaMemcpy(p->d_kperm, kperm.data(), np * 4, cudaMemcpyHostToDevice), "H2D")))
+    return rc;
+  if ((rc = ck(cudaMemcpy(p->d_pk_of, pk_of.data(), np * 4, cudaMemcpyHostToDevice), "H2D")))
+    return rc;
+  if ((rc = ck(cudaMemcpy(p->d_pk_off, p->off.data(), npk * 4, cudaMemcpyHostToDevice), "H2D")))
+    return rc;
+  if ((rc = ck(cudaMemcpy(p->d_kscale, kscale.data(), npk * 8, cudaMemcpyHostToDevice), "H2D")))
+    return rc;
+  p->index_dirty = false;
+  return ESPEC_OK;
+}
+
 extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
                                 const double* sh, const double* sm, double dt_fs, int precision,
                                 int absorb, int quirks) {
@@ -318,7 +354,8 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
   std::map<int, std::vector<SpoPacket>, std::greater<int>> cls;
   for (int i = 0; i < npk; ++i) cls[p->n[i]].push_back(SpoPacket{p->off[i], 0});
   for (auto& kv : cls) {
-    espec_spo_plan::Class c{kv.first, (int)kv.second.size(), nullptr};
+    espec_spo_plan::Class c{kv.first, (int)kv.second.size(), nullptr,
+                            default_variant(kv.first, precision)};
     if ((rc = ck(cudaMalloc(&c.d_pk, sizeof(SpoPacket) * c.count), "cudaMalloc"))) return fail(rc);
     p->classes.push_back(c);
     cudaStream_t s;
@@ -343,7 +380,7 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
   if (precision == ESPEC_FP64) {
     p->tab_bytes = np * 16 * 5;
   } else {
-    p->tab_bytes = np * (16 * 4 + 8);
+    p->tab_bytes = np * (12 * 4 + 8);
   }
   if ((rc = ck(cudaMalloc(&p->d_tab, p->tab_bytes), "cudaMalloc"))) return fail(rc);
   if (quirks & ESPEC_Q_SPO_INPLACE) {
@@ -364,44 +401,29 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
     p->t32.h = c + np;
     p->t32.hm = c + 2 * np;
     p->t32.k = c + 3 * np;
-    p->t32.w = (cpx<float>*)(c + 4 * np);
+    p->t32.w = (cpx<float>*)(c + 4 * np);  // 12-byte phases: w stays 4-byte aligned
   }
-  // host-built index tables: DIGT, final-position frequencies, packet ids
-  std::vector<double> tc(np), kscale(npk);
-  std::vector<int> kperm(np), pk_of(np);
-  std::map<int, std::pair<std::vector<int>, int>> kap_cache;
-  for (int i = 0; i < npk; ++i) {
-    const int n = p->n[i];
-    digt_1d(n, p->sh[i], p->sm[i], tc.data() + p->off[i]);
-    auto it = kap_cache.find(n);
-    if (it == kap_cache.end()) {
-      std::vector<int> kap;
-      int n3 = 0;
-      plan_info(n, kap, n3);
-      it = kap_cache.emplace(n, std::make_pair(kap, n3)).first;
-    }
-    for (int j = 0; j < n; ++j) {
-      kperm[p->off[i] + j] = it->second.first[j];
-      pk_of[p->off[i] + j] = i;
-    }
-    // round trip gain: N, divided by 3 per unitary radix-3 stage of the FP32 form
-    double gain = n;
-    if (precision == ESPEC_MIXED)
-      for (int k = 0; k < it->second.second; ++k) gain /= 3.0;
-    kscale[i] = 1.0 / gain;
-  }
-  if ((rc = ck(cudaMemcpy(p->d_tc, tc.data(), np * 8, cudaMemcpyHostToDevice), "H2D"))) return fail(rc);
-  if ((rc = ck(cudaMemcpy(p->d_kperm, kperm.data(), np * 4, cudaMemcpyHostToDevice), "H2D")))
-    return fail(rc);
-  if ((rc = ck(cudaMemcpy(p->d_pk_of, pk_of.data(), np * 4, cudaMemcpyHostToDevice), "H2D")))
-    return fail(rc);
-  if ((rc = ck(cudaMemcpy(p->d_pk_off, p->off.data(), npk * 4, cudaMemcpyHostToDevice), "H2D")))
-    return fail(rc);
-  if ((rc = ck(cudaMemcpy(p->d_kscale, kscale.data(), npk * 8, cudaMemcpyHostToDevice), "H2D")))
-    return fail(rc);
+  if ((rc = spo_index_tables(p))) return fail(rc);
   *out = p;
   return ESPEC_OK;
 }
+
+extern "C" int espec_spo_set_variant(espec_spo_plan* p, int npts, int variant) {
+  if (!p) return set_error(ESPEC_EINVAL, "null plan");
+  if (variant < 0 || variant >= kNumVariants) return set_error(ESPEC_EINVAL, "unknown variant");
+  bool found = false;
+  for (auto& c : p->classes)
+    if (c.n == npts) {
+      c.variant = variant;
+      found = true;
+    }
+  if (!found) return set_error(ESPEC_EINVAL, "no packet of that size in the plan");
+  p->index_dirty = true;
+  p->loaded = false;  // tables depend on the plan's final layout
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spo_variant_count(void) { return kNumVariants; }
 
 extern "C" void espec_spo_destroy(espec_spo_plan* p) {
   if (!p) return;
@@ -413,6 +435,10 @@ extern "C" int espec_spo_npoints(const espec_spo_plan* p) { return p ? p->npts :
 
 // set-up of all tables from state already in the plan's device buffers
 static int spo_build_tables(espec_spo_plan* p, cudaStream_t st) {
+  if (p->index_dirty) {
+    int rc = spo_index_tables(p);
+    if (rc) return rc;
+  }
   SetupArgs a{};
   a.vpot = p->d_vpot;
   a.vabc = p->d_vabc;
@@ -503,7 +529,7 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
       a.kq_s = p->d_kq_s;
       a.kq_scale = 1.0 / c.n;
       a.nsteps = nsteps;
-      e = launch_n<double>(c.n, a, c.count, quirk, cs);
+      e = launch_n<double>(c.n, c.variant, a, c.count, quirk, cs);
     } else {
       SpoArgs<float> a{};
       a.tab = p->t32;
@@ -512,7 +538,7 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
       a.psi_out = p->d_psi;
       a.c_out = p->d_c;
       a.nsteps = nsteps;
-      e = launch_n<float>(c.n, a, c.count, false, cs);
+      e = launch_n<float>(c.n, c.variant, a, c.count, false, cs);
     }
     if (e != cudaSuccess) return set_cuda_error("spo1d_kernel launch", e);
     ESPEC_CK(cudaEventRecord(p->events[ci], cs));

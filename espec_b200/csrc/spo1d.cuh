@@ -16,6 +16,8 @@
 // half-swaps of spofft.f:120-133/178-191 (an fftshift before the forward and
 // after the inverse transform) cancel exactly and are not performed.
 #pragma once
+#include <string.h>
+
 #include "cplx.cuh"
 
 namespace espec {
@@ -43,6 +45,34 @@ struct Plan {
     return o;
   }
   static constexpr int NTW = tw_off(S) > 0 ? tw_off(S) : 1;
+  static __host__ __device__ constexpr int m(int s) { return M(s) / r[s]; }
+  static __host__ __device__ constexpr int Q(int s) { return P_ / r[s]; }
+  // butterflies of a warp form whole sub-problems at stage s
+  static __host__ __device__ constexpr bool warp_aligned(int s) { return (32 * Q(s)) % m(s) == 0; }
+  // the exchange between stages s and s+1 stays inside each warp
+  static __host__ __device__ constexpr bool local(int s) {
+    return T <= 32 || (warp_aligned(s) && warp_aligned(s + 1));
+  }
+  static __host__ __device__ constexpr int n_local() {
+    int c = 0;
+    for (int i = 0; i + 1 < S; ++i) c += local(i) ? 1 : 0;
+    return c;
+  }
+  static __host__ __device__ constexpr int n_global() { return (S - 1) - n_local(); }
+  // Shared buffers: CTA-wide exchanges alternate between buffers 0 and 1,
+  // warp-local exchanges between buffers 2 and 3 (each kind alternates over
+  // the forward then the inverse sequence; both counts per step are even).
+  static __host__ __device__ constexpr int buf_fwd(int s) {
+    int c = 0;
+    for (int i = 0; i < s; ++i) c += (local(i) == local(s)) ? 1 : 0;
+    return (local(s) ? 2 : 0) + (c & 1);
+  }
+  static __host__ __device__ constexpr int buf_inv(int s) {
+    int c = local(s) ? n_local() : n_global();
+    for (int i = S - 2; i > s; --i) c += (local(i) == local(s)) ? 1 : 0;
+    return (local(s) ? 2 : 0) + (c & 1);
+  }
+  static constexpr int NBUF = (n_local() > 0 && n_global() > 0) ? 4 : 2;
   static constexpr bool valid() {
     int prod = 1;
     for (int i = 0; i < S; ++i) {
@@ -63,14 +93,17 @@ struct Plan {
 
 template <int N>
 struct DefaultPlan;
+// Default plans: one cross-warp stage first, then stages whose sub-problems
+// fit inside one warp (32 * P points), so that only one exchange per
+// transform needs a CTA-wide barrier and the others a warp barrier.
 template <> struct DefaultPlan<256>  { using type = Plan<256, 8, 8, 8, 4>; };
-template <> struct DefaultPlan<512>  { using type = Plan<512, 8, 8, 8, 8>; };
-template <> struct DefaultPlan<1024> { using type = Plan<1024, 8, 8, 8, 8, 2>; };
+template <> struct DefaultPlan<512>  { using type = Plan<512, 8, 2, 8, 8, 4>; };
+template <> struct DefaultPlan<1024> { using type = Plan<1024, 8, 4, 8, 8, 4>; };
 template <> struct DefaultPlan<2048> { using type = Plan<2048, 8, 8, 8, 8, 4>; };
-template <> struct DefaultPlan<4096> { using type = Plan<4096, 16, 16, 16, 16>; };
+template <> struct DefaultPlan<4096> { using type = Plan<4096, 16, 8, 16, 16, 2>; };
 template <> struct DefaultPlan<384>  { using type = Plan<384, 12, 12, 4, 4, 2>; };
-template <> struct DefaultPlan<768>  { using type = Plan<768, 12, 12, 4, 4, 4>; };
-template <> struct DefaultPlan<1536> { using type = Plan<1536, 12, 12, 4, 4, 4, 2>; };
+template <> struct DefaultPlan<768>  { using type = Plan<768, 12, 2, 12, 4, 4, 2>; };
+template <> struct DefaultPlan<1536> { using type = Plan<1536, 12, 4, 12, 4, 4, 2>; };
 
 // ---------------------------------------------------------------------------
 // per-precision table formats
@@ -82,24 +115,25 @@ struct Tab<double> {
   using rot_t = RotD;
   using phase_t = cpx<double>;   // complex factor (rotation x magnitude)
   using weight_t = cpx<double>;
-  static __device__ __forceinline__ cpx<double> apply(const phase_t& f, cpx<double> a) {
+  static ESPEC_HD cpx<double> apply(const phase_t& f, cpx<double> a) {
     return mk(fma(a.x, f.x, -a.y * f.y), fma(a.x, f.y, a.y * f.x));
   }
 };
 template <>
 struct Tab<float> {
   using rot_t = RotF;
+  // lifting rotation by phi' followed by the real factor ag = g * a (the
+  // exact negation of make_rotf folded into the magnitude a)
   struct phase_t {
-    float t, s, g, a;  // lifting rotation, then real scale a
+    float t, s, ag;
   };
   using weight_t = cpx<float>;
-  static __device__ __forceinline__ cpx<float> apply(const phase_t& f, cpx<float> v) {
-    RotF r;
-    r.t = f.t;
-    r.s = f.s;
-    r.g = f.g;
-    cpx<float> o = rot<false>(r, v);
-    return mk(o.x * f.a, o.y * f.a);
+  static ESPEC_HD cpx<float> apply(const phase_t& f, cpx<float> v) {
+    float x = v.x, y = v.y;
+    x = fmaf(-f.t, y, x);
+    y = fmaf(f.s, x, y);
+    x = fmaf(-f.t, y, x);
+    return mk(x * f.ag, y * f.ag);
   }
 };
 
@@ -147,9 +181,21 @@ struct SpoThread {
 
   rot_t tw[PL::NTW];
 
-  static ESPEC_HD int sidx(int i) { return i; }
+  // shared-memory swizzle: flips the low 4 bits of an element index with
+  // bits 3..7, a bijection inside every 16-element block that makes all the
+  // exchange patterns of the plans above bank-conflict free (8- and 16-byte
+  // elements)
+  static ESPEC_HD int sidx(int i) { return i ^ (((i >> 3) ^ (i >> 4)) & 15); }
 
   ESPEC_HD void init_twiddles(int t) { init_stage<0>(t); }
+
+  // butterfly handled by thread t in slot q of stage s: warp-major, lanes
+  // cyclic inside the warp (consecutive lanes -> consecutive butterflies)
+  template <int s>
+  static ESPEC_HD int beta(int t, int q) {
+    constexpr int Q = PL::Q(s);
+    return (t >> 5) * 32 * Q + (t & 31) + 32 * q;
+  }
 
   template <int s>
   ESPEC_HD void init_stage(int t) {
@@ -162,8 +208,7 @@ struct SpoThread {
         constexpr int o = PL::tw_off(s);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-          const int beta = t + T * q;
-          const int n1 = beta % m;
+          const int n1 = beta<s>(t, q) % m;
 #pragma unroll
           for (int k = 1; k < RR; ++k) {
             int j = (n1 * k) % M;
@@ -229,8 +274,8 @@ struct SpoThread {
   static ESPEC_HD int out_pos(int t, int q, int k) {
     constexpr int RR = PL::r[s];
     constexpr int m = PL::M(s) / RR;
-    const int beta = t + T * q;
-    const int p = beta / m, n1 = beta % m;
+    const int b = beta<s>(t, q);
+    const int p = b / m, n1 = b % m;
     return (p * RR + k) * m + n1;
   }
   // positions of stage-s inputs held by thread t (slot q*R + k)
@@ -239,9 +284,18 @@ struct SpoThread {
     constexpr int RR = PL::r[s];
     constexpr int M = PL::M(s);
     constexpr int m = M / RR;
-    const int beta = t + T * q;
-    const int p = beta / m, n1 = beta % m;
+    const int b = beta<s>(t, q);
+    const int p = b / m, n1 = b % m;
     return p * M + n1 + m * k;
+  }
+
+  template <int s>
+  static __device__ __forceinline__ void xsync() {
+    if constexpr (PL::local(s)) {
+      __syncwarp();
+    } else {
+      __syncthreads();
+    }
   }
 
   // exchange after forward stage s (s < S-1): outputs of s -> inputs of s+1
@@ -253,7 +307,7 @@ struct SpoThread {
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
       for (int k = 0; k < R0; ++k) buf[sidx(out_pos<s>(t, q, k))] = v[q * R0 + k];
-    group_sync<T>();
+    xsync<s>();
 #pragma unroll
     for (int q = 0; q < Q1; ++q)
 #pragma unroll
@@ -268,7 +322,7 @@ struct SpoThread {
     for (int q = 0; q < Q1; ++q)
 #pragma unroll
       for (int k = 0; k < R1; ++k) buf[sidx(in_pos<s + 1>(t, q, k))] = v[q * R1 + k];
-    group_sync<T>();
+    xsync<s>();
 #pragma unroll
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
@@ -276,22 +330,24 @@ struct SpoThread {
   }
 
   template <int s>
-  __device__ __forceinline__ void forward(cpx<R>* v, cpx<R>* b0, cpx<R>* b1, int t) const {
+  __device__ __forceinline__ void forward(cpx<R>* v, cpx<R>* bufs, int t) const {
     if constexpr (s < S) {
       fwd_bfly<s>(v);
       if constexpr (s + 1 < S) {
-        xchg_fwd<s>(v, (s & 1) ? b1 : b0, t);
-        forward<s + 1>(v, b0, b1, t);
+        constexpr int b = PL::NBUF == 4 ? PL::buf_fwd(s) : (PL::buf_fwd(s) & 1);
+        xchg_fwd<s>(v, bufs + b * N, t);
+        forward<s + 1>(v, bufs, t);
       }
     }
   }
   template <int s>
-  __device__ __forceinline__ void inverse(cpx<R>* v, cpx<R>* b0, cpx<R>* b1, int t) const {
+  __device__ __forceinline__ void inverse(cpx<R>* v, cpx<R>* bufs, int t) const {
     if constexpr (s >= 0) {
       inv_bfly<s>(v);
       if constexpr (s > 0) {
-        xchg_inv<s - 1>(v, (s & 1) ? b1 : b0, t);  // exchange of stage s-1 uses buffer (s-1+1)&1
-        inverse<s - 1>(v, b0, b1, t);
+        constexpr int b = PL::NBUF == 4 ? PL::buf_inv(s - 1) : (PL::buf_inv(s - 1) & 1);
+        xchg_inv<s - 1>(v, bufs + b * N, t);
+        inverse<s - 1>(v, bufs, t);
       }
     }
   }
@@ -305,24 +361,89 @@ struct SpoThread {
   // final-layout position of slot j (for the k-space table)
   static ESPEC_HD int final_pos(int t, int j) {
     constexpr int RR = PL::r[S - 1];
-    const int q = j / RR, k = j % RR;
-    return (t + T * q) * RR + k;
+    return out_pos<S - 1>(t, j / RR, j % RR);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// where the per-point tables live during the time loop
+//   kTab = 0: registers (P phases g, P kinetic phases k, P weights w per thread)
+//   kTab = 1: shared memory, structure of arrays [component][slot][thread]
+//            (conflict-free: consecutive threads read consecutive words)
+// ---------------------------------------------------------------------------
+template <typename R, class PL, int kTab>
+struct TabStore;
+
+template <typename R, class PL>
+struct TabStore<R, PL, 0> {
+  using ph = typename Tab<R>::phase_t;
+  using wt = typename Tab<R>::weight_t;
+  static constexpr size_t smem_bytes = 0;
+  ph g[PL::P], k[PL::P];
+  wt w[PL::P];
+  __device__ __forceinline__ void init(void*) {}
+  __device__ __forceinline__ void put(int j, int, const ph& gg, const ph& kk, const wt& ww) {
+    g[j] = gg;
+    k[j] = kk;
+    w[j] = ww;
+  }
+  __device__ __forceinline__ ph G(int j, int) const { return g[j]; }
+  __device__ __forceinline__ ph K(int j, int) const { return k[j]; }
+  __device__ __forceinline__ wt W(int j, int) const { return w[j]; }
+};
+
+template <typename R, class PL>
+struct TabStore<R, PL, 1> {
+  using ph = typename Tab<R>::phase_t;
+  using wt = typename Tab<R>::weight_t;
+  static constexpr int CP = sizeof(ph) / sizeof(R);  // scalars per phase
+  static constexpr int CW = sizeof(wt) / sizeof(R);
+  static constexpr int P = PL::P, T = PL::T;
+  static constexpr size_t smem_bytes = (size_t)(2 * CP + CW) * PL::N * sizeof(R);
+  R* base;
+  __device__ __forceinline__ void init(void* p) { base = reinterpret_cast<R*>(p); }
+  template <typename X, int C>
+  __device__ __forceinline__ void st(R* arr, int j, int t, const X& x) {
+    R tmp[C];
+    memcpy(tmp, &x, sizeof(X));
+#pragma unroll
+    for (int c = 0; c < C; ++c) arr[(c * P + j) * T + t] = tmp[c];
+  }
+  template <typename X, int C>
+  __device__ __forceinline__ X ld(const R* arr, int j, int t) const {
+    R tmp[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) tmp[c] = arr[(c * P + j) * T + t];
+    X x;
+    memcpy(&x, tmp, sizeof(X));
+    return x;
+  }
+  __device__ __forceinline__ void put(int j, int t, const ph& gg, const ph& kk, const wt& ww) {
+    st<ph, CP>(base, j, t, gg);
+    st<ph, CP>(base + CP * PL::N, j, t, kk);
+    st<wt, CW>(base + 2 * CP * PL::N, j, t, ww);
+  }
+  __device__ __forceinline__ ph G(int j, int t) const { return ld<ph, CP>(base, j, t); }
+  __device__ __forceinline__ ph K(int j, int t) const { return ld<ph, CP>(base + CP * PL::N, j, t); }
+  __device__ __forceinline__ wt W(int j, int t) const {
+    return ld<wt, CW>(base + 2 * CP * PL::N, j, t);
   }
 };
 
 // ---------------------------------------------------------------------------
 // the kernel: one CTA per packet of size N
 // ---------------------------------------------------------------------------
-template <typename R, class PL, bool kCap, bool kQuirk>
-__global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
+template <typename R, class PL, bool kCap, bool kQuirk, int kTab, int kMinBlocks>
+__global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) {
   constexpr int N = PL::N, P = PL::P, T = PL::T;
   constexpr int NW = (T + 31) / 32;
   using Th = SpoThread<R, PL>;
   using TB = Tab<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  cpx<R>* b0 = reinterpret_cast<cpx<R>*>(smem_raw);
-  cpx<R>* b1 = b0 + N;
-  double2* cpart = reinterpret_cast<double2*>(b1 + N);  // [2][NW]
+  cpx<R>* bufs = reinterpret_cast<cpx<R>*>(smem_raw);
+  double2* cpart = reinterpret_cast<double2*>(bufs + PL::NBUF * N);  // [2][NW]
+  TabStore<R, PL, kTab> tab;
+  tab.init(cpart + 2 * NW);
 
   const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
@@ -334,8 +455,6 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
   th.init_twiddles(t);
 
   cpx<R> v[P];
-  typename TB::phase_t g[P], kk[P];
-  typename TB::weight_t w[P];
   double c0r = 0.0;
 #pragma unroll
   for (int j = 0; j < P; ++j) {
@@ -343,9 +462,9 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
     const double2 p0 = a.psi0[x];
     c0r += p0.x * p0.x + p0.y * p0.y;
     v[j] = mk((R)p0.x, (R)p0.y);
-    g[j] = a.tab.g[x];
-    w[j] = a.tab.w[x];
-    if constexpr (!kQuirk) kk[j] = a.tab.k[base + Th::final_pos(t, j)];
+    typename TB::phase_t kk{};
+    if constexpr (!kQuirk) kk = a.tab.k[base + Th::final_pos(t, j)];
+    tab.put(j, t, a.tab.g[x], kk, a.tab.w[x]);
   }
   // C(0) = <psi0|psi0>
   {
@@ -369,9 +488,9 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
       for (int j = 0; j < P; ++j) v[j] = TB::apply(a.tab.h[base + Th::x_pos(t, j)], v[j]);
     } else {
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = TB::apply(g[j], v[j]);
+      for (int j = 0; j < P; ++j) v[j] = TB::apply(tab.G(j, t), v[j]);
     }
-    th.template forward<0>(v, b0, b1, t);
+    th.template forward<0>(v, bufs, t);
     // sum of the previous step's partial C(t): all partials are visible after
     // the first exchange barrier of this step
     if (T > 32 && t == 0 && step > 1) {
@@ -396,14 +515,15 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
       }
     } else {
 #pragma unroll
-      for (int j = 0; j < P; ++j) v[j] = TB::apply(kk[j], v[j]);
+      for (int j = 0; j < P; ++j) v[j] = TB::apply(tab.K(j, t), v[j]);
     }
-    th.template inverse<PL::S - 1>(v, b0, b1, t);
+    th.template inverse<PL::S - 1>(v, bufs, t);
     // partial C(t) = sum w phi in FP64
     double cr = 0.0, ci = 0.0;
 #pragma unroll
     for (int j = 0; j < P; ++j) {
-      const double wx = (double)w[j].x, wy = (double)w[j].y;
+      const typename TB::weight_t wj = tab.W(j, t);
+      const double wx = (double)wj.x, wy = (double)wj.y;
       const double vx = (double)v[j].x, vy = (double)v[j].y;
       cr = fma(wx, vx, fma(-wy, vy, cr));
       ci = fma(wx, vy, fma(wy, vx, ci));
@@ -442,9 +562,10 @@ __global__ void __launch_bounds__(PL::T) spo1d_kernel(SpoArgs<R> a) {
   }
 }
 
-template <typename R, class PL>
+template <typename R, class PL, int kTab>
 constexpr size_t spo1d_smem_bytes() {
-  return 2 * sizeof(cpx<R>) * PL::N + 2 * sizeof(double2) * ((PL::T + 31) / 32);
+  return PL::NBUF * sizeof(cpx<R>) * PL::N + 2 * sizeof(double2) * ((PL::T + 31) / 32) +
+         TabStore<R, PL, kTab>::smem_bytes;
 }
 
 }  // namespace espec

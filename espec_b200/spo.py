@@ -34,6 +34,11 @@ class SpoBatch:
         N.check(rc, "espec_spo_create")
         self.nsteps = None
 
+    def set_variant(self, npts, variant):
+        """Choose the kernel variant of one packet size (before load)."""
+        N.check(N.load().espec_spo_set_variant(self._h, int(npts), int(variant)),
+                "espec_spo_set_variant")
+
     def load(self, vpot, psi, vabc=None, stream=None):
         """vpot, psi (complex or real), vabc: host numpy arrays (concatenated),
         or device tensors (torch float64) with psi given as (re, im)."""

@@ -77,6 +77,11 @@ int espec_spo_load(espec_spo_plan* plan, const double* vpot, const double* vabc,
 int espec_spo_run(espec_spo_plan* plan, int nsteps, void* stream);
 int espec_spo_results(espec_spo_plan* plan, double* c_re, double* c_im,
                       double* psi_re, double* psi_im, int where, void* stream);
+/* Kernel variant for the packets of size npts (0..espec_spo_variant_count()-1):
+ * radix plan, location of the per-point tables and register budget.  Call
+ * before espec_spo_load.  Defaults come from autotuning on B200. */
+int espec_spo_set_variant(espec_spo_plan* plan, int npts, int variant);
+int espec_spo_variant_count(void);
 /* device pointer of the C(t) buffer (double2, packet-major) */
 const void* espec_spo_device_c(const espec_spo_plan* plan);
 int espec_spo_npoints(const espec_spo_plan* plan);

@@ -127,3 +127,23 @@ def test_scan_subset_mixed_vs_fp64():
     c32, _ = gpu_batch(w["n"], w["sh"], w["sm"], w["vpot"], w["psi"], w["dt_fs"], 1000, "mixed")
     err = np.max(np.abs(c64 - c32))
     assert err <= 5e-6, err
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_every_variant_matches_oracle(oracle, variant):
+    """Each kernel variant (plan / table location / register budget) of each
+    packet size gives the oracle's C(t): FP64 to 1e-10, mixed to 5e-6."""
+    n, off, sh, sm, v, psi = random_packets(SIZES, seed=23)
+    dt = 0.5 * W.SHFS
+    c_ref, p_ref = oracle_batch(oracle, n, off, sh, sm, v, psi, dt, 200)
+    for prec, tol in (("fp64", 1e-10), ("mixed", 5e-6)):
+        b = E.SpoBatch(n, sh, sm, dt, precision=prec)
+        for size in SIZES:
+            b.set_variant(size, variant)
+        b.load(v, psi)
+        b.run(200)
+        c, p = b.results()
+        b.close()
+        err = np.max(np.abs(c - c_ref), axis=1)
+        assert np.all(err <= tol), (prec, dict(zip(n.tolist(), err.tolist())))
+        assert np.max(np.abs(p - p_ref)) <= (1e-10 if prec == "fp64" else 1e-5)
