@@ -181,8 +181,11 @@ static void fill_plan_info(std::vector<int>& kap, int& n3) {
 
 template <int N>
 static void plan_info_n(int v, std::vector<int>& kap, int& n3) {
-  if (v == 3) fill_plan_info<typename AltPlan<N>::type>(kap, n3);
-  else fill_plan_info<typename DefaultPlan<N>::type>(kap, n3);
+  switch (v) {
+    case 2: case 3: fill_plan_info<typename ClassicPlan<N>::type>(kap, n3); break;
+    case 4: fill_plan_info<typename AltPlan<N>::type>(kap, n3); break;
+    default: fill_plan_info<typename DefaultPlan<N>::type>(kap, n3); break;
+  }
 }
 
 // final-layout frequencies and radix-3 count of the plan behind variant v
@@ -200,12 +203,46 @@ static void plan_info(int n, int v, std::vector<int>& kap, int& n3) {
   }
 }
 
-// default variant per size and precision (set from autotuner measurements
-// on B200; see espec_b200/autotune.py)
+static size_t smem_of(int n, int v, int precision) {
+  const bool d = precision == ESPEC_FP64;
+  switch (n) {
+    case 256: return d ? variant_smem<double, 256>(v) : variant_smem<float, 256>(v);
+    case 384: return d ? variant_smem<double, 384>(v) : variant_smem<float, 384>(v);
+    case 512: return d ? variant_smem<double, 512>(v) : variant_smem<float, 512>(v);
+    case 768: return d ? variant_smem<double, 768>(v) : variant_smem<float, 768>(v);
+    case 1024: return d ? variant_smem<double, 1024>(v) : variant_smem<float, 1024>(v);
+    case 1536: return d ? variant_smem<double, 1536>(v) : variant_smem<float, 1536>(v);
+    case 2048: return d ? variant_smem<double, 2048>(v) : variant_smem<float, 2048>(v);
+    case 4096: return d ? variant_smem<double, 4096>(v) : variant_smem<float, 4096>(v);
+    default: return 0;
+  }
+}
+
+static bool variant_fits(int n, int v, int precision) {
+  const size_t b = smem_of(n, v, precision);
+  return b > 0 && b <= kMaxSmem;
+}
+
+// default variant per size and precision: the fastest of espec_b200.autotune
+// on B200 (300 time steps, >= 8 waves of CTAs per size)
 static int default_variant(int n, int precision) {
-  (void)n;
-  (void)precision;
-  return 0;
+  if (precision == ESPEC_MIXED) {
+    switch (n) {
+      case 256: return 2;
+      case 384: return 2;
+      case 512: return 3;
+      case 768: return 2;
+      case 1024: return 1;
+      case 1536: return 3;
+      case 2048: return 0;
+      case 4096: return 2;
+      default: return 0;
+    }
+  }
+  switch (n) {
+    case 256: case 384: case 512: case 768: case 4096: return 2;
+    default: return 0;
+  }
 }
 
 }  // namespace espec
@@ -411,6 +448,8 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
 extern "C" int espec_spo_set_variant(espec_spo_plan* p, int npts, int variant) {
   if (!p) return set_error(ESPEC_EINVAL, "null plan");
   if (variant < 0 || variant >= kNumVariants) return set_error(ESPEC_EINVAL, "unknown variant");
+  if (!variant_fits(npts, variant, p->precision))
+    return set_error(ESPEC_EINVAL, "variant needs more shared memory than a CTA can have");
   bool found = false;
   for (auto& c : p->classes)
     if (c.n == npts) {

@@ -178,6 +178,22 @@ template <typename R, class PL>
 struct SpoThread {
   static constexpr int N = PL::N, P = PL::P, T = PL::T, S = PL::S;
   using rot_t = typename Tab<R>::rot_t;
+  // Warp-local exchanges need four buffers; when those would not fit next to
+  // the tables every exchange uses a CTA-wide barrier and two buffers.
+  static constexpr bool kLocal = PL::NBUF == 2 || (size_t)4 * N * sizeof(cpx<R>) <= 160 * 1024;
+  static constexpr int NBUF = kLocal ? PL::NBUF : 2;
+  template <int s>
+  static __host__ __device__ constexpr bool local_x() {
+    return kLocal ? PL::local(s) : (T <= 32);
+  }
+  template <int s>
+  static __host__ __device__ constexpr int buf_f() {
+    return kLocal ? (NBUF == 4 ? PL::buf_fwd(s) : (PL::buf_fwd(s) & 1)) : (s & 1);
+  }
+  template <int s>
+  static __host__ __device__ constexpr int buf_i() {
+    return kLocal ? (NBUF == 4 ? PL::buf_inv(s) : (PL::buf_inv(s) & 1)) : ((s + 1) & 1);
+  }
 
   rot_t tw[PL::NTW];
 
@@ -291,7 +307,7 @@ struct SpoThread {
 
   template <int s>
   static __device__ __forceinline__ void xsync() {
-    if constexpr (PL::local(s)) {
+    if constexpr (local_x<s>()) {
       __syncwarp();
     } else {
       __syncthreads();
@@ -334,8 +350,7 @@ struct SpoThread {
     if constexpr (s < S) {
       fwd_bfly<s>(v);
       if constexpr (s + 1 < S) {
-        constexpr int b = PL::NBUF == 4 ? PL::buf_fwd(s) : (PL::buf_fwd(s) & 1);
-        xchg_fwd<s>(v, bufs + b * N, t);
+        xchg_fwd<s>(v, bufs + buf_f<s>() * N, t);
         forward<s + 1>(v, bufs, t);
       }
     }
@@ -345,8 +360,7 @@ struct SpoThread {
     if constexpr (s >= 0) {
       inv_bfly<s>(v);
       if constexpr (s > 0) {
-        constexpr int b = PL::NBUF == 4 ? PL::buf_inv(s - 1) : (PL::buf_inv(s - 1) & 1);
-        xchg_inv<s - 1>(v, bufs + b * N, t);
+        xchg_inv<s - 1>(v, bufs + buf_i<s - 1>() * N, t);
         inverse<s - 1>(v, bufs, t);
       }
     }
@@ -441,7 +455,7 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
   using TB = Tab<R>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   cpx<R>* bufs = reinterpret_cast<cpx<R>*>(smem_raw);
-  double2* cpart = reinterpret_cast<double2*>(bufs + PL::NBUF * N);  // [2][NW]
+  double2* cpart = reinterpret_cast<double2*>(bufs + Th::NBUF * N);  // [2][NW]
   TabStore<R, PL, kTab> tab;
   tab.init(cpart + 2 * NW);
 
@@ -564,7 +578,7 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
 
 template <typename R, class PL, int kTab>
 constexpr size_t spo1d_smem_bytes() {
-  return PL::NBUF * sizeof(cpx<R>) * PL::N + 2 * sizeof(double2) * ((PL::T + 31) / 32) +
+  return SpoThread<R, PL>::NBUF * sizeof(cpx<R>) * PL::N + 2 * sizeof(double2) * ((PL::T + 31) / 32) +
          TabStore<R, PL, kTab>::smem_bytes;
 }
 

@@ -1,13 +1,26 @@
 // spo1d_launch.cuh -- launch helpers and the variant registry of the batched
 // 1D split-operator kernel.  A variant fixes the radix plan, where the
 // per-point tables live and the register budget (minimum resident CTAs per
-// SM); the autotuner measures them and picks one per packet size.
+// SM); the autotuner (espec_b200/autotune.py) measures them and the
+// per-size defaults of spo1d.cu come from its results on B200.
 #pragma once
 #include "spo1d.cuh"
 
 namespace espec {
 
-// alternative plans (4 points per thread, radix-4 stages) for powers of two
+// classic plans: largest radix first (the first exchanges are CTA-wide)
+template <int N>
+struct ClassicPlan;
+template <> struct ClassicPlan<256>  { using type = Plan<256, 8, 8, 8, 4>; };
+template <> struct ClassicPlan<512>  { using type = Plan<512, 8, 8, 8, 8>; };
+template <> struct ClassicPlan<1024> { using type = Plan<1024, 8, 8, 8, 8, 2>; };
+template <> struct ClassicPlan<2048> { using type = Plan<2048, 8, 8, 8, 8, 4>; };
+template <> struct ClassicPlan<4096> { using type = Plan<4096, 16, 16, 16, 16>; };
+template <> struct ClassicPlan<384>  { using type = Plan<384, 12, 12, 4, 4, 2>; };
+template <> struct ClassicPlan<768>  { using type = Plan<768, 12, 12, 4, 4, 4>; };
+template <> struct ClassicPlan<1536> { using type = Plan<1536, 12, 12, 4, 4, 4, 2>; };
+
+// radix-4 plans (4 points per thread) for powers of two
 template <int N>
 struct AltPlan {
   using type = typename DefaultPlan<N>::type;
@@ -18,21 +31,8 @@ template <> struct AltPlan<1024> { using type = Plan<1024, 4, 4, 4, 4, 4, 4>; };
 template <> struct AltPlan<2048> { using type = Plan<2048, 4, 4, 4, 4, 4, 4, 2>; };
 template <> struct AltPlan<4096> { using type = Plan<4096, 8, 8, 8, 8, 8>; };
 
-constexpr int kNumVariants = 4;
-
-template <typename R, class PL, bool kQuirk, int kTab, int kMinB>
-static cudaError_t launch_one(const SpoArgs<R>& a, int nblocks, cudaStream_t st) {
-  auto kern = spo1d_kernel<R, PL, false, kQuirk, kTab, kMinB>;
-  const size_t smem = spo1d_smem_bytes<R, PL, kTab>();
-  static bool attr_set = false;  // one flag per instantiation
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
-  kern<<<nblocks, PL::T, smem, st>>>(a);
-  return cudaGetLastError();
-}
+constexpr int kNumVariants = 5;
+constexpr size_t kMaxSmem = 227 * 1024;  // opt-in shared memory per CTA on sm_100
 
 // minimum resident CTAs that caps registers per thread at RegCap
 template <class PL, int RegCap>
@@ -40,25 +40,82 @@ struct MinBlocks {
   static constexpr int v = (65536 / (RegCap * PL::T)) < 1 ? 1 : (65536 / (RegCap * PL::T));
 };
 
+template <typename R, class PL, bool kQuirk, int kTab, int kMinB>
+static cudaError_t launch_one(const SpoArgs<R>& a, int nblocks, cudaStream_t st) {
+  constexpr size_t smem = spo1d_smem_bytes<R, PL, kTab>();
+  if constexpr (smem > kMaxSmem) {
+    return cudaErrorInvalidConfiguration;  // never selected: rejected by variant_fits
+  } else {
+    auto kern = spo1d_kernel<R, PL, false, kQuirk, kTab, kMinB>;
+    static bool attr_set = false;  // one flag per instantiation
+    if (!attr_set) {
+      cudaError_t e =
+          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+      attr_set = true;
+    }
+    kern<<<nblocks, PL::T, smem, st>>>(a);
+    return cudaGetLastError();
+  }
+}
+
 // variant v of size N:
-//   0: default plan, tables in registers, <= 255 registers
-//   1: default plan, tables in shared memory, <= 168 registers
-//   2: default plan, tables in shared memory, <= 128 registers
-//   3: alternative plan (radix-4, 4 points/thread for powers of two), tables
-//      in registers, <= 128 registers
+//   0: warp-local plan, tables in registers
+//   1: warp-local plan, tables in shared memory, <= 168 registers
+//   2: classic plan, tables in registers
+//   3: classic plan, tables in shared memory, <= 168 registers
+//   4: radix-4 plan (4 points/thread for powers of two), tables in
+//      registers, <= 128 registers
+template <int N, int v>
+struct VariantPlan {
+  using type = typename DefaultPlan<N>::type;
+};
+template <int N> struct VariantPlan<N, 2> { using type = typename ClassicPlan<N>::type; };
+template <int N> struct VariantPlan<N, 3> { using type = typename ClassicPlan<N>::type; };
+template <int N> struct VariantPlan<N, 4> { using type = typename AltPlan<N>::type; };
+template <int v> struct VariantTab {
+  static constexpr int value = (v == 1 || v == 3) ? 1 : 0;
+};
+template <int v> struct VariantRegs {
+  static constexpr int cap = v == 4 ? 128 : ((v == 1 || v == 3) ? 168 : 255);
+};
+
+template <typename R, int N, int v>
+static cudaError_t launch_v(const SpoArgs<R>& a, int nblocks, cudaStream_t st) {
+  using PL = typename VariantPlan<N, v>::type;
+  return launch_one<R, PL, false, VariantTab<v>::value, MinBlocks<PL, VariantRegs<v>::cap>::v>(
+      a, nblocks, st);
+}
+
 template <typename R, int N>
 static cudaError_t launch_variant(int v, const SpoArgs<R>& a, int nblocks, bool quirk,
                                   cudaStream_t st) {
-  using D = typename DefaultPlan<N>::type;
-  using A = typename AltPlan<N>::type;
   if constexpr (sizeof(R) == 8) {
-    if (quirk) return launch_one<R, D, true, 0, 1>(a, nblocks, st);
+    if (quirk) return launch_one<R, typename DefaultPlan<N>::type, true, 0, 1>(a, nblocks, st);
   }
   switch (v) {
-    case 1: return launch_one<R, D, false, 1, MinBlocks<D, 168>::v>(a, nblocks, st);
-    case 2: return launch_one<R, D, false, 1, MinBlocks<D, 128>::v>(a, nblocks, st);
-    case 3: return launch_one<R, A, false, 0, MinBlocks<A, 128>::v>(a, nblocks, st);
-    default: return launch_one<R, D, false, 0, 1>(a, nblocks, st);
+    case 1: return launch_v<R, N, 1>(a, nblocks, st);
+    case 2: return launch_v<R, N, 2>(a, nblocks, st);
+    case 3: return launch_v<R, N, 3>(a, nblocks, st);
+    case 4: return launch_v<R, N, 4>(a, nblocks, st);
+    default: return launch_v<R, N, 0>(a, nblocks, st);
+  }
+}
+
+// shared memory of variant v of size N
+template <typename R, int N, int v>
+static size_t smem_v() {
+  return spo1d_smem_bytes<R, typename VariantPlan<N, v>::type, VariantTab<v>::value>();
+}
+template <typename R, int N>
+static size_t variant_smem(int v) {
+  switch (v) {
+    case 0: return smem_v<R, N, 0>();
+    case 1: return smem_v<R, N, 1>();
+    case 2: return smem_v<R, N, 2>();
+    case 3: return smem_v<R, N, 3>();
+    case 4: return smem_v<R, N, 4>();
+    default: return 0;
   }
 }
 

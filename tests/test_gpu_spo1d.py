@@ -129,7 +129,7 @@ def test_scan_subset_mixed_vs_fp64():
     assert err <= 5e-6, err
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_every_variant_matches_oracle(oracle, variant):
     """Each kernel variant (plan / table location / register budget) of each
     packet size gives the oracle's C(t): FP64 to 1e-10, mixed to 5e-6."""
@@ -139,7 +139,10 @@ def test_every_variant_matches_oracle(oracle, variant):
     for prec, tol in (("fp64", 1e-10), ("mixed", 5e-6)):
         b = E.SpoBatch(n, sh, sm, dt, precision=prec)
         for size in SIZES:
-            b.set_variant(size, variant)
+            try:
+                b.set_variant(size, variant)
+            except E.EspecError as e:  # variant does not fit in shared memory
+                assert "shared memory" in str(e)
         b.load(v, psi)
         b.run(200)
         c, p = b.results()
