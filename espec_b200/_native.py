@@ -23,7 +23,7 @@ EXPORTS = [
     "espec_last_error", "espec_version", "espec_device_ok",
     "espec_spo_create", "espec_spo_load", "espec_spo_run", "espec_spo_results",
     "espec_spo_device_c", "espec_spo_npoints", "espec_spo_destroy",
-    "espec_spo_set_variant", "espec_spo_variant_count",
+    "espec_spo_set_variant", "espec_spo_variant_count", "espec_spo_run_static",
 ]
 
 
@@ -57,6 +57,8 @@ def load():
     lib.espec_spo_npoints.argtypes = [vp]
     lib.espec_spo_set_variant.argtypes = [vp, C.c_int, C.c_int]
     lib.espec_spo_variant_count.restype = C.c_int
+    lib.espec_spo_run_static.argtypes = [C.c_int, i, d, d, C.c_double, C.c_int, vp, vp, C.c_int,
+                                         vp, vp, vp]
     lib.espec_spo_destroy.argtypes = [vp]
     lib.espec_spo_destroy.restype = None
     _lib = lib

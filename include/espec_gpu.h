@@ -87,6 +87,31 @@ const void* espec_spo_device_c(const espec_spo_plan* plan);
 int espec_spo_npoints(const espec_spo_plan* plan);
 void espec_spo_destroy(espec_spo_plan* plan);
 
+/* ----------------------------------------------------------------------
+ * Batched 1D split-operator propagation that allocates nothing.
+ *
+ * No counterpart in the reference: eSPec has no GPU and no allocator to
+ * avoid.  For callers that cannot call cudaMalloc -- an application that owns
+ * the whole device memory pool, a code under a fixed memory budget, or code
+ * running while another component captures or replays GPU work.  Inputs and
+ * outputs are device pointers owned by the caller; the intermediate tables
+ * live in one fixed __device__ array inside the library (about 3.2 MB, held on
+ * every GPU that loads the library until the process exits).
+ *
+ * npts/sh/sm: host arrays of npk entries (at most 128 packets, at most 32768
+ * grid points in total; sizes as espec_spo_create).  vpot: npts-sum doubles.
+ * psi0: interleaved complex (re, im) doubles.  c_out: interleaved complex,
+ * npk*(nsteps+1) samples, packet-major.  psi_out: interleaved complex or NULL.
+ * No absorber; C(t) every step, same arithmetic as variant 0 of the plans.
+ * Calls share the array: calls whose GPU work overlaps race; serialise them.
+ * The first call on each device resolves the array's address; make it
+ * before any stream capture.  Sizes beyond the limits return ESPEC_EINVAL.
+ * ---------------------------------------------------------------------- */
+int espec_spo_run_static(int npk, const int* npts, const double* sh,
+                         const double* sm, double dt_fs, int precision,
+                         const double* vpot, const double* psi0, int nsteps,
+                         double* c_out, double* psi_out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
