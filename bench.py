@@ -30,6 +30,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Mgridpt*steps/s (batched 1D Morse scan, mixed precision, C(t) every step)"
 ALG_BYTES = {"mixed": 28.0, "fp64": 56.0}  # per grid point per time step
+# DRAM bytes per grid-point step measured by ncu on one launch of the 2048-point
+# class (592 packets x 8000 steps, profiles/spo1d_kernel_2048_mixed_full.md):
+# the state stays on chip, HBM carries the tables once plus C(t) and psi(TF).
+MEASURED_TRAFFIC_B = {"mixed": 0.0142, "fp64": None}
 
 
 def parse():
@@ -236,8 +240,11 @@ def main():
     kms = ev2.elapsed_time(ev3) / args.steps
     alg = ALG_BYTES[args.precision] * pts_steps
     achieved = alg / (kms * 1e-3) / 1e9
+    tb = MEASURED_TRAFFIC_B[args.precision]
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+            "frac": achieved / peak, "traffic": (tb * pts_steps if tb else None),
+            "traffic_note": "ncu dram bytes of a 2048-point class launch scaled by grid-point steps",
+            "peak_kind": peak_kind,
             "kernel": "spo1d_kernel (7 size classes, concurrent streams)",
             "kernel_ms": kms}
 

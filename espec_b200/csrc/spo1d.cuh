@@ -532,15 +532,20 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
       for (int j = 0; j < P; ++j) v[j] = TB::apply(tab.K(j, t), v[j]);
     }
     th.template inverse<PL::S - 1>(v, bufs, t);
-    // partial C(t) = sum w phi in FP64
-    double cr = 0.0, ci = 0.0;
+    // partial C(t) = sum w phi: the P products of a thread are summed in the
+    // working precision (for FP32 a relative 1e-7 of a partial of size
+    // ~1/N_threads), everything beyond the thread in FP64
+    double cr, ci;
+    {
+      R pr = R(0), pi = R(0);
 #pragma unroll
-    for (int j = 0; j < P; ++j) {
-      const typename TB::weight_t wj = tab.W(j, t);
-      const double wx = (double)wj.x, wy = (double)wj.y;
-      const double vx = (double)v[j].x, vy = (double)v[j].y;
-      cr = fma(wx, vx, fma(-wy, vy, cr));
-      ci = fma(wx, vy, fma(wy, vx, ci));
+      for (int j = 0; j < P; ++j) {
+        const typename TB::weight_t wj = tab.W(j, t);
+        pr = fma(wj.x, v[j].x, fma(-wj.y, v[j].y, pr));
+        pi = fma(wj.x, v[j].y, fma(wj.y, v[j].x, pi));
+      }
+      cr = (double)pr;
+      ci = (double)pi;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
