@@ -6,6 +6,6 @@ and the batched split-operator interface.
 """
 from . import _native
 from ._native import EspecError, load
-from .spo import SpoBatch
+from .spo import SodBatch, SpoBatch
 
-__all__ = ["EspecError", "SpoBatch", "load", "workloads"]
+__all__ = ["EspecError", "SodBatch", "SpoBatch", "load", "workloads"]

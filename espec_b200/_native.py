@@ -15,6 +15,8 @@ OK, EINVAL, ECUDA, ENOMEM = 0, -1, -2, -3
 FP64, MIXED = 0, 1
 ABS_NONE, ABS_VOPTIC, ABS_SMOOTHW = 0, 1, 2
 Q_SPO_INPLACE = 1
+Q_SOD_SMOOTHW = 2
+SPO, SOD = 0, 1
 MEM_HOST, MEM_DEVICE = 0, 1
 SHFS = 2.4188843243e-2
 
@@ -24,6 +26,7 @@ EXPORTS = [
     "espec_spo_create", "espec_spo_load", "espec_spo_run", "espec_spo_results",
     "espec_spo_device_c", "espec_spo_npoints", "espec_spo_destroy",
     "espec_spo_set_variant", "espec_spo_variant_count", "espec_spo_run_static",
+    "espec_prop_create", "espec_prop_previous",
 ]
 
 
@@ -49,6 +52,9 @@ def load():
     lib.espec_device_ok.restype = C.c_int
     lib.espec_spo_create.argtypes = [C.POINTER(vp), C.c_int, i, d, d, C.c_double, C.c_int,
                                      C.c_int, C.c_int]
+    lib.espec_prop_create.argtypes = [C.POINTER(vp), C.c_int, i, d, d, C.c_double, C.c_int,
+                                      C.c_int, C.c_int, C.c_int]
+    lib.espec_prop_previous.argtypes = [vp, vp, vp, C.c_int, vp]
     lib.espec_spo_load.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]
     lib.espec_spo_run.argtypes = [vp, C.c_int, vp]
     lib.espec_spo_results.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]

@@ -12,6 +12,7 @@
 
 #include "espec_gpu.h"
 #include "espec_internal.h"
+#include "sod1d.cuh"
 #include "spo1d_launch.cuh"
 
 namespace espec {
@@ -147,6 +148,23 @@ __global__ void spo_setup_kernel(SetupArgs a) {
   (void)f;
 }
 
+// SOD (.PFSOD) tables: CST V, CST TC/N (final layout), CST VABC or mask, conj(psi0)
+__global__ void sod_setup_kernel(SetupArgs a, SodTables out, double cst) {
+  const int x = blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= a.npts) return;
+  const int pk = a.pk_of[x];
+  const int base = a.pk_off[pk];
+  const_cast<double*>(out.vc)[x] = cst * a.vpot[x];
+  const_cast<double*>(out.kc)[x] = cst * a.tc[base + a.kperm[x]] * a.kscale[pk];
+  if (a.absorb == ESPEC_ABS_VOPTIC) const_cast<double*>(out.ab)[x] = cst * a.vabc[x];
+  if (a.absorb == ESPEC_ABS_SMOOTHW) const_cast<double*>(out.ab)[x] = a.vabc[x];
+  const double2 p0 = a.psi0[x];
+  const_cast<cpx<double>*>(out.w)[x] = mk(p0.x, -p0.y);
+}
+
+cudaError_t sod_launch(int n, int kabs, const SodArgs& a, int nblocks, cudaStream_t st);
+bool sod_size_supported(int n);
+
 // ---------------------------------------------------------------------------
 // per-size-class dispatch
 // ---------------------------------------------------------------------------
@@ -253,7 +271,9 @@ static int default_variant(int n, int precision) {
 using namespace espec;
 
 struct espec_spo_plan {
-  int npk = 0, npts = 0, precision = 0, absorb = 0, quirks = 0;
+  int npk = 0, npts = 0, precision = 0, absorb = 0, quirks = 0, method = ESPEC_SPO;
+  double2* d_psi_prev = nullptr;  // SOD: psi(TF - dt)
+  SodTables tsod{};
   double dt_fs = 0.0;
   std::vector<int> n, off;
   std::vector<double> sh, sm;
@@ -296,7 +316,7 @@ static void plan_free(espec_spo_plan* p) {
   for (auto e : p->events) cudaEventDestroy(e);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   void* bufs[] = {p->d_vpot, p->d_vabc, p->d_psi0, p->d_psi, p->d_tc, p->d_kperm, p->d_pk_of,
-                  p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s};
+                  p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s, p->d_psi_prev};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -351,10 +371,16 @@ static int spo_index_tables(espec_spo_plan* p) {
   return ESPEC_OK;
 }
 
-extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
-                                const double* sh, const double* sm, double dt_fs, int precision,
-                                int absorb, int quirks) {
+extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
+                                 const double* sh, const double* sm, double dt_fs, int method,
+                                 int precision, int absorb, int quirks) {
   if (!out || npk <= 0 || !npts || !sh || !sm) return set_error(ESPEC_EINVAL, "null argument");
+  if (method != ESPEC_SPO && method != ESPEC_SOD)
+    return set_error(ESPEC_EINVAL, "method must be ESPEC_SPO or ESPEC_SOD");
+  if (method == ESPEC_SOD && precision != ESPEC_FP64)
+    return set_error(ESPEC_EINVAL, "the SOD propagator runs in FP64 only");
+  if (method == ESPEC_SOD && (quirks & ESPEC_Q_SPO_INPLACE))
+    return set_error(ESPEC_EINVAL, "ESPEC_Q_SPO_INPLACE applies to the split-operator method");
   if (precision != ESPEC_FP64 && precision != ESPEC_MIXED)
     return set_error(ESPEC_EINVAL, "precision must be ESPEC_FP64 or ESPEC_MIXED");
   if (precision == ESPEC_MIXED && (quirks & ESPEC_Q_SPO_INPLACE))
@@ -362,6 +388,7 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
   if (absorb < ESPEC_ABS_NONE || absorb > ESPEC_ABS_SMOOTHW)
     return set_error(ESPEC_EINVAL, "unknown absorber type");
   auto* p = new espec_spo_plan;
+  p->method = method;
   p->npk = npk;
   p->precision = precision;
   p->absorb = absorb;
@@ -378,6 +405,10 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
       return set_error(ESPEC_EINVAL, "unsupported packet size (supported: 256, 384, 512, 768, "
                                      "1024, 1536, 2048, 4096)");
     }
+    if (method == ESPEC_SOD && !sod_size_supported(p->n[i])) {
+      delete p;
+      return set_error(ESPEC_EINVAL, "unsupported packet size for SOD (supported: 256 to 2048)");
+    }
     p->off[i + 1] = p->off[i] + p->n[i];
   }
   p->npts = p->off[npk];
@@ -392,7 +423,7 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
   for (int i = 0; i < npk; ++i) cls[p->n[i]].push_back(SpoPacket{p->off[i], 0});
   for (auto& kv : cls) {
     espec_spo_plan::Class c{kv.first, (int)kv.second.size(), nullptr,
-                            default_variant(kv.first, precision)};
+                            method == ESPEC_SOD ? 0 : default_variant(kv.first, precision)};
     if ((rc = ck(cudaMalloc(&c.d_pk, sizeof(SpoPacket) * c.count), "cudaMalloc"))) return fail(rc);
     p->classes.push_back(c);
     cudaStream_t s;
@@ -420,6 +451,14 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
     p->tab_bytes = np * (12 * 4 + 8);
   }
   if ((rc = ck(cudaMalloc(&p->d_tab, p->tab_bytes), "cudaMalloc"))) return fail(rc);
+  if (method == ESPEC_SOD) {
+    if ((rc = ck(cudaMalloc(&p->d_psi_prev, np * 16), "cudaMalloc"))) return fail(rc);
+    double* tb = (double*)p->d_tab;  // 40 B per point inside the 80 B FP64 table block
+    p->tsod.vc = tb;
+    p->tsod.kc = tb + np;
+    p->tsod.ab = tb + 2 * np;
+    p->tsod.w = (const cpx<double>*)(tb + 3 * np);
+  }
   if (quirks & ESPEC_Q_SPO_INPLACE) {
     if ((rc = ck(cudaMalloc(&p->d_kq_c, np * 8), "cudaMalloc"))) return fail(rc);
     if ((rc = ck(cudaMalloc(&p->d_kq_s, np * 8), "cudaMalloc"))) return fail(rc);
@@ -445,8 +484,15 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
   return ESPEC_OK;
 }
 
+extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
+                                const double* sh, const double* sm, double dt_fs, int precision,
+                                int absorb, int quirks) {
+  return espec_prop_create(out, npk, npts, sh, sm, dt_fs, ESPEC_SPO, precision, absorb, quirks);
+}
+
 extern "C" int espec_spo_set_variant(espec_spo_plan* p, int npts, int variant) {
   if (!p) return set_error(ESPEC_EINVAL, "null plan");
+  if (p->method != ESPEC_SPO) return set_error(ESPEC_EINVAL, "variants exist for ESPEC_SPO only");
   if (variant < 0 || variant >= kNumVariants) return set_error(ESPEC_EINVAL, "unknown variant");
   if (!variant_fits(npts, variant, p->precision))
     return set_error(ESPEC_EINVAL, "variant needs more shared memory than a CTA can have");
@@ -505,8 +551,12 @@ static int spo_build_tables(espec_spo_plan* p, cudaStream_t st) {
   a.kq_c = p->d_kq_c;
   a.kq_s = p->d_kq_s;
   const int bs = 256;
-  spo_setup_kernel<<<(p->npts + bs - 1) / bs, bs, 0, st>>>(a);
-  int rc = ck(cudaGetLastError(), "spo_setup_kernel");
+  if (p->method == ESPEC_SOD) {
+    sod_setup_kernel<<<(p->npts + bs - 1) / bs, bs, 0, st>>>(a, p->tsod, 2.0 * p->dt_fs / ESPEC_SHFS);
+  } else {
+    spo_setup_kernel<<<(p->npts + bs - 1) / bs, bs, 0, st>>>(a);
+  }
+  int rc = ck(cudaGetLastError(), "set-up kernel");
   if (rc) return rc;
   p->loaded = true;
   return ESPEC_OK;
@@ -557,7 +607,19 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
     cudaStream_t cs = p->streams[ci];
     ESPEC_CK(cudaStreamWaitEvent(cs, p->ev_fork, 0));
     cudaError_t e;
-    if (p->precision == ESPEC_FP64) {
+    if (p->method == ESPEC_SOD) {
+      SodArgs a{};
+      a.tab = p->tsod;
+      a.pk = c.d_pk;
+      a.psi0 = p->d_psi0;
+      a.psi_out = p->d_psi;
+      a.psi_prev_out = p->d_psi_prev;
+      a.c_out = p->d_c;
+      a.nsteps = nsteps;
+      int kabs = p->absorb == ESPEC_ABS_VOPTIC ? 1 : (p->absorb == ESPEC_ABS_SMOOTHW ? 2 : 0);
+      if (kabs == 2 && (p->quirks & ESPEC_Q_SOD_SMOOTHW)) kabs = 0;  // sodfft.f:108
+      e = sod_launch(c.n, kabs, a, c.count, cs);
+    } else if (p->precision == ESPEC_FP64) {
       SpoArgs<double> a{};
       a.tab = p->t64;
       a.pk = c.d_pk;
@@ -602,3 +664,16 @@ extern "C" int espec_spo_results(espec_spo_plan* p, double* c_re, double* c_im, 
 }
 
 extern "C" const void* espec_spo_device_c(const espec_spo_plan* p) { return p ? p->d_c : nullptr; }
+
+extern "C" int espec_prop_previous(espec_spo_plan* p, double* psi_re, double* psi_im, int where,
+                                   void* stream) {
+  if (!p || p->method != ESPEC_SOD || p->c_cap_steps < 0)
+    return set_error(ESPEC_EINVAL, "previous state exists for run SOD plans only");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind = where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t np = p->npts;
+  if (psi_re) ESPEC_CK(cudaMemcpy2DAsync(psi_re, 8, p->d_psi_prev, 16, 8, np, kind, st));
+  if (psi_im) ESPEC_CK(cudaMemcpy2DAsync(psi_im, 8, (char*)p->d_psi_prev + 8, 16, 8, np, kind, st));
+  if (where == ESPEC_MEM_HOST) ESPEC_CK(cudaStreamSynchronize(st));
+  return ESPEC_OK;
+}

@@ -14,6 +14,8 @@ from . import _native as N
 
 
 class SpoBatch:
+    method = N.SPO
+
     def __init__(self, npts, sh, sm, dt_fs, precision="fp64", absorb=N.ABS_NONE, quirks=0):
         lib = N.load()
         self.npts = np.ascontiguousarray(npts, dtype=np.int32)
@@ -26,12 +28,12 @@ class SpoBatch:
         self.precision = {"fp64": N.FP64, "mixed": N.MIXED}[precision]
         self.absorb = absorb
         self._h = C.c_void_p()
-        rc = lib.espec_spo_create(C.byref(self._h), self.npk,
-                                  self.npts.ctypes.data_as(C.POINTER(C.c_int)),
-                                  self.sh.ctypes.data_as(C.POINTER(C.c_double)),
-                                  self.sm.ctypes.data_as(C.POINTER(C.c_double)),
-                                  self.dt_fs, self.precision, absorb, quirks)
-        N.check(rc, "espec_spo_create")
+        rc = lib.espec_prop_create(C.byref(self._h), self.npk,
+                                   self.npts.ctypes.data_as(C.POINTER(C.c_int)),
+                                   self.sh.ctypes.data_as(C.POINTER(C.c_double)),
+                                   self.sm.ctypes.data_as(C.POINTER(C.c_double)),
+                                   self.dt_fs, self.method, self.precision, absorb, quirks)
+        N.check(rc, "espec_prop_create")
         self.nsteps = None
 
     def set_variant(self, npts, variant):
@@ -86,6 +88,24 @@ class SpoBatch:
             self.close()
         except Exception:
             pass
+
+
+class SodBatch(SpoBatch):
+    """Batched second-order-differences propagation with the FFT kinetic term
+    (PSODFFT, psodfft.f:77-206), FP64.  Step 1 is the reference's start-up of
+    two half steps; `previous()` returns psi(TF - dt)."""
+
+    method = N.SOD
+
+    def __init__(self, npts, sh, sm, dt_fs, absorb=N.ABS_NONE, quirks=0):
+        super().__init__(npts, sh, sm, dt_fs, precision="fp64", absorb=absorb, quirks=quirks)
+
+    def previous(self, stream=None):
+        pr = np.zeros(self.total)
+        pi = np.zeros(self.total)
+        N.check(N.load().espec_prop_previous(self._h, N.ptr(pr), N.ptr(pi), N.MEM_HOST, stream),
+                "espec_prop_previous")
+        return pr + 1j * pi
 
 
 def digt_1d(n, sh, sm):

@@ -39,8 +39,13 @@ extern "C" {
 #define ESPEC_ABS_VOPTIC 1
 #define ESPEC_ABS_SMOOTHW 2
 
+/* propagation methods */
+#define ESPEC_SPO 0         /* split operator, FFT kinetic term (.PFSPO)     */
+#define ESPEC_SOD 1         /* second-order differences, FFT kinetic (.PFSOD) */
+
 /* reproduce reference defects on request (FP64 form only) */
 #define ESPEC_Q_SPO_INPLACE 1   /* spofft.f:150-153 kinetic multiply            */
+#define ESPEC_Q_SOD_SMOOTHW 2   /* sodfft.f:108 never applies the .SMOOTHW mask */
 
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
@@ -69,6 +74,16 @@ typedef struct espec_spo_plan espec_spo_plan;
 int espec_spo_create(espec_spo_plan** plan, int npk, const int* npts,
                      const double* sh, const double* sm, double dt_fs,
                      int precision, int absorb, int quirks);
+/* Same plan for another method: ESPEC_SOD replaces the time loop of PSODFFT
+ * (psodfft.f:77-206, sodfft.f:64-126), FP64 only, sizes 256..2048; its first
+ * step is the reference's two-half-step start-up and C(t) again has nsteps+1
+ * samples.  espec_spo_create(...) = espec_prop_create(..., ESPEC_SPO, ...). */
+int espec_prop_create(espec_spo_plan** plan, int npk, const int* npts,
+                      const double* sh, const double* sm, double dt_fs, int method,
+                      int precision, int absorb, int quirks);
+/* SOD plans: psi(TF - dt), the older of the two states the leapfrog keeps */
+int espec_prop_previous(espec_spo_plan* plan, double* psi_re, double* psi_im,
+                        int where, void* stream);
 /* vabc: absorber table (complex-potential values for ESPEC_ABS_VOPTIC, mask
  * for ESPEC_ABS_SMOOTHW), ignored for ESPEC_ABS_NONE; psi_im may be NULL. */
 int espec_spo_load(espec_spo_plan* plan, const double* vpot, const double* vabc,
