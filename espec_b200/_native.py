@@ -26,7 +26,8 @@ EXPORTS = [
     "espec_spo_create", "espec_spo_load", "espec_spo_run", "espec_spo_results",
     "espec_spo_device_c", "espec_spo_npoints", "espec_spo_destroy",
     "espec_spo_set_variant", "espec_spo_variant_count", "espec_spo_run_static",
-    "espec_prop_create", "espec_prop_previous",
+    "espec_prop_create", "espec_prop_previous", "espec_prop_continue", "espec_prop_energies",
+    "espec_format_crl_row", "pspofft_", "psodfft_",
 ]
 
 
@@ -65,6 +66,15 @@ def load():
     lib.espec_spo_variant_count.restype = C.c_int
     lib.espec_spo_run_static.argtypes = [C.c_int, i, d, d, C.c_double, C.c_int, vp, vp, C.c_int,
                                          vp, vp, vp]
+    lib.espec_prop_continue.argtypes = [vp, C.c_int, vp]
+    lib.espec_prop_energies.argtypes = [vp, vp, vp, vp]
+    lib.espec_format_crl_row.argtypes = [C.c_double] * 6 + [C.c_char_p, C.c_int]
+    # Fortran drop-ins: every argument by reference, then one size_t length
+    # per CHARACTER*(*) argument
+    lib.pspofft_.argtypes = [vp] * 30 + [C.c_size_t] * 3
+    lib.pspofft_.restype = None
+    lib.psodfft_.argtypes = [vp] * 32 + [C.c_size_t] * 3
+    lib.psodfft_.restype = None
     lib.espec_spo_destroy.argtypes = [vp]
     lib.espec_spo_destroy.restype = None
     _lib = lib

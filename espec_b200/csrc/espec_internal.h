@@ -5,6 +5,8 @@
 namespace espec {
 int set_error(int code, const char* msg);
 int set_cuda_error(const char* what, cudaError_t e);
+// kinetic table of a 1D packet in FFT order (DIGT, dkeft.f:64-79)
+void digt_1d(int n, double sh, double sm, double* tc);
 inline int ck(cudaError_t e, const char* what) {
   return e == cudaSuccess ? 0 : set_cuda_error(what, e);
 }

@@ -27,6 +27,8 @@ struct SodArgs {
   SodTables tab;
   const SpoPacket* pk;
   const double2* psi0;
+  const double2* psi_start;       // resume: psi(t) ...
+  const double2* psi_prev_start;  // ... and psi(t - dt); no start-up step, C(0) not written
   double2* psi_out;       // psi(TF)
   double2* psi_prev_out;  // psi(TF - dt)
   double2* c_out;
@@ -63,17 +65,22 @@ __global__ void __launch_bounds__(PL::T) sod1d_kernel(SodArgs a) {
 #pragma unroll
   for (int j = 0; j < P; ++j) {
     const int x = base + Th::x_pos(t, j);
-    const double2 p0 = a.psi0[x];
+    const double2 p0 = a.psi_start ? a.psi_start[x] : a.psi0[x];
     cur[j] = mk(p0.x, p0.y);
-    prev[j] = cur[j];
+    if (a.psi_start) {
+      const double2 q = a.psi_prev_start[x];
+      prev[j] = mk(q.x, q.y);
+    } else {
+      prev[j] = cur[j];
+    }
     c0 += p0.x * p0.x + p0.y * p0.y;
     s_vc[j * T + t] = a.tab.vc[x];
     s_kc[j * T + t] = a.tab.kc[base + Th::final_pos(t, j)];
     if constexpr (kAbs != 0) s_ab[j * T + t] = a.tab.ab[x];
     s_w[j * T + t] = a.tab.w[x];
   }
-  // C(0)
-  {
+  // C(0) (not for a resumed run)
+  if (!a.psi_start) {
     double cr = c0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cr += __shfl_xor_sync(0xffffffffu, cr, o);
@@ -146,7 +153,10 @@ __global__ void __launch_bounds__(PL::T) sod1d_kernel(SodArgs a) {
   };
 
   bool cur_newest = true;
-  if (a.nsteps >= 1) {
+  int step = 2;
+  if (a.psi_start) {
+    step = 1;  // resumed: every step is a leapfrog step
+  } else if (a.nsteps >= 1) {
     // start-up (psodfft.f:120-152): E = psi0 - i/2 H psi0 ; psi1 = psi0 - i/2 H E ;
     // then the older state is psi0 again
     sod_update(cur, prev, 0.5);  // prev = E
@@ -158,7 +168,6 @@ __global__ void __launch_bounds__(PL::T) sod1d_kernel(SodArgs a) {
     }
     c_sample(cur, 1);
   }
-  int step = 2;
   for (; step + 1 <= a.nsteps; step += 2) {  // two leapfrog steps, roles alternate
     sod_update(cur, prev, 1.0);
     c_sample(prev, step);

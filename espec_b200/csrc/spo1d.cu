@@ -12,6 +12,7 @@
 
 #include "espec_gpu.h"
 #include "espec_internal.h"
+#include "diag1d.cuh"
 #include "sod1d.cuh"
 #include "spo1d_launch.cuh"
 
@@ -48,7 +49,7 @@ static std::vector<int> final_freq() {
 
 // dkeft.f:64-79 (DIGT, 1D): TC(k) = p^2 / (2 m) in FFT order with the
 // reference's truncated 2 pi and p accumulated by repeated addition.
-static void digt_1d(int n, double sh, double sm, double* tc) {
+void digt_1d(int n, double sh, double sm, double* tc) {
   const double twopi = 6.283185307;
   const double dp = twopi / (n * sh);
   double p = 0.0;
@@ -164,6 +165,7 @@ __global__ void sod_setup_kernel(SetupArgs a, SodTables out, double cst) {
 
 cudaError_t sod_launch(int n, int kabs, const SodArgs& a, int nblocks, cudaStream_t st);
 bool sod_size_supported(int n);
+
 
 // ---------------------------------------------------------------------------
 // per-size-class dispatch
@@ -282,6 +284,8 @@ struct espec_spo_plan {
     int count;
     SpoPacket* d_pk;
     int variant;
+    SpoPacket* d_pkd;  // diagnostics: c_off = packet index
+    int* d_kfreq;      // FFT index at each final position of the diagnostic FFT
   };
   bool index_dirty = true;
   std::vector<Class> classes;
@@ -305,18 +309,25 @@ struct espec_spo_plan {
   double* d_kq_c = nullptr;
   double* d_kq_s = nullptr;
   bool loaded = false;
+  bool has_prev = false;      // SOD: d_psi_prev holds psi(t - dt) of the current state
+  double2* d_diag = nullptr;  // (E, norm) per packet
   // tables (sub-pointers of d_tab)
   SpoTables<double> t64{};
   SpoTables<float> t32{};
 };
 
 static void plan_free(espec_spo_plan* p) {
-  for (auto& c : p->classes) cudaFree(c.d_pk);
+  for (auto& c : p->classes) {
+    cudaFree(c.d_pk);
+    if (c.d_pkd) cudaFree(c.d_pkd);
+    if (c.d_kfreq) cudaFree(c.d_kfreq);
+  }
   for (auto s : p->streams) cudaStreamDestroy(s);
   for (auto e : p->events) cudaEventDestroy(e);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   void* bufs[] = {p->d_vpot, p->d_vabc, p->d_psi0, p->d_psi, p->d_tc, p->d_kperm, p->d_pk_of,
-                  p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s, p->d_psi_prev};
+                  p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s, p->d_psi_prev,
+                  p->d_diag};
   for (void* b : bufs)
     if (b) cudaFree(b);
 }
@@ -423,9 +434,28 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
   for (int i = 0; i < npk; ++i) cls[p->n[i]].push_back(SpoPacket{p->off[i], 0});
   for (auto& kv : cls) {
     espec_spo_plan::Class c{kv.first, (int)kv.second.size(), nullptr,
-                            method == ESPEC_SOD ? 0 : default_variant(kv.first, precision)};
-    if ((rc = ck(cudaMalloc(&c.d_pk, sizeof(SpoPacket) * c.count), "cudaMalloc"))) return fail(rc);
-    p->classes.push_back(c);
+                            method == ESPEC_SOD ? 0 : default_variant(kv.first, precision),
+                            nullptr, nullptr};
+    p->classes.push_back(c);  // owned by the plan from here on (freed by plan_free)
+    auto& cc = p->classes.back();
+    if ((rc = ck(cudaMalloc(&cc.d_pk, sizeof(SpoPacket) * cc.count), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&cc.d_pkd, sizeof(SpoPacket) * cc.count), "cudaMalloc")))
+      return fail(rc);
+    if ((rc = ck(cudaMalloc(&cc.d_kfreq, sizeof(int) * cc.n), "cudaMalloc"))) return fail(rc);
+    {
+      std::vector<SpoPacket> pkd;
+      for (int i = 0; i < npk; ++i)
+        if (p->n[i] == cc.n) pkd.push_back(SpoPacket{p->off[i], i});
+      std::vector<int> kap;
+      int n3 = 0;
+      plan_info(cc.n, 0, kap, n3);
+      if ((rc = ck(cudaMemcpy(cc.d_pkd, pkd.data(), sizeof(SpoPacket) * pkd.size(),
+                              cudaMemcpyHostToDevice), "H2D")))
+        return fail(rc);
+      if ((rc = ck(cudaMemcpy(cc.d_kfreq, kap.data(), sizeof(int) * cc.n, cudaMemcpyHostToDevice),
+                   "H2D")))
+        return fail(rc);
+    }
     cudaStream_t s;
     if ((rc = ck(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking), "stream"))) return fail(rc);
     p->streams.push_back(s);
@@ -445,6 +475,7 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
   if ((rc = ck(cudaMalloc(&p->d_pk_of, np * 4), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_pk_off, npk * 4), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_kscale, npk * 8), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_diag, npk * 16), "cudaMalloc"))) return fail(rc);
   if (precision == ESPEC_FP64) {
     p->tab_bytes = np * 16 * 5;
   } else {
@@ -579,13 +610,15 @@ extern "C" int espec_spo_load(espec_spo_plan* p, const double* vpot, const doubl
   } else {
     ESPEC_CK(cudaMemset2DAsync((char*)p->d_psi0 + 8, 16, 0, 8, np, st));
   }
+  // the current state of a freshly loaded plan is psi0
+  ESPEC_CK(cudaMemcpyAsync(p->d_psi, p->d_psi0, np * 16, cudaMemcpyDeviceToDevice, st));
+  p->has_prev = false;
   return spo_build_tables(p, st);
 }
 
-extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
-  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
-  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spo_load has not been called");
-  cudaStream_t st = (cudaStream_t)stream;
+// one launch per size class over nsteps steps, from psi0 (resume = false) or
+// from the plan's current state (resume = true)
+static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t st) {
   if (p->c_cap_steps != nsteps) {
     if (p->d_c) cudaFree(p->d_c);
     p->d_c = nullptr;
@@ -612,6 +645,10 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
       a.tab = p->tsod;
       a.pk = c.d_pk;
       a.psi0 = p->d_psi0;
+      if (resume) {
+        a.psi_start = p->d_psi;
+        a.psi_prev_start = p->d_psi_prev;
+      }
       a.psi_out = p->d_psi;
       a.psi_prev_out = p->d_psi_prev;
       a.c_out = p->d_c;
@@ -624,6 +661,7 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
       a.tab = p->t64;
       a.pk = c.d_pk;
       a.psi0 = p->d_psi0;
+      if (resume) a.psi_start = p->d_psi;
       a.psi_out = p->d_psi;
       a.c_out = p->d_c;
       a.kq_c = p->d_kq_c;
@@ -636,6 +674,7 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
       a.tab = p->t32;
       a.pk = c.d_pk;
       a.psi0 = p->d_psi0;
+      if (resume) a.psi_start = p->d_psi;
       a.psi_out = p->d_psi;
       a.c_out = p->d_c;
       a.nsteps = nsteps;
@@ -644,6 +683,40 @@ extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
     if (e != cudaSuccess) return set_cuda_error("spo1d_kernel launch", e);
     ESPEC_CK(cudaEventRecord(p->events[ci], cs));
     ESPEC_CK(cudaStreamWaitEvent(st, p->events[ci], 0));
+  }
+  if (p->method == ESPEC_SOD) p->has_prev = true;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spo_run(espec_spo_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spo_load has not been called");
+  return prop_launch(p, nsteps, false, (cudaStream_t)stream);
+}
+
+extern "C" int espec_prop_continue(espec_spo_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spo_load has not been called");
+  if (p->method == ESPEC_SOD && !p->has_prev)
+    return set_error(ESPEC_EINVAL, "a SOD plan continues a run: call espec_spo_run first");
+  return prop_launch(p, nsteps, true, (cudaStream_t)stream);
+}
+
+extern "C" int espec_prop_energies(espec_spo_plan* p, double* e, double* norm, void* stream) {
+  if (!p || !e || !norm) return set_error(ESPEC_EINVAL, "null argument");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spo_load has not been called");
+  cudaStream_t st = (cudaStream_t)stream;
+  for (auto& c : p->classes) {
+    DiagArgs a{p->d_psi, p->d_vpot, p->d_tc, c.d_kfreq, c.d_pkd, p->d_diag};
+    cudaError_t err = diag_launch(c.n, a, c.count, st);
+    if (err != cudaSuccess) return set_cuda_error("diag1d_kernel launch", err);
+  }
+  std::vector<double2> h(p->npk);
+  ESPEC_CK(cudaMemcpyAsync(h.data(), p->d_diag, 16 * (size_t)p->npk, cudaMemcpyDeviceToHost, st));
+  ESPEC_CK(cudaStreamSynchronize(st));
+  for (int i = 0; i < p->npk; ++i) {
+    e[i] = h[i].x;
+    norm[i] = h[i].y;
   }
   return ESPEC_OK;
 }

@@ -157,6 +157,7 @@ struct SpoArgs {
   SpoTables<R> tab;
   const SpoPacket* pk;      // per CTA (packets of this size class)
   const double2* psi0;      // initial psi (x order), FP64
+  const double2* psi_start; // resume from this psi instead of psi0 (C(0) not written)
   double2* psi_out;         // psi(TF) (x order), FP64
   double2* c_out;           // C(t) samples, nsteps+1 per packet
   const double* kq_c;       // FP64 quirk form: cos(CST1*TC) per point (final layout)
@@ -473,15 +474,16 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
 #pragma unroll
   for (int j = 0; j < P; ++j) {
     const int x = base + Th::x_pos(t, j);
-    const double2 p0 = a.psi0[x];
+    const double2 p0 = a.psi_start ? a.psi_start[x] : a.psi0[x];
     c0r += p0.x * p0.x + p0.y * p0.y;
     v[j] = mk((R)p0.x, (R)p0.y);
     typename TB::phase_t kk{};
     if constexpr (!kQuirk) kk = a.tab.k[base + Th::final_pos(t, j)];
     tab.put(j, t, a.tab.g[x], kk, a.tab.w[x]);
   }
-  // C(0) = <psi0|psi0>
-  {
+  // C(0) = <psi0|psi0> (a resumed run continues a series: its first sample
+  // belongs to the previous segment)
+  if (!a.psi_start) {
     double cr = c0r;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cr += __shfl_xor_sync(0xffffffffu, cr, o);

@@ -1,0 +1,83 @@
+"""Python mirror of eSPec's FFT propagator subroutines, called through the
+Fortran ABI of libespecgpu.so (`pspofft_`, `psodfft_`).
+
+`pspofft` and `psodfft` take the arguments of PSPOFFT (pspofft.f:1-3) and
+PSODFFT (psodfft.f:1-3) by name, with the same meaning, and update the same
+arrays in place: U1/V1 (and U2/V2), TC and the LNZVC columns MPR/MPI
+(LNZVC is a Fortran-ordered (MXDCT, ncols) array; MPR/MPI are 1-based).
+They return INFO: 0, 1 for a drift beyond TOL percent, -1 for a case the GPU
+path does not run (the reason goes to standard error).  The partial
+auto-correlation table goes to standard output when PRTCRL is '.YES' or
+'.PARTIAL', as the reference prints it.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+def _arr(a):
+    if (not isinstance(a, np.ndarray) or a.dtype != np.float64
+            or not (a.flags.c_contiguous or a.flags.f_contiguous)):
+        raise TypeError("arrays updated in place must be contiguous float64 numpy arrays")
+    return C.c_void_p(a.ctypes.data)
+
+
+def _common(absorb, dim, prtcrl, tpabsor, lc, mp, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_, sh,
+            sm):
+    keep = dict(
+        absorb=C.c_int(1 if absorb else 0), lc=C.c_int(lc), mp=C.c_int(mp), mpi=C.c_int(mpi),
+        mpr=C.c_int(mpr), mxdct=C.c_int(mxdct), n=C.c_int(n), dt=C.c_double(dt),
+        ti=C.c_double(ti), tf=C.c_double(tf), tol=C.c_double(tol),
+        np=np.ascontiguousarray(np_, dtype=np.int32), sh=N.f64(sh), sm=N.f64(sm),
+        shm=np.zeros(3), dummy=np.zeros(1),
+        dim=dim.encode(), prtcrl=prtcrl.encode(), tpabsor=tpabsor.encode())
+    return keep
+
+
+def pspofft(*, absorb, dim, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_, sh,
+            sm, u1, v1, tc, vpot, vabc, lnzvc, mp=0):
+    """PSPOFFT: split-operator propagation of U1 + i V1 from TI to TF (fs)."""
+    k = _common(absorb, dim, prtcrl, tpabsor, lc, mp, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_,
+                sh, sm)
+    info = C.c_int(0)
+    vp = N.f64(vpot)
+    va = N.f64(vabc) if vabc is not None else np.zeros(n)
+    N.load().pspofft_(
+        C.byref(k["absorb"]), k["dim"], k["prtcrl"], k["tpabsor"], C.byref(info), C.byref(k["lc"]),
+        C.byref(k["mp"]), C.byref(k["mpi"]), C.byref(k["mpr"]), C.byref(k["mxdct"]),
+        C.byref(k["n"]), C.byref(k["dt"]), C.byref(k["ti"]), C.byref(k["tf"]), C.byref(k["tol"]),
+        N.ptr(k["np"]), N.ptr(k["shm"]), N.ptr(k["sh"]), N.ptr(k["sm"]), _arr(u1), _arr(v1),
+        N.ptr(k["dummy"]), N.ptr(k["dummy"]), _arr(tc), N.ptr(vp), N.ptr(va), _arr(lnzvc),
+        N.ptr(k["dummy"]), N.ptr(k["dummy"]), N.ptr(k["dummy"]),
+        len(k["dim"]), len(k["prtcrl"]), len(k["tpabsor"]))
+    return info.value
+
+
+def psodfft(*, absorb, dim, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_, sh,
+            sm, u1, u2, v1, v2, tc, vpot, vabc, lnzvc, mp=0):
+    """PSODFFT: second-order-differences propagation; on return U2 + i V2 is
+    psi(TF) and U1 + i V1 is psi(TF - dt)."""
+    k = _common(absorb, dim, prtcrl, tpabsor, lc, mp, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_,
+                sh, sm)
+    info = C.c_int(0)
+    vp = N.f64(vpot)
+    va = N.f64(vabc) if vabc is not None else np.zeros(n)
+    N.load().psodfft_(
+        C.byref(k["absorb"]), k["dim"], k["prtcrl"], k["tpabsor"], C.byref(info), C.byref(k["lc"]),
+        C.byref(k["mp"]), C.byref(k["mpi"]), C.byref(k["mpr"]), C.byref(k["mxdct"]),
+        C.byref(k["n"]), C.byref(k["dt"]), C.byref(k["ti"]), C.byref(k["tf"]), C.byref(k["tol"]),
+        N.ptr(k["np"]), N.ptr(k["shm"]), N.ptr(k["sh"]), N.ptr(k["sm"]), _arr(u1), _arr(u2),
+        _arr(v1), _arr(v2), N.ptr(k["dummy"]), N.ptr(k["dummy"]), _arr(tc), N.ptr(vp), N.ptr(va),
+        N.ptr(k["dummy"]), N.ptr(k["dummy"]), N.ptr(k["dummy"]), _arr(lnzvc),
+        len(k["dim"]), len(k["prtcrl"]), len(k["tpabsor"]))
+    return info.value
+
+
+def format_crl_row(t, e, cr, ci, ct, fnt):
+    """One row of the partial auto-correlation table (FORMAT 1021, pspofft.f:148)."""
+    buf = C.create_string_buffer(256)
+    n = N.load().espec_format_crl_row(t, e, cr, ci, ct, fnt, buf, 256)
+    N.check(0 if n > 0 else n, "espec_format_crl_row")
+    return buf.value.decode()

@@ -62,6 +62,22 @@ class SpoBatch:
         N.check(N.load().espec_spo_run(self._h, int(nsteps), stream), "espec_spo_run")
         self.nsteps = int(nsteps)
 
+    def advance(self, nsteps, stream=None):
+        """nsteps more steps from the current state; C(t) samples 1..nsteps of
+        this call (sample 0 is not written) -- how PSPOFFT's printed rows
+        split a run (pspofft.f:125-144)."""
+        N.check(N.load().espec_prop_continue(self._h, int(nsteps), stream), "espec_prop_continue")
+        self.nsteps = int(nsteps)
+
+    def energies(self, stream=None):
+        """(E, norm) of every packet's current state: EFFT4 (eigenergfft.f:58-100)
+        in hartree and sum |psi|^2, FP64 on the GPU."""
+        e = np.zeros(self.npk)
+        nr = np.zeros(self.npk)
+        N.check(N.load().espec_prop_energies(self._h, N.ptr(e), N.ptr(nr), stream),
+                "espec_prop_energies")
+        return e, nr
+
     def results(self, stream=None):
         """(C(t) [npk, nsteps+1] complex, psi(TF) concatenated complex), host."""
         ns = self.nsteps

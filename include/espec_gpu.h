@@ -53,6 +53,40 @@ extern "C" {
 
 #define ESPEC_SHFS 2.4188843243e-2  /* fs per atomic unit of time (pspofft.f:76) */
 
+/* ----------------------------------------------------------------------
+ * Fortran-callable drop-ins (1D).  Same arguments, same outputs and the
+ * same printed partial auto-correlation table as the reference routines;
+ * the defects of the reference's arithmetic are reproduced.  DIM other than
+ * '.1D' or an unsupported N sets INFO = -1 (message on standard error).
+ * WRK*, SHM, XI, XF, VAR and MP are accepted and not used.
+ * ---------------------------------------------------------------------- */
+/* replaces SUBROUTINE PSPOFFT (pspofft.f:1-3; called from espec.f:1474) */
+void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
+              const char* tpabsor, int* info, const int* lc, const int* mp,
+              const int* mpi, const int* mpr, const int* mxdct, const int* n,
+              const double* dt, const double* ti, const double* tf,
+              const double* tol, const int* np, const double* shm,
+              const double* sh, const double* sm, double* u1, double* v1,
+              const double* xi, const double* xf, double* tc,
+              const double* vpot, const double* vabc, double* lnzvc,
+              double* wrk1, double* wrk2, const double* var, size_t dim_len,
+              size_t prtcrl_len, size_t tpabsor_len);
+/* replaces SUBROUTINE PSODFFT (psodfft.f:1-3; called from espec.f:1373) */
+void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
+              const char* tpabsor, int* info, const int* lc, const int* mp,
+              const int* mpi, const int* mpr, const int* mxdct, const int* n,
+              const double* dt, const double* ti, const double* tf,
+              const double* tol, const int* np, const double* shm,
+              const double* sh, const double* sm, double* u1, double* u2,
+              double* v1, double* v2, const double* xi, const double* xf,
+              double* tc, const double* vpot, const double* vabc,
+              double* wrkr, double* wrki, const double* var, double* lnzvc,
+              size_t dim_len, size_t prtcrl_len, size_t tpabsor_len);
+/* one row of the partial auto-correlation table in FORMAT 1021 of
+ * pspofft.f:148 (newline included); returns its length */
+int espec_format_crl_row(double t, double e, double cr, double ci, double ct,
+                         double fnt, char* buf, int len);
+
 const char* espec_last_error(void);
 const char* espec_version(void);
 /* 1 when a CUDA device of compute capability 10.x is usable, else 0 */
@@ -92,6 +126,16 @@ int espec_spo_load(espec_spo_plan* plan, const double* vpot, const double* vabc,
 int espec_spo_run(espec_spo_plan* plan, int nsteps, void* stream);
 int espec_spo_results(espec_spo_plan* plan, double* c_re, double* c_im,
                       double* psi_re, double* psi_im, int where, void* stream);
+/* nsteps more steps from the plan's current state (psi0 right after
+ * espec_spo_load, else the state the last run or continuation left; a SOD
+ * plan needs one espec_spo_run first).  C(t) stays <psi0|psi(t)>; sample s
+ * (1..nsteps) is the s-th step of this call, sample 0 is not written.  The
+ * printed rows of PSPOFFT/PSODFFT split a run this way (pspofft.f:125-144). */
+int espec_prop_continue(espec_spo_plan* plan, int nsteps, void* stream);
+/* energy EFFT4 (eigenergfft.f:58-100: sum V|psi|^2 + B sum TC |F psi|^2, B=1/N,
+ * hartree) and norm sum |psi|^2 (pspofft.f:96-98) of each packet's current
+ * state, FP64 on the GPU; e and norm are host arrays of npk entries. */
+int espec_prop_energies(espec_spo_plan* plan, double* e, double* norm, void* stream);
 /* Kernel variant for the packets of size npts (0..espec_spo_variant_count()-1):
  * radix plan, location of the per-point tables and register budget.  Call
  * before espec_spo_load.  Defaults come from autotuning on B200. */

@@ -103,6 +103,27 @@ def parse_table(out, header, ncol):
     return np.array(rows)
 
 
+def partial_text(out, first=150, last=50):
+    """The head of the partial auto-correlation table as printed (the lines
+    from the blank line before its title to the column titles) and the text
+    of its first and last rows, for pinning the drop-ins' Fortran output."""
+    lines = out.splitlines()
+    for i, l in enumerate(lines):
+        if "Partial auto-correlation function:" in l:
+            break
+    head = lines[i - 1:i + 4]
+    rows = []
+    for l in lines[i + 4:]:
+        if len(l.split()) != 6:
+            break
+        rows.append(l)
+    keep = rows[:first] + rows[-last:]
+    return "\n".join(head + keep) + "\n", len(rows)
+
+
+TEXT_CASES = ("morse1d_spo", "morse1d_sod", "morse1d_spo_voptic")
+
+
 def fmt(x):
     return repr(float(x))
 
@@ -210,6 +231,10 @@ def case_morse1d(name, prop, absorb_block, absorb_meta):
     deck = DECK.format(title=name, dim=".1D", np="1024", mass=fmt(mass_amu), prop=prop,
                        tf=fmt(tf), dt=fmt(dt_fs), mp=mp, absorb=absorb_block, mf=12)
     out = run_deck(deck, {"wf_pot.inp": write_1d_file(x, psi, v)})
+    if name in TEXT_CASES:
+        text, nrows = partial_text(out)
+        with open(os.path.join(OUT, name + "_partial.txt"), "w") as f:
+            f.write(text)
     rows = parse_partial(out)
     corr = parse_table(out, "*t/fs*       *C(t)r*       *C(t)i*", 3)
     spec = parse_table(out, "*E (eV)*           *W*           *FFTr*          *FFTi*", 4)
@@ -295,6 +320,12 @@ SMOOTH = """*ABSORBING
 def main():
     if not os.path.exists(BIN):
         sys.exit("eSPec executable not found at " + BIN)
+    if "--text-only" in sys.argv:  # only the *_partial.txt files
+        vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
+        case_morse1d("morse1d_spo", ".PFSPO", "", {})
+        case_morse1d("morse1d_sod", ".PFSOD", "", {})
+        case_morse1d("morse1d_spo_voptic", ".PFSPO", VOPTIC, vmeta)
+        return
     cases = {}
     cases["test8"] = case_test8()
     cases["test4"] = case_test4()

@@ -1,0 +1,225 @@
+"""GPU parity of the Fortran drop-ins pspofft_/psodfft_ (PSPOFFT pspofft.f:1-150,
+PSODFFT psodfft.f:1-211) and of the plan calls they are built from
+(espec_prop_continue, espec_prop_energies).
+
+Each drop-in call is compared with the oracle's restatement of the same
+subroutine on the same inputs: LNZVC columns, psi(TF), TC and INFO (FP64,
+|d| <= 1e-10), and the printed partial auto-correlation table, row by row,
+with the rows the shipped executable printed (tests/golden) at its print
+precision."""
+import numpy as np
+import pytest
+
+import espec_b200 as E
+from espec_b200 import fortran as F
+from espec_b200 import workloads as W
+
+import golden_cases as G
+
+pytestmark = pytest.mark.gpu
+
+CASES = ["morse1d_spo", "morse1d_spo_voptic", "morse1d_spo_smooth",
+         "morse1d_sod", "morse1d_sod_voptic", "morse1d_sod_smooth"]
+TPABSOR = {None: ".NONE", "VOPTIC_POLIN": ".VOPTIC_POLIN", "SMOOTHW": ".SMOOTHW"}
+
+
+def parse_table(out):
+    lines = out.split("\n")
+    i = lines.index(" Partial auto-correlation function:")
+    assert lines[i - 1] == " " and lines[i + 1].startswith(" ====") and lines[i + 2] == ""
+    assert lines[i + 3].split() == ["*t/fs*", "*E/a.u.*", "*Cr(t)*", "*Ci(t)*", "*|C(t)|*",
+                                    "*|C|*"]
+    rows, text = [], []
+    for l in lines[i + 4:]:
+        if len(l.split()) != 6:
+            break
+        text.append(l)
+        rows.append([float(x) for x in l.split()])
+    return np.array(rows), text
+
+
+def call_dropin(case, prtcrl, lc=None, tol=None, mxdct=None, ncols=4, mpr=2, mpi=3, tf=None):
+    m = case["meta"]
+    n = case["np"][0]
+    lc = case["lc"] if lc is None else lc
+    tf = case["tf"] if tf is None else tf
+    nsteps = 2 * int(round((tf - case["ti"]) / case["dt"])) + 4
+    mxdct = nsteps // lc + 4 if mxdct is None else mxdct
+    lnzvc = np.zeros((mxdct, ncols), order="F")
+    u1 = np.array(case["psi"], dtype=np.float64)
+    v1 = np.zeros(n)
+    tc = np.zeros(n)
+    args = dict(absorb=case["absorb"] != 0, dim=".1D", prtcrl=prtcrl,
+                tpabsor=TPABSOR[m.get("absorb")], lc=lc, mpi=mpi, mpr=mpr, mxdct=mxdct, n=n,
+                dt=case["dt"], ti=case["ti"], tf=tf, tol=case["tol"] if tol is None else tol,
+                np_=case["np"], sh=case["sh"], sm=case["sm"], u1=u1, v1=v1, tc=tc,
+                vpot=case["vpot"], vabc=case["vabc"], lnzvc=lnzvc)
+    if m["prop"] == ".PFSPO":
+        info = F.pspofft(**args)
+        return dict(info=info, u=u1, v=v1, tc=tc, lnzvc=lnzvc)
+    u2, v2 = np.zeros(n), np.zeros(n)
+    info = F.psodfft(u2=u2, v2=v2, **args)
+    return dict(info=info, u=u2, v=v2, u_prev=u1, v_prev=v1, tc=tc, lnzvc=lnzvc)
+
+
+def oracle_of(case, prtcrl, lc=None, tol=None, tf=None):
+    c = dict(case)
+    if lc is not None:
+        c["lc"] = lc
+    if tol is not None:
+        c["tol"] = tol
+    if tf is not None:
+        c["tf"] = tf
+    return G.run_oracle(c, case["ref_quirks"], prtcrl=prtcrl)
+
+
+def check_arrays(case, got, ref, mpr=2, mpi=3):
+    nc = ref["nc"]
+    col = got["lnzvc"]
+    assert np.max(np.abs(col[:nc, mpr - 1] - ref["c"].real)) <= 1e-10
+    assert np.max(np.abs(col[:nc, mpi - 1] - ref["c"].imag)) <= 1e-10
+    assert not np.any(col[nc:, [mpr - 1, mpi - 1]]), "samples past NC written"
+    others = [j for j in range(col.shape[1]) if j not in (mpr - 1, mpi - 1)]
+    assert not np.any(col[:, others]), "other LNZVC columns touched"
+    assert np.max(np.abs(got["u"] - ref["u"])) <= 1e-10
+    assert np.max(np.abs(got["v"] - ref["v"])) <= 1e-10
+    if "u_prev" in got:
+        assert np.max(np.abs(got["u_prev"] - ref["u_prev"])) <= 1e-10
+        assert np.max(np.abs(got["v_prev"] - ref["v_prev"])) <= 1e-10
+    tc_ref = E.spo.digt_1d(case["np"][0], case["sh"][0], case["sm"][0])
+    assert np.array_equal(got["tc"], tc_ref)
+    assert got["info"] == ref["info"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_dropin_matches_oracle_and_executable(oracle, capfd, name):
+    case = G.setup_case(name)
+    capfd.readouterr()
+    got = call_dropin(case, ".PARTIAL")
+    out, err = capfd.readouterr()
+    assert err == ""
+    ref = oracle_of(case, oracle.PRT_PARTIAL)
+    check_arrays(case, got, ref)
+    rows, text = parse_table(out)
+    # against the oracle's rows (FP64 values, then printed): within print precision
+    assert rows.shape == ref["rows"].shape
+    half_ulp = np.array([5e-9, 0, 5e-8, 5e-8, 5e-9, 5e-7])
+    d = np.abs(rows - ref["rows"])
+    assert np.all(d[:, [0, 2, 3, 4, 5]] <= half_ulp[[0, 2, 3, 4, 5]] + 1e-10)
+    # E12.6 keeps 6 significant digits
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(ref["rows"][:, 1]))) - 5)
+    assert np.all(np.abs(rows[:, 1] - ref["rows"][:, 1]) <= 0.5 * e_ulp * 1.001)
+    # against the executable's printed rows: the same text except where the
+    # last printed digit rounds the other way
+    gold = case["data"]["rows"]
+    assert rows.shape == gold.shape
+    ulp = np.array([1e-8, 0, 1e-7, 1e-7, 1e-8, 1e-6])
+    dg = np.abs(rows - gold)
+    assert np.all(dg[:, [0, 2, 3, 4, 5]] <= ulp[[0, 2, 3, 4, 5]] * 1.01)
+    assert np.all(np.abs(rows[:, 1] - gold[:, 1]) <= e_ulp * 1.01)
+    if name in ("morse1d_spo", "morse1d_sod", "morse1d_spo_voptic"):
+        with open(f"{G.GOLDEN}/{name}_partial.txt") as f:
+            golden_lines = f.read().split("\n")[5:5 + 150]
+        same = sum(a == b for a, b in zip(text[:150], golden_lines))
+        assert same >= 140, same
+
+
+@pytest.mark.parametrize("name", ["morse1d_spo", "morse1d_sod_voptic"])
+def test_dropin_stride_columns_and_no_print(oracle, capfd, name):
+    case = G.setup_case(name)
+    tf = 300 * case["dt"]
+    capfd.readouterr()
+    got = call_dropin(case, ".NO", lc=7, ncols=8, mpr=5, mpi=6, tf=tf)
+    out, _ = capfd.readouterr()
+    assert out == ""
+    ref = oracle_of(case, oracle.PRT_NONE, lc=7, tf=tf)
+    check_arrays(case, got, ref, mpr=5, mpi=6)
+    # '.PARTIAL' with LC = 7 prints the rows of steps 0, 7, 14, ...
+    got = call_dropin(case, ".PARTIAL", lc=7, ncols=8, mpr=5, mpi=6, tf=tf)
+    out, _ = capfd.readouterr()
+    ref = oracle_of(case, oracle.PRT_PARTIAL, lc=7, tf=tf)
+    check_arrays(case, got, ref, mpr=5, mpi=6)
+    rows, _ = parse_table(out)
+    assert rows.shape == ref["rows"].shape
+    assert np.max(np.abs(rows[:, [0, 2, 3]] - ref["rows"][:, [0, 2, 3]])) <= 5.1e-8
+
+
+@pytest.mark.parametrize("name", ["morse1d_spo", "morse1d_spo_voptic", "morse1d_sod",
+                                  "morse1d_sod_voptic"])
+def test_dropin_info_drift_semantics(oracle, capfd, name):
+    """INFO = 1 on drift: PSPOFFT tests the norm only with an absorber
+    (pspofft.f:137-142), PSODFFT only without one (psodfft.f:178-183)."""
+    case = G.setup_case(name)
+    tf = 200 * case["dt"]
+    for tol in (1e-12, 1e-7, 1e-3, 10.0):
+        got = call_dropin(case, ".YES", tol=tol, tf=tf)
+        ref = oracle_of(case, oracle.PRT_YES, tol=tol, tf=tf)
+        assert got["info"] == ref["info"], (tol, got["info"], ref["info"])
+    capfd.readouterr()
+
+
+def test_dropin_rejects_what_it_does_not_run(capfd):
+    case = G.setup_case("morse1d_spo")
+    capfd.readouterr()
+    n = case["np"][0]
+    lnzvc = np.zeros((8, 3), order="F")
+    u1, v1, tc = np.array(case["psi"]), np.zeros(n), np.zeros(n)
+    info = F.pspofft(absorb=False, dim=".2D", prtcrl=".NO", tpabsor=".NONE", lc=1, mpi=3, mpr=2,
+                     mxdct=8, n=n, dt=case["dt"], ti=0.0, tf=case["dt"], tol=1.0, np_=[n],
+                     sh=case["sh"], sm=case["sm"], u1=u1, v1=v1, tc=tc, vpot=case["vpot"],
+                     vabc=None, lnzvc=lnzvc)
+    _, err = capfd.readouterr()
+    assert info == -1 and "1D" in err
+    assert np.array_equal(u1, case["psi"]) and not lnzvc.any()
+
+
+def test_continue_and_energies_match_single_run(oracle):
+    """A run split by espec_prop_continue follows the same trajectory as one
+    run; energies/norms of the state match the oracle's EFFT4 and norm."""
+    rng = np.random.default_rng(5)
+    sizes = [384, 1024, 2048]
+    packs = []
+    for n in sizes:
+        x0, x1 = 0.5, 8.0
+        sh = (x1 - x0) / (n - 1)
+        x = x0 + np.arange(n) * sh
+        v = W.morse(x, rng.uniform(0.05, 0.25), rng.uniform(0.6, 1.6), rng.uniform(1.0, 2.5))
+        psi = W.gaussian(x, rng.uniform(1.2, 2.5), rng.uniform(0.1, 0.3)) * np.exp(0.3j * x)
+        packs.append((n, sh, rng.uniform(900.0, 30000.0), v, psi))
+    dt = 0.01 * W.SHFS
+    vcat = np.concatenate([p[3] for p in packs])
+    pcat = np.concatenate([p[4] for p in packs])
+    off = np.concatenate([[0], np.cumsum(sizes)])
+    for cls, kw in [(E.SpoBatch, dict(precision="fp64")), (E.SpoBatch, dict(precision="mixed")),
+                    (E.SodBatch, {})]:
+        tol = 2e-6 if kw.get("precision") == "mixed" else 1e-11
+        one = cls(sizes, [p[1] for p in packs], [p[2] for p in packs], dt, **kw)
+        one.load(vcat, pcat)
+        e0, n0 = one.energies()
+        for k, (n, sh, sm, v, psi) in enumerate(packs):
+            tcr = E.spo.digt_1d(n, sh, sm)
+            ref_e = oracle.efft4([n], psi.real, psi.imag, tcr, v, 1.0 / n)
+            assert abs(e0[k] - ref_e) <= 1e-12 * abs(ref_e)
+            assert abs(n0[k] - np.sum(np.abs(psi) ** 2)) <= 1e-12
+        one.run(90)
+        c_one, psi_one = one.results()
+        seg = cls(sizes, [p[1] for p in packs], [p[2] for p in packs], dt, **kw)
+        seg.load(vcat, pcat)
+        seg.run(30)
+        c_a, _ = seg.results()
+        seg.advance(1)
+        c_b, _ = seg.results()
+        seg.advance(59)
+        c_c, psi_seg = seg.results()
+        c_seg = np.concatenate([c_a, c_b[:, 1:], c_c[:, 1:]], axis=1)
+        assert np.max(np.abs(c_seg - c_one)) <= tol, (cls, kw)
+        assert np.max(np.abs(psi_seg - psi_one)) <= tol
+        e1, n1 = seg.energies()
+        for k, (n, sh, sm, v, psi) in enumerate(packs):
+            p = psi_seg[off[k]:off[k + 1]]
+            tcr = E.spo.digt_1d(n, sh, sm)
+            ref_e = oracle.efft4([n], p.real.copy(), p.imag.copy(), tcr, v, 1.0 / n)
+            assert abs(e1[k] - ref_e) <= 1e-12 * abs(ref_e)
+            assert abs(n1[k] - np.sum(np.abs(p) ** 2)) <= 1e-12
+        one.close()
+        seg.close()
