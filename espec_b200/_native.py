@@ -16,7 +16,8 @@ FP64, MIXED = 0, 1
 ABS_NONE, ABS_VOPTIC, ABS_SMOOTHW = 0, 1, 2
 Q_SPO_INPLACE = 1
 Q_SOD_SMOOTHW = 2
-SPO, SOD = 0, 1
+Q_SIL_INPLACE = 4
+SPO, SOD, SIL = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 SHFS = 2.4188843243e-2
 
@@ -28,6 +29,8 @@ EXPORTS = [
     "espec_spo_set_variant", "espec_spo_variant_count", "espec_spo_run_static",
     "espec_prop_create", "espec_prop_previous", "espec_prop_continue", "espec_prop_energies",
     "espec_format_crl_row", "pspofft_", "psodfft_",
+    "espec_grid_create", "espec_grid_load", "espec_grid_run", "espec_grid_continue",
+    "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
 ]
 
 
@@ -75,6 +78,17 @@ def load():
     lib.pspofft_.restype = None
     lib.psodfft_.argtypes = [vp] * 32 + [C.c_size_t] * 3
     lib.psodfft_.restype = None
+    lib.espec_grid_create.argtypes = [C.POINTER(vp), C.c_int, C.c_int, i, d, C.c_double,
+                                      C.c_int, C.c_int, C.c_int, C.c_int]
+    lib.espec_grid_load.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]
+    lib.espec_grid_run.argtypes = [vp, C.c_int, vp]
+    lib.espec_grid_continue.argtypes = [vp, C.c_int, vp]
+    lib.espec_grid_results.argtypes = [vp, vp, vp, vp, vp, C.c_int, vp]
+    lib.espec_grid_energies.argtypes = [vp, vp, vp, vp]
+    lib.espec_grid_npoints.argtypes = [vp]
+    lib.espec_grid_npoints.restype = C.c_long
+    lib.espec_grid_destroy.argtypes = [vp]
+    lib.espec_grid_destroy.restype = None
     lib.espec_spo_destroy.argtypes = [vp]
     lib.espec_spo_destroy.restype = None
     _lib = lib

@@ -1,0 +1,675 @@
+// sil.cu -- short-iterative-Lanczos propagation on one grid (1D/2D/3D),
+// FP64: the cooperative kernel described in sil.cuh, the finite-difference
+// energy kernel, and the grid plan behind espec_grid_* (include/espec_gpu.h).
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "espec_gpu.h"
+#include "espec_internal.h"
+#include "sil.cuh"
+
+namespace espec {
+namespace {
+
+// a barrier wait gives up after this many polls (~ seconds); the kernel then
+// sets the error flag and returns
+constexpr long kSpinLimit = 1L << 24;
+
+struct Range {
+  int lo, hi;
+};
+
+__device__ __forceinline__ Range my_range(long n) {
+  const long chunk = (n + gridDim.x - 1) / gridDim.x;
+  long lo = (long)blockIdx.x * chunk, hi = lo + chunk;
+  if (lo > n) lo = n;
+  if (hi > n) hi = n;
+  return Range{(int)lo, (int)hi};
+}
+
+// Grid barrier fused with a reduction: sp[0..nq) holds this CTA's partial
+// sums; on return st[0..nq) holds the totals over all CTAs, summed by the last
+// CTA to arrive in CTA order (deterministic).  false = a wait gave up.
+__device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int nq,
+                            int* s_flag) {
+  const int b = blockIdx.x, G = gridDim.x, t = threadIdx.x;
+  for (int q = t; q < nq; q += blockDim.x) a.part[(long)b * kSilNQ + q] = sp[q];
+  __threadfence();
+  __syncthreads();
+  if (t == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(a.bar[0]);
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(a.bar[1]);
+    cuda::atomic_ref<int, cuda::thread_scope_device> err(*a.err);
+    const unsigned g = gen.load(cuda::memory_order_acquire);
+    const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+    s_flag[0] = arrived == (unsigned)G - 1;
+    s_flag[1] = 1;
+    if (!s_flag[0]) {
+      long spins = 0;
+      while (gen.load(cuda::memory_order_acquire) == g) {
+        if (++spins > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
+          err.store(1, cuda::memory_order_relaxed);
+          s_flag[1] = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+  }
+  __syncthreads();
+  if (!s_flag[1]) return false;
+  __threadfence();
+  if (s_flag[0]) {
+    for (int q = t; q < nq; q += blockDim.x) {
+      double s = 0.0;
+      for (int i = 0; i < G; ++i) s += __ldcg(a.part + (long)i * kSilNQ + q);
+      st[q] = s;
+      a.tot[q] = s;
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) {
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(a.bar[0]);
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(a.bar[1]);
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.fetch_add(1u, cuda::memory_order_release);
+    }
+  } else {
+    for (int q = t; q < nq; q += blockDim.x) st[q] = __ldcg(a.tot + q);
+  }
+  __syncthreads();
+  return true;
+}
+
+// sum of nv per-thread values over the CTA into sp[0..nv)
+template <int NV>
+__device__ __forceinline__ void block_sum(const double (&x)[NV], double* sp, double* scratch) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < NV; ++i) {
+    double s = x[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) scratch[warp * NV + i] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double s = 0.0;
+    for (int w = 0; w < kSilThreads / 32; ++w) s += scratch[w * NV + threadIdx.x];
+    sp[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
+// H_FD x at point k with every x value divided by d (au1d.f:52-73,
+// au2di.f:57-225, au3d.f:61-117): (30 sum(shm) + V) x_k + sum_a shm_a
+// (x_{-2} - 16 x_{-1} - 16 x_{+1} + x_{+2}), zero outside the grid.
+__device__ __forceinline__ double apply_h(const SilArgs& a, const double* x, int k, double d) {
+  double s = (a.sht30 + __ldg(a.vpot + k)) * (__ldcg(x + k) / d);
+  int idx[3], len[3] = {a.nx, a.ny, a.nz}, str[3];
+  idx[0] = k % a.nx;
+  str[0] = 1;
+  if (a.ndim > 1) {
+    idx[1] = (k / a.nx) % a.ny;
+    str[1] = a.nx;
+  }
+  if (a.ndim > 2) {
+    idx[2] = k / (a.nx * a.ny);
+    str[2] = a.nx * a.ny;
+  }
+  for (int ax = 0; ax < a.ndim; ++ax) {
+    const double h = a.shm[ax];
+    const int i = idx[ax], st = str[ax];
+    if (i >= 2) s += h * (__ldcg(x + k - 2 * st) / d);
+    if (i >= 1) s += -16.0 * h * (__ldcg(x + k - st) / d);
+    if (i + 1 < len[ax]) s += -16.0 * h * (__ldcg(x + k + st) / d);
+    if (i + 2 < len[ax]) s += h * (__ldcg(x + k + 2 * st) / d);
+  }
+  return s;
+}
+
+// Krylov coefficients of both chains (every CTA computes the same values):
+// Z = exp(-i cst T) by Taylor series (degree kTaylor) of T scaled to norm
+// <= 1/4, then squared back.  out[0] = Re Z y_u, out[1] = Im Z y_u (or
+// Im(Z^2) y_u / 2 in the reference-defect form), out[2] = Re Z y_v,
+// out[3] = -Im Z y_v.
+constexpr int kTaylor = 16;
+constexpr int kMM = kSilMaxM * kSilMaxM;
+
+struct KrylovSmem {
+  double2 P[2][kMM];
+  double2 Q[2][kMM];
+};
+
+__device__ void krylov_coeffs(int m, double cst, int quirk, const double (*al)[kSilMaxM],
+                              const double (*bt)[kSilMaxM], const double (*y)[kSilMaxM],
+                              const int* active, KrylovSmem& ks, double (*out)[kSilMaxM]) {
+  __shared__ int s_sq[2];
+  __shared__ double s_scale[2];
+  const int t = threadIdx.x;
+  if (t < 2) {
+    double nrm = 0.0;
+    for (int i = 0; i < m; ++i) {
+      double r = fabs(al[t][i]);
+      if (i > 0) r += fabs(bt[t][i - 1]);
+      if (i + 1 < m) r += fabs(bt[t][i]);
+      nrm = fmax(nrm, r);
+    }
+    nrm *= fabs(cst);
+    int sq = 0;
+    while (nrm > 0.25 && sq < 60) {
+      nrm *= 0.5;
+      ++sq;
+    }
+    s_sq[t] = sq;
+    s_scale[t] = ldexp(cst, -sq);
+  }
+  // P = I
+  for (int e = t; e < 2 * kMM; e += blockDim.x) {
+    const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
+    ks.P[c][i * kSilMaxM + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+  }
+  __syncthreads();
+  // Horner: P = I + B P / k, B = -i scale T (T tridiagonal)
+  for (int k = kTaylor; k >= 1; --k) {
+    const double rk = 1.0 / k;
+    for (int e = t; e < 2 * kMM; e += blockDim.x) {
+      const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
+      if (i >= m || j >= m) continue;
+      const double sc = s_scale[c];
+      double re = 0.0, im = 0.0;
+      // (B P)_{ij} = sum_l (-i sc T_il) P_lj = sum_l sc T_il (Im P_lj, -Re P_lj)
+      const double tii = sc * al[c][i];
+      const double2 pii = ks.P[c][i * kSilMaxM + j];
+      re += tii * pii.y;
+      im -= tii * pii.x;
+      if (i > 0) {
+        const double tl = sc * bt[c][i - 1];
+        const double2 p = ks.P[c][(i - 1) * kSilMaxM + j];
+        re += tl * p.y;
+        im -= tl * p.x;
+      }
+      if (i + 1 < m) {
+        const double tu = sc * bt[c][i];
+        const double2 p = ks.P[c][(i + 1) * kSilMaxM + j];
+        re += tu * p.y;
+        im -= tu * p.x;
+      }
+      ks.Q[c][i * kSilMaxM + j] = make_double2((i == j ? 1.0 : 0.0) + re * rk, im * rk);
+    }
+    __syncthreads();
+    for (int e = t; e < 2 * kMM; e += blockDim.x) {
+      const int c = e / kMM;
+      ks.P[c][e % kMM] = ks.Q[c][e % kMM];
+    }
+    __syncthreads();
+  }
+  // squaring
+  const int nsq = max(s_sq[0], s_sq[1]) + (quirk ? 1 : 0);
+  for (int q = 0; q < nsq; ++q) {
+    for (int e = t; e < 2 * kMM; e += blockDim.x) {
+      const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
+      if (i >= m || j >= m) continue;
+      // the extra squaring of the defect form (Z^2) is kept in Q of chain 0
+      const bool do_sq = q < s_sq[c];
+      const bool do_z2 = quirk && c == 0 && q == s_sq[0];
+      if (!do_sq && !do_z2) continue;
+      double re = 0.0, im = 0.0;
+      for (int l = 0; l < m; ++l) {
+        const double2 x = ks.P[c][i * kSilMaxM + l], z = ks.P[c][l * kSilMaxM + j];
+        re += x.x * z.x - x.y * z.y;
+        im += x.x * z.y + x.y * z.x;
+      }
+      ks.Q[c][i * kSilMaxM + j] = make_double2(re, im);
+    }
+    __syncthreads();
+    for (int e = t; e < 2 * kMM; e += blockDim.x) {
+      const int c = e / kMM;
+      if (q < s_sq[c]) ks.P[c][e % kMM] = ks.Q[c][e % kMM];
+    }
+    __syncthreads();
+  }
+  // coefficients
+  if (t < 2 * kSilMaxM) {
+    const int c = t / kSilMaxM, i = t % kSilMaxM;
+    if (i < m) {
+      double re = 0.0, im = 0.0, im2 = 0.0;
+      if (active[c]) {
+        for (int j = 0; j < m; ++j) {
+          const double2 z = ks.P[c][i * kSilMaxM + j];
+          re += z.x * y[c][j];
+          im += z.y * y[c][j];
+          if (quirk && c == 0) im2 += ks.Q[0][i * kSilMaxM + j].y * y[c][j];
+        }
+      }
+      if (c == 0) {
+        out[0][i] = re;
+        out[1][i] = quirk ? 0.5 * im2 : im;
+      } else {
+        out[2][i] = re;
+        out[3][i] = -im;
+      }
+    }
+  }
+  __syncthreads();
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
+  __shared__ double sp[kSilNQ], st[kSilNQ], scratch[(kSilThreads / 32) * 8];
+  __shared__ int s_flag[2];
+  __shared__ double s_al[2][kSilMaxM], s_bt[2][kSilMaxM], s_proj[2][kSilMaxM];
+  __shared__ double s_r[2][kSilMaxM], s_coef[4][kSilMaxM];
+  __shared__ double s_bt0[2];
+  __shared__ int s_active[2];
+  __shared__ KrylovSmem ks;
+  const Range r = my_range(a.n);
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const long n = a.n;
+  const int m = a.m;
+
+  for (int s = 0;; ++s) {
+    // ---- norms of u, v and C(s) = <psi0|psi(s)> (pspofft.f:119-120 form)
+    {
+      double q[6] = {0, 0, 0, 0, 0, 0};
+      for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+        const double uk = __ldcg(a.u + k), vk = __ldcg(a.v + k);
+        const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
+        q[0] += uk * uk;
+        q[1] += vk * vk;
+        q[2] += u0k * uk;
+        q[3] += v0k * vk;
+        q[4] += u0k * vk;
+        q[5] += v0k * uk;
+      }
+      block_sum<6>(q, sp, scratch);
+      if (!grid_reduce(a, sp, st, 6, s_flag)) return;
+      if (t == 0 && blockIdx.x == 0 && (s > 0 || a.write_c0))
+        a.c_out[s] = make_double2(st[2] + st[3], st[4] - st[5]);
+      if (s == a.nsteps) break;
+      if (t < 2) {
+        s_bt0[t] = sqrt(st[t]);
+        s_active[t] = st[t] != 0.0;  // lnz.f:88 (BT0.EQ.0: no Lanczos vectors)
+      }
+      __syncthreads();
+    }
+    // ---- m Lanczos iterations of both chains
+    for (int it = 0; it < m; ++it) {
+      for (int c = 0; c < 2; ++c) {
+        const double bt0 = s_bt0[c];
+        const bool act = s_active[c];
+        const double* x = c ? a.v : a.u;
+        const double* src = it == 0 ? x : a.work + c * n;
+        double* Lc = a.L + (long)c * m * n;
+        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+          double vi = 0.0, w = 0.0;
+          if (act) {
+            vi = __ldcg(src + k) / bt0;
+            const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
+            w = apply_h(a, src, k, bt0) - bt0 * vprev;
+          }
+          Lc[(long)it * n + k] = vi;
+          a.wbuf[c * n + k] = w;
+        }
+      }
+      __syncthreads();
+      // dot products of the CTA's points, one quantity per warp:
+      // [al_raw, proj, g_it, d_0..d_{it-1}, g_0..g_{it-1}] per chain
+      const int nqc = 3 + 2 * it, nq = 2 * nqc;
+      for (int qi = warp; qi < nq; qi += kSilThreads / 32) {
+        const int c = qi / nqc, j = qi % nqc;
+        const double* Lc = a.L + (long)c * m * n;
+        const double* vi = Lc + (long)it * n;
+        const double* w = a.wbuf + c * n;
+        const double *pa, *pb;
+        if (j == 0) {
+          pa = vi;
+          pb = w;
+        } else if (j == 1) {
+          pa = vi;
+          pb = c ? a.v : a.u;
+        } else if (j == 2) {
+          pa = vi;
+          pb = vi;
+        } else if (j < 3 + it) {
+          pa = w;
+          pb = Lc + (long)(j - 3) * n;
+        } else {
+          pa = vi;
+          pb = Lc + (long)(j - 3 - it) * n;
+        }
+        double sum = 0.0;
+        for (int k = r.lo + lane; k < r.hi; k += 32) sum += __ldcg(pa + k) * __ldcg(pb + k);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (lane == 0) sp[qi] = sum;
+      }
+      __syncthreads();
+      if (!grid_reduce(a, sp, st, nq, s_flag)) return;
+      if (t < 2) {
+        const int c = t, b0 = c * nqc;
+        const double al = st[b0];
+        s_al[c][it] = al;
+        s_proj[c][it] = st[b0 + 1];
+        // reort.f against the it+1 stored vectors: r_q = <w - al vi, L_q>
+        for (int q = 0; q < it; ++q) s_r[c][q] = st[b0 + 3 + q] - al * st[b0 + 3 + it + q];
+        s_r[c][it] = al - al * st[b0 + 2];
+      }
+      __syncthreads();
+      if (it == m - 1) break;  // the last residual is not needed (BT(M) unused)
+      double nn[2] = {0.0, 0.0};
+      for (int c = 0; c < 2; ++c) {
+        const double al = s_al[c][it];
+        const double* Lc = a.L + (long)c * m * n;
+        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+          double acc = __ldcg(a.wbuf + c * n + k) - al * __ldcg(Lc + (long)it * n + k);
+          for (int q = 0; q <= it; ++q) acc -= s_r[c][q] * __ldcg(Lc + (long)q * n + k);
+          a.work[c * n + k] = acc;
+          nn[c] += acc * acc;
+        }
+      }
+      block_sum<2>(nn, sp, scratch);
+      if (!grid_reduce(a, sp, st, 2, s_flag)) return;
+      if (t < 2) {
+        s_bt[t][it] = sqrt(st[t]);
+        s_bt0[t] = s_bt[t][it];
+      }
+      __syncthreads();
+    }
+    // ---- Krylov exponential and the new state
+    krylov_coeffs(m, a.cst, a.quirk, s_al, s_bt, s_proj, s_active, ks, s_coef);
+    const double* Lu = a.L;
+    const double* Lv = a.L + (long)m * n;
+    for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+      double ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
+      for (int j = 0; j < m; ++j) {
+        const double lu = __ldcg(Lu + (long)j * n + k), lv = __ldcg(Lv + (long)j * n + k);
+        ur += lu * s_coef[0][j];
+        ui += lu * s_coef[1][j];
+        vi += lv * s_coef[2][j];
+        vr += lv * s_coef[3][j];
+      }
+      double un = ur + vr, vn = ui + vi;
+      if (a.mask) {  // sil.f:171-175
+        const double mk = __ldg(a.mask + k);
+        un = mk * un;
+        vn = mk * vn;
+      }
+      a.u[k] = un;
+      a.v[k] = vn;
+    }
+    __syncthreads();
+  }
+}
+
+// <u|H u> + <v|H v> and |u|^2 + |v|^2 (EIGENERG, eigenerg.f:56-66): per-CTA
+// partials, then one CTA sums them in CTA order
+__global__ void __launch_bounds__(kSilThreads) sil_energy_kernel(SilArgs a, double* part) {
+  __shared__ double sp[2], scratch[(kSilThreads / 32) * 8];
+  double q[2] = {0.0, 0.0};
+  for (long k = (long)blockIdx.x * kSilThreads + threadIdx.x; k < a.n;
+       k += (long)gridDim.x * kSilThreads) {
+    const double uk = a.u[k], vk = a.v[k];
+    q[0] += uk * apply_h(a, a.u, (int)k, 1.0) + vk * apply_h(a, a.v, (int)k, 1.0);
+    q[1] += uk * uk + vk * vk;
+  }
+  block_sum<2>(q, sp, scratch);
+  if (threadIdx.x < 2) part[blockIdx.x * 2 + threadIdx.x] = sp[threadIdx.x];
+}
+
+__global__ void sum_parts_kernel(const double* part, int nb, double* out) {
+  if (threadIdx.x < 2) {
+    double s = 0.0;
+    for (int i = 0; i < nb; ++i) s += part[i * 2 + threadIdx.x];
+    out[threadIdx.x] = s;
+  }
+}
+
+}  // namespace espec
+
+// ---------------------------------------------------------------------------
+// grid plan
+// ---------------------------------------------------------------------------
+using namespace espec;
+
+struct espec_grid_plan {
+  int method = ESPEC_SIL, ndim = 1, np[3] = {1, 1, 1};
+  long n = 0;
+  double shm[3] = {0, 0, 0};
+  double dt_fs = 0.0;
+  int m = 0, absorb = 0, quirks = 0;
+  int nblocks = 0;
+  bool loaded = false, has_state = false;
+  double *d_vpot = nullptr, *d_mask = nullptr, *d_u = nullptr, *d_v = nullptr;
+  double *d_u0 = nullptr, *d_v0 = nullptr, *d_L = nullptr, *d_work = nullptr, *d_wbuf = nullptr;
+  double *d_part = nullptr, *d_tot = nullptr, *d_epart = nullptr, *d_eout = nullptr;
+  unsigned* d_bar = nullptr;
+  int* d_err = nullptr;
+  double2* d_c = nullptr;
+  int c_cap = -1;  // nsteps of the C(t) buffer
+};
+
+static void grid_free(espec_grid_plan* p) {
+  void* b[] = {p->d_vpot, p->d_mask, p->d_u, p->d_v, p->d_u0, p->d_v0, p->d_L, p->d_work,
+               p->d_wbuf, p->d_part, p->d_tot, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c};
+  for (void* x : b)
+    if (x) cudaFree(x);
+}
+
+#define GRID_CK(call)                                        \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return set_cuda_error(#call, e_); \
+  } while (0)
+
+static SilArgs sil_args(const espec_grid_plan* p) {
+  SilArgs a{};
+  a.ndim = p->ndim;
+  a.nx = p->np[0];
+  a.ny = p->np[1];
+  a.nz = p->np[2];
+  a.n = p->n;
+  for (int i = 0; i < 3; ++i) a.shm[i] = i < p->ndim ? p->shm[i] : 0.0;
+  // (30 * SHT) with SHT summed over the axes in order (au1d.f, au2di.f)
+  double sht = 0.0;
+  for (int i = 0; i < p->ndim; ++i) sht += p->shm[i];
+  a.sht30 = 30.0 * sht;
+  a.vpot = p->d_vpot;
+  a.mask = p->absorb == ESPEC_ABS_SMOOTHW ? p->d_mask : nullptr;
+  a.u = p->d_u;
+  a.v = p->d_v;
+  a.u0 = p->d_u0;
+  a.v0 = p->d_v0;
+  a.L = p->d_L;
+  a.work = p->d_work;
+  a.wbuf = p->d_wbuf;
+  a.part = p->d_part;
+  a.tot = p->d_tot;
+  a.bar = p->d_bar;
+  a.err = p->d_err;
+  a.c_out = p->d_c;
+  a.m = p->m;
+  a.quirk = (p->quirks & ESPEC_Q_SIL_INPLACE) != 0;
+  a.cst = p->dt_fs / ESPEC_SHFS;
+  return a;
+}
+
+extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, const int* np,
+                                 const double* shm, double dt_fs, int mp, int precision,
+                                 int absorb, int quirks) {
+  if (!out || !np || !shm) return set_error(ESPEC_EINVAL, "null argument");
+  if (method != ESPEC_SIL) return set_error(ESPEC_EINVAL, "grid plans run ESPEC_SIL");
+  if (precision != ESPEC_FP64) return set_error(ESPEC_EINVAL, "the SIL propagator runs in FP64");
+  if (ndim < 1 || ndim > 3) return set_error(ESPEC_EINVAL, "ndim must be 1, 2 or 3");
+  if (mp < 1 || mp > kSilMaxM) return set_error(ESPEC_EINVAL, "Lanczos order must be 1..16");
+  if (absorb == ESPEC_ABS_VOPTIC)
+    return set_error(ESPEC_EINVAL, "SIL takes no complex absorbing potential (real Lanczos)");
+  if (absorb != ESPEC_ABS_NONE && absorb != ESPEC_ABS_SMOOTHW)
+    return set_error(ESPEC_EINVAL, "unknown absorber type");
+  if (quirks & ~ESPEC_Q_SIL_INPLACE)
+    return set_error(ESPEC_EINVAL, "only ESPEC_Q_SIL_INPLACE applies to SIL");
+  long n = 1;
+  for (int i = 0; i < ndim; ++i) {
+    if (np[i] < 1) return set_error(ESPEC_EINVAL, "grid size must be positive");
+    n *= np[i];
+  }
+  if (n > (1L << 30)) return set_error(ESPEC_EINVAL, "grid too large");
+  auto* p = new espec_grid_plan;
+  p->method = method;
+  p->ndim = ndim;
+  for (int i = 0; i < ndim; ++i) {
+    p->np[i] = np[i];
+    p->shm[i] = shm[i];
+  }
+  p->n = n;
+  p->dt_fs = dt_fs;
+  p->m = mp;
+  p->absorb = absorb;
+  p->quirks = quirks;
+  // co-resident CTAs for the cooperative launch
+  int dev = 0, nsm = 0, occ = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sil_kernel, kSilThreads, 0);
+  if (e != cudaSuccess) {
+    delete p;
+    return set_cuda_error("device query", e);
+  }
+  long want = (n + kSilThreads - 1) / kSilThreads;
+  if (want > (long)nsm * occ) want = (long)nsm * occ;
+  if (want > nsm) want = nsm;  // one CTA per SM keeps the barriers short
+  p->nblocks = (int)(want > 0 ? want : 1);
+  auto fail = [&](int rc) {
+    grid_free(p);
+    delete p;
+    return rc;
+  };
+  int rc = 0;
+  const size_t nb = (size_t)n * 8;
+  double** bufs8[] = {&p->d_vpot, &p->d_mask, &p->d_u, &p->d_v, &p->d_u0, &p->d_v0};
+  for (double** b : bufs8)
+    if ((rc = ck(cudaMalloc(b, nb), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_L, nb * 2 * mp), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_work, nb * 2), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_wbuf, nb * 2), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_part, sizeof(double) * kSilNQ * p->nblocks), "cudaMalloc")))
+    return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_tot, sizeof(double) * kSilNQ), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_epart, sizeof(double) * 2 * 1024), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_eout, sizeof(double) * 2), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_bar, sizeof(unsigned) * 2), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_err, sizeof(int)), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMemset(p->d_bar, 0, sizeof(unsigned) * 2), "cudaMemset"))) return fail(rc);
+  if ((rc = ck(cudaMemset(p->d_err, 0, sizeof(int)), "cudaMemset"))) return fail(rc);
+  *out = p;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_load(espec_grid_plan* p, const double* vpot, const double* vabc,
+                               const double* psi_re, const double* psi_im, int where,
+                               void* stream) {
+  if (!p || !vpot || !psi_re) return set_error(ESPEC_EINVAL, "null argument");
+  if (p->absorb == ESPEC_ABS_SMOOTHW && !vabc) return set_error(ESPEC_EINVAL, "mask missing");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const size_t nb = (size_t)p->n * 8;
+  GRID_CK(cudaMemcpyAsync(p->d_vpot, vpot, nb, kind, st));
+  if (p->absorb == ESPEC_ABS_SMOOTHW) GRID_CK(cudaMemcpyAsync(p->d_mask, vabc, nb, kind, st));
+  GRID_CK(cudaMemcpyAsync(p->d_u0, psi_re, nb, kind, st));
+  if (psi_im) {
+    GRID_CK(cudaMemcpyAsync(p->d_v0, psi_im, nb, kind, st));
+  } else {
+    GRID_CK(cudaMemsetAsync(p->d_v0, 0, nb, st));
+  }
+  GRID_CK(cudaMemcpyAsync(p->d_u, p->d_u0, nb, cudaMemcpyDeviceToDevice, st));
+  GRID_CK(cudaMemcpyAsync(p->d_v, p->d_v0, nb, cudaMemcpyDeviceToDevice, st));
+  p->loaded = true;
+  return ESPEC_OK;
+}
+
+static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStream_t st) {
+  if (p->c_cap != nsteps) {
+    if (p->d_c) cudaFree(p->d_c);
+    p->d_c = nullptr;
+    GRID_CK(cudaMalloc(&p->d_c, sizeof(double2) * ((size_t)nsteps + 1)));
+    p->c_cap = nsteps;
+  }
+  const size_t nb = (size_t)p->n * 8;
+  if (from_start) {
+    GRID_CK(cudaMemcpyAsync(p->d_u, p->d_u0, nb, cudaMemcpyDeviceToDevice, st));
+    GRID_CK(cudaMemcpyAsync(p->d_v, p->d_v0, nb, cudaMemcpyDeviceToDevice, st));
+  }
+  GRID_CK(cudaMemsetAsync(p->d_bar, 0, sizeof(unsigned) * 2, st));
+  GRID_CK(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
+  SilArgs a = sil_args(p);
+  a.nsteps = nsteps;
+  a.write_c0 = from_start ? 1 : 0;
+  void* args[] = {&a};
+  GRID_CK(cudaLaunchCooperativeKernel((const void*)sil_kernel, dim3(p->nblocks), dim3(kSilThreads),
+                                      args, 0, st));
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_run(espec_grid_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_grid_load has not been called");
+  return grid_launch(p, nsteps, true, (cudaStream_t)stream);
+}
+
+extern "C" int espec_grid_continue(espec_grid_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_grid_load has not been called");
+  return grid_launch(p, nsteps, false, (cudaStream_t)stream);
+}
+
+extern "C" int espec_grid_results(espec_grid_plan* p, double* c_re, double* c_im, double* psi_re,
+                                  double* psi_im, int where, void* stream) {
+  if (!p || p->c_cap < 0) return set_error(ESPEC_EINVAL, "no results: run the plan first");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t nc = (size_t)p->c_cap + 1;
+  if (c_re) GRID_CK(cudaMemcpy2DAsync(c_re, 8, p->d_c, 16, 8, nc, kind, st));
+  if (c_im) GRID_CK(cudaMemcpy2DAsync(c_im, 8, (char*)p->d_c + 8, 16, 8, nc, kind, st));
+  const size_t nb = (size_t)p->n * 8;
+  if (psi_re) GRID_CK(cudaMemcpyAsync(psi_re, p->d_u, nb, kind, st));
+  if (psi_im) GRID_CK(cudaMemcpyAsync(psi_im, p->d_v, nb, kind, st));
+  int err = 0;
+  GRID_CK(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GRID_CK(cudaStreamSynchronize(st));
+  if (err) return set_error(ESPEC_ECUDA, "a grid barrier of the SIL kernel timed out");
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_energies(espec_grid_plan* p, double* e, double* norm, void* stream) {
+  if (!p || !e || !norm) return set_error(ESPEC_EINVAL, "null argument");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_grid_load has not been called");
+  cudaStream_t st = (cudaStream_t)stream;
+  SilArgs a = sil_args(p);
+  long nbk = (p->n + kSilThreads - 1) / kSilThreads;
+  if (nbk > 1024) nbk = 1024;
+  sil_energy_kernel<<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart);
+  GRID_CK(cudaGetLastError());
+  sum_parts_kernel<<<1, 32, 0, st>>>(p->d_epart, (int)nbk, p->d_eout);
+  GRID_CK(cudaGetLastError());
+  double h[2];
+  GRID_CK(cudaMemcpyAsync(h, p->d_eout, sizeof h, cudaMemcpyDeviceToHost, st));
+  GRID_CK(cudaStreamSynchronize(st));
+  *e = h[0];
+  *norm = h[1];
+  return ESPEC_OK;
+}
+
+extern "C" long espec_grid_npoints(const espec_grid_plan* p) { return p ? p->n : -1; }
+
+extern "C" void espec_grid_destroy(espec_grid_plan* p) {
+  if (!p) return;
+  grid_free(p);
+  delete p;
+}

@@ -1,0 +1,55 @@
+// sil.cuh -- short-iterative-Lanczos propagation (eSPec's .PSIL/.PLNZ:
+// plnz.f:71-151, sil.f:70-181, lnz.f:76-119, reort.f:65-80, au1d.f/au2di.f/
+// au3d.f) on one 1D, 2D or 3D grid, FP64, as ONE cooperative persistent
+// kernel.
+//
+// Per time step the real part u and the imaginary part v are propagated by
+// two independent m-step Lanczos chains (run side by side, sharing every
+// grid barrier):
+//   vi = work/bt0 ; w = H vi - bt0 v_prev ; al = <vi,w> ;
+//   work = w - al vi - sum_q <w - al vi, L_q> L_q   (classical Gram-Schmidt
+//   against all stored vectors) ; bt = |work|
+// with H the 4th-order finite-difference Hamiltonian.  The two dot-product
+// rounds of an iteration are merged into one (<w - al vi, L_q> = <w,L_q> -
+// al <vi,L_q>), so an iteration costs two grid barriers.  Each barrier is
+// also the reduction: the last CTA to arrive sums the per-CTA partials in a
+// fixed order (deterministic) and publishes the totals.
+//
+// The Krylov exponential e^{-i cst T} of the m x m tridiagonal T is formed by
+// every CTA (same inputs, same result) by Taylor series with scaling and
+// squaring in FP64 -- the same matrix function the reference forms through
+// the eigenvectors of T (DSTEVX) -- and the new state is the combination of
+// the stored Lanczos vectors.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace espec {
+
+constexpr int kSilMaxM = 16;      // Lanczos order limit
+constexpr int kSilThreads = 256;  // threads per CTA
+constexpr int kSilNQ = 80;        // partial sums per CTA and barrier (>= 2 (3 + 2 (m-1)))
+
+struct SilArgs {
+  int ndim, nx, ny, nz;
+  long n;
+  double shm[3];  // 1/(24 m_a h_a^2) per axis
+  double sht30;   // 30 * (shm[0] + shm[1] + shm[2])
+  const double* vpot;
+  const double* mask;  // .SMOOTHW mask or null
+  double* u;           // state (in / out)
+  double* v;
+  const double* u0;  // psi(0) for C(t)
+  const double* v0;
+  double* L;     // [2][m][n] Lanczos vectors of the u and v chains
+  double* work;  // [2][n]
+  double* wbuf;  // [2][n]
+  double* part;  // [gridDim.x][kSilNQ]
+  double* tot;   // [kSilNQ]
+  unsigned* bar;  // [0] arrivals, [1] generation
+  int* err;       // set when a barrier wait gave up
+  double2* c_out;  // C(t) of every step: slot s for step s (slot 0 only if write_c0)
+  int m, nsteps, quirk, write_c0;
+  double cst;  // dt in atomic units
+};
+
+}  // namespace espec

@@ -1,0 +1,78 @@
+"""Host-side mirror of eSPec's short-iterative-Lanczos propagator on one grid.
+
+`SilGrid` propagates one packet on a 1D, 2D or 3D grid with the method of
+PLNZ/PLNZAUX (plnz.f:71-151, sil.f:70-181): per step two Lanczos chains of
+order mp with full reorthogonalisation (lnz.f, reort.f), the finite-difference
+Hamiltonian of au1d.f/au2di.f/au3d.f and the Krylov exponential, FP64, on the
+GPU.  Arrays are flattened x fastest (the reference's column-major U(N)).
+Units: dt in fs, shm = 1/(24 m h^2) per axis (espec.f:819), V in hartree.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class SilGrid:
+    def __init__(self, np_, shm, dt_fs, mp, absorb=N.ABS_NONE, quirks=0):
+        lib = N.load()
+        self.np = [int(x) for x in np_]
+        self.ndim = len(self.np)
+        self.n = int(np.prod(self.np))
+        npa = np.array(self.np + [1] * (3 - self.ndim), dtype=np.int32)
+        shma = N.f64(list(shm) + [0.0] * (3 - self.ndim))
+        self._h = C.c_void_p()
+        rc = lib.espec_grid_create(C.byref(self._h), N.SIL, self.ndim,
+                                   npa.ctypes.data_as(C.POINTER(C.c_int)),
+                                   shma.ctypes.data_as(C.POINTER(C.c_double)), float(dt_fs),
+                                   int(mp), N.FP64, absorb, quirks)
+        N.check(rc, "espec_grid_create")
+        self.nsteps = None
+
+    def load(self, vpot, psi, vabc=None, stream=None):
+        psi = np.asarray(psi)
+        self._keep = [N.f64(np.ravel(vpot, order="F") if np.ndim(vpot) > 1 else vpot),
+                      N.f64(np.real(psi).ravel(order="F") if psi.ndim > 1 else np.real(psi)),
+                      N.f64(np.imag(psi).ravel(order="F") if psi.ndim > 1 else np.imag(psi)),
+                      None if vabc is None else N.f64(np.ravel(vabc, order="F"))]
+        v, re, im, ab = self._keep
+        rc = N.load().espec_grid_load(self._h, N.ptr(v), N.ptr(ab), N.ptr(re), N.ptr(im),
+                                      N.MEM_HOST, stream)
+        N.check(rc, "espec_grid_load")
+
+    def run(self, nsteps, stream=None):
+        N.check(N.load().espec_grid_run(self._h, int(nsteps), stream), "espec_grid_run")
+        self.nsteps = int(nsteps)
+
+    def advance(self, nsteps, stream=None):
+        N.check(N.load().espec_grid_continue(self._h, int(nsteps), stream), "espec_grid_continue")
+        self.nsteps = int(nsteps)
+
+    def results(self, stream=None):
+        """(C(t) complex [nsteps+1], psi complex [n] flattened x fastest)."""
+        ns = self.nsteps
+        cr, ci = np.zeros(ns + 1), np.zeros(ns + 1)
+        pr, pi = np.zeros(self.n), np.zeros(self.n)
+        rc = N.load().espec_grid_results(self._h, N.ptr(cr), N.ptr(ci), N.ptr(pr), N.ptr(pi),
+                                         N.MEM_HOST, stream)
+        N.check(rc, "espec_grid_results")
+        return cr + 1j * ci, pr + 1j * pi
+
+    def energies(self, stream=None):
+        """(<u|H u> + <v|H v>, |u|^2 + |v|^2) of the current state (eigenerg.f)."""
+        e, nr = C.c_double(), C.c_double()
+        N.check(N.load().espec_grid_energies(self._h, C.byref(e), C.byref(nr), stream),
+                "espec_grid_energies")
+        return e.value, nr.value
+
+    def close(self):
+        if self._h:
+            N.load().espec_grid_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

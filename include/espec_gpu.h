@@ -42,10 +42,12 @@ extern "C" {
 /* propagation methods */
 #define ESPEC_SPO 0         /* split operator, FFT kinetic term (.PFSPO)     */
 #define ESPEC_SOD 1         /* second-order differences, FFT kinetic (.PFSOD) */
+#define ESPEC_SIL 2         /* short-iterative Lanczos, FD Hamiltonian (.PSIL) */
 
 /* reproduce reference defects on request (FP64 form only) */
 #define ESPEC_Q_SPO_INPLACE 1   /* spofft.f:150-153 kinetic multiply            */
 #define ESPEC_Q_SOD_SMOOTHW 2   /* sodfft.f:108 never applies the .SMOOTHW mask */
+#define ESPEC_Q_SIL_INPLACE 4   /* sil.f:145-148 sin term uses the cos-scaled U   */
 
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
@@ -170,6 +172,43 @@ int espec_spo_run_static(int npk, const int* npts, const double* sh,
                          const double* sm, double dt_fs, int precision,
                          const double* vpot, const double* psi0, int nsteps,
                          double* c_out, double* psi_out, void* stream);
+
+/* ----------------------------------------------------------------------
+ * Grid plans: one wave packet on a 1D, 2D or 3D grid (x fastest, the
+ * reference's column-major U(N) layout).
+ *
+ * ESPEC_SIL replaces the time loop of PLNZ (plnz.f:71-151) with PLNZAUX
+ * (sil.f:70-181), LNZ (lnz.f:76-119), REORT (reort.f:65-80) and AU
+ * (au1d.f, au2di.f, au3d.f): per step two m-step Lanczos chains (real and
+ * imaginary part) with full classical Gram-Schmidt reorthogonalisation, the
+ * Krylov exponential of the tridiagonal matrix, FP64.  np: points per axis;
+ * shm: 1/(24 m_a h_a^2) per axis (espec.f:819); mp: Lanczos order 1..16
+ * (already clamped as lnz.f:64-72 does); absorb: ESPEC_ABS_NONE or
+ * ESPEC_ABS_SMOOTHW (mask applied after each step, sil.f:171-175); quirks:
+ * ESPEC_Q_SIL_INPLACE.  One cooperative launch per run; C(t) = <psi0|psi(t)>
+ * every step (nsteps+1 samples).
+ * ---------------------------------------------------------------------- */
+typedef struct espec_grid_plan espec_grid_plan;
+
+int espec_grid_create(espec_grid_plan** plan, int method, int ndim, const int* np,
+                      const double* shm, double dt_fs, int mp, int precision,
+                      int absorb, int quirks);
+/* psi_im may be NULL; vabc: the .SMOOTHW mask (ignored otherwise) */
+int espec_grid_load(espec_grid_plan* plan, const double* vpot, const double* vabc,
+                    const double* psi_re, const double* psi_im, int where,
+                    void* stream);
+int espec_grid_run(espec_grid_plan* plan, int nsteps, void* stream);
+/* nsteps more steps from the current state; sample 0 is not written */
+int espec_grid_continue(espec_grid_plan* plan, int nsteps, void* stream);
+/* synchronises; fails with ESPEC_ECUDA if a grid barrier of the kernel
+ * gave up waiting */
+int espec_grid_results(espec_grid_plan* plan, double* c_re, double* c_im,
+                       double* psi_re, double* psi_im, int where, void* stream);
+/* EIGENERG (eigenerg.f:56-66): <u|H_FD u> + <v|H_FD v>, and |u|^2 + |v|^2,
+ * of the current state */
+int espec_grid_energies(espec_grid_plan* plan, double* e, double* norm, void* stream);
+long espec_grid_npoints(const espec_grid_plan* plan);
+void espec_grid_destroy(espec_grid_plan* plan);
 
 #ifdef __cplusplus
 }
