@@ -31,6 +31,7 @@ EXPORTS = [
     "espec_format_crl_row", "pspofft_", "psodfft_",
     "espec_grid_create", "espec_grid_load", "espec_grid_run", "espec_grid_continue",
     "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
+    "espec_grid_basis", "plnz_",
 ]
 
 
@@ -87,6 +88,9 @@ def load():
     lib.espec_grid_energies.argtypes = [vp, vp, vp, vp]
     lib.espec_grid_npoints.argtypes = [vp]
     lib.espec_grid_npoints.restype = C.c_long
+    lib.espec_grid_basis.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp]
+    lib.plnz_.argtypes = [vp] * 33 + [C.c_size_t] * 3
+    lib.plnz_.restype = None
     lib.espec_grid_destroy.argtypes = [vp]
     lib.espec_grid_destroy.restype = None
     lib.espec_spo_destroy.argtypes = [vp]

@@ -1,5 +1,6 @@
-// dropin.cu -- Fortran-callable drop-ins for eSPec's FFT propagators
-// PSPOFFT (pspofft.f:1-150) and PSODFFT (psodfft.f:1-211), 1D.
+// dropin.cu -- Fortran-callable drop-ins for eSPec's propagators PSPOFFT
+// (pspofft.f:1-150) and PSODFFT (psodfft.f:1-211), 1D, and PLNZ
+// (plnz.f:1-155), 1D/2D/3D.
 //
 // Each call propagates one packet on the GPU through a one-packet plan and
 // leaves in the caller's arrays what the reference routine leaves there:
@@ -13,14 +14,17 @@
 //
 // The arithmetic is the reference's, defects included: the in-place kinetic
 // multiply of spofft.f:150-153 and the never-applied .SMOOTHW mask of
-// sodfft.f:108.  Cases the GPU path does not cover (DIM other than '.1D',
-// packet sizes other than 256..4096 of the form 2^k or 3*2^k) set INFO = -1
-// and write the reason to standard error; nothing is computed on the CPU.
+// sodfft.f:108, and PLNZ's cos-before-sin of sil.f:145-148.  Cases the GPU
+// path does not cover (FFT propagators: DIM other than '.1D', packet sizes
+// other than 256..4096 of the form 2^k or 3*2^k; PLNZ: order above 16) and
+// device errors set INFO = 2 and write the reason to standard error; nothing
+// is computed on the CPU.
 #include <cuda_runtime.h>
 
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -112,24 +116,44 @@ void emit(const std::string& s) {
   std::fwrite(s.data(), 1, s.size(), stdout);
 }
 
+// the table head of plnz.f:96-101: FORMAT 1011 of plnz.f:153
+const char* kSilHead =
+    " \n"
+    " Partial auto-correlation function:\n"
+    " ==================================\n"
+    "\n"
+    "          *t*       *Energy*        *Cr(t)*       *Ci(t)*    *|C(t)|^2*      *|C|*\n";
+
+enum Kind { kSpo, kSod, kSil };
+
+// One packet's propagation through a GPU plan: the segment, C(t) and energy
+// calls of the plan type behind it.
+struct Backend {
+  std::function<int(int)> run;   // k steps from psi0, C(0) written
+  std::function<int(int)> cont;  // k more steps from the current state
+  std::function<int(int, double*, double*)> cvals;  // C samples 0..k of the last call
+  std::function<int(double&, double&)> energy;     // E, sum |psi|^2 of the current state
+};
+
 struct DropIn {
   const char* name;
-  int method;
+  Kind kind;
   // Fortran scalars
   bool absorb;
   int prt;  // 0 none, 1 '.PARTIAL', 2 '.YES'
   int lc, mpr, mpi, mxdct, n;
   double dt, ti, tf, tol;
   double* lnzvc;
-  espec_spo_plan* plan = nullptr;
+  Backend be;
   double e0 = 0, f0 = 0;
   int* info;
+  // text the reference prints inside step s (LNZ's order messages); "" if none
+  std::function<std::string(int)> step_text;
 
-  ~DropIn() { espec_spo_destroy(plan); }
-
+  // INFO = 2: a case the GPU path does not run, or a device error
   int fail(const char* why) {
     std::fprintf(stderr, "espec_gpu %s: %s\n", name, why);
-    *info = -1;
+    *info = 2;
     return -1;
   }
   int fail_lib() { return fail(espec_last_error()); }
@@ -141,19 +165,26 @@ struct DropIn {
     lnzvc[nc + (long)(mpi - 1) * mxdct] = ci;
   }
   bool printed(int s) const { return prt == 2 || (prt == 1 && s % lc == 0); }
+  // E and the printed norm: sqrt(FNR^2 + FNI^2) with FNI = 0 for the FFT
+  // propagators (pspofft.f:96-98), FNR itself for PLNZ (plnz.f:91)
   int energies(double& e, double& fnt) {
     double nr;
-    if (espec_prop_energies(plan, &e, &nr, nullptr)) return fail_lib();
-    fnt = std::sqrt(nr * nr);  // FNI = FCORREL(U,V) - FCORREL(V,U) = 0
+    if (be.energy(e, nr)) return fail_lib();
+    fnt = kind == kSil ? nr : std::sqrt(nr * nr);
     return 0;
   }
-  // INFO drift test; the norm enters with an absorber in PSPOFFT
-  // (pspofft.f:137-142) and without one in PSODFFT (psodfft.f:178-183)
+  // INFO drift test: PSPOFFT tests the norm only with an absorber
+  // (pspofft.f:137-142), PSODFFT only without one (psodfft.f:178-183), PLNZ
+  // always (plnz.f:137-138)
   void drift(double et, double fnt) {
     const bool de = std::fabs((et - e0) / e0) * 1.0e2 > tol;
     const bool dn = std::fabs((fnt - f0) / f0) * 1.0e2 > tol;
-    const bool norm_counts = (method == ESPEC_SPO) == absorb;
+    const bool norm_counts = kind == kSil || (kind == kSpo) == absorb;
     if (de || (norm_counts && dn)) *info = 1;
+  }
+  std::string row(double t, double e, double cr, double ci, double fnt) const {
+    const double ct = kind == kSil ? cr * cr + ci * ci : std::sqrt(cr * cr + ci * ci);
+    return crl_row(t, e, cr, ci, ct, fnt);
   }
 
   // Steps 0..nsteps; t_of(s) gives the printed time of step s, checked(s)
@@ -166,35 +197,30 @@ struct DropIn {
     if (stops.empty() || stops.back() != nsteps) stops.push_back(nsteps);
     std::vector<double> cre, cim;
     int done = 0;
-    auto pull = [&](int k) -> int {  // C samples 0..k of the last segment
-      cre.resize(k + 1);
-      cim.resize(k + 1);
-      if (espec_spo_results(plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST, nullptr))
-        return fail_lib();
-      return 0;
-    };
     for (size_t si = 0; si < stops.size(); ++si) {
       const int stop = stops[si], k = stop - done;
+      cre.resize(k + 1);
+      cim.resize(k + 1);
       if (si == 0) {  // from psi0: writes C(0) as well
-        if (espec_spo_run(plan, k, nullptr)) return fail_lib();
-        if (pull(k)) return -1;
+        if (be.run(k) || be.cvals(k, cre.data(), cim.data())) return fail_lib();
         store_c(0, cre[0], cim[0]);
         if (prt) {
-          emit(kCrlHead);
-          emit(crl_row(ti, e0, cre[0], cim[0], std::sqrt(cre[0] * cre[0] + cim[0] * cim[0]), f0));
+          emit(kind == kSil ? kSilHead : kCrlHead);
+          emit(row(ti, e0, cre[0], cim[0], f0));
         }
       } else {
-        if (espec_prop_continue(plan, k, nullptr)) return fail_lib();
-        if (pull(k)) return -1;
+        if (be.cont(k) || be.cvals(k, cre.data(), cim.data())) return fail_lib();
       }
-      for (int j = 1; j <= k; ++j) store_c(done + j, cre[j], cim[j]);
+      for (int j = 1; j <= k; ++j) {
+        store_c(done + j, cre[j], cim[j]);
+        if (step_text) emit(step_text(done + j));
+      }
       done = stop;
       if (k > 0 && printed(stop)) {
         double et, fnt;
         if (energies(et, fnt)) return -1;
-        const double cr = cre[k], ci = cim[k];
         if (checked(stop)) drift(et, fnt);
-        emit(crl_row(t_of(stop), et, cr, ci, std::sqrt(cr * cr + ci * ci), fnt));
+        emit(row(t_of(stop), et, cre[k], cim[k], fnt));
       }
     }
     return 0;
@@ -202,20 +228,17 @@ struct DropIn {
 };
 
 // absorber of the GPU plan: the prefix tests of spofft.f:65,162 / sodfft.f:66,108
-int absorber(bool absorb, const char* tp, size_t len, int method) {
-  (void)method;  // PSODFFT's mask test never matches: the plan's ESPEC_Q_SOD_SMOOTHW
+int absorber(bool absorb, const char* tp, size_t len) {
   if (!absorb) return ESPEC_ABS_NONE;
   if (fstr_is(tp, len, ".VOPTIC")) return ESPEC_ABS_VOPTIC;
   if (fstr_is(tp, len, ".SMOOTHW")) return ESPEC_ABS_SMOOTHW;
   return ESPEC_ABS_NONE;
 }
 
-int common_setup(DropIn& d, const int* absorb, const char* dim, size_t dim_len, const char* prtcrl,
-                 size_t prtcrl_len, const char* tpabsor, size_t tpabsor_len, const int* lc,
-                 const int* mpi, const int* mpr, const int* mxdct, const int* n, const double* dt,
-                 const double* ti, const double* tf, const double* tol, const int* np,
-                 const double* sh, const double* sm, double* tc, const double* vpot,
-                 const double* vabc, const double* u, const double* v, double* lnzvc) {
+void common_scalars(DropIn& d, const int* absorb, const char* prtcrl, size_t prtcrl_len,
+                    const int* lc, const int* mpi, const int* mpr, const int* mxdct, const int* n,
+                    const double* dt, const double* ti, const double* tf, const double* tol,
+                    double* lnzvc) {
   *d.info = 0;
   d.absorb = *absorb != 0;
   d.prt = fstr_is(prtcrl, prtcrl_len, ".YES") ? 2 : (fstr_is(prtcrl, prtcrl_len, ".PARTIAL") ? 1 : 0);
@@ -229,23 +252,56 @@ int common_setup(DropIn& d, const int* absorb, const char* dim, size_t dim_len, 
   d.tf = *tf;
   d.tol = *tol;
   d.lnzvc = lnzvc;
-  if (!fstr_is(dim, dim_len, ".1D")) return d.fail("only DIM = '.1D' runs on the GPU");
-  if (np[0] != d.n) return d.fail("N differs from NP(1)");
-  if (d.lc < 1) return d.fail("LC must be at least 1");
-  // DIGT (dkeft.f:64-79): the kinetic table is an output of the reference
-  espec::digt_1d(d.n, sh[0], sm[0], tc);
-  const int kind = absorber(d.absorb, tpabsor, tpabsor_len, d.method);
-  const int quirks = d.method == ESPEC_SPO ? ESPEC_Q_SPO_INPLACE : ESPEC_Q_SOD_SMOOTHW;
-  if (espec_prop_create(&d.plan, 1, &d.n, sh, sm, d.dt, d.method, ESPEC_FP64, kind, quirks))
-    return d.fail_lib();
-  if (espec_spo_load(d.plan, vpot, kind == ESPEC_ABS_NONE ? nullptr : vabc, u, v, ESPEC_MEM_HOST,
-                     nullptr))
-    return d.fail_lib();
-  // E0 and the norm of psi0 (the state of a freshly loaded plan)
-  double fnt;
-  if (d.energies(d.e0, fnt)) return -1;
-  d.f0 = fnt;
-  return 0;
+}
+
+// the FFT propagators: one-packet espec_spo_plan
+struct FftDropIn : DropIn {
+  espec_spo_plan* plan = nullptr;
+  ~FftDropIn() { espec_spo_destroy(plan); }
+
+  int setup(int method, const char* dim, size_t dim_len, const char* tpabsor, size_t tpabsor_len,
+            const int* np, const double* sh, const double* sm, double* tc, const double* vpot,
+            const double* vabc, const double* u, const double* v) {
+    if (!fstr_is(dim, dim_len, ".1D")) return fail("only DIM = '.1D' runs on the GPU");
+    if (np[0] != n) return fail("N differs from NP(1)");
+    if (lc < 1) return fail("LC must be at least 1");
+    // DIGT (dkeft.f:64-79): the kinetic table is an output of the reference
+    espec::digt_1d(n, sh[0], sm[0], tc);
+    const int ab = absorber(absorb, tpabsor, tpabsor_len);
+    const int quirks = method == ESPEC_SPO ? ESPEC_Q_SPO_INPLACE : ESPEC_Q_SOD_SMOOTHW;
+    if (espec_prop_create(&plan, 1, &n, sh, sm, dt, method, ESPEC_FP64, ab, quirks))
+      return fail_lib();
+    if (espec_spo_load(plan, vpot, ab == ESPEC_ABS_NONE ? nullptr : vabc, u, v, ESPEC_MEM_HOST,
+                       nullptr))
+      return fail_lib();
+    be.run = [this](int k) { return espec_spo_run(plan, k, nullptr); };
+    be.cont = [this](int k) { return espec_prop_continue(plan, k, nullptr); };
+    be.cvals = [this](int, double* cr, double* ci) {
+      return espec_spo_results(plan, cr, ci, nullptr, nullptr, ESPEC_MEM_HOST, nullptr);
+    };
+    be.energy = [this](double& e, double& nr) {
+      return espec_prop_energies(plan, &e, &nr, nullptr);
+    };
+    // E0 and the norm of psi0 (the state of a freshly loaded plan)
+    double fnt;
+    if (energies(e0, fnt)) return -1;
+    f0 = fnt;
+    return 0;
+  }
+};
+
+// gfortran list-directed text of LNZ's order messages (lnz.f:64-72)
+std::string lnz_order_text(int nreort, int lmtreort, bool change) {
+  char buf[256];
+  std::string s = " Error NREORT > LMTREORT\n";
+  std::snprintf(buf, sizeof buf, " NREORT=%12d   LMTREORT=%12d\n", nreort, lmtreort);
+  s += buf;
+  if (change) {
+    s += " Modifing NREORT to correct value!\n";
+    std::snprintf(buf, sizeof buf, " NREORT=%12d   LMTREORT=%12d\n", lmtreort, lmtreort);
+    s += buf;
+  }
+  return s;
 }
 
 }  // namespace
@@ -260,12 +316,12 @@ extern "C" void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
                          double* wrk2, const double* var, size_t dim_len, size_t prtcrl_len,
                          size_t tpabsor_len) {
   (void)mp; (void)shm; (void)xi; (void)xf; (void)wrk1; (void)wrk2; (void)var;
-  DropIn d;
+  FftDropIn d;
   d.name = "PSPOFFT";
-  d.method = ESPEC_SPO;
+  d.kind = kSpo;
   d.info = info;
-  if (common_setup(d, absorb, dim, dim_len, prtcrl, prtcrl_len, tpabsor, tpabsor_len, lc, mpi, mpr,
-                   mxdct, n, dt, ti, tf, tol, np, sh, sm, tc, vpot, vabc, u1, v1, lnzvc))
+  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  if (d.setup(ESPEC_SPO, dim, dim_len, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u1, v1))
     return;
   // DO T = TI+DT, TF+DT, DT (pspofft.f:110): T accumulates by DT
   const int nsteps = do_count(*ti + *dt, *tf + *dt, *dt);
@@ -290,12 +346,12 @@ extern "C" void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
                          double* wrkr, double* wrki, const double* var, double* lnzvc,
                          size_t dim_len, size_t prtcrl_len, size_t tpabsor_len) {
   (void)mp; (void)shm; (void)xi; (void)xf; (void)wrkr; (void)wrki; (void)var;
-  DropIn d;
+  FftDropIn d;
   d.name = "PSODFFT";
-  d.method = ESPEC_SOD;
+  d.kind = kSod;
   d.info = info;
-  if (common_setup(d, absorb, dim, dim_len, prtcrl, prtcrl_len, tpabsor, tpabsor_len, lc, mpi, mpr,
-                   mxdct, n, dt, ti, tf, tol, np, sh, sm, tc, vpot, vabc, u1, v1, lnzvc))
+  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  if (d.setup(ESPEC_SOD, dim, dim_len, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u1, v1))
     return;
   // start-up step at T = TI+DT (psodfft.f:120-147), then DO T = TI+2*DT,
   // TF+DT, DT (psodfft.f:154); only rows of the loop run the drift test
@@ -314,6 +370,101 @@ extern "C" void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
     d.fail_lib();
     return;
   }
+  std::fflush(stdout);
+}
+
+// PLNZ: one espec_grid_plan (1D, 2D or 3D)
+extern "C" void plnz_(const int* absorb, const int* change, const char* dim, const char* prtcrl,
+                      const char* tpabsor, int* info, const int* lc, const int* lmtreort, int* mp,
+                      const int* mpi, const int* mpr, const int* mxdct, const int* n,
+                      const double* abstol, const double* dt, const double* ti, const double* tf,
+                      const double* tol, const int* np, int* iwork, const double* shm,
+                      const double* vpot, const double* vabc, double* u, double* v,
+                      const double* xi, const double* xf, double* wu, double* wv, double* wp,
+                      double* work, const double* var, double* lnzvc, size_t dim_len,
+                      size_t prtcrl_len, size_t tpabsor_len) {
+  (void)abstol; (void)iwork; (void)xi; (void)xf; (void)wu; (void)wv; (void)wp; (void)work;
+  (void)var;
+  DropIn d;
+  d.name = "PLNZ";
+  d.kind = kSil;
+  d.info = info;
+  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  int ndim = 0;
+  if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
+  if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
+  if (fstr_is(dim, dim_len, ".3D")) ndim = 3;
+  if (!ndim) {
+    d.fail("DIM must be '.1D', '.2D' or '.3D'");
+    return;
+  }
+  long npts = 1;
+  for (int a = 0; a < ndim; ++a) npts *= np[a];
+  if (npts != *n) {
+    d.fail("N differs from the product of NP");
+    return;
+  }
+  if (d.lc < 1) {
+    d.fail("LC must be at least 1");
+    return;
+  }
+  // LNZ's order test (lnz.f:64-72): NREORT and M are both the caller's MP;
+  // with *CHANGE the first call lowers it to LMTREORT for good
+  const int mp_in = *mp;
+  const bool clamp = mp_in > *lmtreort;
+  const int m = clamp && *change ? *lmtreort : mp_in;
+  if (m < 1 || m > 16) {
+    d.fail("the GPU Lanczos order is limited to 1..16");
+    return;
+  }
+  if (clamp) {
+    const bool ch = *change != 0;
+    const int lmt = *lmtreort;
+    d.step_text = [mp_in, lmt, ch](int s) -> std::string {
+      if (ch) return s == 1 ? lnz_order_text(mp_in, lmt, true) : std::string();
+      const std::string one = lnz_order_text(mp_in, lmt, false);
+      return one + one;  // both chains of the step
+    };
+  }
+  // .SMOOTHW mask after each step (sil.f:171); any other absorber is ignored
+  const int ab = d.absorb && fstr_is(tpabsor, tpabsor_len, ".SMOOTHW") ? ESPEC_ABS_SMOOTHW
+                                                                        : ESPEC_ABS_NONE;
+  espec_grid_plan* plan = nullptr;
+  struct Guard {
+    espec_grid_plan*& p;
+    ~Guard() { espec_grid_destroy(p); }
+  } guard{plan};
+  if (espec_grid_create(&plan, ESPEC_SIL, ndim, np, shm, d.dt, m, ESPEC_FP64, ab,
+                        ESPEC_Q_SIL_INPLACE) ||
+      espec_grid_load(plan, vpot, vabc, u, v, ESPEC_MEM_HOST, nullptr)) {
+    d.fail_lib();
+    return;
+  }
+  d.be.run = [&](int k) { return espec_grid_run(plan, k, nullptr); };
+  d.be.cont = [&](int k) { return espec_grid_continue(plan, k, nullptr); };
+  d.be.cvals = [&](int, double* cr, double* ci) {
+    return espec_grid_results(plan, cr, ci, nullptr, nullptr, ESPEC_MEM_HOST, nullptr);
+  };
+  d.be.energy = [&](double& e, double& nr) { return espec_grid_energies(plan, &e, &nr, nullptr); };
+  double fnt;
+  if (d.energies(d.e0, fnt)) return;
+  d.f0 = fnt;
+  // DO T = TI+DT, TF+DT, DT (plnz.f:104)
+  const int nsteps = do_count(*ti + *dt, *tf + *dt, *dt);
+  std::vector<double> tt(nsteps + 1, *ti);
+  if (nsteps >= 1) tt[1] = *ti + *dt;
+  for (int s = 2; s <= nsteps; ++s) tt[s] = tt[s - 1] + *dt;
+  if (d.propagate(nsteps, [&](int s) { return tt[s]; }, [](int) { return true; })) return;
+  // final energy and drift test (plnz.f:141-149)
+  double et;
+  if (d.energies(et, fnt)) return;
+  d.drift(et, fnt);
+  if (espec_grid_results(plan, nullptr, nullptr, u, v, ESPEC_MEM_HOST, nullptr) ||
+      espec_grid_basis(plan, 1, lnzvc, *mxdct, ESPEC_MEM_HOST, nullptr)) {
+    d.fail_lib();
+    return;
+  }
+  if (clamp && *change) *mp = m;  // MP is modified through LNZ's NREORT argument
   std::fflush(stdout);
 }
 

@@ -673,3 +673,18 @@ extern "C" void espec_grid_destroy(espec_grid_plan* p) {
   grid_free(p);
   delete p;
 }
+
+extern "C" int espec_grid_basis(espec_grid_plan* p, int chain, double* dst, int ld, int where,
+                                void* stream) {
+  if (!p || !dst || chain < 0 || chain > 1) return set_error(ESPEC_EINVAL, "bad argument");
+  if (p->c_cap < 0) return set_error(ESPEC_EINVAL, "no basis: run the plan first");
+  if (ld < p->n) return set_error(ESPEC_EINVAL, "leading dimension below the grid size");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const double* src = p->d_L + (size_t)chain * p->m * p->n;
+  GRID_CK(cudaMemcpy2DAsync(dst, (size_t)ld * 8, src, (size_t)p->n * 8, (size_t)p->n * 8, p->m,
+                            kind, st));
+  if (where == ESPEC_MEM_HOST) GRID_CK(cudaStreamSynchronize(st));
+  return ESPEC_OK;
+}

@@ -5,8 +5,8 @@ Fortran ABI of libespecgpu.so (`pspofft_`, `psodfft_`).
 PSODFFT (psodfft.f:1-3) by name, with the same meaning, and update the same
 arrays in place: U1/V1 (and U2/V2), TC and the LNZVC columns MPR/MPI
 (LNZVC is a Fortran-ordered (MXDCT, ncols) array; MPR/MPI are 1-based).
-They return INFO: 0, 1 for a drift beyond TOL percent, -1 for a case the GPU
-path does not run (the reason goes to standard error).  The partial
+They return INFO: 0, 1 for a drift beyond TOL percent, 2 for a case the GPU
+path does not run or a device error (the reason goes to standard error).  The partial
 auto-correlation table goes to standard output when PRTCRL is '.YES' or
 '.PARTIAL', as the reference prints it.
 """
@@ -73,6 +73,35 @@ def psodfft(*, absorb, dim, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, tf,
         N.ptr(k["dummy"]), N.ptr(k["dummy"]), N.ptr(k["dummy"]), _arr(lnzvc),
         len(k["dim"]), len(k["prtcrl"]), len(k["tpabsor"]))
     return info.value
+
+
+def plnz(*, absorb, change, dim, prtcrl, tpabsor, lc, lmtreort, mp, mpi, mpr, mxdct, n, dt,
+         ti, tf, tol, np_, shm, vpot, vabc, u, v, lnzvc, abstol=1e-6):
+    """PLNZ: short-iterative-Lanczos propagation of U + i V (1D/2D/3D grid,
+    flattened x fastest).  Returns (INFO, MP after the call: LNZ lowers MP to
+    LMTREORT when *CHANGE is on, lnz.f:64-72)."""
+    info = C.c_int(0)
+    mp_c = C.c_int(mp)
+    npa = np.array(list(np_) + [1] * (3 - len(np_)), dtype=np.int32)
+    shma = N.f64(list(shm) + [0.0] * (3 - len(shm)))
+    vp = N.f64(vpot)
+    va = N.f64(vabc) if vabc is not None else np.zeros(n)
+    sc = dict(absorb=C.c_int(1 if absorb else 0), change=C.c_int(1 if change else 0),
+              lc=C.c_int(lc), lmt=C.c_int(lmtreort), mpi=C.c_int(mpi), mpr=C.c_int(mpr),
+              mxdct=C.c_int(mxdct), n=C.c_int(n), abstol=C.c_double(abstol), dt=C.c_double(dt),
+              ti=C.c_double(ti), tf=C.c_double(tf), tol=C.c_double(tol))
+    scratch = np.zeros(max(n, 1))
+    iwork = np.zeros(16, dtype=np.int32)
+    b = {k: v.encode() for k, v in dict(dim=dim, prtcrl=prtcrl, tpabsor=tpabsor).items()}
+    N.load().plnz_(
+        C.byref(sc["absorb"]), C.byref(sc["change"]), b["dim"], b["prtcrl"], b["tpabsor"],
+        C.byref(info), C.byref(sc["lc"]), C.byref(sc["lmt"]), C.byref(mp_c), C.byref(sc["mpi"]),
+        C.byref(sc["mpr"]), C.byref(sc["mxdct"]), C.byref(sc["n"]), C.byref(sc["abstol"]),
+        C.byref(sc["dt"]), C.byref(sc["ti"]), C.byref(sc["tf"]), C.byref(sc["tol"]), N.ptr(npa),
+        N.ptr(iwork), N.ptr(shma), N.ptr(vp), N.ptr(va), _arr(u), _arr(v), N.ptr(scratch),
+        N.ptr(scratch), N.ptr(scratch), N.ptr(scratch), N.ptr(scratch), N.ptr(scratch),
+        N.ptr(scratch), _arr(lnzvc), len(b["dim"]), len(b["prtcrl"]), len(b["tpabsor"]))
+    return info.value, mp_c.value
 
 
 def format_crl_row(t, e, cr, ci, ct, fnt):

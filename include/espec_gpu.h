@@ -58,9 +58,11 @@ extern "C" {
 /* ----------------------------------------------------------------------
  * Fortran-callable drop-ins (1D).  Same arguments, same outputs and the
  * same printed partial auto-correlation table as the reference routines;
- * the defects of the reference's arithmetic are reproduced.  DIM other than
- * '.1D' or an unsupported N sets INFO = -1 (message on standard error).
- * WRK*, SHM, XI, XF, VAR and MP are accepted and not used.
+ * the defects of the reference's arithmetic are reproduced.  A case the GPU
+ * path does not run (PSPOFFT/PSODFFT: DIM other than '.1D' or an unsupported
+ * N; PLNZ: order above 16) or a device error sets INFO = 2 (message on
+ * standard error).  Work arrays, XI, XF, VAR, ABSTOL and IWORK are accepted
+ * and not touched.
  * ---------------------------------------------------------------------- */
 /* replaces SUBROUTINE PSPOFFT (pspofft.f:1-3; called from espec.f:1474) */
 void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
@@ -84,6 +86,18 @@ void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
               double* tc, const double* vpot, const double* vabc,
               double* wrkr, double* wrki, const double* var, double* lnzvc,
               size_t dim_len, size_t prtcrl_len, size_t tpabsor_len);
+/* replaces SUBROUTINE PLNZ (plnz.f:1-4; called from espec.f:1499), 1D/2D/3D;
+ * also leaves the last Lanczos basis in LNZVC(1:N, 1:MP) as LNZ does */
+void plnz_(const int* absorb, const int* change, const char* dim,
+           const char* prtcrl, const char* tpabsor, int* info, const int* lc,
+           const int* lmtreort, int* mp, const int* mpi, const int* mpr,
+           const int* mxdct, const int* n, const double* abstol,
+           const double* dt, const double* ti, const double* tf,
+           const double* tol, const int* np, int* iwork, const double* shm,
+           const double* vpot, const double* vabc, double* u, double* v,
+           const double* xi, const double* xf, double* wu, double* wv,
+           double* wp, double* work, const double* var, double* lnzvc,
+           size_t dim_len, size_t prtcrl_len, size_t tpabsor_len);
 /* one row of the partial auto-correlation table in FORMAT 1021 of
  * pspofft.f:148 (newline included); returns its length */
 int espec_format_crl_row(double t, double e, double cr, double ci, double ct,
@@ -207,6 +221,10 @@ int espec_grid_results(espec_grid_plan* plan, double* c_re, double* c_im,
 /* EIGENERG (eigenerg.f:56-66): <u|H_FD u> + <v|H_FD v>, and |u|^2 + |v|^2,
  * of the current state */
 int espec_grid_energies(espec_grid_plan* plan, double* e, double* norm, void* stream);
+/* Lanczos vectors of the last step's chain (0: real part, 1: imaginary part)
+ * into dst(1:N, 1:MP) with leading dimension ld >= N (column-major) */
+int espec_grid_basis(espec_grid_plan* plan, int chain, double* dst, int ld, int where,
+                     void* stream);
 long espec_grid_npoints(const espec_grid_plan* plan);
 void espec_grid_destroy(espec_grid_plan* plan);
 

@@ -124,6 +124,25 @@ def partial_text(out, first=150, last=50):
 TEXT_CASES = ("morse1d_spo", "morse1d_sod", "morse1d_spo_voptic")
 
 
+def case_sil_order_text(change):
+    """.PSIL with MP = 12 > LMTREORT = 10 (param.f:9) for 8 steps (LC = 2): the
+    printed block from the table head to the end of propagation, with LNZ's
+    order messages (lnz.f:64-72) between the rows, *CHANGE .YES or .NO."""
+    x, psi, v = morse1d_inputs()
+    dt_fs = 0.005 * SHFS
+    deck = DECK.format(title="sil order", dim=".1D", np="1024", mass=fmt(918.0 / AMU),
+                       prop=".PSIL", tf=fmt(8 * dt_fs), dt=fmt(dt_fs), mp="  12", absorb="",
+                       mf=3)
+    deck = deck.replace("*CHANGE\n.YES", "*CHANGE\n" + change)
+    out = run_deck(deck, {"wf_pot.inp": write_1d_file(x, psi, v)})
+    lines = out.splitlines()
+    i = [k for k, l in enumerate(lines) if "Partial auto-correlation function:" in l][0]
+    j = [k for k, l in enumerate(lines) if "Eigenvector propagated." in l][0]
+    name = "morse1d_sil_mp12_" + ("change" if change == ".YES" else "nochange")
+    with open(os.path.join(OUT, name + ".txt"), "w") as f:
+        f.write("\n".join(lines[i - 1:j]) + "\n")
+
+
 def fmt(x):
     return repr(float(x))
 
@@ -325,7 +344,11 @@ def main():
         case_morse1d("morse1d_spo", ".PFSPO", "", {})
         case_morse1d("morse1d_sod", ".PFSOD", "", {})
         case_morse1d("morse1d_spo_voptic", ".PFSPO", VOPTIC, vmeta)
+        case_sil_order_text(".YES")
+        case_sil_order_text(".NO")
         return
+    case_sil_order_text(".YES")
+    case_sil_order_text(".NO")
     cases = {}
     cases["test8"] = case_test8()
     cases["test4"] = case_test4()

@@ -169,7 +169,7 @@ def test_dropin_rejects_what_it_does_not_run(capfd):
                      sh=case["sh"], sm=case["sm"], u1=u1, v1=v1, tc=tc, vpot=case["vpot"],
                      vabc=None, lnzvc=lnzvc)
     _, err = capfd.readouterr()
-    assert info == -1 and "1D" in err
+    assert info == 2 and "1D" in err
     assert np.array_equal(u1, case["psi"]) and not lnzvc.any()
 
 
@@ -223,3 +223,86 @@ def test_continue_and_energies_match_single_run(oracle):
             assert abs(n1[k] - np.sum(np.abs(p) ** 2)) <= 1e-12
         one.close()
         seg.close()
+
+
+# ---------------------------------------------------------------------------
+# PLNZ (plnz.f:1-155)
+# ---------------------------------------------------------------------------
+def call_plnz(case, prtcrl, mp=None, change=True, lc=None, tf=None, tol=None, ncols=14):
+    n = int(np.prod(case["np"]))
+    lc = case["lc"] if lc is None else lc
+    tf = case["tf"] if tf is None else tf
+    mp = case["mp"] if mp is None else mp
+    nsteps = int(round((tf - case["ti"]) / case["dt"])) + 4
+    mxdct = max(n, nsteps // lc + 4)
+    lnzvc = np.zeros((mxdct, ncols), order="F")
+    u = np.array(case["psi"], dtype=np.float64)
+    v = np.zeros(n)
+    dim = {1: ".1D", 2: ".2D", 3: ".3D"}[len(case["np"])]
+    absorb = case["absorb"] != 0
+    info, mp_out = F.plnz(absorb=absorb, change=change, dim=dim, prtcrl=prtcrl,
+                          tpabsor=TPABSOR[case["meta"].get("absorb")], lc=lc, lmtreort=10,
+                          mp=mp, mpi=mp + 2, mpr=mp + 1, mxdct=mxdct, n=n, dt=case["dt"],
+                          ti=case["ti"], tf=tf, tol=case["tol"] if tol is None else tol,
+                          np_=case["np"], shm=case["shm"], vpot=case["vpot"], vabc=case["vabc"],
+                          u=u, v=v, lnzvc=lnzvc)
+    return dict(info=info, mp=mp_out, u=u, v=v, lnzvc=lnzvc, mpr=mp + 1, mpi=mp + 2)
+
+
+@pytest.mark.parametrize("name", ["morse1d_sil", "morse1d_sil_smooth", "morse2d_sil"])
+def test_plnz_matches_oracle_and_executable(oracle, capfd, name):
+    case = G.setup_case(name)
+    capfd.readouterr()
+    got = call_plnz(case, ".PARTIAL")
+    out, err = capfd.readouterr()
+    assert err == ""
+    ref = G.run_oracle(case, case["ref_quirks"], prtcrl=oracle.PRT_PARTIAL)
+    nc, col = ref["nc"], got["lnzvc"]
+    assert np.max(np.abs(col[:nc, got["mpr"] - 1] - ref["c"].real)) <= 1e-10
+    assert np.max(np.abs(col[:nc, got["mpi"] - 1] - ref["c"].imag)) <= 1e-10
+    assert np.max(np.abs(got["u"] - ref["u"])) <= 1e-10
+    assert np.max(np.abs(got["v"] - ref["v"])) <= 1e-10
+    assert got["info"] == ref["info"] and got["mp"] == 10
+    # LNZVC(:, 1:MP) holds the last step's Lanczos basis (imaginary-part chain)
+    n = got["u"].size
+    basis = col[:n, :10]
+    assert np.max(np.abs(basis.T @ basis - np.eye(10))) <= 1e-9
+    assert not col[n:, :10].any()
+    lines = out.split("\n")
+    i = lines.index(" Partial auto-correlation function:")
+    assert lines[i + 3] == ("          *t*       *Energy*        *Cr(t)*       *Ci(t)*    "
+                            "*|C(t)|^2*      *|C|*")
+    rows = np.array([[float(x) for x in l.split()] for l in lines[i + 4:] if len(l.split()) == 6])
+    assert rows.shape == ref["rows"].shape
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(ref["rows"][:, 1]))) - 5)
+    d = np.abs(rows - ref["rows"])
+    assert np.all(d[:, [0, 2, 3, 4, 5]] <= np.array([5e-9, 5e-8, 5e-8, 5e-9, 5e-7]) + 1e-10)
+    assert np.all(d[:, 1] <= 0.5 * e_ulp * 1.001)
+    gold = case["data"]["rows"]
+    dg = np.abs(rows - gold)
+    assert np.all(dg[:, [0, 2, 3, 4, 5]] <= np.array([1e-8, 2e-7, 2e-7, 4e-7, 1e-6]) * 1.01)
+
+
+@pytest.mark.parametrize("change", [True, False])
+def test_plnz_order_messages_match_executable(capfd, change):
+    """MP = 12 > LMTREORT = 10: LNZ's messages between the rows, MP lowered
+    with *CHANGE (the executable's text, tests/golden/morse1d_sil_mp12_*.txt)."""
+    case = G.setup_case("morse1d_sil")
+    tf = 8 * case["dt"]
+    capfd.readouterr()
+    got = call_plnz(case, ".PARTIAL", mp=12, change=change, lc=2, tf=tf)
+    out, err = capfd.readouterr()
+    assert err == "" and got["info"] == 0
+    assert got["mp"] == (10 if change else 12)
+    name = "morse1d_sil_mp12_" + ("change" if change else "nochange")
+    with open(f"{G.GOLDEN}/{name}.txt") as f:
+        want = f.read().split("\n")[:-1]
+    have = out.split("\n")[:-1]
+    assert len(have) == len(want)
+    for h, w in zip(have, want):
+        if len(w.split()) == 6 and w.split()[0][0].isdigit():
+            hv, wv = np.array(h.split(), float), np.array(w.split(), float)
+            assert np.all(np.abs(hv - wv) <= np.array([1e-8, 1e-6 * abs(wv[1]), 1.01e-7,
+                                                       1.01e-7, 1.01e-8, 1.01e-6])), (h, w)
+        else:
+            assert h == w
