@@ -34,10 +34,12 @@ __device__ __forceinline__ Range my_range(long n) {
 // sums; on return st[0..nq) holds the totals over all CTAs, summed by the last
 // CTA to arrive in CTA order (deterministic).  false = a wait gave up.
 __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int nq,
-                            int* s_flag) {
+                            int* s_flag, double* s_red /* kSilThreads doubles */) {
   const int b = blockIdx.x, G = gridDim.x, t = threadIdx.x;
+  // The CTA's writes are ordered before thread 0's release (the acq_rel
+  // arrival) by bar.sync, whose ordering is cumulative; the waiters' acquire
+  // loads order everything after.
   for (int q = t; q < nq; q += blockDim.x) a.part[(long)b * kSilNQ + q] = sp[q];
-  __threadfence();
   __syncthreads();
   if (t == 0) {
     cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(a.bar[0]);
@@ -55,21 +57,38 @@ __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int 
           s_flag[1] = 0;
           break;
         }
-        __nanosleep(64);
+        if (spins > 4096) __nanosleep(32);
       }
     }
   }
   __syncthreads();
   if (!s_flag[1]) return false;
-  __threadfence();
   if (s_flag[0]) {
+    // R threads per quantity, each summing every R-th CTA in CTA order, then
+    // the R partial sums in order: a fixed summation order for a fixed grid
+    double* red = reinterpret_cast<double*>(s_red);
+    const int R = nq > 0 ? min(kSilThreads / nq, 32) : 1;
+    if (t < R * nq) {
+      const int q = t % nq, r = t / nq;
+      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+      int i = r, u = 0;
+      for (; i + 7 * R < G; i += 8 * R) {  // eight loads in flight
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[j] += __ldcg(a.part + (long)(i + j * R) * kSilNQ + q);
+      }
+      for (; i < G; i += R, ++u) acc[u & 7] += __ldcg(a.part + (long)i * kSilNQ + q);
+      double s = 0.0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) s += acc[j];
+      red[r * nq + q] = s;
+    }
+    __syncthreads();
     for (int q = t; q < nq; q += blockDim.x) {
       double s = 0.0;
-      for (int i = 0; i < G; ++i) s += __ldcg(a.part + (long)i * kSilNQ + q);
+      for (int r = 0; r < R; ++r) s += red[r * nq + q];
       st[q] = s;
       a.tot[q] = s;
     }
-    __threadfence();
     __syncthreads();
     if (t == 0) {
       cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(a.bar[0]);
@@ -104,11 +123,11 @@ __device__ __forceinline__ void block_sum(const double (&x)[NV], double* sp, dou
   __syncthreads();
 }
 
-// H_FD x at point k with every x value divided by d (au1d.f:52-73,
+// H_FD x at point k with every x value scaled by d (au1d.f:52-73,
 // au2di.f:57-225, au3d.f:61-117): (30 sum(shm) + V) x_k + sum_a shm_a
 // (x_{-2} - 16 x_{-1} - 16 x_{+1} + x_{+2}), zero outside the grid.
 __device__ __forceinline__ double apply_h(const SilArgs& a, const double* x, int k, double d) {
-  double s = (a.sht30 + __ldg(a.vpot + k)) * (__ldcg(x + k) / d);
+  double s = (a.sht30 + __ldg(a.vpot + k)) * (__ldcg(x + k) * d);
   int idx[3], len[3] = {a.nx, a.ny, a.nz}, str[3];
   idx[0] = k % a.nx;
   str[0] = 1;
@@ -123,25 +142,24 @@ __device__ __forceinline__ double apply_h(const SilArgs& a, const double* x, int
   for (int ax = 0; ax < a.ndim; ++ax) {
     const double h = a.shm[ax];
     const int i = idx[ax], st = str[ax];
-    if (i >= 2) s += h * (__ldcg(x + k - 2 * st) / d);
-    if (i >= 1) s += -16.0 * h * (__ldcg(x + k - st) / d);
-    if (i + 1 < len[ax]) s += -16.0 * h * (__ldcg(x + k + st) / d);
-    if (i + 2 < len[ax]) s += h * (__ldcg(x + k + 2 * st) / d);
+    if (i >= 2) s += h * (__ldcg(x + k - 2 * st) * d);
+    if (i >= 1) s += -16.0 * h * (__ldcg(x + k - st) * d);
+    if (i + 1 < len[ax]) s += -16.0 * h * (__ldcg(x + k + st) * d);
+    if (i + 2 < len[ax]) s += h * (__ldcg(x + k + 2 * st) * d);
   }
   return s;
 }
 
 // Krylov coefficients of both chains (every CTA computes the same values):
 // Z = exp(-i cst T) by Taylor series (degree kTaylor) of T scaled to norm
-// <= 1/4, then squared back.  out[0] = Re Z y_u, out[1] = Im Z y_u (or
+// <= 1/2, then squared back.  out[0] = Re Z y_u, out[1] = Im Z y_u (or
 // Im(Z^2) y_u / 2 in the reference-defect form), out[2] = Re Z y_v,
 // out[3] = -Im Z y_v.
-constexpr int kTaylor = 16;
+constexpr int kTaylor = 14;  // |B| <= 1/2: truncation 0.5^15/15! = 2.3e-17
 constexpr int kMM = kSilMaxM * kSilMaxM;
 
 struct KrylovSmem {
-  double2 P[2][kMM];
-  double2 Q[2][kMM];
+  double2 X[2][2][kMM];  // [buffer][chain], ping-pong
 };
 
 __device__ void krylov_coeffs(int m, double cst, int quirk, const double (*al)[kSilMaxM],
@@ -160,89 +178,83 @@ __device__ void krylov_coeffs(int m, double cst, int quirk, const double (*al)[k
     }
     nrm *= fabs(cst);
     int sq = 0;
-    while (nrm > 0.25 && sq < 60) {
+    while (nrm > 0.5 && sq < 60) {
       nrm *= 0.5;
       ++sq;
     }
     s_sq[t] = sq;
     s_scale[t] = ldexp(cst, -sq);
   }
-  // P = I
+  // buffer 0 = I
   for (int e = t; e < 2 * kMM; e += blockDim.x) {
     const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
-    ks.P[c][i * kSilMaxM + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
+    ks.X[0][c][i * kSilMaxM + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
   }
   __syncthreads();
-  // Horner: P = I + B P / k, B = -i scale T (T tridiagonal)
+  // Horner: P <- I + B P / k, B = -i scale T (T tridiagonal)
+  int cur = 0;
   for (int k = kTaylor; k >= 1; --k) {
     const double rk = 1.0 / k;
     for (int e = t; e < 2 * kMM; e += blockDim.x) {
       const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
       if (i >= m || j >= m) continue;
+      const double2* P = ks.X[cur][c];
       const double sc = s_scale[c];
-      double re = 0.0, im = 0.0;
       // (B P)_{ij} = sum_l (-i sc T_il) P_lj = sum_l sc T_il (Im P_lj, -Re P_lj)
       const double tii = sc * al[c][i];
-      const double2 pii = ks.P[c][i * kSilMaxM + j];
-      re += tii * pii.y;
-      im -= tii * pii.x;
+      const double2 pii = P[i * kSilMaxM + j];
+      double re = tii * pii.y, im = -tii * pii.x;
       if (i > 0) {
         const double tl = sc * bt[c][i - 1];
-        const double2 p = ks.P[c][(i - 1) * kSilMaxM + j];
-        re += tl * p.y;
-        im -= tl * p.x;
+        const double2 q = P[(i - 1) * kSilMaxM + j];
+        re += tl * q.y;
+        im -= tl * q.x;
       }
       if (i + 1 < m) {
         const double tu = sc * bt[c][i];
-        const double2 p = ks.P[c][(i + 1) * kSilMaxM + j];
-        re += tu * p.y;
-        im -= tu * p.x;
+        const double2 q = P[(i + 1) * kSilMaxM + j];
+        re += tu * q.y;
+        im -= tu * q.x;
       }
-      ks.Q[c][i * kSilMaxM + j] = make_double2((i == j ? 1.0 : 0.0) + re * rk, im * rk);
+      ks.X[cur ^ 1][c][i * kSilMaxM + j] = make_double2((i == j ? 1.0 : 0.0) + re * rk, im * rk);
     }
     __syncthreads();
-    for (int e = t; e < 2 * kMM; e += blockDim.x) {
-      const int c = e / kMM;
-      ks.P[c][e % kMM] = ks.Q[c][e % kMM];
-    }
-    __syncthreads();
+    cur ^= 1;
   }
-  // squaring
+  // squaring back; the defect form also needs Z^2 of chain 0
+  int cc[2] = {cur, cur};
   const int nsq = max(s_sq[0], s_sq[1]) + (quirk ? 1 : 0);
   for (int q = 0; q < nsq; ++q) {
     for (int e = t; e < 2 * kMM; e += blockDim.x) {
       const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
       if (i >= m || j >= m) continue;
-      // the extra squaring of the defect form (Z^2) is kept in Q of chain 0
-      const bool do_sq = q < s_sq[c];
-      const bool do_z2 = quirk && c == 0 && q == s_sq[0];
-      if (!do_sq && !do_z2) continue;
+      if (q > s_sq[c] || (q == s_sq[c] && !(quirk && c == 0))) continue;
+      const double2* P = ks.X[cc[c]][c];
       double re = 0.0, im = 0.0;
       for (int l = 0; l < m; ++l) {
-        const double2 x = ks.P[c][i * kSilMaxM + l], z = ks.P[c][l * kSilMaxM + j];
+        const double2 x = P[i * kSilMaxM + l], z = P[l * kSilMaxM + j];
         re += x.x * z.x - x.y * z.y;
         im += x.x * z.y + x.y * z.x;
       }
-      ks.Q[c][i * kSilMaxM + j] = make_double2(re, im);
+      ks.X[cc[c] ^ 1][c][i * kSilMaxM + j] = make_double2(re, im);
     }
     __syncthreads();
-    for (int e = t; e < 2 * kMM; e += blockDim.x) {
-      const int c = e / kMM;
-      if (q < s_sq[c]) ks.P[c][e % kMM] = ks.Q[c][e % kMM];
-    }
-    __syncthreads();
+    for (int c = 0; c < 2; ++c)
+      if (q < s_sq[c]) cc[c] ^= 1;
   }
-  // coefficients
+  // coefficients: Z = X[cc[c]][c]; Z^2 of chain 0 in the other buffer
   if (t < 2 * kSilMaxM) {
     const int c = t / kSilMaxM, i = t % kSilMaxM;
     if (i < m) {
+      const double2* Z = ks.X[cc[c]][c];
+      const double2* Z2 = ks.X[cc[0] ^ 1][0];
       double re = 0.0, im = 0.0, im2 = 0.0;
       if (active[c]) {
         for (int j = 0; j < m; ++j) {
-          const double2 z = ks.P[c][i * kSilMaxM + j];
+          const double2 z = Z[i * kSilMaxM + j];
           re += z.x * y[c][j];
           im += z.y * y[c][j];
-          if (quirk && c == 0) im2 += ks.Q[0][i * kSilMaxM + j].y * y[c][j];
+          if (quirk && c == 0) im2 += Z2[i * kSilMaxM + j].y * y[c][j];
         }
       }
       if (c == 0) {
@@ -259,8 +271,30 @@ __device__ void krylov_coeffs(int m, double cst, int quirk, const double (*al)[k
 
 }  // namespace
 
-__global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
+// per-chain slots of the dot products of one Lanczos iteration:
+// [al_raw, proj, g_it, d_0..d_{it-1}, g_0..g_{it-1}]
+__device__ __forceinline__ int slot_of(int c, int it, int i) { return c * (3 + 2 * it) + i; }
+
+// warp sums of acc[0..3+2it) into ws[warp][slot]
+__device__ __forceinline__ void warp_sums(const double (&acc)[3 + 2 * kSilMaxM], int c, int it,
+                                          double* ws) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) {
+    const bool valid = i < 3 || (i < 3 + kSilMaxM ? i - 3 < it : i - 3 - kSilMaxM < it);
+    if (!valid) continue;  // uniform over the CTA
+    double s = acc[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    const int slot = i < 3 ? i : (i < 3 + kSilMaxM ? i : i - kSilMaxM + it);
+    if (lane == 0) ws[warp * kSilNQ + slot_of(c, it, slot)] = s;
+  }
+}
+
+__global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   __shared__ double sp[kSilNQ], st[kSilNQ], scratch[(kSilThreads / 32) * 8];
+  __shared__ double ws[(kSilThreads / 32) * kSilNQ];
+  __shared__ double s_red[kSilThreads];
   __shared__ int s_flag[2];
   __shared__ double s_al[2][kSilMaxM], s_bt[2][kSilMaxM], s_proj[2][kSilMaxM];
   __shared__ double s_r[2][kSilMaxM], s_coef[4][kSilMaxM];
@@ -268,9 +302,10 @@ __global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
   __shared__ int s_active[2];
   __shared__ KrylovSmem ks;
   const Range r = my_range(a.n);
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int t = threadIdx.x;
   const long n = a.n;
   const int m = a.m;
+  constexpr int NW = kSilThreads / 32;
 
   for (int s = 0;; ++s) {
     // ---- norms of u, v and C(s) = <psi0|psi(s)> (pspofft.f:119-120 form)
@@ -287,7 +322,7 @@ __global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
         q[5] += v0k * uk;
       }
       block_sum<6>(q, sp, scratch);
-      if (!grid_reduce(a, sp, st, 6, s_flag)) return;
+      if (!grid_reduce(a, sp, st, 6, s_flag, s_red)) return;
       if (t == 0 && blockIdx.x == 0 && (s > 0 || a.write_c0))
         a.c_out[s] = make_double2(st[2] + st[3], st[4] - st[5]);
       if (s == a.nsteps) break;
@@ -299,59 +334,59 @@ __global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
     }
     // ---- m Lanczos iterations of both chains
     for (int it = 0; it < m; ++it) {
+      // vi = work/bt0, w = H vi - bt0 v_prev at the CTA's points, and the dot
+      // products of the iteration accumulated per thread
       for (int c = 0; c < 2; ++c) {
         const double bt0 = s_bt0[c];
+        // vi = work * (1/bt0) here and for the stencil's neighbours alike, so
+        // the stencil sees exactly the stored vi
+        const double rb = 1.0 / bt0;
         const bool act = s_active[c];
         const double* x = c ? a.v : a.u;
         const double* src = it == 0 ? x : a.work + c * n;
         double* Lc = a.L + (long)c * m * n;
-        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-          double vi = 0.0, w = 0.0;
-          if (act) {
-            vi = __ldcg(src + k) / bt0;
-            const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
-            w = apply_h(a, src, k, bt0) - bt0 * vprev;
-          }
-          Lc[(long)it * n + k] = vi;
-          a.wbuf[c * n + k] = w;
-        }
-      }
-      __syncthreads();
-      // dot products of the CTA's points, one quantity per warp:
-      // [al_raw, proj, g_it, d_0..d_{it-1}, g_0..g_{it-1}] per chain
-      const int nqc = 3 + 2 * it, nq = 2 * nqc;
-      for (int qi = warp; qi < nq; qi += kSilThreads / 32) {
-        const int c = qi / nqc, j = qi % nqc;
-        const double* Lc = a.L + (long)c * m * n;
-        const double* vi = Lc + (long)it * n;
-        const double* w = a.wbuf + c * n;
-        const double *pa, *pb;
-        if (j == 0) {
-          pa = vi;
-          pb = w;
-        } else if (j == 1) {
-          pa = vi;
-          pb = c ? a.v : a.u;
-        } else if (j == 2) {
-          pa = vi;
-          pb = vi;
-        } else if (j < 3 + it) {
-          pa = w;
-          pb = Lc + (long)(j - 3) * n;
-        } else {
-          pa = vi;
-          pb = Lc + (long)(j - 3 - it) * n;
-        }
-        double sum = 0.0;
-        for (int k = r.lo + lane; k < r.hi; k += 32) sum += __ldcg(pa + k) * __ldcg(pb + k);
+        double acc[3 + 2 * kSilMaxM];
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
-        if (lane == 0) sp[qi] = sum;
+        for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) acc[i] = 0.0;
+        if (act) {
+          for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+            double lq[kSilMaxM];
+#pragma unroll
+            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
+            const double vi = __ldcg(src + k) * rb;
+            const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
+            const double w = apply_h(a, src, k, rb) - bt0 * vprev;
+            const double xk = __ldcg(x + k);
+            Lc[(long)it * n + k] = vi;
+            a.wbuf[c * n + k] = w;
+            acc[0] += vi * w;
+            acc[1] += vi * xk;
+            acc[2] += vi * vi;
+#pragma unroll
+            for (int q = 0; q < kSilMaxM; ++q) {
+              acc[3 + q] += w * lq[q];
+              acc[3 + kSilMaxM + q] += vi * lq[q];
+            }
+          }
+        } else {
+          for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+            Lc[(long)it * n + k] = 0.0;
+            a.wbuf[c * n + k] = 0.0;
+          }
+        }
+        warp_sums(acc, c, it, ws);
       }
       __syncthreads();
-      if (!grid_reduce(a, sp, st, nq, s_flag)) return;
+      const int nq = 2 * (3 + 2 * it);
+      for (int q = t; q < nq; q += kSilThreads) {
+        double sum = 0.0;
+        for (int w = 0; w < NW; ++w) sum += ws[w * kSilNQ + q];
+        sp[q] = sum;
+      }
+      __syncthreads();
+      if (!grid_reduce(a, sp, st, nq, s_flag, s_red)) return;
       if (t < 2) {
-        const int c = t, b0 = c * nqc;
+        const int c = t, b0 = slot_of(c, it, 0);
         const double al = st[b0];
         s_al[c][it] = al;
         s_proj[c][it] = st[b0 + 1];
@@ -366,14 +401,24 @@ __global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
         const double al = s_al[c][it];
         const double* Lc = a.L + (long)c * m * n;
         for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-          double acc = __ldcg(a.wbuf + c * n + k) - al * __ldcg(Lc + (long)it * n + k);
-          for (int q = 0; q <= it; ++q) acc -= s_r[c][q] * __ldcg(Lc + (long)q * n + k);
+          double lq[kSilMaxM + 1];
+#pragma unroll
+          for (int q = 0; q <= kSilMaxM; ++q) lq[q] = q <= it ? __ldcg(Lc + (long)q * n + k) : 0.0;
+          double acc = __ldcg(a.wbuf + c * n + k);
+          double vi = 0.0;
+#pragma unroll
+          for (int q = 0; q <= kSilMaxM; ++q)
+            if (q == it) vi = lq[q];
+          acc -= al * vi;
+#pragma unroll
+          for (int q = 0; q <= kSilMaxM; ++q)
+            if (q <= it) acc -= s_r[c][q] * lq[q];
           a.work[c * n + k] = acc;
           nn[c] += acc * acc;
         }
       }
       block_sum<2>(nn, sp, scratch);
-      if (!grid_reduce(a, sp, st, 2, s_flag)) return;
+      if (!grid_reduce(a, sp, st, 2, s_flag, s_red)) return;
       if (t < 2) {
         s_bt[t][it] = sqrt(st[t]);
         s_bt0[t] = s_bt[t][it];
@@ -385,13 +430,21 @@ __global__ void __launch_bounds__(kSilThreads) sil_kernel(SilArgs a) {
     const double* Lu = a.L;
     const double* Lv = a.L + (long)m * n;
     for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+      double lu[kSilMaxM], lv[kSilMaxM];
+#pragma unroll
+      for (int j = 0; j < kSilMaxM; ++j) {
+        lu[j] = j < m ? __ldcg(Lu + (long)j * n + k) : 0.0;
+        lv[j] = j < m ? __ldcg(Lv + (long)j * n + k) : 0.0;
+      }
       double ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
-      for (int j = 0; j < m; ++j) {
-        const double lu = __ldcg(Lu + (long)j * n + k), lv = __ldcg(Lv + (long)j * n + k);
-        ur += lu * s_coef[0][j];
-        ui += lu * s_coef[1][j];
-        vi += lv * s_coef[2][j];
-        vr += lv * s_coef[3][j];
+#pragma unroll
+      for (int j = 0; j < kSilMaxM; ++j) {
+        if (j < m) {
+          ur += lu[j] * s_coef[0][j];
+          ui += lu[j] * s_coef[1][j];
+          vi += lv[j] * s_coef[2][j];
+          vr += lv[j] * s_coef[3][j];
+        }
       }
       double un = ur + vr, vn = ui + vi;
       if (a.mask) {  // sil.f:171-175
