@@ -17,6 +17,7 @@ ABS_NONE, ABS_VOPTIC, ABS_SMOOTHW = 0, 1, 2
 Q_SPO_INPLACE = 1
 Q_SOD_SMOOTHW = 2
 Q_SIL_INPLACE = 4
+Q_FFTNT_SP = 8
 SPO, SOD, SIL = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 SHFS = 2.4188843243e-2
@@ -31,7 +32,8 @@ EXPORTS = [
     "espec_format_crl_row", "pspofft_", "psodfft_",
     "espec_grid_create", "espec_grid_load", "espec_grid_run", "espec_grid_continue",
     "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
-    "espec_grid_basis", "plnz_",
+    "espec_grid_basis", "plnz_", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
+    "spectrumtd_",
 ]
 
 
@@ -91,6 +93,15 @@ def load():
     lib.espec_grid_basis.argtypes = [vp, C.c_int, vp, C.c_int, C.c_int, vp]
     lib.plnz_.argtypes = [vp] * 33 + [C.c_size_t] * 3
     lib.plnz_.restype = None
+    lib.espec_spectrum_dev.argtypes = [C.c_int, C.c_int, vp, C.c_long, C.c_int, C.c_double,
+                                       C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                       C.c_int, vp, vp, vp]
+    lib.espec_spectrum_work_bytes.argtypes = [C.c_int, C.c_int]
+    lib.espec_spectrum_work_bytes.restype = C.c_size_t
+    lib.hwhm_.argtypes = [vp] * 7
+    lib.hwhm_.restype = None
+    lib.spectrumtd_.argtypes = [vp] * 8 + [C.c_size_t]
+    lib.spectrumtd_.restype = None
     lib.espec_grid_destroy.argtypes = [vp]
     lib.espec_grid_destroy.restype = None
     lib.espec_spo_destroy.argtypes = [vp]

@@ -48,6 +48,7 @@ extern "C" {
 #define ESPEC_Q_SPO_INPLACE 1   /* spofft.f:150-153 kinetic multiply            */
 #define ESPEC_Q_SOD_SMOOTHW 2   /* sodfft.f:108 never applies the .SMOOTHW mask */
 #define ESPEC_Q_SIL_INPLACE 4   /* sil.f:145-148 sin term uses the cos-scaled U   */
+#define ESPEC_Q_FFTNT_SP 8      /* cfft.f:35 TWOPI from a single-precision literal */
 
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
@@ -98,6 +99,15 @@ void plnz_(const int* absorb, const int* change, const char* dim,
            const double* xi, const double* xf, double* wu, double* wv,
            double* wp, double* work, const double* var, double* lnzvc,
            size_t dim_len, size_t prtcrl_len, size_t tpabsor_len);
+/* replace SUBROUTINE HWHM (hwhm.f:1-80; TAL is scaled in place) and
+ * SUBROUTINE SPECTRUMTD (spectrumtd.f:1-116; prints the spectrum table,
+ * sets DE < 0 to 0), called at espec.f:1618-1624: the arithmetic runs on the
+ * GPU (espec_spectrum_dev), FFTNT's single-precision 2 pi included */
+void hwhm_(const int* m, const double* dt, const double* tf, double* tal,
+           const double* de, double* u, double* v);
+void spectrumtd_(const char* tpwind, const int* m, const double* dt,
+                 const double* tf, const double* wp, double* de, double* u,
+                 double* v, size_t tpwind_len);
 /* one row of the partial auto-correlation table in FORMAT 1021 of
  * pspofft.f:148 (newline included); returns its length */
 int espec_format_crl_row(double t, double e, double cr, double ci, double ct,
@@ -227,6 +237,24 @@ int espec_grid_basis(espec_grid_plan* plan, int chain, double* dst, int ld, int 
                      void* stream);
 long espec_grid_npoints(const espec_grid_plan* plan);
 void espec_grid_destroy(espec_grid_plan* plan);
+
+/* ----------------------------------------------------------------------
+ * Spectrum stage on the device, batched over packets (FP64).
+ *
+ * For each of npk packets: the 2^mf-point time signal -- assembled from the
+ * first 2^(mf-1) C(t) samples as espec.f:1545-1576 does (assemble = 1; in =
+ * double2 C(t) with stride ld per packet, e.g. espec_spo_device_c with
+ * ld = nsteps+1) or read as given (assemble = 0, stride ld) -- then HWHM
+ * (hwhm.f:59-77; skipped when tal < 0; de = DE - E1I of espec.f:1618), the
+ * window of SPECTRUMTD (window 1 = .SG with parameter wp, 0 = none), the half
+ * swap and the backward DFT / N of FFTNT (spectrumtd.f:58-81, cfft.f).
+ * spec: device double2 [npk][2^mf] in FFTNT's natural order.  work: device
+ * scratch of espec_spectrum_work_bytes(npk, mf).  quirks: ESPEC_Q_FFTNT_SP.
+ * ---------------------------------------------------------------------- */
+int espec_spectrum_dev(int npk, int mf, const void* in, long ld, int assemble,
+                       double dtf, double tf, double tal, double de, int window,
+                       double wp, int quirks, void* spec, void* work, void* stream);
+size_t espec_spectrum_work_bytes(int npk, int mf);
 
 #ifdef __cplusplus
 }

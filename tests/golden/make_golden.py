@@ -124,6 +124,23 @@ def partial_text(out, first=150, last=50):
 TEXT_CASES = ("morse1d_spo", "morse1d_sod", "morse1d_spo_voptic")
 
 
+def case_test8_text():
+    """Reference test 8 run by the executable: the printed spectrum block
+    (SPECTRUMTD, spectrumtd.f:83-98) -- its head, first 100 and last 20 rows."""
+    tt = os.path.join(REF, "ttests")
+    deck = open(os.path.join(tt, "input.test8")).read()
+    out = run_deck(deck, {"correl8.inp": os.path.join(tt, "correl8.inp")})
+    lines = out.splitlines()
+    i = [k for k, l in enumerate(lines) if l.strip() == "Spectrum:"][0]
+    rows = []
+    for l in lines[i + 3:]:
+        if len(l.split()) != 4:
+            break
+        rows.append(l)
+    with open(os.path.join(OUT, "test8_spectrum.txt"), "w") as f:
+        f.write("\n".join(lines[i - 1:i + 3] + rows[:100] + rows[-20:]) + "\n")
+
+
 def case_sil_order_text(change):
     """.PSIL with MP = 12 > LMTREORT = 10 (param.f:9) for 8 steps (LC = 2): the
     printed block from the table head to the end of propagation, with LNZ's
@@ -346,9 +363,11 @@ def main():
         case_morse1d("morse1d_spo_voptic", ".PFSPO", VOPTIC, vmeta)
         case_sil_order_text(".YES")
         case_sil_order_text(".NO")
+        case_test8_text()
         return
     case_sil_order_text(".YES")
     case_sil_order_text(".NO")
+    case_test8_text()
     cases = {}
     cases["test8"] = case_test8()
     cases["test4"] = case_test4()
