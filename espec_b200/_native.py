@@ -33,7 +33,7 @@ EXPORTS = [
     "espec_grid_create", "espec_grid_load", "espec_grid_run", "espec_grid_continue",
     "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
     "espec_grid_basis", "plnz_", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
-    "spectrumtd_",
+    "spectrumtd_", "espec_eig_solve_dev", "espec_eig_lcg_start", "espec_eig_morse2d",
 ]
 
 
@@ -102,6 +102,11 @@ def load():
     lib.hwhm_.restype = None
     lib.spectrumtd_.argtypes = [vp] * 8 + [C.c_size_t]
     lib.spectrumtd_.restype = None
+    lib.espec_eig_solve_dev.argtypes = [C.c_int, i, d, vp, vp, C.c_int, C.c_int, C.c_double,
+                                        C.c_int, vp, vp, vp, vp, vp, vp, vp]
+    lib.espec_eig_lcg_start.argtypes = [vp, C.c_int, C.c_int, vp]
+    lib.espec_eig_morse2d.argtypes = [C.c_int, vp, i, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_double, C.c_double, vp, vp]
     lib.espec_grid_destroy.argtypes = [vp]
     lib.espec_grid_destroy.restype = None
     lib.espec_spo_destroy.argtypes = [vp]

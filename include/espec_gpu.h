@@ -239,6 +239,33 @@ long espec_grid_npoints(const espec_grid_plan* plan);
 void espec_grid_destroy(espec_grid_plan* plan);
 
 /* ----------------------------------------------------------------------
+ * Initial-state eigensolver, batched over potentials (2D grids, FP64).
+ *
+ * LANCZSG (lanczsc.f:56-120): for each of nstates lowest states, restarted
+ * Lanczos of length m (full reorthogonalisation, lnz.f/reort.f) from a start
+ * vector, restarting from the K-th Ritz vector until |H v - theta v| <= tol
+ * (the true residual; one H*v per restart on top of the m Lanczos steps).
+ * All pointers are device pointers: vpot [nprob][n], start [nprob][nstates]
+ * [n], vec [nprob][nstates][n] (the normalised eigenvectors), eval/resid
+ * [nprob][nstates], matvecs [nprob][nstates] (H*v applications per state),
+ * work_L [nprob][m][n] and work_v [nprob][n] scratch.  m <= 40, nstates < m.
+ * ---------------------------------------------------------------------- */
+int espec_eig_solve_dev(int nprob, const int* np, const double* shm,
+                        const double* vpot, const double* start, int nstates, int m,
+                        double tol, int maxrest, double* vec, double* eval,
+                        double* resid, int* matvecs, double* work_L, double* work_v,
+                        void* stream);
+/* the reference's cold start (rans.f:38-39 LCG from NSEED = 1, the first n
+ * draws discarded, then n draws per state; lanczsc.f:56-62) into d_out
+ * [nstates][n] */
+int espec_eig_lcg_start(double* d_out, int n, int nstates, void* stream);
+/* 2D coupled-Morse potentials on an np[0] x np[1] grid over [xi,xf]x[yi,yf]
+ * from params [nprob][5] = (De1, a1, De2, a2, lambda) (device pointers) */
+int espec_eig_morse2d(int nprob, const double* params, const int* np, double xi,
+                      double xf, double yi, double yf, double re1, double re2,
+                      double* vpot, void* stream);
+
+/* ----------------------------------------------------------------------
  * Spectrum stage on the device, batched over packets (FP64).
  *
  * For each of npk packets: the 2^mf-point time signal -- assembled from the

@@ -1205,3 +1205,121 @@ extern "C" int orc_spo_batch(int npk, const int* off, const double* sh, const do
   for (auto& th : pool) th.join();
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Initial-state eigensolver (LANCZSG, lanczsc.f:56-120)
+// ---------------------------------------------------------------------------
+
+// rans.f:38-39  NSEED = MOD(NSEED*L + NC, M), RAN = NSEED/M
+extern "C" double orc_ran(int* nseed) {
+  const long long L = 1029, NC = 221591, M = 1048576;
+  *nseed = (int)(((long long)*nseed * L + NC) % M);
+  return (double)*nseed / (double)M;
+}
+
+// lanczsc.f:56-62: NSEED = 1, N draws discarded, then N draws per state
+extern "C" void orc_lcg_start(int n, int nstates, double* out) {
+  int seed = 1;
+  for (int i = 0; i < n; ++i) orc_ran(&seed);
+  for (int k = 0; k < nstates; ++k)
+    for (int i = 0; i < n; ++i) out[(long)k * n + i] = orc_ran(&seed);
+}
+
+// LNZ (lnz.f:76-119) whose REORT set (reort.f:65-80) also holds nlock
+// locked eigenvectors: all dot products of the step first, then all updates.
+static void lanczos_locked(int ndim, const int* np, const double* shm, const double* vpot, int n,
+                           int mp, const double* s, const double* lock, int nlock, double* L,
+                           double* al, double* bt) {
+  std::vector<double> work(s, s + n), vi(n, 0.0), v0(n), rv(mp + nlock);
+  for (long i = 0; i < (long)n * mp; ++i) L[i] = 0.0;
+  double bt0 = orc_ecnorm(n, work.data());
+  for (int it = 0; it < mp; ++it) {
+    for (int j = 0; j < n; ++j) {
+      v0[j] = vi[j];
+      vi[j] = work[j] / bt0;
+      L[j + (long)n * it] = vi[j];
+    }
+    orc_au(ndim, np, shm, vpot, vi.data(), work.data());
+    double sum1 = 0.0;
+    for (int j = 0; j < n; ++j) {
+      work[j] = work[j] - bt0 * v0[j];
+      sum1 = sum1 + vi[j] * work[j];
+    }
+    al[it] = sum1;
+    for (int j = 0; j < n; ++j) work[j] = work[j] - al[it] * vi[j];
+    for (int q = 0; q < nlock; ++q) {
+      double r = 0.0;
+      for (int j = 0; j < n; ++j) r = r + work[j] * lock[j + (long)n * q];
+      rv[q] = r;
+    }
+    for (int q = 0; q <= it; ++q) {
+      double r = 0.0;
+      for (int j = 0; j < n; ++j) r = r + work[j] * L[j + (long)n * q];
+      rv[nlock + q] = r;
+    }
+    for (int q = 0; q < nlock; ++q)
+      for (int j = 0; j < n; ++j) work[j] = work[j] - rv[q] * lock[j + (long)n * q];
+    for (int q = 0; q <= it; ++q)
+      for (int j = 0; j < n; ++j) work[j] = work[j] - rv[nlock + q] * L[j + (long)n * q];
+    bt[it] = orc_ecnorm(n, work.data());
+    bt0 = bt[it];
+  }
+}
+
+// For each state K: the start vector made orthogonal to the states already
+// found, LNZ (m steps) with those states locked in the REORT set, the lowest
+// Ritz pair of the tridiagonal matrix (DSTEVX('V','I',...) in the reference;
+// QL here), v = L y normalised by ECNORM (lanczsc.f:99-113), and -- in place
+// of the reference's sum |VI(I) - VIAUX(I)| test, whose index is the loop
+// bound (lanczsc.f:103) -- the true residual |H v - theta v| against tol.
+// (Without locking, the reference's K-th Ritz vector can settle on a higher
+// state; espec.f:896-903 restricts LANCZSG to the ground state.)  matvecs
+// counts H*v.  Returns 0, or 1 when a state needed more than maxrest restarts.
+extern "C" int orc_eig_lanczsg(int ndim, const int* np, const double* shm, const double* vpot,
+                               int nstates, int m, double tol, int maxrest, const double* start,
+                               double* evals, double* evecs, double* resid, int* matvecs) {
+  int n = 1;
+  for (int a = 0; a < ndim; ++a) n *= np[a];
+  std::vector<double> L((size_t)n * m), al(m), bt(m), w(m), z((size_t)m * m), v(n), hv(n);
+  int rc = 0;
+  for (int K = 0; K < nstates; ++K) {
+    for (int i = 0; i < n; ++i) v[i] = start[(long)K * n + i];
+    int count = 0;
+    double res = 0.0, theta = 0.0;
+    bool done = false;
+    for (int rs = 0; rs < maxrest && !done; ++rs) {
+      for (int q = 0; q < K; ++q) {  // project out the locked states
+        const double* e = evecs + (long)q * n;
+        const double c = orc_fcorrel(n, e, v.data());
+        for (int i = 0; i < n; ++i) v[i] = v[i] - c * e[i];
+      }
+      lanczos_locked(ndim, np, shm, vpot, n, m, v.data(), evecs, K, L.data(), al.data(),
+                     bt.data());
+      count += m;
+      orc_tridiag_eig(m, al.data(), bt.data(), w.data(), z.data());
+      theta = w[0];
+      for (int i = 0; i < n; ++i) {
+        double s = 0.0;
+        for (int j = 0; j < m; ++j) s += z[j] * L[i + (size_t)n * j];
+        v[i] = s;
+      }
+      const double fatn = orc_ecnorm(n, v.data());
+      for (int i = 0; i < n; ++i) v[i] = v[i] / fatn;
+      orc_au(ndim, np, shm, vpot, v.data(), hv.data());
+      count += 1;
+      double r2 = 0.0;
+      for (int i = 0; i < n; ++i) {
+        const double r = hv[i] - theta * v[i];
+        r2 += r * r;
+      }
+      res = std::sqrt(r2);
+      done = res <= tol;
+    }
+    if (!done) rc = 1;
+    evals[K] = theta;
+    resid[K] = res;
+    matvecs[K] = count;
+    for (int i = 0; i < n; ++i) evecs[(long)K * n + i] = v[i];
+  }
+  return rc;
+}

@@ -134,6 +134,15 @@ int orc_spo_batch(int npk, const int* off, const double* sh, const double* sm,
                   int nsteps, int quirks, double* c_re, double* c_im,
                   int nthreads);
 
+/* Initial-state eigensolver (lanczsc.f LANCZSG with the true residual):
+ * start [nstates][n], evecs [nstates][n]; returns 1 if a state did not
+ * converge within maxrest restarts.  orc_ran / orc_lcg_start: rans.f LCG. */
+double orc_ran(int* nseed);
+void orc_lcg_start(int n, int nstates, double* out);
+int orc_eig_lanczsg(int ndim, const int* np, const double* shm, const double* vpot,
+                    int nstates, int m, double tol, int maxrest, const double* start,
+                    double* evals, double* evecs, double* resid, int* matvecs);
+
 #ifdef __cplusplus
 }
 #endif

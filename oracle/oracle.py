@@ -269,6 +269,26 @@ def spectrumtd(window_sg, mf, dtf, tf, wp, de, u, v, quirks=0):
     return en, u, v
 
 
+def lcg_start(n, nstates):
+    out = np.zeros(n * nstates)
+    lib().orc_lcg_start(C.c_int(n), C.c_int(nstates), _p(out))
+    return out.reshape(nstates, n)
+
+
+def eig_lanczsg(np_, shm, vpot, nstates, m, tol, maxrest, start):
+    nd = len(np_)
+    npa = np.array(list(np_) + [1] * (3 - nd), dtype=np.int32)
+    shma = f64(list(shm) + [0.0] * (3 - nd))
+    n = int(np.prod(np_))
+    st = f64(np.asarray(start).reshape(-1))
+    ev, vec, res = np.zeros(nstates), np.zeros(nstates * n), np.zeros(nstates)
+    mv = np.zeros(nstates, dtype=np.int32)
+    rc = lib().orc_eig_lanczsg(C.c_int(nd), _ip(npa), _p(shma), _p(f64(vpot)), C.c_int(nstates),
+                               C.c_int(m), C.c_double(tol), C.c_int(maxrest), _p(st), _p(ev),
+                               _p(vec), _p(res), mv.ctypes.data_as(C.POINTER(C.c_int)))
+    return dict(evals=ev, evecs=vec.reshape(nstates, n), resid=res, matvecs=mv, rc=rc)
+
+
 def spo_batch(off, sh, sm, vpot, u, v, dt_fs, nsteps, nthreads=1, quirks=0):
     off = np.ascontiguousarray(off, dtype=np.int32)
     npk = off.size - 1
