@@ -34,6 +34,9 @@ EXPORTS = [
     "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
     "espec_grid_basis", "plnz_", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
     "spectrumtd_", "espec_eig_solve_dev", "espec_eig_lcg_start", "espec_eig_morse2d",
+    "espec_gemm_f64", "espec_gemm_f32", "espec_mlp_bias_act", "espec_mlp_tanh_back",
+    "espec_mlp_colsum", "espec_mlp_mse", "espec_mlp_adam", "espec_outer_basis", "espec_convert",
+    "espec_mlp_adam_dev",
 ]
 
 
@@ -107,6 +110,17 @@ def load():
     lib.espec_eig_lcg_start.argtypes = [vp, C.c_int, C.c_int, vp]
     lib.espec_eig_morse2d.argtypes = [C.c_int, vp, i, C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_double, C.c_double, vp, vp]
+    ci, cd, cf, cl = C.c_int, C.c_double, C.c_float, C.c_long
+    lib.espec_gemm_f64.argtypes = [ci, ci, ci, cd, vp, ci, ci, vp, ci, ci, cd, vp, ci, vp]
+    lib.espec_gemm_f32.argtypes = [ci, ci, ci, cf, vp, ci, ci, vp, ci, ci, cf, vp, ci, vp]
+    lib.espec_mlp_bias_act.argtypes = [vp, vp, ci, ci, ci, vp]
+    lib.espec_mlp_tanh_back.argtypes = [vp, vp, cl, vp]
+    lib.espec_mlp_colsum.argtypes = [vp, ci, ci, vp, vp]
+    lib.espec_mlp_mse.argtypes = [vp, vp, ci, ci, vp, vp, vp]
+    lib.espec_mlp_adam.argtypes = [vp, vp, vp, vp, cl, cf, cf, cf, cf, ci, vp]
+    lib.espec_mlp_adam_dev.argtypes = [vp, vp, vp, vp, cl, vp, cf, cf, cf, vp]
+    lib.espec_outer_basis.argtypes = [vp, ci, ci, vp, ci, ci, vp, vp]
+    lib.espec_convert.argtypes = [vp, vp, cl, ci, cd, vp]
     lib.espec_grid_destroy.argtypes = [vp]
     lib.espec_grid_destroy.restype = None
     lib.espec_spo_destroy.argtypes = [vp]

@@ -28,7 +28,7 @@ namespace {
 
 constexpr int kEigThreads = 256;
 constexpr int kEigMaxM = 40;      // NREORT = 40 in lanczsc.f:55
-constexpr int kEigMaxStates = 8;  // locked states held in the reorthogonalisation
+constexpr int kEigMaxStates = 16;  // locked states held in the reorthogonalisation
 
 struct EigArgs {
   int nx, ny, n;
@@ -436,7 +436,7 @@ extern "C" int espec_eig_solve_dev(int nprob, const int* np, const double* shm,
       !work_L || !work_v)
     return set_error(ESPEC_EINVAL, "null argument");
   if (m < 2 || m > kEigMaxM) return set_error(ESPEC_EINVAL, "Lanczos length must be 2..48");
-  if (nstates < 1 || nstates > kEigMaxStates) return set_error(ESPEC_EINVAL, "nstates must be 1..8");
+  if (nstates < 1 || nstates > kEigMaxStates) return set_error(ESPEC_EINVAL, "nstates must be 1..16");
   if (np[0] < 1 || np[1] < 1) return set_error(ESPEC_EINVAL, "bad grid");
   EigArgs a{};
   a.nx = np[0];

@@ -248,7 +248,8 @@ void espec_grid_destroy(espec_grid_plan* plan);
  * All pointers are device pointers: vpot [nprob][n], start [nprob][nstates]
  * [n], vec [nprob][nstates][n] (the normalised eigenvectors), eval/resid
  * [nprob][nstates], matvecs [nprob][nstates] (H*v applications per state),
- * work_L [nprob][m][n] and work_v [nprob][n] scratch.  m <= 40, nstates < m.
+ * work_L [nprob][m][n] and work_v [nprob][n] scratch.  m <= 40, nstates <= 16.
+ * A 1D problem is an np[0] x 1 grid with shm[1] = 0.
  * ---------------------------------------------------------------------- */
 int espec_eig_solve_dev(int nprob, const int* np, const double* shm,
                         const double* vpot, const double* start, int nstates, int m,
@@ -264,6 +265,42 @@ int espec_eig_lcg_start(double* d_out, int n, int nstates, void* stream);
 int espec_eig_morse2d(int nprob, const double* params, const int* np, double xi,
                       double xf, double yi, double yf, double re1, double re2,
                       double* vpot, void* stream);
+
+/* ----------------------------------------------------------------------
+ * Learned warm start for the eigensolver (no counterpart in the reference,
+ * which always starts from its LCG vectors).  Kernels of a small multilayer
+ * perceptron trained on the eigensolver's own eigenvectors; all pointers are
+ * device pointers, matrices row-major.
+ * ---------------------------------------------------------------------- */
+/* C[M,N] = alpha op(A) op(B) + beta C, op(X) = X^T when t* != 0 */
+int espec_gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, int ta,
+                   const double* B, int ldb, int tb, double beta, double* C, int ldc,
+                   void* stream);
+int espec_gemm_f32(int M, int N, int K, float alpha, const float* A, int lda, int ta,
+                   const float* B, int ldb, int tb, float beta, float* C, int ldc,
+                   void* stream);
+/* y[r,c] = act(y[r,c] + b[c]), act = tanh when act != 0 */
+int espec_mlp_bias_act(float* y, const float* b, int rows, int cols, int act, void* stream);
+/* dz *= 1 - y^2 (y = tanh of the layer's input) */
+int espec_mlp_tanh_back(float* dz, const float* y, long count, void* stream);
+/* db[c] = sum_r dy[r,c] */
+int espec_mlp_colsum(const float* dy, int rows, int cols, float* db, void* stream);
+/* mean squared error: row_loss[r] = sum_c (y-t)^2/(rows cols), dy = its gradient */
+int espec_mlp_mse(const float* y, const float* t, int rows, int cols, float* dy,
+                  float* row_loss, void* stream);
+/* one Adam step (step counts from 1) */
+int espec_mlp_adam(float* w, const float* g, float* m1, float* m2, long count, float lr,
+                   float b1, float b2, float eps, int step, void* stream);
+/* Adam step with hyper = device {lr, 1 - b1^t, 1 - b2^t}: replayable from a
+ * captured CUDA graph with new values written into hyper */
+int espec_mlp_adam_dev(float* w, const float* g, float* m1, float* m2, long count,
+                       const float* hyper, float b1, float b2, float eps, void* stream);
+/* B[i*nby+j][x + nx*y] = phi[i][x] chi[j][y] (product basis of two 1D sets) */
+int espec_outer_basis(const double* phi, int nbx, int nx, const double* chi, int nby, int ny,
+                      double* B, void* stream);
+/* element-wise f64 -> f32 (to_f32 != 0) or f32 -> f64, times scale */
+int espec_convert(const void* src, void* dst, long count, int to_f32, double scale,
+                  void* stream);
 
 /* ----------------------------------------------------------------------
  * Spectrum stage on the device, batched over packets (FP64).
