@@ -50,6 +50,11 @@ def parse():
     ap.add_argument("--sizes", default=None, help="comma list of packet sizes (profiling)")
     ap.add_argument("--cpu-sample-steps", type=int, default=400)
     ap.add_argument("--cpu-sample-packets", type=int, default=256)
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the FP64-form, SIL-2D and eigensolver legs")
+    ap.add_argument("--eig-train", type=int, default=4096)
+    ap.add_argument("--eig-test", type=int, default=256)
+    ap.add_argument("--eig-epochs", type=int, default=4000)
     return ap.parse_args()
 
 
@@ -171,6 +176,134 @@ def cpu_baseline(args):
             "sample": f"{w['npk']} packets x {w['nsteps']} time steps of the scan workload"}
 
 
+def fp64_form(args, w, ms_mixed, dev):
+    """The plain FP64 GPU form on the same scan (BASELINE's comparison form),
+    and |dC(t)| of the mixed form against it on 256 packets of the scan."""
+    import torch
+
+    import espec_b200 as E
+    from espec_b200 import workloads as W
+
+    b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision="fp64")
+    vpot_d = torch.from_numpy(w["vpot"]).to(dev)
+    psi_d = torch.from_numpy(w["psi"]).to(dev)
+    zero_d = torch.zeros_like(psi_d)
+    st = torch.cuda.current_stream(dev)
+    k = max(1, min(args.steps, 3))
+    for _ in range(1):
+        b.load(vpot_d, (psi_d, zero_d), stream=st.cuda_stream)
+        b.run(w["nsteps"], stream=st.cuda_stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(k):
+        b.load(vpot_d, (psi_d, zero_d), stream=st.cuda_stream)
+        b.run(w["nsteps"], stream=st.cuda_stream)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    b.close()
+    # accuracy sample: 256 packets, full time loop, both forms
+    ws = W.morse_scan(npk=256, nsteps=w["nsteps"], seed=777)
+    cs = {}
+    for prec in ("mixed", "fp64"):
+        bb = E.SpoBatch(ws["n"], ws["sh"], ws["sm"], ws["dt_fs"], precision=prec)
+        bb.load(ws["vpot"], ws["psi"])
+        bb.run(ws["nsteps"])
+        cs[prec], _ = bb.results()
+        bb.close()
+    dc = np.abs(cs["mixed"] - cs["fp64"])
+    pts = float(w["off"][-1]) * w["nsteps"]
+    return {"value": pts / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s", "ms_per_step": ms,
+            "mixed_over_fp64": ms / ms_mixed,
+            "dC_max_mixed_vs_fp64": float(dc.max()),
+            "dC_rms_mixed_vs_fp64": float(np.sqrt(np.mean(dc ** 2))),
+            "dC_sample": f"256 packets of the scan x {w['nsteps']} steps, every C(t) sample"}
+
+
+def sil_2d(dev, steps=100, cpu_steps=2):
+    """SIL order 12 on the 256 x 256 coupled-Morse grid (dt = 1 au), GPU and the
+    oracle port on the host."""
+    import torch
+
+    import espec_b200 as E
+
+    n = 256
+    x = np.linspace(0.5, 8.0, n)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    morse = lambda q, de, a, re: de * (1 - np.exp(-a * (q - re))) ** 2  # noqa: E731
+    V = morse(X, 0.17, 1.0, 1.4) + morse(Y, 0.12, 1.2, 1.8) + 0.01 * (X - 1.4) * (Y - 1.8)
+    psi = np.exp(-((X - 1.6) ** 2) / (2 * 0.15 ** 2) - ((Y - 2.0) ** 2) / (2 * 0.15 ** 2))
+    psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
+    v = V.ravel(order="F")
+    h = x[1] - x[0]
+    sm = [918.0, 1500.0]
+    shm = [1.0 / (((24.0 * m) * h) * h) for m in sm]
+    dt = 1.0 * 2.4188843243e-2
+    g = E.SilGrid([n, n], shm, dt, 12)
+    g.load(v, psi)
+    g.run(5)
+    g.results()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    st = torch.cuda.current_stream(dev)
+    e0.record(st)
+    g.run(steps)
+    e1.record(st)
+    g.results()
+    ms = e0.elapsed_time(e1) / steps
+    g.close()
+    from oracle import oracle as O
+
+    p = O.make_prop([n, n], dt, 0.0, cpu_steps * dt, [h, h], sm, lc=1, mp=12, lmtreort=16,
+                    change=0, shm=shm)
+    t0 = time.perf_counter()
+    O.plnz(p, v, psi.real.copy(), psi.imag.copy())
+    tc = (time.perf_counter() - t0) / O.do_count(dt, cpu_steps * dt + dt, dt)
+    return {"workload": "SIL order 12, 256x256 coupled Morse, dt = 1 au", "value":
+            n * n / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s", "us_per_step": ms * 1e3,
+            "steps_timed": steps, "cpu_port": {"value": n * n / tc / 1e6,
+                                               "unit": "Mgridpt*steps/s", "cores": 1,
+                                               "sample": f"{cpu_steps} steps"}}
+
+
+def eig_warmstart(args, dev):
+    """Lanczos H*v applications to the 4 lowest states of 128x128 coupled-Morse
+    potentials: cold start (the reference's LCG vectors) vs the learned warm
+    start trained on the solver's own eigenvectors."""
+    import torch
+
+    from espec_b200 import eig as EG
+    from espec_b200 import warmstart as WS
+
+    g = EG.Grid2D((128, 128))
+    t0 = time.perf_counter()
+    ws = WS.WarmStart(g, hidden=(256, 256), seed=0)
+    qtr, qte = WS.sample_params(args.eig_train, 1), WS.sample_params(args.eig_test, 2)
+    rtr = ws.solve(qtr)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    ws.fit(qtr, rtr["vec"], epochs=args.eig_epochs, lr=2e-3)
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    cold = ws.solve(qte)
+    torch.cuda.synchronize()
+    t3 = time.perf_counter()
+    warm = ws.solve_warm(qte)
+    torch.cuda.synchronize()
+    t4 = time.perf_counter()
+    mc = cold["matvecs"].sum(1).double()
+    mw = warm["matvecs"].sum(1).double()
+    return {"workload": "4 lowest states, 128x128 coupled Morse, restarted Lanczos m=40, "
+                        "|Hv - Ev| <= 1e-9",
+            "lanczos_iters_cold": float(mc.mean()), "lanczos_iters_warm": float(mw.mean()),
+            "iters_ratio": float(mc.mean() / mw.mean()), "fallbacks": int(warm["fallback"]),
+            "max_resid_warm": float(warm["resid"].max()),
+            "eval_max_diff": float((warm["eval"] - cold["eval"]).abs().max()),
+            "train_sets": args.eig_train, "held_out": args.eig_test, "epochs": args.eig_epochs,
+            "train_solve_s": t1 - t0, "train_fit_s": t2 - t1, "cold_solve_s": t3 - t2,
+            "warm_solve_s": t4 - t3, "unit": "H*v applications per potential (4 states)"}
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -269,6 +402,11 @@ def main():
                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                "timing": "host wall clock around load+run+results (max over ranks not taken)"}
 
+    extra = {}
+    if rank == 0 and not args.no_extra:
+        extra["fp64_form"] = fp64_form(args, w, ms, dev) if args.precision == "mixed" else None
+        extra["sil_2d"] = sil_2d(dev)
+        extra["eigensolver"] = eig_warmstart(args, dev)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mgridpt*steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -280,7 +418,8 @@ def main():
                            "packets_per_s": args.npk * world / (ms * 1e-3)},
                 "roofline": roof,
                 "cpu_baseline": cpu_baseline(args) if (world == 1 and not args.no_cpu) else None,
-                "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary()}
+                "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary(),
+                **extra}
         print(json.dumps(line), flush=True)
     b.close()
     if world > 1:
