@@ -6,7 +6,7 @@ and the batched split-operator interface.
 """
 from . import _native
 from ._native import EspecError, load
-from .grid import SilGrid
+from .grid import SilGrid, SpoGrid
 from .spo import SodBatch, SpoBatch
 
-__all__ = ["EspecError", "SilGrid", "SodBatch", "SpoBatch", "load", "workloads"]
+__all__ = ["EspecError", "SilGrid", "SpoGrid", "SodBatch", "SpoBatch", "load", "workloads"]

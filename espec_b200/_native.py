@@ -18,6 +18,7 @@ Q_SPO_INPLACE = 1
 Q_SOD_SMOOTHW = 2
 Q_SIL_INPLACE = 4
 Q_FFTNT_SP = 8
+Q_DIGT_ND = 16
 SPO, SOD, SIL = 0, 1, 2
 MEM_HOST, MEM_DEVICE = 0, 1
 SHFS = 2.4188843243e-2
@@ -36,7 +37,8 @@ EXPORTS = [
     "spectrumtd_", "espec_eig_solve_dev", "espec_eig_lcg_start", "espec_eig_morse2d",
     "espec_gemm_f64", "espec_gemm_f32", "espec_mlp_bias_act", "espec_mlp_tanh_back",
     "espec_mlp_colsum", "espec_mlp_mse", "espec_mlp_adam", "espec_outer_basis", "espec_convert",
-    "espec_mlp_adam_dev",
+    "espec_mlp_adam_dev", "espec_spond_create", "espec_spond_load", "espec_spond_run",
+    "espec_spond_results", "espec_spond_destroy",
 ]
 
 
@@ -119,6 +121,12 @@ def load():
     lib.espec_mlp_mse.argtypes = [vp, vp, ci, ci, vp, vp, vp]
     lib.espec_mlp_adam.argtypes = [vp, vp, vp, vp, cl, cf, cf, cf, cf, ci, vp]
     lib.espec_mlp_adam_dev.argtypes = [vp, vp, vp, vp, cl, vp, cf, cf, cf, vp]
+    lib.espec_spond_create.argtypes = [C.POINTER(vp), ci, i, d, d, cd, ci, ci, ci]
+    lib.espec_spond_load.argtypes = [vp, vp, vp, vp, vp, ci, vp]
+    lib.espec_spond_run.argtypes = [vp, ci, vp]
+    lib.espec_spond_results.argtypes = [vp, vp, vp, vp, vp, ci, vp]
+    lib.espec_spond_destroy.argtypes = [vp]
+    lib.espec_spond_destroy.restype = None
     lib.espec_outer_basis.argtypes = [vp, ci, ci, vp, ci, ci, vp, vp]
     lib.espec_convert.argtypes = [vp, vp, cl, ci, cd, vp]
     lib.espec_grid_destroy.argtypes = [vp]

@@ -1,0 +1,816 @@
+// spond.cu -- split-operator propagation (PSPOFFT / PSPOFFTAUX, pspofft.f,
+// spofft.f:64-200) on one 2D or 3D grid, FP64 or mixed (FP32 data, FP64
+// tables), and the plan behind espec_spond_* (include/espec_gpu.h).
+//
+// Line transforms: one warp per line of N = 32 P points (P = 1..16); lane l
+// holds points 32 j + l in register j.  Forward = four-step: a P-point DFT
+// in registers (radix-2 decimation in frequency), twiddles W_N^(l k1), then a
+// 32-point DFT across the lanes by __shfl_xor butterflies (decimation in
+// frequency): lane l, register r ends with frequency brev_P(r) + P brev_32(l).
+// The inverse is the exact mirror with conjugate twiddles (unnormalised).
+// Between the passes of a step each row stays in that permuted frequency
+// order; only the kinetic pass needs the frequencies, via its table.
+//
+// Passes per step (the V half-steps of consecutive steps merged, g = h^2):
+//   2D: x pass [inverse x, C(t), x-space phase, forward x]; y pass [forward y,
+//       kinetic phase, inverse y]
+//   3D: x pass; y pass [forward y]; z pass [forward z, kinetic, inverse z];
+//       y pass [inverse y]
+// Strided passes stage a tile of 8 adjacent x columns in shared memory.  The
+// fftshift swaps of spofft.f:120-133/178-191 cancel and are not done; the
+// 1/N of the reference's B factor is folded into the kinetic table.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <vector>
+
+#include "cplx.cuh"
+#include "espec_gpu.h"
+#include "espec_internal.h"
+
+namespace espec {
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kTile = 8;  // lines per CTA in a strided pass (8 warps)
+
+template <typename R>
+__device__ __forceinline__ cpx<R> cmul(cpx<R> a, cpx<R> b) {
+  return mk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> cmulc(cpx<R> a, cpx<R> b) {  // a * conj(b)
+  return mk(a.x * b.x + a.y * b.y, a.y * b.x - a.x * b.y);
+}
+template <typename R>
+__device__ __forceinline__ cpx<R> shx(cpx<R> v, int m) {
+  return mk(__shfl_xor_sync(kFull, v.x, m), __shfl_xor_sync(kFull, v.y, m));
+}
+__host__ __device__ __forceinline__ int brev_bits(int v, int bits) {
+  int r = 0;
+  for (int i = 0; i < bits; ++i) r |= ((v >> i) & 1) << (bits - 1 - i);
+  return r;
+}
+template <int P>
+constexpr int log2i() {
+  return P <= 1 ? 0 : 1 + log2i<P / 2>();
+}
+// Fixed rotations: FP64 as (cos, sin) applied by a complex product; FP32 as
+// three lifting shears (RotF), whose rounding is unbiased -- a rounded
+// (cos, sin) pair has |w| != 1 and a fixed-angle product loses or gains norm
+// systematically, step after step.
+template <typename R>
+struct Rot;
+template <>
+struct Rot<double> {
+  using type = RotD;
+  static __device__ __forceinline__ RotD make(double k_over_n) {  // exp(-2 pi i k/n)
+    RotD r;
+    sincospi(-2.0 * k_over_n, &r.s, &r.c);
+    return r;
+  }
+};
+template <>
+struct Rot<float> {
+  using type = RotF;
+  static __device__ __forceinline__ RotF make(double k_over_n) {
+    return make_rotf(-6.283185307179586476925287 * k_over_n);
+  }
+};
+template <typename R>
+__device__ __forceinline__ typename Rot<R>::type twid(int k, int n) {
+  return Rot<R>::make((double)k / (double)n);
+}
+
+// x-space and kinetic factors: FP64 complex, or FP32 lifting rotation with a
+// magnitude (the sign of a removed pi folded into it)
+struct PhF {
+  float t, s, ag;
+};
+template <typename R>
+struct Ph;
+template <>
+struct Ph<double> {
+  using type = cpx<double>;
+};
+template <>
+struct Ph<float> {
+  using type = PhF;
+};
+__host__ __device__ __forceinline__ cpx<double> apply_ph(cpx<double> p, cpx<double> v) {
+  return mk(v.x * p.x - v.y * p.y, v.x * p.y + v.y * p.x);
+}
+__host__ __device__ __forceinline__ cpx<float> apply_ph(PhF p, cpx<float> v) {
+  float x = v.x * p.ag, y = v.y * p.ag;
+  x = fmaf(-p.t, y, x);
+  y = fmaf(p.s, x, y);
+  x = fmaf(-p.t, y, x);
+  return mk(x, y);
+}
+// e^{i phi} times a, as stored factors
+__host__ __device__ inline PhF make_phf(double phi, double a) {
+  const RotF r = make_rotf(phi);
+  PhF o;
+  o.t = r.t;
+  o.s = r.s;
+  o.ag = (float)(r.g * a);
+  return o;
+}
+
+template <typename R, int P>
+struct WarpFft {
+  static constexpr int LP = log2i<P>();
+  using T = typename Rot<R>::type;
+  T wl[5];                         // lane stages m = 16 .. 1: W_2m^(lane & (m-1))
+  T wb[P];                         // W_N^(lane k1(r))
+  T wr[P > 1 ? P / 2 : 1];         // W_P^q, q < P/2
+  int lane;
+
+  __device__ void init(int N) {
+    lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+      const int m = 16 >> s;
+      wl[s] = twid<R>(lane & (m - 1), 2 * m);
+    }
+#pragma unroll
+    for (int r = 0; r < P; ++r) wb[r] = twid<R>(lane * brev_bits(r, LP), N);
+#pragma unroll
+    for (int q = 0; q < (P > 1 ? P / 2 : 1); ++q) wr[q] = twid<R>(q, P > 1 ? P : 1);
+  }
+  __device__ void forward(cpx<R>* v) const {
+#pragma unroll
+    for (int h = P / 2; h >= 1; h /= 2)
+#pragma unroll
+      for (int b = 0; b < P; b += 2 * h)
+#pragma unroll
+        for (int q = 0; q < h; ++q) {
+          const cpx<R> a = v[b + q], c = v[b + q + h];
+          v[b + q] = a + c;
+          v[b + q + h] = rot<false>(wr[q * (P / (2 * h))], a - c);
+        }
+#pragma unroll
+    for (int r = 0; r < P; ++r) v[r] = rot<false>(wb[r], v[r]);
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+      const int m = 16 >> s;
+      const bool up = lane & m;
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        const cpx<R> mine = v[r], other = shx(mine, m);
+        v[r] = up ? rot<false>(wl[s], other - mine) : mine + other;
+      }
+    }
+  }
+  __device__ void inverse(cpx<R>* v) const {
+#pragma unroll
+    for (int s = 4; s >= 0; --s) {
+      const int m = 16 >> s;
+      const bool up = lane & m;
+#pragma unroll
+      for (int r = 0; r < P; ++r) {
+        const cpx<R> mine = up ? rot<true>(wl[s], v[r]) : v[r];
+        const cpx<R> other = shx(mine, m);
+        v[r] = up ? other - mine : mine + other;
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < P; ++r) v[r] = rot<true>(wb[r], v[r]);
+#pragma unroll
+    for (int h = 1; h <= P / 2; h *= 2)
+#pragma unroll
+      for (int b = 0; b < P; b += 2 * h)
+#pragma unroll
+        for (int q = 0; q < h; ++q) {
+          const cpx<R> a = v[b + q], t = rot<true>(wr[q * (P / (2 * h))], v[b + q + h]);
+          v[b + q] = a + t;
+          v[b + q + h] = a - t;
+        }
+  }
+};
+
+template <typename R>
+struct NdArgs {
+  int nx, ny, nz, ndim;
+  cpx<R>* psi;            // state
+  const double2* psi0;    // psi(0), natural order (FIRST pass input)
+  double2* psi_out;       // psi(TF), natural order (LAST pass output)
+  using PhT = typename Ph<R>::type;
+  const PhT* g;           // x-space factors, natural order
+  const PhT* h;
+  const PhT* hm;
+  const double2* w;       // conj(psi0) hm, for C(t) (FP64 in both forms)
+  const PhT* K;           // kinetic factors in the kinetic pass's layout
+  const double* kq_c;     // reference-defect form: cos / sin(CST1 TC) in that layout
+  const double* kq_s;
+  double kq_scale;
+  double2* cpart;         // C(t) partial sums [step][x-pass CTA]
+  int step;
+};
+
+enum { kFirst = 0, kMid = 1, kLast = 2 };
+
+// x pass: one warp per row, 8 rows per CTA
+template <typename R, int P, int MODE>
+__global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
+  constexpr int N = 32 * P;
+  __shared__ double2 s_c[8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const long row = (long)blockIdx.x * 8 + warp;
+  const long nrows = (long)a.ny * a.nz;
+  WarpFft<R, P> fft;
+  fft.init(N);
+  cpx<R> v[P];
+  double cr = 0.0, ci = 0.0;
+  if (row < nrows) {
+    const long base = row * N;
+    if (MODE == kFirst) {
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const long x = base + 32 * j + lane;
+        const double2 p = a.psi0[x];
+        cr += p.x * p.x + p.y * p.y;  // C(0) = <psi0|psi0>
+        v[j] = apply_ph(a.h[x], mk((R)p.x, (R)p.y));
+      }
+    } else {
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = a.psi[base + 32 * j + lane];
+      fft.inverse(v);
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const long x = base + 32 * j + lane;
+        const double2 wj = a.w[x];
+        cr += wj.x * (double)v[j].x - wj.y * (double)v[j].y;
+        ci += wj.x * (double)v[j].y + wj.y * (double)v[j].x;
+        v[j] = apply_ph(MODE == kLast ? a.hm[x] : a.g[x], v[j]);
+      }
+    }
+    if (MODE == kLast) {
+#pragma unroll
+      for (int j = 0; j < P; ++j)
+        a.psi_out[base + 32 * j + lane] = make_double2((double)v[j].x, (double)v[j].y);
+    } else {
+      fft.forward(v);
+#pragma unroll
+      for (int j = 0; j < P; ++j) a.psi[base + 32 * j + lane] = v[j];
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cr += __shfl_xor_sync(kFull, cr, o);
+    ci += __shfl_xor_sync(kFull, ci, o);
+  }
+  if (lane == 0) s_c[warp] = make_double2(cr, ci);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double sr = 0.0, si = 0.0;
+    for (int i = 0; i < 8; ++i) {
+      sr += s_c[i].x;
+      si += s_c[i].y;
+    }
+    a.cpart[(long)a.step * gridDim.x + blockIdx.x] = make_double2(sr, si);
+  }
+}
+
+enum { kFwd = 0, kInv = 1, kKin = 2 };
+
+// strided pass along axis 1 (y) or 2 (z): CTA = 8 adjacent x columns of one
+// line set, staged through shared memory; warp w transforms column w
+template <typename R, int P, int MODE, bool QUIRK>
+__global__ void __launch_bounds__(256) axis_pass(NdArgs<R> a, int axis) {
+  constexpr int N = 32 * P;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  cpx<R>* tile = reinterpret_cast<cpx<R>*>(sm_raw);  // [N][kTile + 1]
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int ntx = a.nx / kTile;
+  const long xt = blockIdx.x % ntx, other = blockIdx.x / ntx;
+  long stride, base;
+  if (axis == 1) {  // lines along y: x = 8 xt + c, z = other
+    stride = a.nx;
+    base = other * (long)a.nx * a.ny + xt * kTile;
+  } else {          // lines along z: x = 8 xt + c, y = other
+    stride = (long)a.nx * a.ny;
+    base = other * (long)a.nx + xt * kTile;
+  }
+  for (int e = threadIdx.x; e < N * kTile; e += blockDim.x) {
+    const int t = e / kTile, c = e % kTile;
+    tile[t * (kTile + 1) + c] = a.psi[base + t * stride + c];
+  }
+  __syncthreads();
+  WarpFft<R, P> fft;
+  fft.init(N);
+  cpx<R> v[P];
+#pragma unroll
+  for (int j = 0; j < P; ++j) v[j] = tile[(32 * j + lane) * (kTile + 1) + warp];
+  if (MODE == kFwd || MODE == kKin) fft.forward(v);
+  if (MODE == kKin) {
+    // kinetic table line: x position and the other coordinate
+    const long line = (xt * kTile + warp) + (long)a.nx * other;
+    const long kb = line * N;
+#pragma unroll
+    for (int j = 0; j < P; ++j) {
+      const long f = kb + 32 * j + lane;
+      if constexpr (QUIRK) {
+        // spofft.f:148-154 as written: V(I) uses the already updated U(I)
+        const double c = a.kq_c[f], s = a.kq_s[f];
+        const double un = c * (double)v[j].x + s * (double)v[j].y;
+        const double vn = c * (double)v[j].y - s * un;
+        v[j] = mk((R)(un * a.kq_scale), (R)(vn * a.kq_scale));
+      } else {
+        v[j] = apply_ph(a.K[f], v[j]);
+      }
+    }
+  }
+  if (MODE == kInv || MODE == kKin) fft.inverse(v);
+#pragma unroll
+  for (int j = 0; j < P; ++j) tile[(32 * j + lane) * (kTile + 1) + warp] = v[j];
+  __syncthreads();
+  for (int e = threadIdx.x; e < N * kTile; e += blockDim.x) {
+    const int t = e / kTile, c = e % kTile;
+    a.psi[base + t * stride + c] = tile[t * (kTile + 1) + c];
+  }
+}
+
+// C(t) of each step: the x-pass partial sums in CTA order
+__global__ void csum_kernel(const double2* cpart, int nparts, int nsteps, int first,
+                            double2* c_out) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x + first;
+  if (s > nsteps) return;
+  double sr = 0.0, si = 0.0;
+  for (int i = 0; i < nparts; ++i) {
+    const double2 p = cpart[(long)s * nparts + i];
+    sr += p.x;
+    si += p.y;
+  }
+  c_out[s] = make_double2(sr, si);
+}
+
+// x-space tables (spofft.f:120-133, 162-191): h = e^{-i cst2 V} (x e^{cst2
+// VABC} for .VOPTIC), g = h^2 (x mask), hm = h mask, w = conj(psi0) hm
+__device__ __forceinline__ void put_ph(cpx<double>* o, double phi, double a) {
+  double s, c;
+  sincos(phi, &s, &c);
+  *o = mk(c * a, s * a);
+}
+__device__ __forceinline__ void put_ph(PhF* o, double phi, double a) { *o = make_phf(phi, a); }
+
+template <typename R>
+__global__ void nd_setup_kernel(long n, const double* vpot, const double* vabc, int absorb,
+                                double cst2, const double2* psi0, typename Ph<R>::type* g,
+                                typename Ph<R>::type* h, typename Ph<R>::type* hm, double2* w) {
+  const long x = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  const double th = cst2 * vpot[x];
+  double hmag = 1.0, mask = 1.0;
+  if (absorb == ESPEC_ABS_VOPTIC) hmag = exp(cst2 * vabc[x]);
+  if (absorb == ESPEC_ABS_SMOOTHW) mask = vabc[x];
+  double s1, c1, s2, c2;
+  sincos(th, &s1, &c1);
+  sincos(2.0 * th, &s2, &c2);
+  (void)s2;
+  (void)c2;
+  put_ph(g + x, -2.0 * th, hmag * hmag * mask);
+  put_ph(h + x, -th, hmag);
+  put_ph(hm + x, -th, hmag * mask);
+  const double hr = c1 * hmag * mask, hi = -s1 * hmag * mask;
+  const double2 p = psi0[x];
+  w[x] = make_double2(p.x * hr + p.y * hi, p.x * hi - p.y * hr);
+}
+
+}  // namespace
+}  // namespace espec
+
+// ---------------------------------------------------------------------------
+// plan
+// ---------------------------------------------------------------------------
+using namespace espec;
+
+struct espec_spond_plan {
+  int ndim = 2, np[3] = {1, 1, 1};
+  long n = 0;
+  double sh[3] = {1, 1, 1}, sm[3] = {1, 1, 1};
+  double dt_fs = 0.0;
+  int precision = ESPEC_FP64, absorb = 0, quirks = 0;
+  bool loaded = false;
+  void* d_psi = nullptr;      // cpx<R> state
+  double2* d_psi0 = nullptr;
+  double2* d_out = nullptr;
+  double* d_vpot = nullptr;
+  double* d_vabc = nullptr;
+  void* d_tab = nullptr;      // g, h, hm, w, K (cpx<R>)
+  double* d_kq = nullptr;     // quirk cos/sin tables
+  double2* d_cpart = nullptr;
+  double2* d_c = nullptr;
+  int c_cap = -1, xblocks = 0;
+};
+
+namespace {
+
+bool line_ok(int n) { return n == 32 || n == 64 || n == 128 || n == 256 || n == 512; }
+
+// frequency held at stored position pos of a line of n = 32 P points
+int freq_of(int pos, int n) {
+  const int P = n / 32, lp = P == 1 ? 0 : (P == 2 ? 1 : (P == 4 ? 2 : (P == 8 ? 3 : 4)));
+  return brev_bits(pos / 32, lp) + P * brev_bits(pos % 32, 5);
+}
+
+const double kDigtTwoPi = 6.283185307;  // dkeft.f:38
+
+void digt_axis_host(int n, double sh, double sm, double* t) { espec::digt_1d(n, sh, sm, t); }
+
+// kinetic table TC in the reference's FFT order (x fastest): the outer sum of
+// the axis tables, or with ESPEC_Q_DIGT_ND the 2D/3D loops of dkeft.f:80-137
+// as they are written (only TC(1..NP1) is filled)
+void digt_nd(const espec_spond_plan* p, std::vector<double>& tc) {
+  const int nx = p->np[0], ny = p->np[1], nz = p->ndim > 2 ? p->np[2] : 1;
+  tc.assign((size_t)p->n, 0.0);
+  if (p->quirks & ESPEC_Q_DIGT_ND) {
+    double dp[3];
+    for (int a = 0; a < p->ndim; ++a) dp[a] = kDigtTwoPi / (p->np[a] * p->sh[a]);
+    if (p->ndim == 2) {
+      double p1 = 0, p2 = 0;
+      for (int j = 0; j < ny / 2; ++j) {
+        for (int i = 0; i < nx / 2; ++i) {
+          tc[i] = p1 * p1 / (2 * p->sm[0]) + p2 * p2 / (2 * p->sm[1]);
+          p1 = p1 + dp[0];
+        }
+        p2 = p2 + dp[1];
+      }
+      p1 = -(p1 + dp[0]);
+      p2 = -(p2 + dp[1]);
+      for (int j = ny / 2; j < ny; ++j) {
+        for (int i = nx / 2; i < nx; ++i) {
+          tc[i] = p1 * p1 / (2 * p->sm[0]) + p2 * p2 / (2 * p->sm[1]);
+          p1 = p1 + dp[0];
+        }
+        p2 = p2 + dp[1];
+      }
+    } else {
+      double p1 = 0, p2 = 0, p3 = 0;
+      for (int k = 0; k < nz / 2; ++k) {
+        for (int j = 0; j < ny / 2; ++j) {
+          for (int i = 0; i < nx / 2; ++i) {
+            tc[i] = p1 * p1 / (2 * p->sm[0]) + p2 * p2 / (2 * p->sm[1]) +
+                    p3 * p3 / (2 * p->sm[2]);
+            p1 = p1 + dp[0];
+          }
+          p2 = p2 + dp[1];
+        }
+        p3 = p3 + dp[2];
+      }
+      p1 = -(p1 + dp[0]);
+      p2 = -(p2 + dp[1]);
+      p3 = -(p3 + dp[2]);
+      for (int k = nz / 2; k < nz; ++k) {
+        for (int j = ny / 2; j < ny; ++j) {
+          for (int i = nx / 2; i < nx; ++i) {
+            tc[i] = p1 * p1 / (2 * p->sm[0]) + p2 * p2 / (2 * p->sm[1]) +
+                    p3 * p3 / (2 * p->sm[2]);
+            p1 = p1 + dp[0];
+          }
+          p2 = p2 + dp[1];
+        }
+        p3 = p3 + dp[2];
+      }
+    }
+    return;
+  }
+  std::vector<double> t[3];
+  for (int a = 0; a < p->ndim; ++a) {
+    t[a].resize(p->np[a]);
+    digt_axis_host(p->np[a], p->sh[a], p->sm[a], t[a].data());
+  }
+  for (int k = 0; k < nz; ++k)
+    for (int j = 0; j < ny; ++j)
+      for (int i = 0; i < nx; ++i)
+        tc[i + (size_t)nx * (j + (size_t)ny * k)] =
+            t[0][i] + t[1][j] + (p->ndim > 2 ? t[2][k] : 0.0);
+}
+
+#define ND_CK(call)                                          \
+  do {                                                       \
+    cudaError_t e_ = (call);                                 \
+    if (e_ != cudaSuccess) return set_cuda_error(#call, e_); \
+  } while (0)
+
+// table block: g, h, hm (PhT) | w (double2) | K (PhT), n entries each
+template <typename R>
+struct NdTabs {
+  using PhT = typename Ph<R>::type;
+  PhT *g, *h, *hm, *K;
+  double2* w;
+  static size_t bytes(long n) { return (size_t)n * (4 * sizeof(PhT) + sizeof(double2)); }
+  NdTabs(void* base, long n) {
+    char* b = (char*)base;
+    w = (double2*)b;
+    g = (PhT*)(b + 16 * (size_t)n);
+    h = g + n;
+    hm = h + n;
+    K = hm + n;
+  }
+};
+
+inline cpx<double> k_factor(double th, long n, double) {
+  return mk(std::cos(th) / n, -std::sin(th) / n);
+}
+inline PhF k_factor(double th, long n, float) { return make_phf(-th, 1.0 / n); }
+
+template <typename R>
+int build_tables(espec_spond_plan* p, cudaStream_t st) {
+  const long n = p->n;
+  NdTabs<R> tb(p->d_tab, n);
+  const double cst1 = p->dt_fs / ESPEC_SHFS, cst2 = p->dt_fs / (2.0 * ESPEC_SHFS);
+  nd_setup_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+      n, p->d_vpot, p->d_vabc, p->absorb, cst2, p->d_psi0, tb.g, tb.h, tb.hm, tb.w);
+  ND_CK(cudaGetLastError());
+  // kinetic factors in the kinetic pass's layout: line (x position, other
+  // position), position along the kinetic axis; frequencies mirrored to the
+  // reference's FFT sign (fft3d.f: ISN = +1 is exp(+2 pi i jk/n))
+  std::vector<double> tc;
+  digt_nd(p, tc);
+  const int nx = p->np[0], ny = p->np[1], nz = p->ndim > 2 ? p->np[2] : 1;
+  const int ka = p->ndim - 1;  // kinetic axis: y (2D) or z (3D)
+  const int nk = p->np[ka];
+  std::vector<typename Ph<R>::type> K((size_t)n);
+  std::vector<double> qc, qs;
+  const bool quirk = (p->quirks & ESPEC_Q_SPO_INPLACE) != 0;
+  if (quirk) {
+    qc.resize((size_t)n);
+    qs.resize((size_t)n);
+  }
+  const long nlines = n / nk;
+  for (long line = 0; line < nlines; ++line) {
+    const int px = (int)(line % nx);
+    const int po = (int)(line / nx);  // y position (3D) or unused (2D)
+    const int fx = (nx - freq_of(px, nx)) % nx;
+    const int fy2 = p->ndim > 2 ? (ny - freq_of(po, ny)) % ny : 0;
+    for (int pos = 0; pos < nk; ++pos) {
+      const int fk = (nk - freq_of(pos, nk)) % nk;
+      size_t idx;
+      if (p->ndim == 2) idx = fx + (size_t)nx * fk;
+      else idx = fx + (size_t)nx * (fy2 + (size_t)ny * fk);
+      const double th = cst1 * tc[idx];
+      const size_t o = (size_t)line * nk + pos;
+      K[o] = k_factor(th, n, R(0));
+      if (quirk) {
+        qc[o] = std::cos(th);
+        qs[o] = std::sin(th);
+      }
+    }
+  }
+  (void)nz;
+  ND_CK(cudaMemcpyAsync(tb.K, K.data(), sizeof(K[0]) * n, cudaMemcpyHostToDevice, st));
+  if (quirk) {
+    ND_CK(cudaMemcpyAsync(p->d_kq, qc.data(), 8 * n, cudaMemcpyHostToDevice, st));
+    ND_CK(cudaMemcpyAsync(p->d_kq + n, qs.data(), 8 * n, cudaMemcpyHostToDevice, st));
+  }
+  ND_CK(cudaStreamSynchronize(st));  // the host vectors go out of scope
+  return ESPEC_OK;
+}
+
+template <typename R, int P>
+cudaError_t launch_x(int mode, const NdArgs<R>& a, int blocks, cudaStream_t st) {
+  switch (mode) {
+    case kFirst: x_pass<R, P, kFirst><<<blocks, 256, 0, st>>>(a); break;
+    case kMid: x_pass<R, P, kMid><<<blocks, 256, 0, st>>>(a); break;
+    default: x_pass<R, P, kLast><<<blocks, 256, 0, st>>>(a); break;
+  }
+  return cudaGetLastError();
+}
+
+template <typename R>
+cudaError_t launch_x_n(int nx, int mode, const NdArgs<R>& a, int blocks, cudaStream_t st) {
+  switch (nx) {
+    case 32: return launch_x<R, 1>(mode, a, blocks, st);
+    case 64: return launch_x<R, 2>(mode, a, blocks, st);
+    case 128: return launch_x<R, 4>(mode, a, blocks, st);
+    case 256: return launch_x<R, 8>(mode, a, blocks, st);
+    default: return launch_x<R, 16>(mode, a, blocks, st);
+  }
+}
+
+template <typename R, int P, int MODE, bool Q>
+cudaError_t launch_axis1(const NdArgs<R>& a, int axis, long blocks, cudaStream_t st) {
+  const size_t smem = sizeof(cpx<R>) * 32 * P * (kTile + 1);
+  static bool attr = false;
+  if (!attr) {
+    cudaError_t e = cudaFuncSetAttribute(axis_pass<R, P, MODE, Q>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr = true;
+  }
+  axis_pass<R, P, MODE, Q><<<(unsigned)blocks, 256, smem, st>>>(a, axis);
+  return cudaGetLastError();
+}
+
+template <typename R, int P>
+cudaError_t launch_axis_p(int mode, bool quirk, const NdArgs<R>& a, int axis, long blocks,
+                          cudaStream_t st) {
+  if (mode == kFwd) return launch_axis1<R, P, kFwd, false>(a, axis, blocks, st);
+  if (mode == kInv) return launch_axis1<R, P, kInv, false>(a, axis, blocks, st);
+  if constexpr (sizeof(R) == 8) {
+    if (quirk) return launch_axis1<R, P, kKin, true>(a, axis, blocks, st);
+  }
+  return launch_axis1<R, P, kKin, false>(a, axis, blocks, st);
+}
+
+template <typename R>
+cudaError_t launch_axis(int n, int mode, bool quirk, const NdArgs<R>& a, int axis, long blocks,
+                        cudaStream_t st) {
+  switch (n) {
+    case 32: return launch_axis_p<R, 1>(mode, quirk, a, axis, blocks, st);
+    case 64: return launch_axis_p<R, 2>(mode, quirk, a, axis, blocks, st);
+    case 128: return launch_axis_p<R, 4>(mode, quirk, a, axis, blocks, st);
+    case 256: return launch_axis_p<R, 8>(mode, quirk, a, axis, blocks, st);
+    default: return launch_axis_p<R, 16>(mode, quirk, a, axis, blocks, st);
+  }
+}
+
+template <typename R>
+int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st) {
+  NdArgs<R> a{};
+  a.nx = p->np[0];
+  a.ny = p->np[1];
+  a.nz = p->ndim > 2 ? p->np[2] : 1;
+  a.ndim = p->ndim;
+  a.psi = (cpx<R>*)p->d_psi;
+  a.psi0 = p->d_psi0;
+  a.psi_out = p->d_out;
+  const long n = p->n;
+  NdTabs<R> tb(p->d_tab, n);
+  a.g = tb.g;
+  a.h = tb.h;
+  a.hm = tb.hm;
+  a.w = tb.w;
+  a.K = tb.K;
+  a.kq_c = p->d_kq;
+  a.kq_s = p->d_kq ? p->d_kq + n : nullptr;
+  a.kq_scale = 1.0 / (double)n;
+  a.cpart = p->d_cpart;
+  const bool quirk = (p->quirks & ESPEC_Q_SPO_INPLACE) != 0;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  const int xb = p->xblocks;
+  const long yb = (long)(nx / kTile) * nz;   // y lines: x tiles x z
+  const long zb = (long)(nx / kTile) * ny;   // z lines: x tiles x y
+  cudaError_t e = cudaSuccess;
+  auto kin_step = [&]() {
+    if (p->ndim == 2) {
+      e = launch_axis<R>(ny, kKin, quirk, a, 1, yb, st);
+    } else {
+      e = launch_axis<R>(ny, kFwd, false, a, 1, yb, st);
+      if (e == cudaSuccess) e = launch_axis<R>(nz, kKin, quirk, a, 2, zb, st);
+      if (e == cudaSuccess) e = launch_axis<R>(ny, kInv, false, a, 1, yb, st);
+    }
+  };
+  if (nsteps == 0) {
+    if (from_start) {
+      a.step = 0;
+      e = launch_x_n<R>(nx, kFirst, a, xb, st);  // C(0); the state is left in k layout
+      if (e != cudaSuccess) return set_cuda_error("x pass", e);
+      // psi(TF) = psi(0)
+      ND_CK(cudaMemcpyAsync(p->d_out, p->d_psi0, 16 * n, cudaMemcpyDeviceToDevice, st));
+    }
+    return ESPEC_OK;
+  }
+  for (int s = 0; s <= nsteps; ++s) {
+    a.step = s;
+    int mode = s == 0 ? kFirst : (s == nsteps ? kLast : kMid);
+    if (s == 0 && !from_start) mode = -1;  // resumed: the state is already transformed
+    if (mode >= 0) {
+      e = launch_x_n<R>(nx, mode, a, xb, st);
+      if (e != cudaSuccess) return set_cuda_error("x pass", e);
+    }
+    if (s < nsteps) {
+      kin_step();
+      if (e != cudaSuccess) return set_cuda_error("axis pass", e);
+    }
+  }
+  return ESPEC_OK;
+}
+
+}  // namespace
+
+extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* np,
+                                  const double* sh, const double* sm, double dt_fs,
+                                  int precision, int absorb, int quirks) {
+  if (!out || !np || !sh || !sm) return set_error(ESPEC_EINVAL, "null argument");
+  if (ndim != 2 && ndim != 3) return set_error(ESPEC_EINVAL, "ndim must be 2 or 3");
+  for (int a = 0; a < ndim; ++a)
+    if (!line_ok(np[a]))
+      return set_error(ESPEC_EINVAL, "axis sizes must be 32, 64, 128, 256 or 512");
+  if (precision != ESPEC_FP64 && precision != ESPEC_MIXED)
+    return set_error(ESPEC_EINVAL, "precision must be ESPEC_FP64 or ESPEC_MIXED");
+  if (absorb < ESPEC_ABS_NONE || absorb > ESPEC_ABS_SMOOTHW)
+    return set_error(ESPEC_EINVAL, "unknown absorber type");
+  if (quirks & ~(ESPEC_Q_SPO_INPLACE | ESPEC_Q_DIGT_ND))
+    return set_error(ESPEC_EINVAL, "quirk not applicable to the N-D split operator");
+  if ((quirks & ESPEC_Q_SPO_INPLACE) && precision != ESPEC_FP64)
+    return set_error(ESPEC_EINVAL, "the reference-defect mode exists for FP64 only");
+  auto* p = new espec_spond_plan;
+  p->ndim = ndim;
+  p->n = 1;
+  for (int a = 0; a < ndim; ++a) {
+    p->np[a] = np[a];
+    p->sh[a] = sh[a];
+    p->sm[a] = sm[a];
+    p->n *= np[a];
+  }
+  p->dt_fs = dt_fs;
+  p->precision = precision;
+  p->absorb = absorb;
+  p->quirks = quirks;
+  p->xblocks = (int)((p->n / np[0] + 7) / 8);
+  const size_t n = (size_t)p->n;
+  const size_t cb = precision == ESPEC_FP64 ? 16 : 8;
+  int rc = 0;
+  auto fail = [&](int code) {
+    void* b[] = {p->d_psi, p->d_psi0, p->d_out, p->d_vpot, p->d_vabc, p->d_tab, p->d_kq,
+                 p->d_cpart, p->d_c};
+    for (void* x : b)
+      if (x) cudaFree(x);
+    delete p;
+    return code;
+  };
+  if ((rc = ck(cudaMalloc(&p->d_psi, cb * n), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_psi0, 16 * n), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_out, 16 * n), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_vpot, 8 * n), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_vabc, 8 * n), "cudaMalloc"))) return fail(rc);
+  const size_t tbytes = precision == ESPEC_FP64 ? NdTabs<double>::bytes((long)n)
+                                                : NdTabs<float>::bytes((long)n);
+  if ((rc = ck(cudaMalloc(&p->d_tab, tbytes), "cudaMalloc"))) return fail(rc);
+  if (quirks & ESPEC_Q_SPO_INPLACE)
+    if ((rc = ck(cudaMalloc(&p->d_kq, 16 * n), "cudaMalloc"))) return fail(rc);
+  *out = p;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spond_load(espec_spond_plan* p, const double* vpot, const double* vabc,
+                                const double* psi_re, const double* psi_im, int where,
+                                void* stream) {
+  if (!p || !vpot || !psi_re) return set_error(ESPEC_EINVAL, "null argument");
+  if (p->absorb != ESPEC_ABS_NONE && !vabc) return set_error(ESPEC_EINVAL, "absorber table missing");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t n = (size_t)p->n;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  ND_CK(cudaMemcpyAsync(p->d_vpot, vpot, 8 * n, kind, st));
+  if (p->absorb != ESPEC_ABS_NONE) ND_CK(cudaMemcpyAsync(p->d_vabc, vabc, 8 * n, kind, st));
+  ND_CK(cudaMemcpy2DAsync(p->d_psi0, 16, psi_re, 8, 8, n, kind, st));
+  if (psi_im) {
+    ND_CK(cudaMemcpy2DAsync((char*)p->d_psi0 + 8, 16, psi_im, 8, 8, n, kind, st));
+  } else {
+    ND_CK(cudaMemset2DAsync((char*)p->d_psi0 + 8, 16, 0, 8, n, st));
+  }
+  const int rc = p->precision == ESPEC_FP64 ? build_tables<double>(p, st)
+                                            : build_tables<float>(p, st);
+  if (rc) return rc;
+  p->loaded = true;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spond_run(espec_spond_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spond_load has not been called");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->c_cap != nsteps) {
+    if (p->d_c) cudaFree(p->d_c);
+    if (p->d_cpart) cudaFree(p->d_cpart);
+    p->d_c = nullptr;
+    p->d_cpart = nullptr;
+    ND_CK(cudaMalloc(&p->d_c, sizeof(double2) * ((size_t)nsteps + 1)));
+    ND_CK(cudaMalloc(&p->d_cpart, sizeof(double2) * ((size_t)nsteps + 1) * p->xblocks));
+    p->c_cap = nsteps;
+  }
+  const int rc = p->precision == ESPEC_FP64 ? run_steps<double>(p, nsteps, true, st)
+                                            : run_steps<float>(p, nsteps, true, st);
+  if (rc) return rc;
+  csum_kernel<<<(nsteps + 1 + 255) / 256, 256, 0, st>>>(p->d_cpart, p->xblocks, nsteps, 0,
+                                                         p->d_c);
+  ND_CK(cudaGetLastError());
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spond_results(espec_spond_plan* p, double* c_re, double* c_im,
+                                   double* psi_re, double* psi_im, int where, void* stream) {
+  if (!p || p->c_cap < 0) return set_error(ESPEC_EINVAL, "no results: run the plan first");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t nc = (size_t)p->c_cap + 1, n = (size_t)p->n;
+  if (c_re) ND_CK(cudaMemcpy2DAsync(c_re, 8, p->d_c, 16, 8, nc, kind, st));
+  if (c_im) ND_CK(cudaMemcpy2DAsync(c_im, 8, (char*)p->d_c + 8, 16, 8, nc, kind, st));
+  if (psi_re) ND_CK(cudaMemcpy2DAsync(psi_re, 8, p->d_out, 16, 8, n, kind, st));
+  if (psi_im) ND_CK(cudaMemcpy2DAsync(psi_im, 8, (char*)p->d_out + 8, 16, 8, n, kind, st));
+  if (where == ESPEC_MEM_HOST) ND_CK(cudaStreamSynchronize(st));
+  return ESPEC_OK;
+}
+
+extern "C" void espec_spond_destroy(espec_spond_plan* p) {
+  if (!p) return;
+  void* b[] = {p->d_psi, p->d_psi0, p->d_out, p->d_vpot, p->d_vabc, p->d_tab, p->d_kq,
+               p->d_cpart, p->d_c};
+  for (void* x : b)
+    if (x) cudaFree(x);
+  delete p;
+}

@@ -76,3 +76,56 @@ class SilGrid:
             self.close()
         except Exception:
             pass
+
+
+class SpoGrid:
+    """Split-operator propagation (PSPOFFT/PSPOFFTAUX, pspofft.f:72-145,
+    spofft.f:64-200) of one packet on a 2D or 3D grid, FP64 or mixed, on the
+    GPU.  np: points per axis (32..512, powers of two), sh/sm per axis (bohr,
+    electron masses), arrays flattened x fastest."""
+
+    def __init__(self, np_, sh, sm, dt_fs, precision="fp64", absorb=N.ABS_NONE, quirks=0):
+        lib = N.load()
+        self.np = [int(x) for x in np_]
+        self.n = int(np.prod(self.np))
+        npa = np.array(self.np, dtype=np.int32)
+        sha, sma = N.f64(sh), N.f64(sm)
+        self._h = C.c_void_p()
+        rc = lib.espec_spond_create(C.byref(self._h), len(self.np),
+                                    npa.ctypes.data_as(C.POINTER(C.c_int)),
+                                    sha.ctypes.data_as(C.POINTER(C.c_double)),
+                                    sma.ctypes.data_as(C.POINTER(C.c_double)), float(dt_fs),
+                                    {"fp64": N.FP64, "mixed": N.MIXED}[precision], absorb, quirks)
+        N.check(rc, "espec_spond_create")
+        self.nsteps = None
+
+    def load(self, vpot, psi, vabc=None, stream=None):
+        psi = np.asarray(psi)
+        self._keep = [N.f64(vpot), N.f64(np.real(psi)), N.f64(np.imag(psi)),
+                      None if vabc is None else N.f64(vabc)]
+        v, re, im, ab = self._keep
+        N.check(N.load().espec_spond_load(self._h, N.ptr(v), N.ptr(ab), N.ptr(re), N.ptr(im),
+                                          N.MEM_HOST, stream), "espec_spond_load")
+
+    def run(self, nsteps, stream=None):
+        N.check(N.load().espec_spond_run(self._h, int(nsteps), stream), "espec_spond_run")
+        self.nsteps = int(nsteps)
+
+    def results(self, stream=None):
+        ns = self.nsteps
+        cr, ci = np.zeros(ns + 1), np.zeros(ns + 1)
+        pr, pi = np.zeros(self.n), np.zeros(self.n)
+        N.check(N.load().espec_spond_results(self._h, N.ptr(cr), N.ptr(ci), N.ptr(pr), N.ptr(pi),
+                                             N.MEM_HOST, stream), "espec_spond_results")
+        return cr + 1j * ci, pr + 1j * pi
+
+    def close(self):
+        if self._h:
+            N.load().espec_spond_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -49,6 +49,7 @@ extern "C" {
 #define ESPEC_Q_SOD_SMOOTHW 2   /* sodfft.f:108 never applies the .SMOOTHW mask */
 #define ESPEC_Q_SIL_INPLACE 4   /* sil.f:145-148 sin term uses the cos-scaled U   */
 #define ESPEC_Q_FFTNT_SP 8      /* cfft.f:35 TWOPI from a single-precision literal */
+#define ESPEC_Q_DIGT_ND 16      /* dkeft.f:80-137 2D/3D kinetic table as written   */
 
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
@@ -237,6 +238,26 @@ int espec_grid_basis(espec_grid_plan* plan, int chain, double* dst, int ld, int 
                      void* stream);
 long espec_grid_npoints(const espec_grid_plan* plan);
 void espec_grid_destroy(espec_grid_plan* plan);
+
+/* ----------------------------------------------------------------------
+ * Split-operator propagation on one 2D or 3D grid (PSPOFFT/PSPOFFTAUX,
+ * pspofft.f:72-145, spofft.f:64-200, with the N-D kinetic table of DIGT,
+ * dkeft.f:80-137).  Axis sizes 32, 64, 128, 256 or 512, x fastest; sh, sm per
+ * axis; precision ESPEC_FP64 or ESPEC_MIXED (FP32 state and transforms, FP64
+ * tables and C(t)); absorb as the 1D plans; quirks ESPEC_Q_SPO_INPLACE (FP64)
+ * and ESPEC_Q_DIGT_ND (the reference's 2D/3D table, only TC(1..NP1) filled;
+ * without it the table is the outer sum of the axis tables).  C(t) every step,
+ * nsteps+1 samples; psi(TF) returned by espec_spond_results.
+ * ---------------------------------------------------------------------- */
+typedef struct espec_spond_plan espec_spond_plan;
+int espec_spond_create(espec_spond_plan** plan, int ndim, const int* np, const double* sh,
+                       const double* sm, double dt_fs, int precision, int absorb, int quirks);
+int espec_spond_load(espec_spond_plan* plan, const double* vpot, const double* vabc,
+                     const double* psi_re, const double* psi_im, int where, void* stream);
+int espec_spond_run(espec_spond_plan* plan, int nsteps, void* stream);
+int espec_spond_results(espec_spond_plan* plan, double* c_re, double* c_im, double* psi_re,
+                        double* psi_im, int where, void* stream);
+void espec_spond_destroy(espec_spond_plan* plan);
 
 /* ----------------------------------------------------------------------
  * Initial-state eigensolver, batched over potentials (2D grids, FP64).
