@@ -126,17 +126,20 @@ struct WarpFft {
   T wr[P > 1 ? P / 2 : 1];         // W_P^q, q < P/2
   int lane;
 
-  __device__ void init(int N) {
+  // every twiddle is W_N^k, k < N: read from the line's table (built once
+  // per plan in FP64, tw_table_kernel)
+  __device__ void init(const T* tab) {
+    constexpr int N = 32 * P;
     lane = threadIdx.x & 31;
 #pragma unroll
     for (int s = 0; s < 5; ++s) {
       const int m = 16 >> s;
-      wl[s] = twid<R>(lane & (m - 1), 2 * m);
+      wl[s] = tab[(lane & (m - 1)) * (N / (2 * m))];
     }
 #pragma unroll
-    for (int r = 0; r < P; ++r) wb[r] = twid<R>(lane * brev_bits(r, LP), N);
+    for (int r = 0; r < P; ++r) wb[r] = tab[lane * brev_bits(r, LP)];
 #pragma unroll
-    for (int q = 0; q < (P > 1 ? P / 2 : 1); ++q) wr[q] = twid<R>(q, P > 1 ? P : 1);
+    for (int q = 0; q < (P > 1 ? P / 2 : 1); ++q) wr[q] = tab[q * 32];
   }
   __device__ void forward(cpx<R>* v) const {
 #pragma unroll
@@ -205,8 +208,16 @@ struct NdArgs {
   const double* kq_s;
   double kq_scale;
   double2* cpart;         // C(t) partial sums [step][x-pass CTA]
+  const typename Rot<R>::type* tw[3];  // W_n^k tables of the x, y, z line lengths
   int step;
 };
+
+// W_n^k = exp(-2 pi i k / n), k < n, in the form the line transforms apply
+template <typename R>
+__global__ void tw_table_kernel(typename Rot<R>::type* tab, int n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) tab[k] = twid<R>(k, n);
+}
 
 enum { kFirst = 0, kMid = 1, kLast = 2 };
 
@@ -219,7 +230,7 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
   const long row = (long)blockIdx.x * 8 + warp;
   const long nrows = (long)a.ny * a.nz;
   WarpFft<R, P> fft;
-  fft.init(N);
+  fft.init(a.tw[0]);
   cpx<R> v[P];
   double cr = 0.0, ci = 0.0;
   if (row < nrows) {
@@ -298,7 +309,7 @@ __global__ void __launch_bounds__(256) axis_pass(NdArgs<R> a, int axis) {
   }
   __syncthreads();
   WarpFft<R, P> fft;
-  fft.init(N);
+  fft.init(a.tw[axis]);
   cpx<R> v[P];
 #pragma unroll
   for (int j = 0; j < P; ++j) v[j] = tile[(32 * j + lane) * (kTile + 1) + warp];
@@ -401,6 +412,7 @@ struct espec_spond_plan {
   double* d_kq = nullptr;     // quirk cos/sin tables
   double2* d_cpart = nullptr;
   double2* d_c = nullptr;
+  void* d_tw[3] = {nullptr, nullptr, nullptr};
   int c_cap = -1, xblocks = 0;
 };
 
@@ -647,6 +659,8 @@ int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st)
   a.kq_s = p->d_kq ? p->d_kq + n : nullptr;
   a.kq_scale = 1.0 / (double)n;
   a.cpart = p->d_cpart;
+  for (int ax = 0; ax < 3; ++ax)
+    a.tw[ax] = (const typename Rot<R>::type*)(ax < p->ndim ? p->d_tw[ax] : nullptr);
   const bool quirk = (p->quirks & ESPEC_Q_SPO_INPLACE) != 0;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int xb = p->xblocks;
@@ -725,7 +739,7 @@ extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* n
   int rc = 0;
   auto fail = [&](int code) {
     void* b[] = {p->d_psi, p->d_psi0, p->d_out, p->d_vpot, p->d_vabc, p->d_tab, p->d_kq,
-                 p->d_cpart, p->d_c};
+                 p->d_cpart, p->d_c, p->d_tw[0], p->d_tw[1], p->d_tw[2]};
     for (void* x : b)
       if (x) cudaFree(x);
     delete p;
@@ -741,6 +755,8 @@ extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* n
   if ((rc = ck(cudaMalloc(&p->d_tab, tbytes), "cudaMalloc"))) return fail(rc);
   if (quirks & ESPEC_Q_SPO_INPLACE)
     if ((rc = ck(cudaMalloc(&p->d_kq, 16 * n), "cudaMalloc"))) return fail(rc);
+  for (int ax = 0; ax < ndim; ++ax)
+    if ((rc = ck(cudaMalloc(&p->d_tw[ax], sizeof(RotD) * np[ax]), "cudaMalloc"))) return fail(rc);
   *out = p;
   return ESPEC_OK;
 }
@@ -765,6 +781,14 @@ extern "C" int espec_spond_load(espec_spond_plan* p, const double* vpot, const d
   const int rc = p->precision == ESPEC_FP64 ? build_tables<double>(p, st)
                                             : build_tables<float>(p, st);
   if (rc) return rc;
+  for (int ax = 0; ax < p->ndim; ++ax) {
+    const int nl = p->np[ax];
+    if (p->precision == ESPEC_FP64)
+      tw_table_kernel<double><<<(nl + 255) / 256, 256, 0, st>>>((RotD*)p->d_tw[ax], nl);
+    else
+      tw_table_kernel<float><<<(nl + 255) / 256, 256, 0, st>>>((RotF*)p->d_tw[ax], nl);
+    ND_CK(cudaGetLastError());
+  }
   p->loaded = true;
   return ESPEC_OK;
 }
@@ -809,7 +833,7 @@ extern "C" int espec_spond_results(espec_spond_plan* p, double* c_re, double* c_
 extern "C" void espec_spond_destroy(espec_spond_plan* p) {
   if (!p) return;
   void* b[] = {p->d_psi, p->d_psi0, p->d_out, p->d_vpot, p->d_vabc, p->d_tab, p->d_kq,
-               p->d_cpart, p->d_c};
+               p->d_cpart, p->d_c, p->d_tw[0], p->d_tw[1], p->d_tw[2]};
   for (void* x : b)
     if (x) cudaFree(x);
   delete p;
