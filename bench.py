@@ -266,6 +266,59 @@ def sil_2d(dev, steps=100, cpu_steps=2):
                                                "sample": f"{cpu_steps} steps"}}
 
 
+def spo_nd(dev):
+    """Split operator on 2D (256x256 coupled Morse, FP64, dt = 1 au) and 3D
+    (128^3 anharmonic oscillator, mixed vs FP64, dt = 2 au) grids."""
+    import torch
+
+    import espec_b200 as E
+
+    out = {}
+    shfs = 2.4188843243e-2
+    # 2D: the coupled-Morse potential of the SIL leg
+    x = np.linspace(0.5, 8.0, 256)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    morse = lambda q, de, a, re: de * (1 - np.exp(-a * (q - re))) ** 2  # noqa: E731
+    V = morse(X, 0.17, 1.0, 1.4) + morse(Y, 0.12, 1.2, 1.8) + 0.01 * (X - 1.4) * (Y - 1.8)
+    psi = np.exp(-((X - 1.6) ** 2) / (2 * 0.15 ** 2) - ((Y - 2.0) ** 2) / (2 * 0.15 ** 2))
+    psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
+    cases = [("spo_2d", [256, 256], V.ravel(order="F"), psi, [x[1] - x[0]] * 2, [918.0, 1500.0],
+              1.0, 2000)]
+    # 3D: three harmonic modes (omega = 0.01/0.012/0.015 Eh, m = 1836) + cubic coupling
+    q = np.linspace(-60.0, 60.0, 128)
+    G = np.meshgrid(q, q, q, indexing="ij")
+    w, m = [0.01, 0.012, 0.015], 1836.0
+    V3 = sum(0.5 * m * w[a] ** 2 * G[a] ** 2 for a in range(3)) + 1e-4 * (
+        G[0] ** 2 * G[1] - G[1] ** 3 / 3)
+    p3 = np.exp(-sum(m * w[a] / 2 * (G[a] - (2.0 if a == 0 else 0.0)) ** 2 for a in range(3)))
+    p3 = (p3 / np.sqrt(np.sum(p3 ** 2))).ravel(order="F").astype(complex)
+    cases.append(("spo_3d", [128, 128, 128], V3.ravel(order="F"), p3, [q[1] - q[0]] * 3, [m] * 3,
+                  2.0, 1000))
+    for name, np_, v, psi0, sh, sm, dt_au, nsteps in cases:
+        n = int(np.prod(np_))
+        res, cs = {}, {}
+        for prec in ("mixed", "fp64"):
+            g = E.SpoGrid(np_, sh, sm, dt_au * shfs, precision=prec)
+            g.load(v, psi0)
+            g.run(10)
+            g.results()
+            st = torch.cuda.current_stream(dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            g.run(nsteps)
+            e1.record(st)
+            cs[prec], _ = g.results()
+            ms = e0.elapsed_time(e1) / nsteps
+            res[prec] = {"value": n / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s",
+                         "us_per_step": ms * 1e3}
+            g.close()
+        d = np.abs(cs["mixed"] - cs["fp64"])
+        out[name] = {"grid": "x".join(map(str, np_)), "dt_au": dt_au, "steps_timed": nsteps,
+                     "fp64": res["fp64"], "mixed": res["mixed"],
+                     "dC_max_mixed_vs_fp64": float(d.max())}
+    return out
+
+
 def eig_warmstart(args, dev):
     """Lanczos H*v applications to the 4 lowest states of 128x128 coupled-Morse
     potentials: cold start (the reference's LCG vectors) vs the learned warm
@@ -406,6 +459,7 @@ def main():
     if rank == 0 and not args.no_extra:
         extra["fp64_form"] = fp64_form(args, w, ms, dev) if args.precision == "mixed" else None
         extra["sil_2d"] = sil_2d(dev)
+        extra.update(spo_nd(dev))
         extra["eigensolver"] = eig_warmstart(args, dev)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mgridpt*steps/s", "n_gpus": world,
