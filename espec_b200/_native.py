@@ -38,7 +38,7 @@ EXPORTS = [
     "espec_gemm_f64", "espec_gemm_f32", "espec_mlp_bias_act", "espec_mlp_tanh_back",
     "espec_mlp_colsum", "espec_mlp_mse", "espec_mlp_adam", "espec_outer_basis", "espec_convert",
     "espec_mlp_adam_dev", "espec_spond_create", "espec_spond_load", "espec_spond_run",
-    "espec_spond_results", "espec_spond_destroy",
+    "espec_spond_results", "espec_spond_destroy", "espec_spond_continue", "espec_spond_energies",
 ]
 
 
@@ -125,6 +125,8 @@ def load():
     lib.espec_spond_load.argtypes = [vp, vp, vp, vp, vp, ci, vp]
     lib.espec_spond_run.argtypes = [vp, ci, vp]
     lib.espec_spond_results.argtypes = [vp, vp, vp, vp, vp, ci, vp]
+    lib.espec_spond_continue.argtypes = [vp, ci, vp]
+    lib.espec_spond_energies.argtypes = [vp, vp, vp, vp]
     lib.espec_spond_destroy.argtypes = [vp]
     lib.espec_spond_destroy.restype = None
     lib.espec_outer_basis.argtypes = [vp, ci, ci, vp, ci, ci, vp, vp]

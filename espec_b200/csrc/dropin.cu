@@ -1,6 +1,6 @@
 // dropin.cu -- Fortran-callable drop-ins for eSPec's propagators PSPOFFT
-// (pspofft.f:1-150) and PSODFFT (psodfft.f:1-211), 1D, and PLNZ
-// (plnz.f:1-155), 1D/2D/3D.
+// (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D) and PLNZ
+// (plnz.f:1-155; 1D/2D/3D).
 //
 // Each call propagates one packet on the GPU through a one-packet plan and
 // leaves in the caller's arrays what the reference routine leaves there:
@@ -15,8 +15,9 @@
 // The arithmetic is the reference's, defects included: the in-place kinetic
 // multiply of spofft.f:150-153 and the never-applied .SMOOTHW mask of
 // sodfft.f:108, and PLNZ's cos-before-sin of sil.f:145-148.  Cases the GPU
-// path does not cover (FFT propagators: DIM other than '.1D', packet sizes
-// other than 256..4096 of the form 2^k or 3*2^k; PLNZ: order above 16) and
+// path does not cover (PSPOFFT: 1D sizes other than 256..4096 of the form 2^k
+// or 3*2^k, 2D/3D axes other than 32..512 powers of two; PSODFFT: DIM other
+// than '.1D'; PLNZ: order above 16) and
 // device errors set INFO = 2 and write the reason to standard error; nothing
 // is computed on the CPU.
 #include <cuda_runtime.h>
@@ -257,12 +258,50 @@ void common_scalars(DropIn& d, const int* absorb, const char* prtcrl, size_t prt
 // the FFT propagators: one-packet espec_spo_plan
 struct FftDropIn : DropIn {
   espec_spo_plan* plan = nullptr;
-  ~FftDropIn() { espec_spo_destroy(plan); }
+  espec_spond_plan* nd = nullptr;  // 2D/3D split operator
+  ~FftDropIn() {
+    espec_spo_destroy(plan);
+    espec_spond_destroy(nd);
+  }
+
+  int setup_nd(int ndim, const char* tpabsor, size_t tpabsor_len, const int* np, const double* sh,
+               const double* sm, double* tc, const double* vpot, const double* vabc,
+               const double* u, const double* v) {
+    long npts = 1;
+    for (int a = 0; a < ndim; ++a) npts *= np[a];
+    if (npts != n) return fail("N differs from the product of NP");
+    if (lc < 1) return fail("LC must be at least 1");
+    // DIGT for 2D/3D as the reference computes it (dkeft.f:80-137)
+    const int quirks = ESPEC_Q_SPO_INPLACE | ESPEC_Q_DIGT_ND;
+    espec::digt_nd_table(ndim, np, sh, sm, quirks, tc);
+    const int ab = absorber(absorb, tpabsor, tpabsor_len);
+    if (espec_spond_create(&nd, ndim, np, sh, sm, dt, ESPEC_FP64, ab, quirks) ||
+        espec_spond_load(nd, vpot, ab == ESPEC_ABS_NONE ? nullptr : vabc, u, v, ESPEC_MEM_HOST,
+                         nullptr))
+      return fail_lib();
+    be.run = [this](int k) { return espec_spond_run(nd, k, nullptr); };
+    be.cont = [this](int k) { return espec_spond_continue(nd, k, nullptr); };
+    be.cvals = [this](int, double* cr, double* ci) {
+      return espec_spond_results(nd, cr, ci, nullptr, nullptr, ESPEC_MEM_HOST, nullptr);
+    };
+    be.energy = [this](double& e, double& nr) {
+      return espec_spond_energies(nd, &e, &nr, nullptr);
+    };
+    double fnt;
+    if (energies(e0, fnt)) return -1;
+    f0 = fnt;
+    return 0;
+  }
 
   int setup(int method, const char* dim, size_t dim_len, const char* tpabsor, size_t tpabsor_len,
             const int* np, const double* sh, const double* sm, double* tc, const double* vpot,
             const double* vabc, const double* u, const double* v) {
-    if (!fstr_is(dim, dim_len, ".1D")) return fail("only DIM = '.1D' runs on the GPU");
+    const int ndim = fstr_is(dim, dim_len, ".2D") ? 2 : (fstr_is(dim, dim_len, ".3D") ? 3 : 1);
+    if (ndim > 1) {
+      if (method != ESPEC_SPO) return fail("2D/3D runs on the GPU for PSPOFFT only");
+      return setup_nd(ndim, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u, v);
+    }
+    if (!fstr_is(dim, dim_len, ".1D")) return fail("DIM must be '.1D', '.2D' or '.3D'");
     if (np[0] != n) return fail("N differs from NP(1)");
     if (lc < 1) return fail("LC must be at least 1");
     // DIGT (dkeft.f:64-79): the kinetic table is an output of the reference
@@ -329,7 +368,10 @@ extern "C" void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
   if (nsteps >= 1) tt[1] = *ti + *dt;
   for (int s = 2; s <= nsteps; ++s) tt[s] = tt[s - 1] + *dt;
   if (d.propagate(nsteps, [&](int s) { return tt[s]; }, [](int) { return true; })) return;
-  if (espec_spo_results(d.plan, nullptr, nullptr, u1, v1, ESPEC_MEM_HOST, nullptr)) {
+  const int rc = d.nd ? espec_spond_results(d.nd, nullptr, nullptr, u1, v1, ESPEC_MEM_HOST, nullptr)
+                      : espec_spo_results(d.plan, nullptr, nullptr, u1, v1, ESPEC_MEM_HOST,
+                                          nullptr);
+  if (rc) {
     d.fail_lib();
     return;
   }

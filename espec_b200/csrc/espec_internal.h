@@ -7,6 +7,10 @@ int set_error(int code, const char* msg);
 int set_cuda_error(const char* what, cudaError_t e);
 // kinetic table of a 1D packet in FFT order (DIGT, dkeft.f:64-79)
 void digt_1d(int n, double sh, double sm, double* tc);
+// kinetic table of a 2D/3D grid in the reference's FFT order (dkeft.f:80-137
+// as written with ESPEC_Q_DIGT_ND, else the outer sum of the axis tables)
+void digt_nd_table(int ndim, const int* np, const double* sh, const double* sm, int quirks,
+                   double* tc);
 inline int ck(cudaError_t e, const char* what) {
   return e == cudaSuccess ? 0 : set_cuda_error(what, e);
 }

@@ -197,6 +197,7 @@ struct NdArgs {
   int nx, ny, nz, ndim;
   cpx<R>* psi;            // state
   const double2* psi0;    // psi(0), natural order (FIRST pass input)
+  const double2* psi_start;  // resume / diagnostics: natural-order state read instead
   double2* psi_out;       // psi(TF), natural order (LAST pass output)
   using PhT = typename Ph<R>::type;
   const PhT* g;           // x-space factors, natural order
@@ -219,7 +220,7 @@ __global__ void tw_table_kernel(typename Rot<R>::type* tab, int n) {
   if (k < n) tab[k] = twid<R>(k, n);
 }
 
-enum { kFirst = 0, kMid = 1, kLast = 2 };
+enum { kFirst = 0, kMid = 1, kLast = 2, kFwd0 = 3 };
 
 // x pass: one warp per row, 8 rows per CTA
 template <typename R, int P, int MODE>
@@ -236,12 +237,19 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
   if (row < nrows) {
     const long base = row * N;
     if (MODE == kFirst) {
+      const double2* src = a.psi_start ? a.psi_start : a.psi0;
 #pragma unroll
       for (int j = 0; j < P; ++j) {
         const long x = base + 32 * j + lane;
-        const double2 p = a.psi0[x];
-        cr += p.x * p.x + p.y * p.y;  // C(0) = <psi0|psi0>
+        const double2 p = src[x];
+        cr += p.x * p.x + p.y * p.y;  // C(0) = <psi0|psi0> (not used when resuming)
         v[j] = apply_ph(a.h[x], mk((R)p.x, (R)p.y));
+      }
+    } else if (MODE == kFwd0) {  // plain forward transform of a natural-order state
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const double2 p = a.psi_start[base + 32 * j + lane];
+        v[j] = mk((R)p.x, (R)p.y);
       }
     } else {
 #pragma unroll
@@ -273,7 +281,7 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
   }
   if (lane == 0) s_c[warp] = make_double2(cr, ci);
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (threadIdx.x == 0 && a.cpart) {
     double sr = 0.0, si = 0.0;
     for (int i = 0; i < 8; ++i) {
       sr += s_c[i].x;
@@ -281,6 +289,33 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
     }
     a.cpart[(long)a.step * gridDim.x + blockIdx.x] = make_double2(sr, si);
   }
+}
+
+// EFFT4 (eigenergfft.f:58-100) and the norm of a natural-order state psi
+// given its forward transform khat in the passes' storage order:
+// sum V |psi|^2 + (1/N) sum TC |khat|^2 and sum |psi|^2, per-CTA partials
+__global__ void nd_energy_kernel(const double2* psi, const double* vpot, const cpx<double>* khat,
+                                 const double* tcp, long n, double rn, double2* part) {
+  __shared__ double2 red[256];
+  double e = 0.0, nr = 0.0;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long)gridDim.x * blockDim.x) {
+    const double2 p = psi[i];
+    const double a2 = p.x * p.x + p.y * p.y;
+    const cpx<double> k = khat[i];
+    e += vpot[i] * a2 + rn * tcp[i] * (k.x * k.x + k.y * k.y);
+    nr += a2;
+  }
+  red[threadIdx.x] = make_double2(e, nr);
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      red[threadIdx.x].x += red[threadIdx.x + o].x;
+      red[threadIdx.x].y += red[threadIdx.x + o].y;
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
 }
 
 enum { kFwd = 0, kInv = 1, kKin = 2 };
@@ -414,6 +449,12 @@ struct espec_spond_plan {
   double2* d_c = nullptr;
   void* d_tw[3] = {nullptr, nullptr, nullptr};
   int c_cap = -1, xblocks = 0;
+  bool has_state = false;          // d_out holds the state of the last run
+  // energy diagnostics (FP64 in both forms)
+  cpx<double>* d_khat = nullptr;
+  double* d_tcp = nullptr;         // TC in the passes' storage order
+  RotD* d_tw64[3] = {nullptr, nullptr, nullptr};
+  double2* d_epart = nullptr;
 };
 
 namespace {
@@ -585,6 +626,7 @@ cudaError_t launch_x(int mode, const NdArgs<R>& a, int blocks, cudaStream_t st) 
   switch (mode) {
     case kFirst: x_pass<R, P, kFirst><<<blocks, 256, 0, st>>>(a); break;
     case kMid: x_pass<R, P, kMid><<<blocks, 256, 0, st>>>(a); break;
+    case kFwd0: x_pass<R, P, kFwd0><<<blocks, 256, 0, st>>>(a); break;
     default: x_pass<R, P, kLast><<<blocks, 256, 0, st>>>(a); break;
   }
   return cudaGetLastError();
@@ -648,6 +690,7 @@ int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st)
   a.psi = (cpx<R>*)p->d_psi;
   a.psi0 = p->d_psi0;
   a.psi_out = p->d_out;
+  a.psi_start = from_start ? nullptr : p->d_out;
   const long n = p->n;
   NdTabs<R> tb(p->d_tab, n);
   a.g = tb.g;
@@ -688,12 +731,9 @@ int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st)
   }
   for (int s = 0; s <= nsteps; ++s) {
     a.step = s;
-    int mode = s == 0 ? kFirst : (s == nsteps ? kLast : kMid);
-    if (s == 0 && !from_start) mode = -1;  // resumed: the state is already transformed
-    if (mode >= 0) {
-      e = launch_x_n<R>(nx, mode, a, xb, st);
-      if (e != cudaSuccess) return set_cuda_error("x pass", e);
-    }
+    const int mode = s == 0 ? kFirst : (s == nsteps ? kLast : kMid);
+    e = launch_x_n<R>(nx, mode, a, xb, st);
+    if (e != cudaSuccess) return set_cuda_error("x pass", e);
     if (s < nsteps) {
       kin_step();
       if (e != cudaSuccess) return set_cuda_error("axis pass", e);
@@ -703,6 +743,26 @@ int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st)
 }
 
 }  // namespace
+
+namespace espec {
+// the N-D kinetic table (TC) in the reference's FFT order, for the drop-ins
+void digt_nd_table(int ndim, const int* np, const double* sh, const double* sm, int quirks,
+                   double* tc) {
+  espec_spond_plan q;
+  q.ndim = ndim;
+  q.n = 1;
+  for (int a = 0; a < ndim; ++a) {
+    q.np[a] = np[a];
+    q.sh[a] = sh[a];
+    q.sm[a] = sm[a];
+    q.n *= np[a];
+  }
+  q.quirks = quirks;
+  std::vector<double> t;
+  digt_nd(&q, t);
+  for (long i = 0; i < q.n; ++i) tc[i] = t[i];
+}
+}  // namespace espec
 
 extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* np,
                                   const double* sh, const double* sm, double dt_fs,
@@ -781,6 +841,7 @@ extern "C" int espec_spond_load(espec_spond_plan* p, const double* vpot, const d
   const int rc = p->precision == ESPEC_FP64 ? build_tables<double>(p, st)
                                             : build_tables<float>(p, st);
   if (rc) return rc;
+  p->has_state = false;
   for (int ax = 0; ax < p->ndim; ++ax) {
     const int nl = p->np[ax];
     if (p->precision == ESPEC_FP64)
@@ -812,6 +873,93 @@ extern "C" int espec_spond_run(espec_spond_plan* p, int nsteps, void* stream) {
   csum_kernel<<<(nsteps + 1 + 255) / 256, 256, 0, st>>>(p->d_cpart, p->xblocks, nsteps, 0,
                                                          p->d_c);
   ND_CK(cudaGetLastError());
+  p->has_state = true;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spond_continue(espec_spond_plan* p, int nsteps, void* stream) {
+  if (!p || nsteps < 0) return set_error(ESPEC_EINVAL, "bad plan or step count");
+  if (!p->has_state) return set_error(ESPEC_EINVAL, "continue needs a previous run");
+  cudaStream_t st = (cudaStream_t)stream;
+  if (p->c_cap != nsteps) {
+    if (p->d_c) cudaFree(p->d_c);
+    if (p->d_cpart) cudaFree(p->d_cpart);
+    p->d_c = nullptr;
+    p->d_cpart = nullptr;
+    ND_CK(cudaMalloc(&p->d_c, sizeof(double2) * ((size_t)nsteps + 1)));
+    ND_CK(cudaMalloc(&p->d_cpart, sizeof(double2) * ((size_t)nsteps + 1) * p->xblocks));
+    p->c_cap = nsteps;
+  }
+  if (nsteps == 0) return ESPEC_OK;
+  const int rc = p->precision == ESPEC_FP64 ? run_steps<double>(p, nsteps, false, st)
+                                            : run_steps<float>(p, nsteps, false, st);
+  if (rc) return rc;
+  csum_kernel<<<(nsteps + 255) / 256, 256, 0, st>>>(p->d_cpart, p->xblocks, nsteps, 1, p->d_c);
+  ND_CK(cudaGetLastError());
+  return ESPEC_OK;
+}
+
+// TC of the diagnostic transform's storage order (all axes permuted)
+static int nd_energy_tables(espec_spond_plan* p) {
+  std::vector<double> tc;
+  digt_nd(p, tc);
+  const int nx = p->np[0], ny = p->np[1], nz = p->ndim > 2 ? p->np[2] : 1;
+  std::vector<double> tcp((size_t)p->n);
+  for (int k = 0; k < nz; ++k) {
+    const int fz = p->ndim > 2 ? (nz - freq_of(k, nz)) % nz : 0;
+    for (int j = 0; j < ny; ++j) {
+      const int fy = (ny - freq_of(j, ny)) % ny;
+      for (int i = 0; i < nx; ++i) {
+        const int fx = (nx - freq_of(i, nx)) % nx;
+        tcp[i + (size_t)nx * (j + (size_t)ny * k)] = tc[fx + (size_t)nx * (fy + (size_t)ny * fz)];
+      }
+    }
+  }
+  ND_CK(cudaMemcpy(p->d_tcp, tcp.data(), 8 * tcp.size(), cudaMemcpyHostToDevice));
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spond_energies(espec_spond_plan* p, double* e, double* norm, void* stream) {
+  if (!p || !e || !norm) return set_error(ESPEC_EINVAL, "null argument");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_spond_load has not been called");
+  cudaStream_t st = (cudaStream_t)stream;
+  const long n = p->n;
+  const int nb = 256;
+  if (!p->d_khat) {
+    ND_CK(cudaMalloc(&p->d_khat, sizeof(cpx<double>) * n));
+    ND_CK(cudaMalloc(&p->d_tcp, 8 * n));
+    ND_CK(cudaMalloc(&p->d_epart, sizeof(double2) * (nb + 1)));
+    for (int ax = 0; ax < p->ndim; ++ax) {
+      ND_CK(cudaMalloc(&p->d_tw64[ax], sizeof(RotD) * p->np[ax]));
+      tw_table_kernel<double><<<(p->np[ax] + 255) / 256, 256, 0, st>>>(p->d_tw64[ax], p->np[ax]);
+      ND_CK(cudaGetLastError());
+    }
+    const int rc = nd_energy_tables(p);
+    if (rc) return rc;
+  }
+  NdArgs<double> a{};
+  a.nx = p->np[0];
+  a.ny = p->np[1];
+  a.nz = p->ndim > 2 ? p->np[2] : 1;
+  a.ndim = p->ndim;
+  a.psi = p->d_khat;
+  a.psi_start = p->has_state ? p->d_out : p->d_psi0;
+  for (int ax = 0; ax < 3; ++ax) a.tw[ax] = ax < p->ndim ? p->d_tw64[ax] : nullptr;
+  cudaError_t err = launch_x_n<double>(a.nx, kFwd0, a, p->xblocks, st);
+  if (err == cudaSuccess)
+    err = launch_axis<double>(a.ny, kFwd, false, a, 1, (long)(a.nx / kTile) * a.nz, st);
+  if (err == cudaSuccess && p->ndim > 2)
+    err = launch_axis<double>(a.nz, kFwd, false, a, 2, (long)(a.nx / kTile) * a.ny, st);
+  if (err != cudaSuccess) return set_cuda_error("energy transform", err);
+  nd_energy_kernel<<<nb, 256, 0, st>>>(a.psi_start, p->d_vpot, p->d_khat, p->d_tcp, n,
+                                       1.0 / (double)n, p->d_epart);
+  csum_kernel<<<1, 1, 0, st>>>(p->d_epart, nb, 0, 0, p->d_epart + nb);
+  ND_CK(cudaGetLastError());
+  double2 h;
+  ND_CK(cudaMemcpyAsync(&h, p->d_epart + nb, sizeof h, cudaMemcpyDeviceToHost, st));
+  ND_CK(cudaStreamSynchronize(st));
+  *e = h.x;
+  *norm = h.y;
   return ESPEC_OK;
 }
 
@@ -832,8 +980,9 @@ extern "C" int espec_spond_results(espec_spond_plan* p, double* c_re, double* c_
 
 extern "C" void espec_spond_destroy(espec_spond_plan* p) {
   if (!p) return;
-  void* b[] = {p->d_psi, p->d_psi0, p->d_out, p->d_vpot, p->d_vabc, p->d_tab, p->d_kq,
-               p->d_cpart, p->d_c, p->d_tw[0], p->d_tw[1], p->d_tw[2]};
+  void* b[] = {p->d_psi,    p->d_psi0,  p->d_out,   p->d_vpot,  p->d_vabc,   p->d_tab,
+               p->d_kq,     p->d_cpart, p->d_c,     p->d_tw[0], p->d_tw[1],  p->d_tw[2],
+               p->d_khat,   p->d_tcp,   p->d_epart, p->d_tw64[0], p->d_tw64[1], p->d_tw64[2]};
   for (void* x : b)
     if (x) cudaFree(x);
   delete p;

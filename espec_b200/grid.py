@@ -111,6 +111,19 @@ class SpoGrid:
         N.check(N.load().espec_spond_run(self._h, int(nsteps), stream), "espec_spond_run")
         self.nsteps = int(nsteps)
 
+    def advance(self, nsteps, stream=None):
+        """nsteps more steps from the state of the last run (sample 0 unset)."""
+        N.check(N.load().espec_spond_continue(self._h, int(nsteps), stream),
+                "espec_spond_continue")
+        self.nsteps = int(nsteps)
+
+    def energies(self, stream=None):
+        """(EFFT4 energy, sum |psi|^2) of the current state, FP64."""
+        e, nr = C.c_double(), C.c_double()
+        N.check(N.load().espec_spond_energies(self._h, C.byref(e), C.byref(nr), stream),
+                "espec_spond_energies")
+        return e.value, nr.value
+
     def results(self, stream=None):
         ns = self.nsteps
         cr, ci = np.zeros(ns + 1), np.zeros(ns + 1)

@@ -61,12 +61,14 @@ extern "C" {
  * Fortran-callable drop-ins (1D).  Same arguments, same outputs and the
  * same printed partial auto-correlation table as the reference routines;
  * the defects of the reference's arithmetic are reproduced.  A case the GPU
- * path does not run (PSPOFFT/PSODFFT: DIM other than '.1D' or an unsupported
- * N; PLNZ: order above 16) or a device error sets INFO = 2 (message on
+ * path does not run (PSPOFFT: unsupported grid sizes; PSODFFT: DIM other
+ * than '.1D' or an unsupported N; PLNZ: order above 16) or a device error sets INFO = 2 (message on
  * standard error).  Work arrays, XI, XF, VAR, ABSTOL and IWORK are accepted
  * and not touched.
  * ---------------------------------------------------------------------- */
-/* replaces SUBROUTINE PSPOFFT (pspofft.f:1-3; called from espec.f:1474) */
+/* replaces SUBROUTINE PSPOFFT (pspofft.f:1-3; called from espec.f:1474), 1D
+ * (espec_spo_* plan) and 2D/3D (espec_spond_* plan, the reference's N-D
+ * kinetic table) */
 void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
               const char* tpabsor, int* info, const int* lc, const int* mp,
               const int* mpi, const int* mpr, const int* mxdct, const int* n,
@@ -257,6 +259,11 @@ int espec_spond_load(espec_spond_plan* plan, const double* vpot, const double* v
 int espec_spond_run(espec_spond_plan* plan, int nsteps, void* stream);
 int espec_spond_results(espec_spond_plan* plan, double* c_re, double* c_im, double* psi_re,
                         double* psi_im, int where, void* stream);
+/* nsteps more steps from psi of the last run; sample 0 is not written */
+int espec_spond_continue(espec_spond_plan* plan, int nsteps, void* stream);
+/* EFFT4 (eigenergfft.f:58-100) and sum |psi|^2 of the current state (psi0
+ * before any run), FP64 on the GPU */
+int espec_spond_energies(espec_spond_plan* plan, double* e, double* norm, void* stream);
 void espec_spond_destroy(espec_spond_plan* plan);
 
 /* ----------------------------------------------------------------------

@@ -164,12 +164,12 @@ def test_dropin_rejects_what_it_does_not_run(capfd):
     n = case["np"][0]
     lnzvc = np.zeros((8, 3), order="F")
     u1, v1, tc = np.array(case["psi"]), np.zeros(n), np.zeros(n)
-    info = F.pspofft(absorb=False, dim=".2D", prtcrl=".NO", tpabsor=".NONE", lc=1, mpi=3, mpr=2,
+    info = F.pspofft(absorb=False, dim=".4D", prtcrl=".NO", tpabsor=".NONE", lc=1, mpi=3, mpr=2,
                      mxdct=8, n=n, dt=case["dt"], ti=0.0, tf=case["dt"], tol=1.0, np_=[n],
                      sh=case["sh"], sm=case["sm"], u1=u1, v1=v1, tc=tc, vpot=case["vpot"],
                      vabc=None, lnzvc=lnzvc)
     _, err = capfd.readouterr()
-    assert info == 2 and "1D" in err
+    assert info == 2 and "DIM" in err
     assert np.array_equal(u1, case["psi"]) and not lnzvc.any()
 
 
@@ -306,3 +306,43 @@ def test_plnz_order_messages_match_executable(capfd, change):
                                                        1.01e-7, 1.01e-8, 1.01e-6])), (h, w)
         else:
             assert h == w
+
+
+def test_pspofft_2d_golden_deck(oracle, capfd):
+    """PSPOFFT with DIM = '.2D' on the 32x32 coupled-Morse golden deck: the
+    reference's 2D kinetic table and in-place multiply, LNZVC, psi, TC and the
+    printed rows against the oracle and the executable."""
+    case = G.setup_case("morse2d_spo")
+    capfd.readouterr()
+    n = int(np.prod(case["np"]))
+    nsteps = 2 * int(round((case["tf"] - case["ti"]) / case["dt"])) + 4
+    lnzvc = np.zeros((nsteps + 4, 4), order="F")
+    u1, v1, tc = np.array(case["psi"], dtype=np.float64), np.zeros(n), np.zeros(n)
+    info = F.pspofft(absorb=False, dim=".2D", prtcrl=".PARTIAL", tpabsor=".NONE", lc=case["lc"],
+                     mpi=3, mpr=2, mxdct=nsteps + 4, n=n, dt=case["dt"], ti=case["ti"],
+                     tf=case["tf"], tol=case["tol"], np_=case["np"], sh=case["sh"], sm=case["sm"],
+                     u1=u1, v1=v1, tc=tc, vpot=case["vpot"], vabc=None, lnzvc=lnzvc)
+    out, err = capfd.readouterr()
+    assert err == ""
+    ref = G.run_oracle(case, case["ref_quirks"], prtcrl=oracle.PRT_PARTIAL)
+    assert info == ref["info"]
+    nc = ref["nc"]
+    assert np.max(np.abs(lnzvc[:nc, 1] - ref["c"].real)) <= 1e-10
+    assert np.max(np.abs(lnzvc[:nc, 2] - ref["c"].imag)) <= 1e-10
+    assert np.max(np.abs(u1 - ref["u"])) <= 1e-10 and np.max(np.abs(v1 - ref["v"])) <= 1e-10
+    npa = np.array(case["np"] + [1], dtype=np.int32)
+    import ctypes as C
+    tref, bb = np.zeros(n), C.c_double()
+    oracle.lib().orc_digt(2, oracle._ip(npa), oracle._p(oracle.f64(case["sh"] + [1.0])),
+                          oracle._p(oracle.f64(case["sm"] + [1.0])), oracle._p(tref),
+                          C.byref(bb), case["ref_quirks"])
+    assert np.array_equal(tc, tref)
+    rows, _ = parse_table(out)
+    assert rows.shape == ref["rows"].shape
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(ref["rows"][:, 1]))) - 5)
+    d = np.abs(rows - ref["rows"])
+    assert np.all(d[:, [0, 2, 3, 4, 5]] <= np.array([5e-9, 5e-8, 5e-8, 5e-9, 5e-7]) + 1e-10)
+    assert np.all(d[:, 1] <= 0.5 * e_ulp * 1.001)
+    gold = case["data"]["rows"]
+    dg = np.abs(rows - gold)
+    assert np.max(dg[:, [2, 3]]) <= 4e-6  # the oracle's pin to the executable on this deck
