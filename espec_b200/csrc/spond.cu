@@ -32,7 +32,7 @@ namespace espec {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kTile = 8;  // lines per CTA in a strided pass (8 warps)
+constexpr int kMaxWarps = 8;  // lines per CTA (one warp each); fewer on small grids
 
 template <typename R>
 __device__ __forceinline__ cpx<R> cmul(cpx<R> a, cpx<R> b) {
@@ -226,9 +226,10 @@ enum { kFirst = 0, kMid = 1, kLast = 2, kFwd0 = 3 };
 template <typename R, int P, int MODE>
 __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
   constexpr int N = 32 * P;
-  __shared__ double2 s_c[8];
+  __shared__ double2 s_c[kMaxWarps];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const long row = (long)blockIdx.x * 8 + warp;
+  const int nw = blockDim.x >> 5;
+  const long row = (long)blockIdx.x * nw + warp;
   const long nrows = (long)a.ny * a.nz;
   WarpFft<R, P> fft;
   fft.init(a.tw[0]);
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
   __syncthreads();
   if (threadIdx.x == 0 && a.cpart) {
     double sr = 0.0, si = 0.0;
-    for (int i = 0; i < 8; ++i) {
+    for (int i = 0; i < nw; ++i) {
       sr += s_c[i].x;
       si += s_c[i].y;
     }
@@ -320,12 +321,13 @@ __global__ void nd_energy_kernel(const double2* psi, const double* vpot, const c
 
 enum { kFwd = 0, kInv = 1, kKin = 2 };
 
-// strided pass along axis 1 (y) or 2 (z): CTA = 8 adjacent x columns of one
-// line set, staged through shared memory; warp w transforms column w
+// strided pass along axis 1 (y) or 2 (z): CTA = blockDim/32 adjacent x columns
+// of one line set, staged through shared memory; warp w transforms column w
 template <typename R, int P, int MODE, bool QUIRK>
 __global__ void __launch_bounds__(256) axis_pass(NdArgs<R> a, int axis) {
   constexpr int N = 32 * P;
   extern __shared__ __align__(16) unsigned char sm_raw[];
+  const int kTile = blockDim.x >> 5;  // adjacent x columns per CTA, one warp each
   cpx<R>* tile = reinterpret_cast<cpx<R>*>(sm_raw);  // [N][kTile + 1]
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ntx = a.nx / kTile;
@@ -621,13 +623,23 @@ int build_tables(espec_spond_plan* p, cudaStream_t st) {
   return ESPEC_OK;
 }
 
+// warps per CTA: 8, or fewer when that leaves SMs idle (2 CTAs per SM wanted)
+int warps_for(long lines) {
+  int w = kMaxWarps;
+  while (w > 1 && lines / w < 2 * 148) w /= 2;
+  return w;
+}
+
 template <typename R, int P>
 cudaError_t launch_x(int mode, const NdArgs<R>& a, int blocks, cudaStream_t st) {
+  const long rows = (long)a.ny * a.nz;
+  const int w = warps_for(rows);
+  blocks = (int)((rows + w - 1) / w);
   switch (mode) {
-    case kFirst: x_pass<R, P, kFirst><<<blocks, 256, 0, st>>>(a); break;
-    case kMid: x_pass<R, P, kMid><<<blocks, 256, 0, st>>>(a); break;
-    case kFwd0: x_pass<R, P, kFwd0><<<blocks, 256, 0, st>>>(a); break;
-    default: x_pass<R, P, kLast><<<blocks, 256, 0, st>>>(a); break;
+    case kFirst: x_pass<R, P, kFirst><<<blocks, 32 * w, 0, st>>>(a); break;
+    case kMid: x_pass<R, P, kMid><<<blocks, 32 * w, 0, st>>>(a); break;
+    case kFwd0: x_pass<R, P, kFwd0><<<blocks, 32 * w, 0, st>>>(a); break;
+    default: x_pass<R, P, kLast><<<blocks, 32 * w, 0, st>>>(a); break;
   }
   return cudaGetLastError();
 }
@@ -644,16 +656,20 @@ cudaError_t launch_x_n(int nx, int mode, const NdArgs<R>& a, int blocks, cudaStr
 }
 
 template <typename R, int P, int MODE, bool Q>
-cudaError_t launch_axis1(const NdArgs<R>& a, int axis, long blocks, cudaStream_t st) {
-  const size_t smem = sizeof(cpx<R>) * 32 * P * (kTile + 1);
+cudaError_t launch_axis1(const NdArgs<R>& a, int axis, long, cudaStream_t st) {
   static bool attr = false;
   if (!attr) {
+    const size_t smax = sizeof(cpx<R>) * 32 * P * (kMaxWarps + 1);
     cudaError_t e = cudaFuncSetAttribute(axis_pass<R, P, MODE, Q>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
     if (e != cudaSuccess) return e;
     attr = true;
   }
-  axis_pass<R, P, MODE, Q><<<(unsigned)blocks, 256, smem, st>>>(a, axis);
+  const long other = axis == 1 ? a.nz : a.ny;  // line sets beside the x tiles
+  const int w = warps_for((long)a.nx * other);
+  const long blocks = (long)(a.nx / w) * other;
+  const size_t smem = sizeof(cpx<R>) * 32 * P * (w + 1);
+  axis_pass<R, P, MODE, Q><<<(unsigned)blocks, 32 * w, smem, st>>>(a, axis);
   return cudaGetLastError();
 }
 
@@ -707,8 +723,7 @@ int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st)
   const bool quirk = (p->quirks & ESPEC_Q_SPO_INPLACE) != 0;
   const int nx = a.nx, ny = a.ny, nz = a.nz;
   const int xb = p->xblocks;
-  const long yb = (long)(nx / kTile) * nz;   // y lines: x tiles x z
-  const long zb = (long)(nx / kTile) * ny;   // z lines: x tiles x y
+  const long yb = 0, zb = 0;  // grid sizes are chosen by the launchers
   cudaError_t e = cudaSuccess;
   auto kin_step = [&]() {
     if (p->ndim == 2) {
@@ -793,7 +808,11 @@ extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* n
   p->precision = precision;
   p->absorb = absorb;
   p->quirks = quirks;
-  p->xblocks = (int)((p->n / np[0] + 7) / 8);
+  {
+    const long rows = p->n / np[0];
+    const int w = warps_for(rows);
+    p->xblocks = (int)((rows + w - 1) / w);  // the x pass's grid (C(t) partials per step)
+  }
   const size_t n = (size_t)p->n;
   const size_t cb = precision == ESPEC_FP64 ? 16 : 8;
   int rc = 0;
@@ -947,9 +966,9 @@ extern "C" int espec_spond_energies(espec_spond_plan* p, double* e, double* norm
   for (int ax = 0; ax < 3; ++ax) a.tw[ax] = ax < p->ndim ? p->d_tw64[ax] : nullptr;
   cudaError_t err = launch_x_n<double>(a.nx, kFwd0, a, p->xblocks, st);
   if (err == cudaSuccess)
-    err = launch_axis<double>(a.ny, kFwd, false, a, 1, (long)(a.nx / kTile) * a.nz, st);
+    err = launch_axis<double>(a.ny, kFwd, false, a, 1, 0, st);
   if (err == cudaSuccess && p->ndim > 2)
-    err = launch_axis<double>(a.nz, kFwd, false, a, 2, (long)(a.nx / kTile) * a.ny, st);
+    err = launch_axis<double>(a.nz, kFwd, false, a, 2, 0, st);
   if (err != cudaSuccess) return set_cuda_error("energy transform", err);
   nd_energy_kernel<<<nb, 256, 0, st>>>(a.psi_start, p->d_vpot, p->d_khat, p->d_tcp, n,
                                        1.0 / (double)n, p->d_epart);
