@@ -26,7 +26,7 @@
 namespace espec {
 namespace {
 
-constexpr int kEigThreads = 256;
+constexpr int kEigThreads = 1024;  // 32 warps: enough loads in flight per SM
 constexpr int kEigMaxM = 40;      // NREORT = 40 in lanczsc.f:55
 constexpr int kEigMaxStates = 16;  // locked states held in the reorthogonalisation
 
@@ -104,6 +104,29 @@ __device__ __forceinline__ void cta_sums2(const double (&acc)[MAXV], int e1, int
     double s = 0.0;
     for (int w = 0; w < kEigThreads / 32; ++w) s += ws[w * MAXV + i];
     out[i] = s;
+  }
+  __syncthreads();
+}
+
+// red[q] = <x, Y_q>, q < nl + nlock, with Y_q = L_q (q < nl) or lock_(q-nl):
+// one warp per vector, lanes striding the points (coalesced streams, one per
+// warp); x is read from L1/L2 by every warp
+__device__ __forceinline__ void warp_dots(const double* x, const double* L, int nl,
+                                          const double* lock, int nlock, int n, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int q = warp; q < nl + nlock; q += kEigThreads / 32) {
+    const double* y = q < nl ? L + (long)q * n : lock + (long)(q - nl) * n;
+    double s0 = 0.0, s1 = 0.0;
+    int k = lane;
+    for (; k + 32 < n; k += 64) {
+      s0 += x[k] * y[k];
+      s1 += x[k + 32] * y[k + 32];
+    }
+    for (; k < n; k += 32) s0 += x[k] * y[k];
+    double s = s0 + s1;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) red[q] = s;
   }
   __syncthreads();
 }
@@ -189,16 +212,7 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(EigArgs a) {
     for (int rs = 0; rs < a.maxrest; ++rs) {
       // ---- project the locked states out of v
       if (K > 0) {
-        double acc[kEigMaxStates];
-#pragma unroll
-        for (int j = 0; j < kEigMaxStates; ++j) acc[j] = 0.0;
-        for (int k = t; k < n; k += kEigThreads) {
-          const double vk = v[k];
-#pragma unroll
-          for (int j = 0; j < kEigMaxStates; ++j)
-            if (j < K) acc[j] += lock[(long)j * n + k] * vk;
-        }
-        cta_sums<kEigMaxStates>(acc, K, ws, red);
+        warp_dots(v, nullptr, 0, lock, K, n, red);
         for (int k = t; k < n; k += kEigThreads) {
           double vk = v[k];
           for (int j = 0; j < K; ++j) vk -= red[j] * lock[(long)j * n + k];
@@ -238,23 +252,12 @@ __global__ void __launch_bounds__(kEigThreads) eig_kernel(EigArgs a) {
         // states and L_0..L_it (reort.f:65-80: all dot products, then all
         // updates): one pass for the dots, one for the updates and the norm
         const double al = s_al[it];
-        double acc[NV];
-#pragma unroll
-        for (int i = 0; i < NV; ++i) acc[i] = 0.0;
-        for (int k = t; k < n; k += kEigThreads) {
-          const double w = work[k] - al * Li[k];
-          work[k] = w;
-#pragma unroll
-          for (int q = 0; q < kEigMaxM; ++q)
-            if (q <= it) acc[q] += w * L[(long)q * n + k];
-#pragma unroll
-          for (int j = 0; j < kEigMaxStates; ++j)
-            if (j < K) acc[kEigMaxM + j] += w * lock[(long)j * n + k];
-        }
-        cta_sums2<NV>(acc, it + 1, kEigMaxM, kEigMaxM + K, ws, red);
+        for (int k = t; k < n; k += kEigThreads) work[k] = work[k] - al * Li[k];
+        __syncthreads();
+        warp_dots(work, L, it + 1, lock, K, n, red);
         if (t == 0) {
           for (int q = 0; q <= it; ++q) s_r[q] = red[q];
-          for (int j = 0; j < K; ++j) s_lk[j] = red[kEigMaxM + j];
+          for (int j = 0; j < K; ++j) s_lk[j] = red[it + 1 + j];
         }
         __syncthreads();
         double nn[1] = {0.0};
