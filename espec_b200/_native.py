@@ -39,6 +39,7 @@ EXPORTS = [
     "espec_mlp_colsum", "espec_mlp_mse", "espec_mlp_adam", "espec_outer_basis", "espec_convert",
     "espec_mlp_adam_dev", "espec_spond_create", "espec_spond_load", "espec_spond_run",
     "espec_spond_results", "espec_spond_destroy", "espec_spond_continue", "espec_spond_energies",
+    "espec_spond_create_method", "espec_spond_previous",
 ]
 
 
@@ -126,6 +127,8 @@ def load():
     lib.espec_spond_run.argtypes = [vp, ci, vp]
     lib.espec_spond_results.argtypes = [vp, vp, vp, vp, vp, ci, vp]
     lib.espec_spond_continue.argtypes = [vp, ci, vp]
+    lib.espec_spond_create_method.argtypes = [C.POINTER(vp), ci, ci, i, d, d, cd, ci, ci, ci]
+    lib.espec_spond_previous.argtypes = [vp, vp, vp, ci, vp]
     lib.espec_spond_energies.argtypes = [vp, vp, vp, vp]
     lib.espec_spond_destroy.argtypes = [vp]
     lib.espec_spond_destroy.restype = None

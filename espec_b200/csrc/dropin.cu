@@ -1,5 +1,5 @@
 // dropin.cu -- Fortran-callable drop-ins for eSPec's propagators PSPOFFT
-// (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D) and PLNZ
+// (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D/2D/3D) and PLNZ
 // (plnz.f:1-155; 1D/2D/3D).
 //
 // Each call propagates one packet on the GPU through a one-packet plan and
@@ -16,8 +16,8 @@
 // multiply of spofft.f:150-153 and the never-applied .SMOOTHW mask of
 // sodfft.f:108, and PLNZ's cos-before-sin of sil.f:145-148.  Cases the GPU
 // path does not cover (PSPOFFT: 1D sizes other than 256..4096 of the form 2^k
-// or 3*2^k, 2D/3D axes other than 32..512 powers of two; PSODFFT: DIM other
-// than '.1D'; PLNZ: order above 16) and
+// or 3*2^k, 2D/3D axes other than 32..512 powers of two; PSODFFT: 1D sizes
+// above 2048; PLNZ: order above 16) and
 // device errors set INFO = 2 and write the reason to standard error; nothing
 // is computed on the CPU.
 #include <cuda_runtime.h>
@@ -264,18 +264,19 @@ struct FftDropIn : DropIn {
     espec_spond_destroy(nd);
   }
 
-  int setup_nd(int ndim, const char* tpabsor, size_t tpabsor_len, const int* np, const double* sh,
-               const double* sm, double* tc, const double* vpot, const double* vabc,
-               const double* u, const double* v) {
+  int setup_nd(int method, int ndim, const char* tpabsor, size_t tpabsor_len, const int* np,
+               const double* sh, const double* sm, double* tc, const double* vpot,
+               const double* vabc, const double* u, const double* v) {
     long npts = 1;
     for (int a = 0; a < ndim; ++a) npts *= np[a];
     if (npts != n) return fail("N differs from the product of NP");
     if (lc < 1) return fail("LC must be at least 1");
     // DIGT for 2D/3D as the reference computes it (dkeft.f:80-137)
-    const int quirks = ESPEC_Q_SPO_INPLACE | ESPEC_Q_DIGT_ND;
+    const int quirks = ESPEC_Q_DIGT_ND |
+                       (method == ESPEC_SPO ? ESPEC_Q_SPO_INPLACE : ESPEC_Q_SOD_SMOOTHW);
     espec::digt_nd_table(ndim, np, sh, sm, quirks, tc);
     const int ab = absorber(absorb, tpabsor, tpabsor_len);
-    if (espec_spond_create(&nd, ndim, np, sh, sm, dt, ESPEC_FP64, ab, quirks) ||
+    if (espec_spond_create_method(&nd, method, ndim, np, sh, sm, dt, ESPEC_FP64, ab, quirks) ||
         espec_spond_load(nd, vpot, ab == ESPEC_ABS_NONE ? nullptr : vabc, u, v, ESPEC_MEM_HOST,
                          nullptr))
       return fail_lib();
@@ -297,10 +298,7 @@ struct FftDropIn : DropIn {
             const int* np, const double* sh, const double* sm, double* tc, const double* vpot,
             const double* vabc, const double* u, const double* v) {
     const int ndim = fstr_is(dim, dim_len, ".2D") ? 2 : (fstr_is(dim, dim_len, ".3D") ? 3 : 1);
-    if (ndim > 1) {
-      if (method != ESPEC_SPO) return fail("2D/3D runs on the GPU for PSPOFFT only");
-      return setup_nd(ndim, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u, v);
-    }
+    if (ndim > 1) return setup_nd(method, ndim, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u, v);
     if (!fstr_is(dim, dim_len, ".1D")) return fail("DIM must be '.1D', '.2D' or '.3D'");
     if (np[0] != n) return fail("N differs from NP(1)");
     if (lc < 1) return fail("LC must be at least 1");
@@ -407,8 +405,12 @@ extern "C" void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
   double et, fnt;
   if (d.energies(et, fnt)) return;
   d.drift(et, fnt);
-  if (espec_spo_results(d.plan, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
-      espec_prop_previous(d.plan, u1, v1, ESPEC_MEM_HOST, nullptr)) {
+  const bool bad =
+      d.nd ? (espec_spond_results(d.nd, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
+              espec_spond_previous(d.nd, u1, v1, ESPEC_MEM_HOST, nullptr))
+           : (espec_spo_results(d.plan, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
+              espec_prop_previous(d.plan, u1, v1, ESPEC_MEM_HOST, nullptr));
+  if (bad) {
     d.fail_lib();
     return;
   }

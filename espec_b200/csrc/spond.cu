@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "cplx.cuh"
@@ -211,6 +212,14 @@ struct NdArgs {
   double2* cpart;         // C(t) partial sums [step][x-pass CTA]
   const typename Rot<R>::type* tw[3];  // W_n^k tables of the x, y, z line lengths
   int step;
+  // second-order differences (psodfft.f / sodfft.f:64-126): dst <- dst - i f
+  // (vc src + T src) [+ f ab src, or times the mask], natural order
+  const double2* sod_src;
+  double2* sod_dst;
+  const double* vc;   // CST V
+  const double* ab;   // CST VABC (.VOPTIC) or the .SMOOTHW mask
+  double f;
+  int kabs;           // 0 none, 1 complex potential, 2 mask
 };
 
 // W_n^k = exp(-2 pi i k / n), k < n, in the form the line transforms apply
@@ -220,7 +229,7 @@ __global__ void tw_table_kernel(typename Rot<R>::type* tab, int n) {
   if (k < n) tab[k] = twid<R>(k, n);
 }
 
-enum { kFirst = 0, kMid = 1, kLast = 2, kFwd0 = 3 };
+enum { kFirst = 0, kMid = 1, kLast = 2, kFwd0 = 3, kSodUpd = 4 };
 
 // x pass: one warp per row, 8 rows per CTA
 template <typename R, int P, int MODE>
@@ -246,6 +255,31 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
         cr += p.x * p.x + p.y * p.y;  // C(0) = <psi0|psi0> (not used when resuming)
         v[j] = apply_ph(a.h[x], mk((R)p.x, (R)p.y));
       }
+    } else if (MODE == kSodUpd) {
+      // T src by the inverse of the transformed copy, then the leapfrog update
+#pragma unroll
+      for (int j = 0; j < P; ++j) v[j] = a.psi[base + 32 * j + lane];
+      fft.inverse(v);
+#pragma unroll
+      for (int j = 0; j < P; ++j) {
+        const long x = base + 32 * j + lane;
+        const double2 sj = a.sod_src[x], dj = a.sod_dst[x];
+        const double vc = a.vc[x];
+        const double hx = fma(vc, sj.x, (double)v[j].x), hy = fma(vc, sj.y, (double)v[j].y);
+        double ox = fma(a.f, hy, dj.x), oy = fma(-a.f, hx, dj.y);
+        if (a.kabs == 1) {
+          const double abf = a.f * a.ab[x];
+          ox = fma(abf, sj.x, ox);
+          oy = fma(abf, sj.y, oy);
+        } else if (a.kabs == 2) {
+          ox *= a.ab[x];
+          oy *= a.ab[x];
+        }
+        a.sod_dst[x] = make_double2(ox, oy);
+        const double2 wj = a.w[x];  // conj(psi0)
+        cr += wj.x * ox - wj.y * oy;
+        ci += wj.x * oy + wj.y * ox;
+      }
     } else if (MODE == kFwd0) {  // plain forward transform of a natural-order state
 #pragma unroll
       for (int j = 0; j < P; ++j) {
@@ -265,7 +299,9 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
         v[j] = apply_ph(MODE == kLast ? a.hm[x] : a.g[x], v[j]);
       }
     }
-    if (MODE == kLast) {
+    if (MODE == kSodUpd) {
+      // written above
+    } else if (MODE == kLast) {
 #pragma unroll
       for (int j = 0; j < P; ++j)
         a.psi_out[base + 32 * j + lane] = make_double2((double)v[j].x, (double)v[j].y);
@@ -290,6 +326,32 @@ __global__ void __launch_bounds__(256) x_pass(NdArgs<R> a) {
     }
     a.cpart[(long)a.step * gridDim.x + blockIdx.x] = make_double2(sr, si);
   }
+}
+
+// C(0) = sum |psi0|^2 as x-pass-shaped partials (nb blocks)
+__global__ void c0_kernel(const double2* psi0, long n, double2* part) {
+  __shared__ double red[256];
+  const long lo = n * blockIdx.x / gridDim.x, hi = n * (blockIdx.x + 1) / gridDim.x;
+  double s = 0.0;
+  for (long i = lo + threadIdx.x; i < hi; i += blockDim.x) s += psi0[i].x * psi0[i].x + psi0[i].y * psi0[i].y;
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = make_double2(red[0], 0.0);
+}
+
+// SOD tables: vc = CST V, ab = CST VABC or the mask, w = conj(psi0)
+__global__ void sod_setup_nd_kernel(long n, const double* vpot, const double* vabc, int kabs,
+                                    double cst, const double2* psi0, double* vc, double* ab,
+                                    double2* w) {
+  const long x = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (x >= n) return;
+  vc[x] = cst * vpot[x];
+  ab[x] = kabs == 1 ? cst * vabc[x] : (kabs == 2 ? vabc[x] : 0.0);
+  w[x] = make_double2(psi0[x].x, -psi0[x].y);
 }
 
 // EFFT4 (eigenergfft.f:58-100) and the norm of a natural-order state psi
@@ -438,7 +500,9 @@ struct espec_spond_plan {
   long n = 0;
   double sh[3] = {1, 1, 1}, sm[3] = {1, 1, 1};
   double dt_fs = 0.0;
-  int precision = ESPEC_FP64, absorb = 0, quirks = 0;
+  int precision = ESPEC_FP64, absorb = 0, quirks = 0, method = ESPEC_SPO;
+  double2* d_prev = nullptr;  // SOD: psi(t - dt), natural order
+  double* d_sod = nullptr;    // SOD: vc, ab (n each)
   bool loaded = false;
   void* d_psi = nullptr;      // cpx<R> state
   double2* d_psi0 = nullptr;
@@ -569,14 +633,29 @@ inline cpx<double> k_factor(double th, long n, double) {
   return mk(std::cos(th) / n, -std::sin(th) / n);
 }
 inline PhF k_factor(double th, long n, float) { return make_phf(-th, 1.0 / n); }
+inline cpx<double> k_real(double v, double) { return mk(v, 0.0); }
+inline PhF k_real(double v, float) { return make_phf(0.0, v); }
+
+inline int sod_kabs(const espec_spond_plan* p) {
+  if (p->absorb == ESPEC_ABS_VOPTIC) return 1;
+  if (p->absorb == ESPEC_ABS_SMOOTHW && !(p->quirks & ESPEC_Q_SOD_SMOOTHW)) return 2;
+  return 0;  // sodfft.f:108 compares 7 characters with '.SMOOTHW': never true
+}
 
 template <typename R>
 int build_tables(espec_spond_plan* p, cudaStream_t st) {
   const long n = p->n;
   NdTabs<R> tb(p->d_tab, n);
   const double cst1 = p->dt_fs / ESPEC_SHFS, cst2 = p->dt_fs / (2.0 * ESPEC_SHFS);
-  nd_setup_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
-      n, p->d_vpot, p->d_vabc, p->absorb, cst2, p->d_psi0, tb.g, tb.h, tb.hm, tb.w);
+  const bool sod = p->method == ESPEC_SOD;
+  const double cst_sod = 2.0 * p->dt_fs / ESPEC_SHFS;  // psodfft.f:81
+  if (sod) {
+    sod_setup_nd_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        n, p->d_vpot, p->d_vabc, sod_kabs(p), cst_sod, p->d_psi0, p->d_sod, p->d_sod + n, tb.w);
+  } else {
+    nd_setup_kernel<R><<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+        n, p->d_vpot, p->d_vabc, p->absorb, cst2, p->d_psi0, tb.g, tb.h, tb.hm, tb.w);
+  }
   ND_CK(cudaGetLastError());
   // kinetic factors in the kinetic pass's layout: line (x position, other
   // position), position along the kinetic axis; frequencies mirrored to the
@@ -606,7 +685,11 @@ int build_tables(espec_spond_plan* p, cudaStream_t st) {
       else idx = fx + (size_t)nx * (fy2 + (size_t)ny * fk);
       const double th = cst1 * tc[idx];
       const size_t o = (size_t)line * nk + pos;
-      K[o] = k_factor(th, n, R(0));
+      if (sod) {
+        K[o] = k_real(cst_sod * tc[idx] / n, R(0));  // CST TC B (sodfft.f:100-104,119)
+      } else {
+        K[o] = k_factor(th, n, R(0));
+      }
       if (quirk) {
         qc[o] = std::cos(th);
         qs[o] = std::sin(th);
@@ -639,7 +722,14 @@ cudaError_t launch_x(int mode, const NdArgs<R>& a, int blocks, cudaStream_t st) 
     case kFirst: x_pass<R, P, kFirst><<<blocks, 32 * w, 0, st>>>(a); break;
     case kMid: x_pass<R, P, kMid><<<blocks, 32 * w, 0, st>>>(a); break;
     case kFwd0: x_pass<R, P, kFwd0><<<blocks, 32 * w, 0, st>>>(a); break;
-    default: x_pass<R, P, kLast><<<blocks, 32 * w, 0, st>>>(a); break;
+    case kSodUpd:
+      if constexpr (sizeof(R) == 8) {
+        x_pass<R, P, kSodUpd><<<blocks, 32 * w, 0, st>>>(a);
+        break;
+      }
+      return cudaErrorInvalidValue;  // SOD plans are FP64
+    case kLast: x_pass<R, P, kLast><<<blocks, 32 * w, 0, st>>>(a); break;
+    default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
 }
@@ -757,6 +847,71 @@ int run_steps(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st)
   return ESPEC_OK;
 }
 
+// second-order differences on the grid (psodfft.f:77-206): start-up of two
+// half steps from psi0 (psodfft.f:120-152), then leapfrog steps; the newest
+// state ends in d_out, the one before in d_prev
+int run_sod(espec_spond_plan* p, int nsteps, bool from_start, cudaStream_t st) {
+  NdArgs<double> a{};
+  a.nx = p->np[0];
+  a.ny = p->np[1];
+  a.nz = p->ndim > 2 ? p->np[2] : 1;
+  a.ndim = p->ndim;
+  a.psi = (cpx<double>*)p->d_psi;  // transform scratch
+  const long n = p->n;
+  NdTabs<double> tb(p->d_tab, n);
+  a.w = tb.w;
+  a.K = tb.K;
+  a.vc = p->d_sod;
+  a.ab = p->d_sod + n;
+  a.kabs = sod_kabs(p);
+  a.cpart = p->d_cpart;
+  for (int ax = 0; ax < 3; ++ax) a.tw[ax] = ax < p->ndim ? (const RotD*)p->d_tw[ax] : nullptr;
+  const int nx = a.nx, ny = a.ny, nz = a.nz;
+  cudaError_t e = cudaSuccess;
+  auto op = [&](const double2* src, double2* dst, double f, int step) {
+    a.step = step;
+    a.psi_start = src;
+    e = launch_x_n<double>(nx, kFwd0, a, 0, st);
+    if (e != cudaSuccess) return;
+    if (p->ndim == 2) {
+      e = launch_axis<double>(ny, kKin, false, a, 1, 0, st);
+    } else {
+      e = launch_axis<double>(ny, kFwd, false, a, 1, 0, st);
+      if (e == cudaSuccess) e = launch_axis<double>(nz, kKin, false, a, 2, 0, st);
+      if (e == cudaSuccess) e = launch_axis<double>(ny, kInv, false, a, 1, 0, st);
+    }
+    if (e != cudaSuccess) return;
+    a.sod_src = src;
+    a.sod_dst = dst;
+    a.f = f;
+    e = launch_x_n<double>(nx, kSodUpd, a, 0, st);
+  };
+  double2* cur = p->d_out;
+  double2* prev = p->d_prev;
+  int s0 = 1;
+  if (from_start) {
+    ND_CK(cudaMemcpyAsync(cur, p->d_psi0, 16 * n, cudaMemcpyDeviceToDevice, st));
+    ND_CK(cudaMemcpyAsync(prev, p->d_psi0, 16 * n, cudaMemcpyDeviceToDevice, st));
+    c0_kernel<<<p->xblocks, 256, 0, st>>>(p->d_psi0, n, p->d_cpart);
+    ND_CK(cudaGetLastError());
+    if (nsteps >= 1) {
+      op(cur, prev, 0.5, 1);  // prev = psi0 - i/2 H psi0
+      if (e == cudaSuccess) op(prev, cur, 0.5, 1);  // cur = psi0 - i/2 H prev = psi(dt)
+      if (e != cudaSuccess) return set_cuda_error("SOD start-up", e);
+      ND_CK(cudaMemcpyAsync(prev, p->d_psi0, 16 * n, cudaMemcpyDeviceToDevice, st));
+    }
+    s0 = 2;
+  }
+  for (int s = s0; s <= nsteps; ++s) {
+    op(cur, prev, 1.0, s);
+    if (e != cudaSuccess) return set_cuda_error("SOD step", e);
+    std::swap(cur, prev);
+  }
+  p->d_out = cur;
+  p->d_prev = prev;
+  return ESPEC_OK;
+}
+
 }  // namespace
 
 namespace espec {
@@ -779,10 +934,17 @@ void digt_nd_table(int ndim, const int* np, const double* sh, const double* sm, 
 }
 }  // namespace espec
 
-extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* np,
-                                  const double* sh, const double* sm, double dt_fs,
-                                  int precision, int absorb, int quirks) {
+extern "C" int espec_spond_create_method(espec_spond_plan** out, int method, int ndim,
+                                         const int* np, const double* sh, const double* sm,
+                                         double dt_fs, int precision, int absorb, int quirks) {
   if (!out || !np || !sh || !sm) return set_error(ESPEC_EINVAL, "null argument");
+  if (method != ESPEC_SPO && method != ESPEC_SOD)
+    return set_error(ESPEC_EINVAL, "method must be ESPEC_SPO or ESPEC_SOD");
+  if (method == ESPEC_SOD && precision != ESPEC_FP64)
+    return set_error(ESPEC_EINVAL, "the SOD propagator runs in FP64");
+  const int allowed = method == ESPEC_SOD ? (ESPEC_Q_SOD_SMOOTHW | ESPEC_Q_DIGT_ND)
+                                          : (ESPEC_Q_SPO_INPLACE | ESPEC_Q_DIGT_ND);
+  if (quirks & ~allowed) return set_error(ESPEC_EINVAL, "quirk not applicable to this method");
   if (ndim != 2 && ndim != 3) return set_error(ESPEC_EINVAL, "ndim must be 2 or 3");
   for (int a = 0; a < ndim; ++a)
     if (!line_ok(np[a]))
@@ -791,11 +953,10 @@ extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* n
     return set_error(ESPEC_EINVAL, "precision must be ESPEC_FP64 or ESPEC_MIXED");
   if (absorb < ESPEC_ABS_NONE || absorb > ESPEC_ABS_SMOOTHW)
     return set_error(ESPEC_EINVAL, "unknown absorber type");
-  if (quirks & ~(ESPEC_Q_SPO_INPLACE | ESPEC_Q_DIGT_ND))
-    return set_error(ESPEC_EINVAL, "quirk not applicable to the N-D split operator");
   if ((quirks & ESPEC_Q_SPO_INPLACE) && precision != ESPEC_FP64)
     return set_error(ESPEC_EINVAL, "the reference-defect mode exists for FP64 only");
   auto* p = new espec_spond_plan;
+  p->method = method;
   p->ndim = ndim;
   p->n = 1;
   for (int a = 0; a < ndim; ++a) {
@@ -817,8 +978,9 @@ extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* n
   const size_t cb = precision == ESPEC_FP64 ? 16 : 8;
   int rc = 0;
   auto fail = [&](int code) {
-    void* b[] = {p->d_psi, p->d_psi0, p->d_out, p->d_vpot, p->d_vabc, p->d_tab, p->d_kq,
-                 p->d_cpart, p->d_c, p->d_tw[0], p->d_tw[1], p->d_tw[2]};
+    void* b[] = {p->d_psi,   p->d_psi0,  p->d_out,   p->d_vpot,  p->d_vabc, p->d_tab,
+                 p->d_kq,    p->d_cpart, p->d_c,     p->d_tw[0], p->d_tw[1], p->d_tw[2],
+                 p->d_prev,  p->d_sod};
     for (void* x : b)
       if (x) cudaFree(x);
     delete p;
@@ -834,9 +996,34 @@ extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* n
   if ((rc = ck(cudaMalloc(&p->d_tab, tbytes), "cudaMalloc"))) return fail(rc);
   if (quirks & ESPEC_Q_SPO_INPLACE)
     if ((rc = ck(cudaMalloc(&p->d_kq, 16 * n), "cudaMalloc"))) return fail(rc);
+  if (method == ESPEC_SOD) {
+    if ((rc = ck(cudaMalloc(&p->d_prev, 16 * n), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_sod, 16 * n), "cudaMalloc"))) return fail(rc);
+  }
   for (int ax = 0; ax < ndim; ++ax)
     if ((rc = ck(cudaMalloc(&p->d_tw[ax], sizeof(RotD) * np[ax]), "cudaMalloc"))) return fail(rc);
   *out = p;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spond_create(espec_spond_plan** out, int ndim, const int* np,
+                                  const double* sh, const double* sm, double dt_fs,
+                                  int precision, int absorb, int quirks) {
+  return espec_spond_create_method(out, ESPEC_SPO, ndim, np, sh, sm, dt_fs, precision, absorb,
+                                   quirks);
+}
+
+extern "C" int espec_spond_previous(espec_spond_plan* p, double* psi_re, double* psi_im,
+                                    int where, void* stream) {
+  if (!p || p->method != ESPEC_SOD || !p->has_state)
+    return set_error(ESPEC_EINVAL, "previous state exists for run SOD plans only");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t n = (size_t)p->n;
+  if (psi_re) ND_CK(cudaMemcpy2DAsync(psi_re, 8, p->d_prev, 16, 8, n, kind, st));
+  if (psi_im) ND_CK(cudaMemcpy2DAsync(psi_im, 8, (char*)p->d_prev + 8, 16, 8, n, kind, st));
+  if (where == ESPEC_MEM_HOST) ND_CK(cudaStreamSynchronize(st));
   return ESPEC_OK;
 }
 
@@ -886,8 +1073,10 @@ extern "C" int espec_spond_run(espec_spond_plan* p, int nsteps, void* stream) {
     ND_CK(cudaMalloc(&p->d_cpart, sizeof(double2) * ((size_t)nsteps + 1) * p->xblocks));
     p->c_cap = nsteps;
   }
-  const int rc = p->precision == ESPEC_FP64 ? run_steps<double>(p, nsteps, true, st)
-                                            : run_steps<float>(p, nsteps, true, st);
+  const int rc = p->method == ESPEC_SOD
+                     ? run_sod(p, nsteps, true, st)
+                     : (p->precision == ESPEC_FP64 ? run_steps<double>(p, nsteps, true, st)
+                                                   : run_steps<float>(p, nsteps, true, st));
   if (rc) return rc;
   csum_kernel<<<(nsteps + 1 + 255) / 256, 256, 0, st>>>(p->d_cpart, p->xblocks, nsteps, 0,
                                                          p->d_c);
@@ -910,8 +1099,10 @@ extern "C" int espec_spond_continue(espec_spond_plan* p, int nsteps, void* strea
     p->c_cap = nsteps;
   }
   if (nsteps == 0) return ESPEC_OK;
-  const int rc = p->precision == ESPEC_FP64 ? run_steps<double>(p, nsteps, false, st)
-                                            : run_steps<float>(p, nsteps, false, st);
+  const int rc = p->method == ESPEC_SOD
+                     ? run_sod(p, nsteps, false, st)
+                     : (p->precision == ESPEC_FP64 ? run_steps<double>(p, nsteps, false, st)
+                                                   : run_steps<float>(p, nsteps, false, st));
   if (rc) return rc;
   csum_kernel<<<(nsteps + 255) / 256, 256, 0, st>>>(p->d_cpart, p->xblocks, nsteps, 1, p->d_c);
   ND_CK(cudaGetLastError());
@@ -1001,7 +1192,8 @@ extern "C" void espec_spond_destroy(espec_spond_plan* p) {
   if (!p) return;
   void* b[] = {p->d_psi,    p->d_psi0,  p->d_out,   p->d_vpot,  p->d_vabc,   p->d_tab,
                p->d_kq,     p->d_cpart, p->d_c,     p->d_tw[0], p->d_tw[1],  p->d_tw[2],
-               p->d_khat,   p->d_tcp,   p->d_epart, p->d_tw64[0], p->d_tw64[1], p->d_tw64[2]};
+               p->d_khat,   p->d_tcp,   p->d_epart, p->d_tw64[0], p->d_tw64[1], p->d_tw64[2],
+               p->d_prev,   p->d_sod};
   for (void* x : b)
     if (x) cudaFree(x);
   delete p;

@@ -84,6 +84,8 @@ class SpoGrid:
     GPU.  np: points per axis (32..512, powers of two), sh/sm per axis (bohr,
     electron masses), arrays flattened x fastest."""
 
+    method = N.SPO
+
     def __init__(self, np_, sh, sm, dt_fs, precision="fp64", absorb=N.ABS_NONE, quirks=0):
         lib = N.load()
         self.np = [int(x) for x in np_]
@@ -91,12 +93,14 @@ class SpoGrid:
         npa = np.array(self.np, dtype=np.int32)
         sha, sma = N.f64(sh), N.f64(sm)
         self._h = C.c_void_p()
-        rc = lib.espec_spond_create(C.byref(self._h), len(self.np),
-                                    npa.ctypes.data_as(C.POINTER(C.c_int)),
-                                    sha.ctypes.data_as(C.POINTER(C.c_double)),
-                                    sma.ctypes.data_as(C.POINTER(C.c_double)), float(dt_fs),
-                                    {"fp64": N.FP64, "mixed": N.MIXED}[precision], absorb, quirks)
-        N.check(rc, "espec_spond_create")
+        rc = lib.espec_spond_create_method(C.byref(self._h), self.method, len(self.np),
+                                           npa.ctypes.data_as(C.POINTER(C.c_int)),
+                                           sha.ctypes.data_as(C.POINTER(C.c_double)),
+                                           sma.ctypes.data_as(C.POINTER(C.c_double)),
+                                           float(dt_fs),
+                                           {"fp64": N.FP64, "mixed": N.MIXED}[precision], absorb,
+                                           quirks)
+        N.check(rc, "espec_spond_create_method")
         self.nsteps = None
 
     def load(self, vpot, psi, vabc=None, stream=None):
@@ -142,3 +146,20 @@ class SpoGrid:
             self.close()
         except Exception:
             pass
+
+
+class SodGrid(SpoGrid):
+    """Second-order-differences propagation with the FFT kinetic term
+    (PSODFFT, psodfft.f:77-206) on a 2D or 3D grid, FP64; `previous()` is
+    psi(TF - dt)."""
+
+    method = N.SOD
+
+    def __init__(self, np_, sh, sm, dt_fs, absorb=N.ABS_NONE, quirks=0):
+        super().__init__(np_, sh, sm, dt_fs, precision="fp64", absorb=absorb, quirks=quirks)
+
+    def previous(self, stream=None):
+        pr, pi = np.zeros(self.n), np.zeros(self.n)
+        N.check(N.load().espec_spond_previous(self._h, N.ptr(pr), N.ptr(pi), N.MEM_HOST, stream),
+                "espec_spond_previous")
+        return pr + 1j * pi

@@ -61,8 +61,8 @@ extern "C" {
  * Fortran-callable drop-ins (1D).  Same arguments, same outputs and the
  * same printed partial auto-correlation table as the reference routines;
  * the defects of the reference's arithmetic are reproduced.  A case the GPU
- * path does not run (PSPOFFT: unsupported grid sizes; PSODFFT: DIM other
- * than '.1D' or an unsupported N; PLNZ: order above 16) or a device error sets INFO = 2 (message on
+ * path does not run (PSPOFFT/PSODFFT: unsupported grid sizes; PLNZ: order
+ * above 16) or a device error sets INFO = 2 (message on
  * standard error).  Work arrays, XI, XF, VAR, ABSTOL and IWORK are accepted
  * and not touched.
  * ---------------------------------------------------------------------- */
@@ -79,7 +79,8 @@ void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
               const double* vpot, const double* vabc, double* lnzvc,
               double* wrk1, double* wrk2, const double* var, size_t dim_len,
               size_t prtcrl_len, size_t tpabsor_len);
-/* replaces SUBROUTINE PSODFFT (psodfft.f:1-3; called from espec.f:1373) */
+/* replaces SUBROUTINE PSODFFT (psodfft.f:1-3; called from espec.f:1373), 1D
+ * and 2D/3D */
 void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
               const char* tpabsor, int* info, const int* lc, const int* mp,
               const int* mpi, const int* mpr, const int* mxdct, const int* n,
@@ -254,6 +255,15 @@ void espec_grid_destroy(espec_grid_plan* plan);
 typedef struct espec_spond_plan espec_spond_plan;
 int espec_spond_create(espec_spond_plan** plan, int ndim, const int* np, const double* sh,
                        const double* sm, double dt_fs, int precision, int absorb, int quirks);
+/* the same for a method: ESPEC_SPO, or ESPEC_SOD (PSODFFT, psodfft.f:77-206,
+ * sodfft.f:64-126: FP64, two half-step start-up, then leapfrog; quirks
+ * ESPEC_Q_SOD_SMOOTHW, ESPEC_Q_DIGT_ND) */
+int espec_spond_create_method(espec_spond_plan** plan, int method, int ndim, const int* np,
+                              const double* sh, const double* sm, double dt_fs, int precision,
+                              int absorb, int quirks);
+/* SOD plans: psi(TF - dt) of the last run */
+int espec_spond_previous(espec_spond_plan* plan, double* psi_re, double* psi_im, int where,
+                         void* stream);
 int espec_spond_load(espec_spond_plan* plan, const double* vpot, const double* vabc,
                      const double* psi_re, const double* psi_im, int where, void* stream);
 int espec_spond_run(espec_spond_plan* plan, int nsteps, void* stream);

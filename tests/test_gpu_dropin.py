@@ -346,3 +346,45 @@ def test_pspofft_2d_golden_deck(oracle, capfd):
     gold = case["data"]["rows"]
     dg = np.abs(rows - gold)
     assert np.max(dg[:, [2, 3]]) <= 4e-6  # the oracle's pin to the executable on this deck
+
+
+def test_psodfft_2d_golden_deck(oracle, capfd):
+    """PSODFFT with DIM = '.2D' on the 32x32 coupled-Morse golden deck: the
+    reference's 2D kinetic table makes this deck overflow within a few steps
+    (the executable prints NaN from step 2 on); LNZVC follows the oracle
+    relative to the magnitude until the overflow, psi(TF) and psi(TF - dt)
+    have overflowed on both, TC equals the oracle's, and C(t) the finite
+    values the executable printed."""
+    from test_gpu_spond import close_until_overflow
+
+    case = G.setup_case("morse2d_sod")
+    capfd.readouterr()
+    n = int(np.prod(case["np"]))
+    nsteps = 2 * int(round((case["tf"] - case["ti"]) / case["dt"])) + 4
+    lnzvc = np.zeros((nsteps + 4, 4), order="F")
+    u1, v1, tc = np.array(case["psi"], dtype=np.float64), np.zeros(n), np.zeros(n)
+    u2, v2 = np.zeros(n), np.zeros(n)
+    info = F.psodfft(absorb=False, dim=".2D", prtcrl=".PARTIAL", tpabsor=".NONE", lc=case["lc"],
+                     mpi=3, mpr=2, mxdct=nsteps + 4, n=n, dt=case["dt"], ti=case["ti"],
+                     tf=case["tf"], tol=case["tol"], np_=case["np"], sh=case["sh"], sm=case["sm"],
+                     u1=u1, v1=v1, u2=u2, v2=v2, tc=tc, vpot=case["vpot"], vabc=None,
+                     lnzvc=lnzvc)
+    capfd.readouterr()
+    ref = G.run_oracle(case, case["ref_quirks"], prtcrl=oracle.PRT_PARTIAL)
+    assert info == ref["info"]
+    nc = ref["nc"]
+    close_until_overflow(lnzvc[:nc, 1] + 1j * lnzvc[:nc, 2], ref["c"])
+    for got, r in ((u2 + 1j * v2, ref["u"] + 1j * ref["v"]),
+                   (u1 + 1j * v1, ref["u_prev"] + 1j * ref["v_prev"])):
+        assert not np.isfinite(r).any() and not np.isfinite(got).any()
+    npa = np.array(case["np"] + [1], dtype=np.int32)
+    import ctypes as C
+    tref, bb = np.zeros(n), C.c_double()
+    oracle.lib().orc_digt(2, oracle._ip(npa), oracle._p(oracle.f64(case["sh"] + [1.0])),
+                          oracle._p(oracle.f64(case["sm"] + [1.0])), oracle._p(tref),
+                          C.byref(bb), case["ref_quirks"])
+    assert np.array_equal(tc, tref)
+    gold = case["data"]["rows"]
+    ok = np.isfinite(gold[:, 2])
+    rel = np.abs(lnzvc[:nc, 1][ok] - gold[ok, 2]) / np.maximum(1.0, np.abs(gold[ok, 2]))
+    assert rel.max() < 1e-6
