@@ -35,9 +35,10 @@ EXPORTS = [
     "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
     "espec_grid_basis", "plnz_", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
     "spectrumtd_", "espec_eig_solve_dev", "espec_eig_lcg_start", "espec_eig_morse2d",
-    "espec_gemm_f64", "espec_gemm_f32", "espec_mlp_bias_act", "espec_mlp_tanh_back",
-    "espec_mlp_colsum", "espec_mlp_mse", "espec_mlp_adam", "espec_outer_basis", "espec_convert",
-    "espec_mlp_adam_dev", "espec_spond_create", "espec_spond_load", "espec_spond_run",
+    "espec_gemm_f64", "espec_gemm_f32", "espec_gemm_bf16", "espec_gemm_bf16_status",
+    "espec_mlp_bias_gelu", "espec_mlp_gelu_back", "espec_to_bf16", "espec_mlp_adam_bf16",
+    "espec_mlp_colsum", "espec_mlp_mse", "espec_sep_basis", "espec_convert",
+    "espec_spond_create", "espec_spond_load", "espec_spond_run",
     "espec_spond_results", "espec_spond_destroy", "espec_spond_continue", "espec_spond_energies",
     "espec_spond_create_method", "espec_spond_previous",
 ]
@@ -116,12 +117,14 @@ def load():
     ci, cd, cf, cl = C.c_int, C.c_double, C.c_float, C.c_long
     lib.espec_gemm_f64.argtypes = [ci, ci, ci, cd, vp, ci, ci, vp, ci, ci, cd, vp, ci, vp]
     lib.espec_gemm_f32.argtypes = [ci, ci, ci, cf, vp, ci, ci, vp, ci, ci, cf, vp, ci, vp]
-    lib.espec_mlp_bias_act.argtypes = [vp, vp, ci, ci, ci, vp]
-    lib.espec_mlp_tanh_back.argtypes = [vp, vp, cl, vp]
     lib.espec_mlp_colsum.argtypes = [vp, ci, ci, vp, vp]
     lib.espec_mlp_mse.argtypes = [vp, vp, ci, ci, vp, vp, vp]
-    lib.espec_mlp_adam.argtypes = [vp, vp, vp, vp, cl, cf, cf, cf, cf, ci, vp]
-    lib.espec_mlp_adam_dev.argtypes = [vp, vp, vp, vp, cl, vp, cf, cf, cf, vp]
+    lib.espec_gemm_bf16.argtypes = [ci, ci, ci, cf, vp, ci, ci, vp, ci, ci, cf, vp, ci, vp]
+    lib.espec_gemm_bf16_status.argtypes = [C.POINTER(ci)]
+    lib.espec_mlp_bias_gelu.argtypes = [vp, vp, ci, ci, ci, vp, vp]
+    lib.espec_mlp_gelu_back.argtypes = [vp, vp, cl, vp, vp]
+    lib.espec_to_bf16.argtypes = [vp, vp, cl, vp]
+    lib.espec_mlp_adam_bf16.argtypes = [vp, vp, vp, vp, cl, vp, cf, cf, cf, vp, vp]
     lib.espec_spond_create.argtypes = [C.POINTER(vp), ci, i, d, d, cd, ci, ci, ci]
     lib.espec_spond_load.argtypes = [vp, vp, vp, vp, vp, ci, vp]
     lib.espec_spond_run.argtypes = [vp, ci, vp]
@@ -132,7 +135,7 @@ def load():
     lib.espec_spond_energies.argtypes = [vp, vp, vp, vp]
     lib.espec_spond_destroy.argtypes = [vp]
     lib.espec_spond_destroy.restype = None
-    lib.espec_outer_basis.argtypes = [vp, ci, ci, vp, ci, ci, vp, vp]
+    lib.espec_sep_basis.argtypes = [ci, ci, ci, ci, ci, vp, vp, vp, vp, cf, vp]
     lib.espec_convert.argtypes = [vp, vp, cl, ci, cd, vp]
     lib.espec_grid_destroy.argtypes = [vp]
     lib.espec_grid_destroy.restype = None

@@ -1,13 +1,11 @@
-// mlp.cu -- kernels of the learned warm start for the eigensolver: a small
-// multilayer perceptron (forward, backward, Adam) and the dense products that
-// move eigenvectors in and out of its output basis.
-//
-// The network maps the 5 parameters of a potential to the coefficients of
-// the lowest eigenvectors in a fixed product basis phi_i(x) chi_j(y); it is
-// trained on eigenvectors produced by the plain eigensolver (eig.cu).  The
-// layers are tiny (5 -> 128 -> 128 -> 4 nb), so the products run as tiled
-// SIMT kernels: one 64 x 64 output tile per 256-thread CTA, 16-deep k tiles
-// staged in shared memory, 4 x 4 outputs per thread.
+// mlp.cu -- dense products and loss kernels of the learned warm start for the
+// eigensolver: FP64/FP32 GEMMs that move eigenvectors in and out of the
+// network's output basis (projection onto and expansion in a product basis
+// phi_a(x) chi_b(y), separable), the mean-squared-error loss and the
+// bias-gradient column sums.  The network's own products run on the tensor
+// cores (mlp_tc.cu).  The GEMMs are tiled SIMT kernels: one 64 x 64 output
+// tile per 256-thread CTA, 16-deep k tiles staged in shared memory, 4 x 4
+// outputs per thread.
 #include <cuda_runtime.h>
 
 #include "espec_gpu.h"
@@ -77,28 +75,23 @@ __global__ void __launch_bounds__(256) gemm_kernel(int M, int N, int K, T alpha,
   }
 }
 
-// y = x + b (row broadcast), then tanh when act
-__global__ void bias_act_kernel(float* y, const float* b, int rows, int cols, int act) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long)rows * cols) return;
-  float v = y[i] + b[i % cols];
-  y[i] = act ? tanhf(v) : v;
-}
-
-// dz = dy * (1 - y^2), y = tanh(z)
-__global__ void tanh_back_kernel(float* dz, const float* y, long count) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  dz[i] = dz[i] * (1.0f - y[i] * y[i]);
-}
-
-// db[c] = sum_r dy[r, c] (fixed order over rows)
+// db[c] = sum_r dy[r, c]: 32 columns x 8 row phases per CTA, each phase sums
+// rows r = phase mod 8 in order, then the 8 partials are added in order
+// (deterministic)
 __global__ void colsum_kernel(const float* dy, int rows, int cols, float* db) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= cols) return;
+  __shared__ float part[8][33];
+  const int c = blockIdx.x * 32 + threadIdx.x;
   float s = 0.0f;
-  for (int r = 0; r < rows; ++r) s += dy[(long)r * cols + c];
-  db[c] = s;
+  if (c < cols)
+    for (int r = threadIdx.y; r < rows; r += 8) s += dy[(long)r * cols + c];
+  part[threadIdx.y][threadIdx.x] = s;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < cols) {
+    float t = 0.0f;
+#pragma unroll
+    for (int p = 0; p < 8; ++p) t += part[p][threadIdx.x];
+    db[c] = t;
+  }
 }
 
 // loss = mean over rows of sum (y - t)^2 / cols; dy = 2 (y - t) / (rows cols)
@@ -122,44 +115,69 @@ __global__ void mse_kernel(const float* y, const float* t, int rows, int cols, f
   if (threadIdx.x == 0) row_loss[r] = red[0] / ((float)rows * (float)cols);
 }
 
-// Adam (Kingma & Ba, 2015) with bias correction folded into the step size
-__global__ void adam_kernel(float* w, const float* g, float* m1, float* m2, long count, float lr,
-                            float b1, float b2, float eps, float c1, float c2) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const float gi = g[i];
-  const float a = b1 * m1[i] + (1.0f - b1) * gi;
-  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
-  m1[i] = a;
-  m2[i] = b;
-  w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
-}
+// separable basis transform of one 2D vector per CTA (x fastest in psi,
+// coefficient index a nb + b for phi_a(x) chi_b(y)); shared memory holds
+// phi^T [nx][nb], chi^T [ny][nb] and the half-transformed [ny][nb] block.
+// project: c = scale sum_{x,y} phi_a(x) chi_b(y) psi(x, y)  (psi f64 -> c f32)
+// expand:  psi(x, y) = scale sum_{a,b} phi_a(x) chi_b(y) c_ab  (c f32 -> psi f64)
+constexpr int kSepThreads = 256;
 
-// the same with (lr, c1, c2) read from device memory, so that one captured
-// training step can be replayed with a new step size and bias correction
-__global__ void adam_dev_kernel(float* w, const float* g, float* m1, float* m2, long count,
-                                const float* hyper, float b1, float b2, float eps) {
-  const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= count) return;
-  const float lr = hyper[0], c1 = hyper[1], c2 = hyper[2];
-  const float gi = g[i];
-  const float a = b1 * m1[i] + (1.0f - b1) * gi;
-  const float b = b2 * m2[i] + (1.0f - b2) * gi * gi;
-  m1[i] = a;
-  m2[i] = b;
-  w[i] -= lr * (a / c1) / (sqrtf(b / c2) + eps);
-}
-
-// product basis: B[(i*nby + j), (x + nx*y)] = phi[i][x] chi[j][y]
-__global__ void outer_basis_kernel(const double* phi, int nbx, int nx, const double* chi, int nby,
-                                   int ny, double* B) {
+__global__ void __launch_bounds__(kSepThreads) sep_basis_kernel(int dir, int nx, int ny, int nb,
+                                                                const float* phi, const float* chi,
+                                                                double* psi, float* c,
+                                                                float scale) {
+  extern __shared__ float sep_sm[];
+  float* phiT = sep_sm;           // [nx][nb]
+  float* chiT = phiT + nx * nb;   // [ny][nb]
+  float* half = chiT + ny * nb;   // [ny][nb]
+  const long v = blockIdx.x;
   const long n = (long)nx * ny;
-  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= n * nbx * nby) return;
-  const long b = gid / n, k = gid % n;
-  const int i = (int)(b / nby), j = (int)(b % nby);
-  const int x = (int)(k % nx), y = (int)(k / nx);
-  B[gid] = phi[(long)i * nx + x] * chi[(long)j * ny + y];
+  for (int e = threadIdx.x; e < nx * nb; e += kSepThreads) {
+    const int a = e / nx, x = e % nx;
+    phiT[x * nb + a] = phi[e];
+  }
+  for (int e = threadIdx.x; e < ny * nb; e += kSepThreads) {
+    const int b = e / ny, y = e % ny;
+    chiT[y * nb + b] = chi[e];
+  }
+  __syncthreads();
+  double* pv = psi + v * n;
+  float* cv = c + v * (long)nb * nb;
+  if (dir == 0) {
+    // half[y][a] = sum_x psi(x, y) phi_a(x)
+    for (int e = threadIdx.x; e < ny * nb; e += kSepThreads) {
+      const int y = e / nb, a = e % nb;
+      const double* row = pv + (long)y * nx;
+      float s = 0.0f;
+      for (int x = 0; x < nx; ++x) s = fmaf((float)row[x], phiT[x * nb + a], s);
+      half[e] = s;
+    }
+    __syncthreads();
+    // c[a][b] = sum_y chi_b(y) half[y][a]
+    for (int e = threadIdx.x; e < nb * nb; e += kSepThreads) {
+      const int a = e / nb, b = e % nb;
+      float s = 0.0f;
+      for (int y = 0; y < ny; ++y) s = fmaf(chiT[y * nb + b], half[y * nb + a], s);
+      cv[e] = scale * s;
+    }
+  } else {
+    // half[y][a] = sum_b chi_b(y) c[a][b]
+    for (int e = threadIdx.x; e < ny * nb; e += kSepThreads) {
+      const int y = e / nb, a = e % nb;
+      const float* ca = cv + (long)a * nb;
+      float s = 0.0f;
+      for (int b = 0; b < nb; ++b) s = fmaf(chiT[y * nb + b], ca[b], s);
+      half[e] = s;
+    }
+    __syncthreads();
+    // psi(x, y) = sum_a phi_a(x) half[y][a]
+    for (long e = threadIdx.x; e < n; e += kSepThreads) {
+      const int y = (int)(e / nx), x = (int)(e % nx);
+      float s = 0.0f;
+      for (int a = 0; a < nb; ++a) s = fmaf(phi[(long)a * nx + x], half[y * nb + a], s);
+      pv[e] = (double)(scale * s);
+    }
+  }
 }
 
 __global__ void f64_to_f32_kernel(const double* a, float* b, long count, double scale) {
@@ -208,22 +226,9 @@ extern "C" int espec_gemm_f32(int M, int N, int K, float alpha, const float* A, 
   return gemm_launch<float>(M, N, K, alpha, A, lda, ta, B, ldb, tb, beta, C, ldc, stream);
 }
 
-extern "C" int espec_mlp_bias_act(float* y, const float* b, int rows, int cols, int act,
-                                  void* stream) {
-  bias_act_kernel<<<blocks((long)rows * cols), 256, 0, (cudaStream_t)stream>>>(y, b, rows, cols,
-                                                                              act);
-  MLP_CK();
-  return ESPEC_OK;
-}
-
-extern "C" int espec_mlp_tanh_back(float* dz, const float* y, long count, void* stream) {
-  tanh_back_kernel<<<blocks(count), 256, 0, (cudaStream_t)stream>>>(dz, y, count);
-  MLP_CK();
-  return ESPEC_OK;
-}
-
 extern "C" int espec_mlp_colsum(const float* dy, int rows, int cols, float* db, void* stream) {
-  colsum_kernel<<<blocks(cols), 256, 0, (cudaStream_t)stream>>>(dy, rows, cols, db);
+  colsum_kernel<<<(unsigned)((cols + 31) / 32), dim3(32, 8), 0, (cudaStream_t)stream>>>(dy, rows,
+                                                                                       cols, db);
   MLP_CK();
   return ESPEC_OK;
 }
@@ -235,36 +240,19 @@ extern "C" int espec_mlp_mse(const float* y, const float* t, int rows, int cols,
   return ESPEC_OK;
 }
 
-extern "C" int espec_mlp_adam(float* w, const float* g, float* m1, float* m2, long count,
-                              float lr, float b1, float b2, float eps, int step, void* stream) {
-  if (step < 1) return set_error(ESPEC_EINVAL, "Adam step counts from 1");
-  float c1 = 1.0f, c2 = 1.0f, p1 = 1.0f, p2 = 1.0f;
-  for (int i = 0; i < step; ++i) {
-    p1 *= b1;
-    p2 *= b2;
-  }
-  c1 = 1.0f - p1;
-  c2 = 1.0f - p2;
-  adam_kernel<<<blocks(count), 256, 0, (cudaStream_t)stream>>>(w, g, m1, m2, count, lr, b1, b2,
-                                                               eps, c1, c2);
-  MLP_CK();
-  return ESPEC_OK;
-}
-
-extern "C" int espec_mlp_adam_dev(float* w, const float* g, float* m1, float* m2, long count,
-                                  const float* hyper, float b1, float b2, float eps,
-                                  void* stream) {
-  adam_dev_kernel<<<blocks(count), 256, 0, (cudaStream_t)stream>>>(w, g, m1, m2, count, hyper, b1,
-                                                                   b2, eps);
-  MLP_CK();
-  return ESPEC_OK;
-}
-
-extern "C" int espec_outer_basis(const double* phi, int nbx, int nx, const double* chi, int nby,
-                                 int ny, double* B, void* stream) {
-  const long count = (long)nx * ny * nbx * nby;
-  outer_basis_kernel<<<blocks(count), 256, 0, (cudaStream_t)stream>>>(phi, nbx, nx, chi, nby, ny,
-                                                                      B);
+extern "C" int espec_sep_basis(int dir, int nvec, int nx, int ny, int nb, const float* phi,
+                               const float* chi, double* psi, float* c, float scale,
+                               void* stream) {
+  if (nvec < 0 || nx < 1 || ny < 1 || nb < 1 || !phi || !chi || !psi || !c)
+    return set_error(ESPEC_EINVAL, "bad basis transform");
+  const size_t smem = sizeof(float) * (size_t)nb * (nx + 2 * ny);
+  if (smem > 200 * 1024) return set_error(ESPEC_EINVAL, "basis tables exceed shared memory");
+  if (nvec == 0) return ESPEC_OK;
+  cudaError_t e = cudaFuncSetAttribute(sep_basis_kernel,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e);
+  sep_basis_kernel<<<nvec, kSepThreads, smem, (cudaStream_t)stream>>>(dir ? 1 : 0, nx, ny, nb,
+                                                                     phi, chi, psi, c, scale);
   MLP_CK();
   return ESPEC_OK;
 }

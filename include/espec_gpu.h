@@ -317,28 +317,42 @@ int espec_gemm_f64(int M, int N, int K, double alpha, const double* A, int lda, 
 int espec_gemm_f32(int M, int N, int K, float alpha, const float* A, int lda, int ta,
                    const float* B, int ldb, int tb, float beta, float* C, int ldc,
                    void* stream);
-/* y[r,c] = act(y[r,c] + b[c]), act = tanh when act != 0 */
-int espec_mlp_bias_act(float* y, const float* b, int rows, int cols, int act, void* stream);
-/* dz *= 1 - y^2 (y = tanh of the layer's input) */
-int espec_mlp_tanh_back(float* dz, const float* y, long count, void* stream);
 /* db[c] = sum_r dy[r,c] */
 int espec_mlp_colsum(const float* dy, int rows, int cols, float* db, void* stream);
 /* mean squared error: row_loss[r] = sum_c (y-t)^2/(rows cols), dy = its gradient */
 int espec_mlp_mse(const float* y, const float* t, int rows, int cols, float* dy,
                   float* row_loss, void* stream);
-/* one Adam step (step counts from 1) */
-int espec_mlp_adam(float* w, const float* g, float* m1, float* m2, long count, float lr,
-                   float b1, float b2, float eps, int step, void* stream);
-/* Adam step with hyper = device {lr, 1 - b1^t, 1 - b2^t}: replayable from a
- * captured CUDA graph with new values written into hyper */
-int espec_mlp_adam_dev(float* w, const float* g, float* m1, float* m2, long count,
-                       const float* hyper, float b1, float b2, float eps, void* stream);
-/* B[i*nby+j][x + nx*y] = phi[i][x] chi[j][y] (product basis of two 1D sets) */
-int espec_outer_basis(const double* phi, int nbx, int nx, const double* chi, int nby, int ny,
-                      double* B, void* stream);
+/* separable basis transform, one vector of nx*ny points (x fastest) per CTA;
+ * phi [nb][nx], chi [nb][ny] (float, device); coefficient index a*nb + b:
+ * dir 0: c[v][a*nb+b] = scale sum_{x,y} phi[a][x] chi[b][y] psi[v][x+nx*y]
+ * dir 1: psi[v][x+nx*y] = scale sum_{a,b} phi[a][x] chi[b][y] c[v][a*nb+b]
+ * (FP32 arithmetic; psi double, c float) */
+int espec_sep_basis(int dir, int nvec, int nx, int ny, int nb, const float* phi, const float* chi,
+                    double* psi, float* c, float scale, void* stream);
 /* element-wise f64 -> f32 (to_f32 != 0) or f32 -> f64, times scale */
 int espec_convert(const void* src, void* dst, long count, int to_f32, double scale,
                   void* stream);
+/* C[M,N] (float) = alpha op(A) op(B) + beta C with A, B bfloat16 (raw 16-bit
+ * values), FP32 accumulation on the tensor cores (tcgen05.mma, accumulator in
+ * tensor memory); op(X) = X^T when t* != 0, row-major as espec_gemm_f32 */
+int espec_gemm_bf16(int M, int N, int K, float alpha, const void* A, int lda, int ta,
+                    const void* B, int ldb, int tb, float beta, float* C, int ldc, void* stream);
+/* synchronous: 1 when a tensor-core GEMM gave up waiting for its MMAs since
+ * the last call (its output is then not written), else 0; clears the flag */
+int espec_gemm_bf16_status(int* timed_out);
+/* z[r,c] += b[c]; h = bf16(GELU(z)) (act != 0) or bf16(z); h may be NULL */
+int espec_mlp_bias_gelu(float* z, const float* b, int rows, int cols, int act, void* h_bf16,
+                        void* stream);
+/* dh *= GELU'(z) (z = the layer's pre-activation); dz_bf16 = bf16(dh) */
+int espec_mlp_gelu_back(float* dh, const float* z, long count, void* dz_bf16, void* stream);
+/* y = bf16(x) */
+int espec_to_bf16(const float* x, void* y, long count, void* stream);
+/* one Adam step (Kingma & Ba) on FP32 master weights with hyper = device
+ * {lr, 1 - b1^t, 1 - b2^t} (replayable from a captured CUDA graph with new
+ * values written into hyper), then w_bf16 = bf16(w) (w_bf16 may be NULL) */
+int espec_mlp_adam_bf16(float* w, const float* g, float* m1, float* m2, long count,
+                        const float* hyper, float b1, float b2, float eps, void* w_bf16,
+                        void* stream);
 
 /* ----------------------------------------------------------------------
  * Spectrum stage on the device, batched over packets (FP64).
