@@ -45,7 +45,13 @@ class SpoBatch:
         """vpot, psi (complex or real), vabc: host numpy arrays (concatenated),
         or device tensors (torch float64) with psi given as (re, im)."""
         lib = N.load()
-        if isinstance(psi, tuple):  # device (re, im)
+        if isinstance(psi, tuple) and isinstance(psi[0], np.ndarray):  # host (re, im)
+            self._keep = [N.f64(vpot), N.f64(psi[0]), N.f64(psi[1]),
+                          None if vabc is None else N.f64(vabc)]
+            v, re, im, ab = self._keep
+            rc = lib.espec_spo_load(self._h, N.ptr(v), N.ptr(ab), N.ptr(re), N.ptr(im),
+                                    N.MEM_HOST, stream)
+        elif isinstance(psi, tuple):  # device (re, im)
             re, im = psi
             rc = lib.espec_spo_load(self._h, N.ptr(vpot), N.ptr(vabc), N.ptr(re), N.ptr(im),
                                     N.MEM_DEVICE, stream)
@@ -89,6 +95,14 @@ class SpoBatch:
                                         N.MEM_HOST, stream)
         N.check(rc, "espec_spo_results")
         return (cr + 1j * ci).reshape(self.npk, ns + 1), pr + 1j * pi
+
+    def results_into(self, c_re, c_im, psi_re, psi_im, stream=None):
+        """Copy C(t) ([npk * (nsteps+1)], packet-major) and psi(TF) as separate
+        real and imaginary float64 host arrays into the caller's buffers (any
+        may be None); returns when the copies are done."""
+        N.check(N.load().espec_spo_results(self._h, N.ptr(c_re), N.ptr(c_im), N.ptr(psi_re),
+                                           N.ptr(psi_im), N.MEM_HOST, stream),
+                "espec_spo_results")
 
     def device_c(self):
         """Device address of C(t) (double2, packet-major)."""
