@@ -12,6 +12,7 @@
 
 #include "espec_gpu.h"
 #include "espec_internal.h"
+#include "cplx_io.cuh"
 #include "diag1d.cuh"
 #include "sod1d.cuh"
 #include "spo1d_launch.cuh"
@@ -311,8 +312,7 @@ struct espec_spo_plan {
   bool loaded = false;
   bool has_prev = false;      // SOD: d_psi_prev holds psi(t - dt) of the current state
   double2* d_diag = nullptr;  // (E, norm) per packet
-  double* d_stage = nullptr;  // host transfers: (re | im) blocks, contiguous
-  size_t stage_bytes = 0;
+  HostStage stage;            // host transfers: (re | im) blocks, contiguous
   // tables (sub-pointers of d_tab)
   SpoTables<double> t64{};
   SpoTables<float> t32{};
@@ -329,9 +329,10 @@ static void plan_free(espec_spo_plan* p) {
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   void* bufs[] = {p->d_vpot, p->d_vabc, p->d_psi0, p->d_psi, p->d_tc, p->d_kperm, p->d_pk_of,
                   p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s, p->d_psi_prev,
-                  p->d_diag, p->d_stage};
+                  p->d_diag};
   for (void* b : bufs)
     if (b) cudaFree(b);
+  p->stage.release();
 }
 
 #define ESPEC_CK(call)                                           \
@@ -339,74 +340,6 @@ static void plan_free(espec_spo_plan* p) {
     cudaError_t e_ = (call);                                     \
     if (e_ != cudaSuccess) return set_cuda_error(#call, e_);     \
   } while (0)
-
-// Complex arrays live interleaved (double2) on the device and as separate
-// (re, im) arrays at the interface (the reference's U/V and LNZVC columns).
-// Host transfers go through a contiguous (re | im) staging block, so each is
-// one linear copy; device-side arguments are (de)interleaved in place.
-__global__ void interleave_kernel(const double* re, const double* im, double2* out, size_t n) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    out[i] = make_double2(re[i], im ? im[i] : 0.0);
-}
-
-__global__ void deinterleave_kernel(const double2* in, double* re, double* im, size_t n) {
-  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const double2 v = in[i];
-    if (re) re[i] = v.x;
-    if (im) im[i] = v.y;
-  }
-}
-
-static unsigned split_blocks(size_t n) {
-  const size_t b = (n + 255) / 256;
-  return (unsigned)(b < 148 * 16 ? (b > 0 ? b : 1) : 148 * 16);
-}
-
-static int stage_reserve(espec_spo_plan* p, size_t bytes) {
-  if (p->stage_bytes >= bytes) return ESPEC_OK;
-  if (p->d_stage) cudaFree(p->d_stage);
-  p->d_stage = nullptr;
-  p->stage_bytes = 0;
-  ESPEC_CK(cudaMalloc(&p->d_stage, bytes));
-  p->stage_bytes = bytes;
-  return ESPEC_OK;
-}
-
-// dst (device, n complex) <- (re, im) at `where`; im may be null (zero)
-static int put_complex(espec_spo_plan* p, double2* dst, const double* re, const double* im,
-                       size_t n, int where, cudaStream_t st) {
-  if (where == ESPEC_MEM_HOST) {
-    int rc = stage_reserve(p, 16 * n);
-    if (rc) return rc;
-    ESPEC_CK(cudaMemcpyAsync(p->d_stage, re, 8 * n, cudaMemcpyHostToDevice, st));
-    if (im) ESPEC_CK(cudaMemcpyAsync(p->d_stage + n, im, 8 * n, cudaMemcpyHostToDevice, st));
-    re = p->d_stage;
-    im = im ? p->d_stage + n : nullptr;
-  }
-  interleave_kernel<<<split_blocks(n), 256, 0, st>>>(re, im, dst, n);
-  ESPEC_CK(cudaGetLastError());
-  return ESPEC_OK;
-}
-
-// (re, im) at `where` <- src (device, n complex); either output may be null
-static int get_complex(espec_spo_plan* p, const double2* src, double* re, double* im, size_t n,
-                       int where, cudaStream_t st) {
-  if (!re && !im) return ESPEC_OK;
-  if (where != ESPEC_MEM_HOST) {
-    deinterleave_kernel<<<split_blocks(n), 256, 0, st>>>(src, re, im, n);
-    ESPEC_CK(cudaGetLastError());
-    return ESPEC_OK;
-  }
-  int rc = stage_reserve(p, 16 * n);
-  if (rc) return rc;
-  deinterleave_kernel<<<split_blocks(n), 256, 0, st>>>(src, p->d_stage, p->d_stage + n, n);
-  ESPEC_CK(cudaGetLastError());
-  if (re) ESPEC_CK(cudaMemcpyAsync(re, p->d_stage, 8 * n, cudaMemcpyDeviceToHost, st));
-  if (im) ESPEC_CK(cudaMemcpyAsync(im, p->d_stage + n, 8 * n, cudaMemcpyDeviceToHost, st));
-  return ESPEC_OK;
-}
 
 // host-built index tables: DIGT, final-position frequencies of the chosen
 // plans, packet ids and kinetic scales
@@ -673,7 +606,7 @@ extern "C" int espec_spo_load(espec_spo_plan* p, const double* vpot, const doubl
   const cudaMemcpyKind kind = where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   ESPEC_CK(cudaMemcpyAsync(p->d_vpot, vpot, np * 8, kind, st));
   if (vabc) ESPEC_CK(cudaMemcpyAsync(p->d_vabc, vabc, np * 8, kind, st));
-  int rc = put_complex(p, p->d_psi0, psi_re, psi_im, np, where, st);
+  int rc = put_complex(p->stage, p->d_psi0, psi_re, psi_im, np, where, st);
   if (rc) return rc;
   // the current state of a freshly loaded plan is psi0
   ESPEC_CK(cudaMemcpyAsync(p->d_psi, p->d_psi0, np * 16, cudaMemcpyDeviceToDevice, st));
@@ -791,8 +724,8 @@ extern "C" int espec_spo_results(espec_spo_plan* p, double* c_re, double* c_im, 
   if (!p || p->c_cap_steps < 0) return set_error(ESPEC_EINVAL, "no results: run the plan first");
   cudaStream_t st = (cudaStream_t)stream;
   const size_t nc = (size_t)p->npk * (p->c_cap_steps + 1);
-  int rc = get_complex(p, p->d_c, c_re, c_im, nc, where, st);
-  if (rc == ESPEC_OK) rc = get_complex(p, p->d_psi, psi_re, psi_im, p->npts, where, st);
+  int rc = get_complex(p->stage, p->d_c, c_re, c_im, nc, where, st);
+  if (rc == ESPEC_OK) rc = get_complex(p->stage, p->d_psi, psi_re, psi_im, p->npts, where, st);
   if (rc) return rc;
   if (where == ESPEC_MEM_HOST) ESPEC_CK(cudaStreamSynchronize(st));
   return ESPEC_OK;
@@ -805,7 +738,7 @@ extern "C" int espec_prop_previous(espec_spo_plan* p, double* psi_re, double* ps
   if (!p || p->method != ESPEC_SOD || p->c_cap_steps < 0)
     return set_error(ESPEC_EINVAL, "previous state exists for run SOD plans only");
   cudaStream_t st = (cudaStream_t)stream;
-  const int rc = get_complex(p, p->d_psi_prev, psi_re, psi_im, p->npts, where, st);
+  const int rc = get_complex(p->stage, p->d_psi_prev, psi_re, psi_im, p->npts, where, st);
   if (rc) return rc;
   if (where == ESPEC_MEM_HOST) ESPEC_CK(cudaStreamSynchronize(st));
   return ESPEC_OK;

@@ -28,6 +28,7 @@
 #include "cplx.cuh"
 #include "espec_gpu.h"
 #include "espec_internal.h"
+#include "cplx_io.cuh"
 
 namespace espec {
 namespace {
@@ -521,6 +522,7 @@ struct espec_spond_plan {
   double* d_tcp = nullptr;         // TC in the passes' storage order
   RotD* d_tw64[3] = {nullptr, nullptr, nullptr};
   double2* d_epart = nullptr;
+  HostStage stage;                 // host transfers: (re | im) blocks, contiguous
 };
 
 namespace {
@@ -1018,11 +1020,8 @@ extern "C" int espec_spond_previous(espec_spond_plan* p, double* psi_re, double*
   if (!p || p->method != ESPEC_SOD || !p->has_state)
     return set_error(ESPEC_EINVAL, "previous state exists for run SOD plans only");
   cudaStream_t st = (cudaStream_t)stream;
-  const cudaMemcpyKind kind =
-      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
-  const size_t n = (size_t)p->n;
-  if (psi_re) ND_CK(cudaMemcpy2DAsync(psi_re, 8, p->d_prev, 16, 8, n, kind, st));
-  if (psi_im) ND_CK(cudaMemcpy2DAsync(psi_im, 8, (char*)p->d_prev + 8, 16, 8, n, kind, st));
+  const int rc = get_complex(p->stage, p->d_prev, psi_re, psi_im, (size_t)p->n, where, st);
+  if (rc) return rc;
   if (where == ESPEC_MEM_HOST) ND_CK(cudaStreamSynchronize(st));
   return ESPEC_OK;
 }
@@ -1038,12 +1037,8 @@ extern "C" int espec_spond_load(espec_spond_plan* p, const double* vpot, const d
       where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   ND_CK(cudaMemcpyAsync(p->d_vpot, vpot, 8 * n, kind, st));
   if (p->absorb != ESPEC_ABS_NONE) ND_CK(cudaMemcpyAsync(p->d_vabc, vabc, 8 * n, kind, st));
-  ND_CK(cudaMemcpy2DAsync(p->d_psi0, 16, psi_re, 8, 8, n, kind, st));
-  if (psi_im) {
-    ND_CK(cudaMemcpy2DAsync((char*)p->d_psi0 + 8, 16, psi_im, 8, 8, n, kind, st));
-  } else {
-    ND_CK(cudaMemset2DAsync((char*)p->d_psi0 + 8, 16, 0, 8, n, st));
-  }
+  const int rp = put_complex(p->stage, p->d_psi0, psi_re, psi_im, n, where, st);
+  if (rp) return rp;
   const int rc = p->precision == ESPEC_FP64 ? build_tables<double>(p, st)
                                             : build_tables<float>(p, st);
   if (rc) return rc;
@@ -1177,13 +1172,10 @@ extern "C" int espec_spond_results(espec_spond_plan* p, double* c_re, double* c_
                                    double* psi_re, double* psi_im, int where, void* stream) {
   if (!p || p->c_cap < 0) return set_error(ESPEC_EINVAL, "no results: run the plan first");
   cudaStream_t st = (cudaStream_t)stream;
-  const cudaMemcpyKind kind =
-      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
   const size_t nc = (size_t)p->c_cap + 1, n = (size_t)p->n;
-  if (c_re) ND_CK(cudaMemcpy2DAsync(c_re, 8, p->d_c, 16, 8, nc, kind, st));
-  if (c_im) ND_CK(cudaMemcpy2DAsync(c_im, 8, (char*)p->d_c + 8, 16, 8, nc, kind, st));
-  if (psi_re) ND_CK(cudaMemcpy2DAsync(psi_re, 8, p->d_out, 16, 8, n, kind, st));
-  if (psi_im) ND_CK(cudaMemcpy2DAsync(psi_im, 8, (char*)p->d_out + 8, 16, 8, n, kind, st));
+  int rc = get_complex(p->stage, p->d_c, c_re, c_im, nc, where, st);
+  if (rc == ESPEC_OK) rc = get_complex(p->stage, p->d_out, psi_re, psi_im, n, where, st);
+  if (rc) return rc;
   if (where == ESPEC_MEM_HOST) ND_CK(cudaStreamSynchronize(st));
   return ESPEC_OK;
 }
@@ -1196,5 +1188,6 @@ extern "C" void espec_spond_destroy(espec_spond_plan* p) {
                p->d_prev,   p->d_sod};
   for (void* x : b)
     if (x) cudaFree(x);
+  p->stage.release();
   delete p;
 }
