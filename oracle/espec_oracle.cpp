@@ -803,6 +803,130 @@ extern "C" int orc_psodfft(const orc_prop_t* p, const double* vpot, const double
   return cs.n;
 }
 
+// sod.f:64-123  PSODAUX with H = AU (4th-order finite differences):
+// U2 <- U1 + cst H V2, then V2 <- V1 - cst H U2(old), the old (U2, V2) moving
+// to (U1, V1); .VOPTIC subtracts cst VABC times the old value, .SMOOTHW
+// multiplies the result by the mask (sod.f:71-119)
+static void psod_aux(const orc_prop_t* p, double cst, const double* vpot, const double* vabc,
+                     double* u1, double* u2, double* v1, double* v2, double* work) {
+  const int n = npts(p);
+  orc_au(p->ndim, p->np, p->shm, vpot, v2, work);
+  for (int i = 0; i < n; ++i) {
+    const double uaux = u2[i];
+    if (p->absorb == ORC_ABS_VOPTIC)
+      u2[i] = u1[i] + cst * work[i] - cst * vabc[i] * uaux;
+    else if (p->absorb == ORC_ABS_SMOOTHW)
+      u2[i] = vabc[i] * (u1[i] + cst * work[i]);
+    else
+      u2[i] = u1[i] + cst * work[i];
+    u1[i] = uaux;
+  }
+  orc_au(p->ndim, p->np, p->shm, vpot, u1, work);
+  for (int i = 0; i < n; ++i) {
+    const double vaux = v2[i];
+    if (p->absorb == ORC_ABS_VOPTIC)
+      v2[i] = v1[i] - cst * work[i] - cst * vabc[i] * vaux;
+    else if (p->absorb == ORC_ABS_SMOOTHW)
+      v2[i] = vabc[i] * (v1[i] - cst * work[i]);
+    else
+      v2[i] = v1[i] - cst * work[i];
+    v1[i] = vaux;
+  }
+}
+
+// psod.f:64-205  PSOD: C(0); an Euler half step (CST/4) and a midpoint step
+// (CST/2) to TI + DT; (U1, V1) back to psi0; then leapfrog steps of CST =
+// 2 DT / SHFS.  Printed rows carry |C|^2 and E = EIGENERG(U) + EIGENERG(V);
+// the norm column is sum |psi|^2, squared in the rows of the loop
+// (psod.f:183), which the loop's drift test also uses.
+extern "C" int orc_psod(const orc_prop_t* p, const double* vpot, const double* vabc, double* u1,
+                        double* v1, double* u2, double* v2, double* c_re, double* c_im, int c_cap,
+                        double* rows, int row_cap, int* nrows, int* info) {
+  const int n = npts(p);
+  RowSink rs{rows, row_cap};
+  CSink cs{c_re, c_im, c_cap};
+  *info = 0;
+  double t = p->ti;
+  const double cst = 2.0 * p->dt / ORC_SHFS;
+  const bool absorb = p->absorb != ORC_ABS_NONE;
+  std::vector<double> u0(u1, u1 + n), v0(v1, v1 + n), work(n);
+  for (int i = 0; i < n; ++i) {
+    u2[i] = u0[i];
+    v2[i] = v0[i];
+  }
+  auto corr = [&](double& cr, double& ci) {
+    cr = orc_fcorrel(n, u0.data(), u2) + orc_fcorrel(n, v0.data(), v2);
+    ci = orc_fcorrel(n, u0.data(), v2) - orc_fcorrel(n, v0.data(), u2);
+  };
+  auto energy = [&]() {
+    return orc_eigenerg(p->ndim, p->np, p->shm, vpot, u2) +
+           orc_eigenerg(p->ndim, p->np, p->shm, vpot, v2);
+  };
+  auto norm2 = [&]() { return orc_fcorrel(n, u2, u2) + orc_fcorrel(n, v2, v2); };
+  auto drifted = [&](double et, double e0, double fnt, double f0) {
+    return std::fabs((et - e0) / e0) * 100.0 > p->tol || std::fabs((fnt - f0) / f0) * 100.0 > p->tol;
+  };
+  double cr, ci;
+  corr(cr, ci);
+  cs.put(cr, ci);
+  double et = energy();
+  const double e0 = et;
+  double fnt = norm2();
+  const double f0 = fnt;
+  if (p->prtcrl != ORC_PRT_NONE) rs.put(t, et, cr, ci, cr * cr + ci * ci, fnt);
+  psod_aux(p, cst / 4.0, vpot, vabc, u1, u2, v1, v2, work.data());
+  psod_aux(p, cst / 2.0, vpot, vabc, u1, u2, v1, v2, work.data());
+  int mc = 1;
+  t = p->ti + p->dt;
+  if (mc == p->lc) {
+    mc = 0;
+    corr(cr, ci);
+    cs.put(cr, ci);
+  }
+  if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+    corr(cr, ci);
+    et = energy();
+    fnt = norm2();
+    rs.put(t, et, cr, ci, cr * cr + ci * ci, fnt);
+  }
+  for (int i = 0; i < n; i += 2) {  // psod.f:136-141
+    u1[i] = u0[i];
+    v1[i] = v0[i];
+    if (i + 1 < n) {
+      u1[i + 1] = u0[i + 1];
+      v1[i + 1] = (p->quirks & ORC_Q_PSOD_COPY) ? v0[i] : v0[i + 1];
+    }
+  }
+  const int nit = orc_do_count(p->ti + 2 * p->dt, p->tf + p->dt, p->dt);
+  t = p->ti + 2 * p->dt;
+  for (int it = 0; it < nit; ++it, t = t + p->dt) {
+    psod_aux(p, cst, vpot, vabc, u1, u2, v1, v2, work.data());
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      corr(cr, ci);
+      cs.put(cr, ci);
+    }
+    if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+      corr(cr, ci);
+      et = energy();
+      const double fnr = norm2();
+      fnt = fnr * fnr;
+      if (absorb)
+        *info = 0;
+      else if (drifted(et, e0, fnt, f0))
+        *info = 1;
+      rs.put(t, et, cr, ci, cr * cr + ci * ci, fnt);
+    }
+  }
+  et = energy();
+  fnt = norm2();
+  if (!absorb && drifted(et, e0, fnt, f0)) *info = 1;  // with ABSORB the test sets 0 (psod.f:197)
+  if (absorb) *info = 0;
+  if (nrows) *nrows = rs.n;
+  return cs.n;
+}
+
 // ---------------------------------------------------------------------------
 // Symmetric tridiagonal eigensolver (stands in for DSTEVX('V','A'),
 // dstevx.f).  Implicit-shift QL iteration with Wilkinson shifts on a copy of

@@ -29,6 +29,7 @@ extern "C" {
 #define ORC_Q_DIGT_ND      4  /* dkeft.f:80-137 2D/3D kinetic table filled wrongly   */
 #define ORC_Q_SOD_SMOOTHW  8  /* sodfft.f:108 mask test never true: no .SMOOTHW   */
 #define ORC_Q_FFTNT_SP    16  /* cfft.f TWOPI literal is single precision            */
+#define ORC_Q_PSOD_COPY   32  /* psod.f:136-141 restart copy: V1(I+1) = V0(I)        */
 
 enum { ORC_ABS_NONE = 0, ORC_ABS_VOPTIC = 1, ORC_ABS_SMOOTHW = 2 };
 enum { ORC_PRT_NONE = 0, ORC_PRT_PARTIAL = 1, ORC_PRT_YES = 2 };
@@ -107,6 +108,12 @@ int orc_psodfft(const orc_prop_t* p, const double* vpot, const double* vabc,
 int orc_plnz(const orc_prop_t* p, const double* vpot, const double* vabc,
              double* u, double* v, double* c_re, double* c_im, int c_cap,
              double* rows, int row_cap, int* nrows, int* info);
+/* PSOD (psod.f): second-order differences with the finite-difference H;
+ * on return (u2, v2) = psi(TF), (u1, v1) = psi(TF - dt) */
+int orc_psod(const orc_prop_t* p, const double* vpot, const double* vabc,
+             double* u1, double* v1, double* u2, double* v2, double* c_re,
+             double* c_im, int c_cap, double* rows, int row_cap, int* nrows,
+             int* info);
 
 /* symmetric tridiagonal eigensolver: d[n] diag, e[n-1] offdiag, z[n*n]
  * column-major eigenvectors, eigenvalues ascending in w.  0 on success. */

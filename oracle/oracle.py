@@ -21,6 +21,7 @@ Q_SIL_INPLACE = 2
 Q_DIGT_ND = 4
 Q_SOD_SMOOTHW = 8
 Q_FFTNT_SP = 16
+Q_PSOD_COPY = 32
 Q_ALL = 31
 
 ABS_NONE, ABS_VOPTIC, ABS_SMOOTHW = 0, 1, 2
@@ -204,6 +205,14 @@ def psodfft(p, vpot, u, v, vabc=None):
     u1, v1 = f64(u).copy(), f64(v).copy()
     u2, v2 = np.zeros_like(u1), np.zeros_like(v1)
     r = _run(lib().orc_psodfft, p, vpot, vabc, [u1, v1, u2, v2], *_caps(p))
+    r.update(u=u2, v=v2, u_prev=u1, v_prev=v1)
+    return r
+
+
+def psod(p, vpot, u, v, vabc=None):
+    u1, v1 = f64(u).copy(), f64(v).copy()
+    u2, v2 = np.zeros_like(u1), np.zeros_like(v1)
+    r = _run(lib().orc_psod, p, vpot, vabc, [u1, v1, u2, v2], *_caps(p))
     r.update(u=u2, v=v2, u_prev=u1, v_prev=v1)
     return r
 

@@ -19,6 +19,10 @@ Cases:
               with a .SMOOTHW mask.
   morse2d_*   2D coupled Morse on a 32x32 grid with .PSIL, .PFSPO and .PFSOD
               (the last two pin the reference's 2D kinetic-table defect).
+  *_psod*     the same 1D decks and the 2D deck with .PSOD (second-order
+              differences with the finite-difference Hamiltonian).  With
+              --psod-only only these are generated and merged into the
+              manifest.
 """
 import json
 import os
@@ -353,9 +357,32 @@ SMOOTH = """*ABSORBING
 """
 
 
+def psod_cases():
+    vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
+    smeta = dict(absorb="SMOOTHW", voi=[0.05, 1.0], al=1.55, ar=2.3)
+    return {"morse1d_psod": case_morse1d("morse1d_psod", ".PSOD", "", {}),
+            "morse1d_psod_voptic": case_morse1d("morse1d_psod_voptic", ".PSOD", VOPTIC, vmeta),
+            "morse1d_psod_smooth": case_morse1d("morse1d_psod_smooth", ".PSOD", SMOOTH, smeta),
+            "morse2d_psod": case_morse2d("morse2d_psod", ".PSOD")}
+
+
+def save(cases, manifest):
+    for name, (meta, arrays) in cases.items():
+        np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
+        manifest[name] = meta
+        print(name, {k: getattr(a, "shape", None) for k, a in arrays.items()})
+    with open(os.path.join(OUT, "manifest.json"), "w") as f:
+        json.dump(manifest, f, indent=1, sort_keys=True)
+
+
 def main():
     if not os.path.exists(BIN):
         sys.exit("eSPec executable not found at " + BIN)
+    if "--psod-only" in sys.argv:
+        with open(os.path.join(OUT, "manifest.json")) as f:
+            manifest = json.load(f)
+        save(psod_cases(), manifest)
+        return
     if "--text-only" in sys.argv:  # only the *_partial.txt files
         vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
         case_morse1d("morse1d_spo", ".PFSPO", "", {})
@@ -381,13 +408,8 @@ def main():
         cases[f"morse1d_{tag}_smooth"] = case_morse1d(f"morse1d_{tag}_smooth", prop, SMOOTH, smeta)
     for prop, tag in [(".PSIL", "sil"), (".PFSPO", "spo"), (".PFSOD", "sod")]:
         cases[f"morse2d_{tag}"] = case_morse2d(f"morse2d_{tag}", prop)
-    manifest = {}
-    for name, (meta, arrays) in cases.items():
-        np.savez_compressed(os.path.join(OUT, name + ".npz"), **arrays)
-        manifest[name] = meta
-        print(name, {k: getattr(a, "shape", None) for k, a in arrays.items()})
-    with open(os.path.join(OUT, "manifest.json"), "w") as f:
-        json.dump(manifest, f, indent=1, sort_keys=True)
+    cases.update(psod_cases())
+    save(cases, {})
 
 
 if __name__ == "__main__":

@@ -58,7 +58,7 @@ def shm_of(sm, sh):
 
 
 # reference-defect switches that reproduce the shipped executable per case
-QUIRKS_OF = {".PFSPO": 1, ".PSIL": 2, ".PFSOD": 8}   # oracle.Q_* bits
+QUIRKS_OF = {".PFSPO": 1, ".PSIL": 2, ".PFSOD": 8, ".PSOD": 32}   # oracle.Q_* bits
 DIGT_ND = 4
 
 
@@ -113,5 +113,6 @@ def run_oracle(case, quirks, prtcrl=1):
     p = O.make_prop(case["np"], case["dt"], case["ti"], case["tf"], case["sh"], case["sm"],
                     lc=case["lc"], tol=case["tol"], absorb=case["absorb"], prtcrl=prtcrl,
                     quirks=quirks, mp=case["mp"], change=1, shm=case["shm"])
-    fn = {".PFSPO": O.pspofft, ".PFSOD": O.psodfft, ".PSIL": O.plnz}[case["meta"]["prop"]]
+    fn = {".PFSPO": O.pspofft, ".PFSOD": O.psodfft, ".PSIL": O.plnz,
+          ".PSOD": O.psod}[case["meta"]["prop"]]
     return fn(p, case["vpot"], case["psi"], np.zeros_like(case["psi"]), vabc=case["vabc"])

@@ -17,7 +17,7 @@ CASES_PRINT_EXACT = [
     "morse1d_sod", "morse1d_spo", "morse1d_sil",
     "morse1d_sod_voptic", "morse1d_spo_voptic",
     "morse1d_sod_smooth", "morse1d_spo_smooth", "morse1d_sil_smooth",
-    "morse2d_sil",
+    "morse2d_sil", "morse1d_psod", "morse1d_psod_voptic", "morse1d_psod_smooth", "morse2d_psod",
 ]
 
 
@@ -41,6 +41,33 @@ def test_propagation_matches_executable(oracle, name):
     assert dt <= 5.1e-9          # F14.8 time column
     assert dE <= 2e-6            # E12.6 energy column
     assert r["info"] == 0
+    if case["meta"]["prop"] == ".PSOD":  # |C|^2 (F10.8) and the norm column (F8.6)
+        g = case["data"]["rows"]
+        assert np.max(np.abs(r["rows"][:, 4] - g[:, 4])) <= 1.01e-8
+        assert np.max(np.abs(r["rows"][:, 5] - g[:, 5])) <= 1.01e-6
+
+
+def test_psod_restart_copy_defect(oracle):
+    """psod.f:136-141 copies V0(I) into both V1(I) and V1(I+1) after the
+    start-up: with a complex initial state the defect changes the run, with a
+    real one (every .GETR deck) it does not."""
+    case = G.setup_case("morse1d_psod")
+    from oracle import oracle as O
+    n = len(case["psi"])
+    x = np.arange(n)
+    psi = case["psi"] * np.exp(0.7j * np.sin(x / 37.0))
+    runs = []
+    for q in (0, O.Q_PSOD_COPY):
+        p = O.make_prop(case["np"], case["dt"], 0.0, 50 * case["dt"], case["sh"], case["sm"],
+                        shm=case["shm"], quirks=q)
+        runs.append(O.psod(p, case["vpot"], psi.real, psi.imag))
+    assert np.max(np.abs(runs[0]["c"] - runs[1]["c"])) > 1e-5  # far above rounding
+    real = []
+    for q in (0, O.Q_PSOD_COPY):
+        p = O.make_prop(case["np"], case["dt"], 0.0, 50 * case["dt"], case["sh"], case["sm"],
+                        shm=case["shm"], quirks=q)
+        real.append(O.psod(p, case["vpot"], case["psi"], np.zeros(n)))
+    assert np.array_equal(real[0]["c"], real[1]["c"])
 
 
 def test_spo_kinetic_defect_is_what_the_executable_does(oracle):
