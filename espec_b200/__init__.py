@@ -6,7 +6,7 @@ and the batched split-operator interface.
 """
 from . import _native
 from ._native import EspecError, load
-from .grid import SilGrid, SodGrid, SpoGrid
+from .grid import PsodGrid, SilGrid, SodGrid, SpoGrid
 from .spo import SodBatch, SpoBatch
 
-__all__ = ["EspecError", "SilGrid", "SodGrid", "SpoGrid", "SodBatch", "SpoBatch", "load", "workloads"]
+__all__ = ["EspecError", "PsodGrid", "SilGrid", "SodGrid", "SpoGrid", "SodBatch", "SpoBatch", "load", "workloads"]

@@ -1,10 +1,13 @@
-// sil.cu -- short-iterative-Lanczos propagation on one grid (1D/2D/3D),
-// FP64: the cooperative kernel described in sil.cuh, the finite-difference
-// energy kernel, and the grid plan behind espec_grid_* (include/espec_gpu.h).
+// sil.cu -- propagation on one grid (1D/2D/3D) with the finite-difference
+// Hamiltonian, FP64: the short-iterative-Lanczos cooperative kernel described
+// in sil.cuh, the second-order-differences kernel (.PSOD), the
+// finite-difference energy kernel, and the grid plan behind espec_grid_*
+// (include/espec_gpu.h).
 #include <cuda/atomic>
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <utility>
 #include <vector>
 
 #include "espec_gpu.h"
@@ -459,6 +462,89 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   }
 }
 
+// Second-order differences with H = AU (psod.f:64-205, sod.f:64-123), one
+// cooperative kernel per run.  Each step overwrites the state one step back
+// in place, psi_{n-1} <- psi_{n-1} - i c H psi_n (.VOPTIC: - c VABC psi_n;
+// .SMOOTHW: the whole right side times the mask), reads psi_n's neighbours
+// only, and ends in one grid barrier that also sums C = <psi0|psi_{n+1}>;
+// then the two buffers swap roles.  From the start: C(0), an Euler step of
+// c = CST/4 and a midpoint step of CST/2 to TI + DT, psi_{n-1} reset to psi0
+// (with the reference's copy defect on request), then steps of CST.
+__global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
+  __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
+  __shared__ double s_red[kSilThreads];
+  __shared__ int s_flag[2];
+  const Range r = my_range(a.n);
+  const int t = threadIdx.x;
+  double *un = a.u, *vn = a.v, *um = a.up, *vm = a.vp;
+  auto reduce_c = [&](double (&q)[4], int slot) -> bool {
+    block_sum<4>(q, sp, scratch);
+    if (!grid_reduce(a, sp, st, 4, s_flag, s_red)) return false;
+    if (t == 0 && blockIdx.x == 0 && slot >= 0)
+      a.c_out[slot] = make_double2(st[0] + st[1], st[2] - st[3]);
+    return true;
+  };
+  auto step = [&](double c, int slot) -> bool {
+    double q[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+      const double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
+      const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
+      double nu, nv;
+      if (a.kabs == 1) {
+        const double w = a.vabc[k];
+        nu = um[k] + c * hv - c * w * uk;
+        nv = vm[k] - c * hu - c * w * vk;
+      } else if (a.kabs == 2) {
+        const double w = a.vabc[k];
+        nu = w * (um[k] + c * hv);
+        nv = w * (vm[k] - c * hu);
+      } else {
+        nu = um[k] + c * hv;
+        nv = vm[k] - c * hu;
+      }
+      um[k] = nu;
+      vm[k] = nv;
+      const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
+      q[0] += u0k * nu;
+      q[1] += v0k * nv;
+      q[2] += u0k * nv;
+      q[3] += v0k * nu;
+    }
+    if (!reduce_c(q, slot)) return false;
+    double* x = un;
+    un = um;
+    um = x;
+    x = vn;
+    vn = vm;
+    vm = x;
+    return true;
+  };
+  if (a.write_c0) {  // C(0), psod.f:89-90 with U2 = U0, V2 = V0
+    double q[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+      const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
+      q[0] += u0k * u0k;
+      q[1] += v0k * v0k;
+      q[2] += u0k * v0k;
+      q[3] += v0k * u0k;
+    }
+    if (!reduce_c(q, 0)) return;
+  }
+  int s0 = 1;
+  if (a.start && a.nsteps >= 1) {
+    if (!step(0.25 * a.cst, -1)) return;  // psod.f:120-121
+    if (!step(0.5 * a.cst, 1)) return;    // psod.f:123-124
+    for (int k = r.lo + t; k < r.hi; k += kSilThreads) {  // psod.f:136-141
+      um[k] = __ldg(a.u0 + k);
+      vm[k] = (a.copy_quirk && (k & 1)) ? __ldg(a.v0 + k - 1) : __ldg(a.v0 + k);
+    }
+    __syncthreads();
+    s0 = 2;
+  }
+  for (int s = s0; s <= a.nsteps; ++s)
+    if (!step(a.cst, s)) return;
+}
+
 // <u|H u> + <v|H v> and |u|^2 + |v|^2 (EIGENERG, eigenerg.f:56-66): per-CTA
 // partials, then one CTA sums them in CTA order
 __global__ void __launch_bounds__(kSilThreads) sil_energy_kernel(SilArgs a, double* part) {
@@ -499,6 +585,7 @@ struct espec_grid_plan {
   bool loaded = false, has_state = false;
   double *d_vpot = nullptr, *d_mask = nullptr, *d_u = nullptr, *d_v = nullptr;
   double *d_u0 = nullptr, *d_v0 = nullptr, *d_L = nullptr, *d_work = nullptr, *d_wbuf = nullptr;
+  double *d_up = nullptr, *d_vp = nullptr;  // PSOD: the state one step back
   double *d_part = nullptr, *d_tot = nullptr, *d_epart = nullptr, *d_eout = nullptr;
   unsigned* d_bar = nullptr;
   int* d_err = nullptr;
@@ -508,7 +595,8 @@ struct espec_grid_plan {
 
 static void grid_free(espec_grid_plan* p) {
   void* b[] = {p->d_vpot, p->d_mask, p->d_u, p->d_v, p->d_u0, p->d_v0, p->d_L, p->d_work,
-               p->d_wbuf, p->d_part, p->d_tot, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c};
+               p->d_wbuf, p->d_part, p->d_tot, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c,
+               p->d_up, p->d_vp};
   for (void* x : b)
     if (x) cudaFree(x);
 }
@@ -548,6 +636,15 @@ static SilArgs sil_args(const espec_grid_plan* p) {
   a.m = p->m;
   a.quirk = (p->quirks & ESPEC_Q_SIL_INPLACE) != 0;
   a.cst = p->dt_fs / ESPEC_SHFS;
+  if (p->method == ESPEC_PSOD) {
+    a.cst = 2.0 * p->dt_fs / ESPEC_SHFS;  // psod.f:82
+    a.mask = nullptr;
+    a.up = p->d_up;
+    a.vp = p->d_vp;
+    a.vabc = p->d_mask;
+    a.kabs = p->absorb == ESPEC_ABS_VOPTIC ? 1 : (p->absorb == ESPEC_ABS_SMOOTHW ? 2 : 0);
+    a.copy_quirk = (p->quirks & ESPEC_Q_PSOD_COPY) != 0;
+  }
   return a;
 }
 
@@ -555,16 +652,20 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
                                  const double* shm, double dt_fs, int mp, int precision,
                                  int absorb, int quirks) {
   if (!out || !np || !shm) return set_error(ESPEC_EINVAL, "null argument");
-  if (method != ESPEC_SIL) return set_error(ESPEC_EINVAL, "grid plans run ESPEC_SIL");
-  if (precision != ESPEC_FP64) return set_error(ESPEC_EINVAL, "the SIL propagator runs in FP64");
+  if (method != ESPEC_SIL && method != ESPEC_PSOD)
+    return set_error(ESPEC_EINVAL, "grid plans run ESPEC_SIL or ESPEC_PSOD");
+  if (precision != ESPEC_FP64) return set_error(ESPEC_EINVAL, "grid plans run in FP64");
   if (ndim < 1 || ndim > 3) return set_error(ESPEC_EINVAL, "ndim must be 1, 2 or 3");
-  if (mp < 1 || mp > kSilMaxM) return set_error(ESPEC_EINVAL, "Lanczos order must be 1..16");
-  if (absorb == ESPEC_ABS_VOPTIC)
+  const bool psod = method == ESPEC_PSOD;
+  if (psod) mp = 0;
+  if (!psod && (mp < 1 || mp > kSilMaxM))
+    return set_error(ESPEC_EINVAL, "Lanczos order must be 1..16");
+  if (!psod && absorb == ESPEC_ABS_VOPTIC)
     return set_error(ESPEC_EINVAL, "SIL takes no complex absorbing potential (real Lanczos)");
-  if (absorb != ESPEC_ABS_NONE && absorb != ESPEC_ABS_SMOOTHW)
+  if (absorb != ESPEC_ABS_NONE && absorb != ESPEC_ABS_SMOOTHW && absorb != ESPEC_ABS_VOPTIC)
     return set_error(ESPEC_EINVAL, "unknown absorber type");
-  if (quirks & ~ESPEC_Q_SIL_INPLACE)
-    return set_error(ESPEC_EINVAL, "only ESPEC_Q_SIL_INPLACE applies to SIL");
+  if (quirks & ~(psod ? ESPEC_Q_PSOD_COPY : ESPEC_Q_SIL_INPLACE))
+    return set_error(ESPEC_EINVAL, "quirk not applicable to this method");
   long n = 1;
   for (int i = 0; i < ndim; ++i) {
     if (np[i] < 1) return set_error(ESPEC_EINVAL, "grid size must be positive");
@@ -588,7 +689,8 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, sil_kernel, kSilThreads, 0);
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, psod ? psod_kernel : sil_kernel,
+                                                      kSilThreads, 0);
   if (e != cudaSuccess) {
     delete p;
     return set_cuda_error("device query", e);
@@ -607,9 +709,14 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   double** bufs8[] = {&p->d_vpot, &p->d_mask, &p->d_u, &p->d_v, &p->d_u0, &p->d_v0};
   for (double** b : bufs8)
     if ((rc = ck(cudaMalloc(b, nb), "cudaMalloc"))) return fail(rc);
-  if ((rc = ck(cudaMalloc(&p->d_L, nb * 2 * mp), "cudaMalloc"))) return fail(rc);
-  if ((rc = ck(cudaMalloc(&p->d_work, nb * 2), "cudaMalloc"))) return fail(rc);
-  if ((rc = ck(cudaMalloc(&p->d_wbuf, nb * 2), "cudaMalloc"))) return fail(rc);
+  if (psod) {
+    if ((rc = ck(cudaMalloc(&p->d_up, nb), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_vp, nb), "cudaMalloc"))) return fail(rc);
+  } else {
+    if ((rc = ck(cudaMalloc(&p->d_L, nb * 2 * mp), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_work, nb * 2), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_wbuf, nb * 2), "cudaMalloc"))) return fail(rc);
+  }
   if ((rc = ck(cudaMalloc(&p->d_part, sizeof(double) * kSilNQ * p->nblocks), "cudaMalloc")))
     return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_tot, sizeof(double) * kSilNQ), "cudaMalloc"))) return fail(rc);
@@ -627,13 +734,13 @@ extern "C" int espec_grid_load(espec_grid_plan* p, const double* vpot, const dou
                                const double* psi_re, const double* psi_im, int where,
                                void* stream) {
   if (!p || !vpot || !psi_re) return set_error(ESPEC_EINVAL, "null argument");
-  if (p->absorb == ESPEC_ABS_SMOOTHW && !vabc) return set_error(ESPEC_EINVAL, "mask missing");
+  if (p->absorb != ESPEC_ABS_NONE && !vabc) return set_error(ESPEC_EINVAL, "absorber table missing");
   cudaStream_t st = (cudaStream_t)stream;
   const cudaMemcpyKind kind =
       where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   const size_t nb = (size_t)p->n * 8;
   GRID_CK(cudaMemcpyAsync(p->d_vpot, vpot, nb, kind, st));
-  if (p->absorb == ESPEC_ABS_SMOOTHW) GRID_CK(cudaMemcpyAsync(p->d_mask, vabc, nb, kind, st));
+  if (p->absorb != ESPEC_ABS_NONE) GRID_CK(cudaMemcpyAsync(p->d_mask, vabc, nb, kind, st));
   GRID_CK(cudaMemcpyAsync(p->d_u0, psi_re, nb, kind, st));
   if (psi_im) {
     GRID_CK(cudaMemcpyAsync(p->d_v0, psi_im, nb, kind, st));
@@ -643,6 +750,7 @@ extern "C" int espec_grid_load(espec_grid_plan* p, const double* vpot, const dou
   GRID_CK(cudaMemcpyAsync(p->d_u, p->d_u0, nb, cudaMemcpyDeviceToDevice, st));
   GRID_CK(cudaMemcpyAsync(p->d_v, p->d_v0, nb, cudaMemcpyDeviceToDevice, st));
   p->loaded = true;
+  p->has_state = false;
   return ESPEC_OK;
 }
 
@@ -663,6 +771,26 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
   SilArgs a = sil_args(p);
   a.nsteps = nsteps;
   a.write_c0 = from_start ? 1 : 0;
+  if (p->method == ESPEC_PSOD) {
+    if (from_start) {  // psod.f:83-88: U2 = U1 = U0, V2 = V1 = V0
+      GRID_CK(cudaMemcpyAsync(p->d_up, p->d_u0, nb, cudaMemcpyDeviceToDevice, st));
+      GRID_CK(cudaMemcpyAsync(p->d_vp, p->d_v0, nb, cudaMemcpyDeviceToDevice, st));
+    } else if (!p->has_state) {
+      return set_error(ESPEC_EINVAL, "a PSOD plan continues a run: call espec_grid_run first");
+    }
+    a.start = from_start ? 1 : 0;
+    void* args[] = {&a};
+    GRID_CK(cudaLaunchCooperativeKernel((const void*)psod_kernel, dim3(p->nblocks),
+                                        dim3(kSilThreads), args, 0, st));
+    // the kernel swaps the roles of the two state buffers once per step
+    const long swaps = from_start ? (nsteps >= 1 ? nsteps + 1 : 0) : nsteps;
+    if (swaps & 1) {
+      std::swap(p->d_u, p->d_up);
+      std::swap(p->d_v, p->d_vp);
+    }
+    p->has_state = true;
+    return ESPEC_OK;
+  }
   void* args[] = {&a};
   GRID_CK(cudaLaunchCooperativeKernel((const void*)sil_kernel, dim3(p->nblocks), dim3(kSilThreads),
                                       args, 0, st));
@@ -716,6 +844,23 @@ extern "C" int espec_grid_energies(espec_grid_plan* p, double* e, double* norm, 
   GRID_CK(cudaStreamSynchronize(st));
   *e = h[0];
   *norm = h[1];
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_previous(espec_grid_plan* p, double* psi_re, double* psi_im, int where,
+                                   void* stream) {
+  if (!p || p->method != ESPEC_PSOD || !p->has_state)
+    return set_error(ESPEC_EINVAL, "previous state exists for run PSOD plans only");
+  cudaStream_t st = (cudaStream_t)stream;
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;
+  const size_t nb = (size_t)p->n * 8;
+  if (psi_re) GRID_CK(cudaMemcpyAsync(psi_re, p->d_up, nb, kind, st));
+  if (psi_im) GRID_CK(cudaMemcpyAsync(psi_im, p->d_vp, nb, kind, st));
+  int err = 0;
+  GRID_CK(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GRID_CK(cudaStreamSynchronize(st));
+  if (err) return set_error(ESPEC_ECUDA, "a grid barrier of the PSOD kernel timed out");
   return ESPEC_OK;
 }
 

@@ -1,4 +1,6 @@
-// sil.cuh -- short-iterative-Lanczos propagation (eSPec's .PSIL/.PLNZ:
+// sil.cuh -- grid propagators with the finite-difference Hamiltonian:
+// second-order differences (.PSOD, psod.f/sod.f), and short-iterative-Lanczos
+// propagation (eSPec's .PSIL/.PLNZ:
 // plnz.f:71-151, sil.f:70-181, lnz.f:76-119, reort.f:65-80, au1d.f/au2di.f/
 // au3d.f) on one 1D, 2D or 3D grid, FP64, as ONE cooperative persistent
 // kernel.
@@ -49,7 +51,16 @@ struct SilArgs {
   int* err;       // set when a barrier wait gave up
   double2* c_out;  // C(t) of every step: slot s for step s (slot 0 only if write_c0)
   int m, nsteps, quirk, write_c0;
-  double cst;  // dt in atomic units
+  double cst;  // dt in atomic units (SIL); 2 dt in atomic units (PSOD)
+  // second-order differences with the same H (.PSOD, psod.f / sod.f): the
+  // state one step before (u, v), the absorber (.VOPTIC potential or
+  // .SMOOTHW mask) and its kind, the start-up switch and the restart-copy
+  // defect of psod.f:136-141
+  double* up;
+  double* vp;
+  const double* vabc;
+  int kabs;  // 0 none, 1 .VOPTIC, 2 .SMOOTHW
+  int start, copy_quirk;
 };
 
 }  // namespace espec

@@ -15,6 +15,11 @@ from . import _native as N
 
 
 class SilGrid:
+    """Short-iterative-Lanczos propagation (PLNZ, plnz.f:71-151) of one packet
+    on a 1D/2D/3D grid with the finite-difference Hamiltonian, FP64."""
+
+    method = N.SIL
+
     def __init__(self, np_, shm, dt_fs, mp, absorb=N.ABS_NONE, quirks=0):
         lib = N.load()
         self.np = [int(x) for x in np_]
@@ -23,7 +28,7 @@ class SilGrid:
         npa = np.array(self.np + [1] * (3 - self.ndim), dtype=np.int32)
         shma = N.f64(list(shm) + [0.0] * (3 - self.ndim))
         self._h = C.c_void_p()
-        rc = lib.espec_grid_create(C.byref(self._h), N.SIL, self.ndim,
+        rc = lib.espec_grid_create(C.byref(self._h), self.method, self.ndim,
                                    npa.ctypes.data_as(C.POINTER(C.c_int)),
                                    shma.ctypes.data_as(C.POINTER(C.c_double)), float(dt_fs),
                                    int(mp), N.FP64, absorb, quirks)
@@ -76,6 +81,23 @@ class SilGrid:
             self.close()
         except Exception:
             pass
+
+
+class PsodGrid(SilGrid):
+    """Second-order differences with the finite-difference Hamiltonian (PSOD,
+    psod.f:64-205) of one packet on a 1D/2D/3D grid, FP64; `previous()` is
+    psi(TF - dt)."""
+
+    method = N.PSOD
+
+    def __init__(self, np_, shm, dt_fs, absorb=N.ABS_NONE, quirks=0):
+        super().__init__(np_, shm, dt_fs, 0, absorb=absorb, quirks=quirks)
+
+    def previous(self, stream=None):
+        pr, pi = np.zeros(self.n), np.zeros(self.n)
+        N.check(N.load().espec_grid_previous(self._h, N.ptr(pr), N.ptr(pi), N.MEM_HOST, stream),
+                "espec_grid_previous")
+        return pr + 1j * pi
 
 
 class SpoGrid:

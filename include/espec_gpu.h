@@ -43,6 +43,7 @@ extern "C" {
 #define ESPEC_SPO 0         /* split operator, FFT kinetic term (.PFSPO)     */
 #define ESPEC_SOD 1         /* second-order differences, FFT kinetic (.PFSOD) */
 #define ESPEC_SIL 2         /* short-iterative Lanczos, FD Hamiltonian (.PSIL) */
+#define ESPEC_PSOD 3        /* second-order differences, FD Hamiltonian (.PSOD) */
 
 /* reproduce reference defects on request (FP64 form only) */
 #define ESPEC_Q_SPO_INPLACE 1   /* spofft.f:150-153 kinetic multiply            */
@@ -50,6 +51,7 @@ extern "C" {
 #define ESPEC_Q_SIL_INPLACE 4   /* sil.f:145-148 sin term uses the cos-scaled U   */
 #define ESPEC_Q_FFTNT_SP 8      /* cfft.f:35 TWOPI from a single-precision literal */
 #define ESPEC_Q_DIGT_ND 16      /* dkeft.f:80-137 2D/3D kinetic table as written   */
+#define ESPEC_Q_PSOD_COPY 32    /* psod.f:136-141 restart copy sets V1(I+1) = V0(I) */
 
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
@@ -215,13 +217,21 @@ int espec_spo_run_static(int npk, const int* npts, const double* sh,
  * ESPEC_ABS_SMOOTHW (mask applied after each step, sil.f:171-175); quirks:
  * ESPEC_Q_SIL_INPLACE.  One cooperative launch per run; C(t) = <psi0|psi(t)>
  * every step (nsteps+1 samples).
+ *
+ * ESPEC_PSOD replaces the time loop of PSOD (psod.f:64-205) with PSODAUX
+ * (sod.f:64-123) and the same AU: psi(t+dt) = psi(t-dt) - 2 i dt H psi(t),
+ * started by an Euler step to t + dt/2 and a midpoint step to t + dt; mp is
+ * ignored; absorb: ESPEC_ABS_NONE, ESPEC_ABS_VOPTIC (vabc = the complex
+ * absorbing potential) or ESPEC_ABS_SMOOTHW (vabc = the mask); quirks:
+ * ESPEC_Q_PSOD_COPY.  One cooperative launch per run, one grid barrier per
+ * step.
  * ---------------------------------------------------------------------- */
 typedef struct espec_grid_plan espec_grid_plan;
 
 int espec_grid_create(espec_grid_plan** plan, int method, int ndim, const int* np,
                       const double* shm, double dt_fs, int mp, int precision,
                       int absorb, int quirks);
-/* psi_im may be NULL; vabc: the .SMOOTHW mask (ignored otherwise) */
+/* psi_im may be NULL; vabc: the absorber table (ignored without one) */
 int espec_grid_load(espec_grid_plan* plan, const double* vpot, const double* vabc,
                     const double* psi_re, const double* psi_im, int where,
                     void* stream);
@@ -239,6 +249,9 @@ int espec_grid_energies(espec_grid_plan* plan, double* e, double* norm, void* st
  * into dst(1:N, 1:MP) with leading dimension ld >= N (column-major) */
 int espec_grid_basis(espec_grid_plan* plan, int chain, double* dst, int ld, int where,
                      void* stream);
+/* ESPEC_PSOD plans: psi(TF - dt) of the last run (synchronises) */
+int espec_grid_previous(espec_grid_plan* plan, double* psi_re, double* psi_im, int where,
+                        void* stream);
 long espec_grid_npoints(const espec_grid_plan* plan);
 void espec_grid_destroy(espec_grid_plan* plan);
 
