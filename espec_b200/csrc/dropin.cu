@@ -1,10 +1,10 @@
 // dropin.cu -- Fortran-callable drop-ins for eSPec's propagators PSPOFFT
-// (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D/2D/3D) and PLNZ
-// (plnz.f:1-155; 1D/2D/3D).
+// (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D/2D/3D), PLNZ
+// (plnz.f:1-155; 1D/2D/3D) and PSOD (psod.f:1-208; 1D/2D/3D).
 //
 // Each call propagates one packet on the GPU through a one-packet plan and
 // leaves in the caller's arrays what the reference routine leaves there:
-// psi(TF) in U1/V1 (PSODFFT: psi(TF) in U2/V2 and psi(TF-dt) in U1/V1), the
+// psi(TF) in U1/V1 (PSODFFT, PSOD: psi(TF) in U2/V2 and psi(TF-dt) in U1/V1), the
 // kinetic table in TC, C(t) every LC steps in columns MPR/MPI of LNZVC, and
 // INFO = 1 when the energy (or norm) drifted more than TOL percent.  With
 // PRTCRL = '.YES' or '.PARTIAL' the partial auto-correlation table is written
@@ -125,7 +125,16 @@ const char* kSilHead =
     "\n"
     "          *t*       *Energy*        *Cr(t)*       *Ci(t)*    *|C(t)|^2*      *|C|*\n";
 
-enum Kind { kSpo, kSod, kSil };
+// the table head of psod.f:101-106 (its FORMAT 1011 titles the fifth column
+// *|C(t)|^2*)
+const char* kPsodHead =
+    " \n"
+    " Partial auto-correlation function:\n"
+    " ==================================\n"
+    "\n"
+    "       *t/fs*       *E/a.u.*        *Cr(t)*       *Ci(t)*    *|C(t)|^2*      *|C|*\n";
+
+enum Kind { kSpo, kSod, kSil, kPsod };
 
 // One packet's propagation through a GPU plan: the segment, C(t) and energy
 // calls of the plan type behind it.
@@ -167,24 +176,29 @@ struct DropIn {
   }
   bool printed(int s) const { return prt == 2 || (prt == 1 && s % lc == 0); }
   // E and the printed norm: sqrt(FNR^2 + FNI^2) with FNI = 0 for the FFT
-  // propagators (pspofft.f:96-98), FNR itself for PLNZ (plnz.f:91)
+  // propagators (pspofft.f:96-98), FNR itself for PLNZ (plnz.f:91) and PSOD
+  // (psod.f:95; squared in the rows of its loop, psod.f:183)
   int energies(double& e, double& fnt) {
     double nr;
     if (be.energy(e, nr)) return fail_lib();
-    fnt = kind == kSil ? nr : std::sqrt(nr * nr);
+    fnt = (kind == kSil || kind == kPsod) ? nr : std::sqrt(nr * nr);
     return 0;
   }
   // INFO drift test: PSPOFFT tests the norm only with an absorber
   // (pspofft.f:137-142), PSODFFT only without one (psodfft.f:178-183), PLNZ
   // always (plnz.f:137-138)
+  // always (plnz.f:137-138); PSOD only without an absorber, with which its
+  // INFO stays 0 (psod.f:184-189, 197-202)
   void drift(double et, double fnt) {
+    if (kind == kPsod && absorb) return;
     const bool de = std::fabs((et - e0) / e0) * 1.0e2 > tol;
     const bool dn = std::fabs((fnt - f0) / f0) * 1.0e2 > tol;
-    const bool norm_counts = kind == kSil || (kind == kSpo) == absorb;
+    const bool norm_counts = kind == kSil || kind == kPsod || (kind == kSpo) == absorb;
     if (de || (norm_counts && dn)) *info = 1;
   }
   std::string row(double t, double e, double cr, double ci, double fnt) const {
-    const double ct = kind == kSil ? cr * cr + ci * ci : std::sqrt(cr * cr + ci * ci);
+    const double ct = (kind == kSil || kind == kPsod) ? cr * cr + ci * ci
+                                                      : std::sqrt(cr * cr + ci * ci);
     return crl_row(t, e, cr, ci, ct, fnt);
   }
 
@@ -206,7 +220,7 @@ struct DropIn {
         if (be.run(k) || be.cvals(k, cre.data(), cim.data())) return fail_lib();
         store_c(0, cre[0], cim[0]);
         if (prt) {
-          emit(kind == kSil ? kSilHead : kCrlHead);
+          emit(kind == kSil ? kSilHead : (kind == kPsod ? kPsodHead : kCrlHead));
           emit(row(ti, e0, cre[0], cim[0], f0));
         }
       } else {
@@ -220,6 +234,7 @@ struct DropIn {
       if (k > 0 && printed(stop)) {
         double et, fnt;
         if (energies(et, fnt)) return -1;
+        if (kind == kPsod && stop >= 2) fnt = fnt * fnt;  // psod.f:183
         if (checked(stop)) drift(et, fnt);
         emit(row(t_of(stop), et, cre[k], cim[k], fnt));
       }
@@ -229,6 +244,7 @@ struct DropIn {
 };
 
 // absorber of the GPU plan: the prefix tests of spofft.f:65,162 / sodfft.f:66,108
+// (PSOD tests its own: sod.f:71, 78)
 int absorber(bool absorb, const char* tp, size_t len) {
   if (!absorb) return ESPEC_ABS_NONE;
   if (fstr_is(tp, len, ".VOPTIC")) return ESPEC_ABS_VOPTIC;
@@ -509,6 +525,91 @@ extern "C" void plnz_(const int* absorb, const int* change, const char* dim, con
     return;
   }
   if (clamp && *change) *mp = m;  // MP is modified through LNZ's NREORT argument
+  std::fflush(stdout);
+}
+
+// PSOD: one espec_grid_plan (1D, 2D or 3D), method ESPEC_PSOD
+extern "C" void psod_(const int* absorb, const char* dim, const char* prtcrl, const char* tpabsor,
+                      int* info, const int* lc, const int* mp, const int* mpi, const int* mpr,
+                      const int* mxdct, const int* n, const double* dt, const double* ti,
+                      const double* tf, const double* tol, const int* np, const double* shm,
+                      double* u1, double* u2, double* v1, double* v2, const double* xi,
+                      const double* xf, const double* vpot, const double* vabc, double* work,
+                      const double* var, double* lnzvc, size_t dim_len, size_t prtcrl_len,
+                      size_t tpabsor_len) {
+  (void)mp; (void)xi; (void)xf; (void)work; (void)var;
+  DropIn d;
+  d.name = "PSOD";
+  d.kind = kPsod;
+  d.info = info;
+  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  int ndim = 0;
+  if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
+  if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
+  if (fstr_is(dim, dim_len, ".3D")) ndim = 3;
+  if (!ndim) {
+    d.fail("DIM must be '.1D', '.2D' or '.3D'");
+    return;
+  }
+  long npts = 1;
+  for (int a = 0; a < ndim; ++a) npts *= np[a];
+  if (npts != *n) {
+    d.fail("N differs from the product of NP");
+    return;
+  }
+  if (d.lc < 1) {
+    d.fail("LC must be at least 1");
+    return;
+  }
+  int ab = ESPEC_ABS_NONE;  // sod.f:71-82
+  if (d.absorb) {
+    if (fstr_is(tpabsor, tpabsor_len, ".VOPTIC")) {
+      ab = ESPEC_ABS_VOPTIC;
+    } else if (fstr_is(tpabsor, tpabsor_len, ".SMOOTHW") || fstr_is(tpabsor, tpabsor_len, ".SMRS")) {
+      ab = ESPEC_ABS_SMOOTHW;
+    } else {
+      d.fail("SOD propagation error: absorber type not '.VOPTIC', '.SMOOTHW' or '.SMRS'");
+      return;
+    }
+  }
+  espec_grid_plan* plan = nullptr;
+  struct Guard {
+    espec_grid_plan*& p;
+    ~Guard() { espec_grid_destroy(p); }
+  } guard{plan};
+  if (espec_grid_create(&plan, ESPEC_PSOD, ndim, np, shm, d.dt, 0, ESPEC_FP64, ab,
+                        ESPEC_Q_PSOD_COPY) ||
+      espec_grid_load(plan, vpot, ab == ESPEC_ABS_NONE ? nullptr : vabc, u1, v1, ESPEC_MEM_HOST,
+                      nullptr)) {
+    d.fail_lib();
+    return;
+  }
+  d.be.run = [&](int k) { return espec_grid_run(plan, k, nullptr); };
+  d.be.cont = [&](int k) { return espec_grid_continue(plan, k, nullptr); };
+  d.be.cvals = [&](int, double* cr, double* ci) {
+    return espec_grid_results(plan, cr, ci, nullptr, nullptr, ESPEC_MEM_HOST, nullptr);
+  };
+  d.be.energy = [&](double& e, double& nr) { return espec_grid_energies(plan, &e, &nr, nullptr); };
+  double fnt;
+  if (d.energies(d.e0, fnt)) return;
+  d.f0 = fnt;
+  // start-up to T = TI+DT (psod.f:118-141), then DO T = TI+2*DT, TF+DT, DT
+  // (psod.f:143); only rows of the loop run the drift test
+  const int nsteps = 1 + do_count(*ti + 2 * *dt, *tf + *dt, *dt);
+  std::vector<double> tt(nsteps + 1, *ti);
+  tt[1] = *ti + *dt;
+  if (nsteps >= 2) tt[2] = *ti + 2 * *dt;
+  for (int s = 3; s <= nsteps; ++s) tt[s] = tt[s - 1] + *dt;
+  if (d.propagate(nsteps, [&](int s) { return tt[s]; }, [](int s) { return s >= 2; })) return;
+  // final energy and drift test after the loop (psod.f:192-202)
+  double et;
+  if (d.energies(et, fnt)) return;
+  d.drift(et, fnt);
+  if (espec_grid_results(plan, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
+      espec_grid_previous(plan, u1, v1, ESPEC_MEM_HOST, nullptr)) {
+    d.fail_lib();
+    return;
+  }
   std::fflush(stdout);
 }
 

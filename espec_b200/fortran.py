@@ -104,6 +104,32 @@ def plnz(*, absorb, change, dim, prtcrl, tpabsor, lc, lmtreort, mp, mpi, mpr, mx
     return info.value, mp_c.value
 
 
+def psod(*, absorb, dim, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_, shm,
+         vpot, vabc, u1, v1, u2, v2, lnzvc, mp=0):
+    """PSOD: second-order differences with the finite-difference Hamiltonian
+    (1D/2D/3D grid, flattened x fastest); on return U2 + i V2 is psi(TF) and
+    U1 + i V1 is psi(TF - dt).  Returns INFO."""
+    info = C.c_int(0)
+    npa = np.array(list(np_) + [1] * (3 - len(np_)), dtype=np.int32)
+    shma = N.f64(list(shm) + [0.0] * (3 - len(shm)))
+    vp = N.f64(vpot)
+    va = N.f64(vabc) if vabc is not None else np.zeros(n)
+    sc = dict(absorb=C.c_int(1 if absorb else 0), lc=C.c_int(lc), mp=C.c_int(mp),
+              mpi=C.c_int(mpi), mpr=C.c_int(mpr), mxdct=C.c_int(mxdct), n=C.c_int(n),
+              dt=C.c_double(dt), ti=C.c_double(ti), tf=C.c_double(tf), tol=C.c_double(tol))
+    scratch = np.zeros(max(n, 1))
+    xi = np.zeros(3)
+    b = {k: v.encode() for k, v in dict(dim=dim, prtcrl=prtcrl, tpabsor=tpabsor).items()}
+    N.load().psod_(
+        C.byref(sc["absorb"]), b["dim"], b["prtcrl"], b["tpabsor"], C.byref(info),
+        C.byref(sc["lc"]), C.byref(sc["mp"]), C.byref(sc["mpi"]), C.byref(sc["mpr"]),
+        C.byref(sc["mxdct"]), C.byref(sc["n"]), C.byref(sc["dt"]), C.byref(sc["ti"]),
+        C.byref(sc["tf"]), C.byref(sc["tol"]), N.ptr(npa), N.ptr(shma), _arr(u1), _arr(u2),
+        _arr(v1), _arr(v2), N.ptr(xi), N.ptr(xi), N.ptr(vp), N.ptr(va), N.ptr(scratch),
+        N.ptr(scratch), _arr(lnzvc), len(b["dim"]), len(b["prtcrl"]), len(b["tpabsor"]))
+    return info.value
+
+
 def format_crl_row(t, e, cr, ci, ct, fnt):
     """One row of the partial auto-correlation table (FORMAT 1021, pspofft.f:148)."""
     buf = C.create_string_buffer(256)

@@ -60,7 +60,7 @@ extern "C" {
 #define ESPEC_SHFS 2.4188843243e-2  /* fs per atomic unit of time (pspofft.f:76) */
 
 /* ----------------------------------------------------------------------
- * Fortran-callable drop-ins (1D).  Same arguments, same outputs and the
+ * Fortran-callable drop-ins.  Same arguments, same outputs and the
  * same printed partial auto-correlation table as the reference routines;
  * the defects of the reference's arithmetic are reproduced.  A case the GPU
  * path does not run (PSPOFFT/PSODFFT: unsupported grid sizes; PLNZ: order
@@ -105,6 +105,19 @@ void plnz_(const int* absorb, const int* change, const char* dim,
            const double* xi, const double* xf, double* wu, double* wv,
            double* wp, double* work, const double* var, double* lnzvc,
            size_t dim_len, size_t prtcrl_len, size_t tpabsor_len);
+/* replaces SUBROUTINE PSOD (psod.f:1-3; called from espec.f:1362), 1D/2D/3D
+ * (espec_grid_* plan, method ESPEC_PSOD, the reference's restart-copy
+ * defect): psi(TF) in U2/V2, psi(TF-dt) in U1/V1; an absorber other than
+ * .VOPTIC/.SMOOTHW/.SMRS, where the reference STOPs, sets INFO = 2 */
+void psod_(const int* absorb, const char* dim, const char* prtcrl,
+           const char* tpabsor, int* info, const int* lc, const int* mp,
+           const int* mpi, const int* mpr, const int* mxdct, const int* n,
+           const double* dt, const double* ti, const double* tf,
+           const double* tol, const int* np, const double* shm, double* u1,
+           double* u2, double* v1, double* v2, const double* xi,
+           const double* xf, const double* vpot, const double* vabc,
+           double* work, const double* var, double* lnzvc, size_t dim_len,
+           size_t prtcrl_len, size_t tpabsor_len);
 /* replace SUBROUTINE HWHM (hwhm.f:1-80; TAL is scaled in place) and
  * SUBROUTINE SPECTRUMTD (spectrumtd.f:1-116; prints the spectrum table,
  * sets DE < 0 to 0), called at espec.f:1618-1624: the arithmetic runs on the

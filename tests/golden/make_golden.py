@@ -125,7 +125,7 @@ def partial_text(out, first=150, last=50):
     return "\n".join(head + keep) + "\n", len(rows)
 
 
-TEXT_CASES = ("morse1d_spo", "morse1d_sod", "morse1d_spo_voptic")
+TEXT_CASES = ("morse1d_spo", "morse1d_sod", "morse1d_spo_voptic", "morse1d_psod")
 
 
 def case_test8_text():

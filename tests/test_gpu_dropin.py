@@ -388,3 +388,94 @@ def test_psodfft_2d_golden_deck(oracle, capfd):
     ok = np.isfinite(gold[:, 2])
     rel = np.abs(lnzvc[:nc, 1][ok] - gold[ok, 2]) / np.maximum(1.0, np.abs(gold[ok, 2]))
     assert rel.max() < 1e-6
+
+
+# ---------------------------------------------------------------------------
+def call_psod(case, prtcrl, lc=None, tf=None, tol=None, ncols=4, mpr=2, mpi=3, psi=None):
+    n = int(np.prod(case["np"]))
+    lc = case["lc"] if lc is None else lc
+    tf = case["tf"] if tf is None else tf
+    nsteps = int(round((tf - case["ti"]) / case["dt"])) + 4
+    mxdct = nsteps // lc + 4
+    lnzvc = np.zeros((mxdct, ncols), order="F")
+    psi = np.asarray(case["psi"] if psi is None else psi)
+    u1, v1 = np.array(psi.real, dtype=np.float64), np.array(np.imag(psi), dtype=np.float64)
+    u2, v2 = np.zeros(n), np.zeros(n)
+    dim = {1: ".1D", 2: ".2D", 3: ".3D"}[len(case["np"])]
+    info = F.psod(absorb=case["absorb"] != 0, dim=dim, prtcrl=prtcrl,
+                  tpabsor=TPABSOR[case["meta"].get("absorb")], lc=lc, mpi=mpi, mpr=mpr,
+                  mxdct=mxdct, n=n, dt=case["dt"], ti=case["ti"], tf=tf,
+                  tol=case["tol"] if tol is None else tol, np_=case["np"], shm=case["shm"],
+                  vpot=case["vpot"], vabc=case["vabc"], u1=u1, v1=v1, u2=u2, v2=v2, lnzvc=lnzvc)
+    return dict(info=info, u=u2, v=v2, u_prev=u1, v_prev=v1, lnzvc=lnzvc)
+
+
+def psod_oracle(oracle, case, prtcrl, lc=None, tf=None, tol=None, psi=None):
+    p = oracle.make_prop(case["np"], case["dt"], case["ti"], case["tf"] if tf is None else tf,
+                         case["sh"], case["sm"], lc=case["lc"] if lc is None else lc,
+                         tol=case["tol"] if tol is None else tol, absorb=case["absorb"],
+                         prtcrl=prtcrl, quirks=case["ref_quirks"], shm=case["shm"])
+    psi = np.asarray(case["psi"] if psi is None else psi)
+    return oracle.psod(p, case["vpot"], psi.real, np.imag(psi), vabc=case["vabc"])
+
+
+@pytest.mark.parametrize("name", ["morse1d_psod", "morse1d_psod_voptic", "morse1d_psod_smooth",
+                                  "morse2d_psod"])
+def test_psod_dropin_matches_oracle_and_executable(oracle, capfd, name):
+    case = G.setup_case(name)
+    capfd.readouterr()
+    got = call_psod(case, ".PARTIAL")
+    out, err = capfd.readouterr()
+    assert err == ""
+    ref = psod_oracle(oracle, case, oracle.PRT_PARTIAL)
+    nc, col = ref["nc"], got["lnzvc"]
+    assert np.max(np.abs(col[:nc, 1] - ref["c"].real)) <= 1e-10
+    assert np.max(np.abs(col[:nc, 2] - ref["c"].imag)) <= 1e-10
+    assert not np.any(col[nc:, 1:3]) and not np.any(col[:, [0, 3]])
+    for k in ("u", "v", "u_prev", "v_prev"):
+        assert np.max(np.abs(got[k] - ref[k])) <= 1e-10, k
+    assert got["info"] == ref["info"]
+    lines = out.split("\n")
+    i = lines.index(" Partial auto-correlation function:")
+    assert lines[i + 3] == ("       *t/fs*       *E/a.u.*        *Cr(t)*       *Ci(t)*    "
+                            "*|C(t)|^2*      *|C|*")
+    text = [l for l in lines[i + 4:] if len(l.split()) == 6]
+    rows = np.array([[float(x) for x in l.split()] for l in text])
+    assert rows.shape == ref["rows"].shape
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(ref["rows"][:, 1]))) - 5)
+    d = np.abs(rows - ref["rows"])
+    assert np.all(d[:, [0, 2, 3, 4, 5]] <= np.array([5e-9, 5e-8, 5e-8, 5e-9, 5e-7]) + 1e-10)
+    assert np.all(d[:, 1] <= 0.5 * e_ulp * 1.001)
+    gold = case["data"]["rows"]
+    dg = np.abs(rows - gold)
+    assert np.all(dg[:, [0, 2, 3, 4, 5]] <= np.array([1e-8, 1e-7, 1e-7, 1e-8, 1e-6]) * 1.01)
+    assert np.all(dg[:, 1] <= e_ulp * 1.01)
+    if name == "morse1d_psod":
+        with open(f"{G.GOLDEN}/{name}_partial.txt") as f:
+            want = f.read().split("\n")
+        assert lines[i - 1:i + 4] == want[:5]
+        same = sum(a == b for a, b in zip(text[:150], want[5:5 + 150]))
+        assert same >= 140, same
+
+
+def test_psod_dropin_complex_state_stride_and_info(oracle, capfd):
+    """A complex initial state (the restart-copy defect of psod.f:136-141 acts
+    on V), LC = 5 into columns 5/6 without printing, and INFO on four
+    tolerances (the norm column squared in the loop, psod.f:183)."""
+    case = G.setup_case("morse1d_psod")
+    n = len(case["psi"])
+    psi = case["psi"] * np.exp(0.7j * np.sin(np.arange(n) / 37.0))
+    tf = 150 * case["dt"]
+    capfd.readouterr()
+    got = call_psod(case, ".NO", lc=5, tf=tf, ncols=8, mpr=5, mpi=6, psi=psi)
+    assert capfd.readouterr().out == ""
+    ref = psod_oracle(oracle, case, oracle.PRT_NONE, lc=5, tf=tf, psi=psi)
+    nc, col = ref["nc"], got["lnzvc"]
+    assert np.max(np.abs(col[:nc, 4] + 1j * col[:nc, 5] - ref["c"])) <= 1e-10
+    for k in ("u", "v", "u_prev", "v_prev"):
+        assert np.max(np.abs(got[k] - ref[k])) <= 1e-10, k
+    for tol in (1e-12, 1e-7, 1e-3, 10.0):
+        got = call_psod(case, ".YES", tol=tol, tf=tf, psi=psi)
+        ref = psod_oracle(oracle, case, oracle.PRT_YES, tol=tol, tf=tf, psi=psi)
+        assert got["info"] == ref["info"], (tol, got["info"], ref["info"])
+    capfd.readouterr()
