@@ -1,0 +1,537 @@
+// deck.cpp -- eSPec input decks run through the GPU propagators: the part of
+// the driver (espec.f) from the input deck (rdinput.f) to the spectrum, for
+// time-dependent runs of one packet with a tabulated potential.
+//
+// Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL .FILE, *MASS,
+// *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION), *INIEIGVC .GETR,
+// *CHANGE, *SHIFT_POTENTIAL, *PRTCRL, *MASS_FACTOR, *DONOTSTOP; **TD *PROPAG
+// (.PFSPO, .PFSOD, .PSIL, .PSOD), *PRPGSTATE 0, *TPTRANS .ONE, *PRPTOL,
+// *ABSORBING; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.  Print and output-file
+// switches (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored: no files are
+// written.  Anything else -- analytic potentials, computed initial states
+// (the TI part), pulses, several states -- is refused with a message: there is
+// no CPU path.
+//
+// The run follows espec.f: the .FILE reads of RDPTE / RDPT (rdpte.f, rdpt.f:
+// eigenvector block, then potential block, optionally shifted to its
+// minimum), SH = (XF - XI)/(NP - 1) and SHM = 1/(24 m SH^2) per axis, the C(t)
+// stride NC and the final time of espec.f:1328-1353, the absorber table of
+// ABSORBINGBC (absorb.f:62-205), the propagator drop-in (which prints the
+// partial auto-correlation table), the total correlation of espec.f:1545-1576
+// printed as FORMAT 1041/1042, and HWHM / SPECTRUMTD (espec.f:1596-1606).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "espec_gpu.h"
+#include "espec_internal.h"
+
+namespace {
+
+const double kAmu = 1.836152667539e3;  // espec.f:614
+
+struct DeckError {
+  std::string what;
+};
+
+std::string upper(std::string s) {
+  for (char& c : s) c = (char)std::toupper((unsigned char)c);
+  return s;
+}
+
+std::string trim(const std::string& s) {
+  size_t a = s.find_first_not_of(" \t\r\n"), b = s.find_last_not_of(" \t\r\n");
+  return a == std::string::npos ? std::string() : s.substr(a, b - a + 1);
+}
+
+// free-format numbers of one record, up to a '/' (Fortran list-directed
+// input; D exponents accepted)
+std::vector<double> numbers(const std::string& line) {
+  std::string s = line.substr(0, line.find('/'));
+  for (char& c : s)
+    if (c == 'D' || c == 'd') c = 'E';
+    else if (c == ',') c = ' ';
+  std::istringstream in(s);
+  std::vector<double> v;
+  std::string tok;
+  while (in >> tok) {
+    char* end = nullptr;
+    const double x = std::strtod(tok.c_str(), &end);
+    if (end == tok.c_str()) break;
+    v.push_back(x);
+  }
+  return v;
+}
+
+bool starts(const std::string& s, const char* p) { return s.compare(0, std::strlen(p), p) == 0; }
+
+// One keyword's records, as the lines that follow it (comments after '!'
+// removed, blank lines skipped).
+struct Deck {
+  std::map<std::string, std::map<std::string, std::vector<std::string>>> sec;
+  const std::vector<std::string>* get(const char* s, const char* k) const {
+    auto a = sec.find(s);
+    if (a == sec.end()) return nullptr;
+    auto b = a->second.find(k);
+    return b == a->second.end() ? nullptr : &b->second;
+  }
+};
+
+Deck parse_deck(const std::string& text) {
+  Deck d;
+  std::istringstream in(text);
+  std::string line, section, key;
+  while (std::getline(in, line)) {
+    const size_t bang = line.find('!');
+    if (bang != std::string::npos) line = line.substr(0, bang);
+    const std::string t = trim(line);
+    if (t.empty()) continue;
+    if (starts(t, "**")) {
+      section = upper(t.substr(0, t.find_first_of(" \t")));
+      key.clear();
+    } else if (t[0] == '*') {
+      if (section.empty()) continue;  // the title lines before **MAIN
+      key = upper(t.substr(0, t.find_first_of(" \t")));
+      d.sec[section][key];
+    } else if (!section.empty() && !key.empty()) {
+      d.sec[section][key].push_back(t);
+    }
+  }
+  return d;
+}
+
+// .FILE potential: title, NT eigenvector records, title, NT potential records
+// (rdpte.f:39-58, rdpt.f:40-62), coordinates listed last axis first
+struct FileData {
+  std::vector<double> psi, vpot;
+  double xi[3] = {0, 0, 0}, xf[3] = {0, 0, 0};
+};
+
+FileData read_file(const std::string& path, int nt, int nd, bool shiftp) {
+  std::ifstream f(path);
+  if (!f) throw DeckError{"potential input file \"" + path + "\" cannot be opened"};
+  FileData r;
+  r.psi.resize(nt);
+  r.vpot.resize(nt);
+  std::string line;
+  auto block = [&](std::vector<double>& out, bool coords) {
+    if (!std::getline(f, line)) throw DeckError{"reading file error: " + path};
+    for (int j = 0; j < nt; ++j) {
+      if (!std::getline(f, line)) throw DeckError{"reading file error: " + path};
+      const std::vector<double> v = numbers(line);
+      if ((int)v.size() < nd + 1) throw DeckError{"reading file error: " + path};
+      out[j] = v[nd];
+      if (coords && j == 0)
+        for (int a = 0; a < nd; ++a) r.xi[a] = v[nd - 1 - a];
+      if (coords && j == nt - 1)
+        for (int a = 0; a < nd; ++a) r.xf[a] = v[nd - 1 - a];
+    }
+  };
+  block(r.psi, true);
+  block(r.vpot, true);  // RDPT sets XI, XF again from the potential block
+  if (shiftp) {
+    double vmin = r.vpot[0];
+    for (double x : r.vpot) vmin = x < vmin ? x : vmin;
+    for (double& x : r.vpot) x = x - vmin;
+  }
+  return r;
+}
+
+// ABSORBINGBC (absorb.f:62-205) on the grid
+std::vector<double> absorber_table(int nd, const int* np, const std::string& tp, const double* al,
+                                   const double* ar, const double* sh, const double* xi,
+                                   const double* xf, const double* voi) {
+  long n = 1;
+  for (int a = 0; a < nd; ++a) n *= np[a];
+  std::vector<double> v(n, 0.0);
+  if (nd == 1) {
+    for (long i = 0; i < n; ++i) {
+      const double x = xi[0] + (double)i * sh[0];
+      double r;
+      if (starts(tp, ".SMOOTHW")) {
+        if (x < al[0])
+          r = std::exp(voi[0] * std::pow(x - al[0], voi[1]) / (x + sh[0] - xi[0]));
+        else if (x > ar[0])
+          r = std::exp(-voi[0] * (x - ar[0]) / std::pow(xf[0] + sh[0] - x, voi[1]));
+        else
+          r = 1.0;
+      } else if (starts(tp, ".SMRS")) {
+        r = x < al[0] ? 1.0 - voi[0] * (x - al[0]) * (x - al[0])
+                      : (x > ar[0] ? 1.0 - voi[0] * (x - ar[0]) * (x - ar[0]) : 1.0);
+      } else if (starts(tp, ".VOPTIC_LINEAR")) {
+        r = x < al[0] ? -voi[0] * (x - al[0]) / (x + sh[0] - xi[0])
+                      : (x > ar[0] ? voi[0] * (x - ar[0]) / (xf[0] + sh[0] - x) : 0.0);
+      } else if (starts(tp, ".VOPTIC_KOSLOFF")) {
+        r = x < al[0] ? voi[0] / std::cosh(xi[0] - al[0] / voi[1])
+                      : (x > ar[0] ? voi[0] / std::cosh(xf[0] - al[0] / voi[1]) : 0.0);
+      } else if (starts(tp, ".VOPTIC_POLIN")) {
+        r = x < al[0] ? voi[0] * std::pow(x - al[0], voi[1])
+                      : (x > ar[0] ? voi[0] * std::pow(x - ar[0], voi[1]) : 0.0);
+      } else {
+        throw DeckError{"absorber " + tp + " is not defined for .1D (absorb.f)"};
+      }
+      v[i] = r;
+    }
+    return v;
+  }
+  if (nd == 2 && starts(tp, ".SMOOTHW")) {
+    for (int j = 0; j < np[1]; ++j) {
+      const double y = xi[1] + (double)j * sh[1];
+      for (int i = 0; i < np[0]; ++i) {
+        const double x = xi[0] + (double)i * sh[0];
+        double r;
+        if (x < al[0])
+          r = std::exp(voi[0] * (x - al[0]) / (x + sh[0] - xi[0]));
+        else if (y < al[1])
+          r = std::exp(voi[1] * (y - al[1]) / (y + sh[1] - xi[1]));
+        else if (x > ar[0])
+          r = std::exp(-voi[0] * (x - ar[0]) / (xf[0] + sh[0] - x));
+        else if (y > ar[1])
+          r = std::exp(-voi[1] * (y - ar[1]) / (xf[1] + sh[1] - y));
+        else
+          r = 1.0;
+        v[i + (long)np[0] * j] = r;
+      }
+    }
+    return v;
+  }
+  throw DeckError{"the reference has no absorber " + tp + " for this dimension (absorb.f:196-210)"};
+}
+
+// FORMAT 1003: (/,3X,A68) -- A68 right-justifies a shorter string
+void msg1003(const char* s) {
+  std::string t(s);
+  if (t.size() < 68) t = std::string(68 - t.size(), ' ') + t;
+  std::printf("\n   %s\n", t.substr(0, 68).c_str());
+}
+
+// list-directed REAL*8 as gfortran writes it: 1PG25.17E3 after one blank
+std::string list_real(double x) {
+  char buf[64];
+  const double ax = std::fabs(x);
+  if (ax != 0.0 && (ax < 0.1 || ax >= 1e17)) {
+    std::snprintf(buf, sizeof buf, "%.16E", x);
+    std::string s(buf);
+    const size_t e = s.find('E');
+    const int ex = std::atoi(s.c_str() + e + 1);
+    char eb[16];
+    std::snprintf(eb, sizeof eb, "E%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
+    s = s.substr(0, e) + eb;
+    return std::string(26 - s.size(), ' ') + s;
+  }
+  const int k = ax == 0.0 ? 1 : (int)std::floor(std::log10(ax)) + 1;
+  std::snprintf(buf, sizeof buf, "%.*f", 17 - (k > 0 ? k : 0), x);
+  std::string s(buf);
+  return std::string(21 - s.size(), ' ') + s + "     ";
+}
+
+struct Run {
+  int nd = 1, np[3] = {1, 1, 1};
+  std::string dim = ".1D", potch = ".NULL", potfile, tpclc = ".SPECTRUM", tdi = ".NC";
+  std::string inieigvc = ".CALC", prtcrl = ".NO", tppropg = ".NULL", tptrans = ".ONE";
+  std::string tpabsor, tpwind = ".NONE";
+  bool change = false, shiftp = true, absorb = false, fstop = true, lhwhm = false;
+  double sm[3] = {1, 1, 1}, smf[3] = {1, 1, 1};
+  double ti = 0.0, tf = 1e-4, dt = 1e-4, tol = 3.0, wp = 0.0;
+  double chwhm = 0.0, de = 0.0, e1i = 0.0, ade = 0.0;
+  double voi[3] = {0, 0, 0}, al[3] = {0, 0, 0}, ar[3] = {0, 0, 0};
+  int mf = 13, mp = 10, prpgstate = 0;
+};
+
+const std::string& rec(const std::vector<std::string>* r, size_t i, const char* key) {
+  if (!r || r->size() <= i) throw DeckError{std::string("missing record of ") + key};
+  return (*r)[i];
+}
+
+bool yes_opt(const std::string& o) { return !(starts(o, ".NO") || starts(o, ".OFF")); }
+
+// rdinput.f:125-620 for the keywords covered; print and output-file switches
+// are accepted and not acted on
+Run read_run(const Deck& d) {
+  Run r;
+  static const char* kIgnored[] = {"*TITLE", "*PRTPOT", "*PRTEIGVC", "*PRTVEFF", "*PRTEIGVC2",
+                                   "*PRTPULSE", "*PRTDIPOLE", "*PRTREGION", "*PRTONLYREIM"};
+  auto ignored = [&](const std::string& k) {
+    for (const char* x : kIgnored)
+      if (k == x) return true;
+    return false;
+  };
+  for (const auto& s : d.sec) {
+    const std::string& sname = s.first;
+    if (sname != "**MAIN" && sname != "**TD" && sname != "**SPECTRUM" && sname != "**END")
+      throw DeckError{"section " + sname + " is not covered (time-independent and "
+                      "eigenstate runs are not)"};
+    for (const auto& kv : s.second) {
+      const std::string& k = kv.first;
+      const std::vector<std::string>* v = &kv.second;
+      if (ignored(k)) continue;
+      if (sname == "**MAIN") {
+        if (k == "*DIMENSION") {
+          r.dim = upper(rec(v, 0, "*DIMENSION"));
+          if (starts(r.dim, ".1D") && !starts(r.dim, ".1DC")) r.nd = 1;
+          else if (r.dim.size() >= 3 && starts(r.dim, ".2D") && (r.dim.size() == 3 || r.dim[3] == ' ')) r.nd = 2;
+          else if (starts(r.dim, ".3D")) r.nd = 3;
+          else throw DeckError{"*DIMENSION " + r.dim + " is not covered (.1D, .2D, .3D)"};
+          const std::vector<double> n = numbers(rec(v, 1, "*DIMENSION"));
+          if ((int)n.size() < r.nd) throw DeckError{"*DIMENSION: grid sizes missing"};
+          for (int a = 0; a < r.nd; ++a) r.np[a] = (int)n[a];
+        } else if (k == "*POTENTIAL") {
+          r.potch = upper(rec(v, 0, "*POTENTIAL"));
+          if (!starts(r.potch, ".FILE"))
+            throw DeckError{"*POTENTIAL " + r.potch + ": only .FILE potentials are covered"};
+          r.potfile = rec(v, 1, "*POTENTIAL");
+        } else if (k == "*MASS") {
+          const std::vector<double> m = numbers(rec(v, 0, "*MASS"));
+          for (size_t a = 0; a < m.size() && a < 3; ++a) r.sm[a] = m[a];
+        } else if (k == "*MASS_FACTOR") {
+          const std::vector<double> m = numbers(rec(v, 0, "*MASS_FACTOR"));
+          for (size_t a = 0; a < m.size() && a < 3; ++a) r.smf[a] = m[a];
+        } else if (k == "*TPCALC") {
+          r.tpclc = upper(rec(v, 0, "*TPCALC"));
+          if (starts(r.tpclc, ".SPECTRUM")) r.tdi = upper(rec(v, 1, "*TPCALC"));
+          else if (starts(r.tpclc, ".PROPAGATION") || starts(r.tpclc, ".CORRELATION")) r.tdi = ".TD";
+          else throw DeckError{"*TPCALC " + r.tpclc + " is not covered"};
+        } else if (k == "*INIEIGVC") {
+          r.inieigvc = upper(rec(v, 0, "*INIEIGVC"));
+        } else if (k == "*CHANGE") {
+          r.change = yes_opt(upper(rec(v, 0, "*CHANGE")));
+        } else if (k == "*SHIFT_POTENTIAL") {
+          r.shiftp = yes_opt(upper(rec(v, 0, "*SHIFT_POTENTIAL")));
+        } else if (k == "*DONOTSTOP") {
+          r.fstop = !yes_opt(upper(rec(v, 0, "*DONOTSTOP")));
+        } else if (k == "*PRTCRL") {
+          std::string p = upper(rec(v, 0, "*PRTCRL"));
+          if (starts(p, ".FULL") || starts(p, ".ALL")) p = ".YES";  // rdinput.f:332-338
+          if (starts(p, ".NONE") || starts(p, ".NULL") || starts(p, ".EMPTY")) p = ".NO";
+          r.prtcrl = p;
+        } else {
+          throw DeckError{"keyword " + k + " of **MAIN is not covered"};
+        }
+      } else if (sname == "**TD") {
+        if (k == "*PROPAG") {
+          r.tppropg = upper(rec(v, 0, "*PROPAG"));
+          const std::vector<double> x = numbers(rec(v, 1, "*PROPAG"));
+          const bool sil = starts(r.tppropg, ".PSIL");
+          if (x.size() < (sil ? 4u : 3u)) throw DeckError{"*PROPAG: TI TF DT" + std::string(sil ? " MP" : "")};
+          r.ti = x[0];
+          r.tf = x[1];
+          r.dt = x[2];
+          if (sil) r.mp = (int)x[3];
+        } else if (k == "*PRPGSTATE") {
+          r.prpgstate = (int)numbers(rec(v, 0, "*PRPGSTATE")).at(0);
+        } else if (k == "*TPTRANS") {
+          r.tptrans = upper(rec(v, 0, "*TPTRANS"));
+        } else if (k == "*PRPTOL") {
+          r.tol = numbers(rec(v, 0, "*PRPTOL")).at(0);
+        } else if (k == "*ABSORBING") {
+          r.tpabsor = upper(rec(v, 0, "*ABSORBING"));
+          if (starts(r.tpabsor, ".NULL")) continue;
+          if (!starts(r.tpabsor, ".SMOOTHW") && !starts(r.tpabsor, ".SMRS") &&
+              !starts(r.tpabsor, ".VOPTIC"))
+            throw DeckError{"*ABSORBING " + r.tpabsor + " is not known (rdinput.f:526-548)"};
+          r.absorb = true;
+          const std::vector<double> vo = numbers(rec(v, 1, "*ABSORBING"));
+          const std::vector<double> lr = numbers(rec(v, 2, "*ABSORBING"));
+          for (size_t a = 0; a < 3 && a < vo.size(); ++a) r.voi[a] = vo[a];
+          for (size_t a = 0; a < 3 && 2 * a + 1 < lr.size(); ++a) {
+            r.al[a] = lr[2 * a];
+            r.ar[a] = lr[2 * a + 1];
+          }
+        } else {
+          throw DeckError{"keyword " + k + " of **TD is not covered"};
+        }
+      } else if (sname == "**SPECTRUM") {
+        if (k == "*FOURIER") {
+          r.mf = (int)numbers(rec(v, 0, "*FOURIER")).at(0);
+        } else if (k == "*WINDOWING") {
+          r.tpwind = upper(rec(v, 0, "*WINDOWING"));
+          r.wp = numbers(rec(v, 1, "*WINDOWING")).at(0);
+        } else if (k == "*HWHM") {
+          const std::vector<double> h = numbers(rec(v, 0, "*HWHM"));
+          if (h.size() < 4) throw DeckError{"*HWHM: CHWHM DE E1I ADE"};
+          r.chwhm = h[0];
+          r.de = h[1];
+          r.e1i = h[2];
+          r.ade = h[3];
+          r.lhwhm = true;
+        } else {
+          throw DeckError{"keyword " + k + " of **SPECTRUM is not covered"};
+        }
+      }
+    }
+  }
+  if (!starts(r.inieigvc, ".GETR") && !starts(r.inieigvc, ".READR"))
+    throw DeckError{"*INIEIGVC " + r.inieigvc + ": only .GETR (the eigenvector of the .FILE) is "
+                    "covered"};
+  if (!starts(r.tptrans, ".ONE") || r.prpgstate != 0)
+    throw DeckError{"one propagated state (*TPTRANS .ONE, *PRPGSTATE 0) is covered"};
+  if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD"))
+    throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": only .TD is covered"};
+  if (!starts(r.tppropg, ".PFSPO") && !starts(r.tppropg, ".PFSOD") &&
+      !starts(r.tppropg, ".PSIL") && !starts(r.tppropg, ".PSOD"))
+    throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD)"};
+  return r;
+}
+
+int run_deck(const std::string& deck_path) {
+  std::ifstream in(deck_path);
+  if (!in) throw DeckError{"cannot open " + deck_path};
+  std::stringstream ss;
+  ss << in.rdbuf();
+  Run r = read_run(parse_deck(ss.str()));
+  const size_t slash = deck_path.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? std::string() : deck_path.substr(0, slash + 1);
+  const std::string file = !r.potfile.empty() && r.potfile[0] == '/' ? r.potfile : dir + r.potfile;
+  int n = 1;
+  for (int a = 0; a < r.nd; ++a) n *= r.np[a];
+  FileData fd = read_file(file, n, r.nd, r.shiftp);
+  double sh[3] = {1, 1, 1}, shm[3] = {0, 0, 0}, sm[3] = {1, 1, 1};
+  for (int a = 0; a < r.nd; ++a) {
+    sm[a] = kAmu * r.sm[a];  // espec.f:614
+    sh[a] = (fd.xf[a] - fd.xi[a]) / (r.np[a] - 1.0);
+    shm[a] = 1.0 / ((((24.0 * sm[a]) * r.smf[a]) * sh[a]) * sh[a]);  // espec.f:819
+  }
+  // C(t) stride and final time (espec.f:1328-1353)
+  int nc = 0;
+  if (starts(r.tpclc, ".SPECTRUM") || starts(r.tpclc, ".PROPAG") || starts(r.tpclc, ".CORRELATION")) {
+    for (;;) {
+      const double sc = 2.0 * (r.tf - r.ti) / r.dt;
+      nc = (int)(sc / std::pow(2.0, r.mf));
+      if (std::fabs(sc - nc * std::pow(2.0, r.mf)) >= 1e-10 && r.change) {
+        r.tf = nc * std::pow(2.0, r.mf - 1.0) * r.dt;
+        std::printf(" -> Warning! Final time changed to%s\n", list_real(r.tf).c_str());
+        continue;
+      }
+      if (std::fabs(sc - nc * std::pow(2.0, r.mf)) >= 1e-10 && starts(r.tpclc, ".SPECTRUM")) {
+        std::printf(" <<<>>> Final time is not adequate for FFT <<<>>>\n");
+        if (r.fstop) throw DeckError{"final time is not adequate for FFT"};
+      }
+      break;
+    }
+  }
+  if (nc < 1) throw DeckError{"the C(t) stride is below one step: raise TF or lower MF"};
+  std::vector<double> vabc(n, 0.0);
+  if (r.absorb)
+    vabc = absorber_table(r.nd, r.np, r.tpabsor, r.al, r.ar, sh, fd.xi, fd.xf, r.voi);
+  // propagation: the reference's LNZVC holds the Lanczos basis in columns
+  // 1..MP and C(t) in MP+1, MP+2 (espec.f:1357-1359)
+  const int steps = (int)std::lround((r.tf - r.ti) / r.dt) + 4;
+  const int mxdct = std::max(n, steps / nc + 4);
+  const int mpr = r.mp + 1, mpi = r.mp + 2;
+  std::vector<double> lnzvc((size_t)mxdct * (r.mp + 2), 0.0);
+  std::vector<double> u1 = fd.psi, v1(n, 0.0), u2(n, 0.0), v2(n, 0.0), tc(n, 0.0), wrk(n, 0.0);
+  const int absorb = r.absorb ? 1 : 0, lmt = 10, change = r.change ? 1 : 0;
+  double abstol = 1e-6;
+  std::vector<int> iwork(64, 0);
+  const double xi0 = 0.0;
+  int info = 0, mp = r.mp;
+  const char* pr = r.prtcrl.c_str();
+  const char* dm = r.dim.c_str();
+  const char* ta = r.tpabsor.empty() ? ".NONE" : r.tpabsor.c_str();
+  msg1003("Propagating eigenvector...");
+  // espec.f:1361-1498
+  const char* using_msg = starts(r.tppropg, ".PFSPO")   ? "Using SPO procedure with FFT."
+                          : starts(r.tppropg, ".PFSOD") ? "Using SOD procedure with FFT."
+                          : starts(r.tppropg, ".PSIL")  ? "Using SIL procedure."
+                          : starts(r.tppropg, ".PSOD")  ? "Using SOD procedure."
+                                                        : nullptr;
+  if (using_msg) std::printf(" %s\n", using_msg);
+  std::fflush(stdout);
+  if (starts(r.tppropg, ".PFSPO")) {
+    pspofft_(&absorb, dm, pr, ta, &info, &nc, &mp, &mpi, &mpr, &mxdct, &n, &r.dt, &r.ti, &r.tf,
+             &r.tol, r.np, shm, sh, sm, u1.data(), v1.data(), &xi0, &xi0, tc.data(),
+             fd.vpot.data(), vabc.data(), lnzvc.data(), wrk.data(), wrk.data(), &xi0,
+             std::strlen(dm), std::strlen(pr), std::strlen(ta));
+  } else if (starts(r.tppropg, ".PFSOD")) {
+    psodfft_(&absorb, dm, pr, ta, &info, &nc, &mp, &mpi, &mpr, &mxdct, &n, &r.dt, &r.ti, &r.tf,
+             &r.tol, r.np, shm, sh, sm, u1.data(), u2.data(), v1.data(), v2.data(), &xi0, &xi0,
+             tc.data(), fd.vpot.data(), vabc.data(), wrk.data(), wrk.data(), &xi0, lnzvc.data(),
+             std::strlen(dm), std::strlen(pr), std::strlen(ta));
+  } else if (starts(r.tppropg, ".PSIL")) {
+    plnz_(&absorb, &change, dm, pr, ta, &info, &nc, &lmt, &mp, &mpi, &mpr, &mxdct, &n, &abstol,
+          &r.dt, &r.ti, &r.tf, &r.tol, r.np, iwork.data(), shm, fd.vpot.data(), vabc.data(),
+          u1.data(), v1.data(), &xi0, &xi0, wrk.data(), wrk.data(), wrk.data(), wrk.data(), &xi0,
+          lnzvc.data(), std::strlen(dm), std::strlen(pr), std::strlen(ta));
+  } else if (starts(r.tppropg, ".PSOD")) {
+    psod_(&absorb, dm, pr, ta, &info, &nc, &mp, &mpi, &mpr, &mxdct, &n, &r.dt, &r.ti, &r.tf,
+          &r.tol, r.np, shm, u1.data(), u2.data(), v1.data(), v2.data(), &xi0, &xi0,
+          fd.vpot.data(), vabc.data(), wrk.data(), &xi0, lnzvc.data(), std::strlen(dm),
+          std::strlen(pr), std::strlen(ta));
+  } else {
+    throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD)"};
+  }
+  if (info == 2) throw DeckError{"the GPU propagation failed (INFO = 2)"};
+  if (info != 0) {
+    std::printf(" <<<>>> Propagation operator error <<<>>>\n INFO =%12d\n", info);
+    if (r.fstop) throw DeckError{"propagation operator error (INFO = 1)"};
+  }
+  std::printf(" Eigenvector propagated.\n");
+  if (starts(r.tpclc, ".PROPAGATION")) {
+    std::printf(" \n The eSPec program finished successfully!\n");
+    return ESPEC_OK;
+  }
+  // total correlation (espec.f:1545-1576): C(-t) = C(t)*, 2^MF samples
+  msg1003("Calculating total correlation function...");
+  const int mc = (int)(std::pow(2.0, r.mf) / 2.0);
+  const double dtf = r.tf / mc;
+  std::vector<double> cu(2 * (size_t)mc, 0.0), cv(2 * (size_t)mc, 0.0);
+  const double* cr = lnzvc.data() + (size_t)(mpr - 1) * mxdct;
+  const double* ci = lnzvc.data() + (size_t)(mpi - 1) * mxdct;
+  for (int i = 1; i <= mc; ++i) {
+    cu[mc + i - 1] += cr[i - 1];
+    cu[mc - i + 1] = cu[mc + i - 1];
+    cv[mc + i - 1] += ci[i - 1];
+    cv[mc - i + 1] = -cv[mc + i - 1];
+  }
+  cu[0] += cr[mc - 1];
+  cv[0] += ci[mc - 1];
+  cv[0] = -cv[0];
+  std::printf(" Total correlation function calculated.\n \n Correlation Function:\n"
+              " \"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\n");
+  std::printf("       *t/fs*       *C(t)r*       *C(t)i*\n");  // FORMAT 1041
+  for (int i = 1; i <= 2 * mc; ++i) {
+    const double t = -r.tf + (i - 1.0) * dtf;
+    char buf[128];
+    std::snprintf(buf, sizeof buf, "%15.6f   %10.7f    %10.7f", t, cu[i - 1], cv[i - 1]);
+    std::printf("%s\n", buf);  // FORMAT 1042 (values that fit the fields)
+  }
+  if (starts(r.tpclc, ".CORRELATION")) {
+    std::printf(" \n The eSPec program finished successfully!\n");
+    return ESPEC_OK;
+  }
+  if (r.lhwhm) {
+    double dde = r.de - r.e1i;
+    msg1003("Appling the half-width at half-maximum...");
+    std::fflush(stdout);
+    hwhm_(&r.mf, &dtf, &r.tf, &r.chwhm, &dde, cu.data(), cv.data());
+    std::printf(" Half-width at half-maximum applied.\n");
+  }
+  msg1003("   Processing spectrum...");
+  std::fflush(stdout);
+  double ade = r.ade;
+  spectrumtd_(r.tpwind.c_str(), &r.mf, &dtf, &r.tf, &r.wp, &ade, cu.data(), cv.data(),
+              r.tpwind.size());
+  std::printf(" Spectrum done.\n \n The eSPec program finished successfully!\n");
+  std::fflush(stdout);
+  return ESPEC_OK;
+}
+
+}  // namespace
+
+extern "C" int espec_run_deck(const char* deck_path) {
+  if (!deck_path) return espec::set_error(ESPEC_EINVAL, "null deck path");
+  try {
+    return run_deck(deck_path);
+  } catch (const DeckError& e) {
+    std::fflush(stdout);
+    std::fprintf(stderr, "espec_gpu deck: %s\n", e.what.c_str());
+    return espec::set_error(ESPEC_EINVAL, e.what.c_str());
+  }
+}

@@ -127,6 +127,15 @@ void hwhm_(const int* m, const double* dt, const double* tf, double* tal,
 void spectrumtd_(const char* tpwind, const int* m, const double* dt,
                  const double* tf, const double* wp, double* de, double* u,
                  double* v, size_t tpwind_len);
+/* Runs an eSPec input deck (time-dependent part of espec.f for one packet
+ * with a .FILE potential and its .GETR eigenvector; .PFSPO, .PFSOD, .PSIL,
+ * .PSOD; absorbers, total correlation, HWHM and spectrum) through the GPU
+ * drop-ins, printing to stdout what espec.x prints from "Propagating
+ * eigenvector..." on.  Files named in the deck are relative to the deck's
+ * directory.  An option outside that part is refused (ESPEC_EINVAL, reason
+ * on stderr).  No counterpart entry point in the reference: it replaces the
+ * executable's driver for these decks. */
+int espec_run_deck(const char* deck_path);
 /* one row of the partial auto-correlation table in FORMAT 1021 of
  * pspofft.f:148 (newline included); returns its length */
 int espec_format_crl_row(double t, double e, double cr, double ci, double ct,

@@ -23,6 +23,9 @@ Cases:
               differences with the finite-difference Hamiltonian).  With
               --psod-only only these are generated and merged into the
               manifest.
+  deck_*      whole decks for the deck driver (input.spc, wf_pot.inp and the
+              executable's output from the propagation on); --decks-only
+              generates only these.
 """
 import json
 import os
@@ -357,6 +360,64 @@ SMOOTH = """*ABSORBING
 """
 
 
+VOPTIC_SMALL = """*ABSORBING
+.VOPTIC_POLIN
+ -0.5  2.0  0.0/
+ 0.9  6.5  0.0 0.0 0.0 0.0/
+"""
+SMOOTH_SMALL = """*ABSORBING
+.SMOOTHW
+ 0.05  1.0  0.0/
+ 0.9  6.5  0.0 0.0 0.0 0.0/
+"""
+
+
+DECK_CASES = {
+    # name: (dimension, propagator, MP field, absorber block, HWHM block)
+    "deck_spo_hwhm": (1, ".PFSPO", "", "", "*HWHM\n 0.05 0.0 0.0 0.0/\n"),
+    "deck_psod_voptic": (1, ".PSOD", "", VOPTIC_SMALL, ""),
+    "deck_sil_smooth": (1, ".PSIL", "  10", SMOOTH_SMALL, ""),
+    "deck_sil_2d": (2, ".PSIL", "  10", "", ""),
+}
+
+
+def case_deck(name):
+    """A whole deck for the deck driver: input.spc and wf_pot.inp under
+    tests/golden/<name>/, and the executable's output from its last
+    'Propagating eigenvector...' line to the end as expected.txt.  Small grids
+    (N = 256 on [0.5, 8] bohr, or the 32 x 32 2D grid), 256 steps, MF = 8."""
+    nd, prop, mp, absorb, hwhm = DECK_CASES[name]
+    d = os.path.join(OUT, name)
+    os.makedirs(d, exist_ok=True)
+    if nd == 1:
+        n = 256
+        x = 0.5 + np.arange(n) * (7.5 / (n - 1))
+        v = 0.17 * (1 - np.exp(-1.0 * (x - 1.4))) ** 2
+        psi = np.exp(-((x - 1.8) ** 2) / (2 * 0.2 ** 2))
+        psi = psi / np.sqrt(np.sum(psi ** 2))
+        wf = write_1d_file(x, psi, v)
+        dim, npt, mass = ".1D", "256", fmt(918.0 / AMU)
+        dt_fs = 0.05 * SHFS
+    else:
+        x, y, psi, v = morse2d_inputs()
+        wf = write_2d_file(x, y, psi, v)
+        dim, npt, mass = ".2D", "32 32", f"{fmt(918.0 / AMU)} {fmt(1500.0 / AMU)}"
+        dt_fs = 0.005 * SHFS
+    deck = DECK.format(title=name, dim=dim, np=npt, mass=mass, prop=prop, tf=fmt(256 * dt_fs),
+                       dt=fmt(dt_fs), mp=mp, absorb=absorb, mf=8)
+    if hwhm:
+        deck = deck.replace("**SPECTRUM\n*FOURIER", "**SPECTRUM\n" + hwhm + "*FOURIER")
+    with open(os.path.join(d, "input.spc"), "w") as f:
+        f.write(deck)
+    with open(os.path.join(d, "wf_pot.inp"), "w") as f:
+        f.write(wf)
+    out = run_deck(deck, {"wf_pot.inp": wf})
+    lines = out.splitlines()
+    i = max(k for k, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
+    with open(os.path.join(d, "expected.txt"), "w") as f:
+        f.write("\n".join(lines[i - 1:]) + "\n")
+
+
 def psod_cases():
     vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
     smeta = dict(absorb="SMOOTHW", voi=[0.05, 1.0], al=1.55, ar=2.3)
@@ -378,6 +439,10 @@ def save(cases, manifest):
 def main():
     if not os.path.exists(BIN):
         sys.exit("eSPec executable not found at " + BIN)
+    if "--decks-only" in sys.argv:
+        for name in DECK_CASES:
+            case_deck(name)
+        return
     if "--psod-only" in sys.argv:
         with open(os.path.join(OUT, "manifest.json")) as f:
             manifest = json.load(f)
@@ -410,6 +475,8 @@ def main():
         cases[f"morse2d_{tag}"] = case_morse2d(f"morse2d_{tag}", prop)
     cases.update(psod_cases())
     save(cases, {})
+    for name in DECK_CASES:
+        case_deck(name)
 
 
 if __name__ == "__main__":

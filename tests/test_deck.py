@@ -1,0 +1,51 @@
+"""The deck driver's reading of eSPec input decks (espec_b200/csrc/deck.cpp),
+on the CPU: what it does not cover is refused with the reason before any
+device work, and a .FILE that is missing or short is reported."""
+import os
+
+import pytest
+
+from espec_b200 import _native as N
+from espec_b200 import deck as D
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BASE = open(os.path.join(HERE, "golden", "deck_spo_hwhm", "input.spc")).read()
+
+
+def refused(tmp_path, text, files=None):
+    p = tmp_path / "input.spc"
+    p.write_text(text)
+    for name, body in (files or {}).items():
+        (tmp_path / name).write_text(body)
+    with pytest.raises(N.EspecError) as e:
+        D.run(p)
+    return str(e.value)
+
+
+@pytest.mark.parametrize("old,new,why", [
+    (".FILE\nwf_pot.inp", ".MORSE\n1.1 1943.8 13.7 1.0/\n1.2 1629.2 17.7 1.0/", ".FILE"),
+    (".GETR", ".CALC", ".GETR"),
+    (".PFSPO", ".PPSOD", "propagator"),
+    (".1D\n 256/", ".2DC\n 16 16/", "*DIMENSION"),
+    ("*TPTRANS\n.ONE", "*TPTRANS\n.ALL", "one propagated state"),
+    ("**TD", "**TI\n*TPDIAG\n.LANCZS\n**TD", "section **TI"),
+    ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n*PRPTOL", "*PULSE_AND_DIPOLE"),
+])
+def test_uncovered_decks_are_refused(tmp_path, old, new, why):
+    assert old in BASE
+    msg = refused(tmp_path, BASE.replace(old, new))
+    assert why in msg, msg
+
+
+def test_missing_and_short_files(tmp_path):
+    assert "cannot be opened" in refused(tmp_path, BASE)
+    short = "# Eigenvector:\n 0.5 0.1\n 0.6 0.2\n"
+    assert "reading file error" in refused(tmp_path, BASE, {"wf_pot.inp": short})
+
+
+def test_final_time_not_adequate_for_fft(tmp_path, capfd):
+    text = BASE.replace("*CHANGE\n.YES", "*CHANGE\n.NO").replace("0.3096171935104", "0.31")
+    src = open(os.path.join(HERE, "golden", "deck_spo_hwhm", "wf_pot.inp")).read()
+    msg = refused(tmp_path, text, {"wf_pot.inp": src})
+    assert "not adequate for FFT" in msg
+    assert "<<<>>> Final time is not adequate for FFT <<<>>>" in capfd.readouterr().out
