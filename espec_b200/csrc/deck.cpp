@@ -33,6 +33,8 @@
 #include "espec_gpu.h"
 #include "espec_internal.h"
 
+#include <cuda_runtime.h>
+
 namespace {
 
 const double kAmu = 1.836152667539e3;  // espec.f:614
@@ -203,6 +205,12 @@ std::vector<double> absorber_table(int nd, const int* np, const std::string& tp,
     return v;
   }
   throw DeckError{"the reference has no absorber " + tp + " for this dimension (absorb.f:196-210)"};
+}
+
+// gfortran's real DO loop trip count: max(0, INT((b - a + c) / c))
+int do_count_real(double a, double b, double c) {
+  const double x = (b - a + c) / c;
+  return x > 0.0 ? (int)x : 0;
 }
 
 // FORMAT 1003: (/,3X,A68) -- A68 right-justifies a shorter string
@@ -380,12 +388,70 @@ Run read_run(const Deck& d) {
   return r;
 }
 
-int run_deck(const std::string& deck_path) {
+Run load_run(const std::string& deck_path) {
   std::ifstream in(deck_path);
   if (!in) throw DeckError{"cannot open " + deck_path};
   std::stringstream ss;
   ss << in.rdbuf();
-  Run r = read_run(parse_deck(ss.str()));
+  return read_run(parse_deck(ss.str()));
+}
+
+// C(t) stride NC and the final time (espec.f:1328-1353); prints the
+// reference's warning when TF changes
+int c_stride(Run& r) {
+  int nc = 0;
+  for (;;) {
+    const double sc = 2.0 * (r.tf - r.ti) / r.dt;
+    nc = (int)(sc / std::pow(2.0, r.mf));
+    if (std::fabs(sc - nc * std::pow(2.0, r.mf)) >= 1e-10 && r.change) {
+      r.tf = nc * std::pow(2.0, r.mf - 1.0) * r.dt;
+      std::printf(" -> Warning! Final time changed to%s\n", list_real(r.tf).c_str());
+      continue;
+    }
+    if (std::fabs(sc - nc * std::pow(2.0, r.mf)) >= 1e-10 && starts(r.tpclc, ".SPECTRUM")) {
+      std::printf(" <<<>>> Final time is not adequate for FFT <<<>>>\n");
+      if (r.fstop) throw DeckError{"final time is not adequate for FFT"};
+    }
+    break;
+  }
+  if (nc < 1) throw DeckError{"the C(t) stride is below one step: raise TF or lower MF"};
+  return nc;
+}
+
+// total correlation (espec.f:1545-1576): C(-t) = C(t)*, 2^MF samples from the
+// first MC = 2^(MF-1) recorded C values
+void total_correlation(int mc, const double* cr, const double* ci, std::vector<double>& cu,
+                       std::vector<double>& cv) {
+  cu.assign(2 * (size_t)mc, 0.0);
+  cv.assign(2 * (size_t)mc, 0.0);
+  for (int i = 1; i <= mc; ++i) {
+    cu[mc + i - 1] += cr[i - 1];
+    cu[mc - i + 1] = cu[mc + i - 1];
+    cv[mc + i - 1] += ci[i - 1];
+    cv[mc - i + 1] = -cv[mc + i - 1];
+  }
+  cu[0] += cr[mc - 1];
+  cv[0] += ci[mc - 1];
+  cv[0] = -cv[0];
+}
+
+// the "Correlation Function:" block (FORMAT 1041 / 1042)
+std::string correlation_table(int mc, double tf, const std::vector<double>& cu,
+                              const std::vector<double>& cv) {
+  std::string out = " \n Correlation Function:\n \"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\n";
+  out += "       *t/fs*       *C(t)r*       *C(t)i*\n";
+  const double dtf = tf / mc;
+  char buf[128];
+  for (int i = 1; i <= 2 * mc; ++i) {
+    const double t = -tf + (i - 1.0) * dtf;
+    std::snprintf(buf, sizeof buf, "%15.6f   %10.7f    %10.7f\n", t, cu[i - 1], cv[i - 1]);
+    out += buf;
+  }
+  return out;
+}
+
+int run_deck(const std::string& deck_path) {
+  Run r = load_run(deck_path);
   const size_t slash = deck_path.find_last_of('/');
   const std::string dir = slash == std::string::npos ? std::string() : deck_path.substr(0, slash + 1);
   const std::string file = !r.potfile.empty() && r.potfile[0] == '/' ? r.potfile : dir + r.potfile;
@@ -398,25 +464,7 @@ int run_deck(const std::string& deck_path) {
     sh[a] = (fd.xf[a] - fd.xi[a]) / (r.np[a] - 1.0);
     shm[a] = 1.0 / ((((24.0 * sm[a]) * r.smf[a]) * sh[a]) * sh[a]);  // espec.f:819
   }
-  // C(t) stride and final time (espec.f:1328-1353)
-  int nc = 0;
-  if (starts(r.tpclc, ".SPECTRUM") || starts(r.tpclc, ".PROPAG") || starts(r.tpclc, ".CORRELATION")) {
-    for (;;) {
-      const double sc = 2.0 * (r.tf - r.ti) / r.dt;
-      nc = (int)(sc / std::pow(2.0, r.mf));
-      if (std::fabs(sc - nc * std::pow(2.0, r.mf)) >= 1e-10 && r.change) {
-        r.tf = nc * std::pow(2.0, r.mf - 1.0) * r.dt;
-        std::printf(" -> Warning! Final time changed to%s\n", list_real(r.tf).c_str());
-        continue;
-      }
-      if (std::fabs(sc - nc * std::pow(2.0, r.mf)) >= 1e-10 && starts(r.tpclc, ".SPECTRUM")) {
-        std::printf(" <<<>>> Final time is not adequate for FFT <<<>>>\n");
-        if (r.fstop) throw DeckError{"final time is not adequate for FFT"};
-      }
-      break;
-    }
-  }
-  if (nc < 1) throw DeckError{"the C(t) stride is below one step: raise TF or lower MF"};
+  const int nc = c_stride(r);
   std::vector<double> vabc(n, 0.0);
   if (r.absorb)
     vabc = absorber_table(r.nd, r.np, r.tpabsor, r.al, r.ar, sh, fd.xi, fd.xf, r.voi);
@@ -481,27 +529,11 @@ int run_deck(const std::string& deck_path) {
   msg1003("Calculating total correlation function...");
   const int mc = (int)(std::pow(2.0, r.mf) / 2.0);
   const double dtf = r.tf / mc;
-  std::vector<double> cu(2 * (size_t)mc, 0.0), cv(2 * (size_t)mc, 0.0);
-  const double* cr = lnzvc.data() + (size_t)(mpr - 1) * mxdct;
-  const double* ci = lnzvc.data() + (size_t)(mpi - 1) * mxdct;
-  for (int i = 1; i <= mc; ++i) {
-    cu[mc + i - 1] += cr[i - 1];
-    cu[mc - i + 1] = cu[mc + i - 1];
-    cv[mc + i - 1] += ci[i - 1];
-    cv[mc - i + 1] = -cv[mc + i - 1];
-  }
-  cu[0] += cr[mc - 1];
-  cv[0] += ci[mc - 1];
-  cv[0] = -cv[0];
-  std::printf(" Total correlation function calculated.\n \n Correlation Function:\n"
-              " \"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\n");
-  std::printf("       *t/fs*       *C(t)r*       *C(t)i*\n");  // FORMAT 1041
-  for (int i = 1; i <= 2 * mc; ++i) {
-    const double t = -r.tf + (i - 1.0) * dtf;
-    char buf[128];
-    std::snprintf(buf, sizeof buf, "%15.6f   %10.7f    %10.7f", t, cu[i - 1], cv[i - 1]);
-    std::printf("%s\n", buf);  // FORMAT 1042 (values that fit the fields)
-  }
+  std::vector<double> cu, cv;
+  total_correlation(mc, lnzvc.data() + (size_t)(mpr - 1) * mxdct,
+                    lnzvc.data() + (size_t)(mpi - 1) * mxdct, cu, cv);
+  std::printf(" Total correlation function calculated.\n%s",
+              correlation_table(mc, r.tf, cu, cv).c_str());
   if (starts(r.tpclc, ".CORRELATION")) {
     std::printf(" \n The eSPec program finished successfully!\n");
     return ESPEC_OK;
@@ -523,7 +555,128 @@ int run_deck(const std::string& deck_path) {
   return ESPEC_OK;
 }
 
+// One deck, K .FILE inputs (initial state and potential each), 1D .PFSPO or
+// .PFSOD: one batched plan over all K packets, one batched spectrum launch,
+// per packet the total correlation and spectrum blocks written to
+// <prefix><k>.crl and <prefix><k>.spc (k from 1).
+int run_scan(const std::string& deck_path, int njobs, const char* const* files,
+             const std::string& prefix) {
+  Run r = load_run(deck_path);
+  if (r.nd != 1) throw DeckError{"scans run 1D decks (the batched plans are 1D)"};
+  const bool spo = starts(r.tppropg, ".PFSPO");
+  if (!spo && !starts(r.tppropg, ".PFSOD"))
+    throw DeckError{"scans run .PFSPO or .PFSOD (the batched plans)"};
+  if (!starts(r.tpclc, ".SPECTRUM")) throw DeckError{"scans produce spectra: *TPCALC .SPECTRUM .TD"};
+  if (njobs < 1 || !files) throw DeckError{"no input files"};
+  const size_t slash = deck_path.find_last_of('/');
+  const std::string dir = slash == std::string::npos ? std::string() : deck_path.substr(0, slash + 1);
+  const int n = r.np[0];
+  const double sm = kAmu * r.sm[0];
+  std::vector<double> vpot((size_t)njobs * n), psi((size_t)njobs * n), vabc;
+  std::vector<double> sh(njobs), sms(njobs, sm);
+  std::vector<int> npts(njobs, n);
+  if (r.absorb) vabc.resize((size_t)njobs * n);
+  for (int k = 0; k < njobs; ++k) {
+    const std::string f = files[k][0] == '/' ? std::string(files[k]) : dir + files[k];
+    FileData fd = read_file(f, n, 1, r.shiftp);
+    sh[k] = (fd.xf[0] - fd.xi[0]) / (n - 1.0);
+    std::copy(fd.psi.begin(), fd.psi.end(), psi.begin() + (size_t)k * n);
+    std::copy(fd.vpot.begin(), fd.vpot.end(), vpot.begin() + (size_t)k * n);
+    if (r.absorb) {
+      const double shk = sh[k];
+      const std::vector<double> t =
+          absorber_table(1, r.np, r.tpabsor, r.al, r.ar, &shk, fd.xi, fd.xf, r.voi);
+      std::copy(t.begin(), t.end(), vabc.begin() + (size_t)k * n);
+    }
+  }
+  const int nc = c_stride(r);
+  const int ab = !r.absorb ? ESPEC_ABS_NONE
+                           : (starts(r.tpabsor, ".VOPTIC") ? ESPEC_ABS_VOPTIC : ESPEC_ABS_SMOOTHW);
+  const int quirks = spo ? ESPEC_Q_SPO_INPLACE : ESPEC_Q_SOD_SMOOTHW;
+  // step counts of the drop-ins (pspofft.f:110; psodfft.f:120-154)
+  const int nsteps = spo ? do_count_real(r.ti + r.dt, r.tf + r.dt, r.dt)
+                         : 1 + do_count_real(r.ti + 2 * r.dt, r.tf + r.dt, r.dt);
+  const int mc = (int)(std::pow(2.0, r.mf) / 2.0);
+  if ((long)(mc - 1) * nc > nsteps) throw DeckError{"fewer C(t) samples than 2^(MF-1)"};
+  espec_spo_plan* plan = nullptr;
+  struct Guard {
+    espec_spo_plan*& p;
+    ~Guard() { espec_spo_destroy(p); }
+  } guard{plan};
+  std::vector<double> cre((size_t)njobs * (nsteps + 1)), cim(cre.size());
+  if (espec_prop_create(&plan, njobs, npts.data(), sh.data(), sms.data(), r.dt,
+                        spo ? ESPEC_SPO : ESPEC_SOD, ESPEC_FP64, ab, quirks) ||
+      espec_spo_load(plan, vpot.data(), r.absorb ? vabc.data() : nullptr, psi.data(), nullptr,
+                     ESPEC_MEM_HOST, nullptr) ||
+      espec_spo_run(plan, nsteps, nullptr) ||
+      espec_spo_results(plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST, nullptr))
+    throw DeckError{std::string("batched propagation: ") + espec_last_error()};
+  // every NC-th sample (the LNZVC rows of the drop-ins), packed per packet
+  std::vector<double> cpk((size_t)njobs * mc * 2);
+  for (int k = 0; k < njobs; ++k)
+    for (int s = 0; s < mc; ++s) {
+      const size_t src = (size_t)k * (nsteps + 1) + (size_t)s * nc;
+      cpk[((size_t)k * mc + s) * 2] = cre[src];
+      cpk[((size_t)k * mc + s) * 2 + 1] = cim[src];
+    }
+  const size_t N = (size_t)1 << r.mf;
+  const double dtf = r.tf / mc;
+  int window = -1;
+  if (starts(r.tpwind, ".SG")) window = 1;
+  else if (starts(r.tpwind, ".NONE") || starts(r.tpwind, ".NULL")) window = 0;
+  if (window < 0) throw DeckError{"*WINDOWING " + r.tpwind + " is not defined (spectrumtd.f)"};
+  void *d_in = nullptr, *d_spec = nullptr, *d_work = nullptr;
+  struct Free {
+    void** p[3];
+    ~Free() {
+      for (void** q : p)
+        if (*q) cudaFree(*q);
+    }
+  } fr{{&d_in, &d_spec, &d_work}};
+  std::vector<double> spec((size_t)njobs * N * 2);
+  if (cudaMalloc(&d_in, cpk.size() * 8) != cudaSuccess ||
+      cudaMalloc(&d_spec, spec.size() * 8) != cudaSuccess ||
+      cudaMalloc(&d_work, espec_spectrum_work_bytes(njobs, r.mf)) != cudaSuccess ||
+      cudaMemcpy(d_in, cpk.data(), cpk.size() * 8, cudaMemcpyHostToDevice) != cudaSuccess)
+    throw DeckError{"device buffers for the spectra"};
+  if (espec_spectrum_dev(njobs, r.mf, d_in, mc, 1, dtf, r.tf, r.lhwhm ? r.chwhm : -1.0,
+                         r.de - r.e1i, window, r.wp, ESPEC_Q_FFTNT_SP, d_spec, d_work, nullptr) ||
+      cudaMemcpy(spec.data(), d_spec, spec.size() * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+    throw DeckError{std::string("batched spectrum: ") + espec_last_error()};
+  const double ade = r.ade < 0.0 ? 0.0 : r.ade;  // spectrumtd.f: DE < 0 is set to 0
+  std::vector<double> cr(mc), ci(mc), cu, cv, u(N), v(N);
+  for (int k = 0; k < njobs; ++k) {
+    for (int s = 0; s < mc; ++s) {
+      cr[s] = cpk[((size_t)k * mc + s) * 2];
+      ci[s] = cpk[((size_t)k * mc + s) * 2 + 1];
+    }
+    total_correlation(mc, cr.data(), ci.data(), cu, cv);
+    for (size_t i = 0; i < N; ++i) {
+      u[i] = spec[((size_t)k * N + i) * 2];
+      v[i] = spec[((size_t)k * N + i) * 2 + 1];
+    }
+    const std::string base = prefix + std::to_string(k + 1);
+    std::ofstream fc(base + ".crl"), fs(base + ".spc");
+    if (!fc || !fs) throw DeckError{"cannot write " + base + ".crl / .spc"};
+    fc << correlation_table(mc, r.tf, cu, cv);
+    fs << espec::spectrum_table(r.mf, dtf, ade, u.data(), v.data());
+  }
+  return ESPEC_OK;
+}
+
 }  // namespace
+
+extern "C" int espec_run_scan(const char* deck_path, int njobs, const char* const* data_files,
+                              const char* out_prefix) {
+  if (!deck_path || !out_prefix) return espec::set_error(ESPEC_EINVAL, "null argument");
+  try {
+    return run_scan(deck_path, njobs, data_files, out_prefix);
+  } catch (const DeckError& e) {
+    std::fflush(stdout);
+    std::fprintf(stderr, "espec_gpu scan: %s\n", e.what.c_str());
+    return espec::set_error(ESPEC_EINVAL, e.what.c_str());
+  }
+}
 
 extern "C" int espec_run_deck(const char* deck_path) {
   if (!deck_path) return espec::set_error(ESPEC_EINVAL, "null deck path");

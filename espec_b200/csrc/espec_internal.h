@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <string>
+
 namespace espec {
 int set_error(int code, const char* msg);
 int set_cuda_error(const char* what, cudaError_t e);
@@ -11,6 +13,9 @@ void digt_1d(int n, double sh, double sm, double* tc);
 // as written with ESPEC_Q_DIGT_ND, else the outer sum of the axis tables)
 void digt_nd_table(int ndim, const int* np, const double* sh, const double* sm, int quirks,
                    double* tc);
+// the spectrum block SPECTRUMTD prints (spectrumtd.f:84-97) for FFTNT's
+// output u + i v of 2^mf points
+std::string spectrum_table(int mf, double dt, double de, const double* u, const double* v);
 inline int ck(cudaError_t e, const char* what) {
   return e == cudaSuccess ? 0 : set_cuda_error(what, e);
 }

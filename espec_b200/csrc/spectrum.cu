@@ -282,10 +282,6 @@ extern "C" void spectrumtd_(const char* tpwind, const int* m, const double* dt, 
                             const double* wp, double* de, double* u, double* v,
                             size_t tpwind_len) {
   const int mf = *m;
-  const size_t N = (size_t)1 << mf;
-  double enc = 1.0 / (N * *dt) * kEnc;
-  enc = enc * kFate;
-  double en = -(double)N / 2.0 * enc;
   if (*de < 0.0) *de = 0.0;
   auto is = [&](const char* pat) {
     const size_t k = std::strlen(pat);
@@ -304,16 +300,28 @@ extern "C" void spectrumtd_(const char* tpwind, const int* m, const double* dt, 
     std::fprintf(stderr, "espec_gpu SPECTRUMTD: %s\n", espec_last_error());
     return;
   }
-  // spectrumtd.f:84-97 (list-directed head, FORMAT 1011 and 1021)
+  const std::string out = espec::spectrum_table(mf, *dt, *de, u, v);
+  std::fwrite(out.data(), 1, out.size(), stdout);
+  std::fflush(stdout);
+}
+
+namespace espec {
+// spectrumtd.f:84-97 (list-directed head, FORMAT 1011 and 1021): the energy
+// axis from -N/2 ENC, the FFTNT output from its second half on
+std::string spectrum_table(int mf, double dt, double de, const double* u, const double* v) {
+  const size_t N = (size_t)1 << mf;
+  double enc = 1.0 / (N * dt) * kEnc;
+  enc = enc * kFate;
+  double en = -(double)N / 2.0 * enc;
   std::string out = " \n Spectrum:\n =========\n";
   out += "     *E (eV)*           *W*           *FFTr*          *FFTi*\n";
   auto row = [&](size_t i) {
-    out += " " + fmt_f12_7(en + *de) + "    " + fmt_f12_7(u[i]) + "    " + fmt_f12_7(u[i]) +
+    out += " " + fmt_f12_7(en + de) + "    " + fmt_f12_7(u[i]) + "    " + fmt_f12_7(u[i]) +
            "    " + fmt_f12_7(v[i]) + "\n";
     en = en + enc;
   };
   for (size_t i = N / 2; i < N; ++i) row(i);
   for (size_t i = 0; i < N / 2; ++i) row(i);
-  std::fwrite(out.data(), 1, out.size(), stdout);
-  std::fflush(stdout);
+  return out;
 }
+}  // namespace espec

@@ -136,6 +136,14 @@ void spectrumtd_(const char* tpwind, const int* m, const double* dt,
  * on stderr).  No counterpart entry point in the reference: it replaces the
  * executable's driver for these decks. */
 int espec_run_deck(const char* deck_path);
+/* The same deck over njobs .FILE inputs (each its own initial state and
+ * potential, the deck's grid size), replacing one executable run per file:
+ * 1D .PFSPO or .PFSOD, all packets in one batched plan and one batched
+ * spectrum launch; writes the correlation block to <out_prefix><k>.crl and
+ * the spectrum block to <out_prefix><k>.spc (k = 1..njobs, the text espec.x
+ * prints for that file).  No counterpart entry point in the reference. */
+int espec_run_scan(const char* deck_path, int njobs, const char* const* data_files,
+                   const char* out_prefix);
 /* one row of the partial auto-correlation table in FORMAT 1021 of
  * pspofft.f:148 (newline included); returns its length */
 int espec_format_crl_row(double t, double e, double cr, double ci, double ct,

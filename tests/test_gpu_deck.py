@@ -89,3 +89,39 @@ def test_deck_matches_executable(capfd, name):
     full = np.concatenate([[np.conj(c[mc - 1])], np.conj(c[1:mc][::-1]), c])
     assert np.max(np.abs(corr[:, 1] - full.real)) <= 1.01e-7
     assert np.max(np.abs(corr[:, 2] - full.imag)) <= 1.01e-7
+
+
+def test_scan_equals_one_run_per_file(tmp_path, capfd):
+    """Three .FILE inputs (the fixture's and two displaced Gaussians) through
+    espec_run_scan: each job's correlation and spectrum blocks are the text the
+    single-deck driver prints for that file."""
+    src = os.path.join(G.GOLDEN, "deck_spo_hwhm")
+    deck = open(os.path.join(src, "input.spc")).read()
+    lines = open(os.path.join(src, "wf_pot.inp")).read().split("\n")
+    n = 256
+    x = np.array([float(l.split()[0]) for l in lines[1:1 + n]])
+    files = ["wf_pot.inp"]
+    (tmp_path / "wf_pot.inp").write_text("\n".join(lines))
+    for k, x0 in enumerate((1.7, 1.95)):
+        psi = np.exp(-((x - x0) ** 2) / (2 * 0.18 ** 2))
+        psi /= np.sqrt(np.sum(psi ** 2))
+        body = [lines[0]] + [f" {repr(float(a))}   {repr(float(b))}" for a, b in zip(x, psi)]
+        body += lines[1 + n:]
+        name = f"wf_{k}.inp"
+        (tmp_path / name).write_text("\n".join(body))
+        files.append(name)
+    (tmp_path / "input.spc").write_text(deck)
+    capfd.readouterr()
+    D.run_scan(tmp_path / "input.spc", files, tmp_path / "job")
+    capfd.readouterr()
+    for k, f in enumerate(files, 1):
+        (tmp_path / f"single_{k}.spc").write_text(deck.replace("wf_pot.inp", f))
+        D.run(tmp_path / f"single_{k}.spc")
+        out = capfd.readouterr().out
+        i = out.index(" \n Correlation Function:")
+        j = out.index(" \n Spectrum:")
+        crl = (tmp_path / f"job{k}.crl").read_text()
+        spc = (tmp_path / f"job{k}.spc").read_text()
+        assert out[i:].startswith(crl)
+        assert spc == out[j:j + len(spc)]
+        assert out[j + len(spc):].startswith(" Spectrum done.")
