@@ -16,7 +16,7 @@ SOURCES = ["spo1d.cu", "capi.cu", "spo1d_inst_f32_pow2.cu", "spo1d_inst_f32_r3.c
            "spo1d_inst_f64_pow2.cu", "spo1d_inst_f64_r3.cu", "spo1d_static.cu", "sod1d_inst.cu",
            "diag1d.cu", "dropin.cu", "sil.cu",
            "spectrum.cu", "eig.cu", "mlp.cu", "mlp_tc.cu",
-           "spond.cu", "deck.cpp"]
+           "spond.cu", "deck.cpp", "pulse.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -484,11 +484,17 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
       a.c_out[slot] = make_double2(st[0] + st[1], st[2] - st[3]);
     return true;
   };
-  auto step = [&](double c, int slot) -> bool {
+  auto step = [&](double c, int slot, long call) -> bool {
     double q[4] = {0.0, 0.0, 0.0, 0.0};
+    const double e = a.ef ? a.ef[call] : 0.0;  // chpot.f:46-50: V - DM EF
     for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-      const double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
       const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
+      double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
+      if (a.dm) {
+        const double de = __ldg(a.dm + k) * e;
+        hv -= de * vk;
+        hu -= de * uk;
+      }
       double nu, nv;
       if (a.kabs == 1) {
         const double w = a.vabc[k];
@@ -532,8 +538,8 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   }
   int s0 = 1;
   if (a.start && a.nsteps >= 1) {
-    if (!step(0.25 * a.cst, -1)) return;  // psod.f:120-121
-    if (!step(0.5 * a.cst, 1)) return;    // psod.f:123-124
+    if (!step(0.25 * a.cst, -1, 0)) return;  // psod.f:120-121
+    if (!step(0.5 * a.cst, 1, 1)) return;    // psod.f:123-124
     for (int k = r.lo + t; k < r.hi; k += kSilThreads) {  // psod.f:136-141
       um[k] = __ldg(a.u0 + k);
       vm[k] = (a.copy_quirk && (k & 1)) ? __ldg(a.v0 + k - 1) : __ldg(a.v0 + k);
@@ -542,18 +548,25 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
     s0 = 2;
   }
   for (int s = s0; s <= a.nsteps; ++s)
-    if (!step(a.cst, s)) return;
+    if (!step(a.cst, s, a.slot0 + s)) return;
 }
 
 // <u|H u> + <v|H v> and |u|^2 + |v|^2 (EIGENERG, eigenerg.f:56-66): per-CTA
 // partials, then one CTA sums them in CTA order
-__global__ void __launch_bounds__(kSilThreads) sil_energy_kernel(SilArgs a, double* part) {
+__global__ void __launch_bounds__(kSilThreads) sil_energy_kernel(SilArgs a, double* part,
+                                                                 double ef) {
   __shared__ double sp[2], scratch[(kSilThreads / 32) * 8];
   double q[2] = {0.0, 0.0};
   for (long k = (long)blockIdx.x * kSilThreads + threadIdx.x; k < a.n;
        k += (long)gridDim.x * kSilThreads) {
     const double uk = a.u[k], vk = a.v[k];
-    q[0] += uk * apply_h(a, a.u, (int)k, 1.0) + vk * apply_h(a, a.v, (int)k, 1.0);
+    double hu = apply_h(a, a.u, (int)k, 1.0), hv = apply_h(a, a.v, (int)k, 1.0);
+    if (a.dm) {  // the potential V - DM EF of a pulse (chpot.f)
+      const double de = a.dm[k] * ef;
+      hu -= de * uk;
+      hv -= de * vk;
+    }
+    q[0] += uk * hu + vk * hv;
     q[1] += uk * uk + vk * vk;
   }
   block_sum<2>(q, sp, scratch);
@@ -586,6 +599,8 @@ struct espec_grid_plan {
   double *d_vpot = nullptr, *d_mask = nullptr, *d_u = nullptr, *d_v = nullptr;
   double *d_u0 = nullptr, *d_v0 = nullptr, *d_L = nullptr, *d_work = nullptr, *d_wbuf = nullptr;
   double *d_up = nullptr, *d_vp = nullptr;  // PSOD: the state one step back
+  double *d_dm = nullptr, *d_ef = nullptr;  // PSOD with a pulse: dipole, field per call
+  long n_ef = 0, slot = 0;                  // field entries; steps of the current run
   double *d_part = nullptr, *d_tot = nullptr, *d_epart = nullptr, *d_eout = nullptr;
   unsigned* d_bar = nullptr;
   int* d_err = nullptr;
@@ -596,7 +611,7 @@ struct espec_grid_plan {
 static void grid_free(espec_grid_plan* p) {
   void* b[] = {p->d_vpot, p->d_mask, p->d_u, p->d_v, p->d_u0, p->d_v0, p->d_L, p->d_work,
                p->d_wbuf, p->d_part, p->d_tot, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c,
-               p->d_up, p->d_vp};
+               p->d_up, p->d_vp, p->d_dm, p->d_ef};
   for (void* x : b)
     if (x) cudaFree(x);
 }
@@ -644,6 +659,8 @@ static SilArgs sil_args(const espec_grid_plan* p) {
     a.vabc = p->d_mask;
     a.kabs = p->absorb == ESPEC_ABS_VOPTIC ? 1 : (p->absorb == ESPEC_ABS_SMOOTHW ? 2 : 0);
     a.copy_quirk = (p->quirks & ESPEC_Q_PSOD_COPY) != 0;
+    a.dm = p->d_dm;
+    a.ef = p->d_dm ? p->d_ef : nullptr;
   }
   return a;
 }
@@ -779,6 +796,9 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
       return set_error(ESPEC_EINVAL, "a PSOD plan continues a run: call espec_grid_run first");
     }
     a.start = from_start ? 1 : 0;
+    a.slot0 = from_start ? 0 : p->slot;
+    if (p->d_dm && a.slot0 + nsteps >= p->n_ef)
+      return set_error(ESPEC_EINVAL, "the pulse field table ends before the run does");
     void* args[] = {&a};
     GRID_CK(cudaLaunchCooperativeKernel((const void*)psod_kernel, dim3(p->nblocks),
                                         dim3(kSilThreads), args, 0, st));
@@ -789,6 +809,7 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
       std::swap(p->d_v, p->d_vp);
     }
     p->has_state = true;
+    p->slot = a.slot0 + nsteps;
     return ESPEC_OK;
   }
   void* args[] = {&a};
@@ -828,14 +849,15 @@ extern "C" int espec_grid_results(espec_grid_plan* p, double* c_re, double* c_im
   return ESPEC_OK;
 }
 
-extern "C" int espec_grid_energies(espec_grid_plan* p, double* e, double* norm, void* stream) {
+extern "C" int espec_grid_energies_at(espec_grid_plan* p, double ef, double* e, double* norm,
+                                      void* stream) {
   if (!p || !e || !norm) return set_error(ESPEC_EINVAL, "null argument");
   if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_grid_load has not been called");
   cudaStream_t st = (cudaStream_t)stream;
   SilArgs a = sil_args(p);
   long nbk = (p->n + kSilThreads - 1) / kSilThreads;
   if (nbk > 1024) nbk = 1024;
-  sil_energy_kernel<<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart);
+  sil_energy_kernel<<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart, ef);
   GRID_CK(cudaGetLastError());
   sum_parts_kernel<<<1, 32, 0, st>>>(p->d_epart, (int)nbk, p->d_eout);
   GRID_CK(cudaGetLastError());
@@ -861,6 +883,27 @@ extern "C" int espec_grid_previous(espec_grid_plan* p, double* psi_re, double* p
   GRID_CK(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   GRID_CK(cudaStreamSynchronize(st));
   if (err) return set_error(ESPEC_ECUDA, "a grid barrier of the PSOD kernel timed out");
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_energies(espec_grid_plan* p, double* e, double* norm, void* stream) {
+  return espec_grid_energies_at(p, 0.0, e, norm, stream);
+}
+
+extern "C" int espec_grid_set_pulse(espec_grid_plan* p, const double* dm, const double* ef,
+                                    long ncalls, int where) {
+  if (!p || p->method != ESPEC_PSOD) return set_error(ESPEC_EINVAL, "pulses drive PSOD plans");
+  if (!dm || !ef || ncalls < 1) return set_error(ESPEC_EINVAL, "dipole and field table needed");
+  const cudaMemcpyKind kind =
+      where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  if (p->d_ef) cudaFree(p->d_ef);
+  p->d_ef = nullptr;
+  p->n_ef = 0;
+  if (!p->d_dm) GRID_CK(cudaMalloc(&p->d_dm, (size_t)p->n * 8));
+  GRID_CK(cudaMalloc(&p->d_ef, (size_t)ncalls * 8));
+  GRID_CK(cudaMemcpy(p->d_dm, dm, (size_t)p->n * 8, kind));
+  GRID_CK(cudaMemcpy(p->d_ef, ef, (size_t)ncalls * 8, kind));
+  p->n_ef = ncalls;
   return ESPEC_OK;
 }
 

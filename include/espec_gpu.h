@@ -279,6 +279,17 @@ int espec_grid_energies(espec_grid_plan* plan, double* e, double* norm, void* st
  * into dst(1:N, 1:MP) with leading dimension ld >= N (column-major) */
 int espec_grid_basis(espec_grid_plan* plan, int chain, double* dst, int ld, int where,
                      void* stream);
+/* <u|H u> + <v|H v> and the norm with the potential V - DM EF (a PSOD plan
+ * with a pulse; EF = 0 gives espec_grid_energies) */
+int espec_grid_energies_at(espec_grid_plan* plan, double ef, double* e, double* norm,
+                           void* stream);
+/* Laser pulse for an ESPEC_PSOD plan (PPSOD, ppsod.f with chpot.f): PSODAUX
+ * call j of a run uses the potential V - dm * ef[j] (dm: the dipole function
+ * on the grid; ef: the field of every call, espec_ppsod_field); calls count
+ * from the start of a run (0, 1: the start-up; step s >= 2: call s) and go on
+ * through espec_grid_continue.  Copies both tables. */
+int espec_grid_set_pulse(espec_grid_plan* plan, const double* dm, const double* ef, long ncalls,
+                         int where);
 /* ESPEC_PSOD plans: psi(TF - dt) of the last run (synchronises) */
 int espec_grid_previous(espec_grid_plan* plan, double* psi_re, double* psi_im, int where,
                         void* stream);
@@ -396,6 +407,22 @@ int espec_to_bf16(const float* x, void* y, long count, void* stream);
 int espec_mlp_adam_bf16(float* w, const float* g, float* m1, float* m2, long count,
                         const float* hyper, float b1, float b2, float eps, void* w_bf16,
                         void* stream);
+
+/* ----------------------------------------------------------------------
+ * Laser pulses (ef.f): E(t) in atomic units for the shapes of *PULSE_AND_DIPOLE;
+ * par = {E0, TP, OMG, T0 (.GAUS, .GGAUS) or TD (.SIN2), SNI, KL (.GGAUS)}.
+ * ---------------------------------------------------------------------- */
+#define ESPEC_PULSE_NONE 0
+#define ESPEC_PULSE_GAUS 1
+#define ESPEC_PULSE_GGAUS 2
+#define ESPEC_PULSE_SIN2 3
+double espec_pulse_field(int shape, const double* par, double t);
+/* the field of every PSODAUX call of a PPSOD run from TI to TF (ppsod.f:252-260,
+ * 378-386): ef[0] at (TI+DT)/2, ef[1] at TI+DT, then one per step of DT for
+ * NF = NINT((TF + DT/2 - TI - DT)/DT) steps; returns NF + 2 (the run has
+ * NF + 1 steps) or a negative error code */
+long espec_ppsod_field(int shape, const double* par, double ti, double tf, double dt, double* ef,
+                       long cap);
 
 /* ----------------------------------------------------------------------
  * Spectrum stage on the device, batched over packets (FP64).

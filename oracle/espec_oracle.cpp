@@ -927,6 +927,83 @@ extern "C" int orc_psod(const orc_prop_t* p, const double* vpot, const double* v
   return cs.n;
 }
 
+// ef.f:20-60  EF
+extern "C" double orc_ef(int shape, const double* par, double t) {
+  const double FAT = +2.1132e-9;
+  const double FATE = +2.29371276e+17 * 3.335664e-28;
+  const double FATT = +1.5192676;
+  const double PI = +3.14159265358979323846;
+  const double e0 = par[0], tp = par[1], omg = par[2], t0 = par[3], sni = par[4];
+  if (shape == 1) {
+    double ef = e0 * std::exp(-4.0 * 0.693147181 * (t - t0) * (t - t0) / (tp * tp)) *
+                std::cos(omg * t * FATT + sni);
+    return ef * FATE;
+  }
+  if (shape == 2) {
+    const int kl = (int)par[5];
+    const double a1 = 1.0 / (2.0 * kl);
+    const double tpa = tp / std::pow((double)0.693147181f, a1);  // REAL literal
+    return FAT * std::sqrt(e0 * std::exp(-std::pow((t - t0) / tpa, 2.0 * kl))) *
+           std::cos(omg * t * FATT + sni);
+  }
+  if (shape == 3) {
+    double ef = e0 * std::cos(PI * (t - t0) / tp) * std::cos(PI * (t - t0) / tp) *
+                std::cos(omg * (t - t0) * FATT + sni);
+    return ef * FATE;
+  }
+  return 0.0;
+}
+
+// ppsod.f:64-400  PPSOD's propagation
+extern "C" int orc_ppsod(const orc_prop_t* p, const double* vp, const double* vabc,
+                         const double* dm, int shape, const double* par, double* u1, double* v1,
+                         double* u2, double* v2, double* c_re, double* c_im, int c_cap) {
+  const int n = npts(p);
+  CSink cs{c_re, c_im, c_cap};
+  const double cst = 2.0 * p->dt / ORC_SHFS;
+  std::vector<double> u0(u1, u1 + n), v0(v1, v1 + n), work(n), veff(n);
+  for (int i = 0; i < n; ++i) {
+    u2[i] = u0[i];
+    v2[i] = v0[i];
+  }
+  auto chpot = [&](double t) {  // chpot.f:44-51
+    const double e = orc_ef(shape, par, t);
+    for (int i = 0; i < n; ++i) veff[i] = vp[i] - dm[i] * e;
+  };
+  auto corr = [&]() {
+    cs.put(orc_fcorrel(n, u0.data(), u2) + orc_fcorrel(n, v0.data(), v2),
+           orc_fcorrel(n, u0.data(), v2) - orc_fcorrel(n, v0.data(), u2));
+  };
+  corr();
+  double t = p->ti;
+  chpot((t + p->dt) / 2.0);
+  psod_aux(p, cst / 4.0, veff.data(), vabc, u1, u2, v1, v2, work.data());
+  chpot(t + p->dt);
+  psod_aux(p, cst / 2.0, veff.data(), vabc, u1, u2, v1, v2, work.data());
+  int mc = 1;
+  if (mc == p->lc) {
+    mc = 0;
+    corr();
+  }
+  for (int i = 0; i < n; ++i) {  // ppsod.f:373-376
+    u1[i] = u0[i];
+    v1[i] = v0[i];
+  }
+  t = p->ti + p->dt;
+  const long nf = std::lround((p->tf + p->dt / 2.0 - t) / p->dt);
+  for (long k = 1; k <= nf; ++k) {
+    t = t + p->dt;
+    chpot(t);
+    psod_aux(p, cst, veff.data(), vabc, u1, u2, v1, v2, work.data());
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      corr();
+    }
+  }
+  return cs.n;
+}
+
 // ---------------------------------------------------------------------------
 // Symmetric tridiagonal eigensolver (stands in for DSTEVX('V','A'),
 // dstevx.f).  Implicit-shift QL iteration with Wilkinson shifts on a copy of

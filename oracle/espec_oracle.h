@@ -115,6 +115,18 @@ int orc_psod(const orc_prop_t* p, const double* vpot, const double* vabc,
              double* c_im, int c_cap, double* rows, int row_cap, int* nrows,
              int* info);
 
+/* EF (ef.f:20-60): shape 0 none, 1 .GAUS, 2 .GGAUS, 3 .SIN2;
+ * par = {E0, TP, OMG, T0 or TD, SNI, KL} */
+double orc_ef(int shape, const double* par, double t);
+/* PPSOD's propagation (ppsod.f:64-400 without its printed table, files and
+ * populations): PSOD's steps with the potential VP - DM EF(t) of chpot.f at
+ * (TI+DT)/2, TI+DT and then each step's end time; C(t) every LC steps, the
+ * start-up samples included (the reference stores those only while it
+ * prints) */
+int orc_ppsod(const orc_prop_t* p, const double* vp, const double* vabc, const double* dm,
+              int shape, const double* par, double* u1, double* v1, double* u2, double* v2,
+              double* c_re, double* c_im, int c_cap);
+
 /* symmetric tridiagonal eigensolver: d[n] diag, e[n-1] offdiag, z[n*n]
  * column-major eigenvectors, eigenvalues ascending in w.  0 on success. */
 int orc_tridiag_eig(int n, const double* d, const double* e, double* w,

@@ -66,6 +66,8 @@ def lib():
         _lib.orc_fcorrel.restype = C.c_double
         _lib.orc_ecnorm.restype = C.c_double
         _lib.orc_eigenerg.restype = C.c_double
+        _lib.orc_ef.restype = C.c_double
+        _lib.orc_ef.argtypes = [C.c_int, C.c_void_p, C.c_double]
         _lib.orc_efft4.restype = C.c_double
         _lib.orc_efft4.argtypes = [C.c_int, i, C.c_double, d, d, d, d]
         _lib.orc_spo_step.argtypes = [C.c_int, i, C.c_double, C.c_double, C.c_double,
@@ -215,6 +217,25 @@ def psod(p, vpot, u, v, vabc=None):
     r = _run(lib().orc_psod, p, vpot, vabc, [u1, v1, u2, v2], *_caps(p))
     r.update(u=u2, v=v2, u_prev=u1, v_prev=v1)
     return r
+
+
+def ef(shape, par, t):
+    return lib().orc_ef(int(shape), _p(f64(list(par) + [0.0] * (6 - len(par)))), float(t))
+
+
+def ppsod(p, vp, dm, shape, par, u, v, vabc=None):
+    """PPSOD's propagation: C(t) every LC steps, psi(TF), psi(TF - dt)."""
+    n = int(np.prod([p.np[a] for a in range(p.ndim)]))
+    u1, v1 = f64(u).copy(), f64(v).copy()
+    u2, v2 = np.zeros_like(u1), np.zeros_like(v1)
+    max_c, _ = _caps(p)
+    cre, cim = np.zeros(max_c + 4), np.zeros(max_c + 4)
+    vabc = f64(vabc) if vabc is not None else np.zeros(n)
+    parr = f64(list(par) + [0.0] * (6 - len(par)))
+    nc = lib().orc_ppsod(C.byref(p), _p(f64(vp)), _p(vabc), _p(f64(dm)), int(shape), _p(parr),
+                         _p(u1), _p(v1), _p(u2), _p(v2), _p(cre), _p(cim), C.c_int(max_c + 4))
+    nc = min(nc, max_c + 4)
+    return dict(c=cre[:nc] + 1j * cim[:nc], u=u2, v=v2, u_prev=u1, v_prev=v1, nc=nc)
 
 
 def plnz(p, vpot, u, v, vabc=None):
