@@ -1,6 +1,7 @@
 // pulse.cpp -- the laser field of eSPec's pulse-driven propagators: EF
-// (ef.f:20-60) for the pulse shapes, and the field of every PSODAUX call of a
-// PPSOD run (ppsod.f:252-260, 378-386), the table espec_grid_set_pulse takes.
+// (ef.f:20-60) for the pulse shapes, and the field of every step of a PPSOD
+// run (ppsod.f:252-260, 378-386) or a PPLNZ run (pplnz.f:139-141), the tables
+// espec_grid_set_pulse takes.
 #include <cmath>
 
 #include "espec_gpu.h"
@@ -55,4 +56,20 @@ extern "C" long espec_ppsod_field(int shape, const double* par, double ti, doubl
     ef[1 + k] = espec_pulse_field(shape, par, t);
   }
   return nf + 2;
+}
+
+extern "C" long espec_pplnz_field(int shape, const double* par, double ti, double tf, double dt,
+                                  double* ef, long cap) {
+  if (!ef || cap < 1 || dt <= 0.0) return espec::set_error(ESPEC_EINVAL, "bad field table");
+  // DO T = TI+DT, TF+DT/2, DT (pplnz.f:139): CHPOT(T) before each step
+  const double x = (tf + dt / 2.0 - (ti + dt) + dt) / dt;
+  const long nt = x > 0.0 ? (long)x : 0;
+  if (nt + 1 > cap) return espec::set_error(ESPEC_EINVAL, "field table too short");
+  ef[0] = espec_pulse_field(shape, par, ti);
+  double t = ti + dt;
+  for (long s = 1; s <= nt; ++s) {
+    ef[s] = espec_pulse_field(shape, par, t);
+    t = t + dt;
+  }
+  return nt + 1;
 }

@@ -335,6 +335,9 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
       }
       __syncthreads();
     }
+    // potential of this step with a pulse (pplnz.f:139-141): V - DM EF(T) of
+    // the time the step lands at
+    const double efs = a.dm ? a.ef[a.slot0 + s + 1] : 0.0;
     // ---- m Lanczos iterations of both chains
     for (int it = 0; it < m; ++it) {
       // vi = work/bt0, w = H vi - bt0 v_prev at the CTA's points, and the dot
@@ -358,7 +361,9 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
             for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
             const double vi = __ldcg(src + k) * rb;
             const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
-            const double w = apply_h(a, src, k, rb) - bt0 * vprev;
+            double hv = apply_h(a, src, k, rb);
+            if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
+            const double w = hv - bt0 * vprev;
             const double xk = __ldcg(x + k);
             Lc[(long)it * n + k] = vi;
             a.wbuf[c * n + k] = w;
@@ -659,9 +664,9 @@ static SilArgs sil_args(const espec_grid_plan* p) {
     a.vabc = p->d_mask;
     a.kabs = p->absorb == ESPEC_ABS_VOPTIC ? 1 : (p->absorb == ESPEC_ABS_SMOOTHW ? 2 : 0);
     a.copy_quirk = (p->quirks & ESPEC_Q_PSOD_COPY) != 0;
-    a.dm = p->d_dm;
-    a.ef = p->d_dm ? p->d_ef : nullptr;
   }
+  a.dm = p->d_dm;
+  a.ef = p->d_dm ? p->d_ef : nullptr;
   return a;
 }
 
@@ -812,9 +817,13 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
     p->slot = a.slot0 + nsteps;
     return ESPEC_OK;
   }
+  a.slot0 = from_start ? 0 : p->slot;
+  if (p->d_dm && a.slot0 + nsteps >= p->n_ef)
+    return set_error(ESPEC_EINVAL, "the pulse field table ends before the run does");
   void* args[] = {&a};
   GRID_CK(cudaLaunchCooperativeKernel((const void*)sil_kernel, dim3(p->nblocks), dim3(kSilThreads),
                                       args, 0, st));
+  p->slot = a.slot0 + nsteps;
   return ESPEC_OK;
 }
 
@@ -892,7 +901,7 @@ extern "C" int espec_grid_energies(espec_grid_plan* p, double* e, double* norm, 
 
 extern "C" int espec_grid_set_pulse(espec_grid_plan* p, const double* dm, const double* ef,
                                     long ncalls, int where) {
-  if (!p || p->method != ESPEC_PSOD) return set_error(ESPEC_EINVAL, "pulses drive PSOD plans");
+  if (!p) return set_error(ESPEC_EINVAL, "null plan");
   if (!dm || !ef || ncalls < 1) return set_error(ESPEC_EINVAL, "dipole and field table needed");
   const cudaMemcpyKind kind =
       where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;

@@ -61,10 +61,10 @@ struct SilArgs {
   const double* vabc;
   int kabs;  // 0 none, 1 .VOPTIC, 2 .SMOOTHW
   int start, copy_quirk;
-  // a laser pulse (.PPSOD, ppsod.f with chpot.f): the potential of PSODAUX
-  // call j is V - dm E_j; ef[j] for every call of the run, calls counted from
-  // the start of the run (0, 1: the start-up; step s >= 2: call s), slot0 =
-  // the steps done before this launch
+  // a laser pulse (chpot.f): PSOD -- the potential of PSODAUX call j is
+  // V - dm ef[j], calls counted from the start of the run (0, 1: the
+  // start-up; step s >= 2: call s, .PPSOD); SIL -- the step landing at step
+  // j uses V - dm ef[j] (.PPSIL); slot0 = the steps done before this launch
   const double* dm;
   const double* ef;
   long slot0;

@@ -71,6 +71,22 @@ class SilGrid:
                 "espec_grid_energies")
         return e.value, nr.value
 
+    def set_pulse(self, dm, ef):
+        """A laser pulse (chpot.f): V - dm * ef[j] in PSODAUX call j of a PSOD
+        plan (PPSOD; ef from ppsod_field) or in the step landing at step j of a
+        SIL plan (PPLNZ; ef from pplnz_field)."""
+        self._pulse = (N.f64(np.ravel(dm, order="F")), N.f64(ef))
+        N.check(N.load().espec_grid_set_pulse(self._h, N.ptr(self._pulse[0]),
+                                              N.ptr(self._pulse[1]), len(self._pulse[1]),
+                                              N.MEM_HOST), "espec_grid_set_pulse")
+
+    def energies_at(self, ef, stream=None):
+        """(<u|H u> + <v|H v>, norm) with the potential V - dm * ef."""
+        e, nr = C.c_double(), C.c_double()
+        N.check(N.load().espec_grid_energies_at(self._h, float(ef), C.byref(e), C.byref(nr),
+                                                stream), "espec_grid_energies_at")
+        return e.value, nr.value
+
     def close(self):
         if self._h:
             N.load().espec_grid_destroy(self._h)
@@ -99,22 +115,6 @@ class PsodGrid(SilGrid):
                 "espec_grid_previous")
         return pr + 1j * pi
 
-    def set_pulse(self, dm, ef):
-        """Potential V - dm * ef[j] in PSODAUX call j (PPSOD, chpot.f); ef from
-        ppsod_field()."""
-        self._pulse = (N.f64(np.ravel(dm, order="F")), N.f64(ef))
-        N.check(N.load().espec_grid_set_pulse(self._h, N.ptr(self._pulse[0]),
-                                              N.ptr(self._pulse[1]), len(self._pulse[1]),
-                                              N.MEM_HOST), "espec_grid_set_pulse")
-
-    def energies_at(self, ef, stream=None):
-        """(<u|H u> + <v|H v>, norm) with the potential V - dm * ef."""
-        e, nr = C.c_double(), C.c_double()
-        N.check(N.load().espec_grid_energies_at(self._h, float(ef), C.byref(e), C.byref(nr),
-                                                stream), "espec_grid_energies_at")
-        return e.value, nr.value
-
-
 def pulse_field(shape, par, t):
     """E(t) of ef.f for shape N.PULSE_* and par = (E0, TP, OMG, T0 or TD, SNI[, KL])."""
     p = N.f64(list(par) + [0.0] * (6 - len(par)))
@@ -130,6 +130,18 @@ def ppsod_field(shape, par, ti, tf, dt):
     k = N.load().espec_ppsod_field(int(shape), N.ptr(p), float(ti), float(tf), float(dt),
                                    N.ptr(ef), cap)
     N.check(0 if k > 0 else int(k), "espec_ppsod_field")
+    return ef[:k]
+
+
+def pplnz_field(shape, par, ti, tf, dt):
+    """The field of every step of a PPLNZ run (ef[0] at TI); the run has
+    len(result) - 1 steps."""
+    p = N.f64(list(par) + [0.0] * (6 - len(par)))
+    cap = int(round((tf - ti) / dt)) + 8
+    ef = np.zeros(cap)
+    k = N.load().espec_pplnz_field(int(shape), N.ptr(p), float(ti), float(tf), float(dt),
+                                   N.ptr(ef), cap)
+    N.check(0 if k > 0 else int(k), "espec_pplnz_field")
     return ef[:k]
 
 

@@ -283,11 +283,12 @@ int espec_grid_basis(espec_grid_plan* plan, int chain, double* dst, int ld, int 
  * with a pulse; EF = 0 gives espec_grid_energies) */
 int espec_grid_energies_at(espec_grid_plan* plan, double ef, double* e, double* norm,
                            void* stream);
-/* Laser pulse for an ESPEC_PSOD plan (PPSOD, ppsod.f with chpot.f): PSODAUX
- * call j of a run uses the potential V - dm * ef[j] (dm: the dipole function
- * on the grid; ef: the field of every call, espec_ppsod_field); calls count
- * from the start of a run (0, 1: the start-up; step s >= 2: call s) and go on
- * through espec_grid_continue.  Copies both tables. */
+/* Laser pulse (chpot.f): dm = the dipole function on the grid, ef = a field
+ * table counted from the start of a run and continued through
+ * espec_grid_continue.  ESPEC_PSOD plans (PPSOD, ppsod.f): PSODAUX call j
+ * uses the potential V - dm * ef[j] (0, 1: the start-up; step s >= 2: call s;
+ * espec_ppsod_field).  ESPEC_SIL plans (PPLNZ, pplnz.f): the step landing at
+ * step j uses V - dm * ef[j] (espec_pplnz_field).  Copies both tables. */
 int espec_grid_set_pulse(espec_grid_plan* plan, const double* dm, const double* ef, long ncalls,
                          int where);
 /* ESPEC_PSOD plans: psi(TF - dt) of the last run (synchronises) */
@@ -422,6 +423,11 @@ double espec_pulse_field(int shape, const double* par, double t);
  * NF = NINT((TF + DT/2 - TI - DT)/DT) steps; returns NF + 2 (the run has
  * NF + 1 steps) or a negative error code */
 long espec_ppsod_field(int shape, const double* par, double ti, double tf, double dt, double* ef,
+                       long cap);
+/* the field of every step of a PPLNZ run (pplnz.f:139-141, DO T = TI+DT,
+ * TF+DT/2, DT with CHPOT(T) before each step): ef[0] = EF(TI), ef[s] = EF at
+ * the time step s lands at; returns the number of steps + 1 */
+long espec_pplnz_field(int shape, const double* par, double ti, double tf, double dt, double* ef,
                        long cap);
 
 /* ----------------------------------------------------------------------

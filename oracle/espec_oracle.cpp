@@ -1241,6 +1241,40 @@ extern "C" int orc_plnz(const orc_prop_t* p, const double* vpot, const double* v
   return cs.n;
 }
 
+// pplnz.f:139-141  PPLNZ's propagation: DO T = TI+DT, TF+DT/2, DT with the
+// potential VP - DM EF(T) (chpot.f) in each PLNZAUX step; C(t) every LC steps
+extern "C" int orc_pplnz(const orc_prop_t* p, const double* vp, const double* vabc,
+                         const double* dm, int shape, const double* par, double* u, double* v,
+                         double* c_re, double* c_im, int c_cap) {
+  const int n = npts(p);
+  CSink cs{c_re, c_im, c_cap};
+  const double cst = p->dt / ORC_SHFS;
+  int mp = p->mp;
+  if (p->change && mp > p->lmtreort) mp = p->lmtreort;
+  if (p->absorb == ORC_ABS_VOPTIC) return -1;
+  std::vector<double> u0(u, u + n), v0(v, v + n), veff(n);
+  auto corr = [&]() {
+    cs.put(orc_fcorrel(n, u0.data(), u) + orc_fcorrel(n, v0.data(), v),
+           orc_fcorrel(n, u0.data(), v) - orc_fcorrel(n, v0.data(), u));
+  };
+  corr();
+  int mc = 0;
+  const int nit = orc_do_count(p->ti + p->dt, p->tf + p->dt / 2.0, p->dt);
+  double t = p->ti + p->dt;
+  for (int it = 0; it < nit; ++it, t = t + p->dt) {
+    const double e = orc_ef(shape, par, t);
+    for (int i = 0; i < n; ++i) veff[i] = vp[i] - dm[i] * e;
+    if (sil_step(p, mp, veff.data(), vabc, cst, u, v)) return -1;
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      corr();
+    }
+  }
+  return cs.n;
+}
+
+
 // ---------------------------------------------------------------------------
 // Spectrum stage
 // ---------------------------------------------------------------------------

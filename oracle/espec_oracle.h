@@ -127,6 +127,12 @@ int orc_ppsod(const orc_prop_t* p, const double* vp, const double* vabc, const d
               int shape, const double* par, double* u1, double* v1, double* u2, double* v2,
               double* c_re, double* c_im, int c_cap);
 
+/* PPLNZ's propagation (pplnz.f:139-141, no printing): PLNZ's steps with the
+ * potential VP - DM EF(T) at the time each step lands at */
+int orc_pplnz(const orc_prop_t* p, const double* vp, const double* vabc, const double* dm,
+              int shape, const double* par, double* u, double* v, double* c_re, double* c_im,
+              int c_cap);
+
 /* symmetric tridiagonal eigensolver: d[n] diag, e[n-1] offdiag, z[n*n]
  * column-major eigenvectors, eigenvalues ascending in w.  0 on success. */
 int orc_tridiag_eig(int n, const double* d, const double* e, double* w,

@@ -238,6 +238,22 @@ def ppsod(p, vp, dm, shape, par, u, v, vabc=None):
     return dict(c=cre[:nc] + 1j * cim[:nc], u=u2, v=v2, u_prev=u1, v_prev=v1, nc=nc)
 
 
+def pplnz(p, vp, dm, shape, par, u, v, vabc=None):
+    """PPLNZ's propagation: C(t) every LC steps and psi(TF)."""
+    n = int(np.prod([p.np[a] for a in range(p.ndim)]))
+    u, v = f64(u).copy(), f64(v).copy()
+    max_c, _ = _caps(p)
+    cre, cim = np.zeros(max_c + 4), np.zeros(max_c + 4)
+    vabc = f64(vabc) if vabc is not None else np.zeros(n)
+    parr = f64(list(par) + [0.0] * (6 - len(par)))
+    nc = lib().orc_pplnz(C.byref(p), _p(f64(vp)), _p(vabc), _p(f64(dm)), int(shape), _p(parr),
+                         _p(u), _p(v), _p(cre), _p(cim), C.c_int(max_c + 4))
+    if nc < 0:
+        raise RuntimeError("oracle propagation stopped (reference STOP condition)")
+    nc = min(nc, max_c + 4)
+    return dict(c=cre[:nc] + 1j * cim[:nc], u=u, v=v, nc=nc)
+
+
 def plnz(p, vpot, u, v, vabc=None):
     u, v = f64(u).copy(), f64(v).copy()
     r = _run(lib().orc_plnz, p, vpot, vabc, [u, v], *_caps(p))

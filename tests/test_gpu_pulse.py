@@ -88,3 +88,38 @@ def test_ppsod_continue_and_field_energies(oracle):
     assert abs(e0 - ref_e0) <= 1e-12 * abs(ref_e0)
     one.close()
     seg.close()
+
+
+@pytest.mark.parametrize("np_,pulse,mask,mp", [([301], "gaus", False, 10), ([256], "sin2", True, 12),
+                                              ([40, 36], "ggaus", False, 8),
+                                              ([10, 12, 9], "gaus", True, 6)])
+def test_pplnz_matches_oracle(oracle, np_, pulse, mask, mp):
+    """PPLNZ's time loop (pplnz.f:139-141): SIL steps with V - DM EF(T) at the
+    time each step lands at."""
+    v, psi, sh, grids = packet(np_, sum(np_) + mp)
+    sm = [1000.0 + 400.0 * a for a in range(len(np_))]
+    shm = [G.shm_of(m, h) for m, h in zip(sm, sh)]
+    dm = (0.8 * grids[0] + 0.3 * grids[0] ** 2).ravel(order="F")
+    vabc = np.where(grids[0] > 0.35, 0.97, 1.0).ravel(order="F") if mask else None
+    absorb = NAT.ABS_SMOOTHW if mask else NAT.ABS_NONE
+    shape, par = PULSES[pulse]
+    dt, ti, tf = 0.02 * NAT.SHFS, 0.0, 0.2
+    p = oracle.make_prop(np_, dt, ti, tf, sh, sm, lc=1, absorb=absorb, mp=mp, lmtreort=16,
+                         change=0, shm=shm)
+    ref = oracle.pplnz(p, v, dm, shape, par, np.real(psi), np.imag(psi), vabc=vabc)
+    ef = GR.pplnz_field(shape, par, ti, tf, dt)
+    g = E.SilGrid(np_, shm, dt, mp, absorb=absorb)
+    g.load(v, psi, vabc=vabc)
+    g.set_pulse(dm, ef)
+    g.run(len(ef) - 1)
+    c, out = g.results()
+    assert len(c) == ref["nc"]
+    assert np.max(np.abs(c - ref["c"])) <= 1e-10, np.max(np.abs(c - ref["c"]))
+    assert np.max(np.abs(out - (ref["u"] + 1j * ref["v"]))) <= 1e-10
+    e, _ = g.energies_at(ef[-1])
+    veff = v - dm * ef[-1]
+    ref_e = oracle.eigenerg(np_, shm, veff, out.real) + oracle.eigenerg(np_, shm, veff, out.imag)
+    assert abs(e - ref_e) <= 1e-12 * abs(ref_e)
+    g.close()
+    ref0 = oracle.pplnz(p, v, dm, NAT.PULSE_NONE, par, np.real(psi), np.imag(psi), vabc=vabc)
+    assert np.max(np.abs(ref0["c"] - ref["c"])) > 1e-6
