@@ -220,24 +220,26 @@ void msg1003(const char* s) {
   std::printf("\n   %s\n", t.substr(0, 68).c_str());
 }
 
-// list-directed REAL*8 as gfortran writes it: 1PG25.17E3 after one blank
+// list-directed REAL*8 as the reference's executable writes it: one blank,
+// then 1PG23.15E3 (F form with 15 significant digits and 5 trailing blanks
+// for 0.1 <= |x| < 1e15, else 1.ddd...E+xxx)
 std::string list_real(double x) {
   char buf[64];
   const double ax = std::fabs(x);
-  if (ax != 0.0 && (ax < 0.1 || ax >= 1e17)) {
-    std::snprintf(buf, sizeof buf, "%.16E", x);
+  if (ax != 0.0 && (ax < 0.1 || ax >= 1e15)) {
+    std::snprintf(buf, sizeof buf, "%.15E", x);
     std::string s(buf);
     const size_t e = s.find('E');
     const int ex = std::atoi(s.c_str() + e + 1);
     char eb[16];
     std::snprintf(eb, sizeof eb, "E%c%03d", ex < 0 ? '-' : '+', std::abs(ex));
     s = s.substr(0, e) + eb;
-    return std::string(26 - s.size(), ' ') + s;
+    return " " + std::string(s.size() < 23 ? 23 - s.size() : 0, ' ') + s;
   }
-  const int k = ax == 0.0 ? 1 : (int)std::floor(std::log10(ax)) + 1;
-  std::snprintf(buf, sizeof buf, "%.*f", 17 - (k > 0 ? k : 0), x);
+  const int k = ax == 0.0 ? 0 : (int)std::floor(std::log10(ax)) + 1;
+  std::snprintf(buf, sizeof buf, "%.*f", 15 - (k > 0 ? k : 0), x);
   std::string s(buf);
-  return std::string(21 - s.size(), ' ') + s + "     ";
+  return " " + std::string(s.size() < 18 ? 18 - s.size() : 0, ' ') + s + "     ";
 }
 
 struct Run {

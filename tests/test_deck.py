@@ -49,3 +49,19 @@ def test_final_time_not_adequate_for_fft(tmp_path, capfd):
     msg = refused(tmp_path, text, {"wf_pot.inp": src})
     assert "not adequate for FFT" in msg
     assert "<<<>>> Final time is not adequate for FFT <<<>>>" in capfd.readouterr().out
+
+
+def test_final_time_warning_text(tmp_path, capfd):
+    """*CHANGE .YES with a TF that does not fit 2^MF samples: the warning
+    line as the executable prints it (its list-directed REAL*8 is 1PG23.15E3;
+    text taken from espec_v07.x on this deck with TF = 0.3101).  Printed
+    before any device work, so the check runs with or without a GPU."""
+    src = os.path.join(HERE, "golden", "deck_spo_hwhm")
+    (tmp_path / "wf_pot.inp").write_text(open(os.path.join(src, "wf_pot.inp")).read())
+    (tmp_path / "input.spc").write_text(BASE.replace("0.3096171935104", "0.3101"))
+    try:
+        D.run(tmp_path / "input.spc")
+    except N.EspecError:
+        pass  # no device here: the propagation itself fails after the warning
+    out = capfd.readouterr().out.split("\n")
+    assert " -> Warning! Final time changed to  0.309617193510400     " in out
