@@ -1241,6 +1241,107 @@ extern "C" int orc_plnz(const orc_prop_t* p, const double* vpot, const double* v
   return cs.n;
 }
 
+// ppsod.f:64-400 with its table: rows of 7 + npr values (T, ET, E0, CR, CI,
+// |C|^2, |P_1|^2 .. |P_npr|^2, FNT) as FORMAT 1021 prints them -- ET with the potential of the
+// last CHPOT, E0 with VP, P_k = <W_k|psi> (W real, ppsod.f:158-189), FNT the
+// norm; C(t) stored in LNZVC as ppsod.f does: C(0) and the start-up sample
+// only inside the print test (ppsod.f:145-150, 263-297), the loop's every LC
+// steps; INFO = 1 when the norm drifts (no absorber, ppsod.f:434-438)
+extern "C" int orc_ppsod_table(const orc_prop_t* p, const double* vp, const double* vabc,
+                               const double* dm, int shape, const double* par, int npr,
+                               const double* w, double* u1, double* v1, double* u2, double* v2,
+                               double* c_re, double* c_im, int c_cap, double* rows, int row_cap,
+                               int* nrows, int* info) {
+  const int n = npts(p);
+  CSink cs{c_re, c_im, c_cap};
+  const int ncol = 7 + npr;
+  int nr = 0;
+  *info = 0;
+  const double cst = 2.0 * p->dt / ORC_SHFS;
+  std::vector<double> u0(u1, u1 + n), v0(v1, v1 + n), work(n), veff(vp, vp + n);
+  for (int i = 0; i < n; ++i) {
+    u2[i] = u0[i];
+    v2[i] = v0[i];
+  }
+  auto chpot = [&](double t) {
+    const double e = orc_ef(shape, par, t);
+    for (int i = 0; i < n; ++i) veff[i] = vp[i] - dm[i] * e;
+  };
+  double f0 = 0.0;
+  auto row = [&](double t) {
+    const double cr = orc_fcorrel(n, u0.data(), u2) + orc_fcorrel(n, v0.data(), v2);
+    const double ci = orc_fcorrel(n, u0.data(), v2) - orc_fcorrel(n, v0.data(), u2);
+    if (rows && nr < row_cap) {
+      double* r = rows + (size_t)ncol * nr;
+      r[0] = t;
+      r[1] = orc_eigenerg(p->ndim, p->np, p->shm, veff.data(), u2) +
+             orc_eigenerg(p->ndim, p->np, p->shm, veff.data(), v2);
+      r[2] = orc_eigenerg(p->ndim, p->np, p->shm, vp, u2) +
+             orc_eigenerg(p->ndim, p->np, p->shm, vp, v2);
+      r[3] = cr;
+      r[4] = ci;
+      r[5] = cr * cr + ci * ci;
+      for (int k = 0; k < npr; ++k) {
+        const double pr = orc_fcorrel(n, w + (size_t)n * k, u2);
+        const double pi = orc_fcorrel(n, w + (size_t)n * k, v2);
+        r[6 + k] = pr * pr + pi * pi;
+      }
+    }
+    const double fnt = orc_fcorrel(n, u2, u2) + orc_fcorrel(n, v2, v2);
+    if (rows && nr < row_cap) rows[(size_t)ncol * nr + ncol - 1] = fnt;
+    ++nr;
+    return fnt;
+  };
+  auto store = [&]() {
+    cs.put(orc_fcorrel(n, u0.data(), u2) + orc_fcorrel(n, v0.data(), v2),
+           orc_fcorrel(n, u0.data(), v2) - orc_fcorrel(n, v0.data(), u2));
+  };
+  const bool prt = p->prtcrl != ORC_PRT_NONE;
+  if (prt) {
+    store();
+    f0 = row(p->ti);
+  } else {
+    cs.put(0.0, 0.0);  // LNZVC(1, .) is not written: a placeholder keeps the rows aligned
+    cs.n = 1;
+  }
+  double t = p->ti;
+  chpot((t + p->dt) / 2.0);
+  psod_aux(p, cst / 4.0, veff.data(), vabc, u1, u2, v1, v2, work.data());
+  chpot(t + p->dt);
+  psod_aux(p, cst / 2.0, veff.data(), vabc, u1, u2, v1, v2, work.data());
+  int mc = 1;
+  t = p->ti + p->dt;
+  if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == p->lc)) {
+    if (mc == p->lc) {
+      mc = 0;
+      store();
+    }
+    row(t);
+  }
+  for (int i = 0; i < n; ++i) {
+    u1[i] = u0[i];
+    v1[i] = v0[i];
+  }
+  t = p->ti + p->dt;
+  const long nf = std::lround((p->tf + p->dt / 2.0 - t) / p->dt);
+  for (long k = 1; k <= nf; ++k) {
+    t = t + p->dt;
+    chpot(t);
+    psod_aux(p, cst, veff.data(), vabc, u1, u2, v1, v2, work.data());
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      store();
+    }
+    if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+      const double fnt = row(t);
+      if (p->absorb == ORC_ABS_NONE && std::fabs((fnt - f0) / f0) * 100.0 > p->tol) *info = 1;
+    }
+  }
+  if (nrows) *nrows = nr;
+  return cs.n;
+}
+
 // pplnz.f:139-141  PPLNZ's propagation: DO T = TI+DT, TF+DT/2, DT with the
 // potential VP - DM EF(T) (chpot.f) in each PLNZAUX step; C(t) every LC steps
 extern "C" int orc_pplnz(const orc_prop_t* p, const double* vp, const double* vabc,

@@ -127,6 +127,14 @@ int orc_ppsod(const orc_prop_t* p, const double* vp, const double* vabc, const d
               int shape, const double* par, double* u1, double* v1, double* u2, double* v2,
               double* c_re, double* c_im, int c_cap);
 
+/* PPSOD with its table and LNZVC rules (ppsod.f:64-400; no files): rows of
+ * 7 + npr columns (T, ET, E0, Cr, Ci, |C|^2, |P_k|^2 for the npr real vectors
+ * w[k*n..], FNT); C(0) and the start-up sample are stored only when printed,
+ * as the reference does (with PRTCRL = NONE the first C slot is a placeholder) */
+int orc_ppsod_table(const orc_prop_t* p, const double* vp, const double* vabc, const double* dm,
+                    int shape, const double* par, int npr, const double* w, double* u1,
+                    double* v1, double* u2, double* v2, double* c_re, double* c_im, int c_cap,
+                    double* rows, int row_cap, int* nrows, int* info);
 /* PPLNZ's propagation (pplnz.f:139-141, no printing): PLNZ's steps with the
  * potential VP - DM EF(T) at the time each step lands at */
 int orc_pplnz(const orc_prop_t* p, const double* vp, const double* vabc, const double* dm,

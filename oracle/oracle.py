@@ -238,6 +238,30 @@ def ppsod(p, vp, dm, shape, par, u, v, vabc=None):
     return dict(c=cre[:nc] + 1j * cim[:nc], u=u2, v=v2, u_prev=u1, v_prev=v1, nc=nc)
 
 
+def ppsod_table(p, vp, dm, shape, par, w, u, v, vabc=None):
+    """PPSOD with its printed rows (T, ET, E0, Cr, Ci, |C|^2, |P_k|^2.., FNT),
+    the LNZVC C(t) rows, INFO, psi(TF) and psi(TF - dt); w: [npr, n] real."""
+    n = int(np.prod([p.np[a] for a in range(p.ndim)]))
+    w = f64(w).reshape(-1, n)
+    npr = w.shape[0]
+    u1, v1 = f64(u).copy(), f64(v).copy()
+    u2, v2 = np.zeros_like(u1), np.zeros_like(v1)
+    nsteps = do_count(p.ti + p.dt, p.tf + p.dt, p.dt) + 4
+    max_c = nsteps // max(p.lc, 1) + 4
+    cre, cim = np.zeros(max_c), np.zeros(max_c)
+    rows = np.zeros((nsteps + 4) * (7 + npr))
+    nrows, info = C.c_int(), C.c_int()
+    vabc = f64(vabc) if vabc is not None else np.zeros(n)
+    parr = f64(list(par) + [0.0] * (6 - len(par)))
+    nc = lib().orc_ppsod_table(C.byref(p), _p(f64(vp)), _p(vabc), _p(f64(dm)), int(shape),
+                               _p(parr), npr, _p(np.ascontiguousarray(w) if npr else np.zeros(1)), _p(u1), _p(v1), _p(u2),
+                               _p(v2), _p(cre), _p(cim), C.c_int(max_c), _p(rows),
+                               C.c_int(nsteps + 4), C.byref(nrows), C.byref(info))
+    nr = min(nrows.value, nsteps + 4)
+    return dict(c=cre[:nc] + 1j * cim[:nc], rows=rows[:nr * (7 + npr)].reshape(nr, 7 + npr),
+                info=info.value, u=u2, v=v2, u_prev=u1, v_prev=v1, nc=nc)
+
+
 def pplnz(p, vp, dm, shape, par, u, v, vabc=None):
     """PPLNZ's propagation: C(t) every LC steps and psi(TF)."""
     n = int(np.prod([p.np[a] for a in range(p.ndim)]))

@@ -360,6 +360,12 @@ SMOOTH = """*ABSORBING
 """
 
 
+PULSE_EXP = """*PULSE_AND_DIPOLE
+.GAUS
+ 5.0D7  0.1  2.5  0.15  0.0/
+.EXP
+ 0.5 0.3 0.0/
+"""
 VOPTIC_SMALL = """*ABSORBING
 .VOPTIC_POLIN
  -0.5  2.0  0.0/
@@ -378,6 +384,7 @@ DECK_CASES = {
     "deck_psod_voptic": (1, ".PSOD", "", VOPTIC_SMALL, ""),
     "deck_sil_smooth": (1, ".PSIL", "  10", SMOOTH_SMALL, ""),
     "deck_sil_2d": (2, ".PSIL", "  10", "", ""),
+    "deck_ppsod": (1, ".PPSOD", "", PULSE_EXP, ""),
 }
 
 
@@ -407,6 +414,8 @@ def case_deck(name):
                        dt=fmt(dt_fs), mp=mp, absorb=absorb, mf=8)
     if hwhm:
         deck = deck.replace("**SPECTRUM\n*FOURIER", "**SPECTRUM\n" + hwhm + "*FOURIER")
+    if prop == ".PPSOD":  # propagation only; the pulse block goes to **TD
+        deck = deck.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.PROPAGATION")
     with open(os.path.join(d, "input.spc"), "w") as f:
         f.write(deck)
     with open(os.path.join(d, "wf_pot.inp"), "w") as f:

@@ -6,6 +6,8 @@ results.test4).  The executable prints C(t) with F10.7, so agreement to
 5e-8 (half a unit in the last printed place) plus rounding of the printed
 time column is the sharpest pin available.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -161,3 +163,36 @@ def test_reference_test8_spectrum(oracle, quirks):
     assert np.max(np.abs(en[order] + ade - gold[:, 0])) <= 5.1e-8
     assert np.max(np.abs(su[order] - gold[:, 1])) <= 5.1e-8
     assert np.max(np.abs(sv[order] - gold[:, 3])) <= 5.1e-8
+
+
+def test_ppsod_pulse_deck(oracle):
+    """A .PPSOD deck (Gaussian pulse, .EXP dipole mu(R) = 0.5 R exp(-0.3 R),
+    tests/golden/deck_ppsod) run by the executable: the oracle's PPSOD rows --
+    time, E with and without the field, Cr, Ci, |C|^2 and the norm -- agree to
+    half a unit of every printed digit (ppsod.f FORMAT 1021)."""
+    d = os.path.join(G.GOLDEN, "deck_ppsod")
+    lines = open(os.path.join(d, "wf_pot.inp")).read().split("\n")
+    n = 256
+    x = np.array([float(l.split()[0]) for l in lines[1:1 + n]])
+    psi = np.array([float(l.split()[1]) for l in lines[1:1 + n]])
+    v = np.array([float(l.split()[1]) for l in lines[2 + n:2 + 2 * n]])
+    sh = (x[-1] - x[0]) / (n - 1)
+    shm = G.shm_of(918.0, sh)
+    dt = 0.05 * 2.4188843243e-2
+    r_ab = x[0] + np.arange(n) * sh  # dipl.f:62-66
+    dm = 0.5 * r_ab * np.exp(-0.3 * r_ab)
+    p = oracle.make_prop([n], dt, 0.0, 256 * dt, [sh], [918.0], lc=2, tol=1e3,
+                         prtcrl=oracle.PRT_PARTIAL, shm=[shm])
+    r = oracle.ppsod_table(p, v, dm, 1, (5.0e7, 0.1, 2.5, 0.15, 0.0), np.zeros((0, n)), psi,
+                           np.zeros(n))
+    text = open(os.path.join(d, "expected.txt")).read().split("\n")
+    gold = np.array([[float(t) for t in l.split()] for l in text
+                     if len(l.split()) == 7 and l.split()[0][0].isdigit()])
+    assert r["rows"].shape == gold.shape
+    half = np.array([5e-7, 0, 0, 5e-6, 5e-6, 5e-7, 5e-7]) * 1.01
+    d_ = np.abs(r["rows"] - gold)
+    assert np.all(d_[:, [0, 3, 4, 5, 6]] <= half[[0, 3, 4, 5, 6]])
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(gold[:, 1:3]))) - 5)
+    assert np.all(d_[:, 1:3] <= 0.5 * e_ulp * 1.01)
+    assert np.max(np.abs(gold[:, 1] - gold[:, 2])) > 1e-6  # the field shows in ET
+    assert r["info"] == 0
