@@ -5,12 +5,14 @@
 // Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL .FILE, *MASS,
 // *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION), *INIEIGVC .GETR,
 // *CHANGE, *SHIFT_POTENTIAL, *PRTCRL, *MASS_FACTOR, *DONOTSTOP; **TD *PROPAG
-// (.PFSPO, .PFSOD, .PSIL, .PSOD), *PRPGSTATE 0, *TPTRANS .ONE, *PRPTOL,
-// *ABSORBING; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.  Print and output-file
-// switches (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored: no files are
-// written.  Anything else -- analytic potentials, computed initial states
-// (the TI part), pulses, several states -- is refused with a message: there is
-// no CPU path.
+// (.PFSPO, .PFSOD, .PSIL, .PSOD, .PPSOD), *PRPGSTATE 0, *TPTRANS .ONE,
+// *PRPTOL, *ABSORBING, *PULSE_AND_DIPOLE (.GAUS, .GGAUS, .SIN2, .NONE with
+// the dipoles .CONST, .EXP, .NONE, .NULL), *NPROJECTIONS (no projection left
+// after rdinput.f's rule), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.
+// Print and output-file switches (*PRTPOT, *PRTEIGVC, ...) are accepted and
+// ignored: no files are written.  Anything else -- analytic potentials,
+// computed initial states (the TI part), several states, dipoles read from a
+// file -- is refused with a message: there is no CPU path.
 //
 // The run follows espec.f: the .FILE reads of RDPTE / RDPT (rdpte.f, rdpt.f:
 // eigenvector block, then potential block, optionally shifted to its
@@ -253,6 +255,11 @@ struct Run {
   double chwhm = 0.0, de = 0.0, e1i = 0.0, ade = 0.0;
   double voi[3] = {0, 0, 0}, al[3] = {0, 0, 0}, ar[3] = {0, 0, 0};
   int mf = 13, mp = 10, prpgstate = 0;
+  // *PULSE_AND_DIPOLE (rdinput.f:549-578; defaults espec.f:124-177)
+  std::string efc = ".NONE", tpdipl = ".NULL";
+  double e0 = 0.0, tp = 0.0, omg = 0.0, t0 = 0.0, td = 0.0, sni = 0.0;
+  int kl = 0, npr = 1, kp = 1;
+  std::vector<double> cstdm;
 };
 
 const std::string& rec(const std::vector<std::string>* r, size_t i, const char* key) {
@@ -340,6 +347,43 @@ Run read_run(const Deck& d) {
           r.tptrans = upper(rec(v, 0, "*TPTRANS"));
         } else if (k == "*PRPTOL") {
           r.tol = numbers(rec(v, 0, "*PRPTOL")).at(0);
+        } else if (k == "*NSHOT") {
+          continue;  // the snapshot period of the files PPSOD writes
+        } else if (k == "*NPROJECTIONS") {
+          const std::vector<double> x = numbers(rec(v, 0, "*NPROJECTIONS"));
+          if (x.size() < 2) throw DeckError{"*NPROJECTIONS: NPR KP"};
+          r.npr = (int)x[0];
+          r.kp = (int)x[1];
+        } else if (k == "*PULSE_AND_DIPOLE") {
+          r.efc = upper(rec(v, 0, "*PULSE_AND_DIPOLE"));
+          size_t i = 1;
+          const bool gaus = starts(r.efc, ".GAUS"), ggaus = starts(r.efc, ".GGAUS");
+          const bool sin2 = starts(r.efc, ".SIN2"), none = starts(r.efc, ".NONE");
+          if (!gaus && !ggaus && !sin2 && !none)
+            throw DeckError{"*PULSE_AND_DIPOLE " + r.efc + ": the pulse is not known (ef.f:44-60)"};
+          const std::vector<double> x = numbers(rec(v, i++, "*PULSE_AND_DIPOLE"));
+          if (!none) {
+            if (x.size() < (ggaus ? 6u : 5u))
+              throw DeckError{"*PULSE_AND_DIPOLE: E0 TP OMG " + std::string(sin2 ? "TD" : "T0") +
+                              " SNI" + (ggaus ? " KL" : "")};
+            r.e0 = x[0];
+            r.tp = x[1];
+            r.omg = x[2];
+            (sin2 ? r.td : r.t0) = x[3];
+            r.sni = x[4];
+            if (ggaus) r.kl = (int)x[5];
+          }
+          r.tpdipl = upper(rec(v, i++, "*PULSE_AND_DIPOLE"));
+          if (starts(r.tpdipl, ".READ") || starts(r.tpdipl, ".GET") || starts(r.tpdipl, ".EXP+"))
+            throw DeckError{"dipole " + r.tpdipl + " is not covered (.CONST, .EXP, .NONE, .NULL)"};
+          if (!starts(r.tpdipl, ".NULL")) {
+            if (!starts(r.tpdipl, ".CONST") && !starts(r.tpdipl, ".EXP") &&
+                !starts(r.tpdipl, ".NONE"))
+              throw DeckError{"desired dipole moment " + r.tpdipl + " wasn't found (dipl.f:86-89)"};
+            r.cstdm = numbers(rec(v, i++, "*PULSE_AND_DIPOLE"));
+            if (r.cstdm.size() < (starts(r.tpdipl, ".EXP") ? 2u : 1u))
+              throw DeckError{"*PULSE_AND_DIPOLE: dipole constants missing"};
+          }
         } else if (k == "*ABSORBING") {
           r.tpabsor = upper(rec(v, 0, "*ABSORBING"));
           if (starts(r.tpabsor, ".NULL")) continue;
@@ -385,8 +429,16 @@ Run read_run(const Deck& d) {
   if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD"))
     throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": only .TD is covered"};
   if (!starts(r.tppropg, ".PFSPO") && !starts(r.tppropg, ".PFSOD") &&
-      !starts(r.tppropg, ".PSIL") && !starts(r.tppropg, ".PSOD"))
-    throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD)"};
+      !starts(r.tppropg, ".PSIL") && !starts(r.tppropg, ".PSOD") && !starts(r.tppropg, ".PPSOD"))
+    throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD, "
+                    ".PPSOD)"};
+  // rdinput.f:650-660 with NIS = 1 (.GETR): the projections PPSOD prints are
+  // on LNZVC columns KP+1.. which .GETR leaves empty
+  if (r.npr + r.kp > 1) r.npr -= 1;
+  if (r.npr > 6) r.npr = 6;
+  if (starts(r.tppropg, ".PPSOD") && r.npr > 0)
+    throw DeckError{"*NPROJECTIONS: projections on computed eigenstates are not covered "
+                    "(.GETR gives one state)"};
   return r;
 }
 
@@ -491,7 +543,9 @@ int run_deck(const std::string& deck_path) {
                           : starts(r.tppropg, ".PFSOD") ? "Using SOD procedure with FFT."
                           : starts(r.tppropg, ".PSIL")  ? "Using SIL procedure."
                           : starts(r.tppropg, ".PSOD")  ? "Using SOD procedure."
-                                                        : nullptr;
+                          : starts(r.tppropg, ".PPSOD")
+                              ? "Using time dependent SOD procedure with pulse and printing facilities."
+                              : nullptr;
   if (using_msg) std::printf(" %s\n", using_msg);
   std::fflush(stdout);
   if (starts(r.tppropg, ".PFSPO")) {
@@ -514,8 +568,25 @@ int run_deck(const std::string& deck_path) {
           &r.tol, r.np, shm, u1.data(), u2.data(), v1.data(), v2.data(), &xi0, &xi0,
           fd.vpot.data(), vabc.data(), wrk.data(), &xi0, lnzvc.data(), std::strlen(dm),
           std::strlen(pr), std::strlen(ta));
+  } else if (starts(r.tppropg, ".PPSOD")) {
+    // DIPLMMT (dipl.f:61-85): R = XI(1) + (I - 1) SH(1) for every I of the grid
+    std::vector<double> dmv(n, 0.0);
+    for (int i = 0; i < n; ++i) {
+      const double rab = fd.xi[0] + i * sh[0];
+      if (starts(r.tpdipl, ".CONST")) dmv[i] = r.cstdm[0] / rab;
+      else if (starts(r.tpdipl, ".EXP")) dmv[i] = r.cstdm[0] * rab * std::exp(-r.cstdm[1] * rab);
+    }
+    const int off = 0, nshot = 10, nispg = r.prpgstate + 1;  // espec.f:240
+    const char* ef = r.efc.c_str();
+    ppsod_(&absorb, &off, &off, &off, dm, ef, pr, ta, &info, &nc, &mp, &mpi, &mpr, &mxdct, &n,
+           &nshot, &r.npr, &r.kp, &nispg, &r.e0, &r.t0, &r.td, &r.tp, &r.omg, &r.sni, &r.kl, &r.dt,
+           &r.ti, &r.tf, &r.tol, r.np, r.np, sh, shm, u1.data(), u2.data(), v1.data(), v2.data(),
+           fd.xi, fd.xi, fd.xf, dmv.data(), fd.vpot.data(), vabc.data(), wrk.data(), &xi0,
+           lnzvc.data(), &off, &off, &xi0, &off, std::strlen(dm), std::strlen(ef), std::strlen(pr),
+           std::strlen(ta));
   } else {
-    throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD)"};
+    throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD, "
+                    ".PPSOD)"};
   }
   if (info == 2) throw DeckError{"the GPU propagation failed (INFO = 2)"};
   if (info != 0) {

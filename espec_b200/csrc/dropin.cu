@@ -1,6 +1,7 @@
 // dropin.cu -- Fortran-callable drop-ins for eSPec's propagators PSPOFFT
 // (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D/2D/3D), PLNZ
-// (plnz.f:1-155; 1D/2D/3D) and PSOD (psod.f:1-208; 1D/2D/3D).
+// (plnz.f:1-155; 1D/2D/3D), PSOD (psod.f:1-208; 1D/2D/3D) and PPSOD
+// (ppsod.f:1-470; PSOD with a laser pulse; 1D/2D/3D).
 //
 // Each call propagates one packet on the GPU through a one-packet plan and
 // leaves in the caller's arrays what the reference routine leaves there:
@@ -22,6 +23,7 @@
 // is computed on the CPU.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -610,6 +612,209 @@ extern "C" void psod_(const int* absorb, const char* dim, const char* prtcrl, co
     d.fail_lib();
     return;
   }
+  std::fflush(stdout);
+}
+
+// PPSOD (ppsod.f:1-470): PSOD with the potential VP - DM EF(t) (chpot.f, ef.f)
+// in every PSODAUX call, on a grid plan of method ESPEC_PSOD with the field
+// table of espec_ppsod_field; without psod.f's restart-copy defect (PPSOD
+// copies U0 into U1 after its start-up, ppsod.f:378-381).  Its table: FORMAT
+// 1021 rows of T, ET (with the field), E0 (without), Cr, Ci, |C|^2, the
+// populations |<W_k|psi>|^2 of W_k = LNZVC(., KP+k), and the norm; C(0) and
+// the start-up sample are stored in LNZVC only inside the print test, as the
+// reference does.
+extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigvc2,
+                       const int* prtpuls, const char* dim, const char* efc, const char* prtcrl,
+                       const char* tpabsor, int* info, const int* lc, const int* mp,
+                       const int* mpi, const int* mpr, const int* mxdct, const int* n,
+                       const int* nshot, const int* npr_in, const int* kp, const int* nispg,
+                       const double* e0, const double* t0, const double* td, const double* tp,
+                       const double* omg, const double* sni, const int* kl, const double* dt,
+                       const double* ti, const double* tf, const double* tol, const int* np,
+                       const int* nd, const double* sh, const double* shm, double* u1,
+                       double* u2, double* v1, double* v2, const double* xi, const double* xp,
+                       const double* xf, const double* dm, double* vpot, const double* vabc,
+                       double* work, const double* var, double* lnzvc, const int* prtregion,
+                       const int* nreg, const double* range, const int* prtonlyreim,
+                       size_t dim_len, size_t efc_len, size_t prtcrl_len, size_t tpabsor_len) {
+  (void)mp; (void)nshot; (void)nd; (void)sh; (void)xi; (void)xp; (void)xf; (void)work;
+  (void)var; (void)prtregion; (void)nreg; (void)range; (void)prtonlyreim; (void)prtveff;
+  (void)prteigvc2; (void)prtpuls;
+  *info = 0;
+  auto fail = [&](const char* why) {
+    std::fprintf(stderr, "espec_gpu PPSOD: %s\n", why);
+    *info = 2;
+  };
+  int ndim = 0;
+  if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
+  if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
+  if (fstr_is(dim, dim_len, ".3D")) ndim = 3;
+  if (!ndim) return fail("DIM must be '.1D', '.2D' or '.3D'");
+  long npts = 1;
+  for (int a = 0; a < ndim; ++a) npts *= np[a];
+  if (npts != *n) return fail("N differs from the product of NP");
+  if (*lc < 1) return fail("LC must be at least 1");
+  if (*npr_in > 6) return fail("NPR must be at most 6 (rdinput.f:660)");
+  const int npr = std::max(*npr_in, 0);  // NPR < 1: no projections (ppsod.f:99-104)
+  int shape = -1;  // ef.f:44-60
+  if (fstr_is(efc, efc_len, ".GAUS")) shape = ESPEC_PULSE_GAUS;
+  else if (fstr_is(efc, efc_len, ".GGAUS")) shape = ESPEC_PULSE_GGAUS;
+  else if (fstr_is(efc, efc_len, ".SIN2")) shape = ESPEC_PULSE_SIN2;
+  else if (fstr_is(efc, efc_len, ".NONE") || fstr_is(efc, efc_len, ".NULL")) shape = ESPEC_PULSE_NONE;
+  if (shape < 0) return fail("desired laser pulse wasn't found (ef.f:58-60)");
+  const double par[6] = {*e0, *tp, *omg, shape == ESPEC_PULSE_SIN2 ? *td : *t0, *sni, (double)*kl};
+  int ab = ESPEC_ABS_NONE;  // sod.f:71-82
+  if (*absorb) {
+    if (fstr_is(tpabsor, tpabsor_len, ".VOPTIC")) ab = ESPEC_ABS_VOPTIC;
+    else if (fstr_is(tpabsor, tpabsor_len, ".SMOOTHW") || fstr_is(tpabsor, tpabsor_len, ".SMRS"))
+      ab = ESPEC_ABS_SMOOTHW;
+    else return fail("SOD propagation error: absorber type not '.VOPTIC', '.SMOOTHW' or '.SMRS'");
+  }
+  const int prt = fstr_is(prtcrl, prtcrl_len, ".YES") ? 2
+                  : (fstr_is(prtcrl, prtcrl_len, ".PARTIAL") ? 1 : 0);
+  const long nn = *n;
+  // the field of every PSODAUX call (ppsod.f:252-260, 378-386)
+  std::vector<double> ef((size_t)std::max(8L, (long)((*tf - *ti) / *dt) + 8));
+  const long ncalls = espec_ppsod_field(shape, par, *ti, *tf, *dt, ef.data(), (long)ef.size());
+  if (ncalls < 2) return fail(espec_last_error());
+  const int nsteps = (int)ncalls - 1;  // slot 1: the start-up; slot s >= 2: loop step s - 1
+  std::vector<double> vp(vpot, vpot + nn);
+  espec_grid_plan* plan = nullptr;
+  double* d_w = nullptr;
+  struct Guard {
+    espec_grid_plan*& p;
+    double*& w;
+    ~Guard() {
+      espec_grid_destroy(p);
+      if (w) cudaFree(w);
+    }
+  } guard{plan, d_w};
+  if (espec_grid_create(&plan, ESPEC_PSOD, ndim, np, shm, *dt, 0, ESPEC_FP64, ab, 0) ||
+      espec_grid_load(plan, vp.data(), ab == ESPEC_ABS_NONE ? nullptr : vabc, u1, v1,
+                      ESPEC_MEM_HOST, nullptr) ||
+      espec_grid_set_pulse(plan, dm, ef.data(), ncalls, ESPEC_MEM_HOST))
+    return fail(espec_last_error());
+  if (npr > 0) {  // W_k = LNZVC(:, KP+k) (ppsod.f:99-104)
+    if (cudaMalloc(&d_w, sizeof(double) * nn * npr) != cudaSuccess) return fail("device memory");
+    for (int k = 0; k < npr; ++k)
+      if (cudaMemcpy(d_w + (size_t)k * nn, lnzvc + (size_t)(*kp + k) * *mxdct, sizeof(double) * nn,
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail("copy of the projection vectors");
+  }
+  auto store = [&](long nc, double cr, double ci) {  // LNZVC(NC, MPR/MPI), NC from 1
+    lnzvc[(nc - 1) + (long)(*mpr - 1) * *mxdct] = cr;
+    lnzvc[(nc - 1) + (long)(*mpi - 1) * *mxdct] = ci;
+  };
+  // the energies, populations and norm of the state on the device
+  struct Row {
+    double et = 0, e0 = 0, fnr = 0;
+    std::vector<double> pj;
+  };
+  auto measure = [&](double efs, Row& r) -> bool {
+    double nr0;
+    r.pj.assign(2 * (size_t)std::max(npr, 1), 0.0);
+    if (espec_grid_energies_at(plan, efs, &r.et, &r.fnr, nullptr) ||
+        espec_grid_energies_at(plan, 0.0, &r.e0, &nr0, nullptr) ||
+        (npr > 0 && espec_grid_project(plan, d_w, npr, r.pj.data(), nullptr))) {
+      fail(espec_last_error());
+      return false;
+    }
+    return true;
+  };
+  double f0 = 0.0;
+  // kind 0: the first row (sets F0), 1: the start-up row, 2: a loop row (drift
+  // test, ppsod.f:440-444)
+  auto print_row = [&](double t, const Row& m, double cr, double ci, int kind) {
+    // FORMAT 1021: (1X,F14.6,3X,E12.6,3X,E12.6,2(3X,F8.5),(3X,F8.6)...)
+    std::string row = " " + fmt_f(t, 14, 6) + "   " + fmt_e(m.et, 12, 6) + "   " +
+                      fmt_e(m.e0, 12, 6) + "   " + fmt_f(cr, 8, 5) + "   " + fmt_f(ci, 8, 5) +
+                      "   " + fmt_f(cr * cr + ci * ci, 8, 6);
+    for (int k = 0; k < npr; ++k)
+      row += "   " + fmt_f(m.pj[2 * k] * m.pj[2 * k] + m.pj[2 * k + 1] * m.pj[2 * k + 1], 8, 6);
+    row += "   " + fmt_f(m.fnr, 8, 6) + "\n";
+    if (kind == 2 && ab == ESPEC_ABS_NONE && std::fabs((m.fnr - f0) / f0) * 1.0e2 > *tol) *info = 1;
+    if (kind == 0) f0 = m.fnr;
+    emit(row);
+  };
+  // which slots print and which store C (ppsod.f:262-263, 388-396)
+  std::vector<char> printed(nsteps + 1, 0), stored(nsteps + 1, 0);
+  int mc = 1;
+  if (prt == 2 || (prt == 1 && mc == *lc)) {
+    printed[1] = 1;
+    if (mc == *lc) {
+      stored[1] = 1;
+      mc = 0;
+    }
+  }
+  for (int s = 2; s <= nsteps; ++s) {
+    mc = mc + 1;
+    if (mc == *lc) {
+      mc = 0;
+      stored[s] = 1;
+    }
+    if (prt == 2 || (prt == 1 && mc == 0)) printed[s] = 1;
+  }
+  long nc = 1;
+  std::vector<double> cre, cim;
+  if (prt) {
+    // the table head (ppsod.f:172-200): the title, then FORMAT 1011 or 1012
+    std::string head = " \n";
+    head += (dim_len >= 3 && std::memcmp(dim, ".1D", 3) == 0 &&
+             std::string(dim + 3, dim_len - 3).find_first_not_of(' ') == std::string::npos)
+                ? " Auto-correlation function:\n"
+                : " Partial auto-correlation function:\n";
+    head += " ==================================\n\n";
+    head += "        *t/fs*     *ET/a.u.*      *E0/a.u.*      *Pr(t)*    *Pi(t)*   ";
+    const bool wide = *npr_in + *kp - 1 > 10;
+    auto group = [&](const char* a, int i, const char* b, bool last) {
+      char buf[32];
+      std::snprintf(buf, sizeof buf, wide ? "%2d" : "%1d", i);
+      std::string d(buf);
+      if ((int)d.size() > (wide ? 2 : 1)) d = std::string(wide ? 2 : 1, '*');
+      head += std::string(a) + d + b + (last ? "" : "   ");
+    };
+    group("*|P", *nispg - 1, "|^2*", false);
+    for (int i = 1; i <= npr; ++i) group("*|P", i - 1 + *kp, "|^2*", false);
+    group(" |c", *nispg - 1, "|^2 ", true);
+    emit(head + "\n");
+  }
+  // the first row: psi0 with the potential before any CHPOT (ET = E0,
+  // ppsod.f:158-201), printed once the run has given C(0)
+  Row first;
+  if (prt && !measure(0.0, first)) return;
+  // the run, split at the printed slots and resumed on the device
+  int done = 0;
+  for (int s = 1; s <= nsteps; ++s) {
+    if (!printed[s] && s != nsteps) continue;
+    const int k = s - done;
+    cre.resize(k + 1);
+    cim.resize(k + 1);
+    if ((done == 0 ? espec_grid_run(plan, k, nullptr) : espec_grid_continue(plan, k, nullptr)) ||
+        espec_grid_results(plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST,
+                           nullptr))
+      return fail(espec_last_error());
+    if (done == 0 && prt) {
+      store(nc, cre[0], cim[0]);
+      print_row(*ti, first, cre[0], cim[0], 0);
+    }
+    for (int j = 1; j <= k; ++j)
+      if (stored[done + j]) store(++nc, cre[j], cim[j]);
+    done = s;
+    if (printed[s]) {
+      // the time of slot s: TI + DT for the start-up, then T accumulating DT
+      double t = *ti + *dt;
+      for (int q = 2; q <= s; ++q) t = t + *dt;
+      Row m;
+      if (!measure(ef[s], m)) return;
+      print_row(t, m, cre[k], cim[k], s >= 2 ? 2 : 1);
+    }
+  }
+  if (done == 0) return fail("no steps");
+  // psi(TF), psi(TF - dt), and VPOT as CHPOT leaves it
+  if (espec_grid_results(plan, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
+      espec_grid_previous(plan, u1, v1, ESPEC_MEM_HOST, nullptr))
+    return fail(espec_last_error());
+  for (long i = 0; i < nn; ++i) vpot[i] = vp[i] - dm[i] * ef[nsteps];
   std::fflush(stdout);
 }
 

@@ -586,6 +586,38 @@ __global__ void sum_parts_kernel(const double* part, int nb, double* out) {
   }
 }
 
+// <w_j|u> and <w_j|v> for nvec real vectors w_j (FCORREL of ppsod.f:268-300):
+// CTA (x, j) sums a strided slice of the grid for vector j; the per-CTA
+// partials are summed in CTA order by project_sum_kernel
+constexpr int kProjBlocks = 128;
+constexpr int kProjMaxVec = 8;
+
+__global__ void __launch_bounds__(kSilThreads) project_kernel(const double* w, const double* u,
+                                                              const double* v, long n,
+                                                              double* part) {
+  __shared__ double sp[2], scratch[(kSilThreads / 32) * 8];
+  const double* wj = w + (size_t)blockIdx.y * n;
+  double q[2] = {0.0, 0.0};
+  for (long k = (long)blockIdx.x * kSilThreads + threadIdx.x; k < n;
+       k += (long)gridDim.x * kSilThreads) {
+    const double wk = wj[k];
+    q[0] += wk * u[k];
+    q[1] += wk * v[k];
+  }
+  block_sum<2>(q, sp, scratch);
+  if (threadIdx.x < 2) part[((size_t)blockIdx.y * gridDim.x + blockIdx.x) * 2 + threadIdx.x] = sp[threadIdx.x];
+}
+
+__global__ void project_sum_kernel(const double* part, int nb, int nvec, double* out) {
+  const int t = threadIdx.x;  // 2 per vector
+  if (t < 2 * nvec) {
+    const int j = t >> 1, c = t & 1;
+    double s = 0.0;
+    for (int i = 0; i < nb; ++i) s += part[((size_t)j * nb + i) * 2 + c];
+    out[t] = s;
+  }
+}
+
 }  // namespace espec
 
 // ---------------------------------------------------------------------------
@@ -607,6 +639,7 @@ struct espec_grid_plan {
   double *d_dm = nullptr, *d_ef = nullptr;  // PSOD with a pulse: dipole, field per call
   long n_ef = 0, slot = 0;                  // field entries; steps of the current run
   double *d_part = nullptr, *d_tot = nullptr, *d_epart = nullptr, *d_eout = nullptr;
+  double* d_ppart = nullptr;  // projections: per-CTA partials, then the sums
   unsigned* d_bar = nullptr;
   int* d_err = nullptr;
   double2* d_c = nullptr;
@@ -616,7 +649,7 @@ struct espec_grid_plan {
 static void grid_free(espec_grid_plan* p) {
   void* b[] = {p->d_vpot, p->d_mask, p->d_u, p->d_v, p->d_u0, p->d_v0, p->d_L, p->d_work,
                p->d_wbuf, p->d_part, p->d_tot, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c,
-               p->d_up, p->d_vp, p->d_dm, p->d_ef};
+               p->d_up, p->d_vp, p->d_dm, p->d_ef, p->d_ppart};
   for (void* x : b)
     if (x) cudaFree(x);
 }
@@ -913,6 +946,27 @@ extern "C" int espec_grid_set_pulse(espec_grid_plan* p, const double* dm, const 
   GRID_CK(cudaMemcpy(p->d_dm, dm, (size_t)p->n * 8, kind));
   GRID_CK(cudaMemcpy(p->d_ef, ef, (size_t)ncalls * 8, kind));
   p->n_ef = ncalls;
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_project(espec_grid_plan* p, const double* w, int nvec, double* out,
+                                  void* stream) {
+  if (!p || !w || !out) return set_error(ESPEC_EINVAL, "null argument");
+  if (nvec < 1 || nvec > kProjMaxVec) return set_error(ESPEC_EINVAL, "1..8 projection vectors");
+  if (!p->loaded) return set_error(ESPEC_EINVAL, "espec_grid_load has not been called");
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t nsum = (size_t)kProjMaxVec * kProjBlocks * 2;
+  if (!p->d_ppart) GRID_CK(cudaMalloc(&p->d_ppart, sizeof(double) * (nsum + 2 * kProjMaxVec)));
+  long nb = (p->n + kSilThreads - 1) / kSilThreads;
+  if (nb > kProjBlocks) nb = kProjBlocks;
+  project_kernel<<<dim3((unsigned)nb, (unsigned)nvec), kSilThreads, 0, st>>>(w, p->d_u, p->d_v, p->n,
+                                                                             p->d_ppart);
+  GRID_CK(cudaGetLastError());
+  project_sum_kernel<<<1, 2 * kProjMaxVec, 0, st>>>(p->d_ppart, (int)nb, nvec, p->d_ppart + nsum);
+  GRID_CK(cudaGetLastError());
+  GRID_CK(cudaMemcpyAsync(out, p->d_ppart + nsum, sizeof(double) * 2 * nvec,
+                          cudaMemcpyDeviceToHost, st));
+  GRID_CK(cudaStreamSynchronize(st));
   return ESPEC_OK;
 }
 

@@ -130,6 +130,42 @@ def psod(*, absorb, dim, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, tf, to
     return info.value
 
 
+def ppsod(*, absorb, dim, efc, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, np_,
+          shm, e0, tp, omg, dm, vpot, vabc, u1, v1, u2, v2, lnzvc, t0=0.0, td=0.0, sni=0.0, kl=0,
+          npr=0, kp=1, nispg=1):
+    """PPSOD: PSOD with the laser pulse efc ('.GAUS', '.GGAUS', '.SIN2',
+    '.NONE') and the dipole function dm; the projection vectors are the
+    columns kp..kp+npr-1 (0-based) of lnzvc.  On return U2 + i V2 is psi(TF),
+    U1 + i V1 is psi(TF - dt) and vpot holds VP - DM EF of the last step.
+    Returns INFO."""
+    info = C.c_int(0)
+    npa = np.array(list(np_) + [1] * (3 - len(np_)), dtype=np.int32)
+    shma = N.f64(list(shm) + [0.0] * (3 - len(shm)))
+    dma = N.f64(dm)
+    va = N.f64(vabc) if vabc is not None else np.zeros(n)
+    ints = {k: C.c_int(v) for k, v in dict(
+        absorb=1 if absorb else 0, off=0, lc=lc, mp=0, mpi=mpi, mpr=mpr, mxdct=mxdct, n=n,
+        nshot=10, npr=npr, kp=kp, nispg=nispg, kl=kl).items()}
+    dbl = {k: C.c_double(v) for k, v in dict(
+        e0=e0, t0=t0, td=td, tp=tp, omg=omg, sni=sni, dt=dt, ti=ti, tf=tf, tol=tol).items()}
+    z3 = np.zeros(3)
+    scratch = np.zeros(max(n, 1))
+    rng = np.zeros(36)
+    b = {k: v.encode() for k, v in dict(dim=dim, efc=efc, prtcrl=prtcrl, tpabsor=tpabsor).items()}
+    r = C.byref
+    N.load().ppsod_(
+        r(ints["absorb"]), r(ints["off"]), r(ints["off"]), r(ints["off"]), b["dim"], b["efc"],
+        b["prtcrl"], b["tpabsor"], r(info), r(ints["lc"]), r(ints["mp"]), r(ints["mpi"]),
+        r(ints["mpr"]), r(ints["mxdct"]), r(ints["n"]), r(ints["nshot"]), r(ints["npr"]),
+        r(ints["kp"]), r(ints["nispg"]), r(dbl["e0"]), r(dbl["t0"]), r(dbl["td"]), r(dbl["tp"]),
+        r(dbl["omg"]), r(dbl["sni"]), r(ints["kl"]), r(dbl["dt"]), r(dbl["ti"]), r(dbl["tf"]),
+        r(dbl["tol"]), N.ptr(npa), N.ptr(npa), N.ptr(z3), N.ptr(shma), _arr(u1), _arr(u2),
+        _arr(v1), _arr(v2), N.ptr(z3), N.ptr(z3), N.ptr(z3), N.ptr(dma), _arr(vpot), N.ptr(va),
+        N.ptr(scratch), N.ptr(z3), _arr(lnzvc), r(ints["off"]), r(ints["off"]), N.ptr(rng),
+        r(ints["off"]), len(b["dim"]), len(b["efc"]), len(b["prtcrl"]), len(b["tpabsor"]))
+    return info.value
+
+
 def format_crl_row(t, e, cr, ci, ct, fnt):
     """One row of the partial auto-correlation table (FORMAT 1021, pspofft.f:148)."""
     buf = C.create_string_buffer(256)

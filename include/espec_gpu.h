@@ -118,6 +118,26 @@ void psod_(const int* absorb, const char* dim, const char* prtcrl,
            const double* xf, const double* vpot, const double* vabc,
            double* work, const double* var, double* lnzvc, size_t dim_len,
            size_t prtcrl_len, size_t tpabsor_len);
+/* replaces SUBROUTINE PPSOD (ppsod.f:1-5; called from espec.f:1398): PSOD with
+ * the laser pulse EFC (.GAUS, .GGAUS, .SIN2, .NONE; E0, TP, OMG, T0 / TD, SNI,
+ * KL as ef.f) and dipole DM, 1D/2D/3D; prints the table of ppsod.f (E with and
+ * without the field, C(t), the populations of LNZVC(., KP+1..KP+NPR), the
+ * norm); C(t) in LNZVC(., MPR/MPI); psi(TF) in U2/V2, psi(TF - dt) in U1/V1;
+ * VPOT left holding VP - DM EF of the last step.  The movie, potential and
+ * pulse files of PRTVEFF, PRTEIGVC2, PRTPULS are not written. */
+void ppsod_(const int* absorb, const int* prtveff, const int* prteigvc2, const int* prtpuls,
+            const char* dim, const char* efc, const char* prtcrl, const char* tpabsor,
+            int* info, const int* lc, const int* mp, const int* mpi, const int* mpr,
+            const int* mxdct, const int* n, const int* nshot, const int* npr, const int* kp,
+            const int* nispg, const double* e0, const double* t0, const double* td,
+            const double* tp, const double* omg, const double* sni, const int* kl,
+            const double* dt, const double* ti, const double* tf, const double* tol,
+            const int* np, const int* nd, const double* sh, const double* shm, double* u1,
+            double* u2, double* v1, double* v2, const double* xi, const double* xp,
+            const double* xf, const double* dm, double* vpot, const double* vabc, double* work,
+            const double* var, double* lnzvc, const int* prtregion, const int* nreg,
+            const double* range, const int* prtonlyreim, size_t dim_len, size_t efc_len,
+            size_t prtcrl_len, size_t tpabsor_len);
 /* replace SUBROUTINE HWHM (hwhm.f:1-80; TAL is scaled in place) and
  * SUBROUTINE SPECTRUMTD (spectrumtd.f:1-116; prints the spectrum table,
  * sets DE < 0 to 0), called at espec.f:1618-1624: the arithmetic runs on the
@@ -291,6 +311,11 @@ int espec_grid_energies_at(espec_grid_plan* plan, double ef, double* e, double* 
  * step j uses V - dm * ef[j] (espec_pplnz_field).  Copies both tables. */
 int espec_grid_set_pulse(espec_grid_plan* plan, const double* dm, const double* ef, long ncalls,
                          int where);
+/* <w_j|u> and <w_j|v> of the current state u + i v for nvec <= 8 real
+ * device vectors w (column j at w + j N): out[2j], out[2j+1] on the host
+ * (the populations of ppsod.f:268-300; synchronises) */
+int espec_grid_project(espec_grid_plan* plan, const double* w, int nvec, double* out,
+                       void* stream);
 /* ESPEC_PSOD plans: psi(TF - dt) of the last run (synchronises) */
 int espec_grid_previous(espec_grid_plan* plan, double* psi_re, double* psi_im, int where,
                         void* stream);

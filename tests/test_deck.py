@@ -25,16 +25,32 @@ def refused(tmp_path, text, files=None):
 @pytest.mark.parametrize("old,new,why", [
     (".FILE\nwf_pot.inp", ".MORSE\n1.1 1943.8 13.7 1.0/\n1.2 1629.2 17.7 1.0/", ".FILE"),
     (".GETR", ".CALC", ".GETR"),
-    (".PFSPO", ".PPSOD", "propagator"),
+    (".PFSPO", ".P2PABM", "propagator"),
     (".1D\n 256/", ".2DC\n 16 16/", "*DIMENSION"),
     ("*TPTRANS\n.ONE", "*TPTRANS\n.ALL", "one propagated state"),
     ("**TD", "**TI\n*TPDIAG\n.LANCZS\n**TD", "section **TI"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n*PRPTOL", "*PULSE_AND_DIPOLE"),
+    ("*PRPTOL", "*PULSE_AND_DIPOLE\n.LASER\n 1 2 3 4 5/\n.NULL\n*PRPTOL", "pulse is not known"),
+    ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.READ\ndm.inp\n*PRPTOL", "dipole .READ"),
+    ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.EXP\n 0.5/\n*PRPTOL", "constants"),
 ])
 def test_uncovered_decks_are_refused(tmp_path, old, new, why):
     assert old in BASE
     msg = refused(tmp_path, BASE.replace(old, new))
     assert why in msg, msg
+
+
+def test_ppsod_projections(tmp_path):
+    """rdinput.f:659-660 with one state from .GETR: NPR + KP > 1 lowers NPR
+    by one; what is left of NPR would project on states the deck does not
+    have."""
+    text = BASE.replace(".PFSPO", ".PPSOD")
+    msg = refused(tmp_path, text.replace("*PRPTOL", "*NPROJECTIONS\n 3 1/\n*PRPTOL"))
+    assert "*NPROJECTIONS" in msg, msg
+    # NPR = 1, KP = 1 leaves none: the deck passes the reading and stops at
+    # its (absent) .FILE
+    msg = refused(tmp_path, text.replace("*PRPTOL", "*NPROJECTIONS\n 1 1/\n*PRPTOL"))
+    assert "cannot be opened" in msg, msg
 
 
 def test_missing_and_short_files(tmp_path):

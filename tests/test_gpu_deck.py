@@ -22,7 +22,7 @@ import golden_cases as G
 
 pytestmark = pytest.mark.gpu
 
-DECKS = ["deck_spo_hwhm", "deck_psod_voptic", "deck_sil_smooth", "deck_sil_2d"]
+DECKS = ["deck_spo_hwhm", "deck_psod_voptic", "deck_sil_smooth", "deck_sil_2d", "deck_ppsod"]
 NUM = re.compile(r"^-?(\d+\.?\d*|\.\d+)([EeDd][-+]?\d+)?$")
 
 
