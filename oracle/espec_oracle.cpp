@@ -1375,6 +1375,85 @@ extern "C" int orc_pplnz(const orc_prop_t* p, const double* vp, const double* va
   return cs.n;
 }
 
+// pplnz.f:76-320 PPLNZ with its table: rows of 6 + npr values (T, ET, E0, CR,
+// CI, CT(1..NPR), FNT) as FORMAT 1021 prints them -- CT(1) = |C|^2 and CT(k+1)
+// = |<W_k|psi>|^2 for k < NPR (pplnz.f:110-142: the last W read is not
+// printed), ET with the potential of the last CHPOT, E0 with VP, FNT the norm
+// except on the first row, where it is the norm squared (pplnz.f:146-147);
+// C(t) in LNZVC: C(0) inside the print test only, then every LC steps;
+// INFO = 1 when a printed row's FNT drifts from the first row's (no absorber,
+// pplnz.f:270-274); w: the npr - 1 printed projection vectors
+extern "C" int orc_pplnz_table(const orc_prop_t* p, const double* vp, const double* vabc,
+                               const double* dm, int shape, const double* par, int npr,
+                               const double* w, double* u, double* v, double* c_re,
+                               double* c_im, int c_cap, double* rows, int row_cap, int* nrows,
+                               int* info) {
+  const int n = npts(p);
+  CSink cs{c_re, c_im, c_cap};
+  const int ncol = 6 + (npr > 0 ? npr : 0);
+  int nr = 0;
+  *info = 0;
+  const double cst = p->dt / ORC_SHFS;
+  int mp = p->mp;
+  if (p->change && mp > p->lmtreort) mp = p->lmtreort;
+  if (p->absorb == ORC_ABS_VOPTIC) return -1;
+  std::vector<double> u0(u, u + n), v0(v, v + n), veff(vp, vp + n);
+  double f0 = 0.0;
+  auto row = [&](double t, bool first) {
+    const double cr = orc_fcorrel(n, u0.data(), u) + orc_fcorrel(n, v0.data(), v);
+    const double ci = orc_fcorrel(n, u0.data(), v) - orc_fcorrel(n, v0.data(), u);
+    const double fnr = orc_fcorrel(n, u, u) + orc_fcorrel(n, v, v);
+    const double fnt = first ? fnr * fnr : fnr;
+    if (rows && nr < row_cap) {
+      double* r = rows + (size_t)ncol * nr;
+      r[0] = t;
+      r[1] = orc_eigenerg(p->ndim, p->np, p->shm, veff.data(), u) +
+             orc_eigenerg(p->ndim, p->np, p->shm, veff.data(), v);
+      r[2] = orc_eigenerg(p->ndim, p->np, p->shm, vp, u) + orc_eigenerg(p->ndim, p->np, p->shm, vp, v);
+      r[3] = cr;
+      r[4] = ci;
+      if (npr >= 1) r[5] = cr * cr + ci * ci;
+      for (int k = 1; k < npr; ++k) {
+        const double pr = orc_fcorrel(n, w + (size_t)n * (k - 1), u);
+        const double pi = orc_fcorrel(n, w + (size_t)n * (k - 1), v);
+        r[5 + k] = pr * pr + pi * pi;
+      }
+      r[ncol - 1] = fnt;
+    }
+    ++nr;
+    return fnt;
+  };
+  auto store = [&]() {
+    cs.put(orc_fcorrel(n, u0.data(), u) + orc_fcorrel(n, v0.data(), v),
+           orc_fcorrel(n, u0.data(), v) - orc_fcorrel(n, v0.data(), u));
+  };
+  if (p->prtcrl != ORC_PRT_NONE) {
+    store();
+    f0 = row(p->ti, true);
+  } else {
+    cs.put(0.0, 0.0);  // LNZVC(1, .) is not written: a placeholder keeps the rows aligned
+    cs.n = 1;
+  }
+  int mc = 0;
+  const int nit = orc_do_count(p->ti + p->dt, p->tf + p->dt / 2.0, p->dt);
+  double t = p->ti + p->dt;
+  for (int it = 0; it < nit; ++it, t = t + p->dt) {
+    const double e = orc_ef(shape, par, t);
+    for (int i = 0; i < n; ++i) veff[i] = vp[i] - dm[i] * e;
+    if (sil_step(p, mp, veff.data(), vabc, cst, u, v)) return -1;
+    mc = mc + 1;
+    if (mc == p->lc) {
+      mc = 0;
+      store();
+    }
+    if (p->prtcrl == ORC_PRT_YES || (p->prtcrl == ORC_PRT_PARTIAL && mc == 0)) {
+      const double fnt = row(t, false);
+      if (p->absorb == ORC_ABS_NONE && std::fabs((fnt - f0) / f0) * 100.0 > p->tol) *info = 1;
+    }
+  }
+  if (nrows) *nrows = nr;
+  return cs.n;
+}
 
 // ---------------------------------------------------------------------------
 // Spectrum stage

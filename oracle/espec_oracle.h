@@ -140,6 +140,12 @@ int orc_ppsod_table(const orc_prop_t* p, const double* vp, const double* vabc, c
 int orc_pplnz(const orc_prop_t* p, const double* vp, const double* vabc, const double* dm,
               int shape, const double* par, double* u, double* v, double* c_re, double* c_im,
               int c_cap);
+/* PPLNZ with its table (pplnz.f:76-320): rows of 6 + npr values, LNZVC's
+ * C(t) rows and INFO; w holds the npr - 1 printed projection vectors */
+int orc_pplnz_table(const orc_prop_t* p, const double* vp, const double* vabc, const double* dm,
+                    int shape, const double* par, int npr, const double* w, double* u, double* v,
+                    double* c_re, double* c_im, int c_cap, double* rows, int row_cap, int* nrows,
+                    int* info);
 
 /* symmetric tridiagonal eigensolver: d[n] diag, e[n-1] offdiag, z[n*n]
  * column-major eigenvectors, eigenvalues ascending in w.  0 on success. */

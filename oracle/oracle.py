@@ -278,6 +278,32 @@ def pplnz(p, vp, dm, shape, par, u, v, vabc=None):
     return dict(c=cre[:nc] + 1j * cim[:nc], u=u, v=v, nc=nc)
 
 
+def pplnz_table(p, vp, dm, shape, par, npr, w, u, v, vabc=None):
+    """PPLNZ with its printed rows (T, ET, E0, Cr, Ci, CT(1..npr), FNT), the
+    LNZVC C(t) rows, INFO and psi(TF); w: [npr - 1, n] real (the printed
+    projections)."""
+    n = int(np.prod([p.np[a] for a in range(p.ndim)]))
+    w = f64(w).reshape(-1, n) if npr > 1 else np.zeros((1, n))
+    u, v = f64(u).copy(), f64(v).copy()
+    nsteps = do_count(p.ti + p.dt, p.tf + p.dt / 2.0, p.dt) + 4
+    max_c = nsteps // max(p.lc, 1) + 4
+    cre, cim = np.zeros(max_c), np.zeros(max_c)
+    ncol = 6 + max(npr, 0)
+    rows = np.zeros((nsteps + 4) * ncol)
+    nrows, info = C.c_int(), C.c_int()
+    vabc = f64(vabc) if vabc is not None else np.zeros(n)
+    parr = f64(list(par) + [0.0] * (6 - len(par)))
+    nc = lib().orc_pplnz_table(C.byref(p), _p(f64(vp)), _p(vabc), _p(f64(dm)), int(shape),
+                               _p(parr), int(npr), _p(np.ascontiguousarray(w)), _p(u), _p(v),
+                               _p(cre), _p(cim), C.c_int(max_c), _p(rows), C.c_int(nsteps + 4),
+                               C.byref(nrows), C.byref(info))
+    if nc < 0:
+        raise RuntimeError("oracle propagation stopped (reference STOP condition)")
+    nr = min(nrows.value, nsteps + 4)
+    return dict(c=cre[:nc] + 1j * cim[:nc], rows=rows[:nr * ncol].reshape(nr, ncol),
+                info=info.value, u=u, v=v, nc=nc)
+
+
 def plnz(p, vpot, u, v, vabc=None):
     u, v = f64(u).copy(), f64(v).copy()
     r = _run(lib().orc_plnz, p, vpot, vabc, [u, v], *_caps(p))

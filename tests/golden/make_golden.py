@@ -25,7 +25,7 @@ Cases:
               manifest.
   deck_*      whole decks for the deck driver (input.spc, wf_pot.inp and the
               executable's output from the propagation on); --decks-only
-              generates only these.
+              [name ...] generates only these (or the named ones).
 """
 import json
 import os
@@ -385,6 +385,12 @@ DECK_CASES = {
     "deck_sil_smooth": (1, ".PSIL", "  10", SMOOTH_SMALL, ""),
     "deck_sil_2d": (2, ".PSIL", "  10", "", ""),
     "deck_ppsod": (1, ".PPSOD", "", PULSE_EXP, ""),
+    # NPR = 2, KP = 0 becomes NPR = 1 (rdinput.f:659): |<W1|psi>|^2 with W1 the
+    # deck's own eigenvector, LNZVC(., KP+1) = EIGVC(., 1)
+    "deck_ppsod_proj": (1, ".PPSOD", "", PULSE_EXP + "*NPROJECTIONS\n 2 0/\n", ""),
+    "deck_ppsil": (1, ".PPSIL", "  10", PULSE_EXP, ""),
+    # NPR = 3, KP = 0 becomes NPR = 2: PPLNZ prints |C|^2 and |<W1|psi>|^2
+    "deck_ppsil_proj": (1, ".PPSIL", "  10", PULSE_EXP + "*NPROJECTIONS\n 3 0/\n", ""),
 }
 
 
@@ -414,7 +420,7 @@ def case_deck(name):
                        dt=fmt(dt_fs), mp=mp, absorb=absorb, mf=8)
     if hwhm:
         deck = deck.replace("**SPECTRUM\n*FOURIER", "**SPECTRUM\n" + hwhm + "*FOURIER")
-    if prop == ".PPSOD":  # propagation only; the pulse block goes to **TD
+    if prop in (".PPSOD", ".PPSIL"):  # propagation only; the pulse block goes to **TD
         deck = deck.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.PROPAGATION")
     with open(os.path.join(d, "input.spc"), "w") as f:
         f.write(deck)
@@ -449,7 +455,8 @@ def main():
     if not os.path.exists(BIN):
         sys.exit("eSPec executable not found at " + BIN)
     if "--decks-only" in sys.argv:
-        for name in DECK_CASES:
+        names = [a for a in sys.argv[1:] if a in DECK_CASES] or list(DECK_CASES)
+        for name in names:
             case_deck(name)
         return
     if "--psod-only" in sys.argv:
