@@ -36,7 +36,7 @@ EXPORTS = [
     "espec_grid_create", "espec_grid_load", "espec_grid_run", "espec_grid_continue",
     "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
     "espec_grid_basis", "espec_grid_previous", "espec_grid_energies_at",
-    "espec_grid_set_pulse", "espec_pulse_field", "espec_ppsod_field", "espec_pplnz_field", "plnz_", "psod_", "ppsod_", "espec_grid_project", "espec_run_deck", "espec_run_scan", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
+    "espec_grid_set_pulse", "espec_pulse_field", "espec_ppsod_field", "espec_pplnz_field", "plnz_", "psod_", "ppsod_", "pplnz_", "espec_grid_project", "espec_run_deck", "espec_run_scan", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
     "spectrumtd_", "espec_eig_solve_dev", "espec_eig_lcg_start", "espec_eig_morse2d",
     "espec_gemm_f64", "espec_gemm_f32", "espec_gemm_bf16", "espec_gemm_bf16_status",
     "espec_mlp_bias_gelu", "espec_mlp_gelu_back", "espec_to_bf16", "espec_mlp_adam_bf16",
@@ -118,6 +118,8 @@ def load():
     lib.psod_.restype = None
     lib.ppsod_.argtypes = [vp] * 51 + [C.c_size_t] * 4
     lib.ppsod_.restype = None
+    lib.pplnz_.argtypes = [vp] * 51 + [C.c_size_t] * 4
+    lib.pplnz_.restype = None
     lib.espec_grid_project.argtypes = [vp, vp, C.c_int, vp, vp]
     lib.espec_run_deck.argtypes = [C.c_char_p]
     lib.espec_run_scan.argtypes = [C.c_char_p, C.c_int, C.POINTER(C.c_char_p), C.c_char_p]

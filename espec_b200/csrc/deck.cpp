@@ -5,10 +5,10 @@
 // Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL .FILE, *MASS,
 // *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION), *INIEIGVC .GETR,
 // *CHANGE, *SHIFT_POTENTIAL, *PRTCRL, *MASS_FACTOR, *DONOTSTOP; **TD *PROPAG
-// (.PFSPO, .PFSOD, .PSIL, .PSOD, .PPSOD), *PRPGSTATE 0, *TPTRANS .ONE,
+// (.PFSPO, .PFSOD, .PSIL, .PSOD, .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE 0, *TPTRANS .ONE,
 // *PRPTOL, *ABSORBING, *PULSE_AND_DIPOLE (.GAUS, .GGAUS, .SIN2, .NONE with
-// the dipoles .CONST, .EXP, .NONE, .NULL), *NPROJECTIONS (no projection left
-// after rdinput.f's rule), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.
+// the dipoles .CONST, .EXP, .NONE, .NULL), *NPROJECTIONS (projections on
+// LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.
 // Print and output-file switches (*PRTPOT, *PRTEIGVC, ...) are accepted and
 // ignored: no files are written.  Anything else -- analytic potentials,
 // computed initial states (the TI part), several states, dipoles read from a
@@ -335,7 +335,8 @@ Run read_run(const Deck& d) {
         if (k == "*PROPAG") {
           r.tppropg = upper(rec(v, 0, "*PROPAG"));
           const std::vector<double> x = numbers(rec(v, 1, "*PROPAG"));
-          const bool sil = starts(r.tppropg, ".PSIL");
+          const bool sil = starts(r.tppropg, ".PSIL") || starts(r.tppropg, ".PPSIL") ||
+                           starts(r.tppropg, ".PPLNZ");  // rdinput.f:439-444
           if (x.size() < (sil ? 4u : 3u)) throw DeckError{"*PROPAG: TI TF DT" + std::string(sil ? " MP" : "")};
           r.ti = x[0];
           r.tf = x[1];
@@ -429,16 +430,22 @@ Run read_run(const Deck& d) {
   if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD"))
     throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": only .TD is covered"};
   if (!starts(r.tppropg, ".PFSPO") && !starts(r.tppropg, ".PFSOD") &&
-      !starts(r.tppropg, ".PSIL") && !starts(r.tppropg, ".PSOD") && !starts(r.tppropg, ".PPSOD"))
+      !starts(r.tppropg, ".PSIL") && !starts(r.tppropg, ".PSOD") && !starts(r.tppropg, ".PPSOD") &&
+      !starts(r.tppropg, ".PPSIL") && !starts(r.tppropg, ".PPLNZ"))
     throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD, "
-                    ".PPSOD)"};
-  // rdinput.f:650-660 with NIS = 1 (.GETR): the projections PPSOD prints are
-  // on LNZVC columns KP+1.. which .GETR leaves empty
+                    ".PPSOD, .PPSIL, .PPLNZ)"};
+  // rdinput.f:650-660 with NIS = 1 (.GETR).  The populations PPSOD prints are
+  // on LNZVC(., KP+1..KP+NPR), PPLNZ's on LNZVC(., KP+1..KP+NPR-1): the deck's
+  // eigenvector matrix, of which the executable holds column 1 at zero at the
+  // call; columns past it would be computed eigenstates (the TI branch)
   if (r.npr + r.kp > 1) r.npr -= 1;
   if (r.npr > 6) r.npr = 6;
-  if (starts(r.tppropg, ".PPSOD") && r.npr > 0)
+  const int printed_w = starts(r.tppropg, ".PPSOD") ? r.npr
+                        : (starts(r.tppropg, ".PPSIL") || starts(r.tppropg, ".PPLNZ")) ? r.npr - 1
+                                                                                        : 0;
+  if (printed_w > 0 && (r.kp != 0 || printed_w > 1))
     throw DeckError{"*NPROJECTIONS: projections on computed eigenstates are not covered "
-                    "(.GETR gives one state)"};
+                    "(.GETR gives one state; KP = 0 with one printed projection is)"};
   return r;
 }
 
@@ -545,6 +552,8 @@ int run_deck(const std::string& deck_path) {
                           : starts(r.tppropg, ".PSOD")  ? "Using SOD procedure."
                           : starts(r.tppropg, ".PPSOD")
                               ? "Using time dependent SOD procedure with pulse and printing facilities."
+                          : starts(r.tppropg, ".PPSIL") || starts(r.tppropg, ".PPLNZ")
+                              ? "Using time dependent SIL procedure with pulse and printing facilities."
                               : nullptr;
   if (using_msg) std::printf(" %s\n", using_msg);
   std::fflush(stdout);
@@ -568,7 +577,8 @@ int run_deck(const std::string& deck_path) {
           &r.tol, r.np, shm, u1.data(), u2.data(), v1.data(), v2.data(), &xi0, &xi0,
           fd.vpot.data(), vabc.data(), wrk.data(), &xi0, lnzvc.data(), std::strlen(dm),
           std::strlen(pr), std::strlen(ta));
-  } else if (starts(r.tppropg, ".PPSOD")) {
+  } else if (starts(r.tppropg, ".PPSOD") || starts(r.tppropg, ".PPSIL") ||
+             starts(r.tppropg, ".PPLNZ")) {
     // DIPLMMT (dipl.f:61-85): R = XI(1) + (I - 1) SH(1) for every I of the grid
     std::vector<double> dmv(n, 0.0);
     for (int i = 0; i < n; ++i) {
@@ -578,15 +588,24 @@ int run_deck(const std::string& deck_path) {
     }
     const int off = 0, nshot = 10, nispg = r.prpgstate + 1;  // espec.f:240
     const char* ef = r.efc.c_str();
-    ppsod_(&absorb, &off, &off, &off, dm, ef, pr, ta, &info, &nc, &mp, &mpi, &mpr, &mxdct, &n,
-           &nshot, &r.npr, &r.kp, &nispg, &r.e0, &r.t0, &r.td, &r.tp, &r.omg, &r.sni, &r.kl, &r.dt,
-           &r.ti, &r.tf, &r.tol, r.np, r.np, sh, shm, u1.data(), u2.data(), v1.data(), v2.data(),
-           fd.xi, fd.xi, fd.xf, dmv.data(), fd.vpot.data(), vabc.data(), wrk.data(), &xi0,
-           lnzvc.data(), &off, &off, &xi0, &off, std::strlen(dm), std::strlen(ef), std::strlen(pr),
-           std::strlen(ta));
+    if (!starts(r.tppropg, ".PPSOD")) {  // espec.f:1513-1518
+      pplnz_(&absorb, &change, &off, &off, &off, dm, ef, pr, ta, &info, &nc, &lmt, &mp, &mpi,
+             &mpr, &mxdct, &n, &nshot, &r.kl, &r.npr, &r.kp, &abstol, &r.dt, &r.ti, &r.tf, &r.tol,
+             &r.e0, &r.t0, &r.td, &r.tp, &r.omg, &r.sni, r.np, r.np, iwork.data(), sh, shm,
+             fd.vpot.data(), vabc.data(), u1.data(), v1.data(), fd.xi, fd.xf, fd.xi, dmv.data(),
+             wrk.data(), wrk.data(), wrk.data(), wrk.data(), &xi0, lnzvc.data(), std::strlen(dm),
+             std::strlen(ef), std::strlen(pr), std::strlen(ta));
+    } else {
+      ppsod_(&absorb, &off, &off, &off, dm, ef, pr, ta, &info, &nc, &mp, &mpi, &mpr, &mxdct, &n,
+             &nshot, &r.npr, &r.kp, &nispg, &r.e0, &r.t0, &r.td, &r.tp, &r.omg, &r.sni, &r.kl,
+             &r.dt, &r.ti, &r.tf, &r.tol, r.np, r.np, sh, shm, u1.data(), u2.data(), v1.data(),
+             v2.data(), fd.xi, fd.xi, fd.xf, dmv.data(), fd.vpot.data(), vabc.data(), wrk.data(),
+             &xi0, lnzvc.data(), &off, &off, &xi0, &off, std::strlen(dm), std::strlen(ef),
+             std::strlen(pr), std::strlen(ta));
+    }
   } else {
     throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD, "
-                    ".PPSOD)"};
+                    ".PPSOD, .PPSIL, .PPLNZ)"};
   }
   if (info == 2) throw DeckError{"the GPU propagation failed (INFO = 2)"};
   if (info != 0) {

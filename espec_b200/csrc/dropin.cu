@@ -1,7 +1,8 @@
 // dropin.cu -- Fortran-callable drop-ins for eSPec's propagators PSPOFFT
 // (pspofft.f:1-150; 1D/2D/3D), PSODFFT (psodfft.f:1-211; 1D/2D/3D), PLNZ
-// (plnz.f:1-155; 1D/2D/3D), PSOD (psod.f:1-208; 1D/2D/3D) and PPSOD
-// (ppsod.f:1-470; PSOD with a laser pulse; 1D/2D/3D).
+// (plnz.f:1-155; 1D/2D/3D), PSOD (psod.f:1-208; 1D/2D/3D), PPSOD
+// (ppsod.f:1-470; PSOD with a laser pulse) and PPLNZ (pplnz.f:1-340; PLNZ
+// with a laser pulse), 1D/2D/3D.
 //
 // Each call propagates one packet on the GPU through a one-packet plan and
 // leaves in the caller's arrays what the reference routine leaves there:
@@ -815,6 +816,215 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
       espec_grid_previous(plan, u1, v1, ESPEC_MEM_HOST, nullptr))
     return fail(espec_last_error());
   for (long i = 0; i < nn; ++i) vpot[i] = vp[i] - dm[i] * ef[nsteps];
+  std::fflush(stdout);
+}
+
+// PPLNZ (pplnz.f:1-340): PLNZ with the potential VP - DM EF(T) (chpot.f, ef.f)
+// in each PLNZAUX step, DO T = TI+DT, TF+DT/2, DT, on a grid plan of method
+// ESPEC_SIL with the field table of espec_pplnz_field and sil.f's in-place
+// cos-before-sin.  Its table: FORMAT 1021 rows of T, ET (with the field), E0
+// (without), Cr, Ci, CT(1..NPR) and the norm, where CT(1) = |C|^2 and CT(k+1)
+// = |<W_k|psi>|^2 with W_k = LNZVC(., KP+k), k < NPR; on the first row the
+// norm is printed squared (pplnz.f:146-147).  C(0) is stored in LNZVC only
+// inside the print test, then every LC steps.
+extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
+                       const int* prteigvc2, const int* prtpuls, const char* dim, const char* efc,
+                       const char* prtcrl, const char* tpabsor, int* info, const int* lc,
+                       const int* lmtreort, int* mp, const int* mpi, const int* mpr,
+                       const int* mxdct, const int* n, const int* nshot, const int* kl,
+                       const int* npr_in, const int* kp, const double* abstol, const double* dt,
+                       const double* ti, const double* tf, const double* tol, const double* e0,
+                       const double* t0, const double* td, const double* tp, const double* omg,
+                       const double* sni, const int* np, const int* nd, int* iwork,
+                       const double* sh, const double* shm, double* vpot, const double* vabc,
+                       double* u, double* v, const double* xi, const double* xf, const double* xp,
+                       const double* dm, double* wu, double* wv, double* wp, double* work,
+                       const double* var, double* lnzvc, size_t dim_len, size_t efc_len,
+                       size_t prtcrl_len, size_t tpabsor_len) {
+  (void)prtveff; (void)prteigvc2; (void)prtpuls; (void)nshot; (void)abstol; (void)nd;
+  (void)iwork; (void)sh; (void)xi; (void)xf; (void)xp; (void)wu; (void)wv; (void)wp; (void)work;
+  (void)var;
+  *info = 0;
+  auto fail = [&](const char* why) {
+    std::fprintf(stderr, "espec_gpu PPLNZ: %s\n", why);
+    *info = 2;
+  };
+  int ndim = 0;
+  if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
+  if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
+  if (fstr_is(dim, dim_len, ".3D")) ndim = 3;
+  if (!ndim) return fail("DIM must be '.1D', '.2D' or '.3D'");
+  long npts = 1;
+  for (int a = 0; a < ndim; ++a) npts *= np[a];
+  if (npts != *n) return fail("N differs from the product of NP");
+  if (*lc < 1) return fail("LC must be at least 1");
+  if (*npr_in > 6) return fail("NPR must be at most 6 (rdinput.f:660)");
+  const int npr = std::max(*npr_in, 0);
+  const int nw = std::max(npr - 1, 0);  // printed projections: W_1 .. W_{NPR-1}
+  int shape = -1;  // ef.f:44-60
+  if (fstr_is(efc, efc_len, ".GAUS")) shape = ESPEC_PULSE_GAUS;
+  else if (fstr_is(efc, efc_len, ".GGAUS")) shape = ESPEC_PULSE_GGAUS;
+  else if (fstr_is(efc, efc_len, ".SIN2")) shape = ESPEC_PULSE_SIN2;
+  else if (fstr_is(efc, efc_len, ".NONE") || fstr_is(efc, efc_len, ".NULL")) shape = ESPEC_PULSE_NONE;
+  if (shape < 0) return fail("desired laser pulse wasn't found (ef.f:58-60)");
+  const double par[6] = {*e0, *tp, *omg, shape == ESPEC_PULSE_SIN2 ? *td : *t0, *sni, (double)*kl};
+  // LNZ's order test (lnz.f:64-72), as in PLNZ: with *CHANGE the first call
+  // lowers MP to LMTREORT for good
+  const int mp_in = *mp;
+  const bool clamp = mp_in > *lmtreort;
+  const int m = clamp && *change ? *lmtreort : mp_in;
+  if (m < 1 || m > 16) return fail("the GPU Lanczos order is limited to 1..16");
+  // .SMOOTHW mask after each step (sil.f:171); any other absorber is ignored
+  const int ab = *absorb && fstr_is(tpabsor, tpabsor_len, ".SMOOTHW") ? ESPEC_ABS_SMOOTHW
+                                                                     : ESPEC_ABS_NONE;
+  const int prt = fstr_is(prtcrl, prtcrl_len, ".YES") ? 2
+                  : (fstr_is(prtcrl, prtcrl_len, ".PARTIAL") ? 1 : 0);
+  const long nn = *n;
+  std::vector<double> ef((size_t)std::max(8L, (long)((*tf - *ti) / *dt) + 8));
+  const long nfield = espec_pplnz_field(shape, par, *ti, *tf, *dt, ef.data(), (long)ef.size());
+  if (nfield < 1) return fail(espec_last_error());
+  const int nsteps = (int)nfield - 1;  // step s lands at T_s and uses EF(T_s)
+  std::vector<double> vp(vpot, vpot + nn);
+  espec_grid_plan* plan = nullptr;
+  double* d_w = nullptr;
+  struct Guard {
+    espec_grid_plan*& p;
+    double*& w;
+    ~Guard() {
+      espec_grid_destroy(p);
+      if (w) cudaFree(w);
+    }
+  } guard{plan, d_w};
+  if (espec_grid_create(&plan, ESPEC_SIL, ndim, np, shm, *dt, m, ESPEC_FP64, ab,
+                        ESPEC_Q_SIL_INPLACE) ||
+      espec_grid_load(plan, vp.data(), ab == ESPEC_ABS_NONE ? nullptr : vabc, u, v,
+                      ESPEC_MEM_HOST, nullptr) ||
+      espec_grid_set_pulse(plan, dm, ef.data(), nfield, ESPEC_MEM_HOST))
+    return fail(espec_last_error());
+  if (nw > 0) {  // W_k = LNZVC(:, KP+k) (pplnz.f:93-98)
+    if (cudaMalloc(&d_w, sizeof(double) * nn * nw) != cudaSuccess) return fail("device memory");
+    for (int k = 0; k < nw; ++k)
+      if (cudaMemcpy(d_w + (size_t)k * nn, lnzvc + (size_t)(*kp + k) * *mxdct, sizeof(double) * nn,
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail("copy of the projection vectors");
+  }
+  auto store = [&](long nc, double cr, double ci) {  // LNZVC(NC, MPR/MPI), NC from 1
+    lnzvc[(nc - 1) + (long)(*mpr - 1) * *mxdct] = cr;
+    lnzvc[(nc - 1) + (long)(*mpi - 1) * *mxdct] = ci;
+  };
+  struct Row {
+    double et = 0, e0 = 0, fnr = 0;
+    std::vector<double> pj;
+  };
+  auto measure = [&](double efs, Row& r) -> bool {
+    double nr0;
+    r.pj.assign(2 * (size_t)std::max(nw, 1), 0.0);
+    if (espec_grid_energies_at(plan, efs, &r.et, &r.fnr, nullptr) ||
+        espec_grid_energies_at(plan, 0.0, &r.e0, &nr0, nullptr) ||
+        (nw > 0 && espec_grid_project(plan, d_w, nw, r.pj.data(), nullptr))) {
+      fail(espec_last_error());
+      return false;
+    }
+    return true;
+  };
+  double f0 = 0.0;
+  auto print_row = [&](double t, const Row& r, double cr, double ci, bool first) {
+    const double fnt = first ? r.fnr * r.fnr : r.fnr;
+    // FORMAT 1021: (1X,F14.6,3X,2(E12.6,3X),2(F8.5,3X),10(F8.6,3X))
+    std::string row = " " + fmt_f(t, 14, 6) + "   " + fmt_e(r.et, 12, 6) + "   " +
+                      fmt_e(r.e0, 12, 6) + "   " + fmt_f(cr, 8, 5) + "   " + fmt_f(ci, 8, 5);
+    if (npr >= 1) row += "   " + fmt_f(cr * cr + ci * ci, 8, 6);
+    for (int k = 0; k < nw; ++k)
+      row += "   " + fmt_f(r.pj[2 * k] * r.pj[2 * k] + r.pj[2 * k + 1] * r.pj[2 * k + 1], 8, 6);
+    row += "   " + fmt_f(fnt, 8, 6) + "\n";
+    if (first) f0 = fnt;
+    else if (!*absorb && std::fabs((fnt - f0) / f0) * 1.0e2 > *tol) *info = 1;
+    emit(row);
+  };
+  // LNZ's messages of step s (both chains; with *CHANGE only the first call)
+  auto step_text = [&](int s) -> std::string {
+    if (!clamp) return std::string();
+    if (*change) return s == 1 ? lnz_order_text(mp_in, *lmtreort, true) : std::string();
+    const std::string one = lnz_order_text(mp_in, *lmtreort, false);
+    return one + one;
+  };
+  // which steps store C and which print (pplnz.f:211-224)
+  std::vector<char> printed(nsteps + 1, 0), stored(nsteps + 1, 0);
+  int mc = 0;
+  for (int s = 1; s <= nsteps; ++s) {
+    mc = mc + 1;
+    if (mc == *lc) {
+      mc = 0;
+      stored[s] = 1;
+    }
+    if (prt == 2 || (prt == 1 && mc == 0)) printed[s] = 1;
+  }
+  long nc = 1;
+  Row first;
+  if (prt) {
+    if (!measure(0.0, first)) return;
+    std::string head = " \n";
+    head += (dim_len >= 3 && std::memcmp(dim, ".1D", 3) == 0 &&
+             std::string(dim + 3, dim_len - 3).find_first_not_of(' ') == std::string::npos)
+                ? " Auto-correlation function:\n"
+                : " Partial auto-correlation function:\n";
+    head += " ==================================\n\n";
+    // FORMAT 1011 (pplnz.f:331-332): groups (A3,I1,A4) joined by 3X
+    head += "        *t/fs*     *ET/a.u.*      *E0/a.u.*      *Pr(t)*    *Pi(t)*   ";
+    auto group = [&](const char* a, int i, bool last) {
+      head += std::string(a) + (i >= 0 && i <= 9 ? std::string(1, (char)('0' + i)) : "*") +
+              "|^2*" + (last ? "" : "   ");
+    };
+    for (int i = 1; i <= npr; ++i) group("*|P", i - 1, false);
+    group("*|c", 0, true);
+    emit(head + "\n");
+  }
+  std::vector<double> cre, cim;
+  int done = 0;
+  if (nsteps == 0 && prt) {  // no step: the first row alone
+    std::vector<double> c0(2);
+    if (espec_grid_run(plan, 0, nullptr) ||
+        espec_grid_results(plan, &c0[0], &c0[1], nullptr, nullptr, ESPEC_MEM_HOST, nullptr))
+      return fail(espec_last_error());
+    store(nc, c0[0], c0[1]);
+    print_row(*ti, first, c0[0], c0[1], true);
+  }
+  for (int s = 1; s <= nsteps; ++s) {
+    if (!printed[s] && s != nsteps) continue;
+    const int k = s - done;
+    cre.resize(k + 1);
+    cim.resize(k + 1);
+    if ((done == 0 ? espec_grid_run(plan, k, nullptr) : espec_grid_continue(plan, k, nullptr)) ||
+        espec_grid_results(plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST,
+                           nullptr))
+      return fail(espec_last_error());
+    if (done == 0 && prt) {
+      store(nc, cre[0], cim[0]);
+      print_row(*ti, first, cre[0], cim[0], true);
+    }
+    std::string text;
+    for (int j = 1; j <= k; ++j) {
+      text += step_text(done + j);
+      if (stored[done + j]) store(++nc, cre[j], cim[j]);
+    }
+    emit(text);
+    done = s;
+    if (printed[s]) {
+      double t = *ti + *dt;  // the DO variable, accumulating DT
+      for (int q = 2; q <= s; ++q) t = t + *dt;
+      Row r;
+      if (!measure(ef[s], r)) return;
+      print_row(t, r, cre[k], cim[k], false);
+    }
+  }
+  // psi(TF), the last step's Lanczos basis (LNZVC(., 1..MP), the V chain),
+  // VPOT as CHPOT leaves it, MP as LNZ leaves it
+  if (espec_grid_results(plan, nullptr, nullptr, u, v, ESPEC_MEM_HOST, nullptr) ||
+      (nsteps > 0 && espec_grid_basis(plan, 1, lnzvc, *mxdct, ESPEC_MEM_HOST, nullptr)))
+    return fail(espec_last_error());
+  if (nsteps > 0)
+    for (long i = 0; i < nn; ++i) vpot[i] = vp[i] - dm[i] * ef[nsteps];
+  if (clamp && *change) *mp = m;
   std::fflush(stdout);
 }
 

@@ -166,6 +166,44 @@ def ppsod(*, absorb, dim, efc, prtcrl, tpabsor, lc, mpi, mpr, mxdct, n, dt, ti, 
     return info.value
 
 
+def pplnz(*, absorb, change, dim, efc, prtcrl, tpabsor, lc, lmtreort, mp, mpi, mpr, mxdct, n,
+          dt, ti, tf, tol, np_, shm, e0, tp, omg, dm, vpot, vabc, u, v, lnzvc, t0=0.0, td=0.0,
+          sni=0.0, kl=0, npr=0, kp=1, abstol=1e-6):
+    """PPLNZ: PLNZ with the laser pulse efc and the dipole function dm; the
+    projection vectors are the columns kp..kp+npr-2 (0-based) of lnzvc.  On
+    return U + i V is psi(TF) and vpot holds VP - DM EF of the last step.
+    Returns (INFO, MP after the call)."""
+    info = C.c_int(0)
+    mp_c = C.c_int(mp)
+    npa = np.array(list(np_) + [1] * (3 - len(np_)), dtype=np.int32)
+    shma = N.f64(list(shm) + [0.0] * (3 - len(shm)))
+    dma = N.f64(dm)
+    va = N.f64(vabc) if vabc is not None else np.zeros(n)
+    ints = {k: C.c_int(v) for k, v in dict(
+        absorb=1 if absorb else 0, change=1 if change else 0, off=0, lc=lc, lmt=lmtreort,
+        mpi=mpi, mpr=mpr, mxdct=mxdct, n=n, nshot=10, kl=kl, npr=npr, kp=kp).items()}
+    dbl = {k: C.c_double(v) for k, v in dict(
+        abstol=abstol, dt=dt, ti=ti, tf=tf, tol=tol, e0=e0, t0=t0, td=td, tp=tp, omg=omg,
+        sni=sni).items()}
+    z3 = np.zeros(3)
+    scratch = np.zeros(max(n, 1))
+    iwork = np.zeros(16, dtype=np.int32)
+    b = {k: v.encode() for k, v in dict(dim=dim, efc=efc, prtcrl=prtcrl, tpabsor=tpabsor).items()}
+    r = C.byref
+    N.load().pplnz_(
+        r(ints["absorb"]), r(ints["change"]), r(ints["off"]), r(ints["off"]), r(ints["off"]),
+        b["dim"], b["efc"], b["prtcrl"], b["tpabsor"], r(info), r(ints["lc"]), r(ints["lmt"]),
+        r(mp_c), r(ints["mpi"]), r(ints["mpr"]), r(ints["mxdct"]), r(ints["n"]), r(ints["nshot"]),
+        r(ints["kl"]), r(ints["npr"]), r(ints["kp"]), r(dbl["abstol"]), r(dbl["dt"]),
+        r(dbl["ti"]), r(dbl["tf"]), r(dbl["tol"]), r(dbl["e0"]), r(dbl["t0"]), r(dbl["td"]),
+        r(dbl["tp"]), r(dbl["omg"]), r(dbl["sni"]), N.ptr(npa), N.ptr(npa), N.ptr(iwork),
+        N.ptr(z3), N.ptr(shma), _arr(vpot), N.ptr(va), _arr(u), _arr(v), N.ptr(z3), N.ptr(z3),
+        N.ptr(z3), N.ptr(dma), N.ptr(scratch), N.ptr(scratch), N.ptr(scratch), N.ptr(scratch),
+        N.ptr(z3), _arr(lnzvc), len(b["dim"]), len(b["efc"]), len(b["prtcrl"]),
+        len(b["tpabsor"]))
+    return info.value, mp_c.value
+
+
 def format_crl_row(t, e, cr, ci, ct, fnt):
     """One row of the partial auto-correlation table (FORMAT 1021, pspofft.f:148)."""
     buf = C.create_string_buffer(256)

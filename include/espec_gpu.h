@@ -138,6 +138,25 @@ void ppsod_(const int* absorb, const int* prtveff, const int* prteigvc2, const i
             const double* var, double* lnzvc, const int* prtregion, const int* nreg,
             const double* range, const int* prtonlyreim, size_t dim_len, size_t efc_len,
             size_t prtcrl_len, size_t tpabsor_len);
+/* replaces SUBROUTINE PPLNZ (pplnz.f:1-5; called from espec.f:1513 for
+ * '.PPSIL' / '.PPLNZ'): PLNZ with the laser pulse EFC and dipole DM, 1D/2D/3D;
+ * prints pplnz.f's table (E with and without the field, C(t), |C|^2 and the
+ * populations of LNZVC(., KP+1..KP+NPR-1), the norm); C(t) in LNZVC(., MPR/MPI),
+ * the last step's Lanczos basis in LNZVC(., 1..MP); psi(TF) in U/V; VPOT
+ * left holding VP - DM EF of the last step; MP lowered as LNZ lowers it.  The
+ * files of PRTVEFF, PRTEIGVC2, PRTPULS and '.LASTWP' are not written. */
+void pplnz_(const int* absorb, const int* change, const int* prtveff, const int* prteigvc2,
+            const int* prtpuls, const char* dim, const char* efc, const char* prtcrl,
+            const char* tpabsor, int* info, const int* lc, const int* lmtreort, int* mp,
+            const int* mpi, const int* mpr, const int* mxdct, const int* n, const int* nshot,
+            const int* kl, const int* npr, const int* kp, const double* abstol, const double* dt,
+            const double* ti, const double* tf, const double* tol, const double* e0,
+            const double* t0, const double* td, const double* tp, const double* omg,
+            const double* sni, const int* np, const int* nd, int* iwork, const double* sh,
+            const double* shm, double* vpot, const double* vabc, double* u, double* v,
+            const double* xi, const double* xf, const double* xp, const double* dm, double* wu,
+            double* wv, double* wp, double* work, const double* var, double* lnzvc,
+            size_t dim_len, size_t efc_len, size_t prtcrl_len, size_t tpabsor_len);
 /* replace SUBROUTINE HWHM (hwhm.f:1-80; TAL is scaled in place) and
  * SUBROUTINE SPECTRUMTD (spectrumtd.f:1-116; prints the spectrum table,
  * sets DE < 0 to 0), called at espec.f:1618-1624: the arithmetic runs on the

@@ -45,12 +45,22 @@ def test_ppsod_projections(tmp_path):
     by one; what is left of NPR would project on states the deck does not
     have."""
     text = BASE.replace(".PFSPO", ".PPSOD")
-    msg = refused(tmp_path, text.replace("*PRPTOL", "*NPROJECTIONS\n 3 1/\n*PRPTOL"))
-    assert "*NPROJECTIONS" in msg, msg
-    # NPR = 1, KP = 1 leaves none: the deck passes the reading and stops at
-    # its (absent) .FILE
-    msg = refused(tmp_path, text.replace("*PRPTOL", "*NPROJECTIONS\n 1 1/\n*PRPTOL"))
-    assert "cannot be opened" in msg, msg
+    for npr_kp in ("3 1", "2 1", "3 0"):
+        msg = refused(tmp_path, text.replace("*PRPTOL", f"*NPROJECTIONS\n {npr_kp}/\n*PRPTOL"))
+        assert "*NPROJECTIONS" in msg, (npr_kp, msg)
+    # NPR = 1, KP = 1 leaves none; NPR = 2, KP = 0 leaves one on LNZVC(., 1):
+    # the deck passes the reading and stops at its (absent) .FILE
+    for npr_kp in ("1 1", "2 0"):
+        msg = refused(tmp_path, text.replace("*PRPTOL", f"*NPROJECTIONS\n {npr_kp}/\n*PRPTOL"))
+        assert "cannot be opened" in msg, (npr_kp, msg)
+    # PPLNZ prints NPR - 1 projections after |C|^2
+    text = BASE.replace(".PFSPO\n 0.0  0.3096171935104  0.00120944216215/",
+                        ".PPSIL\n 0.0  0.3096171935104  0.00120944216215 10/")
+    assert text != BASE
+    for npr_kp, why in (("3 0", "cannot be opened"), ("4 0", "*NPROJECTIONS"),
+                        ("3 1", "*NPROJECTIONS"), ("2 1", "cannot be opened")):
+        msg = refused(tmp_path, text.replace("*PRPTOL", f"*NPROJECTIONS\n {npr_kp}/\n*PRPTOL"))
+        assert why in msg, (npr_kp, msg)
 
 
 def test_missing_and_short_files(tmp_path):

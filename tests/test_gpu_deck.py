@@ -3,7 +3,7 @@ against the shipped executable's output for the same decks and files
 (tests/golden/deck_*/expected.txt, from the propagation to the end): every
 line of text identical; every printed number within one unit of its last
 printed digit (both sides rounded FP64 values; E-format fields relative).
-.PSIL decks get 4e-7 more: the reference bisects the eigenvalues of its
+.PSIL and .PPSIL decks get 4e-7 more: the reference bisects the eigenvalues of its
 Krylov matrices only to ABSTOL = 1e-6 (espec.f:157), which moves C(t) by a
 few 1e-8 over these runs (the same allowance as the PLNZ drop-in's test).
 For .PSIL the executable's total correlation is corrupted (it stores C(t)
@@ -22,7 +22,8 @@ import golden_cases as G
 
 pytestmark = pytest.mark.gpu
 
-DECKS = ["deck_spo_hwhm", "deck_psod_voptic", "deck_sil_smooth", "deck_sil_2d", "deck_ppsod"]
+DECKS = ["deck_spo_hwhm", "deck_psod_voptic", "deck_sil_smooth", "deck_sil_2d", "deck_ppsod",
+         "deck_ppsod_proj", "deck_ppsil", "deck_ppsil_proj"]
 NUM = re.compile(r"^-?(\d+\.?\d*|\.\d+)([EeDd][-+]?\d+)?$")
 
 
@@ -71,7 +72,7 @@ def test_deck_matches_executable(capfd, name):
     with open(os.path.join(d, "expected.txt")) as f:
         want = f.read().split("\n")
     if "_sil" not in name:
-        exact = compare(have, want)
+        exact = compare(have, want, slack=4e-7 if "ppsil" in name else 0.0)
         assert exact >= 0.9 * len(want), (exact, len(want))
         return
     k = have.index(" Correlation Function:")
