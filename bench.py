@@ -52,6 +52,9 @@ def parse():
     ap.add_argument("--cpu-sample-packets", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the FP64-form, SIL-2D and eigensolver legs")
+    ap.add_argument("--leg", default=None, choices=["sil_2d", "psod_2d"],
+                    help="run one grid-plan leg alone and print its JSON (profiling)")
+    ap.add_argument("--leg-steps", type=int, default=100)
     ap.add_argument("--eig-train", type=int, default=50000)
     ap.add_argument("--eig-test", type=int, default=2048)
     ap.add_argument("--eig-epochs", type=int, default=100)
@@ -278,18 +281,80 @@ def sil_2d(dev, steps=100, cpu_steps=2):
     g.results()
     ms = e0.elapsed_time(e1) / steps
     g.close()
-    from oracle import oracle as O
+    m = 12
+    peak, peak_kind = measured_peaks()
+    achieved = sil_bytes(m) * n * n / (ms * 1e-3) / 1e9
+    out = {"workload": "SIL order 12, 256x256 coupled Morse, dt = 1 au", "value":
+           n * n / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s", "us_per_step": ms * 1e3,
+           "steps_timed": steps,
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak, "peak_kind": peak_kind,
+                        "bytes_per_gridpt_step": sil_bytes(m),
+                        "note": "basis (12.6 MB) and state stay in L2: the step is bound by its "
+                                "2m grid-wide reductions, not by HBM"}}
+    if cpu_steps:
+        from oracle import oracle as O
 
-    p = O.make_prop([n, n], dt, 0.0, cpu_steps * dt, [h, h], sm, lc=1, mp=12, lmtreort=16,
-                    change=0, shm=shm)
-    t0 = time.perf_counter()
-    O.plnz(p, v, psi.real.copy(), psi.imag.copy())
-    tc = (time.perf_counter() - t0) / O.do_count(dt, cpu_steps * dt + dt, dt)
-    return {"workload": "SIL order 12, 256x256 coupled Morse, dt = 1 au", "value":
-            n * n / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s", "us_per_step": ms * 1e3,
-            "steps_timed": steps, "cpu_port": {"value": n * n / tc / 1e6,
-                                               "unit": "Mgridpt*steps/s", "cores": 1,
-                                               "sample": f"{cpu_steps} steps"}}
+        p = O.make_prop([n, n], dt, 0.0, cpu_steps * dt, [h, h], sm, lc=1, mp=m, lmtreort=16,
+                        change=0, shm=shm)
+        t0 = time.perf_counter()
+        O.plnz(p, v, psi.real.copy(), psi.imag.copy())
+        tc = (time.perf_counter() - t0) / O.do_count(dt, cpu_steps * dt + dt, dt)
+        out["cpu_port"] = {"value": n * n / tc / 1e6, "unit": "Mgridpt*steps/s", "cores": 1,
+                           "sample": f"{cpu_steps} steps"}
+    return out
+
+
+def sil_bytes(m):
+    """Algorithmic bytes per grid point and step of SIL order m (FP64), both
+    chains: m H.psi (read psi and V, write H psi: 24 B each), the
+    reorthogonalisation's 2 sum_{j<=m} j vector reads (8 B each), m basis
+    writes and m basis reads of the expansion (8 B each)."""
+    return 2 * (24 * m + 8 * m * (m + 1) + 16 * m)
+
+
+PSOD_BYTES = 72  # read psi_n, psi_{n-1}, psi0 (16 B each) and V (8 B); write psi_{n+1} (16 B)
+
+
+def psod_2d(dev, steps=100, cpu_steps=2):
+    """Second-order differences (PSOD, FD stencil, FP64) on 2D coupled-Morse
+    grids: 256 x 256 (state in L2) and 2048 x 2048 (state in HBM), dt below
+    the SOD stability limit 1 / E_max of each grid."""
+    import torch
+
+    import espec_b200 as E
+
+    peak, peak_kind = measured_peaks()
+    out = {"workload": "PSOD, 2D coupled Morse, FP64, C(t) every step"}
+    for n, dt_au in ((256, 0.1), (2048, 0.002)):
+        x = np.linspace(0.5, 8.0, n)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        morse = lambda q, de, a, re: de * (1 - np.exp(-a * (q - re))) ** 2  # noqa: E731
+        V = morse(X, 0.17, 1.0, 1.4) + morse(Y, 0.12, 1.2, 1.8) + 0.01 * (X - 1.4) * (Y - 1.8)
+        psi = np.exp(-((X - 1.6) ** 2) / (2 * 0.15 ** 2) - ((Y - 2.0) ** 2) / (2 * 0.15 ** 2))
+        psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
+        h = x[1] - x[0]
+        shm = [1.0 / (((24.0 * m) * h) * h) for m in (918.0, 1500.0)]
+        g = E.PsodGrid([n, n], shm, dt_au * 2.4188843243e-2)
+        g.load(V.ravel(order="F"), psi)
+        g.run(5)
+        g.results()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = torch.cuda.current_stream(dev)
+        e0.record(st)
+        g.run(steps)
+        e1.record(st)
+        c, _ = g.results()
+        ms = e0.elapsed_time(e1) / steps
+        g.close()
+        achieved = PSOD_BYTES * n * n / (ms * 1e-3) / 1e9
+        out[f"{n}x{n}"] = {
+            "dt_au": dt_au, "value": n * n / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s",
+            "us_per_step": ms * 1e3, "steps_timed": steps, "finite": bool(np.isfinite(c).all()),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind,
+                         "bytes_per_gridpt_step": PSOD_BYTES}}
+    return out
 
 
 def spo_nd(dev):
@@ -403,6 +468,12 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.leg:
+        if rank == 0:
+            leg = {"sil_2d": sil_2d, "psod_2d": psod_2d}[args.leg]
+            print(json.dumps({"leg": args.leg, **leg(dev, steps=args.leg_steps, cpu_steps=0)}),
+                  flush=True)
+        return
     sizes = tuple(int(x) for x in args.sizes.split(",")) if args.sizes else W.SCAN_SIZES
     w = W.morse_scan(npk=args.npk, nsteps=args.nsteps, seed=rank_seed(rank), sizes=sizes)
     pts_steps = float(w["off"][-1]) * w["nsteps"]
@@ -496,6 +567,7 @@ def main():
     if rank == 0 and not args.no_extra:
         extra["fp64_form"] = fp64_form(args, w, ms, dev) if args.precision == "mixed" else None
         extra["sil_2d"] = sil_2d(dev)
+        extra["psod_2d"] = psod_2d(dev)
         extra.update(spo_nd(dev))
         extra["eigensolver"] = eig_warmstart(args, dev)
     if rank == 0:

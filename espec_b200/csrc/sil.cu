@@ -34,27 +34,37 @@ __device__ __forceinline__ Range my_range(long n) {
 }
 
 // Grid barrier fused with a reduction: sp[0..nq) holds this CTA's partial
-// sums; on return st[0..nq) holds the totals over all CTAs, summed by the last
-// CTA to arrive in CTA order (deterministic).  false = a wait gave up.
+// sums; on return st[0..nq) holds the totals over all CTAs.  After the
+// barrier every CTA sums the G partials itself, in one fixed order, so all
+// CTAs hold the same bits and no CTA waits for another's sum.  The partials
+// alternate between two buffers by barrier parity (phase, counted alike by
+// every thread of every CTA): a CTA runs at most one barrier ahead of the
+// slowest, which can still be reading the other buffer.  false = a wait
+// gave up.
 __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int nq,
-                            int* s_flag, double* s_red /* kSilThreads doubles */) {
+                            int* s_flag, double* s_red /* kSilThreads doubles */,
+                            unsigned& phase) {
   const int b = blockIdx.x, G = gridDim.x, t = threadIdx.x;
-  // The CTA's writes are ordered before thread 0's release (the acq_rel
-  // arrival) by bar.sync, whose ordering is cumulative; the waiters' acquire
-  // loads order everything after.
-  for (int q = t; q < nq; q += blockDim.x) a.part[(long)b * kSilNQ + q] = sp[q];
+  double* part = a.part + (size_t)(phase & 1u) * G * kSilNQ;
+  // a.bar counts the arrivals of the launch (zeroed before it): barrier k is
+  // passed once it reaches (k + 1) G
+  const unsigned long long target = (unsigned long long)(phase + 1u) * (unsigned)G;
+  ++phase;
+  // The CTA's writes are ordered before thread 0's arrival (a release RMW) by
+  // bar.sync, whose ordering is cumulative; every arrival continues the
+  // release sequence of the earlier ones, so a waiter's acquire load of the
+  // final count synchronises with all of them.
+  for (int q = t; q < nq; q += blockDim.x) part[(long)b * kSilNQ + q] = sp[q];
   __syncthreads();
   if (t == 0) {
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(a.bar[0]);
-    cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(a.bar[1]);
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device> cnt(
+        *reinterpret_cast<unsigned long long*>(a.bar));
     cuda::atomic_ref<int, cuda::thread_scope_device> err(*a.err);
-    const unsigned g = gen.load(cuda::memory_order_acquire);
-    const unsigned arrived = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-    s_flag[0] = arrived == (unsigned)G - 1;
+    const unsigned long long arrived = cnt.fetch_add(1ull, cuda::memory_order_acq_rel) + 1ull;
     s_flag[1] = 1;
-    if (!s_flag[0]) {
+    if (arrived < target) {
       long spins = 0;
-      while (gen.load(cuda::memory_order_acquire) == g) {
+      while (cnt.load(cuda::memory_order_acquire) < target) {
         if (++spins > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
           err.store(1, cuda::memory_order_relaxed);
           s_flag[1] = 0;
@@ -66,41 +76,35 @@ __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int 
   }
   __syncthreads();
   if (!s_flag[1]) return false;
-  if (s_flag[0]) {
-    // R threads per quantity, each summing every R-th CTA in CTA order, then
-    // the R partial sums in order: a fixed summation order for a fixed grid
-    double* red = reinterpret_cast<double*>(s_red);
-    const int R = nq > 0 ? min(kSilThreads / nq, 32) : 1;
-    if (t < R * nq) {
-      const int q = t % nq, r = t / nq;
-      double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-      int i = r, u = 0;
-      for (; i + 7 * R < G; i += 8 * R) {  // eight loads in flight
+  // R threads per quantity, each summing every R-th CTA in CTA order with up
+  // to 16 loads in flight, then the R partial sums in order
+  double* red = s_red;
+  const int R = nq > 0 ? min(kSilThreads / nq, 32) : 1;
+  if (t < R * nq) {
+    const int q = t % nq, r = t / nq;
+    double acc[16];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[j] += __ldcg(a.part + (long)(i + j * R) * kSilNQ + q);
+    for (int j = 0; j < 16; ++j) acc[j] = 0.0;
+    for (int i0 = r; i0 < G; i0 += 16 * R) {
+      double x[16];
+#pragma unroll
+      for (int j = 0; j < 16; ++j) {
+        const int i = i0 + j * R;
+        x[j] = i < G ? __ldcg(part + (long)i * kSilNQ + q) : 0.0;
       }
-      for (; i < G; i += R, ++u) acc[u & 7] += __ldcg(a.part + (long)i * kSilNQ + q);
-      double s = 0.0;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) s += acc[j];
-      red[r * nq + q] = s;
+      for (int j = 0; j < 16; ++j) acc[j] += x[j];
     }
-    __syncthreads();
-    for (int q = t; q < nq; q += blockDim.x) {
-      double s = 0.0;
-      for (int r = 0; r < R; ++r) s += red[r * nq + q];
-      st[q] = s;
-      a.tot[q] = s;
-    }
-    __syncthreads();
-    if (t == 0) {
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> cnt(a.bar[0]);
-      cuda::atomic_ref<unsigned, cuda::thread_scope_device> gen(a.bar[1]);
-      cnt.store(0u, cuda::memory_order_relaxed);
-      gen.fetch_add(1u, cuda::memory_order_release);
-    }
-  } else {
-    for (int q = t; q < nq; q += blockDim.x) st[q] = __ldcg(a.tot + q);
+    double s = 0.0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) s += acc[j];
+    red[r * nq + q] = s;
+  }
+  __syncthreads();
+  for (int q = t; q < nq; q += blockDim.x) {
+    double s = 0.0;
+    for (int r = 0; r < R; ++r) s += red[r * nq + q];
+    st[q] = s;
   }
   __syncthreads();
   return true;
@@ -308,6 +312,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   const int t = threadIdx.x;
   const long n = a.n;
   const int m = a.m;
+  unsigned phase = 0;  // grid barriers passed in this launch
   constexpr int NW = kSilThreads / 32;
 
   for (int s = 0;; ++s) {
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         q[5] += v0k * uk;
       }
       block_sum<6>(q, sp, scratch);
-      if (!grid_reduce(a, sp, st, 6, s_flag, s_red)) return;
+      if (!grid_reduce(a, sp, st, 6, s_flag, s_red, phase)) return;
       if (t == 0 && blockIdx.x == 0 && (s > 0 || a.write_c0))
         a.c_out[s] = make_double2(st[2] + st[3], st[4] - st[5]);
       if (s == a.nsteps) break;
@@ -392,7 +397,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         sp[q] = sum;
       }
       __syncthreads();
-      if (!grid_reduce(a, sp, st, nq, s_flag, s_red)) return;
+      if (!grid_reduce(a, sp, st, nq, s_flag, s_red, phase)) return;
       if (t < 2) {
         const int c = t, b0 = slot_of(c, it, 0);
         const double al = st[b0];
@@ -426,7 +431,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         }
       }
       block_sum<2>(nn, sp, scratch);
-      if (!grid_reduce(a, sp, st, 2, s_flag, s_red)) return;
+      if (!grid_reduce(a, sp, st, 2, s_flag, s_red, phase)) return;
       if (t < 2) {
         s_bt[t][it] = sqrt(st[t]);
         s_bt0[t] = s_bt[t][it];
@@ -481,10 +486,11 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   __shared__ int s_flag[2];
   const Range r = my_range(a.n);
   const int t = threadIdx.x;
+  unsigned phase = 0;  // grid barriers passed in this launch
   double *un = a.u, *vn = a.v, *um = a.up, *vm = a.vp;
   auto reduce_c = [&](double (&q)[4], int slot) -> bool {
     block_sum<4>(q, sp, scratch);
-    if (!grid_reduce(a, sp, st, 4, s_flag, s_red)) return false;
+    if (!grid_reduce(a, sp, st, 4, s_flag, s_red, phase)) return false;
     if (t == 0 && blockIdx.x == 0 && slot >= 0)
       a.c_out[slot] = make_double2(st[0] + st[1], st[2] - st[3]);
     return true;
@@ -638,7 +644,7 @@ struct espec_grid_plan {
   double *d_up = nullptr, *d_vp = nullptr;  // PSOD: the state one step back
   double *d_dm = nullptr, *d_ef = nullptr;  // PSOD with a pulse: dipole, field per call
   long n_ef = 0, slot = 0;                  // field entries; steps of the current run
-  double *d_part = nullptr, *d_tot = nullptr, *d_epart = nullptr, *d_eout = nullptr;
+  double *d_part = nullptr, *d_epart = nullptr, *d_eout = nullptr;
   double* d_ppart = nullptr;  // projections: per-CTA partials, then the sums
   unsigned* d_bar = nullptr;
   int* d_err = nullptr;
@@ -648,7 +654,7 @@ struct espec_grid_plan {
 
 static void grid_free(espec_grid_plan* p) {
   void* b[] = {p->d_vpot, p->d_mask, p->d_u, p->d_v, p->d_u0, p->d_v0, p->d_L, p->d_work,
-               p->d_wbuf, p->d_part, p->d_tot, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c,
+               p->d_wbuf, p->d_part, p->d_epart, p->d_eout, p->d_bar, p->d_err, p->d_c,
                p->d_up, p->d_vp, p->d_dm, p->d_ef, p->d_ppart};
   for (void* x : b)
     if (x) cudaFree(x);
@@ -682,7 +688,6 @@ static SilArgs sil_args(const espec_grid_plan* p) {
   a.work = p->d_work;
   a.wbuf = p->d_wbuf;
   a.part = p->d_part;
-  a.tot = p->d_tot;
   a.bar = p->d_bar;
   a.err = p->d_err;
   a.c_out = p->d_c;
@@ -772,9 +777,8 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
     if ((rc = ck(cudaMalloc(&p->d_work, nb * 2), "cudaMalloc"))) return fail(rc);
     if ((rc = ck(cudaMalloc(&p->d_wbuf, nb * 2), "cudaMalloc"))) return fail(rc);
   }
-  if ((rc = ck(cudaMalloc(&p->d_part, sizeof(double) * kSilNQ * p->nblocks), "cudaMalloc")))
+  if ((rc = ck(cudaMalloc(&p->d_part, sizeof(double) * 2 * kSilNQ * p->nblocks), "cudaMalloc")))
     return fail(rc);
-  if ((rc = ck(cudaMalloc(&p->d_tot, sizeof(double) * kSilNQ), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_epart, sizeof(double) * 2 * 1024), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_eout, sizeof(double) * 2), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_bar, sizeof(unsigned) * 2), "cudaMalloc"))) return fail(rc);

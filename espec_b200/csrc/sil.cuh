@@ -45,9 +45,8 @@ struct SilArgs {
   double* L;     // [2][m][n] Lanczos vectors of the u and v chains
   double* work;  // [2][n]
   double* wbuf;  // [2][n]
-  double* part;  // [gridDim.x][kSilNQ]
-  double* tot;   // [kSilNQ]
-  unsigned* bar;  // [0] arrivals, [1] generation
+  double* part;  // [2][gridDim.x][kSilNQ]: partial sums, by barrier parity
+  unsigned* bar;  // [0..1]: one 64-bit count of the grid barrier arrivals of the launch
   int* err;       // set when a barrier wait gave up
   double2* c_out;  // C(t) of every step: slot s for step s (slot 0 only if write_c0)
   int m, nsteps, quirk, write_c0;
