@@ -360,25 +360,40 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 #pragma unroll
         for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) acc[i] = 0.0;
         if (act) {
-          for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-            double lq[kSilMaxM];
+          // two points per thread at a time, stores after both: their loads
+          // are in flight together
+          for (int k0 = r.lo + t; k0 < r.hi; k0 += 2 * kSilThreads) {
+            double vis[2], ws2[2];
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
-            const double vi = __ldcg(src + k) * rb;
-            const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
-            double hv = apply_h(a, src, k, rb);
-            if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
-            const double w = hv - bt0 * vprev;
-            const double xk = __ldcg(x + k);
-            Lc[(long)it * n + k] = vi;
-            a.wbuf[c * n + k] = w;
-            acc[0] += vi * w;
-            acc[1] += vi * xk;
-            acc[2] += vi * vi;
+            for (int j = 0; j < 2; ++j) {
+              const int k = k0 + j * kSilThreads;
+              if (k >= r.hi) continue;
+              double lq[kSilMaxM];
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q) {
-              acc[3 + q] += w * lq[q];
-              acc[3 + kSilMaxM + q] += vi * lq[q];
+              for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
+              const double vi = __ldcg(src + k) * rb;
+              const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
+              double hv = apply_h(a, src, k, rb);
+              if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
+              const double w = hv - bt0 * vprev;
+              const double xk = __ldcg(x + k);
+              vis[j] = vi;
+              ws2[j] = w;
+              acc[0] += vi * w;
+              acc[1] += vi * xk;
+              acc[2] += vi * vi;
+#pragma unroll
+              for (int q = 0; q < kSilMaxM; ++q) {
+                acc[3 + q] += w * lq[q];
+                acc[3 + kSilMaxM + q] += vi * lq[q];
+              }
+            }
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+              const int k = k0 + j * kSilThreads;
+              if (k >= r.hi) continue;
+              Lc[(long)it * n + k] = vis[j];
+              a.wbuf[c * n + k] = ws2[j];
             }
           }
         } else {
@@ -409,11 +424,14 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
       }
       __syncthreads();
       if (it == m - 1) break;  // the last residual is not needed (BT(M) unused)
+      // both chains at each point: their loads are in flight together
       double nn[2] = {0.0, 0.0};
-      for (int c = 0; c < 2; ++c) {
-        const double al = s_al[c][it];
-        const double* Lc = a.L + (long)c * m * n;
-        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+      for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+        double res[2];
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const double al = s_al[c][it];
+          const double* Lc = a.L + (long)c * m * n;
           double lq[kSilMaxM + 1];
 #pragma unroll
           for (int q = 0; q <= kSilMaxM; ++q) lq[q] = q <= it ? __ldcg(Lc + (long)q * n + k) : 0.0;
@@ -426,8 +444,12 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 #pragma unroll
           for (int q = 0; q <= kSilMaxM; ++q)
             if (q <= it) acc -= s_r[c][q] * lq[q];
-          a.work[c * n + k] = acc;
-          nn[c] += acc * acc;
+          res[c] = acc;
+        }
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          a.work[c * n + k] = res[c];
+          nn[c] += res[c] * res[c];
         }
       }
       block_sum<2>(nn, sp, scratch);
@@ -480,6 +502,8 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 // then the two buffers swap roles.  From the start: C(0), an Euler step of
 // c = CST/4 and a midpoint step of CST/2 to TI + DT, psi_{n-1} reset to psi0
 // (with the reference's copy defect on request), then steps of CST.
+constexpr int kPsodIlp = 4;
+
 __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
   __shared__ double s_red[kSilThreads];
@@ -498,34 +522,48 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   auto step = [&](double c, int slot, long call) -> bool {
     double q[4] = {0.0, 0.0, 0.0, 0.0};
     const double e = a.ef ? a.ef[call] : 0.0;  // chpot.f:46-50: V - DM EF
-    for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-      const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
-      double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
-      if (a.dm) {
-        const double de = __ldg(a.dm + k) * e;
-        hv -= de * vk;
-        hu -= de * uk;
+    // kPsodIlp points per thread at a time: all their loads are issued before
+    // the first store, so they are in flight together (a store to psi_{n-1}
+    // would otherwise hold back the next point's loads)
+    for (int k0 = r.lo + t; k0 < r.hi; k0 += kPsodIlp * kSilThreads) {
+      double nu[kPsodIlp], nv[kPsodIlp], u0k[kPsodIlp], v0k[kPsodIlp];
+#pragma unroll
+      for (int j = 0; j < kPsodIlp; ++j) {
+        const int k = k0 + j * kSilThreads;
+        if (k >= r.hi) continue;
+        const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
+        double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
+        if (a.dm) {
+          const double de = __ldg(a.dm + k) * e;
+          hv -= de * vk;
+          hu -= de * uk;
+        }
+        if (a.kabs == 1) {
+          const double w = a.vabc[k];
+          nu[j] = um[k] + c * hv - c * w * uk;
+          nv[j] = vm[k] - c * hu - c * w * vk;
+        } else if (a.kabs == 2) {
+          const double w = a.vabc[k];
+          nu[j] = w * (um[k] + c * hv);
+          nv[j] = w * (vm[k] - c * hu);
+        } else {
+          nu[j] = um[k] + c * hv;
+          nv[j] = vm[k] - c * hu;
+        }
+        u0k[j] = __ldg(a.u0 + k);
+        v0k[j] = __ldg(a.v0 + k);
       }
-      double nu, nv;
-      if (a.kabs == 1) {
-        const double w = a.vabc[k];
-        nu = um[k] + c * hv - c * w * uk;
-        nv = vm[k] - c * hu - c * w * vk;
-      } else if (a.kabs == 2) {
-        const double w = a.vabc[k];
-        nu = w * (um[k] + c * hv);
-        nv = w * (vm[k] - c * hu);
-      } else {
-        nu = um[k] + c * hv;
-        nv = vm[k] - c * hu;
+#pragma unroll
+      for (int j = 0; j < kPsodIlp; ++j) {
+        const int k = k0 + j * kSilThreads;
+        if (k >= r.hi) continue;
+        um[k] = nu[j];
+        vm[k] = nv[j];
+        q[0] += u0k[j] * nu[j];
+        q[1] += v0k[j] * nv[j];
+        q[2] += u0k[j] * nv[j];
+        q[3] += v0k[j] * nu[j];
       }
-      um[k] = nu;
-      vm[k] = nv;
-      const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
-      q[0] += u0k * nu;
-      q[1] += v0k * nv;
-      q[2] += u0k * nv;
-      q[3] += v0k * nu;
     }
     if (!reduce_c(q, slot)) return false;
     double* x = un;
