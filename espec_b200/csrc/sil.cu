@@ -132,27 +132,34 @@ __device__ __forceinline__ void block_sum(const double (&x)[NV], double* sp, dou
 
 // H_FD x at point k with every x value scaled by d (au1d.f:52-73,
 // au2di.f:57-225, au3d.f:61-117): (30 sum(shm) + V) x_k + sum_a shm_a
-// (x_{-2} - 16 x_{-1} - 16 x_{+1} + x_{+2}), zero outside the grid.
+// (x_{-2} - 16 x_{-1} - 16 x_{+1} + x_{+2}), zero outside the grid.  Every
+// neighbour load is issued unconditionally (from x_k where the neighbour is
+// off the grid or the axis absent) so that no branch separates a point's
+// loads from the next point's; the sums skip the off-grid terms as before.
 __device__ __forceinline__ double apply_h(const SilArgs& a, const double* x, int k, double d) {
+  const int kq = k / a.nx;
+  const int idx[3] = {k - kq * a.nx, a.ndim > 1 ? kq % a.ny : 0, a.ndim > 2 ? kq / a.ny : 0};
+  const int len[3] = {a.nx, a.ny, a.nz}, str[3] = {1, a.nx, a.nx * a.ny};
+  double xm2[3], xm1[3], xp1[3], xp2[3];
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    const bool on = ax < a.ndim;
+    const int i = idx[ax], st = str[ax], L = len[ax];
+    xm2[ax] = __ldcg(x + (on && i >= 2 ? k - 2 * st : k));
+    xm1[ax] = __ldcg(x + (on && i >= 1 ? k - st : k));
+    xp1[ax] = __ldcg(x + (on && i + 1 < L ? k + st : k));
+    xp2[ax] = __ldcg(x + (on && i + 2 < L ? k + 2 * st : k));
+  }
   double s = (a.sht30 + __ldg(a.vpot + k)) * (__ldcg(x + k) * d);
-  int idx[3], len[3] = {a.nx, a.ny, a.nz}, str[3];
-  idx[0] = k % a.nx;
-  str[0] = 1;
-  if (a.ndim > 1) {
-    idx[1] = (k / a.nx) % a.ny;
-    str[1] = a.nx;
-  }
-  if (a.ndim > 2) {
-    idx[2] = k / (a.nx * a.ny);
-    str[2] = a.nx * a.ny;
-  }
-  for (int ax = 0; ax < a.ndim; ++ax) {
+#pragma unroll
+  for (int ax = 0; ax < 3; ++ax) {
+    if (ax >= a.ndim) break;
     const double h = a.shm[ax];
-    const int i = idx[ax], st = str[ax];
-    if (i >= 2) s += h * (__ldcg(x + k - 2 * st) * d);
-    if (i >= 1) s += -16.0 * h * (__ldcg(x + k - st) * d);
-    if (i + 1 < len[ax]) s += -16.0 * h * (__ldcg(x + k + st) * d);
-    if (i + 2 < len[ax]) s += h * (__ldcg(x + k + 2 * st) * d);
+    const int i = idx[ax], L = len[ax];
+    if (i >= 2) s += h * (xm2[ax] * d);
+    if (i >= 1) s += -16.0 * h * (xm1[ax] * d);
+    if (i + 1 < L) s += -16.0 * h * (xp1[ax] * d);
+    if (i + 2 < L) s += h * (xp2[ax] * d);
   }
   return s;
 }
@@ -360,41 +367,45 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 #pragma unroll
         for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) acc[i] = 0.0;
         if (act) {
-          // two points per thread at a time, stores after both: their loads
-          // are in flight together
-          for (int k0 = r.lo + t; k0 < r.hi; k0 += 2 * kSilThreads) {
-            double vis[2], ws2[2];
+          // vi and w at point k, the iteration's dot products accumulated
+          auto point = [&](int k, double& vi_out, double& w_out) {
+            double lq[kSilMaxM];
 #pragma unroll
-            for (int j = 0; j < 2; ++j) {
-              const int k = k0 + j * kSilThreads;
-              if (k >= r.hi) continue;
-              double lq[kSilMaxM];
+            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
+            const double vi = __ldcg(src + k) * rb;
+            const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
+            double hv = apply_h(a, src, k, rb);
+            if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
+            const double w = hv - bt0 * vprev;
+            const double xk = __ldcg(x + k);
+            vi_out = vi;
+            w_out = w;
+            acc[0] += vi * w;
+            acc[1] += vi * xk;
+            acc[2] += vi * vi;
 #pragma unroll
-              for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
-              const double vi = __ldcg(src + k) * rb;
-              const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
-              double hv = apply_h(a, src, k, rb);
-              if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
-              const double w = hv - bt0 * vprev;
-              const double xk = __ldcg(x + k);
-              vis[j] = vi;
-              ws2[j] = w;
-              acc[0] += vi * w;
-              acc[1] += vi * xk;
-              acc[2] += vi * vi;
-#pragma unroll
-              for (int q = 0; q < kSilMaxM; ++q) {
-                acc[3 + q] += w * lq[q];
-                acc[3 + kSilMaxM + q] += vi * lq[q];
-              }
+            for (int q = 0; q < kSilMaxM; ++q) {
+              acc[3 + q] += w * lq[q];
+              acc[3 + kSilMaxM + q] += vi * lq[q];
             }
-#pragma unroll
-            for (int j = 0; j < 2; ++j) {
-              const int k = k0 + j * kSilThreads;
-              if (k >= r.hi) continue;
-              Lc[(long)it * n + k] = vis[j];
-              a.wbuf[c * n + k] = ws2[j];
-            }
+          };
+          // two points per thread at a time with no branch between them and
+          // the stores after both, so their loads are in flight together
+          int k0 = r.lo + t;
+          for (; k0 + kSilThreads < r.hi; k0 += 2 * kSilThreads) {
+            double vi0, w0, vi1, w1;
+            point(k0, vi0, w0);
+            point(k0 + kSilThreads, vi1, w1);
+            Lc[(long)it * n + k0] = vi0;
+            a.wbuf[c * n + k0] = w0;
+            Lc[(long)it * n + k0 + kSilThreads] = vi1;
+            a.wbuf[c * n + k0 + kSilThreads] = w1;
+          }
+          for (; k0 < r.hi; k0 += kSilThreads) {
+            double vi0, w0;
+            point(k0, vi0, w0);
+            Lc[(long)it * n + k0] = vi0;
+            a.wbuf[c * n + k0] = w0;
           }
         } else {
           for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
@@ -504,6 +515,75 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 // (with the reference's copy defect on request), then steps of CST.
 constexpr int kPsodIlp = 4;
 
+// psi_{n-1}(k) <- psi_{n-1}(k) - i c H psi_n(k) with absorber KABS (0 none,
+// 1 .VOPTIC, 2 .SMOOTHW) and, with DM, the field term; returns the new value
+template <int KABS, bool DM>
+__device__ __forceinline__ void psod_point(const SilArgs& a, const double* un, const double* vn,
+                                           const double* um, const double* vm, int k, double c,
+                                           double e, double& nu, double& nv) {
+  const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
+  double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
+  if (DM) {
+    const double de = __ldg(a.dm + k) * e;
+    hv -= de * vk;
+    hu -= de * uk;
+  }
+  if (KABS == 1) {
+    const double w = a.vabc[k];
+    nu = um[k] + c * hv - c * w * uk;
+    nv = vm[k] - c * hu - c * w * vk;
+  } else if (KABS == 2) {
+    const double w = a.vabc[k];
+    nu = w * (um[k] + c * hv);
+    nv = w * (vm[k] - c * hu);
+  } else {
+    nu = um[k] + c * hv;
+    nv = vm[k] - c * hu;
+  }
+}
+
+// one PSOD step over the CTA's points, kPsodIlp points per thread at a time
+// with all their loads issued before the first store (no branch between
+// them), then the rest one by one; q gets <psi0|psi_{n+1}>'s four sums in
+// point order
+template <int KABS, bool DM>
+__device__ void psod_points(const SilArgs& a, Range r, const double* un, const double* vn,
+                            double* um, double* vm, double c, double e, double (&q)[4]) {
+  const int t = threadIdx.x;
+  int k0 = r.lo + t;
+  for (; k0 + (kPsodIlp - 1) * kSilThreads < r.hi; k0 += kPsodIlp * kSilThreads) {
+    double nu[kPsodIlp], nv[kPsodIlp], u0k[kPsodIlp], v0k[kPsodIlp];
+#pragma unroll
+    for (int j = 0; j < kPsodIlp; ++j) {
+      const int k = k0 + j * kSilThreads;
+      psod_point<KABS, DM>(a, un, vn, um, vm, k, c, e, nu[j], nv[j]);
+      u0k[j] = __ldg(a.u0 + k);
+      v0k[j] = __ldg(a.v0 + k);
+    }
+#pragma unroll
+    for (int j = 0; j < kPsodIlp; ++j) {
+      const int k = k0 + j * kSilThreads;
+      um[k] = nu[j];
+      vm[k] = nv[j];
+      q[0] += u0k[j] * nu[j];
+      q[1] += v0k[j] * nv[j];
+      q[2] += u0k[j] * nv[j];
+      q[3] += v0k[j] * nu[j];
+    }
+  }
+  for (; k0 < r.hi; k0 += kSilThreads) {
+    double nu, nv;
+    psod_point<KABS, DM>(a, un, vn, um, vm, k0, c, e, nu, nv);
+    const double u0k = __ldg(a.u0 + k0), v0k = __ldg(a.v0 + k0);
+    um[k0] = nu;
+    vm[k0] = nv;
+    q[0] += u0k * nu;
+    q[1] += v0k * nv;
+    q[2] += u0k * nv;
+    q[3] += v0k * nu;
+  }
+}
+
 __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
   __shared__ double s_red[kSilThreads];
@@ -522,48 +602,14 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   auto step = [&](double c, int slot, long call) -> bool {
     double q[4] = {0.0, 0.0, 0.0, 0.0};
     const double e = a.ef ? a.ef[call] : 0.0;  // chpot.f:46-50: V - DM EF
-    // kPsodIlp points per thread at a time: all their loads are issued before
-    // the first store, so they are in flight together (a store to psi_{n-1}
-    // would otherwise hold back the next point's loads)
-    for (int k0 = r.lo + t; k0 < r.hi; k0 += kPsodIlp * kSilThreads) {
-      double nu[kPsodIlp], nv[kPsodIlp], u0k[kPsodIlp], v0k[kPsodIlp];
-#pragma unroll
-      for (int j = 0; j < kPsodIlp; ++j) {
-        const int k = k0 + j * kSilThreads;
-        if (k >= r.hi) continue;
-        const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
-        double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
-        if (a.dm) {
-          const double de = __ldg(a.dm + k) * e;
-          hv -= de * vk;
-          hu -= de * uk;
-        }
-        if (a.kabs == 1) {
-          const double w = a.vabc[k];
-          nu[j] = um[k] + c * hv - c * w * uk;
-          nv[j] = vm[k] - c * hu - c * w * vk;
-        } else if (a.kabs == 2) {
-          const double w = a.vabc[k];
-          nu[j] = w * (um[k] + c * hv);
-          nv[j] = w * (vm[k] - c * hu);
-        } else {
-          nu[j] = um[k] + c * hv;
-          nv[j] = vm[k] - c * hu;
-        }
-        u0k[j] = __ldg(a.u0 + k);
-        v0k[j] = __ldg(a.v0 + k);
-      }
-#pragma unroll
-      for (int j = 0; j < kPsodIlp; ++j) {
-        const int k = k0 + j * kSilThreads;
-        if (k >= r.hi) continue;
-        um[k] = nu[j];
-        vm[k] = nv[j];
-        q[0] += u0k[j] * nu[j];
-        q[1] += v0k[j] * nv[j];
-        q[2] += u0k[j] * nv[j];
-        q[3] += v0k[j] * nu[j];
-      }
+    const int kind = a.kabs + (a.dm ? 3 : 0);
+    switch (kind) {  // the absorber and the field as template arguments
+      case 0: psod_points<0, false>(a, r, un, vn, um, vm, c, e, q); break;
+      case 1: psod_points<1, false>(a, r, un, vn, um, vm, c, e, q); break;
+      case 2: psod_points<2, false>(a, r, un, vn, um, vm, c, e, q); break;
+      case 3: psod_points<0, true>(a, r, un, vn, um, vm, c, e, q); break;
+      case 4: psod_points<1, true>(a, r, un, vn, um, vm, c, e, q); break;
+      default: psod_points<2, true>(a, r, un, vn, um, vm, c, e, q); break;
     }
     if (!reduce_c(q, slot)) return false;
     double* x = un;
