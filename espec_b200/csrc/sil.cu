@@ -33,6 +33,13 @@ __device__ __forceinline__ Range my_range(long n) {
   return Range{(int)lo, (int)hi};
 }
 
+// Loads of state that other CTAs wrote before the last grid barrier: plain
+// loads.  The barrier's acquire (thread 0) and bar.sync order them after the
+// writers' release, so the memory model gives them the written values; unlike
+// the volatile __ldcg they leave the compiler free to issue several points'
+// loads together.
+__device__ __forceinline__ double ld_state(const double* p) { return *p; }
+
 // Grid barrier fused with a reduction: sp[0..nq) holds this CTA's partial
 // sums; on return st[0..nq) holds the totals over all CTAs.  After the
 // barrier every CTA sums the G partials itself, in one fixed order, so all
@@ -145,15 +152,64 @@ __device__ __forceinline__ double apply_h(const SilArgs& a, const double* x, int
   for (int ax = 0; ax < 3; ++ax) {
     const bool on = ax < a.ndim;
     const int i = idx[ax], st = str[ax], L = len[ax];
-    xm2[ax] = __ldcg(x + (on && i >= 2 ? k - 2 * st : k));
-    xm1[ax] = __ldcg(x + (on && i >= 1 ? k - st : k));
-    xp1[ax] = __ldcg(x + (on && i + 1 < L ? k + st : k));
-    xp2[ax] = __ldcg(x + (on && i + 2 < L ? k + 2 * st : k));
+    xm2[ax] = ld_state(x + (on && i >= 2 ? k - 2 * st : k));
+    xm1[ax] = ld_state(x + (on && i >= 1 ? k - st : k));
+    xp1[ax] = ld_state(x + (on && i + 1 < L ? k + st : k));
+    xp2[ax] = ld_state(x + (on && i + 2 < L ? k + 2 * st : k));
   }
-  double s = (a.sht30 + __ldg(a.vpot + k)) * (__ldcg(x + k) * d);
+  double s = (a.sht30 + __ldg(a.vpot + k)) * (ld_state(x + k) * d);
 #pragma unroll
   for (int ax = 0; ax < 3; ++ax) {
     if (ax >= a.ndim) break;
+    const double h = a.shm[ax];
+    const int i = idx[ax], L = len[ax];
+    if (i >= 2) s += h * (xm2[ax] * d);
+    if (i >= 1) s += -16.0 * h * (xm1[ax] * d);
+    if (i + 1 < L) s += -16.0 * h * (xp1[ax] * d);
+    if (i + 2 < L) s += h * (xp2[ax] * d);
+  }
+  return s;
+}
+
+// (x, y, z) indices of point k on an NDIM grid, x fastest.  (k + 1/2)/nx
+// by one FP64 multiplication: its rounding error (< k 2^-52) is far below the
+// 1/(2 nx) distance to the nearest integer, so the truncation is exact.
+template <int NDIM>
+__device__ __forceinline__ void grid_index(const SilArgs& a, int k, int (&idx)[3]) {
+  idx[1] = idx[2] = 0;
+  if (NDIM == 1) {
+    idx[0] = k;
+  } else {
+    const int q = (int)(((double)k + 0.5) * a.inv_nx);
+    idx[0] = k - q * a.nx;
+    if (NDIM == 2) {
+      idx[1] = q;
+    } else {
+      const int z = (int)(((double)q + 0.5) * a.inv_ny);
+      idx[1] = q - z * a.ny;
+      idx[2] = z;
+    }
+  }
+}
+
+// apply_h for a known NDIM with the point's indices given: the same terms in
+// the same order, only the axes that exist
+template <int NDIM>
+__device__ __forceinline__ double apply_h_nd(const SilArgs& a, const double* x, int k, double d,
+                                             const int (&idx)[3]) {
+  const int len[3] = {a.nx, a.ny, a.nz}, str[3] = {1, a.nx, a.nx * a.ny};
+  double xm2[NDIM], xm1[NDIM], xp1[NDIM], xp2[NDIM];
+#pragma unroll
+  for (int ax = 0; ax < NDIM; ++ax) {
+    const int i = idx[ax], st = str[ax], L = len[ax];
+    xm2[ax] = ld_state(x + (i >= 2 ? k - 2 * st : k));
+    xm1[ax] = ld_state(x + (i >= 1 ? k - st : k));
+    xp1[ax] = ld_state(x + (i + 1 < L ? k + st : k));
+    xp2[ax] = ld_state(x + (i + 2 < L ? k + 2 * st : k));
+  }
+  double s = (a.sht30 + __ldg(a.vpot + k)) * (ld_state(x + k) * d);
+#pragma unroll
+  for (int ax = 0; ax < NDIM; ++ax) {
     const double h = a.shm[ax];
     const int i = idx[ax], L = len[ax];
     if (i >= 2) s += h * (xm2[ax] * d);
@@ -327,7 +383,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
     {
       double q[6] = {0, 0, 0, 0, 0, 0};
       for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-        const double uk = __ldcg(a.u + k), vk = __ldcg(a.v + k);
+        const double uk = ld_state(a.u + k), vk = ld_state(a.v + k);
         const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
         q[0] += uk * uk;
         q[1] += vk * vk;
@@ -371,13 +427,13 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
           auto point = [&](int k, double& vi_out, double& w_out) {
             double lq[kSilMaxM];
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? __ldcg(Lc + (long)q * n + k) : 0.0;
-            const double vi = __ldcg(src + k) * rb;
-            const double vprev = it ? __ldcg(Lc + (long)(it - 1) * n + k) : 0.0;
+            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? ld_state(Lc + (long)q * n + k) : 0.0;
+            const double vi = ld_state(src + k) * rb;
+            const double vprev = it ? ld_state(Lc + (long)(it - 1) * n + k) : 0.0;
             double hv = apply_h(a, src, k, rb);
             if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
             const double w = hv - bt0 * vprev;
-            const double xk = __ldcg(x + k);
+            const double xk = ld_state(x + k);
             vi_out = vi;
             w_out = w;
             acc[0] += vi * w;
@@ -445,8 +501,8 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
           const double* Lc = a.L + (long)c * m * n;
           double lq[kSilMaxM + 1];
 #pragma unroll
-          for (int q = 0; q <= kSilMaxM; ++q) lq[q] = q <= it ? __ldcg(Lc + (long)q * n + k) : 0.0;
-          double acc = __ldcg(a.wbuf + c * n + k);
+          for (int q = 0; q <= kSilMaxM; ++q) lq[q] = q <= it ? ld_state(Lc + (long)q * n + k) : 0.0;
+          double acc = ld_state(a.wbuf + c * n + k);
           double vi = 0.0;
 #pragma unroll
           for (int q = 0; q <= kSilMaxM; ++q)
@@ -479,8 +535,8 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
       double lu[kSilMaxM], lv[kSilMaxM];
 #pragma unroll
       for (int j = 0; j < kSilMaxM; ++j) {
-        lu[j] = j < m ? __ldcg(Lu + (long)j * n + k) : 0.0;
-        lv[j] = j < m ? __ldcg(Lv + (long)j * n + k) : 0.0;
+        lu[j] = j < m ? ld_state(Lu + (long)j * n + k) : 0.0;
+        lv[j] = j < m ? ld_state(Lv + (long)j * n + k) : 0.0;
       }
       double ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
 #pragma unroll
@@ -515,14 +571,35 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 // (with the reference's copy defect on request), then steps of CST.
 constexpr int kPsodIlp = 4;
 
+template <int KABS, bool DM, int NDIM>
+__device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const double* un,
+                                            const double* vn, double* um, double* vm, double c,
+                                            double e, double (&q)[4]);
+
+template <int NDIM>
+__device__ __forceinline__ void psod_dispatch(const SilArgs& a, Range r, const double* un,
+                                              const double* vn, double* um, double* vm, double c,
+                                              double e, double (&q)[4]) {
+  switch (a.kabs + (a.dm ? 3 : 0)) {
+    case 0: psod_points<0, false, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
+    case 1: psod_points<1, false, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
+    case 2: psod_points<2, false, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
+    case 3: psod_points<0, true, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
+    case 4: psod_points<1, true, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
+    default: psod_points<2, true, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
+  }
+}
+
 // psi_{n-1}(k) <- psi_{n-1}(k) - i c H psi_n(k) with absorber KABS (0 none,
 // 1 .VOPTIC, 2 .SMOOTHW) and, with DM, the field term; returns the new value
-template <int KABS, bool DM>
+template <int KABS, bool DM, int NDIM>
 __device__ __forceinline__ void psod_point(const SilArgs& a, const double* un, const double* vn,
                                            const double* um, const double* vm, int k, double c,
                                            double e, double& nu, double& nv) {
-  const double uk = __ldcg(un + k), vk = __ldcg(vn + k);
-  double hv = apply_h(a, vn, k, 1.0), hu = apply_h(a, un, k, 1.0);
+  const double uk = ld_state(un + k), vk = ld_state(vn + k);
+  int idx[3];
+  grid_index<NDIM>(a, k, idx);
+  double hv = apply_h_nd<NDIM>(a, vn, k, 1.0, idx), hu = apply_h_nd<NDIM>(a, un, k, 1.0, idx);
   if (DM) {
     const double de = __ldg(a.dm + k) * e;
     hv -= de * vk;
@@ -546,9 +623,10 @@ __device__ __forceinline__ void psod_point(const SilArgs& a, const double* un, c
 // with all their loads issued before the first store (no branch between
 // them), then the rest one by one; q gets <psi0|psi_{n+1}>'s four sums in
 // point order
-template <int KABS, bool DM>
-__device__ void psod_points(const SilArgs& a, Range r, const double* un, const double* vn,
-                            double* um, double* vm, double c, double e, double (&q)[4]) {
+template <int KABS, bool DM, int NDIM>
+__device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const double* un,
+                                            const double* vn, double* um, double* vm, double c,
+                                            double e, double (&q)[4]) {
   const int t = threadIdx.x;
   int k0 = r.lo + t;
   for (; k0 + (kPsodIlp - 1) * kSilThreads < r.hi; k0 += kPsodIlp * kSilThreads) {
@@ -556,7 +634,7 @@ __device__ void psod_points(const SilArgs& a, Range r, const double* un, const d
 #pragma unroll
     for (int j = 0; j < kPsodIlp; ++j) {
       const int k = k0 + j * kSilThreads;
-      psod_point<KABS, DM>(a, un, vn, um, vm, k, c, e, nu[j], nv[j]);
+      psod_point<KABS, DM, NDIM>(a, un, vn, um, vm, k, c, e, nu[j], nv[j]);
       u0k[j] = __ldg(a.u0 + k);
       v0k[j] = __ldg(a.v0 + k);
     }
@@ -573,7 +651,7 @@ __device__ void psod_points(const SilArgs& a, Range r, const double* un, const d
   }
   for (; k0 < r.hi; k0 += kSilThreads) {
     double nu, nv;
-    psod_point<KABS, DM>(a, un, vn, um, vm, k0, c, e, nu, nv);
+    psod_point<KABS, DM, NDIM>(a, un, vn, um, vm, k0, c, e, nu, nv);
     const double u0k = __ldg(a.u0 + k0), v0k = __ldg(a.v0 + k0);
     um[k0] = nu;
     vm[k0] = nv;
@@ -584,6 +662,7 @@ __device__ void psod_points(const SilArgs& a, Range r, const double* un, const d
   }
 }
 
+template <int NDIM>
 __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
   __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
   __shared__ double s_red[kSilThreads];
@@ -599,18 +678,11 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
       a.c_out[slot] = make_double2(st[0] + st[1], st[2] - st[3]);
     return true;
   };
-  auto step = [&](double c, int slot, long call) -> bool {
+  auto step = [&](double c, int slot, long call) __attribute__((always_inline)) -> bool {
     double q[4] = {0.0, 0.0, 0.0, 0.0};
     const double e = a.ef ? a.ef[call] : 0.0;  // chpot.f:46-50: V - DM EF
-    const int kind = a.kabs + (a.dm ? 3 : 0);
-    switch (kind) {  // the absorber and the field as template arguments
-      case 0: psod_points<0, false>(a, r, un, vn, um, vm, c, e, q); break;
-      case 1: psod_points<1, false>(a, r, un, vn, um, vm, c, e, q); break;
-      case 2: psod_points<2, false>(a, r, un, vn, um, vm, c, e, q); break;
-      case 3: psod_points<0, true>(a, r, un, vn, um, vm, c, e, q); break;
-      case 4: psod_points<1, true>(a, r, un, vn, um, vm, c, e, q); break;
-      default: psod_points<2, true>(a, r, un, vn, um, vm, c, e, q); break;
-    }
+    // the absorber, the field and the dimension as template arguments
+    psod_dispatch<NDIM>(a, r, un, vn, um, vm, c, e, q);
     if (!reduce_c(q, slot)) return false;
     double* x = un;
     un = um;
@@ -762,6 +834,8 @@ static SilArgs sil_args(const espec_grid_plan* p) {
   double sht = 0.0;
   for (int i = 0; i < p->ndim; ++i) sht += p->shm[i];
   a.sht30 = 30.0 * sht;
+  a.inv_nx = 1.0 / p->np[0];
+  a.inv_ny = 1.0 / p->np[1];
   a.vpot = p->d_vpot;
   a.mask = p->absorb == ESPEC_ABS_SMOOTHW ? p->d_mask : nullptr;
   a.u = p->d_u;
@@ -833,7 +907,7 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, psod ? psod_kernel : sil_kernel,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, psod ? psod_kernel<3> : sil_kernel,
                                                       kSilThreads, 0);
   if (e != cudaSuccess) {
     delete p;
@@ -926,7 +1000,10 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
     if (p->d_dm && a.slot0 + nsteps >= p->n_ef)
       return set_error(ESPEC_EINVAL, "the pulse field table ends before the run does");
     void* args[] = {&a};
-    GRID_CK(cudaLaunchCooperativeKernel((const void*)psod_kernel, dim3(p->nblocks),
+    const void* kern = p->ndim == 1   ? (const void*)psod_kernel<1>
+                       : p->ndim == 2 ? (const void*)psod_kernel<2>
+                                      : (const void*)psod_kernel<3>;
+    GRID_CK(cudaLaunchCooperativeKernel(kern, dim3(p->nblocks),
                                         dim3(kSilThreads), args, 0, st));
     // the kernel swaps the roles of the two state buffers once per step
     const long swaps = from_start ? (nsteps >= 1 ? nsteps + 1 : 0) : nsteps;
