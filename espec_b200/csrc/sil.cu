@@ -361,6 +361,7 @@ __device__ __forceinline__ void warp_sums(const double (&acc)[3 + 2 * kSilMaxM],
   }
 }
 
+template <int NDIM>
 __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   __shared__ double sp[kSilNQ], st[kSilNQ], scratch[(kSilThreads / 32) * 8];
   __shared__ double ws[(kSilThreads / 32) * kSilNQ];
@@ -424,13 +425,15 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) acc[i] = 0.0;
         if (act) {
           // vi and w at point k, the iteration's dot products accumulated
-          auto point = [&](int k, double& vi_out, double& w_out) {
+          auto point = [&](int k, double& vi_out, double& w_out) __attribute__((always_inline)) {
             double lq[kSilMaxM];
 #pragma unroll
             for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? ld_state(Lc + (long)q * n + k) : 0.0;
             const double vi = ld_state(src + k) * rb;
             const double vprev = it ? ld_state(Lc + (long)(it - 1) * n + k) : 0.0;
-            double hv = apply_h(a, src, k, rb);
+            int idx[3];
+            grid_index<NDIM>(a, k, idx);
+            double hv = apply_h_nd<NDIM>(a, src, k, rb, idx);
             if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
             const double w = hv - bt0 * vprev;
             const double xk = ld_state(x + k);
@@ -907,7 +910,7 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, psod ? psod_kernel<3> : sil_kernel,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, psod ? psod_kernel<3> : sil_kernel<3>,
                                                       kSilThreads, 0);
   if (e != cudaSuccess) {
     delete p;
@@ -1019,7 +1022,10 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
   if (p->d_dm && a.slot0 + nsteps >= p->n_ef)
     return set_error(ESPEC_EINVAL, "the pulse field table ends before the run does");
   void* args[] = {&a};
-  GRID_CK(cudaLaunchCooperativeKernel((const void*)sil_kernel, dim3(p->nblocks), dim3(kSilThreads),
+  const void* kern = p->ndim == 1   ? (const void*)sil_kernel<1>
+                     : p->ndim == 2 ? (const void*)sil_kernel<2>
+                                    : (const void*)sil_kernel<3>;
+  GRID_CK(cudaLaunchCooperativeKernel(kern, dim3(p->nblocks), dim3(kSilThreads),
                                       args, 0, st));
   p->slot = a.slot0 + nsteps;
   return ESPEC_OK;
