@@ -360,6 +360,93 @@ std::string lnz_order_text(int nreort, int lmtreort, bool change) {
   return s;
 }
 
+// ------------------------------------------------------------------------
+// Shared by the pulse drop-ins (PPSOD, PPLNZ)
+// ------------------------------------------------------------------------
+
+// DIM of a grid drop-in: 1, 2 or 3; 0 if not one of those
+int grid_dim(const char* dim, size_t len) {
+  if (fstr_is(dim, len, ".1D")) return 1;
+  if (fstr_is(dim, len, ".2D")) return 2;
+  if (fstr_is(dim, len, ".3D")) return 3;
+  return 0;
+}
+
+// EFC (ef.f:44-60) and its parameters in espec_pulse_field's order; -1 when
+// the pulse is not known
+int pulse_shape(const char* efc, size_t len, double e0, double tp, double omg, double t0,
+                double td, double sni, int kl, double (&par)[6]) {
+  int shape = -1;
+  if (fstr_is(efc, len, ".GAUS")) shape = ESPEC_PULSE_GAUS;
+  else if (fstr_is(efc, len, ".GGAUS")) shape = ESPEC_PULSE_GGAUS;
+  else if (fstr_is(efc, len, ".SIN2")) shape = ESPEC_PULSE_SIN2;
+  else if (fstr_is(efc, len, ".NONE") || fstr_is(efc, len, ".NULL")) shape = ESPEC_PULSE_NONE;
+  const double p[6] = {e0, tp, omg, shape == ESPEC_PULSE_SIN2 ? td : t0, sni, (double)kl};
+  for (int i = 0; i < 6; ++i) par[i] = p[i];
+  return shape;
+}
+
+// the lines before a pulse table's column titles: a blank record, the title
+// ('Auto-' when DIM .EQ. '.1D'), its rule and FORMAT 1011's leading empty record
+std::string pulse_title(const char* dim, size_t len) {
+  const bool one = len >= 3 && std::memcmp(dim, ".1D", 3) == 0 &&
+                   std::string(dim + 3, len - 3).find_first_not_of(' ') == std::string::npos;
+  return std::string(" \n") + (one ? " Auto-correlation function:\n"
+                                    : " Partial auto-correlation function:\n") +
+         " ==================================\n\n";
+}
+
+// the column titles common to both tables (FORMAT 1011 up to the groups)
+const char* kPulseCols = "        *t/fs*     *ET/a.u.*      *E0/a.u.*      *Pr(t)*    *Pi(t)*   ";
+
+// a grid plan and the device copy of the projection vectors, freed together
+struct PulsePlan {
+  espec_grid_plan* plan = nullptr;
+  double* d_w = nullptr;
+  int nw = 0;
+  PulsePlan() = default;
+  PulsePlan(const PulsePlan&) = delete;
+  PulsePlan& operator=(const PulsePlan&) = delete;
+  ~PulsePlan() {
+    espec_grid_destroy(plan);
+    if (d_w) cudaFree(d_w);
+  }
+  // W_k = LNZVC(1:N, KP+k), k = 1..nw (leading dimension MXDCT)
+  bool load_w(const double* lnzvc, long mxdct, int kp, int count, long n) {
+    nw = count;
+    if (count <= 0) return true;
+    if (cudaMalloc(&d_w, sizeof(double) * n * count) != cudaSuccess) return false;
+    for (int k = 0; k < count; ++k)
+      if (cudaMemcpy(d_w + (size_t)k * n, lnzvc + (size_t)(kp + k) * mxdct, sizeof(double) * n,
+                     cudaMemcpyHostToDevice) != cudaSuccess)
+        return false;
+    return true;
+  }
+};
+
+// what a printed row needs from the state on the device: the energy with the
+// field EF and without it, the norm, and <W_k|u>, <W_k|v> per vector
+struct PulseRow {
+  double et = 0, e0 = 0, fnr = 0;
+  std::vector<double> pj;
+  double pop(int k) const { return pj[2 * k] * pj[2 * k] + pj[2 * k + 1] * pj[2 * k + 1]; }
+};
+
+int measure_row(PulsePlan& pp, double ef, PulseRow& r) {
+  double nr0;
+  r.pj.assign(2 * (size_t)std::max(pp.nw, 1), 0.0);
+  if (int rc = espec_grid_energies_at(pp.plan, ef, &r.et, &r.fnr, nullptr)) return rc;
+  if (int rc = espec_grid_energies_at(pp.plan, 0.0, &r.e0, &nr0, nullptr)) return rc;
+  if (pp.nw > 0) return espec_grid_project(pp.plan, pp.d_w, pp.nw, r.pj.data(), nullptr);
+  return ESPEC_OK;
+}
+
+// FORMAT 1021 up to Ci: (1X,F14.6,3X,2(E12.6,3X),2(F8.5,3X) ...
+std::string pulse_row_start(double t, const PulseRow& r, double cr, double ci) {
+  return " " + fmt_f(t, 14, 6) + "   " + fmt_e(r.et, 12, 6) + "   " + fmt_e(r.e0, 12, 6) + "   " +
+         fmt_f(cr, 8, 5) + "   " + fmt_f(ci, 8, 5);
+}
+
 }  // namespace
 
 extern "C" void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
@@ -646,10 +733,7 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
     std::fprintf(stderr, "espec_gpu PPSOD: %s\n", why);
     *info = 2;
   };
-  int ndim = 0;
-  if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
-  if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
-  if (fstr_is(dim, dim_len, ".3D")) ndim = 3;
+  const int ndim = grid_dim(dim, dim_len);
   if (!ndim) return fail("DIM must be '.1D', '.2D' or '.3D'");
   long npts = 1;
   for (int a = 0; a < ndim; ++a) npts *= np[a];
@@ -657,13 +741,9 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
   if (*lc < 1) return fail("LC must be at least 1");
   if (*npr_in > 6) return fail("NPR must be at most 6 (rdinput.f:660)");
   const int npr = std::max(*npr_in, 0);  // NPR < 1: no projections (ppsod.f:99-104)
-  int shape = -1;  // ef.f:44-60
-  if (fstr_is(efc, efc_len, ".GAUS")) shape = ESPEC_PULSE_GAUS;
-  else if (fstr_is(efc, efc_len, ".GGAUS")) shape = ESPEC_PULSE_GGAUS;
-  else if (fstr_is(efc, efc_len, ".SIN2")) shape = ESPEC_PULSE_SIN2;
-  else if (fstr_is(efc, efc_len, ".NONE") || fstr_is(efc, efc_len, ".NULL")) shape = ESPEC_PULSE_NONE;
+  double par[6];
+  const int shape = pulse_shape(efc, efc_len, *e0, *tp, *omg, *t0, *td, *sni, *kl, par);
   if (shape < 0) return fail("desired laser pulse wasn't found (ef.f:58-60)");
-  const double par[6] = {*e0, *tp, *omg, shape == ESPEC_PULSE_SIN2 ? *td : *t0, *sni, (double)*kl};
   int ab = ESPEC_ABS_NONE;  // sod.f:71-82
   if (*absorb) {
     if (fstr_is(tpabsor, tpabsor_len, ".VOPTIC")) ab = ESPEC_ABS_VOPTIC;
@@ -680,58 +760,25 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
   if (ncalls < 2) return fail(espec_last_error());
   const int nsteps = (int)ncalls - 1;  // slot 1: the start-up; slot s >= 2: loop step s - 1
   std::vector<double> vp(vpot, vpot + nn);
-  espec_grid_plan* plan = nullptr;
-  double* d_w = nullptr;
-  struct Guard {
-    espec_grid_plan*& p;
-    double*& w;
-    ~Guard() {
-      espec_grid_destroy(p);
-      if (w) cudaFree(w);
-    }
-  } guard{plan, d_w};
-  if (espec_grid_create(&plan, ESPEC_PSOD, ndim, np, shm, *dt, 0, ESPEC_FP64, ab, 0) ||
-      espec_grid_load(plan, vp.data(), ab == ESPEC_ABS_NONE ? nullptr : vabc, u1, v1,
+  PulsePlan pp;
+  if (espec_grid_create(&pp.plan, ESPEC_PSOD, ndim, np, shm, *dt, 0, ESPEC_FP64, ab, 0) ||
+      espec_grid_load(pp.plan, vp.data(), ab == ESPEC_ABS_NONE ? nullptr : vabc, u1, v1,
                       ESPEC_MEM_HOST, nullptr) ||
-      espec_grid_set_pulse(plan, dm, ef.data(), ncalls, ESPEC_MEM_HOST))
+      espec_grid_set_pulse(pp.plan, dm, ef.data(), ncalls, ESPEC_MEM_HOST))
     return fail(espec_last_error());
-  if (npr > 0) {  // W_k = LNZVC(:, KP+k) (ppsod.f:99-104)
-    if (cudaMalloc(&d_w, sizeof(double) * nn * npr) != cudaSuccess) return fail("device memory");
-    for (int k = 0; k < npr; ++k)
-      if (cudaMemcpy(d_w + (size_t)k * nn, lnzvc + (size_t)(*kp + k) * *mxdct, sizeof(double) * nn,
-                     cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail("copy of the projection vectors");
-  }
+  // W_k = LNZVC(:, KP+k), k = 1..NPR (ppsod.f:99-104)
+  if (!pp.load_w(lnzvc, *mxdct, *kp, npr, nn)) return fail("copy of the projection vectors");
   auto store = [&](long nc, double cr, double ci) {  // LNZVC(NC, MPR/MPI), NC from 1
     lnzvc[(nc - 1) + (long)(*mpr - 1) * *mxdct] = cr;
     lnzvc[(nc - 1) + (long)(*mpi - 1) * *mxdct] = ci;
   };
-  // the energies, populations and norm of the state on the device
-  struct Row {
-    double et = 0, e0 = 0, fnr = 0;
-    std::vector<double> pj;
-  };
-  auto measure = [&](double efs, Row& r) -> bool {
-    double nr0;
-    r.pj.assign(2 * (size_t)std::max(npr, 1), 0.0);
-    if (espec_grid_energies_at(plan, efs, &r.et, &r.fnr, nullptr) ||
-        espec_grid_energies_at(plan, 0.0, &r.e0, &nr0, nullptr) ||
-        (npr > 0 && espec_grid_project(plan, d_w, npr, r.pj.data(), nullptr))) {
-      fail(espec_last_error());
-      return false;
-    }
-    return true;
-  };
   double f0 = 0.0;
   // kind 0: the first row (sets F0), 1: the start-up row, 2: a loop row (drift
-  // test, ppsod.f:440-444)
-  auto print_row = [&](double t, const Row& m, double cr, double ci, int kind) {
-    // FORMAT 1021: (1X,F14.6,3X,E12.6,3X,E12.6,2(3X,F8.5),(3X,F8.6)...)
-    std::string row = " " + fmt_f(t, 14, 6) + "   " + fmt_e(m.et, 12, 6) + "   " +
-                      fmt_e(m.e0, 12, 6) + "   " + fmt_f(cr, 8, 5) + "   " + fmt_f(ci, 8, 5) +
-                      "   " + fmt_f(cr * cr + ci * ci, 8, 6);
-    for (int k = 0; k < npr; ++k)
-      row += "   " + fmt_f(m.pj[2 * k] * m.pj[2 * k] + m.pj[2 * k + 1] * m.pj[2 * k + 1], 8, 6);
+  // test, ppsod.f:440-444).  FORMAT 1021: ..., (3X,F8.6) for |C|^2, the
+  // populations and the norm
+  auto print_row = [&](double t, const PulseRow& m, double cr, double ci, int kind) {
+    std::string row = pulse_row_start(t, m, cr, ci) + "   " + fmt_f(cr * cr + ci * ci, 8, 6);
+    for (int k = 0; k < npr; ++k) row += "   " + fmt_f(m.pop(k), 8, 6);
     row += "   " + fmt_f(m.fnr, 8, 6) + "\n";
     if (kind == 2 && ab == ESPEC_ABS_NONE && std::fabs((m.fnr - f0) / f0) * 1.0e2 > *tol) *info = 1;
     if (kind == 0) f0 = m.fnr;
@@ -756,16 +803,9 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
     if (prt == 2 || (prt == 1 && mc == 0)) printed[s] = 1;
   }
   long nc = 1;
-  std::vector<double> cre, cim;
   if (prt) {
-    // the table head (ppsod.f:172-200): the title, then FORMAT 1011 or 1012
-    std::string head = " \n";
-    head += (dim_len >= 3 && std::memcmp(dim, ".1D", 3) == 0 &&
-             std::string(dim + 3, dim_len - 3).find_first_not_of(' ') == std::string::npos)
-                ? " Auto-correlation function:\n"
-                : " Partial auto-correlation function:\n";
-    head += " ==================================\n\n";
-    head += "        *t/fs*     *ET/a.u.*      *E0/a.u.*      *Pr(t)*    *Pi(t)*   ";
+    // the table head (ppsod.f:172-200): FORMAT 1011 or 1012 (two-digit indices)
+    std::string head = pulse_title(dim, dim_len) + kPulseCols;
     const bool wide = *npr_in + *kp - 1 > 10;
     auto group = [&](const char* a, int i, const char* b, bool last) {
       char buf[32];
@@ -781,17 +821,18 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
   }
   // the first row: psi0 with the potential before any CHPOT (ET = E0,
   // ppsod.f:158-201), printed once the run has given C(0)
-  Row first;
-  if (prt && !measure(0.0, first)) return;
+  PulseRow first;
+  if (prt && measure_row(pp, 0.0, first)) return fail(espec_last_error());
   // the run, split at the printed slots and resumed on the device
+  std::vector<double> cre, cim;
   int done = 0;
   for (int s = 1; s <= nsteps; ++s) {
     if (!printed[s] && s != nsteps) continue;
     const int k = s - done;
     cre.resize(k + 1);
     cim.resize(k + 1);
-    if ((done == 0 ? espec_grid_run(plan, k, nullptr) : espec_grid_continue(plan, k, nullptr)) ||
-        espec_grid_results(plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST,
+    if ((done == 0 ? espec_grid_run(pp.plan, k, nullptr) : espec_grid_continue(pp.plan, k, nullptr)) ||
+        espec_grid_results(pp.plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST,
                            nullptr))
       return fail(espec_last_error());
     if (done == 0 && prt) {
@@ -805,15 +846,15 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
       // the time of slot s: TI + DT for the start-up, then T accumulating DT
       double t = *ti + *dt;
       for (int q = 2; q <= s; ++q) t = t + *dt;
-      Row m;
-      if (!measure(ef[s], m)) return;
+      PulseRow m;
+      if (measure_row(pp, ef[s], m)) return fail(espec_last_error());
       print_row(t, m, cre[k], cim[k], s >= 2 ? 2 : 1);
     }
   }
   if (done == 0) return fail("no steps");
   // psi(TF), psi(TF - dt), and VPOT as CHPOT leaves it
-  if (espec_grid_results(plan, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
-      espec_grid_previous(plan, u1, v1, ESPEC_MEM_HOST, nullptr))
+  if (espec_grid_results(pp.plan, nullptr, nullptr, u2, v2, ESPEC_MEM_HOST, nullptr) ||
+      espec_grid_previous(pp.plan, u1, v1, ESPEC_MEM_HOST, nullptr))
     return fail(espec_last_error());
   for (long i = 0; i < nn; ++i) vpot[i] = vp[i] - dm[i] * ef[nsteps];
   std::fflush(stdout);
@@ -849,10 +890,7 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
     std::fprintf(stderr, "espec_gpu PPLNZ: %s\n", why);
     *info = 2;
   };
-  int ndim = 0;
-  if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
-  if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
-  if (fstr_is(dim, dim_len, ".3D")) ndim = 3;
+  const int ndim = grid_dim(dim, dim_len);
   if (!ndim) return fail("DIM must be '.1D', '.2D' or '.3D'");
   long npts = 1;
   for (int a = 0; a < ndim; ++a) npts *= np[a];
@@ -861,13 +899,9 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
   if (*npr_in > 6) return fail("NPR must be at most 6 (rdinput.f:660)");
   const int npr = std::max(*npr_in, 0);
   const int nw = std::max(npr - 1, 0);  // printed projections: W_1 .. W_{NPR-1}
-  int shape = -1;  // ef.f:44-60
-  if (fstr_is(efc, efc_len, ".GAUS")) shape = ESPEC_PULSE_GAUS;
-  else if (fstr_is(efc, efc_len, ".GGAUS")) shape = ESPEC_PULSE_GGAUS;
-  else if (fstr_is(efc, efc_len, ".SIN2")) shape = ESPEC_PULSE_SIN2;
-  else if (fstr_is(efc, efc_len, ".NONE") || fstr_is(efc, efc_len, ".NULL")) shape = ESPEC_PULSE_NONE;
+  double par[6];
+  const int shape = pulse_shape(efc, efc_len, *e0, *tp, *omg, *t0, *td, *sni, *kl, par);
   if (shape < 0) return fail("desired laser pulse wasn't found (ef.f:58-60)");
-  const double par[6] = {*e0, *tp, *omg, shape == ESPEC_PULSE_SIN2 ? *td : *t0, *sni, (double)*kl};
   // LNZ's order test (lnz.f:64-72), as in PLNZ: with *CHANGE the first call
   // lowers MP to LMTREORT for good
   const int mp_in = *mp;
@@ -885,57 +919,26 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
   if (nfield < 1) return fail(espec_last_error());
   const int nsteps = (int)nfield - 1;  // step s lands at T_s and uses EF(T_s)
   std::vector<double> vp(vpot, vpot + nn);
-  espec_grid_plan* plan = nullptr;
-  double* d_w = nullptr;
-  struct Guard {
-    espec_grid_plan*& p;
-    double*& w;
-    ~Guard() {
-      espec_grid_destroy(p);
-      if (w) cudaFree(w);
-    }
-  } guard{plan, d_w};
-  if (espec_grid_create(&plan, ESPEC_SIL, ndim, np, shm, *dt, m, ESPEC_FP64, ab,
+  PulsePlan pp;
+  if (espec_grid_create(&pp.plan, ESPEC_SIL, ndim, np, shm, *dt, m, ESPEC_FP64, ab,
                         ESPEC_Q_SIL_INPLACE) ||
-      espec_grid_load(plan, vp.data(), ab == ESPEC_ABS_NONE ? nullptr : vabc, u, v,
+      espec_grid_load(pp.plan, vp.data(), ab == ESPEC_ABS_NONE ? nullptr : vabc, u, v,
                       ESPEC_MEM_HOST, nullptr) ||
-      espec_grid_set_pulse(plan, dm, ef.data(), nfield, ESPEC_MEM_HOST))
+      espec_grid_set_pulse(pp.plan, dm, ef.data(), nfield, ESPEC_MEM_HOST))
     return fail(espec_last_error());
-  if (nw > 0) {  // W_k = LNZVC(:, KP+k) (pplnz.f:93-98)
-    if (cudaMalloc(&d_w, sizeof(double) * nn * nw) != cudaSuccess) return fail("device memory");
-    for (int k = 0; k < nw; ++k)
-      if (cudaMemcpy(d_w + (size_t)k * nn, lnzvc + (size_t)(*kp + k) * *mxdct, sizeof(double) * nn,
-                     cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail("copy of the projection vectors");
-  }
+  // W_k = LNZVC(:, KP+k) (pplnz.f:93-98), the printed ones
+  if (!pp.load_w(lnzvc, *mxdct, *kp, nw, nn)) return fail("copy of the projection vectors");
   auto store = [&](long nc, double cr, double ci) {  // LNZVC(NC, MPR/MPI), NC from 1
     lnzvc[(nc - 1) + (long)(*mpr - 1) * *mxdct] = cr;
     lnzvc[(nc - 1) + (long)(*mpi - 1) * *mxdct] = ci;
   };
-  struct Row {
-    double et = 0, e0 = 0, fnr = 0;
-    std::vector<double> pj;
-  };
-  auto measure = [&](double efs, Row& r) -> bool {
-    double nr0;
-    r.pj.assign(2 * (size_t)std::max(nw, 1), 0.0);
-    if (espec_grid_energies_at(plan, efs, &r.et, &r.fnr, nullptr) ||
-        espec_grid_energies_at(plan, 0.0, &r.e0, &nr0, nullptr) ||
-        (nw > 0 && espec_grid_project(plan, d_w, nw, r.pj.data(), nullptr))) {
-      fail(espec_last_error());
-      return false;
-    }
-    return true;
-  };
   double f0 = 0.0;
-  auto print_row = [&](double t, const Row& r, double cr, double ci, bool first) {
+  // FORMAT 1021: ..., CT(1..NPR) = |C|^2 then the populations, FNT
+  auto print_row = [&](double t, const PulseRow& r, double cr, double ci, bool first) {
     const double fnt = first ? r.fnr * r.fnr : r.fnr;
-    // FORMAT 1021: (1X,F14.6,3X,2(E12.6,3X),2(F8.5,3X),10(F8.6,3X))
-    std::string row = " " + fmt_f(t, 14, 6) + "   " + fmt_e(r.et, 12, 6) + "   " +
-                      fmt_e(r.e0, 12, 6) + "   " + fmt_f(cr, 8, 5) + "   " + fmt_f(ci, 8, 5);
+    std::string row = pulse_row_start(t, r, cr, ci);
     if (npr >= 1) row += "   " + fmt_f(cr * cr + ci * ci, 8, 6);
-    for (int k = 0; k < nw; ++k)
-      row += "   " + fmt_f(r.pj[2 * k] * r.pj[2 * k] + r.pj[2 * k + 1] * r.pj[2 * k + 1], 8, 6);
+    for (int k = 0; k < nw; ++k) row += "   " + fmt_f(r.pop(k), 8, 6);
     row += "   " + fmt_f(fnt, 8, 6) + "\n";
     if (first) f0 = fnt;
     else if (!*absorb && std::fabs((fnt - f0) / f0) * 1.0e2 > *tol) *info = 1;
@@ -960,17 +963,11 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
     if (prt == 2 || (prt == 1 && mc == 0)) printed[s] = 1;
   }
   long nc = 1;
-  Row first;
+  PulseRow first;
   if (prt) {
-    if (!measure(0.0, first)) return;
-    std::string head = " \n";
-    head += (dim_len >= 3 && std::memcmp(dim, ".1D", 3) == 0 &&
-             std::string(dim + 3, dim_len - 3).find_first_not_of(' ') == std::string::npos)
-                ? " Auto-correlation function:\n"
-                : " Partial auto-correlation function:\n";
-    head += " ==================================\n\n";
+    if (measure_row(pp, 0.0, first)) return fail(espec_last_error());
     // FORMAT 1011 (pplnz.f:331-332): groups (A3,I1,A4) joined by 3X
-    head += "        *t/fs*     *ET/a.u.*      *E0/a.u.*      *Pr(t)*    *Pi(t)*   ";
+    std::string head = pulse_title(dim, dim_len) + kPulseCols;
     auto group = [&](const char* a, int i, bool last) {
       head += std::string(a) + (i >= 0 && i <= 9 ? std::string(1, (char)('0' + i)) : "*") +
               "|^2*" + (last ? "" : "   ");
@@ -983,8 +980,8 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
   int done = 0;
   if (nsteps == 0 && prt) {  // no step: the first row alone
     std::vector<double> c0(2);
-    if (espec_grid_run(plan, 0, nullptr) ||
-        espec_grid_results(plan, &c0[0], &c0[1], nullptr, nullptr, ESPEC_MEM_HOST, nullptr))
+    if (espec_grid_run(pp.plan, 0, nullptr) ||
+        espec_grid_results(pp.plan, &c0[0], &c0[1], nullptr, nullptr, ESPEC_MEM_HOST, nullptr))
       return fail(espec_last_error());
     store(nc, c0[0], c0[1]);
     print_row(*ti, first, c0[0], c0[1], true);
@@ -994,8 +991,8 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
     const int k = s - done;
     cre.resize(k + 1);
     cim.resize(k + 1);
-    if ((done == 0 ? espec_grid_run(plan, k, nullptr) : espec_grid_continue(plan, k, nullptr)) ||
-        espec_grid_results(plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST,
+    if ((done == 0 ? espec_grid_run(pp.plan, k, nullptr) : espec_grid_continue(pp.plan, k, nullptr)) ||
+        espec_grid_results(pp.plan, cre.data(), cim.data(), nullptr, nullptr, ESPEC_MEM_HOST,
                            nullptr))
       return fail(espec_last_error());
     if (done == 0 && prt) {
@@ -1012,15 +1009,15 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
     if (printed[s]) {
       double t = *ti + *dt;  // the DO variable, accumulating DT
       for (int q = 2; q <= s; ++q) t = t + *dt;
-      Row r;
-      if (!measure(ef[s], r)) return;
+      PulseRow r;
+      if (measure_row(pp, ef[s], r)) return fail(espec_last_error());
       print_row(t, r, cre[k], cim[k], false);
     }
   }
   // psi(TF), the last step's Lanczos basis (LNZVC(., 1..MP), the V chain),
   // VPOT as CHPOT leaves it, MP as LNZ leaves it
-  if (espec_grid_results(plan, nullptr, nullptr, u, v, ESPEC_MEM_HOST, nullptr) ||
-      (nsteps > 0 && espec_grid_basis(plan, 1, lnzvc, *mxdct, ESPEC_MEM_HOST, nullptr)))
+  if (espec_grid_results(pp.plan, nullptr, nullptr, u, v, ESPEC_MEM_HOST, nullptr) ||
+      (nsteps > 0 && espec_grid_basis(pp.plan, 1, lnzvc, *mxdct, ESPEC_MEM_HOST, nullptr)))
     return fail(espec_last_error());
   if (nsteps > 0)
     for (long i = 0; i < nn; ++i) vpot[i] = vp[i] - dm[i] * ef[nsteps];
