@@ -137,40 +137,6 @@ __device__ __forceinline__ void block_sum(const double (&x)[NV], double* sp, dou
   __syncthreads();
 }
 
-// H_FD x at point k with every x value scaled by d (au1d.f:52-73,
-// au2di.f:57-225, au3d.f:61-117): (30 sum(shm) + V) x_k + sum_a shm_a
-// (x_{-2} - 16 x_{-1} - 16 x_{+1} + x_{+2}), zero outside the grid.  Every
-// neighbour load is issued unconditionally (from x_k where the neighbour is
-// off the grid or the axis absent) so that no branch separates a point's
-// loads from the next point's; the sums skip the off-grid terms as before.
-__device__ __forceinline__ double apply_h(const SilArgs& a, const double* x, int k, double d) {
-  const int kq = k / a.nx;
-  const int idx[3] = {k - kq * a.nx, a.ndim > 1 ? kq % a.ny : 0, a.ndim > 2 ? kq / a.ny : 0};
-  const int len[3] = {a.nx, a.ny, a.nz}, str[3] = {1, a.nx, a.nx * a.ny};
-  double xm2[3], xm1[3], xp1[3], xp2[3];
-#pragma unroll
-  for (int ax = 0; ax < 3; ++ax) {
-    const bool on = ax < a.ndim;
-    const int i = idx[ax], st = str[ax], L = len[ax];
-    xm2[ax] = ld_state(x + (on && i >= 2 ? k - 2 * st : k));
-    xm1[ax] = ld_state(x + (on && i >= 1 ? k - st : k));
-    xp1[ax] = ld_state(x + (on && i + 1 < L ? k + st : k));
-    xp2[ax] = ld_state(x + (on && i + 2 < L ? k + 2 * st : k));
-  }
-  double s = (a.sht30 + __ldg(a.vpot + k)) * (ld_state(x + k) * d);
-#pragma unroll
-  for (int ax = 0; ax < 3; ++ax) {
-    if (ax >= a.ndim) break;
-    const double h = a.shm[ax];
-    const int i = idx[ax], L = len[ax];
-    if (i >= 2) s += h * (xm2[ax] * d);
-    if (i >= 1) s += -16.0 * h * (xm1[ax] * d);
-    if (i + 1 < L) s += -16.0 * h * (xp1[ax] * d);
-    if (i + 2 < L) s += h * (xp2[ax] * d);
-  }
-  return s;
-}
-
 // (x, y, z) indices of point k on an NDIM grid, x fastest.  (k + 1/2)/nx
 // by one FP64 multiplication: its rounding error (< k 2^-52) is far below the
 // 1/(2 nx) distance to the nearest integer, so the truncation is exact.
@@ -192,8 +158,12 @@ __device__ __forceinline__ void grid_index(const SilArgs& a, int k, int (&idx)[3
   }
 }
 
-// apply_h for a known NDIM with the point's indices given: the same terms in
-// the same order, only the axes that exist
+// H_FD x at point k of an NDIM grid, every x value scaled by d (au1d.f:52-73,
+// au2di.f:57-225, au3d.f:61-117): (30 sum(shm) + V) x_k + sum_a shm_a
+// (x_{-2} - 16 x_{-1} - 16 x_{+1} + x_{+2}), zero outside the grid; idx from
+// grid_index.  Every neighbour load is issued unconditionally (from x_k where
+// the neighbour is off the grid) so that no branch separates a point's loads
+// from the next point's; the sums skip the off-grid terms.
 template <int NDIM>
 __device__ __forceinline__ double apply_h_nd(const SilArgs& a, const double* x, int k, double d,
                                              const int (&idx)[3]) {
@@ -723,6 +693,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
 
 // <u|H u> + <v|H v> and |u|^2 + |v|^2 (EIGENERG, eigenerg.f:56-66): per-CTA
 // partials, then one CTA sums them in CTA order
+template <int NDIM>
 __global__ void __launch_bounds__(kSilThreads) sil_energy_kernel(SilArgs a, double* part,
                                                                  double ef) {
   __shared__ double sp[2], scratch[(kSilThreads / 32) * 8];
@@ -730,7 +701,10 @@ __global__ void __launch_bounds__(kSilThreads) sil_energy_kernel(SilArgs a, doub
   for (long k = (long)blockIdx.x * kSilThreads + threadIdx.x; k < a.n;
        k += (long)gridDim.x * kSilThreads) {
     const double uk = a.u[k], vk = a.v[k];
-    double hu = apply_h(a, a.u, (int)k, 1.0), hv = apply_h(a, a.v, (int)k, 1.0);
+    int idx[3];
+    grid_index<NDIM>(a, (int)k, idx);
+    double hu = apply_h_nd<NDIM>(a, a.u, (int)k, 1.0, idx);
+    double hv = apply_h_nd<NDIM>(a, a.v, (int)k, 1.0, idx);
     if (a.dm) {  // the potential V - DM EF of a pulse (chpot.f)
       const double de = a.dm[k] * ef;
       hu -= de * uk;
@@ -1070,7 +1044,9 @@ extern "C" int espec_grid_energies_at(espec_grid_plan* p, double ef, double* e, 
   SilArgs a = sil_args(p);
   long nbk = (p->n + kSilThreads - 1) / kSilThreads;
   if (nbk > 1024) nbk = 1024;
-  sil_energy_kernel<<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart, ef);
+  if (p->ndim == 1) sil_energy_kernel<1><<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart, ef);
+  else if (p->ndim == 2) sil_energy_kernel<2><<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart, ef);
+  else sil_energy_kernel<3><<<(int)nbk, kSilThreads, 0, st>>>(a, p->d_epart, ef);
   GRID_CK(cudaGetLastError());
   sum_parts_kernel<<<1, 32, 0, st>>>(p->d_epart, (int)nbk, p->d_eout);
   GRID_CK(cudaGetLastError());
