@@ -63,6 +63,37 @@ def test_ppsod_projections(tmp_path):
         assert why in msg, (npr_kp, msg)
 
 
+PULSE_BLOCKS = ["*PULSE_AND_DIPOLE\n.GAUS\n 5.0D7  0.1  2.5  0.15  0.0/\n.EXP\n 0.5 0.3 0.0/",
+                "*PULSE_AND_DIPOLE\n.GGAUS\n 3D11 0.08 2.5 0.12 0.3 2/\n.CONST\n 1.0/",
+                "*PULSE_AND_DIPOLE\n.SIN2\n 6D7 0.2 3.0 0.05 0.0/\n.NULL",
+                "*PULSE_AND_DIPOLE\n.NONE\n 0 0 0/\n.NONE\n 0.0/"]
+
+
+@pytest.mark.parametrize("prop", [".PPSOD\n 0.0  0.3096171935104  0.00120944216215/",
+                                  ".PPSIL\n 0.0  0.3096171935104  0.00120944216215 10/"])
+@pytest.mark.parametrize("block", PULSE_BLOCKS)
+def test_pulse_blocks_are_read(tmp_path, prop, block):
+    """rdinput.f:549-578: each pulse shape's parameter record and each
+    dipole form's record; a deck that reads through stops at its (absent)
+    .FILE, before any device work."""
+    text = BASE.replace(".PFSPO\n 0.0  0.3096171935104  0.00120944216215/", prop)
+    text = text.replace("*PRPTOL", block + "\n*PRPTOL")
+    assert text != BASE
+    msg = refused(tmp_path, text)
+    assert "cannot be opened" in msg, msg
+
+
+@pytest.mark.parametrize("block,why", [
+    ("*PULSE_AND_DIPOLE\n.GGAUS\n 3D11 0.08 2.5 0.12 0.3/\n.NULL", "KL"),
+    ("*PULSE_AND_DIPOLE\n.SIN2\n 6D7 0.2 3.0/\n.NULL", "TD"),
+    ("*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.EXP+\n 0.5 0.3/", "dipole .EXP+"),
+    ("*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.LINEAR\n 0.5/", "wasn't found"),
+])
+def test_pulse_blocks_refused(tmp_path, block, why):
+    msg = refused(tmp_path, BASE.replace("*PRPTOL", block + "\n*PRPTOL"))
+    assert why in msg, msg
+
+
 def test_missing_and_short_files(tmp_path):
     assert "cannot be opened" in refused(tmp_path, BASE)
     short = "# Eigenvector:\n 0.5 0.1\n 0.6 0.2\n"
