@@ -316,7 +316,7 @@ def sil_bytes(m):
 PSOD_BYTES = 72  # read psi_n, psi_{n-1}, psi0 (16 B each) and V (8 B); write psi_{n+1} (16 B)
 
 
-def psod_2d(dev, steps=100, cpu_steps=2):
+def psod_2d(dev, steps=100, cpu_steps=20):
     """Second-order differences (PSOD, FD stencil, FP64) on 2D coupled-Morse
     grids: 256 x 256 (state in L2) and 2048 x 2048 (state in HBM), dt below
     the SOD stability limit 1 / E_max of each grid."""
@@ -354,6 +354,17 @@ def psod_2d(dev, steps=100, cpu_steps=2):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind,
                          "bytes_per_gridpt_step": PSOD_BYTES}}
+        if cpu_steps and n == 256:  # the oracle port of PSOD on one host core
+            from oracle import oracle as O
+
+            dt = dt_au * 2.4188843243e-2
+            p = O.make_prop([n, n], dt, 0.0, cpu_steps * dt, [h, h], [918.0, 1500.0], lc=1,
+                            shm=shm)
+            t0 = time.perf_counter()
+            O.psod(p, V.ravel(order="F"), psi.real.copy(), psi.imag.copy())
+            tc = (time.perf_counter() - t0) / O.do_count(dt, cpu_steps * dt + dt, dt)
+            out[f"{n}x{n}"]["cpu_port"] = {"value": n * n / tc / 1e6, "unit": "Mgridpt*steps/s",
+                                          "cores": 1, "sample": f"{cpu_steps} steps"}
     return out
 
 
