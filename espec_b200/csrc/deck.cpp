@@ -341,6 +341,8 @@ Run read_run(const Deck& d) {
           r.ti = x[0];
           r.tf = x[1];
           r.dt = x[2];
+          if (!(r.dt > 0.0) || !((r.tf - r.ti) / r.dt < 1.0e9))
+            throw DeckError{"*PROPAG: DT must be positive and (TF - TI)/DT below 1e9"};
           if (sil) r.mp = (int)x[3];
         } else if (k == "*PRPGSTATE") {
           r.prpgstate = (int)numbers(rec(v, 0, "*PRPGSTATE")).at(0);

@@ -739,6 +739,8 @@ extern "C" void ppsod_(const int* absorb, const int* prtveff, const int* prteigv
   for (int a = 0; a < ndim; ++a) npts *= np[a];
   if (npts != *n) return fail("N differs from the product of NP");
   if (*lc < 1) return fail("LC must be at least 1");
+  if (!(*dt > 0.0) || !((*tf - *ti) / *dt < 1.0e9))
+    return fail("DT must be positive and (TF - TI)/DT below 1e9");
   if (*npr_in > 6) return fail("NPR must be at most 6 (rdinput.f:660)");
   const int npr = std::max(*npr_in, 0);  // NPR < 1: no projections (ppsod.f:99-104)
   double par[6];
@@ -896,6 +898,8 @@ extern "C" void pplnz_(const int* absorb, const int* change, const int* prtveff,
   for (int a = 0; a < ndim; ++a) npts *= np[a];
   if (npts != *n) return fail("N differs from the product of NP");
   if (*lc < 1) return fail("LC must be at least 1");
+  if (!(*dt > 0.0) || !((*tf - *ti) / *dt < 1.0e9))
+    return fail("DT must be positive and (TF - TI)/DT below 1e9");
   if (*npr_in > 6) return fail("NPR must be at most 6 (rdinput.f:660)");
   const int npr = std::max(*npr_in, 0);
   const int nw = std::max(npr - 1, 0);  // printed projections: W_1 .. W_{NPR-1}

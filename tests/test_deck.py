@@ -26,6 +26,7 @@ def refused(tmp_path, text, files=None):
     (".FILE\nwf_pot.inp", ".MORSE\n1.1 1943.8 13.7 1.0/\n1.2 1629.2 17.7 1.0/", ".FILE"),
     (".GETR", ".CALC", ".GETR"),
     (".PFSPO", ".P2PABM", "propagator"),
+    (" 0.0  0.3096171935104  0.00120944216215/", " 0.0  0.3096171935104  0.0/", "DT must be"),
     (".1D\n 256/", ".2DC\n 16 16/", "*DIMENSION"),
     ("*TPTRANS\n.ONE", "*TPTRANS\n.ALL", "one propagated state"),
     ("**TD", "**TI\n*TPDIAG\n.LANCZS\n**TD", "section **TI"),
