@@ -255,7 +255,9 @@ int absorber(bool absorb, const char* tp, size_t len) {
   return ESPEC_ABS_NONE;
 }
 
-void common_scalars(DropIn& d, const int* absorb, const char* prtcrl, size_t prtcrl_len,
+// false (INFO = 2, reason on stderr) when DT is not positive or the run
+// would take more than 1e9 steps: the step counts below assume both
+bool common_scalars(DropIn& d, const int* absorb, const char* prtcrl, size_t prtcrl_len,
                     const int* lc, const int* mpi, const int* mpr, const int* mxdct, const int* n,
                     const double* dt, const double* ti, const double* tf, const double* tol,
                     double* lnzvc) {
@@ -272,6 +274,11 @@ void common_scalars(DropIn& d, const int* absorb, const char* prtcrl, size_t prt
   d.tf = *tf;
   d.tol = *tol;
   d.lnzvc = lnzvc;
+  if (!(d.dt > 0.0) || !((d.tf - d.ti) / d.dt < 1.0e9)) {
+    d.fail("DT must be positive and (TF - TI)/DT below 1e9");
+    return false;
+  }
+  return true;
 }
 
 // the FFT propagators: one-packet espec_spo_plan
@@ -463,7 +470,9 @@ extern "C" void pspofft_(const int* absorb, const char* dim, const char* prtcrl,
   d.name = "PSPOFFT";
   d.kind = kSpo;
   d.info = info;
-  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  if (!common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol,
+                      lnzvc))
+    return;
   if (d.setup(ESPEC_SPO, dim, dim_len, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u1, v1))
     return;
   // DO T = TI+DT, TF+DT, DT (pspofft.f:110): T accumulates by DT
@@ -496,7 +505,9 @@ extern "C" void psodfft_(const int* absorb, const char* dim, const char* prtcrl,
   d.name = "PSODFFT";
   d.kind = kSod;
   d.info = info;
-  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  if (!common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol,
+                      lnzvc))
+    return;
   if (d.setup(ESPEC_SOD, dim, dim_len, tpabsor, tpabsor_len, np, sh, sm, tc, vpot, vabc, u1, v1))
     return;
   // start-up step at T = TI+DT (psodfft.f:120-147), then DO T = TI+2*DT,
@@ -539,7 +550,9 @@ extern "C" void plnz_(const int* absorb, const int* change, const char* dim, con
   d.name = "PLNZ";
   d.kind = kSil;
   d.info = info;
-  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  if (!common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol,
+                      lnzvc))
+    return;
   int ndim = 0;
   if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
   if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
@@ -632,7 +645,9 @@ extern "C" void psod_(const int* absorb, const char* dim, const char* prtcrl, co
   d.name = "PSOD";
   d.kind = kPsod;
   d.info = info;
-  common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol, lnzvc);
+  if (!common_scalars(d, absorb, prtcrl, prtcrl_len, lc, mpi, mpr, mxdct, n, dt, ti, tf, tol,
+                      lnzvc))
+    return;
   int ndim = 0;
   if (fstr_is(dim, dim_len, ".1D")) ndim = 1;
   if (fstr_is(dim, dim_len, ".2D")) ndim = 2;
