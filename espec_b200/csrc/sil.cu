@@ -635,8 +635,10 @@ __device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const dou
   }
 }
 
+// two CTAs per SM where the registers allow it without spills (1D, 2D): the
+// passes over a large grid are load-latency bound, and more warps hide it
 template <int NDIM>
-__global__ void __launch_bounds__(kSilThreads, 1) psod_kernel(SilArgs a) {
+__global__ void __launch_bounds__(kSilThreads, NDIM == 3 ? 1 : 2) psod_kernel(SilArgs a) {
   __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
   __shared__ double s_red[kSilThreads];
   __shared__ int s_flag[2];
@@ -881,18 +883,27 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   p->quirks = quirks;
   // co-resident CTAs for the cooperative launch
   int dev = 0, nsm = 0, occ = 0;
+  const void* kern =
+      psod ? (ndim == 1   ? (const void*)psod_kernel<1>
+              : ndim == 2 ? (const void*)psod_kernel<2>
+                          : (const void*)psod_kernel<3>)
+           : (ndim == 1   ? (const void*)sil_kernel<1>
+              : ndim == 2 ? (const void*)sil_kernel<2>
+                          : (const void*)sil_kernel<3>);
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-  if (e == cudaSuccess)
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, psod ? psod_kernel<3> : sil_kernel<3>,
-                                                      kSilThreads, 0);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSilThreads, 0);
   if (e != cudaSuccess) {
     delete p;
     return set_cuda_error("device query", e);
   }
   long want = (n + kSilThreads - 1) / kSilThreads;
+  // one CTA per SM keeps the barriers short; a PSOD pass over a large grid
+  // (16 points or more per thread) takes every co-resident CTA instead
+  long cap = nsm;
+  if (psod && n >= 16L * nsm * kSilThreads) cap = (long)nsm * occ;
   if (want > (long)nsm * occ) want = (long)nsm * occ;
-  if (want > nsm) want = nsm;  // one CTA per SM keeps the barriers short
+  if (want > cap) want = cap;
   p->nblocks = (int)(want > 0 ? want : 1);
   auto fail = [&](int rc) {
     grid_free(p);

@@ -79,6 +79,30 @@ def test_psod_random_grids(oracle, np_, absorb, quirk):
     assert np.max(np.abs(prev - (ref["u_prev"] + 1j * ref["v_prev"]))) <= 1e-10
 
 
+@pytest.mark.parametrize("np_,dt_au,absorb", [([1024, 640], 2e-4, 0), ([1024, 640], 2e-4, 1),
+                                               ([700000], 5e-10, 2)])
+def test_psod_large_grids(oracle, np_, dt_au, absorb):
+    """Grids of 16 or more points per thread, where the plan takes every
+    co-resident CTA (two per SM in 1D/2D) instead of one per SM: the same
+    results as the oracle; dt below the SOD limit 1 / E_max of each grid."""
+    v, psi, sh, grids = packet(np_, 3 + absorb)
+    sm = [1000.0 + 400.0 * a for a in range(len(np_))]
+    shm = [G.shm_of(m, h) for m, h in zip(sm, sh)]
+    vabc = None
+    if absorb == NAT.ABS_VOPTIC:
+        vabc = -0.05 * np.clip(grids[0] - 0.3, 0, None).ravel(order="F") ** 2
+    elif absorb == NAT.ABS_SMOOTHW:
+        vabc = np.where(grids[0] > 0.35, 0.97, 1.0).ravel(order="F")
+    dt = dt_au * NAT.SHFS
+    p = oracle.make_prop(np_, dt, 0.0, 8 * dt, sh, sm, lc=1, absorb=absorb, shm=shm)
+    ref = oracle.psod(p, v, np.real(psi), np.imag(psi), vabc=vabc)
+    c, out, prev = gpu_psod(np_, shm, dt, v, psi, ref["nc"] - 1, absorb=absorb, vabc=vabc)
+    assert np.isfinite(ref["c"]).all()
+    assert np.max(np.abs(c - ref["c"])) <= 1e-10, np.max(np.abs(c - ref["c"]))
+    assert np.max(np.abs(out - (ref["u"] + 1j * ref["v"]))) <= 1e-10
+    assert np.max(np.abs(prev - (ref["u_prev"] + 1j * ref["v_prev"]))) <= 1e-10
+
+
 def test_psod_continue_and_energies(oracle):
     np_ = [64, 48]
     v, psi, sh, _ = packet(np_, 9)
