@@ -542,7 +542,10 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 // then the two buffers swap roles.  From the start: C(0), an Euler step of
 // c = CST/4 and a midpoint step of CST/2 to TI + DT, psi_{n-1} reset to psi0
 // (with the reference's copy defect on request), then steps of CST.
-constexpr int kPsodIlp = 4;
+// points per thread whose loads are in flight together: four in 1D/2D, two in
+// 3D (its 13-point stencils), within 128 registers
+template <int NDIM>
+constexpr int kPsodIlp = NDIM == 3 ? 2 : 4;
 
 template <int KABS, bool DM, int NDIM>
 __device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const double* un,
@@ -602,17 +605,17 @@ __device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const dou
                                             double e, double (&q)[4]) {
   const int t = threadIdx.x;
   int k0 = r.lo + t;
-  for (; k0 + (kPsodIlp - 1) * kSilThreads < r.hi; k0 += kPsodIlp * kSilThreads) {
-    double nu[kPsodIlp], nv[kPsodIlp], u0k[kPsodIlp], v0k[kPsodIlp];
+  for (; k0 + (kPsodIlp<NDIM> - 1) * kSilThreads < r.hi; k0 += kPsodIlp<NDIM> * kSilThreads) {
+    double nu[kPsodIlp<NDIM>], nv[kPsodIlp<NDIM>], u0k[kPsodIlp<NDIM>], v0k[kPsodIlp<NDIM>];
 #pragma unroll
-    for (int j = 0; j < kPsodIlp; ++j) {
+    for (int j = 0; j < kPsodIlp<NDIM>; ++j) {
       const int k = k0 + j * kSilThreads;
       psod_point<KABS, DM, NDIM>(a, un, vn, um, vm, k, c, e, nu[j], nv[j]);
       u0k[j] = __ldg(a.u0 + k);
       v0k[j] = __ldg(a.v0 + k);
     }
 #pragma unroll
-    for (int j = 0; j < kPsodIlp; ++j) {
+    for (int j = 0; j < kPsodIlp<NDIM>; ++j) {
       const int k = k0 + j * kSilThreads;
       um[k] = nu[j];
       vm[k] = nv[j];
@@ -635,10 +638,10 @@ __device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const dou
   }
 }
 
-// two CTAs per SM where the registers allow it without spills (1D, 2D): the
-// passes over a large grid are load-latency bound, and more warps hide it
+// two CTAs per SM (128 registers, no spills): the passes over a large grid are
+// load-latency bound, and more warps hide it
 template <int NDIM>
-__global__ void __launch_bounds__(kSilThreads, NDIM == 3 ? 1 : 2) psod_kernel(SilArgs a) {
+__global__ void __launch_bounds__(kSilThreads, 2) psod_kernel(SilArgs a) {
   __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
   __shared__ double s_red[kSilThreads];
   __shared__ int s_flag[2];

@@ -80,10 +80,10 @@ def test_psod_random_grids(oracle, np_, absorb, quirk):
 
 
 @pytest.mark.parametrize("np_,dt_au,absorb", [([1024, 640], 2e-4, 0), ([1024, 640], 2e-4, 1),
-                                               ([700000], 5e-10, 2)])
+                                               ([700000], 5e-10, 2), ([100, 96, 64], 0.01, 1)])
 def test_psod_large_grids(oracle, np_, dt_au, absorb):
     """Grids of 16 or more points per thread, where the plan takes every
-    co-resident CTA (two per SM in 1D/2D) instead of one per SM: the same
+    co-resident CTA (two per SM) instead of one per SM: the same
     results as the oracle; dt below the SOD limit 1 / E_max of each grid."""
     v, psi, sh, grids = packet(np_, 3 + absorb)
     sm = [1000.0 + 400.0 * a for a in range(len(np_))]
