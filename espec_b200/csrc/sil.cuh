@@ -14,8 +14,8 @@
 // with H the 4th-order finite-difference Hamiltonian.  The two dot-product
 // rounds of an iteration are merged into one (<w - al vi, L_q> = <w,L_q> -
 // al <vi,L_q>), so an iteration costs two grid barriers.  Each barrier is
-// also the reduction: the last CTA to arrive sums the per-CTA partials in a
-// fixed order (deterministic) and publishes the totals.
+// also the reduction: after it every CTA sums the per-CTA partials itself in
+// one fixed order, so all CTAs hold the same (deterministic) totals.
 //
 // The Krylov exponential e^{-i cst T} of the m x m tridiagonal T is formed by
 // every CTA (same inputs, same result) by Taylor series with scaling and
