@@ -4,8 +4,9 @@
     python -m espec_b200.deck path/to/input.spc data1.inp data2.inp ... out_prefix
 
 covers the time-dependent part of espec.f for one packet with a .FILE
-potential and its .GETR eigenvector (.PFSPO, .PFSOD, .PSIL, .PSOD, absorbers,
-total correlation, HWHM, spectrum) and prints what espec.x prints from
+potential and its .GETR eigenvector (.PFSPO, .PFSOD, .PSIL, .PSOD, and .PPSOD /
+.PPSIL with a laser pulse; absorbers, total correlation, HWHM, spectrum) and
+prints what espec.x prints from
 "Propagating eigenvector..." on; other decks are refused with the reason.
 """
 import sys
