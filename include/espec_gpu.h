@@ -168,7 +168,8 @@ void spectrumtd_(const char* tpwind, const int* m, const double* dt,
                  double* v, size_t tpwind_len);
 /* Runs an eSPec input deck (time-dependent part of espec.f for one packet
  * with a .FILE potential and its .GETR eigenvector; .PFSPO, .PFSOD, .PSIL,
- * .PSOD; absorbers, total correlation, HWHM and spectrum) through the GPU
+ * .PSOD, and .PPSOD / .PPSIL with *PULSE_AND_DIPOLE; absorbers, total
+ * correlation, HWHM and spectrum) through the GPU
  * drop-ins, printing to stdout what espec.x prints from "Propagating
  * eigenvector..." on.  Files named in the deck are relative to the deck's
  * directory.  An option outside that part is refused (ESPEC_EINVAL, reason
