@@ -391,6 +391,9 @@ DECK_CASES = {
     "deck_ppsil": (1, ".PPSIL", "  10", PULSE_EXP, ""),
     # NPR = 3, KP = 0 becomes NPR = 2: PPLNZ prints |C|^2 and |<W1|psi>|^2
     "deck_ppsil_proj": (1, ".PPSIL", "  10", PULSE_EXP + "*NPROJECTIONS\n 3 0/\n", ""),
+    # 2D: DIPLMMT's R = XI(1) + (I - 1) SH(1) runs over all NT points of the grid
+    "deck_ppsod_2d": (2, ".PPSOD", "", PULSE_EXP, ""),
+    "deck_ppsil_2d": (2, ".PPSIL", "  10", PULSE_EXP, ""),
 }
 
 

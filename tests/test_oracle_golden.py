@@ -218,3 +218,50 @@ def test_pulse_decks(oracle, name, npr):
     assert r["info"] == 0
     if npr:  # the projection on the zero vector
         assert not gold[:, -2].any() and not r["rows"][:, -2].any()
+
+
+@pytest.mark.parametrize("name", ["deck_ppsod_2d", "deck_ppsil_2d"])
+def test_pulse_decks_2d(oracle, name):
+    """The 2D pulse decks (32 x 32 coupled Morse, the .EXP dipole): DIPLMMT
+    evaluates mu(R) at R = XI(1) + (I - 1) SH(1) for every I of the whole
+    grid (dipl.f:62-66), not at each point's x; the oracle's rows with that
+    dipole agree with the executable to half a printed unit, and the
+    per-point-x dipole would not (ET off by 3e-5)."""
+    d = os.path.join(G.GOLDEN, name)
+    lines = [l for l in open(os.path.join(d, "wf_pot.inp")).read().split("\n") if l.strip()]
+    n = 32 * 32
+    rows = np.array([[float(t) for t in l.split()] for l in lines[1:1 + n]])
+    vrows = np.array([[float(t) for t in l.split()] for l in lines[2 + n:2 + 2 * n]])
+    x, y = rows[:32, 1], rows[::32, 0]
+    psi, v = rows[:, 2], vrows[:, 2]
+    sh = [(x[-1] - x[0]) / 31, (y[-1] - y[0]) / 31]
+    sm = [918.0, 1500.0]
+    shm = [G.shm_of(m, h) for m, h in zip(sm, sh)]
+    dt = 0.005 * 2.4188843243e-2
+    sil = "ppsil" in name
+    p = oracle.make_prop([32, 32], dt, 0.0, 256 * dt, sh, sm, lc=2, tol=1e3,
+                         prtcrl=oracle.PRT_PARTIAL, shm=shm, mp=10, lmtreort=10, change=1,
+                         quirks=oracle.Q_SIL_INPLACE if sil else 0)
+    pulse = (5.0e7, 0.1, 2.5, 0.15, 0.0)
+    text = open(os.path.join(d, "expected.txt")).read().split("\n")
+    ncol = 6 if sil else 7
+    gold = np.array([[float(t) for t in l.split()] for l in text
+                     if len(l.split()) == ncol and l.split()[0][0].isdigit()])
+
+    def rows_with(r_ab):
+        dm = 0.5 * r_ab * np.exp(-0.3 * r_ab)
+        if sil:
+            return oracle.pplnz_table(p, v, dm, 1, pulse, 0, np.zeros((1, n)), psi,
+                                      np.zeros(n))["rows"]
+        return oracle.ppsod_table(p, v, dm, 1, pulse, np.zeros((0, n)), psi, np.zeros(n))["rows"]
+
+    got = rows_with(x[0] + np.arange(n) * sh[0])
+    assert got.shape == gold.shape == (129, ncol)
+    d_ = np.abs(got - gold)
+    half = np.array([5e-7, 0, 0, 5e-6, 5e-6] + [5e-7] * (ncol - 5)) * 1.01
+    num = [0] + list(range(3, ncol))
+    assert np.all(d_[:, num] <= half[num]), d_.max(axis=0)
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(gold[:, 1:3]))) - 5)
+    assert np.all(d_[:, 1:3] <= 0.5 * e_ulp * 1.01)
+    other = rows_with(x[np.arange(n) % 32])
+    assert np.max(np.abs(other[:, 1] - gold[:, 1])) > 1e-5
