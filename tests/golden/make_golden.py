@@ -366,6 +366,18 @@ PULSE_EXP = """*PULSE_AND_DIPOLE
 .EXP
  0.5 0.3 0.0/
 """
+PULSE_GGAUS_CONST = """*PULSE_AND_DIPOLE
+.GGAUS
+ 3.0D11  0.1  2.5  0.15  0.3  4.0/
+.CONST
+ 0.8/
+"""
+PULSE_SIN2_EXP = """*PULSE_AND_DIPOLE
+.SIN2
+ 5.0D7  0.2  2.5  0.05  0.0/
+.EXP
+ 0.5 0.3 0.0/
+"""
 VOPTIC_SMALL = """*ABSORBING
 .VOPTIC_POLIN
  -0.5  2.0  0.0/
@@ -394,6 +406,9 @@ DECK_CASES = {
     # 2D: DIPLMMT's R = XI(1) + (I - 1) SH(1) runs over all NT points of the grid
     "deck_ppsod_2d": (2, ".PPSOD", "", PULSE_EXP, ""),
     "deck_ppsil_2d": (2, ".PPSIL", "  10", PULSE_EXP, ""),
+    # the other pulse shapes of ef.f and the .CONST dipole (mu = c / R)
+    "deck_ppsod_ggaus": (1, ".PPSOD", "", PULSE_GGAUS_CONST, ""),
+    "deck_ppsod_sin2": (1, ".PPSOD", "", PULSE_SIN2_EXP, ""),
 }
 
 

@@ -23,7 +23,8 @@ import golden_cases as G
 pytestmark = pytest.mark.gpu
 
 DECKS = ["deck_spo_hwhm", "deck_psod_voptic", "deck_sil_smooth", "deck_sil_2d", "deck_ppsod",
-         "deck_ppsod_proj", "deck_ppsil", "deck_ppsil_proj", "deck_ppsod_2d", "deck_ppsil_2d"]
+         "deck_ppsod_proj", "deck_ppsil", "deck_ppsil_proj", "deck_ppsod_2d", "deck_ppsil_2d",
+         "deck_ppsod_ggaus", "deck_ppsod_sin2"]
 NUM = re.compile(r"^-?(\d+\.?\d*|\.\d+)([EeDd][-+]?\d+)?$")
 
 

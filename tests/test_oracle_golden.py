@@ -220,6 +220,38 @@ def test_pulse_decks(oracle, name, npr):
         assert not gold[:, -2].any() and not r["rows"][:, -2].any()
 
 
+@pytest.mark.parametrize("name,shape,par,dipole", [
+    ("deck_ppsod_ggaus", 2, (3.0e11, 0.1, 2.5, 0.15, 0.3, 4), "const"),
+    ("deck_ppsod_sin2", 3, (5.0e7, 0.2, 2.5, 0.05, 0.0), "exp")])
+def test_pulse_shapes(oracle, name, shape, par, dipole):
+    """ef.f's .GGAUS (order KL = 4, the single-precision ln 2 literal) with the
+    .CONST dipole mu = c / R, and .SIN2 with .EXP, run by the executable: the
+    oracle's PPSOD rows agree to half a unit of every printed digit."""
+    d = os.path.join(G.GOLDEN, "deck_ppsod")
+    lines = open(os.path.join(d, "wf_pot.inp")).read().split("\n")
+    n = 256
+    x = np.array([float(l.split()[0]) for l in lines[1:1 + n]])
+    psi = np.array([float(l.split()[1]) for l in lines[1:1 + n]])
+    v = np.array([float(l.split()[1]) for l in lines[2 + n:2 + 2 * n]])
+    sh = (x[-1] - x[0]) / (n - 1)
+    dt = 0.05 * 2.4188843243e-2
+    r_ab = x[0] + np.arange(n) * sh  # dipl.f:62-74
+    dm = 0.8 / r_ab if dipole == "const" else 0.5 * r_ab * np.exp(-0.3 * r_ab)
+    p = oracle.make_prop([n], dt, 0.0, 256 * dt, [sh], [918.0], lc=2, tol=1e3,
+                         prtcrl=oracle.PRT_PARTIAL, shm=[G.shm_of(918.0, sh)])
+    r = oracle.ppsod_table(p, v, dm, shape, par, np.zeros((0, n)), psi, np.zeros(n))
+    text = open(os.path.join(G.GOLDEN, name, "expected.txt")).read().split("\n")
+    gold = np.array([[float(t) for t in l.split()] for l in text
+                     if len(l.split()) == 7 and l.split()[0][0].isdigit()])
+    assert r["rows"].shape == gold.shape == (129, 7)
+    d_ = np.abs(r["rows"] - gold)
+    half = np.array([5e-7, 0, 0, 5e-6, 5e-6, 5e-7, 5e-7]) * 1.01
+    assert np.all(d_[:, [0, 3, 4, 5, 6]] <= half[[0, 3, 4, 5, 6]])
+    e_ulp = 10.0 ** (np.floor(np.log10(np.abs(gold[:, 1:3]))) - 5)
+    assert np.all(d_[:, 1:3] <= 0.5 * e_ulp * 1.01)
+    assert np.max(np.abs(gold[:, 1] - gold[:, 2])) > 1e-4  # the field shows in ET
+
+
 @pytest.mark.parametrize("name", ["deck_ppsod_2d", "deck_ppsil_2d"])
 def test_pulse_decks_2d(oracle, name):
     """The 2D pulse decks (32 x 32 coupled Morse, the .EXP dipole): DIPLMMT
