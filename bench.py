@@ -484,6 +484,8 @@ def main():
             leg = {"sil_2d": sil_2d, "psod_2d": psod_2d}[args.leg]
             print(json.dumps({"leg": args.leg, **leg(dev, steps=args.leg_steps, cpu_steps=0)}),
                   flush=True)
+        if world > 1:
+            torch.distributed.destroy_process_group()
         return
     sizes = tuple(int(x) for x in args.sizes.split(",")) if args.sizes else W.SCAN_SIZES
     w = W.morse_scan(npk=args.npk, nsteps=args.nsteps, seed=rank_seed(rank), sizes=sizes)
