@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--cpu-sample-packets", type=int, default=256)
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the FP64-form, SIL-2D and eigensolver legs")
-    ap.add_argument("--leg", default=None, choices=["sil_2d", "psod_2d"],
+    ap.add_argument("--leg", default=None, choices=["sil_2d", "psod_2d", "grid_sweep"],
                     help="run one grid-plan leg alone and print its JSON (profiling)")
     ap.add_argument("--leg-steps", type=int, default=100)
     ap.add_argument("--eig-train", type=int, default=50000)
@@ -305,6 +305,41 @@ def sil_2d(dev, steps=100, cpu_steps=2):
     return out
 
 
+def grid_sweep(dev, steps=50, cpu_steps=0):
+    """Per-step time of the grid kernels against the grid size: SIL of order
+    12 and 4 and PSOD on n x n coupled-Morse grids, n = 64 .. 1024 (small
+    time steps: the cost of a step does not depend on dt)."""
+    import torch
+
+    import espec_b200 as E
+
+    out = {"workload": "SIL order 12 / 4 and PSOD per step on n x n grids", "unit": "us/step"}
+    for n in (64, 128, 256, 512, 1024):
+        x = np.linspace(0.5, 8.0, n)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        V = 0.17 * (1 - np.exp(-(X - 1.4))) ** 2 + 0.12 * (1 - np.exp(-1.2 * (Y - 1.8))) ** 2
+        psi = np.exp(-((X - 1.6) ** 2) / 0.045 - ((Y - 2.0) ** 2) / 0.045)
+        psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
+        h = x[1] - x[0]
+        shm = [1.0 / (24.0 * m * h * h) for m in (918.0, 1500.0)]
+        row = {}
+        for kind, m in (("sil12", 12), ("sil4", 4), ("psod", 0)):
+            g = E.PsodGrid([n, n], shm, 1e-4) if kind == "psod" else E.SilGrid([n, n], shm, 1e-3, m)
+            g.load(V.ravel(order="F"), psi)
+            g.run(3)
+            g.results()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            st = torch.cuda.current_stream(dev)
+            e0.record(st)
+            g.run(steps)
+            e1.record(st)
+            g.results()
+            row[kind] = e0.elapsed_time(e1) / steps * 1e3
+            g.close()
+        out[f"{n}x{n}"] = row
+    return out
+
+
 def sil_bytes(m):
     """Algorithmic bytes per grid point and step of SIL order m (FP64), both
     chains: m H.psi (read psi and V, write H psi: 24 B each), the
@@ -481,7 +516,7 @@ def main():
     torch.cuda.set_device(dev)
     if args.leg:
         if rank == 0:
-            leg = {"sil_2d": sil_2d, "psod_2d": psod_2d}[args.leg]
+            leg = {"sil_2d": sil_2d, "psod_2d": psod_2d, "grid_sweep": grid_sweep}[args.leg]
             print(json.dumps({"leg": args.leg, **leg(dev, steps=args.leg_steps, cpu_steps=0)}),
                   flush=True)
         if world > 1:
