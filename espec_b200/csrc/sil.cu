@@ -534,14 +534,6 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   }
 }
 
-// Second-order differences with H = AU (psod.f:64-205, sod.f:64-123), one
-// cooperative kernel per run.  Each step overwrites the state one step back
-// in place, psi_{n-1} <- psi_{n-1} - i c H psi_n (.VOPTIC: - c VABC psi_n;
-// .SMOOTHW: the whole right side times the mask), reads psi_n's neighbours
-// only, and ends in one grid barrier that also sums C = <psi0|psi_{n+1}>;
-// then the two buffers swap roles.  From the start: C(0), an Euler step of
-// c = CST/4 and a midpoint step of CST/2 to TI + DT, psi_{n-1} reset to psi0
-// (with the reference's copy defect on request), then steps of CST.
 // points per thread whose loads are in flight together: four in 1D/2D, two in
 // 3D (its 13-point stencils), within 128 registers
 template <int NDIM>
@@ -638,8 +630,17 @@ __device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const dou
   }
 }
 
-// two CTAs per SM (128 registers, no spills): the passes over a large grid are
-// load-latency bound, and more warps hide it
+// Second-order differences with H = AU (psod.f:64-205, sod.f:64-123), one
+// cooperative kernel per run.  Each step overwrites the state one step back
+// in place, psi_{n-1} <- psi_{n-1} - i c H psi_n (.VOPTIC: - c VABC psi_n;
+// .SMOOTHW: the whole right side times the mask), reads psi_n's neighbours
+// only, and ends in one grid barrier that also sums C = <psi0|psi_{n+1}>;
+// then the two buffers swap roles.  From the start: C(0), an Euler step of
+// c = CST/4 and a midpoint step of CST/2 to TI + DT, psi_{n-1} reset to psi0
+// (with the reference's copy defect on request), then steps of CST.
+//
+// Two CTAs per SM (128 registers, no spills): the passes over a large grid are
+// load-latency bound, and more warps hide it.
 template <int NDIM>
 __global__ void __launch_bounds__(kSilThreads, 2) psod_kernel(SilArgs a) {
   __shared__ double sp[4], st[4], scratch[(kSilThreads / 32) * 8];
