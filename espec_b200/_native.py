@@ -27,21 +27,21 @@ SHFS = 2.4188843243e-2
 
 # every symbol the header declares (checked by the CPU test suite)
 EXPORTS = [
-    "espec_last_error", "espec_version", "espec_device_ok",
-    "espec_spo_create", "espec_spo_load", "espec_spo_run", "espec_spo_results",
-    "espec_spo_device_c", "espec_spo_npoints", "espec_spo_destroy",
-    "espec_spo_set_variant", "espec_spo_variant_count", "espec_spo_run_static",
-    "espec_prop_create", "espec_prop_previous", "espec_prop_continue", "espec_prop_energies",
-    "espec_format_crl_row", "pspofft_", "psodfft_",
-    "espec_grid_create", "espec_grid_load", "espec_grid_run", "espec_grid_continue",
-    "espec_grid_results", "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy",
-    "espec_grid_basis", "espec_grid_previous", "espec_grid_energies_at",
-    "espec_grid_set_pulse", "espec_pulse_field", "espec_ppsod_field", "espec_pplnz_field", "plnz_", "psod_", "ppsod_", "pplnz_", "espec_grid_project", "espec_run_deck", "espec_run_scan", "espec_spectrum_dev", "espec_spectrum_work_bytes", "hwhm_",
-    "spectrumtd_", "espec_eig_solve_dev", "espec_eig_lcg_start", "espec_eig_morse2d",
-    "espec_gemm_f64", "espec_gemm_f32", "espec_gemm_bf16", "espec_gemm_bf16_status",
-    "espec_mlp_bias_gelu", "espec_mlp_gelu_back", "espec_to_bf16", "espec_mlp_adam_bf16",
-    "espec_mlp_colsum", "espec_mlp_mse", "espec_sep_basis", "espec_convert",
-    "espec_spond_create", "espec_spond_load", "espec_spond_run",
+    "espec_last_error", "espec_version", "espec_device_ok", "espec_spo_create", "espec_spo_load",
+    "espec_spo_run", "espec_spo_results", "espec_spo_device_c", "espec_spo_npoints",
+    "espec_spo_destroy", "espec_spo_set_variant", "espec_spo_variant_count",
+    "espec_spo_run_static", "espec_prop_create", "espec_prop_previous", "espec_prop_continue",
+    "espec_prop_energies", "espec_format_crl_row", "pspofft_", "psodfft_", "espec_grid_create",
+    "espec_grid_load", "espec_grid_run", "espec_grid_continue", "espec_grid_results",
+    "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy", "espec_grid_basis",
+    "espec_grid_previous", "espec_grid_energies_at", "espec_grid_set_pulse", "espec_pulse_field",
+    "espec_ppsod_field", "espec_pplnz_field", "plnz_", "psod_", "ppsod_", "pplnz_",
+    "espec_grid_project", "espec_run_deck", "espec_run_scan", "espec_spectrum_dev",
+    "espec_spectrum_work_bytes", "hwhm_", "spectrumtd_", "espec_eig_solve_dev",
+    "espec_eig_lcg_start", "espec_eig_morse2d", "espec_gemm_f64", "espec_gemm_f32",
+    "espec_gemm_bf16", "espec_gemm_bf16_status", "espec_mlp_bias_gelu", "espec_mlp_gelu_back",
+    "espec_to_bf16", "espec_mlp_adam_bf16", "espec_mlp_colsum", "espec_mlp_mse", "espec_sep_basis",
+    "espec_convert", "espec_spond_create", "espec_spond_load", "espec_spond_run",
     "espec_spond_results", "espec_spond_destroy", "espec_spond_continue", "espec_spond_energies",
     "espec_spond_create_method", "espec_spond_previous",
 ]
