@@ -349,19 +349,28 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   unsigned phase = 0;  // grid barriers passed in this launch
   constexpr int NW = kSilThreads / 32;
 
+  // this thread's sums for the norms of u, v and C of the state it wrote last
+  // (the expansion below accumulates them for the next step, in the same
+  // point order as the loop here)
+  double qn[6] = {0, 0, 0, 0, 0, 0};
   for (int s = 0;; ++s) {
     // ---- norms of u, v and C(s) = <psi0|psi(s)> (pspofft.f:119-120 form)
     {
       double q[6] = {0, 0, 0, 0, 0, 0};
-      for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-        const double uk = ld_state(a.u + k), vk = ld_state(a.v + k);
-        const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
-        q[0] += uk * uk;
-        q[1] += vk * vk;
-        q[2] += u0k * uk;
-        q[3] += v0k * vk;
-        q[4] += u0k * vk;
-        q[5] += v0k * uk;
+      if (s == 0) {
+        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+          const double uk = ld_state(a.u + k), vk = ld_state(a.v + k);
+          const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
+          q[0] += uk * uk;
+          q[1] += vk * vk;
+          q[2] += u0k * uk;
+          q[3] += v0k * vk;
+          q[4] += u0k * vk;
+          q[5] += v0k * uk;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < 6; ++i) q[i] = qn[i];
       }
       block_sum<6>(q, sp, scratch);
       if (!grid_reduce(a, sp, st, 6, s_flag, s_red, phase)) return;
@@ -504,6 +513,8 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
     krylov_coeffs(m, a.cst, a.quirk, s_al, s_bt, s_proj, s_active, ks, s_coef);
     const double* Lu = a.L;
     const double* Lv = a.L + (long)m * n;
+#pragma unroll
+    for (int i = 0; i < 6; ++i) qn[i] = 0.0;
     for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
       double lu[kSilMaxM], lv[kSilMaxM];
 #pragma unroll
@@ -529,6 +540,13 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
       }
       a.u[k] = un;
       a.v[k] = vn;
+      const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
+      qn[0] += un * un;
+      qn[1] += vn * vn;
+      qn[2] += u0k * un;
+      qn[3] += v0k * vn;
+      qn[4] += u0k * vn;
+      qn[5] += v0k * un;
     }
     __syncthreads();
   }
