@@ -76,13 +76,9 @@ static cudaError_t launch_diag_n(const DiagArgs& a, int nblocks, cudaStream_t st
     return cudaErrorInvalidConfiguration;
   } else {
     auto kern = diag1d_kernel<PL>;
-    static bool attr_set = false;
-    if (!attr_set) {
-      cudaError_t e =
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      attr_set = true;
-    }
+    static DeviceFlags attr_set;
+    cudaError_t e = set_max_smem_once(attr_set, kern, smem);
+    if (e != cudaSuccess) return e;
     kern<<<nblocks, PL::T, smem, st>>>(a);
     return cudaGetLastError();
   }

@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <string>
 
 namespace espec {
@@ -18,5 +19,24 @@ void digt_nd_table(int ndim, const int* np, const double* sh, const double* sm, 
 std::string spectrum_table(int mf, double dt, double de, const double* u, const double* v);
 inline int ck(cudaError_t e, const char* what) {
   return e == cudaSuccess ? 0 : set_cuda_error(what, e);
+}
+
+// cudaFuncSetAttribute(MaxDynamicSharedMemorySize) applies to the current
+// device only, so a kernel that needs more than 48 KB must have it set once
+// on every device it runs on.  One bit per device ordinal below 64 records
+// that; on higher ordinals the attribute is set before every launch.
+struct DeviceFlags {
+  std::atomic<unsigned long long> bits{0};
+};
+template <class K>
+inline cudaError_t set_max_smem_once(DeviceFlags& f, K kern, size_t smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const unsigned long long bit = (dev >= 0 && dev < 64) ? (1ull << dev) : 0ull;
+  if (bit && (f.bits.load(std::memory_order_acquire) & bit)) return cudaSuccess;
+  e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && bit) f.bits.fetch_or(bit, std::memory_order_release);
+  return e;
 }
 }  // namespace espec

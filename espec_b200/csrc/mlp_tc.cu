@@ -328,12 +328,10 @@ inline unsigned nblk(long count) { return (unsigned)((count + 255) / 256); }
 
 template <int BN>
 int launch_tc(const TcGemm& g, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
-    const cudaError_t e = cudaFuncSetAttribute(
-        gemm_bf16_tc<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes<BN>());
+  static DeviceFlags attr;
+  {
+    const cudaError_t e = set_max_smem_once(attr, gemm_bf16_tc<BN>, tc_smem_bytes<BN>());
     if (e != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e);
-    attr = true;
   }
   dim3 grid((g.N + BN - 1) / BN, (g.M + kBM - 1) / kBM);
   gemm_bf16_tc<BN><<<grid, kTcThreads, tc_smem_bytes<BN>(), st>>>(g);

@@ -11,13 +11,9 @@ static cudaError_t launch_sod_one(const SodArgs& a, int nblocks, cudaStream_t st
     return cudaErrorInvalidConfiguration;  // size rejected at plan creation
   } else {
     auto kern = sod1d_kernel<PL, kAbs>;
-    static bool attr_set = false;
-    if (!attr_set) {
-      cudaError_t e =
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      attr_set = true;
-    }
+    static DeviceFlags attr_set;
+    cudaError_t e = set_max_smem_once(attr_set, kern, smem);
+    if (e != cudaSuccess) return e;
     kern<<<nblocks, PL::T, smem, st>>>(a);
     return cudaGetLastError();
   }

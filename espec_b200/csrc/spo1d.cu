@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -423,6 +424,10 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
       delete p;
       return set_error(ESPEC_EINVAL, "unsupported packet size for SOD (supported: 256 to 2048)");
     }
+    if ((long long)p->off[i] + p->n[i] > INT_MAX) {
+      delete p;
+      return set_error(ESPEC_EINVAL, "more than 2^31 - 1 grid points in one plan");
+    }
     p->off[i + 1] = p->off[i] + p->n[i];
   }
   p->npts = p->off[npk];
@@ -625,7 +630,7 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
     // packet descriptors carry the C(t) offsets
     std::map<int, std::vector<SpoPacket>> cls;
     for (int i = 0; i < p->npk; ++i)
-      cls[p->n[i]].push_back(SpoPacket{p->off[i], i * (nsteps + 1)});
+      cls[p->n[i]].push_back(SpoPacket{p->off[i], (long long)i * (nsteps + 1)});
     for (auto& c : p->classes) {
       auto& v = cls[c.n];
       ESPEC_CK(cudaMemcpy(c.d_pk, v.data(), sizeof(SpoPacket) * v.size(), cudaMemcpyHostToDevice));

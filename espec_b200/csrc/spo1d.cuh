@@ -148,8 +148,8 @@ struct SpoTables {
 };
 
 struct SpoPacket {
-  int off;       // first point of the packet in the concatenated arrays
-  int c_off;     // first C(t) sample of the packet
+  int off;         // first point of the packet in the concatenated arrays
+  long long c_off;  // first C(t) sample of the packet (npk * (nsteps + 1) may pass 2^31)
 };
 
 template <typename R>

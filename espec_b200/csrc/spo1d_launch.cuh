@@ -4,6 +4,7 @@
 // SM); the autotuner (espec_b200/autotune.py) measures them and the
 // per-size defaults of spo1d.cu come from its results on B200.
 #pragma once
+#include "espec_internal.h"
 #include "spo1d.cuh"
 
 namespace espec {
@@ -47,13 +48,9 @@ static cudaError_t launch_one(const SpoArgs<R>& a, int nblocks, cudaStream_t st)
     return cudaErrorInvalidConfiguration;  // never selected: rejected by variant_fits
   } else {
     auto kern = spo1d_kernel<R, PL, false, kQuirk, kTab, kMinB>;
-    static bool attr_set = false;  // one flag per instantiation
-    if (!attr_set) {
-      cudaError_t e =
-          cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      if (e != cudaSuccess) return e;
-      attr_set = true;
-    }
+    static DeviceFlags attr_set;  // per instantiation, one bit per device
+    cudaError_t e = set_max_smem_once(attr_set, kern, smem);
+    if (e != cudaSuccess) return e;
     kern<<<nblocks, PL::T, smem, st>>>(a);
     return cudaGetLastError();
   }

@@ -26,6 +26,10 @@
 // with cudaGetSymbolAddress and caches it for that device (device code
 // names the array directly, host code only passes the resolved pointer).
 // Make that first call on each device before any stream capture begins.
+// The cached address assumes one CUDA context per device for the life of the
+// process (the runtime's primary context): after cudaDeviceReset the cache
+// would hold a stale address, so a process that resets a device must not
+// call this entry on it again.
 #include <cuda_runtime.h>
 
 #include "espec_gpu.h"
@@ -241,7 +245,7 @@ extern "C" int espec_spo_run_static(int npk, const int* npts, const double* sh, 
     cls_count[c] = 0;
     for (int i = 0; i < npk; ++i)
       if (npts[i] == sr.n[c]) {
-        pk[m++] = SpoPacket{off[i], i * (nsteps + 1)};
+        pk[m++] = SpoPacket{off[i], (long long)i * (nsteps + 1)};
         cls_count[c]++;
       }
   }

@@ -749,13 +749,11 @@ cudaError_t launch_x_n(int nx, int mode, const NdArgs<R>& a, int blocks, cudaStr
 
 template <typename R, int P, int MODE, bool Q>
 cudaError_t launch_axis1(const NdArgs<R>& a, int axis, long, cudaStream_t st) {
-  static bool attr = false;
-  if (!attr) {
+  static DeviceFlags attr;
+  {
     const size_t smax = sizeof(cpx<R>) * 32 * P * (kMaxWarps + 1);
-    cudaError_t e = cudaFuncSetAttribute(axis_pass<R, P, MODE, Q>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smax);
+    cudaError_t e = set_max_smem_once(attr, axis_pass<R, P, MODE, Q>, smax);
     if (e != cudaSuccess) return e;
-    attr = true;
   }
   const long other = axis == 1 ? a.nz : a.ny;  // line sets beside the x tiles
   const int w = warps_for((long)a.nx * other);

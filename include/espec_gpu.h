@@ -266,7 +266,9 @@ void espec_spo_destroy(espec_spo_plan* plan);
  * No absorber; C(t) every step, same arithmetic as variant 0 of the plans.
  * Calls share the array: calls whose GPU work overlaps race; serialise them.
  * The first call on each device resolves the array's address; make it
- * before any stream capture.  Sizes beyond the limits return ESPEC_EINVAL.
+ * before any stream capture.  That address is cached for the life of the
+ * process (one primary context per device; do not call again on a device
+ * after cudaDeviceReset).  Sizes beyond the limits return ESPEC_EINVAL.
  * ---------------------------------------------------------------------- */
 int espec_spo_run_static(int npk, const int* npts, const double* sh,
                          const double* sm, double dt_fs, int precision,

@@ -167,7 +167,16 @@ void stockham_pass(const cd* x, cd* y, int n, int l, int r, const cd* tw, int si
 
 // unnormalised DFT of x in place: sign > 0 -> exp(+2 pi i jk/n)
 void dft_line(cd* x, int n, int sign) {
-  const FftPlan& pl = fft_plan(n);
+  // per-thread memo of the last plan: the shared cache's lock is taken once
+  // per length and thread, not once per line (host threads of the batched
+  // CPU runs would otherwise contend on it every step)
+  thread_local int memo_n = 0;
+  thread_local const FftPlan* memo = nullptr;
+  if (memo_n != n) {
+    memo = &fft_plan(n);
+    memo_n = n;
+  }
+  const FftPlan& pl = *memo;
   thread_local std::vector<cd> buf;
   if ((int)buf.size() < n) buf.resize(n);
   cd* a = x;
@@ -1584,12 +1593,80 @@ extern "C" int orc_spectrumtd(int window_sg, int mf, double dtf, double tf, doub
 // step (pspofft.f:115-123, LC = 1).  Packets are spread over nthreads host
 // threads through a shared packet counter.
 // ---------------------------------------------------------------------------
+// The same step as orc_spo_step for a 1D packet without absorber, with the
+// cosines and sines of the V half-phase and of the kinetic phase computed
+// once per packet instead of every step (spofft.f recomputes them, 3N DCOS
+// and DSIN per step).  Every product and sum is the one orc_spo_step forms,
+// in the same order, so the results are bit for bit the same; only the
+// repeated sincos calls are gone, which makes this CPU baseline faster per
+// core than the reference's own loop.
+struct SpoCached {
+  int n = 0;
+  std::vector<double> cv, sv;  // cos/sin(cst2 V(i))
+  std::vector<double> ck, sk;  // cos/sin(cst1 TC(i))
+};
+
+static void spo_cached_init(SpoCached& c, int n, double cst1, double cst2, const double* tc,
+                            const double* vpot) {
+  c.n = n;
+  c.cv.resize(n);
+  c.sv.resize(n);
+  c.ck.resize(n);
+  c.sk.resize(n);
+  for (int i = 0; i < n; ++i) {
+    sincos(cst2 * vpot[i], &c.sv[i], &c.cv[i]);
+    sincos(cst1 * tc[i], &c.sk[i], &c.ck[i]);
+  }
+}
+
+static void spo_step_cached(const SpoCached& c, double b, int quirks, double* u, double* v) {
+  const int n = c.n, nh = n / 2;
+  const double *cv = c.cv.data(), *sv = c.sv.data();
+  for (int i = 0; i < nh; ++i) {
+    const double c1 = cv[i], s1 = sv[i];
+    double ua = c1 * u[i] + s1 * v[i];
+    double va = c1 * v[i] - s1 * u[i];
+    const double c2 = cv[i + nh], s2 = sv[i + nh];
+    u[i] = c2 * u[i + nh] + s2 * v[i + nh];
+    v[i] = c2 * v[i + nh] - s2 * u[i + nh];
+    u[i + nh] = ua;
+    v[i + nh] = va;
+  }
+  int np[3] = {n, 1, 1};
+  fft_all_axes(1, np, n, u, v, 1);
+  for (int i = 0; i < n; ++i) {
+    const double cc = c.ck[i], s = c.sk[i];
+    double un = cc * u[i] + s * v[i];
+    if (quirks & ORC_Q_SPO_INPLACE) {
+      u[i] = un;
+      v[i] = cc * v[i] - s * u[i];
+    } else {
+      v[i] = cc * v[i] - s * u[i];
+      u[i] = un;
+    }
+  }
+  fft_all_axes(1, np, n, u, v, -1);
+  for (int i = 0; i < nh; ++i) {
+    const double c1 = cv[i + nh], s1 = sv[i + nh];
+    double ua = c1 * b * u[i] + s1 * b * v[i];
+    double va = c1 * b * v[i] - s1 * b * u[i];
+    const double c2 = cv[i], s2 = sv[i];
+    double un = c2 * b * u[i + nh] + s2 * b * v[i + nh];
+    double vn = c2 * b * v[i + nh] - s2 * b * u[i + nh];
+    u[i] = un;
+    v[i] = vn;
+    u[i + nh] = ua;
+    v[i + nh] = va;
+  }
+}
+
 extern "C" int orc_spo_batch(int npk, const int* off, const double* sh, const double* sm,
                              const double* vpot, double* u, double* v, double dt_fs,
                              int nsteps, int quirks, double* c_re, double* c_im,
                              int nthreads) {
   std::atomic<int> next{0};
   auto worker = [&]() {
+    SpoCached cache;
     for (;;) {
       const int k = next.fetch_add(1);
       if (k >= npk) return;
@@ -1602,12 +1679,11 @@ extern "C" int orc_spo_batch(int npk, const int* off, const double* sh, const do
       int np[3] = {n, 1, 1};
       orc_digt(1, np, sh + k, sm + k, tc.data(), &b, 0);
       const double cst1 = dt_fs / ORC_SHFS, cst2 = dt_fs / (2.0 * ORC_SHFS);
+      spo_cached_init(cache, n, cst1, cst2, tc.data(), vp);
       double* cr = c_re + (size_t)k * (nsteps + 1);
       double* ci = c_im + (size_t)k * (nsteps + 1);
       for (int s = 0; s <= nsteps; ++s) {
-        if (s > 0)
-          orc_spo_step(1, np, b, cst1, cst2, tc.data(), vp, nullptr, ORC_ABS_NONE, quirks, uk,
-                       vk);
+        if (s > 0) spo_step_cached(cache, b, quirks, uk, vk);
         cr[s] = orc_fcorrel(n, u0.data(), uk) + orc_fcorrel(n, v0.data(), vk);
         ci[s] = orc_fcorrel(n, u0.data(), vk) - orc_fcorrel(n, v0.data(), uk);
       }

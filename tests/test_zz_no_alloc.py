@@ -28,7 +28,9 @@ def _plan_reference(E, w, precision):
     return c, p
 
 
-def _static_call(lib, w, precision, torch):
+def _static_buffers(w, torch):
+    """Device inputs and outputs of one call, allocated by the test (the
+    entry point itself allocates nothing)."""
     dev = torch.device("cuda")
     npk = int(w["npk"])
     ns = int(w["nsteps"])
@@ -38,6 +40,13 @@ def _static_call(lib, w, precision, torch):
     p0 = torch.from_numpy(psi).to(dev)
     c_out = torch.full((2 * npk * (ns + 1),), np.nan, dtype=torch.float64, device=dev)
     p_out = torch.full((2 * w["psi"].size,), np.nan, dtype=torch.float64, device=dev)
+    return v, p0, c_out, p_out
+
+
+def _static_run(lib, w, precision, torch, bufs):
+    v, p0, c_out, p_out = bufs
+    npk = int(w["npk"])
+    ns = int(w["nsteps"])
     n = np.ascontiguousarray(w["n"], dtype=np.int32)
     sh = np.ascontiguousarray(w["sh"], dtype=np.float64)
     sm = np.ascontiguousarray(w["sm"], dtype=np.float64)
@@ -49,9 +58,20 @@ def _static_call(lib, w, precision, torch):
                                   p_out.data_ptr(), stream)
     assert rc == 0, lib.espec_last_error()
     torch.cuda.synchronize()
-    c = c_out.cpu().numpy()
-    p = p_out.cpu().numpy()
+
+
+def _static_read(w, bufs):
+    npk = int(w["npk"])
+    ns = int(w["nsteps"])
+    c = bufs[2].cpu().numpy()
+    p = bufs[3].cpu().numpy()
     return (c[0::2] + 1j * c[1::2]).reshape(npk, ns + 1), p[0::2] + 1j * p[1::2]
+
+
+def _static_call(lib, w, precision, torch):
+    bufs = _static_buffers(w, torch)
+    _static_run(lib, w, precision, torch, bufs)
+    return _static_read(w, bufs)
 
 
 @pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 5e-6)])
@@ -72,6 +92,36 @@ def test_static_entry_matches_plan_entry_on_two_calls(precision, tol):
         assert np.all(np.isfinite(c)) and np.all(np.isfinite(p))
         assert np.max(np.abs(c - c_ref)) <= tol
         assert np.max(np.abs(p - p_ref)) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [("fp64", 1e-10), ("mixed", 5e-6)])
+def test_static_entry_at_its_limit_allocates_nothing(precision, tol):
+    """128 packets of 256 points (exactly the 32768-point, 128-packet limit of
+    the scratch layout).  The first call may load kernels; the free device
+    memory seen by cudaMemGetInfo around the second, identical call must not
+    move."""
+    torch = pytest.importorskip("torch")
+    import espec_b200 as E
+    from espec_b200 import _native as N
+    from espec_b200 import workloads as W
+
+    lib = N.load()
+    prec = {"fp64": N.FP64, "mixed": N.MIXED}[precision]
+    w = W.morse_scan(npk=128, nsteps=120, seed=43, sizes=(256,))
+    assert int(w["off"][-1]) == 32768
+    bufs = _static_buffers(w, torch)
+    _static_run(lib, w, prec, torch, bufs)
+    c1, p1 = _static_read(w, bufs)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    _static_run(lib, w, prec, torch, bufs)
+    free1, _ = torch.cuda.mem_get_info()
+    c2, p2 = _static_read(w, bufs)
+    c_ref, p_ref = _plan_reference(E, w, precision)
+    assert np.array_equal(c1, c2) and np.array_equal(p1, p2)
+    assert np.max(np.abs(c2 - c_ref)) <= tol
+    assert np.max(np.abs(p2 - p_ref)) <= tol
+    assert free1 == free0
 
 
 def test_static_entry_rejects_sizes_beyond_its_limit():
