@@ -1,15 +1,21 @@
 #!/usr/bin/env python3
-"""Benchmark: batched 1D Morse scan, mixed precision, one persistent launch.
+"""Benchmark: batched 1D Morse scan at |dC(t)| <= 1e-6, one GPU.
 
 Workload (one "step" = one full propagation of the batch): 4096 independent
 1D Morse packets with N ~ U{256,384,512,768,1024,1536,2048} on [0.5, 8] bohr,
 De ~ U[0.05,0.25] Eh, a ~ U[0.6,1.6] /bohr, re ~ U[1.0,2.5] bohr,
 m ~ U[900,30000] m_e, Gaussian packets, dt = 0.5 au, 8000 time steps, C(t)
 recorded every time step (seed 20261203).  Metric: grid-point time steps per
-second (Mgridpt*steps/s) over the whole job; packets/s reported beside it.
+second (Mgridpt*steps/s) over the whole job, of the form that holds
+|dC(t)| <= 1e-6 against the FP64 oracle: the FP64 form (<= 1e-10).  The
+mixed form (FP32 state) is a further leg with its measured error: an FP32
+state cannot hold 1e-6 over 8000 steps of this scan
+(tests/test_fp32_state_floor.py).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision mixed|fp64] [--npk 4096] [--nsteps 8000]
+                    [--precision fp64|mixed] [--npk 4096] [--nsteps 8000]
+    python bench.py --leg c1|c2|c3|mixed|sil_2d|psod_2d|grid_sweep|eig
+    python bench.py --case eig|spond2d|spond3d|spectrum|sil|gemm   (profiling)
 
 Multi-GPU (torchrun): packets are independent, each rank propagates its own
 batch (seed + rank) with no collective on the data path -> weak scaling.
@@ -28,12 +34,17 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "Mgridpt*steps/s (batched 1D Morse scan, mixed precision, C(t) every step)"
-ALG_BYTES = {"mixed": 28.0, "fp64": 56.0}  # per grid point per time step
-# DRAM bytes per grid-point step measured by ncu on one launch of the 2048-point
-# class (592 packets x 8000 steps, profiles/spo1d_kernel_2048_mixed_full.md):
-# the state stays on chip, HBM carries the tables once plus C(t) and psi(TF).
+METRIC = "Mgridpt*steps/s at |dC(t)| <= 1e-6 (batched 1D Morse scan, C(t) every step)"
+SHFS = 2.4188843243e-2  # fs per atomic time unit
+# algorithmic bytes per grid point and time step of the split operator: read
+# psi, write psi, read psi0 (for C(t)), read V
+ALG_BYTES = {"mixed": 28.0, "fp64": 56.0}
+# DRAM bytes per grid-point step measured by ncu on one launch of the
+# 2048-point class (592 packets x 8000 steps): the state stays on chip, HBM
+# carries the tables once plus C(t) and psi(TF)
 MEASURED_TRAFFIC_B = {"mixed": 0.0142, "fp64": None}
+SCAN_SEED = 20261203
+GATE = 1e-6
 
 
 def parse():
@@ -42,18 +53,22 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"])
     ap.add_argument("--npk", type=int, default=4096)
     ap.add_argument("--nsteps", type=int, default=8000)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--sizes", default=None, help="comma list of packet sizes (profiling)")
-    ap.add_argument("--cpu-sample-steps", type=int, default=400)
-    ap.add_argument("--cpu-sample-packets", type=int, default=256)
-    ap.add_argument("--no-extra", action="store_true",
-                    help="skip the FP64-form, SIL-2D and eigensolver legs")
-    ap.add_argument("--leg", default=None, choices=["sil_2d", "psod_2d", "grid_sweep"],
-                    help="run one grid-plan leg alone and print its JSON (profiling)")
+    ap.add_argument("--ref-steps", type=int, default=200,
+                    help="time steps per timed step of the reference arm (all packets)")
+    ap.add_argument("--cpu-sample-steps", type=int, default=100)
+    ap.add_argument("--no-extra", action="store_true", help="skip the further legs")
+    ap.add_argument("--leg", default=None,
+                    choices=["c1", "c2", "c3", "mixed", "sil_2d", "psod_2d", "grid_sweep", "eig"],
+                    help="run one leg alone and print its JSON")
+    ap.add_argument("--case", default=None,
+                    choices=["eig", "spond2d", "spond3d", "spectrum", "sil", "gemm"],
+                    help="small self-checking workload for profiling one kernel")
     ap.add_argument("--leg-steps", type=int, default=100)
     ap.add_argument("--eig-train", type=int, default=50000)
     ap.add_argument("--eig-test", type=int, default=2048)
@@ -68,6 +83,24 @@ def measured_peaks():
             d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
+
+
+def scan_config(args):
+    """The workload's description, identical in both arms."""
+    return {"workload": "morse_scan_1d", "npk": args.npk, "nsteps": args.nsteps,
+            "seed": SCAN_SEED, "dt_au": 0.5, "precision": args.precision,
+            "l2": "inputs, tables and C(t) exceed L2 (126 MB) between timed steps"}
+
+
+def roofline(bytes_per_unit, units, ms, note=None, traffic=None):
+    peak, kind = measured_peaks()
+    achieved = bytes_per_unit * units / (ms * 1e-3) / 1e9
+    r = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+         "frac": achieved / peak, "peak_kind": kind, "bytes_per_gridpt_step": bytes_per_unit,
+         "traffic": traffic}
+    if note:
+        r["note"] = note
+    return r
 
 
 class ClockSampler:
@@ -116,8 +149,6 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
-SCAN_SEED = 20261203
-
 
 def rank_seed(rank):
     """Each rank propagates its own independent batch of the scan."""
@@ -158,14 +189,19 @@ def dist_init(args):
 
 
 def run_reference(args, world, rank):
-    """CPU reference arm: the oracle port of spofft.f/pspofft.f on all host
-    cores, on a bounded sample of the same workload."""
+    """CPU reference arm: the oracle port of spofft.f/pspofft.f (FP64, the
+    reference's arithmetic; phases computed once per packet, so it runs
+    faster per core than the shipped executable) on all host cores.  Each
+    timed step propagates ALL packets of the same seeded scan for
+    --ref-steps of its time steps: the cost of a time step does not depend
+    on its index, so the rate is the scan's.  Under torchrun rank 0 alone
+    runs; the other ranks exit without work."""
     if rank != 0:
         return
     from espec_b200 import workloads as W
     from oracle import oracle as O
 
-    w = W.morse_scan(npk=args.cpu_sample_packets, nsteps=args.cpu_sample_steps)
+    w = W.morse_scan(npk=args.npk, nsteps=args.ref_steps, seed=rank_seed(0))
     cores = os.cpu_count() or 1
     rates = []
     for it in range(args.warmup + args.steps):
@@ -176,12 +212,16 @@ def run_reference(args, world, rank):
         if it >= args.warmup:
             rates.append(w["off"][-1] * w["nsteps"] / dt / 1e6)
     v = float(np.median(rates))
-    sample = (f"{w['npk']} packets x {w['nsteps']} time steps of the scan workload per step "
-              f"({int(w['off'][-1])} grid points)")
+    sample = (f"all {w['npk']} packets of the scan (seed {SCAN_SEED}, {int(w['off'][-1])} grid "
+              f"points), {w['nsteps']} of the {args.nsteps} time steps per timed step")
     line = {"metric": METRIC, "value": v, "unit": "Mgridpt*steps/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
             "impl": "reference", "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "morse_scan_1d", "npk": args.npk, "nsteps": args.nsteps},
+            "config": scan_config(args),
+            "nsteps_timed": w["nsteps"],
+            "time_step_truncation": f"{w['nsteps']} of {args.nsteps} time steps per timed step, "
+                                    "all packets; per-time-step cost is independent of the step",
+            "ms_per_step": float(w["off"][-1] * w["nsteps"] / v / 1e3),
             "cpu_baseline": {"value": v, "unit": "Mgridpt*steps/s", "cores": cores,
                              "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "Mgridpt*steps/s", "h2d_bytes_per_step": 0,
@@ -191,10 +231,12 @@ def run_reference(args, world, rank):
 
 
 def cpu_baseline(args):
+    """The oracle port on all host cores, on a bounded sample: every packet of
+    the scan for --cpu-sample-steps time steps."""
     from espec_b200 import workloads as W
     from oracle import oracle as O
 
-    w = W.morse_scan(npk=args.cpu_sample_packets, nsteps=args.cpu_sample_steps)
+    w = W.morse_scan(npk=args.npk, nsteps=args.cpu_sample_steps, seed=rank_seed(0))
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
     O.spo_batch(w["off"], w["sh"], w["sm"], w["vpot"], w["psi"], np.zeros_like(w["psi"]),
@@ -202,38 +244,111 @@ def cpu_baseline(args):
     dt = time.perf_counter() - t0
     return {"value": float(w["off"][-1] * w["nsteps"] / dt / 1e6), "unit": "Mgridpt*steps/s",
             "cores": cores, "kind": "port",
-            "sample": f"{w['npk']} packets x {w['nsteps']} time steps of the scan workload"}
+            "sample": f"all {w['npk']} packets of the scan x {w['nsteps']} time steps"}
 
 
-def fp64_form(args, w, ms_mixed, dev):
-    """The plain FP64 GPU form on the same scan (BASELINE's comparison form),
-    and |dC(t)| of the mixed form against it on 256 packets of the scan."""
+def spectral_peaks(spec_abs, frac=0.02):
+    """Fractional bin positions of the local maxima of |S| above frac * max of
+    each row (parabola through log|S| of the three bins around a maximum)."""
+    out = []
+    for row in spec_abs:
+        l, r = np.roll(row, 1), np.roll(row, -1)
+        idx = np.nonzero((row > l) & (row >= r) & (row > frac * row.max()))[0]
+        a, b, c = (np.log(np.maximum(x[idx], 1e-300)) for x in (l, row, r))
+        den = a - 2.0 * b + c
+        d = np.where(den != 0.0, 0.5 * (a - c) / np.where(den != 0.0, den, 1.0), 0.0)
+        out.append(idx + d)
+    return out
+
+
+def peak_error_eh(spec_a, spec_b, dt_au):
+    """Largest shift (Eh) between the spectral peaks of two sets of spectra
+    (rows = packets, FFTNT order, 2^mf bins of 2 pi / (2^mf dt) Eh), each
+    peak of a matched to the nearest peak of b, and the number of peaks."""
+    n = spec_a.shape[1]
+    pa = spectral_peaks(np.abs(spec_a))
+    pb = spectral_peaks(np.abs(spec_b))
+    worst, count = 0.0, 0
+    for x, y in zip(pa, pb):
+        for p in x:
+            if len(y) == 0:
+                return float("inf"), count
+            d = (y - p + n / 2) % n - n / 2
+            worst = max(worst, float(np.min(np.abs(d))))
+            count += 1
+    return worst * 2.0 * np.pi / (n * dt_au), count
+
+
+def spectra_of(c, mf, dt_fs, dev):
+    """Spectra of C(t) rows on the GPU (espec_spectrum_dev: the C(t) assembly
+    of espec.f:1545-1576, the .SG window, FFTNT), as host arrays."""
+    import torch
+
+    from espec_b200 import spectrum as S
+
+    cd = torch.from_numpy(np.ascontiguousarray(c)).to(dev)
+    n = 1 << mf
+    out = S.spectra(cd, mf, dt_fs, (n // 2 - 1) * dt_fs, tal=None, window="SG", wp=1e-3)
+    return out.cpu().numpy()
+
+
+def dc_stats(c, c_ref):
+    d = np.abs(c - c_ref)
+    return {"max": float(d.max()), "rms": float(np.sqrt(np.mean(d ** 2))),
+            "frac_packets_within_1e-6": float(np.mean(d.max(axis=1) <= GATE))}
+
+
+def timed(fn, steps, dev):
+    """ms per call of fn on the current stream (CUDA events)."""
+    import torch
+
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    for _ in range(steps):
+        fn()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def leg_mixed(args, dev, ms_fp64=None, npk_acc=256):
+    """The mixed form (FP32 state and FFT, FP64 tables and C(t) sums) on the
+    scan: its rate against the FP64 form, and its error on 256 packets of the
+    scan over the full time loop against the oracle and the FP64 GPU form
+    (C(t) every step and the spectral peaks)."""
     import torch
 
     import espec_b200 as E
     from espec_b200 import workloads as W
+    from oracle import oracle as O
 
-    b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision="fp64")
+    out = {"workload": f"scan of {args.npk} packets x {args.nsteps} steps, mixed precision"}
+    w = W.morse_scan(npk=args.npk, nsteps=args.nsteps, seed=rank_seed(0))
+    pts = float(w["off"][-1]) * w["nsteps"]
     vpot_d = torch.from_numpy(w["vpot"]).to(dev)
     psi_d = torch.from_numpy(w["psi"]).to(dev)
     zero_d = torch.zeros_like(psi_d)
-    st = torch.cuda.current_stream(dev)
-    k = max(1, min(args.steps, 3))
-    for _ in range(1):
-        b.load(vpot_d, (psi_d, zero_d), stream=st.cuda_stream)
-        b.run(w["nsteps"], stream=st.cuda_stream)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(st)
-    for _ in range(k):
-        b.load(vpot_d, (psi_d, zero_d), stream=st.cuda_stream)
-        b.run(w["nsteps"], stream=st.cuda_stream)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / k
-    b.close()
-    # accuracy sample: 256 packets, full time loop, both forms
-    ws = W.morse_scan(npk=256, nsteps=w["nsteps"], seed=777)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    forms = {}
+    for prec in ("mixed", "fp64") if ms_fp64 is None else ("mixed",):
+        b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision=prec)
+
+        def step():
+            b.load(vpot_d, (psi_d, zero_d), stream=st)
+            b.run(w["nsteps"], stream=st)
+
+        step()
+        forms[prec] = timed(step, 3, dev)
+        b.close()
+    ms_fp64 = forms.get("fp64", ms_fp64)
+    out.update({"value": pts / (forms["mixed"] * 1e-3) / 1e6, "unit": "Mgridpt*steps/s",
+                "ms_per_step": forms["mixed"], "fp64_ms_per_step": ms_fp64,
+                "mixed_over_fp64": ms_fp64 / forms["mixed"],
+                "roofline": roofline(ALG_BYTES["mixed"], pts, forms["mixed"])})
+    # accuracy: the full time loop of npk_acc packets of the scan
+    ws = W.morse_scan(npk=npk_acc, nsteps=args.nsteps, seed=rank_seed(0))
     cs = {}
     for prec in ("mixed", "fp64"):
         bb = E.SpoBatch(ws["n"], ws["sh"], ws["sm"], ws["dt_fs"], precision=prec)
@@ -241,13 +356,171 @@ def fp64_form(args, w, ms_mixed, dev):
         bb.run(ws["nsteps"])
         cs[prec], _ = bb.results()
         bb.close()
-    dc = np.abs(cs["mixed"] - cs["fp64"])
-    pts = float(w["off"][-1]) * w["nsteps"]
-    return {"value": pts / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s", "ms_per_step": ms,
-            "mixed_over_fp64": ms / ms_mixed,
-            "dC_max_mixed_vs_fp64": float(dc.max()),
-            "dC_rms_mixed_vs_fp64": float(np.sqrt(np.mean(dc ** 2))),
-            "dC_sample": f"256 packets of the scan x {w['nsteps']} steps, every C(t) sample"}
+    cs["oracle"], _, _ = O.spo_batch(ws["off"], ws["sh"], ws["sm"], ws["vpot"], ws["psi"],
+                                     np.zeros_like(ws["psi"]), ws["dt_fs"], ws["nsteps"],
+                                     nthreads=os.cpu_count() or 1)
+    mf = int(np.floor(np.log2(ws["nsteps"] + 1))) + 1
+    sp = {k: spectra_of(v, mf, ws["dt_fs"], dev) for k, v in cs.items()}
+    pe_m, npeaks = peak_error_eh(sp["mixed"], sp["oracle"], 0.5)
+    pe_d, _ = peak_error_eh(sp["fp64"], sp["oracle"], 0.5)
+    out["accuracy"] = {
+        "sample": f"first {npk_acc} packets of the scan x {ws['nsteps']} steps, every C(t) "
+                  f"sample; spectra of 2^{mf} points (.SG window), {npeaks} peaks",
+        "mixed_vs_oracle_dC": dc_stats(cs["mixed"], cs["oracle"]),
+        "mixed_vs_fp64_dC": dc_stats(cs["mixed"], cs["fp64"]),
+        "fp64_vs_oracle_dC": dc_stats(cs["fp64"], cs["oracle"]),
+        "peak_err_eh_mixed": pe_m, "peak_err_eh_fp64": pe_d,
+        "gate": {"dC": GATE, "peak_eh": GATE},
+        "note": "an FP32 state alone (one rounding per step, exact arithmetic otherwise) "
+                "passes 1e-6 on the scan's heavy N = 256/384 packets within 8000 steps "
+                "(tests/test_fp32_state_floor.py); the FP64 form meets the gate"}
+    return out
+
+
+def _box_cap(q, strength=0.01, frac=0.15):
+    """Quadratic absorbing potential W(q) = strength * s^2 on the outer frac of
+    an axis (s = depth into the layer, 0 at its inner edge, 1 at the box edge)."""
+    lo, hi = q[0], q[-1]
+    width = frac * (hi - lo)
+    s = np.maximum(np.maximum(lo + width - q, q - (hi - width)), 0.0) / width
+    return strength * s ** 2
+
+
+def leg_c1(dev):
+    """Config 1: one 1D Morse packet (N = 1024 on [0.5, 8] bohr, De 0.17 Eh,
+    a 1 /bohr, re 1.4 bohr, m 918 m_e, Gaussian at 1.8 bohr, sigma 0.2),
+    dt = 0.5 au, 20000 steps, C(t) every step; FP64 and mixed against the
+    oracle, with the spectral peaks of C(t)."""
+    import espec_b200 as E
+    from espec_b200 import workloads as W
+    from oracle import oracle as O
+
+    w = W.morse1d()
+    n, ns = w["n"], w["nsteps"]
+    off = np.array([0, n])
+    c_ref, _, _ = O.spo_batch(off, [w["sh"]], [w["sm"]], w["vpot"], w["psi"], np.zeros(n),
+                              w["dt_fs"], ns)
+    out = {"workload": "1D Morse, N = 1024, dt = 0.5 au, 20000 steps, one packet",
+           "unit": "Mgridpt*steps/s"}
+    mf = int(np.floor(np.log2(ns + 1))) + 1
+    sp_ref = spectra_of(c_ref, mf, w["dt_fs"], dev)
+    for prec in ("fp64", "mixed"):
+        b = E.SpoBatch([n], [w["sh"]], [w["sm"]], w["dt_fs"], precision=prec)
+        b.load(w["vpot"], w["psi"])
+        b.run(ns)
+
+        def step():
+            b.run(ns)
+
+        ms = timed(step, 2, dev)
+        c, _ = b.results()
+        b.close()
+        pe, npk_ = peak_error_eh(spectra_of(c, mf, w["dt_fs"], dev), sp_ref, 0.5)
+        out[prec] = {"value": n * ns / (ms * 1e-3) / 1e6, "us_per_step": ms * 1e3 / ns,
+                     "ms_per_run": ms, "dC_vs_oracle_max": float(np.max(np.abs(c - c_ref))),
+                     "peak_err_eh": pe, "peaks": npk_,
+                     "roofline": roofline(ALG_BYTES[prec], n * ns, ms,
+                                          note="one packet = one CTA on one SM: the run is "
+                                               "bound by the step's latency")}
+    return out
+
+
+def leg_c2(dev, nsteps=10000):
+    """Config 2: 2D coupled Morse on 256 x 256 ([0.5, 8] bohr both axes, masses
+    918 / 1500, bilinear coupling 0.01), quadratic CAP 0.01 Eh on the outer
+    15 % of each edge, displaced Gaussian, dt = 1 au, 10000 steps: the split
+    operator (FP64 and mixed; CAP as .VOPTIC) and SIL of order 12 (CAP as the
+    per-step mask exp(-W dt), SIL's .SMOOTHW form)."""
+    import espec_b200 as E
+    from espec_b200 import _native as N
+
+    n = 256
+    x = np.linspace(0.5, 8.0, n)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    morse = lambda q, de, a, re: de * (1 - np.exp(-a * (q - re))) ** 2  # noqa: E731
+    V = morse(X, 0.17, 1.0, 1.4) + morse(Y, 0.12, 1.2, 1.8) + 0.01 * (X - 1.4) * (Y - 1.8)
+    Wc = _box_cap(x)[:, None] + _box_cap(x)[None, :]
+    psi = np.exp(-((X - 1.6) ** 2) / (2 * 0.15 ** 2) - ((Y - 2.0) ** 2) / (2 * 0.15 ** 2))
+    psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
+    v, wv = V.ravel(order="F"), Wc.ravel(order="F")
+    h = x[1] - x[0]
+    dt_au = 1.0
+    dt = dt_au * SHFS
+    out = {"workload": "2D coupled Morse 256x256, CAP 0.01 Eh on the outer 15 %, dt = 1 au, "
+                       f"{nsteps} steps", "unit": "Mgridpt*steps/s"}
+    cs = {}
+    for prec in ("fp64", "mixed"):
+        g = E.SpoGrid([n, n], [h, h], [918.0, 1500.0], dt, precision=prec, absorb=N.ABS_VOPTIC)
+        g.load(v, psi, vabc=-wv)
+        g.run(10)
+        ms = timed(lambda: g.run(nsteps), 1, dev)
+        cs[prec], _ = g.results()
+        g.close()
+        out[f"spo_{prec}"] = {"value": n * n * nsteps / (ms * 1e-3) / 1e6,
+                              "us_per_step": ms * 1e3 / nsteps,
+                              "roofline": roofline(ALG_BYTES[prec], n * n * nsteps, ms)}
+    out["spo_mixed_vs_fp64_dC_max"] = float(np.max(np.abs(cs["mixed"] - cs["fp64"])))
+    m = 12
+    shm = [1.0 / (((24.0 * mm) * h) * h) for mm in (918.0, 1500.0)]
+    g = E.SilGrid([n, n], shm, dt, m, absorb=N.ABS_SMOOTHW)
+    g.load(v, psi, vabc=np.exp(-wv * dt_au))
+    g.run(5)
+    ms = timed(lambda: g.run(nsteps), 1, dev)
+    c_sil, _ = g.results()
+    g.close()
+    out["sil12_fp64"] = {"value": n * n * nsteps / (ms * 1e-3) / 1e6,
+                         "us_per_step": ms * 1e3 / nsteps,
+                         "roofline": roofline(sil_bytes(m), n * n * nsteps, ms,
+                                              note="basis (12.6 MB) and state stay in L2: the "
+                                                   "step is bound by its 2m grid-wide "
+                                                   "reductions")}
+    out["sil_vs_spo_fp64_dC_max"] = float(np.max(np.abs(c_sil - cs["fp64"])))
+    return out
+
+
+def leg_c3(dev, nsteps=5000, box=2.5):
+    """Config 3: 3D anharmonic oscillator on 128^3 (q in [-2.5, 2.5] bohr per
+    axis), harmonic omega = 0.01 / 0.012 / 0.015 Eh, m = 1836 m_e, cubic
+    coupling 1e-4 (x^2 y - y^3/3), quadratic CAP 0.01 Eh on the outer 15 % of
+    every edge, ground-state-width Gaussian displaced by 0.3 bohr along x,
+    dt = 2 au, 5000 steps: mixed against FP64 (C(t) and spectral peaks)."""
+    import espec_b200 as E
+    from espec_b200 import _native as N
+
+    n = 128
+    q = np.linspace(-box, box, n)
+    G = np.meshgrid(q, q, q, indexing="ij")
+    om, m = [0.01, 0.012, 0.015], 1836.0
+    V = sum(0.5 * m * om[a] ** 2 * G[a] ** 2 for a in range(3)) + 1e-4 * (
+        G[0] ** 2 * G[1] - G[1] ** 3 / 3)
+    cap = _box_cap(q)
+    Wc = cap[:, None, None] + cap[None, :, None] + cap[None, None, :]
+    p3 = np.exp(-sum(m * om[a] / 2 * (G[a] - (0.3 if a == 0 else 0.0)) ** 2 for a in range(3)))
+    p3 = (p3 / np.sqrt(np.sum(p3 ** 2))).ravel(order="F").astype(complex)
+    v, wv = V.ravel(order="F"), Wc.ravel(order="F")
+    dt_au = 2.0
+    dt = dt_au * SHFS
+    npts = n ** 3
+    out = {"workload": f"3D anharmonic oscillator 128^3, CAP at the edges, dt = 2 au, "
+                       f"{nsteps} steps", "unit": "Mgridpt*steps/s"}
+    cs = {}
+    for prec in ("fp64", "mixed"):
+        g = E.SpoGrid([n, n, n], [q[1] - q[0]] * 3, [m] * 3, dt, precision=prec,
+                      absorb=N.ABS_VOPTIC)
+        g.load(v, p3, vabc=-wv)
+        g.run(10)
+        ms = timed(lambda: g.run(nsteps), 1, dev)
+        cs[prec], _ = g.results()
+        g.close()
+        out[prec] = {"value": npts * nsteps / (ms * 1e-3) / 1e6, "us_per_step": ms * 1e3 / nsteps,
+                     "roofline": roofline(ALG_BYTES[prec], npts * nsteps, ms)}
+    d = np.abs(cs["mixed"] - cs["fp64"])
+    mf = int(np.floor(np.log2(nsteps + 1))) + 1
+    pe, npeaks = peak_error_eh(spectra_of(cs["mixed"][None, :], mf, dt, dev),
+                               spectra_of(cs["fp64"][None, :], mf, dt, dev), dt_au)
+    out["mixed_vs_fp64"] = {"dC_max": float(d.max()), "dC_at_1000": float(d[:1001].max()),
+                            "peak_err_eh": pe, "peaks": npeaks}
+    return out
 
 
 def sil_2d(dev, steps=100, cpu_steps=2):
@@ -403,59 +676,6 @@ def psod_2d(dev, steps=100, cpu_steps=20):
     return out
 
 
-def spo_nd(dev):
-    """Split operator on 2D (256x256 coupled Morse, FP64, dt = 1 au) and 3D
-    (128^3 anharmonic oscillator, mixed vs FP64, dt = 2 au) grids."""
-    import torch
-
-    import espec_b200 as E
-
-    out = {}
-    shfs = 2.4188843243e-2
-    # 2D: the coupled-Morse potential of the SIL leg
-    x = np.linspace(0.5, 8.0, 256)
-    X, Y = np.meshgrid(x, x, indexing="ij")
-    morse = lambda q, de, a, re: de * (1 - np.exp(-a * (q - re))) ** 2  # noqa: E731
-    V = morse(X, 0.17, 1.0, 1.4) + morse(Y, 0.12, 1.2, 1.8) + 0.01 * (X - 1.4) * (Y - 1.8)
-    psi = np.exp(-((X - 1.6) ** 2) / (2 * 0.15 ** 2) - ((Y - 2.0) ** 2) / (2 * 0.15 ** 2))
-    psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
-    cases = [("spo_2d", [256, 256], V.ravel(order="F"), psi, [x[1] - x[0]] * 2, [918.0, 1500.0],
-              1.0, 2000)]
-    # 3D: three harmonic modes (omega = 0.01/0.012/0.015 Eh, m = 1836) + cubic coupling
-    q = np.linspace(-60.0, 60.0, 128)
-    G = np.meshgrid(q, q, q, indexing="ij")
-    w, m = [0.01, 0.012, 0.015], 1836.0
-    V3 = sum(0.5 * m * w[a] ** 2 * G[a] ** 2 for a in range(3)) + 1e-4 * (
-        G[0] ** 2 * G[1] - G[1] ** 3 / 3)
-    p3 = np.exp(-sum(m * w[a] / 2 * (G[a] - (2.0 if a == 0 else 0.0)) ** 2 for a in range(3)))
-    p3 = (p3 / np.sqrt(np.sum(p3 ** 2))).ravel(order="F").astype(complex)
-    cases.append(("spo_3d", [128, 128, 128], V3.ravel(order="F"), p3, [q[1] - q[0]] * 3, [m] * 3,
-                  2.0, 1000))
-    for name, np_, v, psi0, sh, sm, dt_au, nsteps in cases:
-        n = int(np.prod(np_))
-        res, cs = {}, {}
-        for prec in ("mixed", "fp64"):
-            g = E.SpoGrid(np_, sh, sm, dt_au * shfs, precision=prec)
-            g.load(v, psi0)
-            g.run(10)
-            g.results()
-            st = torch.cuda.current_stream(dev)
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(st)
-            g.run(nsteps)
-            e1.record(st)
-            cs[prec], _ = g.results()
-            ms = e0.elapsed_time(e1) / nsteps
-            res[prec] = {"value": n / (ms * 1e-3) / 1e6, "unit": "Mgridpt*steps/s",
-                         "us_per_step": ms * 1e3}
-            g.close()
-        d = np.abs(cs["mixed"] - cs["fp64"])
-        out[name] = {"grid": "x".join(map(str, np_)), "dt_au": dt_au, "steps_timed": nsteps,
-                     "fp64": res["fp64"], "mixed": res["mixed"],
-                     "dC_max_mixed_vs_fp64": float(d.max())}
-    return out
-
-
 def eig_warmstart(args, dev):
     """Lanczos H*v applications to the 4 lowest states of 128x128 coupled-Morse
     potentials: cold start (the reference's LCG vectors) vs the learned warm
@@ -497,6 +717,76 @@ def eig_warmstart(args, dev):
             "warm_solve_s": t4 - t3, "unit": "H*v applications per potential (4 states)"}
 
 
+def profile_case(name, dev):
+    """Small, self-checking workloads for profiling one kernel of the library
+    (one launch or a few, a few MB on the device); returns a finite number."""
+    import torch
+
+    import espec_b200 as E
+
+    if name == "eig":  # eig_kernel: 32 potentials, 128x128, 4 states
+        from espec_b200 import eig as EG
+        from espec_b200 import warmstart as WS
+
+        g = EG.Grid2D((128, 128))
+        q = torch.tensor(WS.sample_params(32, 7), dtype=torch.float64, device=dev)
+        v = EG.morse2d_potentials(g, q)
+        st = EG.lcg_start(g.n, 4, dev).expand(32, 4, g.n).contiguous()
+        r = EG.solve(g, v, st, nstates=4, m=40, tol=1e-9, maxrest=300)
+        return float(r["resid"].max())
+    if name in ("spond2d", "spond3d"):  # x_pass / axis_pass passes
+        np_, prec, nsteps = ([256, 256], "fp64", 20) if name == "spond2d" else \
+            ([128, 128, 128], "mixed", 10)
+        axes = [np.linspace(0.6, 3.6, k) for k in np_]
+        G = np.meshgrid(*axes, indexing="ij")
+        v = sum(0.15 * (1 - np.exp(-(g - 1.6))) ** 2 for g in G)
+        psi = np.exp(-sum((g - 1.9) ** 2 / 0.05 for g in G)).astype(complex)
+        psi /= np.sqrt(np.sum(np.abs(psi) ** 2))
+        s = E.SpoGrid(np_, [a[1] - a[0] for a in axes], [918.0] * len(np_), 0.5 * SHFS,
+                      precision=prec)
+        s.load(v.ravel(order="F"), psi.ravel(order="F"))
+        s.run(nsteps)
+        c, _ = s.results()
+        s.close()
+        return float(np.abs(c[-1]))
+    if name == "spectrum":  # spec_* kernels: 4096 packets' C(t), 2^13 points
+        from espec_b200 import spectrum as S
+
+        t = np.arange(4096)[:, None] * 0.01
+        c = np.exp(-1j * t * np.linspace(0.1, 0.5, 4096)[None, :]).T.copy()
+        out = S.spectra(torch.from_numpy(c).to(dev), 13, 0.01, 4096 * 0.01, tal=0.01,
+                        window="SG")
+        return float(out.abs().max())
+    if name == "sil":  # sil_kernel: 256x256, order 12, 20 steps
+        n = 256
+        x = np.linspace(0.5, 8.0, n)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        v = 0.17 * (1 - np.exp(-(X - 1.4))) ** 2 + 0.12 * (1 - np.exp(-1.2 * (Y - 1.8))) ** 2
+        psi = np.exp(-((X - 1.6) ** 2 + (Y - 2.0) ** 2) / 0.045).astype(complex)
+        psi /= np.sqrt(np.sum(np.abs(psi) ** 2))
+        h = x[1] - x[0]
+        g = E.SilGrid([n, n], [1 / (24 * 918 * h * h), 1 / (24 * 1500 * h * h)], SHFS, 12)
+        g.load(v.ravel(order="F"), psi.ravel(order="F"))
+        g.run(20)
+        c, _ = g.results()
+        g.close()
+        return float(np.abs(c[-1]))
+    if name == "gemm":  # gemm_bf16_tc: the warm start's output layer on 2048 proposals
+        from espec_b200 import warmstart as WS
+
+        gen = torch.Generator(device=dev).manual_seed(3)
+        a = torch.randn(2048, 256, device=dev, generator=gen).to(torch.bfloat16)
+        b = torch.randn(256, 4096, device=dev, generator=gen).to(torch.bfloat16)
+        for _ in range(3):
+            c = WS.gemm_bf16(a, b)
+        ms = timed(lambda: WS.gemm_bf16(a, b, c), 20, dev)
+        err = (c - a.float() @ b.float()).abs().max().item()
+        print(f"gemm_bf16 2048x4096x256: {2 * 2048 * 4096 * 256 / (ms * 1e-3) / 1e12:.1f} "
+              f"TFLOP/s, max |err| vs torch fp32 = {err:.2e}")
+        return err
+    raise ValueError(name)
+
+
 def main():
     args = parse()
     world, rank, local = dist_init(args)
@@ -514,11 +804,19 @@ def main():
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if args.case:
+        val = profile_case(args.case, dev)
+        print(args.case, val)
+        sys.exit(0 if np.isfinite(val) else 1)
     if args.leg:
         if rank == 0:
-            leg = {"sil_2d": sil_2d, "psod_2d": psod_2d, "grid_sweep": grid_sweep}[args.leg]
-            print(json.dumps({"leg": args.leg, **leg(dev, steps=args.leg_steps, cpu_steps=0)}),
-                  flush=True)
+            legs = {"c1": lambda: leg_c1(dev), "c2": lambda: leg_c2(dev),
+                    "c3": lambda: leg_c3(dev), "mixed": lambda: leg_mixed(args, dev),
+                    "sil_2d": lambda: sil_2d(dev, steps=args.leg_steps, cpu_steps=0),
+                    "psod_2d": lambda: psod_2d(dev, steps=args.leg_steps, cpu_steps=0),
+                    "grid_sweep": lambda: grid_sweep(dev, steps=args.leg_steps),
+                    "eig": lambda: eig_warmstart(args, dev)}
+            print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         if world > 1:
             torch.distributed.destroy_process_group()
         return
@@ -561,24 +859,14 @@ def main():
     launches = len(set(int(x) for x in w["n"])) + 2
 
     # roofline of the propagation kernels (algorithmic bytes per launch group)
-    peak, peak_kind = measured_peaks()
-    ev2 = torch.cuda.Event(enable_timing=True)
-    ev3 = torch.cuda.Event(enable_timing=True)
-    ev2.record(stream)
-    for _ in range(args.steps):
-        b.run(w["nsteps"], stream=sh)
-    ev3.record(stream)
-    torch.cuda.synchronize()
-    kms = ev2.elapsed_time(ev3) / args.steps
-    alg = ALG_BYTES[args.precision] * pts_steps
-    achieved = alg / (kms * 1e-3) / 1e9
+    kms = timed(lambda: b.run(w["nsteps"], stream=sh), args.steps, dev)
     tb = MEASURED_TRAFFIC_B[args.precision]
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": (tb * pts_steps if tb else None),
-            "traffic_note": "ncu dram bytes of a 2048-point class launch scaled by grid-point steps",
-            "peak_kind": peak_kind,
-            "kernel": "spo1d_kernel (7 size classes, concurrent streams)",
-            "kernel_ms": kms}
+    roof = roofline(ALG_BYTES[args.precision], pts_steps, kms,
+                    traffic=(tb * pts_steps if tb else None))
+    roof.update({"traffic_note": "ncu dram bytes of a 2048-point class launch scaled by "
+                                 "grid-point steps",
+                 "kernel": "spo1d_kernel (7 size classes, concurrent streams)",
+                 "kernel_ms": kms})
 
     # end-to-end through the C-ABI with host buffers
     e2e = None
@@ -604,35 +892,33 @@ def main():
             if it > 0:
                 t_e.append(t1 - t0)
         e2e_rate, _, _ = job_rate(pts_steps, 1e3 * float(np.median(t_e)), world, dev)
-        h2d = 3 * 8 * npts
-        d2h = 2 * 8 * (nc + npts)
         e2e = {"value": e2e_rate, "unit": "Mgridpt*steps/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+               "h2d_bytes_per_step": int(3 * 8 * npts), "d2h_bytes_per_step": int(2 * 8 * (nc + npts)),
                "timing": "host wall clock around load + run + results_into with pinned host "
                          "buffers (median of 3 steps, max over ranks)"}
+    b.close()
 
     extra = {}
     if rank == 0 and not args.no_extra:
-        extra["fp64_form"] = fp64_form(args, w, ms, dev) if args.precision == "mixed" else None
-        extra["sil_2d"] = sil_2d(dev)
+        extra["mixed_form"] = leg_mixed(args, dev, ms_fp64=ms if args.precision == "fp64" else None)
+        extra["c1_morse1d"] = leg_c1(dev)
+        extra["c2_morse2d"] = leg_c2(dev)
+        extra["c3_anharmonic3d"] = leg_c3(dev)
         extra["psod_2d"] = psod_2d(dev)
-        extra.update(spo_nd(dev))
         extra["eigensolver"] = eig_warmstart(args, dev)
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "Mgridpt*steps/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32+f64" if args.precision == "mixed" else "f64", "data": "synthetic",
-                "config": {"workload": "morse_scan_1d", "npk": args.npk, "nsteps": args.nsteps,
-                           "precision": args.precision, "parallelism": f"packets x {world} GPU",
-                           "l2": "tables and C(t) output exceed L2 (126 MB)",
-                           "packets_per_s": args.npk * world / (ms * 1e-3)},
+                "config": scan_config(args),
+                "packets_per_s": args.npk * world / (ms * 1e-3),
+                "parallelism": f"packets x {world} GPU",
                 "roofline": roof,
                 "cpu_baseline": cpu_baseline(args) if (world == 1 and not args.no_cpu) else None,
                 "e2e": e2e, "gpu_launches": launches * args.steps, "clocks": clk.summary(),
                 **extra}
         print(json.dumps(line), flush=True)
-    b.close()
     if world > 1:
         torch.distributed.destroy_process_group()
 

@@ -1,8 +1,8 @@
 #!/usr/bin/env python3
 """Generate the golden fixtures that pin the CPU oracle to eSPec itself.
 
-Run in a container where the reference tree is mounted at /root/reference
-(the path can be overridden with ESPEC_REF).  The script only RUNS the shipped
+Run where the reference tree is available (its path in the ESPEC_REF
+environment variable, or the default below).  The script only RUNS the shipped
 eSPec executable (espec_v07.x) as a black box on input decks, and reads the
 reference's own test fixtures (ttests/) as text; it never inspects the
 executable.  Outputs go to tests/golden/*.npz plus manifest.json.
