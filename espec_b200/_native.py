@@ -23,6 +23,7 @@ Q_PSOD_COPY = 32
 PULSE_NONE, PULSE_GAUS, PULSE_GGAUS, PULSE_SIN2 = 0, 1, 2, 3
 SPO, SOD, SIL, PSOD = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
+LAUNCH_CLASSES, LAUNCH_PERSISTENT = 0, 1
 SHFS = 2.4188843243e-2
 
 # every symbol the header declares (checked by the CPU test suite)
@@ -30,7 +31,8 @@ EXPORTS = [
     "espec_last_error", "espec_version", "espec_device_ok", "espec_spo_create", "espec_spo_load",
     "espec_spo_run", "espec_spo_results", "espec_spo_device_c", "espec_spo_npoints",
     "espec_spo_destroy", "espec_spo_set_variant", "espec_spo_variant_count",
-    "espec_spo_run_static", "espec_prop_create", "espec_prop_previous", "espec_prop_continue",
+    "espec_spo_run_static", "espec_spo_set_launch", "espec_spo_set_item_cost", "espec_prop_nonfinite",
+    "espec_prop_create", "espec_prop_previous", "espec_prop_continue",
     "espec_prop_energies", "espec_format_crl_row", "pspofft_", "psodfft_", "espec_grid_create",
     "espec_grid_load", "espec_grid_run", "espec_grid_continue", "espec_grid_results",
     "espec_grid_energies", "espec_grid_npoints", "espec_grid_destroy", "espec_grid_basis",
@@ -44,6 +46,8 @@ EXPORTS = [
     "espec_convert", "espec_spond_create", "espec_spond_load", "espec_spond_run",
     "espec_spond_results", "espec_spond_destroy", "espec_spond_continue", "espec_spond_energies",
     "espec_spond_create_method", "espec_spond_previous",
+    "espec_set_wait_limit", "espec_selftest_short_arrivals", "espec_selftest_mbar_wait",
+    "espec_pot_kind", "espec_gvpot_1d", "espec_gvpot_nd",
 ]
 
 
@@ -79,6 +83,15 @@ def load():
     lib.espec_spo_device_c.restype = vp
     lib.espec_spo_npoints.argtypes = [vp]
     lib.espec_spo_set_variant.argtypes = [vp, C.c_int, C.c_int]
+    lib.espec_spo_set_launch.argtypes = [vp, C.c_int]
+    lib.espec_prop_nonfinite.argtypes = [vp, C.POINTER(C.c_int), vp]
+    lib.espec_set_wait_limit.argtypes = [C.c_long]
+    lib.espec_pot_kind.argtypes = [C.c_char_p, C.c_size_t, C.c_int]
+    lib.espec_gvpot_1d.argtypes = [C.c_int, vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp]
+    lib.espec_gvpot_nd.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, vp]
+    lib.espec_selftest_short_arrivals.argtypes = [C.c_int]
+    lib.espec_selftest_mbar_wait.argtypes = [C.c_long, C.POINTER(C.c_int)]
+    lib.espec_spo_set_item_cost.argtypes = [vp, C.c_int, C.c_double]
     lib.espec_spo_variant_count.restype = C.c_int
     lib.espec_spo_run_static.argtypes = [C.c_int, i, d, d, C.c_double, C.c_int, vp, vp, C.c_int,
                                          vp, vp, vp]

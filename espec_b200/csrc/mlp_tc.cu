@@ -128,9 +128,10 @@ __device__ __forceinline__ void stage_tile(uint8_t* dst, const uint16_t* X, int 
 }
 
 // bounded wait for the completion of the mbarrier phase with this parity
-__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity) {
+__device__ __forceinline__ bool wait_phase(uint64_t* bar, uint32_t parity,
+                                           long limit = kWaitLimit) {
   const uint32_t a = smem_u32(bar);
-  for (long i = 0; i < kWaitLimit; ++i) {
+  for (long i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -365,6 +366,38 @@ extern "C" int espec_gemm_bf16(int M, int N, int K, float alpha, const void* A, 
   const long tiles256 = (long)((N + 255) / 256) * ((M + kBM - 1) / kBM);
   return (N > 128 && tiles256 >= 148) ? launch_tc<256>(g, (cudaStream_t)stream)
                                       : launch_tc<128>(g, (cudaStream_t)stream);
+}
+
+namespace espec {
+namespace {
+// One thread waits, with the GEMM's bounded wait, on an mbarrier that nothing
+// arrives on and no copy or MMA is attached to: the wait must give up after
+// `polls` polls and set the status word.  The barrier is invalidated before
+// the CTA exits.
+__global__ void mbar_timeout_probe(long polls, int* gave_up) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bar)));
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    const bool ok = wait_phase(&bar, 0u, polls);
+    *gave_up = ok ? 0 : 1;
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];\n" ::"r"(smem_u32(&bar)) : "memory");
+  }
+}
+}  // namespace
+}  // namespace espec
+
+extern "C" int espec_selftest_mbar_wait(long polls, int* gave_up) {
+  if (polls < 1 || !gave_up) return set_error(ESPEC_EINVAL, "polls must be positive");
+  int* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(int));
+  if (e != cudaSuccess) return set_cuda_error("cudaMalloc", e);
+  mbar_timeout_probe<<<1, 32>>>(polls, d);
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpy(gave_up, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return set_cuda_error("mbarrier wait self-test", e);
+  return ESPEC_OK;
 }
 
 extern "C" int espec_gemm_bf16_status(int* timed_out) {

@@ -6,6 +6,7 @@
 #include <cuda/atomic>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <utility>
 #include <vector>
@@ -72,7 +73,7 @@ __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int 
     if (arrived < target) {
       long spins = 0;
       while (cnt.load(cuda::memory_order_acquire) < target) {
-        if (++spins > kSpinLimit || err.load(cuda::memory_order_relaxed) != 0) {
+        if (++spins > a.spin_limit || err.load(cuda::memory_order_relaxed) != 0) {
           err.store(1, cuda::memory_order_relaxed);
           s_flag[1] = 0;
           break;
@@ -823,6 +824,14 @@ static void grid_free(espec_grid_plan* p) {
     if (e_ != cudaSuccess) return set_cuda_error(#call, e_); \
   } while (0)
 
+// Bounded waits of the grid barriers: the poll limit of the next launches
+// (espec_set_wait_limit), and the number of next launches whose arrival count
+// starts one short (espec_selftest_short_arrivals): their first barrier can
+// never complete, so every CTA's wait runs out, sets the error flag and the
+// kernel returns -- the time-out path exercised without any fault.
+static std::atomic<long> g_wait_limit{kSpinLimit};
+static std::atomic<int> g_short_arrivals{0};
+
 static SilArgs sil_args(const espec_grid_plan* p) {
   SilArgs a{};
   a.ndim = p->ndim;
@@ -849,6 +858,7 @@ static SilArgs sil_args(const espec_grid_plan* p) {
   a.part = p->d_part;
   a.bar = p->d_bar;
   a.err = p->d_err;
+  a.spin_limit = g_wait_limit.load();
   a.c_out = p->d_c;
   a.m = p->m;
   a.quirk = (p->quirks & ESPEC_Q_SIL_INPLACE) != 0;
@@ -993,7 +1003,10 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
     GRID_CK(cudaMemcpyAsync(p->d_u, p->d_u0, nb, cudaMemcpyDeviceToDevice, st));
     GRID_CK(cudaMemcpyAsync(p->d_v, p->d_v0, nb, cudaMemcpyDeviceToDevice, st));
   }
-  GRID_CK(cudaMemsetAsync(p->d_bar, 0, sizeof(unsigned) * 2, st));
+  // the 64-bit arrival count starts at 0, or at 2^64 - 1 (one short of the
+  // first barrier's G arrivals, modulo 2^64) for a self-test launch
+  const bool short_start = g_short_arrivals.load() > 0 && g_short_arrivals.fetch_sub(1) > 0;
+  GRID_CK(cudaMemsetAsync(p->d_bar, short_start ? 0xFF : 0, sizeof(unsigned) * 2, st));
   GRID_CK(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
   SilArgs a = sil_args(p);
   a.nsteps = nsteps;
@@ -1147,6 +1160,18 @@ extern "C" int espec_grid_project(espec_grid_plan* p, const double* w, int nvec,
   GRID_CK(cudaMemcpyAsync(out, p->d_ppart + nsum, sizeof(double) * 2 * nvec,
                           cudaMemcpyDeviceToHost, st));
   GRID_CK(cudaStreamSynchronize(st));
+  return ESPEC_OK;
+}
+
+extern "C" int espec_set_wait_limit(long polls) {
+  if (polls < 0) return set_error(ESPEC_EINVAL, "negative poll limit");
+  g_wait_limit.store(polls == 0 ? kSpinLimit : polls);
+  return ESPEC_OK;
+}
+
+extern "C" int espec_selftest_short_arrivals(int launches) {
+  if (launches < 0) return set_error(ESPEC_EINVAL, "negative launch count");
+  g_short_arrivals.store(launches);
   return ESPEC_OK;
 }
 

@@ -49,6 +49,7 @@ struct SilArgs {
   double* part;  // [2][gridDim.x][kSilNQ]: partial sums, by barrier parity
   unsigned* bar;  // [0..1]: one 64-bit count of the grid barrier arrivals of the launch
   int* err;       // set when a barrier wait gave up
+  long spin_limit;  // polls before a barrier wait gives up
   double2* c_out;  // C(t) of every step: slot s for step s (slot 0 only if write_c0)
   int m, nsteps, quirk, write_c0;
   double cst;  // dt in atomic units (SIL); 2 dt in atomic units (PSOD)

@@ -17,6 +17,7 @@
 #include "diag1d.cuh"
 #include "sod1d.cuh"
 #include "spo1d_launch.cuh"
+#include "spo1d_persist.cuh"
 
 namespace espec {
 
@@ -291,6 +292,18 @@ struct espec_spo_plan {
   };
   bool index_dirty = true;
   std::vector<Class> classes;
+  // persistent launch: items of packets (one size class each), claimed by
+  // the CTAs of one kernel in decreasing cost
+  int launch = ESPEC_LAUNCH_CLASSES;
+  bool persist_ok = false;           // every packet size has a persistent class
+  std::vector<SpoItem> items;        // in claim order
+  std::vector<int> slot_pk;          // packet index of each slot of the item list
+  std::map<int, double> item_cost;   // per packet size: cost of one item
+  SpoItem* d_items = nullptr;
+  SpoPacket* d_pk_items = nullptr;   // packet descriptors in slot order
+  unsigned int* d_next = nullptr;    // claim counter
+  bool items_dirty = true;
+  int items_steps = -1;              // nsteps the item descriptors' C(t) offsets are for
   std::vector<cudaStream_t> streams;
   std::vector<cudaEvent_t> events;
   cudaEvent_t ev_fork = nullptr;
@@ -313,6 +326,7 @@ struct espec_spo_plan {
   bool loaded = false;
   bool has_prev = false;      // SOD: d_psi_prev holds psi(t - dt) of the current state
   double2* d_diag = nullptr;  // (E, norm) per packet
+  int* d_nonfinite = nullptr; // packets whose C(t) went non-finite in the last run
   HostStage stage;            // host transfers: (re | im) blocks, contiguous
   // tables (sub-pointers of d_tab)
   SpoTables<double> t64{};
@@ -328,9 +342,10 @@ static void plan_free(espec_spo_plan* p) {
   for (auto s : p->streams) cudaStreamDestroy(s);
   for (auto e : p->events) cudaEventDestroy(e);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
-  void* bufs[] = {p->d_vpot, p->d_vabc, p->d_psi0, p->d_psi, p->d_tc, p->d_kperm, p->d_pk_of,
-                  p->d_pk_off, p->d_kscale, p->d_tab, p->d_c, p->d_kq_c, p->d_kq_s, p->d_psi_prev,
-                  p->d_diag};
+  void* bufs[] = {p->d_vpot, p->d_vabc, p->d_psi0, p->d_psi,  p->d_tc,       p->d_kperm,
+                  p->d_pk_of, p->d_pk_off, p->d_kscale, p->d_tab, p->d_c,  p->d_kq_c,
+                  p->d_kq_s, p->d_psi_prev, p->d_diag, p->d_items, p->d_pk_items, p->d_next,
+                  p->d_nonfinite};
   for (void* b : bufs)
     if (b) cudaFree(b);
   p->stage.release();
@@ -351,7 +366,9 @@ static int spo_index_tables(espec_spo_plan* p) {
   std::vector<double> tc(np), kscale(npk);
   std::vector<int> kperm(np), pk_of(np);
   std::map<int, int> var_of;
-  for (auto& c : p->classes) var_of[c.n] = c.variant;
+  const bool persist = p->launch == ESPEC_LAUNCH_PERSISTENT;
+  for (auto& c : p->classes)
+    var_of[c.n] = persist ? persist_variant(c.n, p->precision == ESPEC_FP64) : c.variant;
   std::map<int, std::pair<std::vector<int>, int>> kap_cache;
   for (int i = 0; i < npk; ++i) {
     const int n = p->n[i];
@@ -484,6 +501,8 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
   if ((rc = ck(cudaMalloc(&p->d_pk_off, npk * 4), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_kscale, npk * 8), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_diag, npk * 16), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMalloc(&p->d_nonfinite, sizeof(int)), "cudaMalloc"))) return fail(rc);
+  if ((rc = ck(cudaMemset(p->d_nonfinite, 0, sizeof(int)), "cudaMemset"))) return fail(rc);
   if (precision == ESPEC_FP64) {
     p->tab_bytes = np * 16 * 5;
   } else {
@@ -518,6 +537,16 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
     p->t32.k = c + 3 * np;
     p->t32.w = (cpx<float>*)(c + 4 * np);  // 12-byte phases: w stays 4-byte aligned
   }
+  // the persistent launch covers the SPO method without the in-place defect
+  // when every packet size has a class in the persistent kernel
+  p->persist_ok = method == ESPEC_SPO && !(quirks & ESPEC_Q_SPO_INPLACE);
+  for (int i = 0; i < npk && p->persist_ok; ++i) p->persist_ok = persist_class(p->n[i]) >= 0;
+  if (p->persist_ok) {
+    p->launch = ESPEC_LAUNCH_PERSISTENT;
+    if ((rc = ck(cudaMalloc(&p->d_pk_items, sizeof(SpoPacket) * npk), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_items, sizeof(SpoItem) * npk), "cudaMalloc"))) return fail(rc);
+    if ((rc = ck(cudaMalloc(&p->d_next, sizeof(unsigned int)), "cudaMalloc"))) return fail(rc);
+  }
   if ((rc = spo_index_tables(p))) return fail(rc);
   *out = p;
   return ESPEC_OK;
@@ -542,8 +571,31 @@ extern "C" int espec_spo_set_variant(espec_spo_plan* p, int npts, int variant) {
       found = true;
     }
   if (!found) return set_error(ESPEC_EINVAL, "no packet of that size in the plan");
+  p->launch = ESPEC_LAUNCH_CLASSES;  // the persistent kernel has fixed variants
   p->index_dirty = true;
   p->loaded = false;  // tables depend on the plan's final layout
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spo_set_launch(espec_spo_plan* p, int mode) {
+  if (!p) return set_error(ESPEC_EINVAL, "null plan");
+  if (mode != ESPEC_LAUNCH_CLASSES && mode != ESPEC_LAUNCH_PERSISTENT)
+    return set_error(ESPEC_EINVAL, "unknown launch shape");
+  if (mode == ESPEC_LAUNCH_PERSISTENT && !p->persist_ok)
+    return set_error(ESPEC_EINVAL, "the persistent launch needs a split-operator plan without "
+                                   "the in-place defect and packet sizes 256..2048");
+  if (mode != p->launch) {
+    p->launch = mode;
+    p->index_dirty = true;
+    p->loaded = false;  // the final layouts of the two shapes may differ
+  }
+  return ESPEC_OK;
+}
+
+extern "C" int espec_spo_set_item_cost(espec_spo_plan* p, int npts, double cost) {
+  if (!p || !(cost > 0.0)) return set_error(ESPEC_EINVAL, "null plan or non-positive cost");
+  p->item_cost[npts] = cost;
+  p->items_dirty = true;
   return ESPEC_OK;
 }
 
@@ -619,6 +671,93 @@ extern "C" int espec_spo_load(espec_spo_plan* p, const double* vpot, const doubl
   return spo_build_tables(p, st);
 }
 
+// Items of the persistent launch: the packets of each size in groups of
+// persist_group(n) (one CTA's worth), ordered by decreasing cost of an item
+// (longest processing time first; default cost = points of an item x log2 n),
+// and their packet descriptors in slot order with the C(t) offsets of a run
+// of nsteps steps.
+static int persist_items(espec_spo_plan* p, int nsteps) {
+  const bool d = p->precision == ESPEC_FP64;
+  struct Raw {
+    SpoItem it;
+    double cost;
+    std::vector<int> pk;
+  };
+  std::vector<Raw> raw;
+  std::map<int, std::vector<int>> by_size;
+  for (int i = 0; i < p->npk; ++i) by_size[p->n[i]].push_back(i);
+  for (auto& kv : by_size) {
+    const int n = kv.first, g = persist_group(n, d), cls = persist_class(n);
+    if (g < 1 || cls < 0) return set_error(ESPEC_EINVAL, "packet size without a persistent class");
+    auto c = p->item_cost.find(n);
+    const double cost = c != p->item_cost.end() ? c->second : (double)g * n * std::log2((double)n);
+    for (size_t k = 0; k < kv.second.size(); k += g) {
+      Raw r;
+      r.it.cls = cls;
+      r.it.count = (int)std::min<size_t>(g, kv.second.size() - k);
+      r.it.first = 0;
+      r.cost = cost;
+      r.pk.assign(kv.second.begin() + k, kv.second.begin() + k + r.it.count);
+      raw.push_back(std::move(r));
+    }
+  }
+  std::stable_sort(raw.begin(), raw.end(), [](const Raw& a, const Raw& b) { return a.cost > b.cost; });
+  p->items.clear();
+  p->slot_pk.clear();
+  std::vector<SpoPacket> pk;
+  for (auto& r : raw) {
+    r.it.first = (int)p->slot_pk.size();
+    p->items.push_back(r.it);
+    for (int i : r.pk) {
+      p->slot_pk.push_back(i);
+      pk.push_back(SpoPacket{p->off[i], (long long)i * (nsteps + 1)});
+    }
+  }
+  ESPEC_CK(cudaMemcpy(p->d_items, p->items.data(), sizeof(SpoItem) * p->items.size(),
+                      cudaMemcpyHostToDevice));
+  ESPEC_CK(cudaMemcpy(p->d_pk_items, pk.data(), sizeof(SpoPacket) * pk.size(),
+                      cudaMemcpyHostToDevice));
+  p->items_dirty = false;
+  return ESPEC_OK;
+}
+
+// the whole batch in one persistent launch
+static int persist_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t st) {
+  ESPEC_CK(cudaMemsetAsync(p->d_next, 0, sizeof(unsigned int), st));
+  cudaError_t e;
+  if (p->precision == ESPEC_FP64) {
+    SpoPersistArgs<double> pa{};
+    pa.a.tab = p->t64;
+    pa.a.pk = p->d_pk_items;
+    pa.a.psi0 = p->d_psi0;
+    if (resume) pa.a.psi_start = p->d_psi;
+    pa.a.psi_out = p->d_psi;
+    pa.a.c_out = p->d_c;
+    pa.a.nsteps = nsteps;
+    pa.a.nonfinite = p->d_nonfinite;
+    pa.items = p->d_items;
+    pa.nitems = (int)p->items.size();
+    pa.next = p->d_next;
+    e = spo_persist_launch_f64(pa, st);
+  } else {
+    SpoPersistArgs<float> pa{};
+    pa.a.tab = p->t32;
+    pa.a.pk = p->d_pk_items;
+    pa.a.psi0 = p->d_psi0;
+    if (resume) pa.a.psi_start = p->d_psi;
+    pa.a.psi_out = p->d_psi;
+    pa.a.c_out = p->d_c;
+    pa.a.nsteps = nsteps;
+    pa.a.nonfinite = p->d_nonfinite;
+    pa.items = p->d_items;
+    pa.nitems = (int)p->items.size();
+    pa.next = p->d_next;
+    e = spo_persist_launch_f32(pa, st);
+  }
+  if (e != cudaSuccess) return set_cuda_error("spo1d_persistent launch", e);
+  return ESPEC_OK;
+}
+
 // one launch per size class over nsteps steps, from psi0 (resume = false) or
 // from the plan's current state (resume = true)
 static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t st) {
@@ -637,6 +776,15 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
     }
   }
   const bool quirk = (p->quirks & ESPEC_Q_SPO_INPLACE) != 0;
+  ESPEC_CK(cudaMemsetAsync(p->d_nonfinite, 0, sizeof(int), st));
+  if (p->method == ESPEC_SPO && p->launch == ESPEC_LAUNCH_PERSISTENT) {
+    if (p->items_dirty || p->items_steps != nsteps) {
+      int rc = persist_items(p, nsteps);
+      if (rc) return rc;
+      p->items_steps = nsteps;
+    }
+    return persist_launch(p, nsteps, resume, st);
+  }
   ESPEC_CK(cudaEventRecord(p->ev_fork, st));
   for (size_t ci = 0; ci < p->classes.size(); ++ci) {
     auto& c = p->classes[ci];
@@ -671,6 +819,7 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
       a.kq_s = p->d_kq_s;
       a.kq_scale = 1.0 / c.n;
       a.nsteps = nsteps;
+      a.nonfinite = p->d_nonfinite;
       e = launch_n<double>(c.n, c.variant, a, c.count, quirk, cs);
     } else {
       SpoArgs<float> a{};
@@ -681,6 +830,7 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
       a.psi_out = p->d_psi;
       a.c_out = p->d_c;
       a.nsteps = nsteps;
+      a.nonfinite = p->d_nonfinite;
       e = launch_n<float>(c.n, c.variant, a, c.count, false, cs);
     }
     if (e != cudaSuccess) return set_cuda_error("spo1d_kernel launch", e);
@@ -737,6 +887,14 @@ extern "C" int espec_spo_results(espec_spo_plan* p, double* c_re, double* c_im, 
 }
 
 extern "C" const void* espec_spo_device_c(const espec_spo_plan* p) { return p ? p->d_c : nullptr; }
+
+extern "C" int espec_prop_nonfinite(espec_spo_plan* p, int* count, void* stream) {
+  if (!p || !count) return set_error(ESPEC_EINVAL, "null argument");
+  cudaStream_t st = (cudaStream_t)stream;
+  ESPEC_CK(cudaMemcpyAsync(count, p->d_nonfinite, sizeof(int), cudaMemcpyDeviceToHost, st));
+  ESPEC_CK(cudaStreamSynchronize(st));
+  return ESPEC_OK;
+}
 
 extern "C" int espec_prop_previous(espec_spo_plan* p, double* psi_re, double* psi_im, int where,
                                    void* stream) {

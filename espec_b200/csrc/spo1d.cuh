@@ -164,15 +164,42 @@ struct SpoArgs {
   const double* kq_s;       //                    sin(CST1*TC)
   double kq_scale;          //                    1/N
   int nsteps;
+  int* nonfinite;           // count of packets with a non-finite C(t) sample (or null)
 };
 
+// Sum of the NW per-warp partials of one C(t) sample, compensated
+// (Neumaier: the rounding error of every addition is carried along and added
+// back at the end), in warp order on one thread.
+template <int NW>
+__device__ __forceinline__ double2 sum_partials(const double2* cp) {
+  double sr = 0.0, si = 0.0, er = 0.0, ei = 0.0;
+#pragma unroll
+  for (int i = 0; i < NW; ++i) {
+    const double xr = cp[i].x, xi = cp[i].y;
+    const double tr = sr + xr, ti = si + xi;
+    er += fabs(sr) >= fabs(xr) ? (sr - tr) + xr : (xr - tr) + sr;
+    ei += fabs(si) >= fabs(xi) ? (si - ti) + xi : (xi - ti) + si;
+    sr = tr;
+    si = ti;
+  }
+  return make_double2(sr + er, si + ei);
+}
+
+// Barrier of the T threads that propagate one packet.  A CTA may hold
+// several such groups (the persistent kernel packs small packets): group g
+// uses hardware barrier id g + 1 with T threads, a group that is the whole
+// CTA uses id 0 (then bar.sync 0, T is __syncthreads).
 template <int T>
-__device__ __forceinline__ void group_sync() {
+__device__ __forceinline__ void group_bar(int id) {
   if constexpr (T <= 32) {
     __syncwarp();
   } else {
-    __syncthreads();
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(T) : "memory");
   }
+}
+template <int T>
+__device__ __forceinline__ void group_sync() {
+  group_bar<T>(0);
 }
 
 template <typename R, class PL>
@@ -197,6 +224,7 @@ struct SpoThread {
   }
 
   rot_t tw[PL::NTW];
+  int bar = 0;  // hardware barrier id of this thread's packet group (group_bar)
 
   // shared-memory swizzle: flips the low 4 bits of an element index with
   // bits 3..7, a bijection inside every 16-element block that makes all the
@@ -307,17 +335,17 @@ struct SpoThread {
   }
 
   template <int s>
-  static __device__ __forceinline__ void xsync() {
+  __device__ __forceinline__ void xsync() const {
     if constexpr (local_x<s>()) {
       __syncwarp();
     } else {
-      __syncthreads();
+      group_bar<T>(bar);
     }
   }
 
   // exchange after forward stage s (s < S-1): outputs of s -> inputs of s+1
   template <int s>
-  static __device__ __forceinline__ void xchg_fwd(cpx<R>* v, cpx<R>* buf, int t) {
+  __device__ __forceinline__ void xchg_fwd(cpx<R>* v, cpx<R>* buf, int t) const {
     constexpr int R0 = PL::r[s], Q0 = P / R0;
     constexpr int R1 = PL::r[s + 1], Q1 = P / R1;
 #pragma unroll
@@ -332,7 +360,7 @@ struct SpoThread {
   }
   // reverse exchange: inputs of s+1 -> outputs of s
   template <int s>
-  static __device__ __forceinline__ void xchg_inv(cpx<R>* v, cpx<R>* buf, int t) {
+  __device__ __forceinline__ void xchg_inv(cpx<R>* v, cpx<R>* buf, int t) const {
     constexpr int R0 = PL::r[s], Q0 = P / R0;
     constexpr int R1 = PL::r[s + 1], Q1 = P / R1;
 #pragma unroll
@@ -448,26 +476,29 @@ struct TabStore<R, PL, 1> {
 // ---------------------------------------------------------------------------
 // the kernel: one CTA per packet of size N
 // ---------------------------------------------------------------------------
-template <typename R, class PL, bool kCap, bool kQuirk, int kTab, int kMinBlocks>
-__global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) {
+// The whole time loop of one packet, run by the T = PL::T threads of one
+// group (t = 0..T-1 inside the group, bar = the group's barrier id, smem =
+// the group's spo1d_smem_bytes<R, PL, kTab>() bytes of shared memory).
+template <typename R, class PL, bool kQuirk, int kTab>
+__device__ __forceinline__ void spo_packet(const SpoArgs<R>& a, const SpoPacket pk, const int t,
+                                           unsigned char* smem, const int bar) {
   constexpr int N = PL::N, P = PL::P, T = PL::T;
   constexpr int NW = (T + 31) / 32;
   using Th = SpoThread<R, PL>;
   using TB = Tab<R>;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  cpx<R>* bufs = reinterpret_cast<cpx<R>*>(smem_raw);
+  cpx<R>* bufs = reinterpret_cast<cpx<R>*>(smem);
   double2* cpart = reinterpret_cast<double2*>(bufs + Th::NBUF * N);  // [2][NW]
   TabStore<R, PL, kTab> tab;
   tab.init(cpart + 2 * NW);
 
-  const int t = threadIdx.x;
   const int lane = t & 31, warp = t >> 5;
-  const SpoPacket pk = a.pk[blockIdx.x];
   const int base = pk.off;
   double2* cout = a.c_out + pk.c_off;
 
   Th th;
+  th.bar = bar;
   th.init_twiddles(t);
+  bool finite = true;  // C(t) samples written by this thread stayed finite
 
   cpx<R> v[P];
   double c0r = 0.0;
@@ -488,13 +519,13 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) cr += __shfl_xor_sync(0xffffffffu, cr, o);
     if (lane == 0) cpart[warp] = make_double2(cr, 0.0);
-    group_sync<T>();
+    group_bar<T>(bar);
     if (t == 0) {
       double sr = 0.0;
       for (int i = 0; i < NW; ++i) sr += cpart[i].x;
       cout[0] = make_double2(sr, 0.0);
     }
-    group_sync<T>();
+    group_bar<T>(bar);
   }
 
   for (int step = 1; step <= a.nsteps; ++step) {
@@ -510,13 +541,9 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
     // sum of the previous step's partial C(t): all partials are visible after
     // the first exchange barrier of this step
     if (T > 32 && t == 0 && step > 1) {
-      double sr = 0.0, si = 0.0;
-      const double2* cp = cpart + ((step - 1) & 1) * NW;
-      for (int i = 0; i < NW; ++i) {
-        sr += cp[i].x;
-        si += cp[i].y;
-      }
-      cout[step - 1] = make_double2(sr, si);
+      const double2 c = sum_partials<NW>(cpart + ((step - 1) & 1) * NW);
+      finite = finite && isfinite(c.x) && isfinite(c.y);
+      cout[step - 1] = c;
     }
     // kinetic phase
     if constexpr (kQuirk) {
@@ -555,23 +582,24 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
       ci += __shfl_xor_sync(0xffffffffu, ci, o);
     }
     if constexpr (T <= 32) {
-      if (lane == 0) cout[step] = make_double2(cr, ci);
+      if (lane == 0) {
+        finite = finite && isfinite(cr) && isfinite(ci);
+        cout[step] = make_double2(cr, ci);
+      }
     } else {
       if (lane == 0) cpart[(step & 1) * NW + warp] = make_double2(cr, ci);
     }
   }
   if constexpr (T > 32) {
-    group_sync<T>();
+    group_bar<T>(bar);
     if (t == 0 && a.nsteps > 0) {
-      double sr = 0.0, si = 0.0;
-      const double2* cp = cpart + (a.nsteps & 1) * NW;
-      for (int i = 0; i < NW; ++i) {
-        sr += cp[i].x;
-        si += cp[i].y;
-      }
-      cout[a.nsteps] = make_double2(sr, si);
+      const double2 c = sum_partials<NW>(cpart + (a.nsteps & 1) * NW);
+      finite = finite && isfinite(c.x) && isfinite(c.y);
+      cout[a.nsteps] = c;
     }
   }
+  // one count per packet whose C(t) went non-finite during the run
+  if (!finite && a.nonfinite) atomicAdd(a.nonfinite, 1);
   // psi(TF) = hm . phi
   if (a.psi_out) {
 #pragma unroll
@@ -581,6 +609,13 @@ __global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) 
       a.psi_out[x] = make_double2((double)o.x, (double)o.y);
     }
   }
+}
+
+// one CTA of PL::T threads per packet of one size class
+template <typename R, class PL, bool kCap, bool kQuirk, int kTab, int kMinBlocks>
+__global__ void __launch_bounds__(PL::T, kMinBlocks) spo1d_kernel(SpoArgs<R> a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  spo_packet<R, PL, kQuirk, kTab>(a, a.pk[blockIdx.x], threadIdx.x, smem_raw, 0);
 }
 
 template <typename R, class PL, int kTab>

@@ -36,8 +36,20 @@ class SpoBatch:
         N.check(rc, "espec_prop_create")
         self.nsteps = None
 
+    def set_launch(self, mode):
+        """"persistent" (one kernel over all packet sizes, items claimed
+        longest first) or "classes" (one kernel per size class); before load."""
+        m = {"classes": N.LAUNCH_CLASSES, "persistent": N.LAUNCH_PERSISTENT}[mode]
+        N.check(N.load().espec_spo_set_launch(self._h, m), "espec_spo_set_launch")
+
+    def set_item_cost(self, npts, cost):
+        """Relative cost of one persistent item of packets of size npts."""
+        N.check(N.load().espec_spo_set_item_cost(self._h, int(npts), float(cost)),
+                "espec_spo_set_item_cost")
+
     def set_variant(self, npts, variant):
-        """Choose the kernel variant of one packet size (before load)."""
+        """Choose the kernel variant of one packet size (before load); selects
+        the per-class launch."""
         N.check(N.load().espec_spo_set_variant(self._h, int(npts), int(variant)),
                 "espec_spo_set_variant")
 
@@ -103,6 +115,12 @@ class SpoBatch:
         N.check(N.load().espec_spo_results(self._h, N.ptr(c_re), N.ptr(c_im), N.ptr(psi_re),
                                            N.ptr(psi_im), N.MEM_HOST, stream),
                 "espec_spo_results")
+
+    def nonfinite(self, stream=None):
+        """Packets whose C(t) went NaN/Inf during the last run or segment."""
+        n = C.c_int(0)
+        N.check(N.load().espec_prop_nonfinite(self._h, C.byref(n), stream), "espec_prop_nonfinite")
+        return n.value
 
     def device_c(self):
         """Device address of C(t) (double2, packet-major)."""

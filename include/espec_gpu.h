@@ -52,10 +52,41 @@ extern "C" {
 #define ESPEC_Q_FFTNT_SP 8      /* cfft.f:35 TWOPI from a single-precision literal */
 #define ESPEC_Q_DIGT_ND 16      /* dkeft.f:80-137 2D/3D kinetic table as written   */
 #define ESPEC_Q_PSOD_COPY 32    /* psod.f:136-141 restart copy sets V1(I+1) = V0(I) */
+#define ESPEC_Q_GVPOT_3D 64     /* gvpot.f:96 3D grid takes RX from the z index    */
+
+/* analytic potential forms (potfuncs.f; espec_pot_kind maps the deck's name) */
+#define ESPEC_POT_OHS 1          /* 1D/2D/3D harmonic                             */
+#define ESPEC_POT_DOHS 2         /* 1D                                            */
+#define ESPEC_POT_MORSEM 3       /* 1D                                            */
+#define ESPEC_POT_ANTI_MORSEM 4  /* 1D                                            */
+#define ESPEC_POT_MOD_MORSE 5    /* 1D                                            */
+#define ESPEC_POT_MORSE 6        /* 1D/2D                                         */
+#define ESPEC_POT_ANTI_MORSE 7   /* 1D                                            */
+#define ESPEC_POT_DMORSE 8       /* 1D                                            */
+#define ESPEC_POT_STEP 9         /* 1D/3D                                         */
+#define ESPEC_POT_BARRIER 10     /* 1D/2D/3D                                      */
+#define ESPEC_POT_CONST 11       /* .CONST / .FREE                                */
+#define ESPEC_POT_LSM 12         /* 2D                                            */
+#define ESPEC_POT_LS 13
+#define ESPEC_POT_LBH_CC 14
+#define ESPEC_POT_LBH 15
+#define ESPEC_POT_LEPS_CC 16
+#define ESPEC_POT_LEPS 17        /* 2D/3D                                         */
+#define ESPEC_POT_WELLXY 18
+#define ESPEC_POT_WELLX 19
+#define ESPEC_POT_WELLY 20
+#define ESPEC_POT_WELL 21
+#define ESPEC_POT_BARRIERXY 22
+#define ESPEC_POT_BARRIERX 23
+#define ESPEC_POT_BARRIERY 24
 
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
 #define ESPEC_MEM_DEVICE 1
+
+/* launch shape of a batched split-operator run (espec_spo_set_launch) */
+#define ESPEC_LAUNCH_CLASSES 0     /* one kernel per packet size, concurrent streams */
+#define ESPEC_LAUNCH_PERSISTENT 1  /* one persistent kernel over every packet size   */
 
 #define ESPEC_SHFS 2.4188843243e-2  /* fs per atomic unit of time (pspofft.f:76) */
 
@@ -243,6 +274,24 @@ int espec_prop_energies(espec_spo_plan* plan, double* e, double* norm, void* str
  * before espec_spo_load.  Defaults come from autotuning on B200. */
 int espec_spo_set_variant(espec_spo_plan* plan, int npts, int variant);
 int espec_spo_variant_count(void);
+/* Launch shape of espec_spo_run / espec_prop_continue.  ESPEC_LAUNCH_PERSISTENT
+ * (the default when every packet size is 256..2048 and the plan is an FP64 or
+ * mixed split operator without the in-place defect): one kernel whose CTAs
+ * claim items -- groups of packets of one size filling a CTA -- from a device
+ * counter, longest items first.  ESPEC_LAUNCH_CLASSES: one kernel per size
+ * class on concurrent streams, each with the variant espec_spo_set_variant
+ * chose (setting a variant selects this shape).  Call before espec_spo_load;
+ * no counterpart in the reference (its scans run one process per packet). */
+int espec_spo_set_launch(espec_spo_plan* plan, int mode);
+/* Relative cost of one persistent item of packets of size npts (the claim
+ * order is by decreasing cost; default: points of an item x log2 npts). */
+int espec_spo_set_item_cost(espec_spo_plan* plan, int npts, double cost);
+/* Number of packets whose C(t) became NaN or infinite during the last run or
+ * continued segment of a split-operator plan (checked on the device at every
+ * C(t) sample, counted once per packet; synchronises with the stream).  The
+ * drop-ins keep the reference's INFO (a NaN fails none of its drift tests);
+ * a batched caller reads this count after each segment. */
+int espec_prop_nonfinite(espec_spo_plan* plan, int* count, void* stream);
 /* device pointer of the C(t) buffer (double2, packet-major) */
 const void* espec_spo_device_c(const espec_spo_plan* plan);
 int espec_spo_npoints(const espec_spo_plan* plan);
@@ -343,6 +392,40 @@ int espec_grid_previous(espec_grid_plan* plan, double* psi_re, double* psi_im, i
                         void* stream);
 long espec_grid_npoints(const espec_grid_plan* plan);
 void espec_grid_destroy(espec_grid_plan* plan);
+/* Bounded waits of the grid kernels (no counterpart in the reference, which
+ * has no device waits).  Every grid-barrier wait of the SIL and PSOD kernels
+ * gives up after `polls` polls of the arrival count (0: the default, 2^24,
+ * seconds); the kernel then sets its error flag and returns, and
+ * espec_grid_results reports ESPEC_ECUDA ("timed out"), the drop-ins INFO = 2.
+ * espec_selftest_short_arrivals(k): the next k grid launches start their
+ * arrival count one short, so their first barrier never completes and every
+ * wait runs out -- the time-out path exercised without any fault; the device
+ * stays usable. */
+int espec_set_wait_limit(long polls);
+int espec_selftest_short_arrivals(int launches);
+
+/* ----------------------------------------------------------------------
+ * Analytic potentials on the GPU: the forms of POT1D / POT2D / POT3D
+ * (potfuncs.f:3-497) on the grid loop of GVPOT (gvpot.f:1-111), with its
+ * shift by the grid minimum when shiftp is set (1D and 3D: when the minimum
+ * is above 1e-6; 2D: when its magnitude is).  cst: the 14 constants (MXCST)
+ * GVPOT receives, i.e. after MAKECST, in atomic units.
+ *
+ * espec_pot_kind: ESPEC_POT_* of the name POTCH for a grid of ndim axes (the
+ * first of the reference's prefix tests that matches), 0 if none.
+ * espec_gvpot_1d: npk packets (a parameter scan; packet k: npts[k] points at
+ * xi[k] + i sh[k], constants cst[k*14 .. k*14+13]) in one launch; vpot:
+ * device, concatenated; xmin: host [npk] or NULL, the grid point of each
+ * minimum (GVPOT's XMIN) when shiftp.  Synchronous.
+ * espec_gvpot_nd: one 2D or 3D grid (x fastest); sm: masses per axis (the
+ * .LBH_CC / .LEPS_CC mass-scaled coordinates); quirks: ESPEC_Q_GVPOT_3D.
+ * ---------------------------------------------------------------------- */
+int espec_pot_kind(const char* potch, size_t len, int ndim);
+int espec_gvpot_1d(int npk, const int* npts, const double* xi, const double* sh, int kind,
+                   const double* cst, int shiftp, double* vpot, double* xmin, void* stream);
+int espec_gvpot_nd(int ndim, const int* np, const double* xi, const double* sh,
+                   const double* sm, int kind, const double* cst, int shiftp, int quirks,
+                   double* vpot, void* stream);
 
 /* ----------------------------------------------------------------------
  * Split-operator propagation on one 2D or 3D grid (PSPOFFT/PSPOFFTAUX,
@@ -442,6 +525,11 @@ int espec_gemm_bf16(int M, int N, int K, float alpha, const void* A, int lda, in
 /* synchronous: 1 when a tensor-core GEMM gave up waiting for its MMAs since
  * the last call (its output is then not written), else 0; clears the flag */
 int espec_gemm_bf16_status(int* timed_out);
+/* Self-test of the tensor-core GEMM's bounded mbarrier wait: one thread waits
+ * on an mbarrier nothing arrives on (no copy or MMA attached) with a limit of
+ * `polls` polls; *gave_up = 1 when the wait gave up as it must (the GEMM
+ * status flag is set too: read it with espec_gemm_bf16_status).  Synchronous. */
+int espec_selftest_mbar_wait(long polls, int* gave_up);
 /* z[r,c] += b[c]; h = bf16(GELU(z)) (act != 0) or bf16(z); h may be NULL */
 int espec_mlp_bias_gelu(float* z, const float* b, int rows, int cols, int act, void* h_bf16,
                         void* stream);

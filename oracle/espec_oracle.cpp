@@ -1814,3 +1814,171 @@ extern "C" int orc_eig_lanczsg(int ndim, const int* np, const double* shm, const
   }
   return rc;
 }
+
+// ---------------------------------------------------------------------------
+// potfuncs.f:3-497  POT1D / POT2D / POT3D: the analytic potentials, chosen by
+// the first prefix test of POTCH that matches, in the reference's order.
+// ---------------------------------------------------------------------------
+static bool pot_is(const char* potch, const char* p) {
+  return std::strncmp(potch, p, std::strlen(p)) == 0;
+}
+
+extern "C" double orc_pot1d(const char* potch, const double* cst, double rx) {
+  const double* c = cst - 1;  // CST(1..) as in the Fortran
+  if (pot_is(potch, ".OHS")) return 5.0e-1 * c[2] * std::pow(rx - c[1], 2);  // :63-64
+  if (pot_is(potch, ".DOHS"))                                                 // :66-68
+    return 5.0e-1 * c[2] * std::pow(rx - c[1], 2) +
+           c[5] * std::exp(std::pow(rx - c[3], 2) / std::pow(c[4], 2));
+  if (pot_is(potch, ".MORSEM"))  // :70-79
+    return c[3] * (std::exp(-2.0 * c[2] * (rx - c[1])) - 2.0 * std::exp(-c[2] * (rx - c[1])));
+  if (pot_is(potch, ".ANTI-MORSEM"))  // :85-92
+    return c[3] / 2.0 * (std::exp(-2.0 * c[2] * (rx - c[1])) + 2.0 * std::exp(-c[2] * (rx - c[1])));
+  if (pot_is(potch, ".MOD-MORSE"))  // :100-102
+    return c[3] * std::pow(c[4] - std::exp(-c[2] * (rx - c[1])), 2) + c[5];
+  if (pot_is(potch, ".MORSE")) return c[3] * std::pow(1.0 - std::exp(-c[2] * (rx - c[1])), 2);
+  if (pot_is(potch, ".ANTI-MORSE"))
+    return c[3] / 2.0 * std::pow(1.0 + std::exp(-c[2] * (rx - c[1])), 2);
+  if (pot_is(potch, ".DMORSE"))  // :113-115
+    return c[3] * std::pow(1.0 - std::exp(-c[4] * (rx - c[1])), 2) +
+           c[5] * std::exp(-c[6] * std::pow(rx - c[2], 2));
+  if (pot_is(potch, ".STEP")) return (rx >= c[1] && rx <= c[2]) ? 0.0 : c[3];
+  if (pot_is(potch, ".BARRIER")) return (rx >= c[1] && rx <= c[2]) ? c[3] : 0.0;
+  if (pot_is(potch, ".CONST") || pot_is(potch, ".FREE")) return c[1];
+  return std::nan("");  // the reference prints an error and STOPs
+}
+
+extern "C" double orc_pot3d(const char* potch, const double* cst, double rx, double ry,
+                            double rz) {
+  const double* c = cst - 1;
+  if (pot_is(potch, ".OHS"))
+    return 5.0e-1 * c[2] * std::pow(rx - c[1], 2) + 5.0e-1 * c[4] * std::pow(ry - c[3], 2) +
+           5.0e-1 * c[6] * std::pow(rz - c[5], 2);
+  if (pot_is(potch, ".STEP"))
+    return (rx >= c[1] && rx <= c[2] && ry >= c[3] && ry <= c[4] && rz >= c[5] && rz <= c[6])
+               ? 0.0 : c[7];
+  if (pot_is(potch, ".BARRIER"))  // :425-431, the third test on RY as written
+    return (rx >= c[1] && rx <= c[2] && ry >= c[3] && ry <= c[4] && ry >= c[5] && ry <= c[6])
+               ? c[7] : 0.0;
+  if (pot_is(potch, ".LEPS")) {  // :433-487
+    const double a = c[10], b = c[11], g = c[12];
+    const double q1 = 5.0e-1 * (orc_pot1d(".MORSEM", cst, rx) +
+                                (1 - a) / (1 + a) * orc_pot1d(".ANTI-MORSEM", cst, rx));
+    const double q2 = 5.0e-1 * (orc_pot1d(".MORSEM", cst + 3, ry) +
+                                (1 - b) / (1 + b) * orc_pot1d(".ANTI-MORSEM", cst + 3, ry));
+    const double q3 = 5.0e-1 * (orc_pot1d(".MORSEM", cst + 6, rz) +
+                                (1 - g) / (1 + g) * orc_pot1d(".ANTI-MORSEM", cst + 6, rz));
+    const double j1 = 5.0e-1 * (orc_pot1d(".MORSEM", cst, rx) -
+                                (1 - a) / (1 + a) * orc_pot1d(".ANTI-MORSEM", cst, rx));
+    const double j2 = 5.0e-1 * (orc_pot1d(".MORSEM", cst + 3, ry) -
+                                (1 - b) / (1 + b) * orc_pot1d(".ANTI-MORSEM", cst + 3, ry));
+    const double j3 = 5.0e-1 * (orc_pot1d(".MORSEM", cst + 6, rz) -
+                                (1 - g) / (1 + g) * orc_pot1d(".ANTI-MORSEM", cst + 6, rz));
+    return q1 + q2 + q3 -
+           std::sqrt(j1 * j1 + j2 * j2 + j3 * j3 - j1 * j2 - j2 * j3 - j1 * j3);
+  }
+  if (pot_is(potch, ".CONST") || pot_is(potch, ".FREE")) return c[1];
+  return std::nan("");
+}
+
+extern "C" double orc_pot2d(const char* potch, const double* sm, const double* cst, double rx,
+                            double ry) {
+  const double* c = cst - 1;
+  const double* m = sm - 1;
+  if (pot_is(potch, ".OHS"))
+    return 5.0e-1 * c[2] * std::pow(rx - c[1], 2) + 5.0e-1 * c[4] * std::pow(ry - c[3], 2);
+  if (pot_is(potch, ".MORSE"))
+    return c[3] * std::pow(1.0 - std::exp(-c[2] * (rx - c[1])), 2) +
+           c[6] * std::pow(1.0 - std::exp(-c[5] * (ry - c[4])), 2);
+  if (pot_is(potch, ".LSM") || pot_is(potch, ".LS")) {  // :214-233
+    const double v1a = c[3] * (1.0 - std::exp(-c[2] * std::pow(rx - c[1], 2) / (2.0 * rx + 1.0e-99)));
+    const double v1b =
+        c[5] * (1.0 - std::exp(-c[4] * std::pow(ry - rx - c[1], 2) / (2.0 * (ry - c[1]) + 1.0e-99)));
+    if (!pot_is(potch, ".LSM")) return v1a + v1b;
+    const double v2 = c[2] * std::pow(1.0 - std::exp(-c[7] * (ry - c[6])), 2);
+    return v1a + v1b + v2;
+  }
+  if (pot_is(potch, ".LBH_CC") || pot_is(potch, ".LBH")) {  // :234-253
+    double rxa = rx, rya = ry;
+    if (pot_is(potch, ".LBH_CC")) {
+      rya = ry / std::sqrt(m[2] * m[3] * (m[1] + m[2] + m[3]) / (std::pow(m[2] + m[3], 2) * m[1]));
+      rxa = rx + m[2] * rya / (m[2] + m[3]) - rya;
+    }
+    const double vab = c[1] * std::exp(-1.0 / c[2] * rxa);
+    const double vbc = c[3] * (std::exp(-2.0 * c[4] * (rya - c[5])) - 2.0 * std::exp(-c[4] * (rya - c[5])));
+    return vab + vbc;
+  }
+  if (pot_is(potch, ".LEPS_CC")) {
+    const double rya =
+        ry / std::sqrt(m[2] * m[3] * (m[1] + m[2] + m[3]) / (std::pow(m[2] + m[3], 2) * m[1]));
+    const double rxa = rx - m[2] * rya / (m[2] + m[3]);
+    const double rza = std::sqrt(rxa * rxa + rya * rya - 2.0 * rxa * rya * std::cos(c[13]));
+    return orc_pot3d(".LEPS", cst, rxa, rya, rza);
+  }
+  if (pot_is(potch, ".LEPS")) {
+    const double rz = std::sqrt(rx * rx + ry * ry - 2.0 * rx * ry * std::cos(c[13]));
+    return orc_pot3d(".LEPS", cst, rx, ry, rz);
+  }
+  if (pot_is(potch, ".WELLXY"))
+    return ((rx >= c[1] && rx <= c[2]) ? 0.0 : c[3]) + ((ry >= c[4] && ry <= c[5]) ? 0.0 : c[6]);
+  if (pot_is(potch, ".WELLX")) return (rx >= c[1] && rx <= c[2]) ? 0.0 : c[3];
+  if (pot_is(potch, ".WELLY")) return (ry >= c[1] && ry <= c[2]) ? 0.0 : c[3];
+  if (pot_is(potch, ".WELL"))
+    return (rx >= c[1] && rx <= c[2] && ry >= c[3] && ry <= c[4]) ? 0.0 : c[5];
+  if (pot_is(potch, ".BARRIERXY"))
+    return ((rx >= c[1] && rx <= c[2]) ? c[3] : 0.0) + ((ry >= c[4] && ry <= c[5]) ? c[6] : 0.0);
+  if (pot_is(potch, ".BARRIERX")) return (rx >= c[1] && rx <= c[2]) ? c[3] : 0.0;
+  if (pot_is(potch, ".BARRIERY")) return (ry >= c[1] && ry <= c[2]) ? c[3] : 0.0;
+  if (pot_is(potch, ".BARRIER"))
+    return (rx >= c[1] && rx <= c[2] && ry >= c[3] && ry <= c[4]) ? c[5] : 0.0;
+  if (pot_is(potch, ".CONST") || pot_is(potch, ".FREE")) return c[1];
+  return std::nan("");
+}
+
+// gvpot.f:1-111  GVPOT: the potential on the grid (x fastest) and, with
+// SHIFTP, the shift by its minimum (1D and 3D: when above 1e-6; 2D: when its
+// magnitude is); 1D returns XMIN.  The 3D loop takes RX from the K index
+// (gvpot.f:96) when quirk3d is set.
+extern "C" void orc_gvpot(int shiftp, const char* potch, int ndim, const int* np,
+                          const double* xi, const double* sm, const double* sh,
+                          const double* cst, int quirk3d, double* vpot, double* xmin) {
+  double aux = 1.0e+99;
+  if (ndim == 1) {
+    for (int i = 0; i < np[0]; ++i) {
+      const double rx = xi[0] + i * sh[0];
+      vpot[i] = orc_pot1d(potch, cst, rx);
+      if (shiftp && vpot[i] < aux) {
+        aux = vpot[i];
+        *xmin = rx;
+      }
+    }
+    if (shiftp && aux > 1.0e-6)
+      for (int i = 0; i < np[0]; ++i) vpot[i] -= aux;
+  } else if (ndim == 2) {
+    for (int j = 0; j < np[1]; ++j) {
+      const double ry = xi[1] + j * sh[1];
+      for (int i = 0; i < np[0]; ++i) {
+        const double rx = xi[0] + i * sh[0];
+        const long l = i + (long)j * np[0];
+        vpot[l] = orc_pot2d(potch, sm, cst, rx, ry);
+        if (shiftp && vpot[l] < aux) aux = vpot[l];
+      }
+    }
+    if (shiftp && std::fabs(aux) > 1.0e-6)
+      for (long l = 0; l < (long)np[0] * np[1]; ++l) vpot[l] -= aux;
+  } else {
+    for (int k = 0; k < np[2]; ++k) {
+      const double rz = xi[2] + k * sh[2];
+      for (int j = 0; j < np[1]; ++j) {
+        const double ry = xi[1] + j * sh[1];
+        for (int i = 0; i < np[0]; ++i) {
+          const double rx = xi[0] + (quirk3d ? k : i) * sh[0];
+          const long l = i + (long)j * np[0] + (long)k * np[0] * np[1];
+          vpot[l] = orc_pot3d(potch, cst, rx, ry, rz);
+          if (shiftp && vpot[l] < aux) aux = vpot[l];
+        }
+      }
+    }
+    if (shiftp && aux > 1.0e-6)
+      for (long l = 0; l < (long)np[0] * np[1] * np[2]; ++l) vpot[l] -= aux;
+  }
+}

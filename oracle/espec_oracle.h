@@ -182,6 +182,14 @@ int orc_eig_lanczsg(int ndim, const int* np, const double* shm, const double* vp
                     int nstates, int m, double tol, int maxrest, const double* start,
                     double* evals, double* evecs, double* resid, int* matvecs);
 
+/* potfuncs.f POT1D / POT2D / POT3D and gvpot.f GVPOT (CST(1..14) as cst[0..13]) */
+double orc_pot1d(const char* potch, const double* cst, double rx);
+double orc_pot2d(const char* potch, const double* sm, const double* cst, double rx, double ry);
+double orc_pot3d(const char* potch, const double* cst, double rx, double ry, double rz);
+void orc_gvpot(int shiftp, const char* potch, int ndim, const int* np, const double* xi,
+               const double* sm, const double* sh, const double* cst, int quirk3d,
+               double* vpot, double* xmin);
+
 #ifdef __cplusplus
 }
 #endif

@@ -396,3 +396,23 @@ def spo_batch(off, sh, sm, vpot, u, v, dt_fs, nsteps, nthreads=1, quirks=0):
                         nsteps, quirks, _p(cre), _p(cim), nthreads)
     c = (cre + 1j * cim).reshape(npk, nsteps + 1)
     return c, u, v
+
+
+def gvpot(shiftp, potch, np_, xi, sh, cst, sm=None, quirk3d=0):
+    """GVPOT (gvpot.f) with POT1D/2D/3D (potfuncs.f): (vpot x fastest, XMIN)."""
+    nd = len(np_)
+    l = lib()
+    l.orc_gvpot.argtypes = [C.c_int, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double),
+                            C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    npa = np.array(list(np_) + [1] * (3 - nd), dtype=np.int32)
+    xia = f64(list(xi) + [0.0] * (3 - nd))
+    sha = f64(list(sh) + [0.0] * (3 - nd))
+    sma = f64(list(sm) + [1.0] * (3 - len(sm))) if sm is not None else f64([1.0, 1.0, 1.0])
+    c = np.zeros(14)
+    c[:len(cst)] = cst
+    out = np.zeros(int(np.prod(np_)))
+    xmin = C.c_double(0.0)
+    l.orc_gvpot(int(bool(shiftp)), potch.encode(), nd, _ip(npa), _p(xia), _p(sma), _p(sha),
+                _p(c), int(quirk3d), _p(out), C.byref(xmin))
+    return out, xmin.value

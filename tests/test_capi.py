@@ -34,3 +34,17 @@ def test_errors_are_reported_without_a_device_call():
     rc = lib.espec_spo_create(C.byref(h), 0, None, None, None, 0.0, 0, 0, 0)
     assert rc == N.EINVAL
     assert b"null" in lib.espec_last_error()
+
+
+def test_fortran_shim_binds_exported_drop_ins():
+    """include/espec_gpu.f90 binds (bind(C)) only symbols the library exports,
+    one per reference routine it replaces, with three hidden lengths each."""
+    src = open(os.path.join(ROOT, "include", "espec_gpu.f90")).read()
+    names = re.findall(r'bind\(C,\s*name="([a-z_]+)"\)', src)
+    assert sorted(names) == ["plnz_", "psod_", "psodfft_", "pspofft_"]
+    lib = N.load()
+    for name in names:
+        assert hasattr(lib, name), name
+    assert src.count("integer(c_size_t), value :: dim_len, prtcrl_len, tpabsor_len") == 4
+    for routine in ("espec_pspofft", "espec_psodfft", "espec_plnz", "espec_psod"):
+        assert f"subroutine {routine}(" in src and f"end subroutine {routine}" in src
