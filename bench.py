@@ -826,8 +826,13 @@ def main():
     stream = torch.cuda.current_stream(dev)
     sh = stream.cuda_stream
     b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision=args.precision)
-    # inputs resident in HBM before timing
-    vpot_d = torch.from_numpy(w["vpot"]).to(dev)
+    # inputs resident in HBM before timing: the potentials built on the GPU
+    # from the scan's parameter table (GVPOT with the .MORSE form)
+    from espec_b200 import potential as P
+
+    p = w["params"]
+    vpot_d, _ = P.gvpot_1d(w["n"], np.full(w["npk"], 0.5), w["sh"], ".MORSE",
+                           np.stack([p["re"], p["a"], p["de"]], axis=1), shiftp=False)
     psi_d = torch.from_numpy(w["psi"]).to(dev)
     zero_d = torch.zeros_like(psi_d)
     b.load(vpot_d, (psi_d, zero_d), stream=sh)

@@ -24,6 +24,7 @@ PULSE_NONE, PULSE_GAUS, PULSE_GGAUS, PULSE_SIN2 = 0, 1, 2, 3
 SPO, SOD, SIL, PSOD = 0, 1, 2, 3
 MEM_HOST, MEM_DEVICE = 0, 1
 LAUNCH_CLASSES, LAUNCH_PERSISTENT = 0, 1
+VARIANT_TC = 5
 SHFS = 2.4188843243e-2
 
 # every symbol the header declares (checked by the CPU test suite)
@@ -32,6 +33,7 @@ EXPORTS = [
     "espec_spo_run", "espec_spo_results", "espec_spo_device_c", "espec_spo_npoints",
     "espec_spo_destroy", "espec_spo_set_variant", "espec_spo_variant_count",
     "espec_spo_run_static", "espec_spo_set_launch", "espec_spo_set_item_cost", "espec_prop_nonfinite",
+    "espec_spo_tc_status",
     "espec_prop_create", "espec_prop_previous", "espec_prop_continue",
     "espec_prop_energies", "espec_format_crl_row", "pspofft_", "psodfft_", "espec_grid_create",
     "espec_grid_load", "espec_grid_run", "espec_grid_continue", "espec_grid_results",
@@ -85,6 +87,7 @@ def load():
     lib.espec_spo_set_variant.argtypes = [vp, C.c_int, C.c_int]
     lib.espec_spo_set_launch.argtypes = [vp, C.c_int]
     lib.espec_prop_nonfinite.argtypes = [vp, C.POINTER(C.c_int), vp]
+    lib.espec_spo_tc_status.argtypes = [C.POINTER(C.c_int)]
     lib.espec_set_wait_limit.argtypes = [C.c_long]
     lib.espec_pot_kind.argtypes = [C.c_char_p, C.c_size_t, C.c_int]
     lib.espec_gvpot_1d.argtypes = [C.c_int, vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp]

@@ -212,7 +212,18 @@ static void plan_info_n(int v, std::vector<int>& kap, int& n3) {
 }
 
 // final-layout frequencies and radix-3 count of the plan behind variant v
+// the tensor-core variant of 256-point packets (spo_tc.cu)
+void spo_tc256_final_freq(int* kap);
+cudaError_t spo_tc256_launch(const SpoArgs<float>& a, int npk, cudaStream_t st);
+int spo_tc_status(int* timed_out);
+
 static void plan_info(int n, int v, std::vector<int>& kap, int& n3) {
+  if (v == ESPEC_VARIANT_TC) {  // n == 256, mixed: no radix-3 stage
+    kap.assign(256, 0);
+    spo_tc256_final_freq(kap.data());
+    n3 = 0;
+    return;
+  }
   switch (n) {
     case 256: plan_info_n<256>(v, kap, n3); break;
     case 384: plan_info_n<384>(v, kap, n3); break;
@@ -561,9 +572,14 @@ extern "C" int espec_spo_create(espec_spo_plan** out, int npk, const int* npts,
 extern "C" int espec_spo_set_variant(espec_spo_plan* p, int npts, int variant) {
   if (!p) return set_error(ESPEC_EINVAL, "null plan");
   if (p->method != ESPEC_SPO) return set_error(ESPEC_EINVAL, "variants exist for ESPEC_SPO only");
-  if (variant < 0 || variant >= kNumVariants) return set_error(ESPEC_EINVAL, "unknown variant");
-  if (!variant_fits(npts, variant, p->precision))
+  if (variant == ESPEC_VARIANT_TC) {
+    if (npts != 256 || p->precision != ESPEC_MIXED)
+      return set_error(ESPEC_EINVAL, "the tensor-core variant runs 256-point packets, mixed form");
+  } else if (variant < 0 || variant >= kNumVariants) {
+    return set_error(ESPEC_EINVAL, "unknown variant");
+  } else if (!variant_fits(npts, variant, p->precision)) {
     return set_error(ESPEC_EINVAL, "variant needs more shared memory than a CTA can have");
+  }
   bool found = false;
   for (auto& c : p->classes)
     if (c.n == npts) {
@@ -831,7 +847,8 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
       a.c_out = p->d_c;
       a.nsteps = nsteps;
       a.nonfinite = p->d_nonfinite;
-      e = launch_n<float>(c.n, c.variant, a, c.count, false, cs);
+      e = c.variant == ESPEC_VARIANT_TC ? spo_tc256_launch(a, c.count, cs)
+                                         : launch_n<float>(c.n, c.variant, a, c.count, false, cs);
     }
     if (e != cudaSuccess) return set_cuda_error("spo1d_kernel launch", e);
     ESPEC_CK(cudaEventRecord(p->events[ci], cs));
@@ -887,6 +904,11 @@ extern "C" int espec_spo_results(espec_spo_plan* p, double* c_re, double* c_im, 
 }
 
 extern "C" const void* espec_spo_device_c(const espec_spo_plan* p) { return p ? p->d_c : nullptr; }
+
+extern "C" int espec_spo_tc_status(int* timed_out) {
+  if (!timed_out) return set_error(ESPEC_EINVAL, "null argument");
+  return spo_tc_status(timed_out);
+}
 
 extern "C" int espec_prop_nonfinite(espec_spo_plan* p, int* count, void* stream) {
   if (!p || !count) return set_error(ESPEC_EINVAL, "null argument");

@@ -274,6 +274,14 @@ int espec_prop_energies(espec_spo_plan* plan, double* e, double* norm, void* str
  * before espec_spo_load.  Defaults come from autotuning on B200. */
 int espec_spo_set_variant(espec_spo_plan* plan, int npts, int variant);
 int espec_spo_variant_count(void);
+/* ESPEC_VARIANT_TC (256-point packets, mixed form only): the FFT as dense
+ * 16-point DFT GEMMs on the tensor cores (tcgen05.mma, BF16 x 3 split
+ * operands, FP32 accumulation in tensor memory), 8 packets per CTA; the
+ * phases, twiddles and C(t) as the other mixed variants.  No counterpart in
+ * the reference (its FFT is fft3d.f).  espec_spo_tc_status: 1 when one of its
+ * bounded mbarrier waits gave up since the last call (synchronous; clears). */
+#define ESPEC_VARIANT_TC 5
+int espec_spo_tc_status(int* timed_out);
 /* Launch shape of espec_spo_run / espec_prop_continue.  ESPEC_LAUNCH_PERSISTENT
  * (the default when every packet size is 256..2048 and the plan is an FP64 or
  * mixed split operator without the in-place defect): one kernel whose CTAs
