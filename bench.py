@@ -64,7 +64,8 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=100)
     ap.add_argument("--no-extra", action="store_true", help="skip the further legs")
     ap.add_argument("--leg", default=None,
-                    choices=["c1", "c2", "c3", "mixed", "sil_2d", "psod_2d", "grid_sweep", "eig"],
+                    choices=["c1", "c2", "c3", "mixed", "sil_2d", "sil_ctas", "psod_2d",
+                             "grid_sweep", "eig"],
                     help="run one leg alone and print its JSON")
     ap.add_argument("--case", default=None,
                     choices=["eig", "spond2d", "spond3d", "spectrum", "sil", "gemm"],
@@ -613,6 +614,39 @@ def grid_sweep(dev, steps=50, cpu_steps=0):
     return out
 
 
+def sil_ctas(dev, steps=50, n=256, m=12):
+    """SIL order m on the n x n coupled-Morse grid with different CTA counts of
+    the cooperative launch: us per step (a step is 2m grid barriers)."""
+    import espec_b200 as E
+
+    x = np.linspace(0.5, 8.0, n)
+    X, Y = np.meshgrid(x, x, indexing="ij")
+    V = 0.17 * (1 - np.exp(-(X - 1.4))) ** 2 + 0.12 * (1 - np.exp(-1.2 * (Y - 1.8))) ** 2
+    psi = np.exp(-((X - 1.6) ** 2) / 0.045 - ((Y - 2.0) ** 2) / 0.045)
+    psi = (psi / np.sqrt(np.sum(psi ** 2))).ravel(order="F").astype(complex)
+    h = x[1] - x[0]
+    shm = [1.0 / (24.0 * mm * h * h) for mm in (918.0, 1500.0)]
+    out = {"workload": f"SIL order {m}, {n}x{n} coupled Morse, us per step by CTA count"}
+    ref = None
+    for ctas in (8, 16, 32, 48, 64, 96, 128, 0):
+        g = E.SilGrid([n, n], shm, 1e-3, m)
+        try:
+            g.set_ctas(ctas)
+        except E.EspecError:
+            g.close()
+            continue
+        g.load(V.ravel(order="F"), psi)
+        g.run(3)
+        g.results()
+        ms = timed(lambda: g.run(steps), 1, dev) / steps
+        c, _ = g.results()
+        g.close()
+        ref = c if ref is None else ref
+        out[str(ctas) if ctas else "max"] = {"us_per_step": ms * 1e3,
+                                             "dC_vs_first": float(np.max(np.abs(c - ref)))}
+    return out
+
+
 def sil_bytes(m):
     """Algorithmic bytes per grid point and step of SIL order m (FP64), both
     chains: m H.psi (read psi and V, write H psi: 24 B each), the
@@ -815,6 +849,7 @@ def main():
                     "sil_2d": lambda: sil_2d(dev, steps=args.leg_steps, cpu_steps=0),
                     "psod_2d": lambda: psod_2d(dev, steps=args.leg_steps, cpu_steps=0),
                     "grid_sweep": lambda: grid_sweep(dev, steps=args.leg_steps),
+                    "sil_ctas": lambda: sil_ctas(dev),
                     "eig": lambda: eig_warmstart(args, dev)}
             print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         if world > 1:

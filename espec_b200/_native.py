@@ -49,6 +49,7 @@ EXPORTS = [
     "espec_spond_results", "espec_spond_destroy", "espec_spond_continue", "espec_spond_energies",
     "espec_spond_create_method", "espec_spond_previous",
     "espec_set_wait_limit", "espec_selftest_short_arrivals", "espec_selftest_mbar_wait",
+    "espec_grid_set_ctas",
     "espec_pot_kind", "espec_gvpot_1d", "espec_gvpot_nd",
 ]
 
@@ -89,6 +90,7 @@ def load():
     lib.espec_prop_nonfinite.argtypes = [vp, C.POINTER(C.c_int), vp]
     lib.espec_spo_tc_status.argtypes = [C.POINTER(C.c_int)]
     lib.espec_set_wait_limit.argtypes = [C.c_long]
+    lib.espec_grid_set_ctas.argtypes = [vp, C.c_int]
     lib.espec_pot_kind.argtypes = [C.c_char_p, C.c_size_t, C.c_int]
     lib.espec_gvpot_1d.argtypes = [C.c_int, vp, vp, vp, C.c_int, vp, C.c_int, vp, vp, vp]
     lib.espec_gvpot_nd.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int, vp, C.c_int, C.c_int, vp, vp]

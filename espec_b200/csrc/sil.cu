@@ -795,7 +795,7 @@ struct espec_grid_plan {
   double shm[3] = {0, 0, 0};
   double dt_fs = 0.0;
   int m = 0, absorb = 0, quirks = 0;
-  int nblocks = 0;
+  int nblocks = 0, nblocks_max = 0;  // CTAs of the cooperative launches (<= co-resident)
   bool loaded = false, has_state = false;
   double *d_vpot = nullptr, *d_mask = nullptr, *d_u = nullptr, *d_v = nullptr;
   double *d_u0 = nullptr, *d_v0 = nullptr, *d_L = nullptr, *d_work = nullptr, *d_wbuf = nullptr;
@@ -937,6 +937,7 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   if (want > (long)nsm * occ) want = (long)nsm * occ;
   if (want > cap) want = cap;
   p->nblocks = (int)(want > 0 ? want : 1);
+  p->nblocks_max = p->nblocks;
   auto fail = [&](int rc) {
     grid_free(p);
     delete p;
@@ -1172,6 +1173,14 @@ extern "C" int espec_set_wait_limit(long polls) {
 extern "C" int espec_selftest_short_arrivals(int launches) {
   if (launches < 0) return set_error(ESPEC_EINVAL, "negative launch count");
   g_short_arrivals.store(launches);
+  return ESPEC_OK;
+}
+
+extern "C" int espec_grid_set_ctas(espec_grid_plan* p, int nctas) {
+  if (!p || nctas < 0) return set_error(ESPEC_EINVAL, "null plan or negative CTA count");
+  if (nctas > p->nblocks_max)
+    return set_error(ESPEC_EINVAL, "more CTAs than the plan's co-resident maximum");
+  p->nblocks = nctas == 0 ? p->nblocks_max : nctas;
   return ESPEC_OK;
 }
 

@@ -71,6 +71,10 @@ class SilGrid:
                 "espec_grid_energies")
         return e.value, nr.value
 
+    def set_ctas(self, nctas):
+        """CTAs of the cooperative launches (0: the plan's maximum)."""
+        N.check(N.load().espec_grid_set_ctas(self._h, int(nctas)), "espec_grid_set_ctas")
+
     def set_pulse(self, dm, ef):
         """A laser pulse (chpot.f): V - dm * ef[j] in PSODAUX call j of a PSOD
         plan (PPSOD; ef from ppsod_field) or in the step landing at step j of a

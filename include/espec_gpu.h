@@ -411,6 +411,12 @@ void espec_grid_destroy(espec_grid_plan* plan);
  * stays usable. */
 int espec_set_wait_limit(long polls);
 int espec_selftest_short_arrivals(int launches);
+/* CTAs of the plan's cooperative launches: 1 .. the co-resident maximum chosen
+ * at creation (one per SM, or every co-resident CTA for large PSOD grids);
+ * 0 restores that maximum.  Fewer CTAs make each grid barrier's reduction
+ * cheaper on small grids (a tuning knob; results do not depend on it beyond
+ * the order of the partial sums). */
+int espec_grid_set_ctas(espec_grid_plan* plan, int nctas);
 
 /* ----------------------------------------------------------------------
  * Analytic potentials on the GPU: the forms of POT1D / POT2D / POT3D
