@@ -168,6 +168,13 @@ __device__ VMin block_min(VMin m, VMin* sh) {
 
 constexpr int kPotThreads = 256;
 
+// grid coordinate XI + (I-1) SH with the product rounded before the sum, as
+// the reference's Fortran computes it (a fused multiply-add would differ in
+// the last bit, and XMIN with it)
+__device__ __forceinline__ double coord(double xi, long i, double h) {
+  return __dadd_rn(xi, __dmul_rn((double)i, h));
+}
+
 struct Gv1 {
   const int* off;    // [npk + 1] first point of each packet
   const double* xi;  // [npk]
@@ -188,14 +195,14 @@ __global__ void __launch_bounds__(kPotThreads) gvpot1d_kernel(Gv1 a) {
   const double xi = a.xi[pk], h = a.sh[pk];
   VMin m{DBL_MAX, -1};
   for (long i = threadIdx.x; i < n; i += kPotThreads) {
-    const double v = pot1d(a.kind, c, xi + (double)i * h);
+    const double v = pot1d(a.kind, c, coord(xi, i, h));
     a.vpot[o + i] = v;
     m = vmin(m, VMin{v, i});
   }
   m = block_min<kPotThreads>(m, sh);
   if (threadIdx.x == 0) {
     s_min = m.v;
-    if (a.xmin) a.xmin[pk] = a.shiftp ? xi + (double)m.i * h : 0.0;
+    if (a.xmin) a.xmin[pk] = a.shiftp ? coord(xi, m.i, h) : 0.0;
   }
   __syncthreads();
   if (a.shiftp && s_min > 1.0e-6)
@@ -223,10 +230,10 @@ __global__ void __launch_bounds__(kPotThreads) gvpotnd_kernel(GvN a) {
     const long i = l % a.nx, j = (l / a.nx) % a.ny, k = l / ((long)a.nx * a.ny);
     double v;
     if (a.ndim == 2) {
-      v = pot2d(a.kind, a.sm, a.cst, a.xi[0] + (double)i * a.sh[0], a.xi[1] + (double)j * a.sh[1]);
+      v = pot2d(a.kind, a.sm, a.cst, coord(a.xi[0], i, a.sh[0]), coord(a.xi[1], j, a.sh[1]));
     } else {
-      const double rx = a.xi[0] + (double)(a.quirk3d ? k : i) * a.sh[0];
-      v = pot3d(a.kind, a.cst, rx, a.xi[1] + (double)j * a.sh[1], a.xi[2] + (double)k * a.sh[2]);
+      const double rx = coord(a.xi[0], a.quirk3d ? k : i, a.sh[0]);
+      v = pot3d(a.kind, a.cst, rx, coord(a.xi[1], j, a.sh[1]), coord(a.xi[2], k, a.sh[2]));
     }
     a.vpot[l] = v;
     m = vmin(m, VMin{v, l});
