@@ -379,7 +379,7 @@ extern "C" int espec_gvpot_1d(int npk, const int* npts, const double* xi, const 
 extern "C" int espec_gvpot_nd(int ndim, const int* np, const double* xi, const double* sh,
                               const double* sm, int kind, const double* cst, int shiftp,
                               int quirks, double* vpot, void* stream) {
-  if ((ndim != 2 && ndim != 3) || !np || !xi || !sh || !cst || !vpot || (ndim == 2 && !sm))
+  if ((ndim != 2 && ndim != 3) || !np || !xi || !sh || !cst || !vpot)
     return set_error(ESPEC_EINVAL, "espec_gvpot_nd: null or invalid argument");
   if (!kind_ok(kind, ndim)) return set_error(ESPEC_EINVAL, "espec_gvpot_nd: not a form of this dimension");
   GvN a{};
@@ -392,8 +392,9 @@ extern "C" int espec_gvpot_nd(int ndim, const int* np, const double* xi, const d
   for (int d = 0; d < ndim; ++d) {
     a.xi[d] = xi[d];
     a.sh[d] = sh[d];
-    a.sm[d] = sm ? sm[d] : 0.0;
   }
+  // the three masses SM(1..3) of the mass-scaled forms (.LBH_CC, .LEPS_CC)
+  for (int d = 0; d < 3; ++d) a.sm[d] = sm ? sm[d] : 1.0;
   std::memcpy(a.cst, cst, sizeof(a.cst));
   a.kind = kind;
   a.quirk3d = (quirks & ESPEC_Q_GVPOT_3D) ? 1 : 0;

@@ -431,8 +431,9 @@ int espec_grid_set_ctas(espec_grid_plan* plan, int nctas);
  * xi[k] + i sh[k], constants cst[k*14 .. k*14+13]) in one launch; vpot:
  * device, concatenated; xmin: host [npk] or NULL, the grid point of each
  * minimum (GVPOT's XMIN) when shiftp.  Synchronous.
- * espec_gvpot_nd: one 2D or 3D grid (x fastest); sm: masses per axis (the
- * .LBH_CC / .LEPS_CC mass-scaled coordinates); quirks: ESPEC_Q_GVPOT_3D.
+ * espec_gvpot_nd: one 2D or 3D grid (x fastest); sm: NULL or the three
+ * masses SM(1..3) of the .LBH_CC / .LEPS_CC mass-scaled coordinates (unused
+ * by the other forms); quirks: ESPEC_Q_GVPOT_3D.
  * ---------------------------------------------------------------------- */
 int espec_pot_kind(const char* potch, size_t len, int ndim);
 int espec_gvpot_1d(int npk, const int* npts, const double* xi, const double* sh, int kind,

@@ -29,7 +29,15 @@ FORMS_3D = {".OHS": [1.7, 0.08, 2.0, 0.05, 1.9, 0.06], ".STEP": [1.0, 4.0, 1.5, 
 
 
 def _close(a, b):
-    return np.max(np.abs(a - b) / np.maximum(1.0, np.abs(b))) <= 1e-13
+    # the reference's formulas overflow on parts of some grids (.LS's 1/(2(RY -
+    # CST(1))) term): the same non-finite values at the same points, the
+    # finite ones to 1e-13
+    fa, fb = np.isfinite(a), np.isfinite(b)
+    if not np.array_equal(fa, fb):
+        return False
+    if not np.array_equal(a[~fb], b[~fb], equal_nan=True):
+        return False
+    return not fb.any() or np.max(np.abs(a[fb] - b[fb]) / np.maximum(1.0, np.abs(b[fb]))) <= 1e-13
 
 
 @pytest.mark.parametrize("shiftp", [False, True])
