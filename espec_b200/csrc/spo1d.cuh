@@ -89,6 +89,68 @@ struct Plan {
       if (r[i] % 3 == 0) ++c;
     return c;
   }
+
+  // Shared-memory layout of exchange s (outputs of stage s -> inputs of
+  // stage s+1): one of three XOR swizzles of the low four index bits, each a
+  // bijection inside every 16-element block, chosen at compile time as the
+  // one with the fewest bank conflicts for the exchange's store and load
+  // patterns: 16-byte elements are served per quarter warp (8 lanes must hit
+  // distinct index residues mod 8), 8-byte elements per half warp (16 lanes,
+  // residues mod 16).  The radix-12 and radix-4 chains conflict under the
+  // first swizzle (a stride-2 index pattern in their last exchanges).
+  static __host__ __device__ constexpr int swz_apply(int kind, int i) {
+    return kind == 0 ? i ^ (((i >> 3) ^ (i >> 4)) & 15)
+                     : (kind == 1 ? i ^ (((i >> 1) ^ (i >> 2)) & 15) : i ^ (((i >> 1) ^ (i >> 3)) & 15));
+  }
+  static __host__ __device__ constexpr int c_beta(int s, int t, int q) {
+    return (t >> 5) * 32 * Q(s) + (t & 31) + 32 * q;
+  }
+  // element of lane t: output k of butterfly q of stage s (out = true), or
+  // input k of butterfly q of stage s
+  static __host__ __device__ constexpr int c_pos(bool out, int s, int t, int q, int k) {
+    const int m = M(s) / r[s], b = c_beta(s, t, q);
+    return out ? ((b / m) * r[s] + k) * m + b % m : (b / m) * M(s) + b % m + m * k;
+  }
+  // extra wavefronts of one warp instruction of warp w, for elements of 16
+  // and of 8 bytes
+  static __host__ __device__ constexpr int extra(int kind, int w, bool out, int s, int q, int k) {
+    int tot = 0;
+    for (int es = 0; es < 2; ++es) {
+      const int lanes = es == 0 ? 8 : 16;
+      for (int g = 0; g < 32; g += lanes) {
+        int cnt[16] = {}, mx = 0;
+        for (int l = g; l < g + lanes && w * 32 + l < T; ++l) {
+          const int res = swz_apply(kind, c_pos(out, s, w * 32 + l, q, k)) % lanes;
+          cnt[res] += 1;
+          if (cnt[res] > mx) mx = cnt[res];
+        }
+        if (mx > 1) tot += mx - 1;
+      }
+    }
+    return tot;
+  }
+  static __host__ __device__ constexpr int conflicts(int s, int kind) {
+    int tot = 0;
+    const int W = T < 32 ? 1 : T / 32;
+    for (int w = 0; w < W; ++w) {
+      for (int q = 0; q < Q(s); ++q)
+        for (int k = 0; k < r[s]; ++k) tot += extra(kind, w, true, s, q, k);
+      for (int q = 0; q < Q(s + 1); ++q)
+        for (int k = 0; k < r[s + 1]; ++k) tot += extra(kind, w, false, s + 1, q, k);
+    }
+    return tot;
+  }
+  static __host__ __device__ constexpr int swz_pick(int s) {
+    int best = 0, bc = conflicts(s, 0);
+    for (int kind = 1; kind < 3; ++kind) {
+      const int c = conflicts(s, kind);
+      if (c < bc) {
+        best = kind;
+        bc = c;
+      }
+    }
+    return best;
+  }
 };
 
 template <int N>
@@ -226,11 +288,12 @@ struct SpoThread {
   rot_t tw[PL::NTW];
   int bar = 0;  // hardware barrier id of this thread's packet group (group_bar)
 
-  // shared-memory swizzle: flips the low 4 bits of an element index with
-  // bits 3..7, a bijection inside every 16-element block that makes all the
-  // exchange patterns of the plans above bank-conflict free (8- and 16-byte
-  // elements)
-  static ESPEC_HD int sidx(int i) { return i ^ (((i >> 3) ^ (i >> 4)) & 15); }
+  // shared-memory layout of exchange s (Plan::swz_pick, chosen at compile time)
+  template <int s>
+  static ESPEC_HD int sidx(int i) {
+    constexpr int kind = PL::swz_pick(s);
+    return PL::swz_apply(kind, i);
+  }
 
   ESPEC_HD void init_twiddles(int t) { init_stage<0>(t); }
 
@@ -351,12 +414,12 @@ struct SpoThread {
 #pragma unroll
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
-      for (int k = 0; k < R0; ++k) buf[sidx(out_pos<s>(t, q, k))] = v[q * R0 + k];
+      for (int k = 0; k < R0; ++k) buf[sidx<s>(out_pos<s>(t, q, k))] = v[q * R0 + k];
     xsync<s>();
 #pragma unroll
     for (int q = 0; q < Q1; ++q)
 #pragma unroll
-      for (int k = 0; k < R1; ++k) v[q * R1 + k] = buf[sidx(in_pos<s + 1>(t, q, k))];
+      for (int k = 0; k < R1; ++k) v[q * R1 + k] = buf[sidx<s>(in_pos<s + 1>(t, q, k))];
   }
   // reverse exchange: inputs of s+1 -> outputs of s
   template <int s>
@@ -366,12 +429,12 @@ struct SpoThread {
 #pragma unroll
     for (int q = 0; q < Q1; ++q)
 #pragma unroll
-      for (int k = 0; k < R1; ++k) buf[sidx(in_pos<s + 1>(t, q, k))] = v[q * R1 + k];
+      for (int k = 0; k < R1; ++k) buf[sidx<s>(in_pos<s + 1>(t, q, k))] = v[q * R1 + k];
     xsync<s>();
 #pragma unroll
     for (int q = 0; q < Q0; ++q)
 #pragma unroll
-      for (int k = 0; k < R0; ++k) v[q * R0 + k] = buf[sidx(out_pos<s>(t, q, k))];
+      for (int k = 0; k < R0; ++k) v[q * R0 + k] = buf[sidx<s>(out_pos<s>(t, q, k))];
   }
 
   template <int s>
