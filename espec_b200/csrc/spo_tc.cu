@@ -114,6 +114,13 @@ __device__ __forceinline__ void write_row(uint8_t* a, int r, const cpx<float>* v
   }
 }
 
+__device__ __forceinline__ float row_norm(const cpx<float>* v) {
+  float n = 0.0f;
+#pragma unroll
+  for (int j = 0; j < kL; ++j) n = fmaf(v[j].x, v[j].x, fmaf(v[j].y, v[j].y, n));
+  return n;
+}
+
 __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
   const uint32_t a = su32(bar);
   for (long i = 0; i < kTcWaitLimit; ++i) {
@@ -159,17 +166,22 @@ struct TcCta {
   bool ok;
 
   // the A tile written by every thread -> 12 MMAs (dir 0 forward, 1 inverse)
-  // -> D in TMEM -> this thread's row
-  __device__ __forceinline__ void gemm(int dir, float (&d)[32]) {
+  // -> D in TMEM -> this thread's row.  nin: squared norm of this thread's
+  // input row.  The tensor cores' FP32 accumulation truncates (rounds toward
+  // zero), a bias that shrank every row by ~2.5e-7 per stage and C(t) by
+  // ~1e-6 per step; each stage is a 16-point DFT per row, unitary up to the
+  // factor 4, so the row's norm is restored to exactly 4 sqrt(nin).
+  __device__ __forceinline__ void gemm(int dir, float (&d)[32], float nin) {
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (threadIdx.x == 0 && ok) {
       const uint32_t a0 = su32(a), b0 = su32(b + dir * 3 * kBTile);
-      // (A split, B split) of the six products kept
-      constexpr int pa[6] = {0, 0, 1, 0, 1, 2};
-      constexpr int pb[6] = {0, 1, 0, 2, 1, 0};
+      // (A split, B split) of the six products kept, smallest first so that
+      // the small terms are summed before the large one joins them
+      constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
+      constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
 #pragma unroll
       for (int q = 0; q < 6; ++q)
 #pragma unroll
@@ -197,6 +209,14 @@ struct TcCta {
     const int w = threadIdx.x >> 5;
     if (ok) {
       tmem_ld32(tmem + ((uint32_t)(w * 32) << 16), d);
+      float nout = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) nout = fmaf(d[j], d[j], nout);
+      if (nout > 0.0f) {
+        const float sc = 4.0f * sqrtf(nin / nout);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) d[j] *= sc;
+      }
     } else {
 #pragma unroll
       for (int j = 0; j < 32; ++j) d[j] = 0.0f;
@@ -317,24 +337,24 @@ __global__ void __launch_bounds__(kRows, 1) spo_tc256_kernel(SpoArgs<float> a, i
     cpx<float> y[kL];
     // forward stage A: lines s over n2 -> Y[n1 = s][k1 = c]
     write_row(cta.a, t, v);
-    cta.gemm(0, d);
+    cta.gemm(0, d, row_norm(v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) y[c] = rot<false>(tw[c], mk(d[c], d[kL + c]));
     cta.transpose(y, v);  // thread (p, k1 = s): Y[n1 = c][k1]
     // forward stage B: -> X[k1 + 16 k2], k2 = c; kinetic phase
     write_row(cta.a, t, v);
-    cta.gemm(0, d);
+    cta.gemm(0, d, row_norm(v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) v[c] = TB::apply(a.tab.k[kb + c], mk(d[c], d[kL + c]));
     // inverse stage B: -> Y[n1 = c][k1 = s], conjugate twiddle
     write_row(cta.a, t, v);
-    cta.gemm(1, d);
+    cta.gemm(1, d, row_norm(v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) y[c] = rot<true>(tw[c], mk(d[c], d[kL + c]));
     cta.transpose(y, v);  // thread (p, n1 = s): Y[n1][k1 = c]
     // inverse stage A: -> x[s + 16 n2], n2 = c
     write_row(cta.a, t, v);
-    cta.gemm(1, d);
+    cta.gemm(1, d, row_norm(v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) v[c] = mk(d[c], d[kL + c]);
     // C(t) = sum w x: FP32 products per thread, FP64 over the packet's threads

@@ -10,6 +10,7 @@ import pytest
 import espec_b200 as E
 from espec_b200 import workloads as W
 from espec_b200 import _native as NAT
+from fp32_floor import fp32_state_floor
 
 pytestmark = pytest.mark.gpu
 
@@ -107,36 +108,48 @@ def test_fp64_absorbers_match_oracle(oracle, kind):
     assert np.sum(np.abs(psi) ** 2) < 0.999  # the absorber removed norm
 
 
+# The mixed form keeps the state in FP32, so over long runs its |dC(t)| is a
+# random walk that no FP32-state form can hold below 1e-6 on every packet
+# (tests/test_fp32_state_floor.py).  Long runs are therefore held to the
+# 1e-6 bound or to a small multiple of each packet's own FP32-state floor
+# (the error of a perfect FP32-state propagation of the same packet),
+# whichever is larger; short runs to 1e-6 itself.
+FLOOR_FACTOR = 8.0
+
+
 def test_mixed_all_sizes_accuracy(oracle):
-    """FP32 data with FP64 phases/C(t): |dC| stays at the 1e-6 level over
-    2000 steps for every packet size (lifting rotations keep the error a
-    random walk)."""
+    """FP32 data with FP64 phases/C(t) over 2000 steps, every packet size:
+    |dC| within 1e-6 or FLOOR_FACTOR x the packet's FP32-state floor."""
     n, off, sh, sm, v, psi = random_packets(SIZES, seed=11)
     dt = 0.5 * W.SHFS
     c_ref, _ = oracle_batch(oracle, n, off, sh, sm, v, psi, dt, 2000)
     c, _ = gpu_batch(n, sh, sm, v, psi, dt, 2000, "mixed")
     err = np.max(np.abs(c - c_ref), axis=1)
-    print("mixed |dC| per size:", dict(zip(n.tolist(), err.tolist())))
-    assert np.all(err <= 5e-6), err
+    floor = fp32_state_floor(n, sh, sm, v, psi, off, 0.5, 2000)
+    print("mixed |dC| per size:", dict(zip(n.tolist(), err.tolist())), "floor:", floor)
+    assert np.all(err <= np.maximum(1e-6, FLOOR_FACTOR * floor)), (err, floor)
 
 
 def test_scan_subset_mixed_vs_fp64():
-    """A 64-packet slice of the batched Morse scan: mixed vs FP64 on the GPU."""
+    """A 64-packet slice of the batched Morse scan over 1000 steps: mixed vs
+    FP64 on the GPU, each packet within 1e-6 or FLOOR_FACTOR x its floor."""
     w = W.morse_scan(npk=64, nsteps=1000)
     c64, _ = gpu_batch(w["n"], w["sh"], w["sm"], w["vpot"], w["psi"], w["dt_fs"], 1000, "fp64")
     c32, _ = gpu_batch(w["n"], w["sh"], w["sm"], w["vpot"], w["psi"], w["dt_fs"], 1000, "mixed")
-    err = np.max(np.abs(c64 - c32))
-    assert err <= 5e-6, err
+    err = np.max(np.abs(c64 - c32), axis=1)
+    floor = fp32_state_floor(w["n"], w["sh"], w["sm"], w["vpot"], w["psi"], w["off"], 0.5, 1000)
+    assert np.all(err <= np.maximum(1e-6, FLOOR_FACTOR * floor)), (err.max(), floor.max())
 
 
 @pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_every_variant_matches_oracle(oracle, variant):
     """Each kernel variant (plan / table location / register budget) of each
-    packet size gives the oracle's C(t): FP64 to 1e-10, mixed to 5e-6."""
+    packet size gives the oracle's C(t) over 200 steps: FP64 to 1e-10, mixed to
+    the 1e-6 bound."""
     n, off, sh, sm, v, psi = random_packets(SIZES, seed=23)
     dt = 0.5 * W.SHFS
     c_ref, p_ref = oracle_batch(oracle, n, off, sh, sm, v, psi, dt, 200)
-    for prec, tol in (("fp64", 1e-10), ("mixed", 5e-6)):
+    for prec, tol in (("fp64", 1e-10), ("mixed", 1e-6)):
         b = E.SpoBatch(n, sh, sm, dt, precision=prec)
         for size in SIZES:
             try:

@@ -76,7 +76,8 @@ def test_mixed_form_against_fp64(np_):
     dt = 0.1 * NAT.SHFS
     c64, p64 = gpu_spo(np_, sh, sm, dt, v, psi, 400)
     c32, p32 = gpu_spo(np_, sh, sm, dt, v, psi, 400, precision="mixed")
-    assert np.max(np.abs(c32 - c64)) <= 2e-5, np.max(np.abs(c32 - c64))
+    # 400 steps of a packet spread over many points: inside the 1e-6 bound
+    assert np.max(np.abs(c32 - c64)) <= 1e-6, np.max(np.abs(c32 - c64))
     assert np.max(np.abs(p32 - p64)) <= 2e-4
 
 
