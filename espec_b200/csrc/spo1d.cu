@@ -549,11 +549,12 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
     p->t32.w = (cpx<float>*)(c + 4 * np);  // 12-byte phases: w stays 4-byte aligned
   }
   // the persistent launch covers the SPO method without the in-place defect
-  // when every packet size has a class in the persistent kernel
+  // when every packet size has a class in the persistent kernel; it is an
+  // option (espec_spo_set_launch): on the 4096-packet Morse scan one kernel
+  // per size class with each size's own variant runs 6-9% faster
   p->persist_ok = method == ESPEC_SPO && !(quirks & ESPEC_Q_SPO_INPLACE);
   for (int i = 0; i < npk && p->persist_ok; ++i) p->persist_ok = persist_class(p->n[i]) >= 0;
   if (p->persist_ok) {
-    p->launch = ESPEC_LAUNCH_PERSISTENT;
     if ((rc = ck(cudaMalloc(&p->d_pk_items, sizeof(SpoPacket) * npk), "cudaMalloc"))) return fail(rc);
     if ((rc = ck(cudaMalloc(&p->d_items, sizeof(SpoItem) * npk), "cudaMalloc"))) return fail(rc);
     if ((rc = ck(cudaMalloc(&p->d_next, sizeof(unsigned int)), "cudaMalloc"))) return fail(rc);

@@ -282,14 +282,15 @@ int espec_spo_variant_count(void);
  * bounded mbarrier waits gave up since the last call (synchronous; clears). */
 #define ESPEC_VARIANT_TC 5
 int espec_spo_tc_status(int* timed_out);
-/* Launch shape of espec_spo_run / espec_prop_continue.  ESPEC_LAUNCH_PERSISTENT
- * (the default when every packet size is 256..2048 and the plan is an FP64 or
- * mixed split operator without the in-place defect): one kernel whose CTAs
- * claim items -- groups of packets of one size filling a CTA -- from a device
- * counter, longest items first.  ESPEC_LAUNCH_CLASSES: one kernel per size
- * class on concurrent streams, each with the variant espec_spo_set_variant
- * chose (setting a variant selects this shape).  Call before espec_spo_load;
- * no counterpart in the reference (its scans run one process per packet). */
+/* Launch shape of espec_spo_run / espec_prop_continue.  ESPEC_LAUNCH_CLASSES
+ * (the default): one kernel per size class on concurrent streams, each with
+ * the variant espec_spo_set_variant chose (setting a variant selects this
+ * shape).  ESPEC_LAUNCH_PERSISTENT (available when every packet size is
+ * 256..2048 and the plan is an FP64 or mixed split operator without the
+ * in-place defect): one kernel whose CTAs claim items -- groups of packets of
+ * one size filling a CTA -- from a device counter, longest items first.  Call
+ * before espec_spo_load; no counterpart in the reference (its scans run one
+ * process per packet). */
 int espec_spo_set_launch(espec_spo_plan* plan, int mode);
 /* Relative cost of one persistent item of packets of size npts (the claim
  * order is by decreasing cost; default: points of an item x log2 npts). */
