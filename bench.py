@@ -14,8 +14,8 @@ state cannot hold 1e-6 over 8000 steps of this scan
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp64|mixed] [--npk 4096] [--nsteps 8000]
-    python bench.py --leg c1|c2|c3|mixed|sil_2d|psod_2d|grid_sweep|eig
-    python bench.py --case eig|spond2d|spond3d|spectrum|sil|gemm   (profiling)
+    python bench.py --leg c1|c2|c3|mixed|sil_2d|sil_ctas|psod_2d|grid_sweep|eig|tc256
+    python bench.py --case eig|spond2d|spond3d|spectrum|sil|gemm|tc256   (profiling)
 
 Multi-GPU (torchrun): packets are independent, each rank propagates its own
 batch (seed + rank) with no collective on the data path -> weak scaling.
@@ -65,10 +65,10 @@ def parse():
     ap.add_argument("--no-extra", action="store_true", help="skip the further legs")
     ap.add_argument("--leg", default=None,
                     choices=["c1", "c2", "c3", "mixed", "sil_2d", "sil_ctas", "psod_2d",
-                             "grid_sweep", "eig"],
+                             "grid_sweep", "eig", "tc256"],
                     help="run one leg alone and print its JSON")
     ap.add_argument("--case", default=None,
-                    choices=["eig", "spond2d", "spond3d", "spectrum", "sil", "gemm"],
+                    choices=["eig", "spond2d", "spond3d", "spectrum", "sil", "gemm", "tc256"],
                     help="small self-checking workload for profiling one kernel")
     ap.add_argument("--leg-steps", type=int, default=100)
     ap.add_argument("--eig-train", type=int, default=50000)
@@ -375,6 +375,54 @@ def leg_mixed(args, dev, ms_fp64=None, npk_acc=256):
         "note": "an FP32 state alone (one rounding per step, exact arithmetic otherwise) "
                 "passes 1e-6 on the scan's heavy N = 256/384 packets within 8000 steps "
                 "(tests/test_fp32_state_floor.py); the FP64 form meets the gate"}
+    return out
+
+
+def leg_tc256(dev, npk=4096, nsteps=2000, npk_acc=64):
+    """256-point packets of the Morse scan's family, mixed form: the
+    tensor-core DFT variant (ESPEC_VARIANT_TC) against the register-FFT
+    variants, rate and |dC| against the FP64 GPU form."""
+    import torch
+
+    import espec_b200 as E
+    from espec_b200 import _native as NAT
+    from espec_b200 import workloads as W
+
+    w = W.morse_scan(npk=npk, nsteps=nsteps, seed=rank_seed(0), sizes=(256,))
+    pts = float(w["off"][-1]) * nsteps
+    vpot_d = torch.from_numpy(w["vpot"]).to(dev)
+    psi_d = torch.from_numpy(w["psi"]).to(dev)
+    zero_d = torch.zeros_like(psi_d)
+    st = torch.cuda.current_stream(dev).cuda_stream
+    out = {"workload": f"{npk} packets of 256 points x {nsteps} steps, mixed form"}
+    for name, var in (("register_default", None), ("register_v0", 0), ("tc", NAT.VARIANT_TC)):
+        b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision="mixed")
+        if var is not None:
+            b.set_variant(256, var)
+
+        def step():
+            b.load(vpot_d, (psi_d, zero_d), stream=st)
+            b.run(nsteps, stream=st)
+
+        step()
+        ms = timed(step, 3, dev)
+        b.close()
+        out[name] = {"ms": ms, "Mgridpt*steps/s": pts / (ms * 1e-3) / 1e6}
+    # accuracy on the first npk_acc packets over the same steps
+    ws = W.morse_scan(npk=npk_acc, nsteps=nsteps, seed=rank_seed(0), sizes=(256,))
+    cs = {}
+    for name, prec, var in (("fp64", "fp64", None), ("register", "mixed", None),
+                            ("tc", "mixed", NAT.VARIANT_TC)):
+        bb = E.SpoBatch(ws["n"], ws["sh"], ws["sm"], ws["dt_fs"], precision=prec)
+        if var is not None:
+            bb.set_variant(256, var)
+        bb.load(ws["vpot"], ws["psi"])
+        bb.run(nsteps)
+        cs[name], _ = bb.results()
+        bb.close()
+    out["dC_vs_fp64"] = {"register": dc_stats(cs["register"], cs["fp64"]),
+                         "tc": dc_stats(cs["tc"], cs["fp64"])}
+    out["tc_over_register"] = out["register_default"]["ms"] / out["tc"]["ms"]
     return out
 
 
@@ -805,6 +853,19 @@ def profile_case(name, dev):
         c, _ = g.results()
         g.close()
         return float(np.abs(c[-1]))
+    if name == "tc256":  # spo_tc256_kernel: 1184 packets of 256 points (8 per CTA), 200 steps
+        from espec_b200 import _native as NAT
+        from espec_b200 import workloads as W
+
+        w = W.morse_scan(npk=1184, nsteps=200, seed=3, sizes=(256,))
+        b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision="mixed")
+        b.set_variant(256, NAT.VARIANT_TC)
+        b.load(w["vpot"], w["psi"])
+        for _ in range(3):
+            b.run(w["nsteps"])
+        c, _ = b.results()
+        b.close()
+        return float(np.abs(c[:, -1]).max())
     if name == "gemm":  # gemm_bf16_tc: the warm start's output layer on 2048 proposals
         from espec_b200 import warmstart as WS
 
@@ -849,7 +910,7 @@ def main():
                     "sil_2d": lambda: sil_2d(dev, steps=args.leg_steps, cpu_steps=0),
                     "psod_2d": lambda: psod_2d(dev, steps=args.leg_steps, cpu_steps=0),
                     "grid_sweep": lambda: grid_sweep(dev, steps=args.leg_steps),
-                    "sil_ctas": lambda: sil_ctas(dev),
+                    "sil_ctas": lambda: sil_ctas(dev), "tc256": lambda: leg_tc256(dev),
                     "eig": lambda: eig_warmstart(args, dev)}
             print(json.dumps({"leg": args.leg, **legs[args.leg]()}), flush=True)
         if world > 1:

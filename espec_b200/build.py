@@ -18,6 +18,9 @@ SOURCES = ["spo1d.cu", "capi.cu", "spo1d_inst_f32_pow2.cu", "spo1d_inst_f32_r3.c
            "spectrum.cu", "potential.cu", "eig.cu", "mlp.cu", "mlp_tc.cu",
            "spond.cu", "deck.cpp", "pulse.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# per-file flags: the analytic potentials follow the reference's arithmetic
+# (no fused multiply-add), so that they match it to the last bit of exp/cos
+FILE_FLAGS = {"potential.cu": ["-fmad=false"]}
 
 
 def nvcc():
@@ -50,7 +53,8 @@ def build(force=False, verbose=False):
     for src in SOURCES:
         obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
         objs.append(obj)
-        procs.append((src, subprocess.Popen(common + ["-c", os.path.join(CSRC, src), "-o", obj])))
+        cmd = common + FILE_FLAGS.get(src, []) + ["-c", os.path.join(CSRC, src), "-o", obj]
+        procs.append((src, subprocess.Popen(cmd)))
     bad = [src for src, pr in procs if pr.wait() != 0]
     if bad:
         raise RuntimeError("nvcc failed for " + ", ".join(bad))

@@ -24,32 +24,26 @@ namespace {
 
 constexpr int kCst = 14;  // MXCST (param.f)
 
+// Every form keeps the association of the Fortran expression it restates
+// (A*B**2/C is (A*(B*B))/C, left to right) and the file is compiled without
+// FMA contraction, so a potential differs from the reference's only through
+// the last bit of exp / cos.
+__device__ __forceinline__ double sq(double v) { return v * v; }
+
 __device__ double pot1d(int k, const double* c, double x) {
   switch (k) {
-    case ESPEC_POT_OHS: return 0.5 * c[1] * (x - c[0]) * (x - c[0]);
+    case ESPEC_POT_OHS: return 0.5 * c[1] * sq(x - c[0]);
     case ESPEC_POT_DOHS:  // potfuncs.f:66-68 (exponent with a + sign, as written)
-      return 0.5 * c[1] * (x - c[0]) * (x - c[0]) +
-             c[4] * exp((x - c[2]) * (x - c[2]) / (c[3] * c[3]));
+      return 0.5 * c[1] * sq(x - c[0]) + c[4] * exp(sq(x - c[2]) / sq(c[3]));
     case ESPEC_POT_MORSEM:
       return c[2] * (exp(-2.0 * c[1] * (x - c[0])) - 2.0 * exp(-c[1] * (x - c[0])));
     case ESPEC_POT_ANTI_MORSEM:
       return c[2] / 2.0 * (exp(-2.0 * c[1] * (x - c[0])) + 2.0 * exp(-c[1] * (x - c[0])));
-    case ESPEC_POT_MOD_MORSE: {
-      const double e = c[3] - exp(-c[1] * (x - c[0]));
-      return c[2] * e * e + c[4];
-    }
-    case ESPEC_POT_MORSE: {
-      const double e = 1.0 - exp(-c[1] * (x - c[0]));
-      return c[2] * e * e;
-    }
-    case ESPEC_POT_ANTI_MORSE: {
-      const double e = 1.0 + exp(-c[1] * (x - c[0]));
-      return c[2] / 2.0 * e * e;
-    }
-    case ESPEC_POT_DMORSE: {
-      const double e = 1.0 - exp(-c[3] * (x - c[0]));
-      return c[2] * e * e + c[4] * exp(-c[5] * (x - c[1]) * (x - c[1]));
-    }
+    case ESPEC_POT_MOD_MORSE: return c[2] * sq(c[3] - exp(-c[1] * (x - c[0]))) + c[4];
+    case ESPEC_POT_MORSE: return c[2] * sq(1.0 - exp(-c[1] * (x - c[0])));
+    case ESPEC_POT_ANTI_MORSE: return c[2] / 2.0 * sq(1.0 + exp(-c[1] * (x - c[0])));
+    case ESPEC_POT_DMORSE:
+      return c[2] * sq(1.0 - exp(-c[3] * (x - c[0]))) + c[4] * exp(-(c[5] * sq(x - c[1])));
     case ESPEC_POT_STEP: return (x >= c[0] && x <= c[1]) ? 0.0 : c[2];
     case ESPEC_POT_BARRIER: return (x >= c[0] && x <= c[1]) ? c[2] : 0.0;
     default: return c[0];  // ESPEC_POT_CONST (.CONST / .FREE)
@@ -71,8 +65,7 @@ __device__ double leps(const double* c, double x, double y, double z) {
 __device__ double pot3d(int k, const double* c, double x, double y, double z) {
   switch (k) {
     case ESPEC_POT_OHS:
-      return 0.5 * c[1] * (x - c[0]) * (x - c[0]) + 0.5 * c[3] * (y - c[2]) * (y - c[2]) +
-             0.5 * c[5] * (z - c[4]) * (z - c[4]);
+      return 0.5 * c[1] * sq(x - c[0]) + 0.5 * c[3] * sq(y - c[2]) + 0.5 * c[5] * sq(z - c[4]);
     case ESPEC_POT_STEP:
       return (x >= c[0] && x <= c[1] && y >= c[2] && y <= c[3] && z >= c[4] && z <= c[5]) ? 0.0
                                                                                            : c[6];
@@ -86,19 +79,16 @@ __device__ double pot3d(int k, const double* c, double x, double y, double z) {
 
 __device__ double pot2d(int k, const double* sm, const double* c, double x, double y) {
   switch (k) {
-    case ESPEC_POT_OHS:
-      return 0.5 * c[1] * (x - c[0]) * (x - c[0]) + 0.5 * c[3] * (y - c[2]) * (y - c[2]);
-    case ESPEC_POT_MORSE: {
-      const double ex = 1.0 - exp(-c[1] * (x - c[0])), ey = 1.0 - exp(-c[4] * (y - c[3]));
-      return c[2] * ex * ex + c[5] * ey * ey;
-    }
+    case ESPEC_POT_OHS: return 0.5 * c[1] * sq(x - c[0]) + 0.5 * c[3] * sq(y - c[2]);
+    case ESPEC_POT_MORSE:
+      return c[2] * sq(1.0 - exp(-c[1] * (x - c[0]))) + c[5] * sq(1.0 - exp(-c[4] * (y - c[3])));
     case ESPEC_POT_LSM: case ESPEC_POT_LS: {
-      const double va = c[2] * (1.0 - exp(-c[1] * (x - c[0]) * (x - c[0]) / (2.0 * x + 1.0e-99)));
-      const double d = y - x - c[0];
-      const double vb = c[4] * (1.0 - exp(-c[3] * d * d / (2.0 * (y - c[0]) + 1.0e-99)));
+      const double va = c[2] * (1.0 - exp(-(c[1] * sq(x - c[0]) / (2.0 * x + 1.0e-99))));
+      const double vb =
+          c[4] * (1.0 - exp(-(c[3] * sq(y - x - c[0]) / (2.0 * (y - c[0]) + 1.0e-99))));
       if (k == ESPEC_POT_LS) return va + vb;
-      const double e = 1.0 - exp(-c[6] * (y - c[5]));
-      return va + vb + c[1] * e * e;  // potfuncs.f:221: the well depth is CST(2), as written
+      // potfuncs.f:221: the well depth is CST(2), as written
+      return va + vb + c[1] * sq(1.0 - exp(-c[6] * (y - c[5])));
     }
     case ESPEC_POT_LBH_CC: case ESPEC_POT_LBH: {
       double rx = x, ry = y;
