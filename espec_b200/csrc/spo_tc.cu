@@ -18,19 +18,30 @@
 // the conjugate matrix in reverse; the kinetic phase sits between the two
 // transforms on thread (p, k1)'s frequencies k1 + 16 k2.
 //
-// Precision: operands are BF16, each FP32 value v split exactly into
-// v = h + m + l (three BF16 parts); the six products h H, h M, m H, h L, m M,
-// l H of data and DFT matrix accumulate in FP32 in tensor memory, which
-// leaves the products' error near FP32 rounding (the dropped products are
-// below 2^-24 of the result).  Twelve tcgen05.mma (kind::f16, M = 128,
-// N = 32, K = 16) per stage, issued by one thread and committed to an
-// mbarrier whose waits are bounded; the accumulator is read back with
-// tcgen05.ld (warp w: TMEM lanes 32w .. 32w + 31).  Operand tiles are "core
-// matrices" of 8 rows x 16 bytes without swizzle, K-major, the layout the
-// warm-start GEMM (mlp_tc.cu) uses.
+// Precision: fixed-point slices, so that the tensor cores add exactly.  Each
+// row of data is scaled by a power of two 2^-e to |y| < 1 and cut into three
+// BF16 slices y = a0 + a1 + a2 + r, a_i an integer multiple of 2^-8(i+1)
+// (|a0| <= 1, |a1| <= 2^-9, |a2| <= 2^-17, each slice rounded to nearest, the
+// residual |r| <= 2^-25 unbiased); the DFT matrix, |b| <= 1, is cut the same
+// way into four slices b0..b3 (32 bits: the forward and inverse matrices are
+// each other's inverse to 2^-33, so no fixed per-step bias remains).  The
+// products of order i + j = 0, 1, 2, 3 accumulate in four separate TMEM
+// accumulators: within one order every term is a multiple of 2^-8(i+j+2) and
+// the 32-term sums span at most 23 bits, so each accumulator holds its exact
+// sum whatever rounding the tensor cores' FP32 adders use (truncating adders
+// left a bias of ~1e-7 per step in C(t) when all orders shared one
+// accumulator).  The row is then P0 + (P1 + (P2 + P3)), rounded to nearest,
+// times 2^e.  Nine products, 18 tcgen05.mma (kind::f16, M = 128, N = 32,
+// K = 16) per stage, issued by one thread and committed to an mbarrier whose
+// waits are bounded; the accumulators are read back with tcgen05.ld (warp w:
+// TMEM lanes 32w .. 32w + 31).  Operand tiles are "core matrices" of 8 rows x
+// 16 bytes without swizzle, K-major, the layout the warm-start GEMM
+// (mlp_tc.cu) uses.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#include <cfloat>
 
 #include "espec_gpu.h"
 #include "espec_internal.h"
@@ -44,16 +55,20 @@ constexpr int kL = 16;           // line length (and number of lines) of a packe
 constexpr int kRows = 128;       // GEMM rows = threads = 8 packets x 16 lines
 constexpr int kPk = kRows / kL;  // packets per CTA
 constexpr int kK = 32;           // real K (and N) of one stage
-constexpr int kTmemCols = 32;
+constexpr int kAcc = 4;          // accumulators: product orders 0..3
+constexpr int kASl = 3;          // slices of a data row
+constexpr int kBSl = 4;          // slices of the DFT matrix
+constexpr int kTmemCols = kAcc * 32;
+static_assert(kTmemCols == 128, "TMEM allocations are powers of two >= 32 columns");
 constexpr long kTcWaitLimit = 1L << 22;
 constexpr int kStage = 33;       // staging row stride in floats (conflict-free columns)
 
 // shared-memory layout (bytes from a 1024-aligned base)
 constexpr int kATile = kRows * kK * 2;             // one BF16 split of the A tile: 8 KB
 constexpr int kBTile = kK * kK * 2;                // one BF16 split of a DFT matrix: 2 KB
-constexpr int kOffA = 0;                           // 3 splits
-constexpr int kOffB = kOffA + 3 * kATile;          // 2 directions x 3 splits
-constexpr int kOffStage = kOffB + 6 * kBTile;      // 128 x 33 floats
+constexpr int kOffA = 0;                           // kASl slices
+constexpr int kOffB = kOffA + kASl * kATile;       // 2 directions x kBSl slices
+constexpr int kOffStage = kOffB + 2 * kBSl * kBTile;  // 128 x 33 floats
 constexpr int kOffBar = kOffStage + kRows * kStage * 4;
 constexpr int kSmemBytes = 1024 + kOffBar + 64;
 
@@ -78,31 +93,46 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
 constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kK >> 3) << 17) |
                             ((uint32_t)(kRows >> 4) << 24);
 
-// v = h + m + l exactly (each difference is exact in FP32)
-__device__ __forceinline__ void split3(float v, uint16_t& h, uint16_t& m, uint16_t& l) {
-  const __nv_bfloat16 bh = __float2bfloat16_rn(v);
-  const float r1 = v - __bfloat162float(bh);
-  const __nv_bfloat16 bm = __float2bfloat16_rn(r1);
-  const float r2 = r1 - __bfloat162float(bm);
-  h = __bfloat16_as_ushort(bh);
-  m = __bfloat16_as_ushort(bm);
-  l = __bfloat16_as_ushort(__float2bfloat16_rn(r2));
+__device__ __forceinline__ uint16_t bf16_bits(float v) {  // v exact in BF16
+  return __bfloat16_as_ushort(__float2bfloat16_rn(v));
+}
+
+// y (|y| < 1) = a0 + a1 + a2 + r: a_i = round(y_i 2^(8i+8)) 2^-(8i+8) of the
+// remainder y_i, an integer of at most 8 bits times a power of two (exact in
+// BF16); every difference is exact in FP32
+__device__ __forceinline__ void slice3(float y, uint16_t& h, uint16_t& m, uint16_t& l) {
+  const float a0 = rintf(y * 256.0f) * (1.0f / 256.0f);
+  const float r1 = y - a0;
+  const float a1 = rintf(r1 * 65536.0f) * (1.0f / 65536.0f);
+  const float r2 = r1 - a1;
+  const float a2 = rintf(r2 * 16777216.0f) * (1.0f / 16777216.0f);
+  h = bf16_bits(a0);
+  m = bf16_bits(a1);
+  l = bf16_bits(a2);
 }
 
 __device__ __forceinline__ uint32_t pk2(uint16_t a, uint16_t b) {
   return (uint32_t)a | ((uint32_t)b << 16);
 }
 
-// row r of the A tile (three splits) from its 16 complex values
-__device__ __forceinline__ void write_row(uint8_t* a, int r, const cpx<float>* v) {
+// row r of the A tile (three slices) from its 16 complex values; returns
+// the row's scale 2^e (the GEMM's output row is scaled back by it)
+__device__ __forceinline__ float write_row(uint8_t* a, int r, const cpx<float>* v) {
+  float mx = 0.0f;
+#pragma unroll
+  for (int j = 0; j < kL; ++j) mx = fmaxf(mx, fmaxf(fabsf(v[j].x), fabsf(v[j].y)));
+  // mx 2^-e in [0.5, 1) for a normal mx (clamped to keep 2^e and 2^-e normal)
+  int e = 0;
+  if (mx > 0.0f && mx <= FLT_MAX) e = max(-126, min(126, ((__float_as_int(mx) >> 23) & 0xff) - 126));
+  const float down = __int_as_float((127 - e) << 23);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {  // k group: 8 consecutive K entries
     uint16_t h[8], m[8], l[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) {
-      const int k = 8 * q + e;
+    for (int e8 = 0; e8 < 8; ++e8) {
+      const int k = 8 * q + e8;
       const float x = k < kL ? v[k].x : v[k - kL].y;
-      split3(x, h[e], m[e], l[e]);
+      slice3(x * down, h[e8], m[e8], l[e8]);
     }
     const int off = core_off<kRows>(r, 8 * q);
     *reinterpret_cast<uint4*>(a + off) =
@@ -112,13 +142,7 @@ __device__ __forceinline__ void write_row(uint8_t* a, int r, const cpx<float>* v
     *reinterpret_cast<uint4*>(a + 2 * kATile + off) =
         make_uint4(pk2(l[0], l[1]), pk2(l[2], l[3]), pk2(l[4], l[5]), pk2(l[6], l[7]));
   }
-}
-
-__device__ __forceinline__ float row_norm(const cpx<float>* v) {
-  float n = 0.0f;
-#pragma unroll
-  for (int j = 0; j < kL; ++j) n = fmaf(v[j].x, v[j].x, fmaf(v[j].y, v[j].y, n));
-  return n;
+  return __int_as_float((127 + e) << 23);
 }
 
 __device__ __forceinline__ bool wait_parity(uint64_t* bar, uint32_t parity) {
@@ -165,34 +189,34 @@ struct TcCta {
   uint32_t phase;   // parity of the next mbarrier completion
   bool ok;
 
-  // the A tile written by every thread -> 12 MMAs (dir 0 forward, 1 inverse)
-  // -> D in TMEM -> this thread's row.  nin: squared norm of this thread's
-  // input row.  The tensor cores' FP32 accumulation truncates (rounds toward
-  // zero), a bias that shrank every row by ~2.5e-7 per stage and C(t) by
-  // ~1e-6 per step; each stage is a 16-point DFT per row, unitary up to the
-  // factor 4, so the row's norm is restored to exactly 4 sqrt(nin).
-  __device__ __forceinline__ void gemm(int dir, float (&d)[32], float nin) {
+  // the A tile written by every thread -> 18 MMAs (dir 0 forward, 1 inverse)
+  // into the four order accumulators -> this thread's row, P0 + (P1 + (P2 +
+  // P3)) times the row's scale
+  __device__ __forceinline__ void gemm(int dir, float (&d)[32], float scale) {
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     if (threadIdx.x == 0 && ok) {
-      const uint32_t a0 = su32(a), b0 = su32(b + dir * 3 * kBTile);
-      // (A split, B split) of the six products kept, smallest first so that
-      // the small terms are summed before the large one joins them
-      constexpr int pa[6] = {2, 1, 0, 1, 0, 0};
-      constexpr int pb[6] = {0, 1, 2, 0, 1, 0};
+      const uint32_t a0 = su32(a), b0 = su32(b + dir * kBSl * kBTile);
+      // (A slice, B slice) of the nine products kept, by order i + j; the
+      // first product of an order starts its accumulator
+      constexpr int pa[9] = {0, 1, 0, 2, 1, 0, 2, 1, 0};
+      constexpr int pb[9] = {0, 0, 1, 0, 1, 2, 1, 2, 3};
 #pragma unroll
-      for (int q = 0; q < 6; ++q)
+      for (int q = 0; q < 9; ++q)
 #pragma unroll
         for (int j = 0; j < 2; ++j) {
+          const int ord = pa[q] + pb[q];
+          const bool first = (q == 0 || pa[q - 1] + pb[q - 1] != ord) && j == 0;
           const uint64_t da = sdesc(a0 + pa[q] * kATile + j * 2 * (kRows * 16), kRows * 16, 128);
           const uint64_t db = sdesc(b0 + pb[q] * kBTile + j * 2 * (kK * 16), kK * 16, 128);
-          const uint32_t acc = (q > 0 || j > 0) ? 1u : 0u;
+          const uint32_t acc = first ? 0u : 1u;
           asm volatile(
               "{\n\t.reg .pred p;\n\t"
               "setp.ne.b32 p, %4, 0;\n\t"
-              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+              "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(
+                  tmem + (uint32_t)(ord * 32)),
               "l"(da), "l"(db), "r"(kIdesc), "r"(acc));
         }
       asm volatile(
@@ -208,15 +232,18 @@ struct TcCta {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const int w = threadIdx.x >> 5;
     if (ok) {
-      tmem_ld32(tmem + ((uint32_t)(w * 32) << 16), d);
-      float nout = 0.0f;
+      const uint32_t lane = tmem + ((uint32_t)(w * 32) << 16);
+      float e[32];
+      tmem_ld32(lane + 96, d);
+      tmem_ld32(lane + 64, e);
 #pragma unroll
-      for (int j = 0; j < 32; ++j) nout = fmaf(d[j], d[j], nout);
-      if (nout > 0.0f) {
-        const float sc = 4.0f * sqrtf(nin / nout);
+      for (int j = 0; j < 32; ++j) d[j] = __fadd_rn(e[j], d[j]);
+      tmem_ld32(lane + 32, e);
 #pragma unroll
-        for (int j = 0; j < 32; ++j) d[j] *= sc;
-      }
+      for (int j = 0; j < 32; ++j) d[j] = __fadd_rn(e[j], d[j]);
+      tmem_ld32(lane, e);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) d[j] = __fmul_rn(__fadd_rn(e[j], d[j]), scale);
     } else {
 #pragma unroll
       for (int j = 0; j < 32; ++j) d[j] = 0.0f;
@@ -241,8 +268,9 @@ struct TcCta {
   }
 };
 
-// The 32 x 32 real form of the 16-point DFT in K-major BF16 splits:
-// B[n][k] (row = output index N, column = input index K); dir 1 conjugate.
+// The 32 x 32 real form of the 16-point DFT in K-major BF16 slices (four,
+// cut from the FP64 value): B[n][k] (row = output index N, column = input
+// index K); dir 1 conjugate.
 __device__ void build_dft_tiles(uint8_t* b) {
   for (int e = threadIdx.x; e < 2 * kK * kK; e += blockDim.x) {
     const int dir = e / (kK * kK), nn = (e / kK) % kK, kk = e % kK;
@@ -254,13 +282,15 @@ __device__ void build_dft_tiles(uint8_t* b) {
     double v;
     if (nn < kL) v = kk < kL ? c : -s;
     else v = kk < kL ? s : c;
-    uint16_t h, m, l;
-    split3((float)v, h, m, l);  // |v| <= 1: the FP32 value keeps 24 bits
-    uint8_t* base = b + dir * 3 * kBTile;
+    uint8_t* base = b + dir * kBSl * kBTile;
     const int off = core_off<kK>(nn, kk);
-    *reinterpret_cast<uint16_t*>(base + off) = h;
-    *reinterpret_cast<uint16_t*>(base + kBTile + off) = m;
-    *reinterpret_cast<uint16_t*>(base + 2 * kBTile + off) = l;
+    double r = v, sc = 256.0;
+#pragma unroll
+    for (int i = 0; i < kBSl; ++i, sc *= 256.0) {
+      const double bi = rint(r * sc) / sc;  // an integer of <= 8 bits times 2^-(8i+8)
+      r -= bi;
+      *reinterpret_cast<uint16_t*>(base + i * kBTile + off) = bf16_bits((float)bi);
+    }
   }
 }
 
@@ -336,25 +366,21 @@ __global__ void __launch_bounds__(kRows, 1) spo_tc256_kernel(SpoArgs<float> a, i
     float d[32];
     cpx<float> y[kL];
     // forward stage A: lines s over n2 -> Y[n1 = s][k1 = c]
-    write_row(cta.a, t, v);
-    cta.gemm(0, d, row_norm(v));
+    cta.gemm(0, d, write_row(cta.a, t, v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) y[c] = rot<false>(tw[c], mk(d[c], d[kL + c]));
     cta.transpose(y, v);  // thread (p, k1 = s): Y[n1 = c][k1]
     // forward stage B: -> X[k1 + 16 k2], k2 = c; kinetic phase
-    write_row(cta.a, t, v);
-    cta.gemm(0, d, row_norm(v));
+    cta.gemm(0, d, write_row(cta.a, t, v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) v[c] = TB::apply(a.tab.k[kb + c], mk(d[c], d[kL + c]));
     // inverse stage B: -> Y[n1 = c][k1 = s], conjugate twiddle
-    write_row(cta.a, t, v);
-    cta.gemm(1, d, row_norm(v));
+    cta.gemm(1, d, write_row(cta.a, t, v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) y[c] = rot<true>(tw[c], mk(d[c], d[kL + c]));
     cta.transpose(y, v);  // thread (p, n1 = s): Y[n1][k1 = c]
     // inverse stage A: -> x[s + 16 n2], n2 = c
-    write_row(cta.a, t, v);
-    cta.gemm(1, d, row_norm(v));
+    cta.gemm(1, d, write_row(cta.a, t, v));
 #pragma unroll
     for (int c = 0; c < kL; ++c) v[c] = mk(d[c], d[kL + c]);
     // C(t) = sum w x: FP32 products per thread, FP64 over the packet's threads

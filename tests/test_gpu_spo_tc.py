@@ -4,7 +4,15 @@ the oracle and against the register-FFT mixed variant.
 
 Its arithmetic is FP32-class, like the other mixed variants: the error
 against the FP64 oracle is held to the same bound as the register kernels'
-mixed form over the same steps."""
+mixed form over the same steps (1e-6, or 8x the batch's FP32-state floor)."""
+
+FLOOR_FACTOR = 8.0
+
+
+def _bound(w):
+    floor = fp32_state_floor(w["n"], w["sh"], w["sm"], w["vpot"], w["psi"], w["off"], 0.5,
+                             w["nsteps"])
+    return max(1e-6, FLOOR_FACTOR * np.max(floor))
 import ctypes as C
 
 import numpy as np
@@ -13,6 +21,7 @@ import pytest
 import espec_b200 as E
 from espec_b200 import _native as N
 from espec_b200 import workloads as W
+from fp32_floor import fp32_state_floor
 
 pytestmark = pytest.mark.gpu
 
@@ -40,7 +49,8 @@ def test_tensor_core_variant_matches_oracle_and_register_fft(oracle):
     e_tc = np.max(np.abs(c_tc - c_ref))
     e_rf = np.max(np.abs(c_rf - c_ref))
     assert np.all(np.isfinite(c_tc))
-    assert e_tc <= 5e-6, (e_tc, e_rf)
+    print("tensor-core |dC|", e_tc, "register-FFT |dC|", e_rf)
+    assert e_tc <= _bound(w), (e_tc, e_rf)
     assert np.max(np.abs(p_tc - (u + 1j * v))) <= 5e-5
 
 
@@ -49,7 +59,7 @@ def test_tensor_core_variant_in_a_mixed_size_batch(oracle):
     c_tc, _ = _run(w, N.VARIANT_TC)
     c_ref, _, _ = oracle.spo_batch(w["off"], w["sh"], w["sm"], w["vpot"], w["psi"],
                                    np.zeros_like(w["psi"]), w["dt_fs"], w["nsteps"], nthreads=8)
-    assert np.max(np.abs(c_tc - c_ref)) <= 5e-6
+    assert np.max(np.abs(c_tc - c_ref)) <= _bound(w)
 
 
 def test_tensor_core_variant_refused_outside_its_case():
