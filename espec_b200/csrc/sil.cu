@@ -192,118 +192,138 @@ __device__ __forceinline__ double apply_h_nd(const SilArgs& a, const double* x, 
 }
 
 // Krylov coefficients of both chains (every CTA computes the same values):
-// Z = exp(-i cst T) by Taylor series (degree kTaylor) of T scaled to norm
-// <= 1/2, then squared back.  out[0] = Re Z y_u, out[1] = Im Z y_u (or
-// Im(Z^2) y_u / 2 in the reference-defect form), out[2] = Re Z y_v,
-// out[3] = -Im Z y_v.
-constexpr int kTaylor = 14;  // |B| <= 1/2: truncation 0.5^15/15! = 2.3e-17
-constexpr int kMM = kSilMaxM * kSilMaxM;
+// Z y = exp(-i cst T) y for the m x m symmetric tridiagonal T of each chain
+// (diagonal al, off-diagonal bt), without forming Z: the Chebyshev series of
+// the exponential on T's Gershgorin interval [c - h, c + h],
+//   exp(-i tau T) y = e^{-i tau c} sum_k eps_k (-i)^k J_k(tau h) T_k((T - c)/h) y
+// (eps_0 = 1, eps_k = 2; the Bessel values J_k by Miller's downward
+// recurrence), i.e. one three-term vector recurrence with a tridiagonal
+// product per term: one warp per series, lane i holding row i, no CTA
+// barrier.  The series is cut where 2 |J_{K+1}| < 1e-17 (K = 1.5 tau h + 25
+// terms, within kChebMax; a longer tau is split into equal parts applied in
+// turn).  The reference forms the same matrix function through the
+// eigenvectors of T (DSTEVX).  out[0] = Re Z y_u, out[1] = Im Z y_u (or
+// Im(Z^2 y_u) / 2 in the reference-defect form, the series for 2 cst on a
+// third warp), out[2] = Re Z y_v, out[3] = -Im Z y_v.
+constexpr int kChebMax = 176;  // Bessel values kept per series
 
 struct KrylovSmem {
-  double2 X[2][2][kMM];  // [buffer][chain], ping-pong
+  double J[3][kChebMax + 1];  // per series (warp)
 };
+
+// exp(-i tau T) y, row `lane` (m <= 32), by the whole warp; J: kChebMax + 1
+// doubles of shared memory for this warp's Bessel values
+__device__ double2 expm_tridiag_apply(int m, double tau, const double* al, const double* bt,
+                                      const double* y, double* J) {
+  const int lane = threadIdx.x & 31;
+  const unsigned full = 0xffffffffu;
+  const bool row = lane < m;
+  const double a_i = row ? al[lane] : 0.0;
+  const double b_lo = (row && lane > 0) ? bt[lane - 1] : 0.0;  // T_{i,i-1}
+  const double b_up = (row && lane + 1 < m) ? bt[lane] : 0.0;  // T_{i,i+1}
+  // Gershgorin interval of T
+  double lo = row ? a_i - fabs(b_lo) - fabs(b_up) : 1e300;
+  double hi = row ? a_i + fabs(b_lo) + fabs(b_up) : -1e300;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    lo = fmin(lo, __shfl_xor_sync(full, lo, o));
+    hi = fmax(hi, __shfl_xor_sync(full, hi, o));
+  }
+  const double c = 0.5 * (lo + hi), h = 0.5 * (hi - lo);
+  double xr = row ? y[lane] : 0.0, xi = 0.0;  // the vector the next part acts on
+  if (h > 0.0) {
+    const double za = fabs(tau) * h;
+    const int parts = (int)ceil(za / 100.0) > 1 ? (int)ceil(za / 100.0) : 1;
+    const double zp = za / parts;                    // |tau h| of one part
+    const int K = min((int)(1.5 * zp) + 25, kChebMax);
+    const double sgn = tau < 0.0 ? -1.0 : 1.0;       // J_k(-z) = (-1)^k J_k(z)
+    if (lane == 0) {
+      // Miller: J_{j-1} = (2j/z) J_j - J_{j+1} downward from a start well
+      // above K, normalised by J_0 + 2 sum_k J_2k = 1
+      const int nstart = 2 * ((K + 30 + (int)sqrt(40.0 * K)) / 2);
+      const double tz = 2.0 / zp;
+      double bjp = 0.0, bj = 1e-280, sum = 0.0;
+      for (int j = nstart; j > 0; --j) {
+        const double bjm = j * tz * bj - bjp;
+        bjp = bj;
+        bj = bjm;
+        if (fabs(bj) > 1e200) {
+          bj *= 1e-200;
+          bjp *= 1e-200;
+          sum *= 1e-200;
+          for (int k = j; k <= K; ++k) J[k] *= 1e-200;
+        }
+        if (j - 1 <= K) J[j - 1] = bj;
+        if (((j - 1) & 1) == 0 && j - 1 > 0) sum += bj;
+      }
+      const double rn = 1.0 / (bj + 2.0 * sum);
+      for (int k = 0; k <= K; ++k) J[k] *= ((k & 1) && sgn < 0.0 ? -rn : rn);
+    }
+    __syncwarp();
+    const double rh = 1.0 / h;
+    // (T - c)/h times v, row lane
+    auto tmul = [&](double v) {
+      const double vl = __shfl_up_sync(full, v, 1), vu = __shfl_down_sync(full, v, 1);
+      return ((a_i - c) * v + b_lo * (lane > 0 ? vl : 0.0) + b_up * vu) * rh;
+    };
+    double sr, si;
+    const double ph = -(tau / parts) * c;  // e^{-i (tau/parts) c}
+    double ps, pc;
+    sincos(ph, &ps, &pc);
+    for (int part = 0; part < parts; ++part) {
+      // real and imaginary parts of the input run through the same real
+      // recurrence; (-i)^k cycles 1, -i, -1, i
+      double w0r = xr, w0i = xi;
+      double w1r = tmul(w0r), w1i = tmul(w0i);
+      sr = J[0] * w0r;
+      si = J[0] * w0i;
+      // k = 1: -2i J_1 w1
+      sr += 2.0 * J[1] * w1i;
+      si -= 2.0 * J[1] * w1r;
+      for (int k = 2; k <= K; ++k) {
+        const double w2r = 2.0 * tmul(w1r) - w0r, w2i = 2.0 * tmul(w1i) - w0i;
+        const double ck = 2.0 * J[k];
+        switch (k & 3) {
+          case 0: sr += ck * w2r; si += ck * w2i; break;
+          case 1: sr += ck * w2i; si -= ck * w2r; break;
+          case 2: sr -= ck * w2r; si -= ck * w2i; break;
+          default: sr -= ck * w2i; si += ck * w2r; break;
+        }
+        w0r = w1r; w0i = w1i;
+        w1r = w2r; w1i = w2i;
+      }
+      xr = pc * sr - ps * si;
+      xi = pc * si + ps * sr;
+    }
+  } else {
+    // T = c I (a 1 x 1 T or a zero off-diagonal with equal diagonal)
+    double ps, pc;
+    sincos(-tau * c, &ps, &pc);
+    xi = ps * xr;
+    xr = pc * xr;
+  }
+  return make_double2(xr, xi);
+}
 
 __device__ void krylov_coeffs(int m, double cst, int quirk, const double (*al)[kSilMaxM],
                               const double (*bt)[kSilMaxM], const double (*y)[kSilMaxM],
                               const int* active, KrylovSmem& ks, double (*out)[kSilMaxM]) {
-  __shared__ int s_sq[2];
-  __shared__ double s_scale[2];
-  const int t = threadIdx.x;
-  if (t < 2) {
-    double nrm = 0.0;
-    for (int i = 0; i < m; ++i) {
-      double r = fabs(al[t][i]);
-      if (i > 0) r += fabs(bt[t][i - 1]);
-      if (i + 1 < m) r += fabs(bt[t][i]);
-      nrm = fmax(nrm, r);
-    }
-    nrm *= fabs(cst);
-    int sq = 0;
-    while (nrm > 0.5 && sq < 60) {
-      nrm *= 0.5;
-      ++sq;
-    }
-    s_sq[t] = sq;
-    s_scale[t] = ldexp(cst, -sq);
-  }
-  // buffer 0 = I
-  for (int e = t; e < 2 * kMM; e += blockDim.x) {
-    const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
-    ks.X[0][c][i * kSilMaxM + j] = make_double2(i == j ? 1.0 : 0.0, 0.0);
-  }
-  __syncthreads();
-  // Horner: P <- I + B P / k, B = -i scale T (T tridiagonal)
-  int cur = 0;
-  for (int k = kTaylor; k >= 1; --k) {
-    const double rk = 1.0 / k;
-    for (int e = t; e < 2 * kMM; e += blockDim.x) {
-      const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
-      if (i >= m || j >= m) continue;
-      const double2* P = ks.X[cur][c];
-      const double sc = s_scale[c];
-      // (B P)_{ij} = sum_l (-i sc T_il) P_lj = sum_l sc T_il (Im P_lj, -Re P_lj)
-      const double tii = sc * al[c][i];
-      const double2 pii = P[i * kSilMaxM + j];
-      double re = tii * pii.y, im = -tii * pii.x;
-      if (i > 0) {
-        const double tl = sc * bt[c][i - 1];
-        const double2 q = P[(i - 1) * kSilMaxM + j];
-        re += tl * q.y;
-        im -= tl * q.x;
-      }
-      if (i + 1 < m) {
-        const double tu = sc * bt[c][i];
-        const double2 q = P[(i + 1) * kSilMaxM + j];
-        re += tu * q.y;
-        im -= tu * q.x;
-      }
-      ks.X[cur ^ 1][c][i * kSilMaxM + j] = make_double2((i == j ? 1.0 : 0.0) + re * rk, im * rk);
-    }
-    __syncthreads();
-    cur ^= 1;
-  }
-  // squaring back; the defect form also needs Z^2 of chain 0
-  int cc[2] = {cur, cur};
-  const int nsq = max(s_sq[0], s_sq[1]) + (quirk ? 1 : 0);
-  for (int q = 0; q < nsq; ++q) {
-    for (int e = t; e < 2 * kMM; e += blockDim.x) {
-      const int c = e / kMM, i = (e % kMM) / kSilMaxM, j = e % kSilMaxM;
-      if (i >= m || j >= m) continue;
-      if (q > s_sq[c] || (q == s_sq[c] && !(quirk && c == 0))) continue;
-      const double2* P = ks.X[cc[c]][c];
-      double re = 0.0, im = 0.0;
-      for (int l = 0; l < m; ++l) {
-        const double2 x = P[i * kSilMaxM + l], z = P[l * kSilMaxM + j];
-        re += x.x * z.x - x.y * z.y;
-        im += x.x * z.y + x.y * z.x;
-      }
-      ks.X[cc[c] ^ 1][c][i * kSilMaxM + j] = make_double2(re, im);
-    }
-    __syncthreads();
-    for (int c = 0; c < 2; ++c)
-      if (q < s_sq[c]) cc[c] ^= 1;
-  }
-  // coefficients: Z = X[cc[c]][c]; Z^2 of chain 0 in the other buffer
-  if (t < 2 * kSilMaxM) {
-    const int c = t / kSilMaxM, i = t % kSilMaxM;
-    if (i < m) {
-      const double2* Z = ks.X[cc[c]][c];
-      const double2* Z2 = ks.X[cc[0] ^ 1][0];
-      double re = 0.0, im = 0.0, im2 = 0.0;
-      if (active[c]) {
-        for (int j = 0; j < m; ++j) {
-          const double2 z = Z[i * kSilMaxM + j];
-          re += z.x * y[c][j];
-          im += z.y * y[c][j];
-          if (quirk && c == 0) im2 += Z2[i * kSilMaxM + j].y * y[c][j];
-        }
-      }
-      if (c == 0) {
-        out[0][i] = re;
-        out[1][i] = quirk ? 0.5 * im2 : im;
+  // warp 0: chain u, warp 1: chain v, warp 2: chain u over 2 cst (defect form)
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (w < 2 || (w == 2 && quirk)) {
+    const int c = w == 1 ? 1 : 0;
+    const double tau = w == 2 ? 2.0 * cst : cst;
+    double2 z = make_double2(0.0, 0.0);
+    if (active[c]) z = expm_tridiag_apply(m, tau, al[c], bt[c], y[c], ks.J[w]);
+    if (lane < m) {
+      if (w == 0) {
+        out[0][lane] = z.x;
+        if (!quirk) out[1][lane] = z.y;
+      } else if (w == 1) {
+        out[2][lane] = z.x;
+        out[3][lane] = -z.y;
       } else {
-        out[2][i] = re;
-        out[3][i] = -im;
+        out[1][lane] = 0.5 * z.y;
       }
     }
   }
@@ -312,33 +332,138 @@ __device__ void krylov_coeffs(int m, double cst, int quirk, const double (*al)[k
 
 }  // namespace
 
-// per-chain slots of the dot products of one Lanczos iteration:
-// [al_raw, proj, g_it, d_0..d_{it-1}, g_0..g_{it-1}]
-__device__ __forceinline__ int slot_of(int c, int it, int i) { return c * (3 + 2 * it) + i; }
+// per-chain slots of the partial sums of Lanczos iteration it:
+//   it = 0: [<vi,H vi>, <vi,x>, <vi,vi>]
+//   it > 0, res = the residual of iteration it-1 (unnormalised), vp = that
+//   iteration's vector: [<res,H res>, <res,x>, <res,res>, <H res,L_q> (q < it),
+//   <res,L_q> (q < it), <vp,L_q> (q < it)]
+__device__ __forceinline__ int nslots(int it) { return 3 + 3 * it; }
+__device__ __forceinline__ int slot_of(int c, int it, int i) { return c * nslots(it) + i; }
 
-// warp sums of acc[0..3+2it) into ws[warp][slot]
-__device__ __forceinline__ void warp_sums(const double (&acc)[3 + 2 * kSilMaxM], int c, int it,
-                                          double* ws) {
+// warp sum of x into ws[warp][slot] (called by the whole CTA alike)
+__device__ __forceinline__ void warp_put(double x, int slot, double* ws) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
-  for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) {
-    const bool valid = i < 3 || (i < 3 + kSilMaxM ? i - 3 < it : i - 3 - kSilMaxM < it);
-    if (!valid) continue;  // uniform over the CTA
-    double s = acc[i];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    const int slot = i < 3 ? i : (i < 3 + kSilMaxM ? i : i - kSilMaxM + it);
-    if (lane == 0) ws[warp * kSilNQ + slot_of(c, it, slot)] = s;
-  }
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+  if (lane == 0) ws[warp * kSilNQ + slot] = x;
 }
 
-template <int NDIM>
+// Warp reduce-scatter of V values per lane (V = 16 or 32): returns, in lane
+// l, the warp's sum of value l (V = 32) or of value l & 15 (V = 16).  Each
+// round sends half of the values still held to the partner lane and keeps
+// the other half: V - 1 shuffles in all, against five per value for
+// one-value-at-a-time sums.
+template <int V>
+__device__ __forceinline__ double warp_scatter(double (&x)[V]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int half = V / 2; half >= 1; half >>= 1) {
+    const bool up = (lane & half) != 0;
+#pragma unroll
+    for (int j = 0; j < half; ++j) {
+      const double give = up ? x[j] : x[j + half];
+      const double keep = up ? x[j + half] : x[j];
+      x[j] = keep + __shfl_xor_sync(0xffffffffu, give, half);
+    }
+  }
+  double r = x[0];
+  if (V == 16) r += __shfl_xor_sync(0xffffffffu, r, 16);
+  return r;
+}
+
+// Neighbour handshake of a pass whose results other CTAs' stencils read:
+// after this CTA's writes it publishes epoch ep in its flag (a release after
+// bar.sync, as in grid_reduce), then waits until every CTA owning a point
+// within `reach` of its own range has published ep (acquire loads; flags are
+// zeroed before the launch and grow by one per handshake, and no CTA can be a
+// whole handshake ahead: the grid reduction between two handshakes waits for
+// all).  false = a wait gave up (error flag set).
+__device__ bool halo_sync(const SilArgs& a, Range r, long reach, unsigned ep) {
+  const int b = blockIdx.x, G = gridDim.x, t = threadIdx.x;
+  __syncthreads();
+  if (t == 0) {
+    cuda::atomic_ref<unsigned, cuda::thread_scope_device> f(a.nflag[b]);
+    f.store(ep, cuda::memory_order_release);
+  }
+  bool ok = true;
+  if (r.lo < r.hi) {
+    const long chunk = (a.n + G - 1) / G;
+    const long lo = r.lo - reach > 0 ? r.lo - reach : 0;
+    const long hi = r.hi - 1 + reach < a.n - 1 ? r.hi - 1 + reach : a.n - 1;
+    const int first = (int)(lo / chunk), last = (int)(hi / chunk);
+    cuda::atomic_ref<int, cuda::thread_scope_device> err(*a.err);
+    for (int j = first + t; j <= last && ok; j += blockDim.x) {
+      if (j == b) continue;
+      cuda::atomic_ref<unsigned, cuda::thread_scope_device> f(a.nflag[j]);
+      long spins = 0;
+      while (f.load(cuda::memory_order_acquire) < ep) {
+        if (++spins > a.spin_limit || err.load(cuda::memory_order_relaxed) != 0) {
+          err.store(1, cuda::memory_order_relaxed);
+          ok = false;
+          break;
+        }
+        if (spins > 4096) __nanosleep(32);
+      }
+    }
+  }
+  return __syncthreads_and(ok) != 0;
+}
+
+// Where a step's Lanczos vectors, its H residual and the CTA's copy of its
+// residual live.  All three are read at the CTA's own points only, so with
+// kS they stay in the CTA's shared memory ([2][m][chunk] vectors, [2][chunk]
+// H residual, [2][chunk] residual; kl = point - first point of the CTA) and
+// the vectors reach global memory in the launch's last step only (the
+// drop-ins return that basis).  The residual is also written to global
+// memory: the neighbouring CTAs' stencils read it there.
+template <bool kS>
+struct SilVecs {
+  double* L;   // global [2][m][n]
+  double* wb;  // global [2][n]
+  double* wk;  // global [2][n]
+  double* sm;  // shared (kS)
+  long n;
+  int m, chunk;
+  __device__ __forceinline__ double l(int c, int q, int k, int kl) const {
+    if constexpr (kS) return sm[((long)c * m + q) * chunk + kl];
+    else return ld_state(L + ((long)c * m + q) * n + k);
+  }
+  __device__ __forceinline__ void set_l(int c, int q, int k, int kl, double v) const {
+    if constexpr (kS) sm[((long)c * m + q) * chunk + kl] = v;
+    else L[((long)c * m + q) * n + k] = v;
+  }
+  __device__ __forceinline__ double w(int c, int k, int kl) const {
+    if constexpr (kS) return sm[(long)(2 * m + c) * chunk + kl];
+    else return ld_state(wb + (long)c * n + k);
+  }
+  __device__ __forceinline__ void set_w(int c, int k, int kl, double v) const {
+    if constexpr (kS) sm[(long)(2 * m + c) * chunk + kl] = v;
+    else wb[(long)c * n + k] = v;
+  }
+  __device__ __forceinline__ double res(int c, int k, int kl) const {
+    if constexpr (kS) return sm[(long)(2 * m + 2 + c) * chunk + kl];
+    else return ld_state(wk + (long)c * n + k);
+  }
+  __device__ __forceinline__ void set_res(int c, int k, int kl, double v) const {
+    if constexpr (kS) sm[(long)(2 * m + 2 + c) * chunk + kl] = v;
+    wk[(long)c * n + k] = v;
+  }
+};
+
+// dynamic shared memory of the kS form for m vectors and chunk points per CTA
+__host__ __device__ constexpr size_t sil_vec_smem(int m, long chunk) {
+  return (size_t)(2 * m + 4) * (size_t)chunk * sizeof(double);
+}
+
+template <int NDIM, bool kS>
 __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
+  extern __shared__ double sil_dyn[];
   __shared__ double sp[kSilNQ], st[kSilNQ], scratch[(kSilThreads / 32) * 8];
   __shared__ double ws[(kSilThreads / 32) * kSilNQ];
   __shared__ double s_red[kSilThreads];
   __shared__ int s_flag[2];
   __shared__ double s_al[2][kSilMaxM], s_bt[2][kSilMaxM], s_proj[2][kSilMaxM];
+  __shared__ double s_rbt[2][kSilMaxM];  // 1/bt, the scale of the next vector
   __shared__ double s_r[2][kSilMaxM], s_coef[4][kSilMaxM];
   __shared__ double s_bt0[2];
   __shared__ int s_active[2];
@@ -347,8 +472,19 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   const int t = threadIdx.x;
   const long n = a.n;
   const int m = a.m;
+  SilVecs<kS> vs;
+  vs.L = a.L;
+  vs.wb = a.wbuf;
+  vs.wk = a.work;
+  vs.sm = sil_dyn;
+  vs.n = n;
+  vs.m = m;
+  vs.chunk = (int)((n + gridDim.x - 1) / gridDim.x);
   unsigned phase = 0;  // grid barriers passed in this launch
+  unsigned hep = 0;    // neighbour handshakes passed in this launch
   constexpr int NW = kSilThreads / 32;
+  // farthest point the 4th-order stencil reads: two lines of the slowest axis
+  const long reach = 2L * (NDIM == 1 ? 1L : NDIM == 2 ? (long)a.nx : (long)a.nx * a.ny);
 
   // this thread's sums for the norms of u, v and C of the state it wrote last
   // (the expansion below accumulates them for the next step, in the same
@@ -387,75 +523,176 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
     // potential of this step with a pulse (pplnz.f:139-141): V - DM EF(T) of
     // the time the step lands at
     const double efs = a.dm ? a.ef[a.slot0 + s + 1] : 0.0;
-    // ---- m Lanczos iterations of both chains
+    // ---- m Lanczos iterations of both chains, one grid-wide reduction each
     for (int it = 0; it < m; ++it) {
-      // vi = work/bt0, w = H vi - bt0 v_prev at the CTA's points, and the dot
-      // products of the iteration accumulated per thread
-      for (int c = 0; c < 2; ++c) {
-        const double bt0 = s_bt0[c];
-        // vi = work * (1/bt0) here and for the stencil's neighbours alike, so
-        // the stencil sees exactly the stored vi
-        const double rb = 1.0 / bt0;
-        const bool act = s_active[c];
-        const double* x = c ? a.v : a.u;
-        const double* src = it == 0 ? x : a.work + c * n;
-        double* Lc = a.L + (long)c * m * n;
-        double acc[3 + 2 * kSilMaxM];
+      if (it == 0) {
+        // vi = x/bt0 and w = H vi at the CTA's points; <vi,w>, <vi,x>, <vi,vi>
+        for (int c = 0; c < 2; ++c) {
+          const double bt0 = s_bt0[c];
+          // vi = x * (1/bt0) here and for the stencil's neighbours alike, so
+          // the stencil sees exactly the stored vi
+          const double rb = 1.0 / bt0;
+          const double* x = c ? a.v : a.u;
+          double acc[3] = {0.0, 0.0, 0.0};
+          if (s_active[c]) {
+            auto point = [&](int k, double& vi_out, double& w_out) __attribute__((always_inline)) {
+              const double xk = ld_state(x + k);
+              const double vi = xk * rb;
+              int idx[3];
+              grid_index<NDIM>(a, k, idx);
+              double hv = apply_h_nd<NDIM>(a, x, k, rb, idx);
+              if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
+              vi_out = vi;
+              w_out = hv;  // no previous vector: w = H vi
+              acc[0] += vi * hv;
+              acc[1] += vi * xk;
+              acc[2] += vi * vi;
+            };
+            int k0 = r.lo + t;
+            for (; k0 + kSilThreads < r.hi; k0 += 2 * kSilThreads) {
+              double vi0, w0, vi1, w1;
+              point(k0, vi0, w0);
+              point(k0 + kSilThreads, vi1, w1);
+              vs.set_l(c, 0, k0, k0 - r.lo, vi0);
+              vs.set_w(c, k0, k0 - r.lo, w0);
+              vs.set_l(c, 0, k0 + kSilThreads, k0 + kSilThreads - r.lo, vi1);
+              vs.set_w(c, k0 + kSilThreads, k0 + kSilThreads - r.lo, w1);
+            }
+            for (; k0 < r.hi; k0 += kSilThreads) {
+              double vi0, w0;
+              point(k0, vi0, w0);
+              vs.set_l(c, 0, k0, k0 - r.lo, vi0);
+              vs.set_w(c, k0, k0 - r.lo, w0);
+            }
+          } else {
+            for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+              vs.set_l(c, 0, k, k - r.lo, 0.0);
+              vs.set_w(c, k, k - r.lo, 0.0);
+            }
+          }
 #pragma unroll
-        for (int i = 0; i < 3 + 2 * kSilMaxM; ++i) acc[i] = 0.0;
-        if (act) {
-          // vi and w at point k, the iteration's dot products accumulated
-          auto point = [&](int k, double& vi_out, double& w_out) __attribute__((always_inline)) {
+          for (int i = 0; i < 3; ++i) warp_put(acc[i], slot_of(c, 0, i), ws);
+        }
+      } else {
+        // pass 1: the residual of iteration p = it - 1 at the CTA's points
+        // (lnz.f / reort.f: work = w - al vi - sum_q r_q L_q); vi_p and w_p
+        // from the previous pass's unnormalised residual and H residual:
+        // vi_p = res * (1/bt), w_p = (H res) * (1/bt) - bt vi_{p-1}
+        const int p = it - 1;
+        // per chain: [0] <res,res>, [1 + q] <vi_p, L_q> (q <= p <= 14)
+        double acc1[2][16];
+#pragma unroll
+        for (int c = 0; c < 2; ++c)
+#pragma unroll
+          for (int i = 0; i < 16; ++i) acc1[c][i] = 0.0;
+        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+          const int kl = k - r.lo;
+#pragma unroll
+          for (int c = 0; c < 2; ++c) {
+            if (!s_active[c]) {
+              if (p >= 1) vs.set_l(c, p, k, kl, 0.0);
+              vs.set_res(c, k, kl, 0.0);
+              continue;
+            }
             double lq[kSilMaxM];
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? ld_state(Lc + (long)q * n + k) : 0.0;
-            const double vi = ld_state(src + k) * rb;
-            const double vprev = it ? ld_state(Lc + (long)(it - 1) * n + k) : 0.0;
-            int idx[3];
-            grid_index<NDIM>(a, k, idx);
-            double hv = apply_h_nd<NDIM>(a, src, k, rb, idx);
-            if (a.dm) hv -= __ldg(a.dm + k) * efs * vi;
-            const double w = hv - bt0 * vprev;
-            const double xk = ld_state(x + k);
-            vi_out = vi;
-            w_out = w;
-            acc[0] += vi * w;
-            acc[1] += vi * xk;
-            acc[2] += vi * vi;
+            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < p ? vs.l(c, q, k, kl) : 0.0;
+            double vi, w;
+            if (p == 0) {
+              vi = vs.l(c, 0, k, kl);
+              w = vs.w(c, k, kl);
+            } else {
+              const double bp = s_bt[c][p - 1];
+              const double rbp = s_rbt[c][p - 1];
+              double vprev = 0.0;
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q) {
-              acc[3 + q] += w * lq[q];
-              acc[3 + kSilMaxM + q] += vi * lq[q];
+              for (int q = 0; q < kSilMaxM; ++q)
+                if (q == p - 1) vprev = lq[q];
+              vi = vs.res(c, k, kl) * rbp;
+              w = vs.w(c, k, kl) * rbp - bp * vprev;
+              vs.set_l(c, p, k, kl, vi);
             }
-          };
-          // two points per thread at a time with no branch between them and
-          // the stores after both, so their loads are in flight together
-          int k0 = r.lo + t;
-          for (; k0 + kSilThreads < r.hi; k0 += 2 * kSilThreads) {
-            double vi0, w0, vi1, w1;
-            point(k0, vi0, w0);
-            point(k0 + kSilThreads, vi1, w1);
-            Lc[(long)it * n + k0] = vi0;
-            a.wbuf[c * n + k0] = w0;
-            Lc[(long)it * n + k0 + kSilThreads] = vi1;
-            a.wbuf[c * n + k0 + kSilThreads] = w1;
-          }
-          for (; k0 < r.hi; k0 += kSilThreads) {
-            double vi0, w0;
-            point(k0, vi0, w0);
-            Lc[(long)it * n + k0] = vi0;
-            a.wbuf[c * n + k0] = w0;
-          }
-        } else {
-          for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-            Lc[(long)it * n + k] = 0.0;
-            a.wbuf[c * n + k] = 0.0;
+            double res = w - s_al[c][p] * vi;
+#pragma unroll
+            for (int q = 0; q < kSilMaxM; ++q)
+              if (q < p) res -= s_r[c][q] * lq[q];
+            res -= s_r[c][p] * vi;
+            vs.set_res(c, k, kl, res);
+            acc1[c][0] += res * res;
+#pragma unroll
+            for (int q = 0; q < 15; ++q) {
+              if (q < p) acc1[c][1 + q] += vi * lq[q];
+              if (q == p) acc1[c][1 + q] += vi * vi;
+            }
           }
         }
-        warp_sums(acc, c, it, ws);
+#pragma unroll
+        for (int c = 0; c < 2; ++c) {
+          const double v = warp_scatter<16>(acc1[c]);
+          const int lane = t & 31, i = lane;
+          if (i == 0) ws[(t >> 5) * kSilNQ + slot_of(c, it, 2)] = v;
+          else if (i <= it) ws[(t >> 5) * kSilNQ + slot_of(c, it, 3 + 2 * it + i - 1)] = v;
+        }
+        // the residual at the points this CTA's stencil reaches is written
+        if (!halo_sync(a, r, reach, ++hep)) return;
+        // pass 2: H res at the CTA's points and the unnormalised dot products
+        // of iteration it: <res,H res>, <res,x>, <H res,L_q>, <res,L_q>
+        for (int c = 0; c < 2; ++c) {
+          const double* x = c ? a.v : a.u;
+          const double* rc = a.work + (long)c * n;
+          // [0] <res,H res>, [1] <res,x>, [2 + q] <H res,L_q>, [17 + q] <res,L_q>
+          // (q < it <= 15)
+          double acc[32];
+#pragma unroll
+          for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+          if (s_active[c]) {
+            auto point = [&](int k, double& h_out) __attribute__((always_inline)) {
+              const int kl = k - r.lo;
+              double lq[kSilMaxM];
+#pragma unroll
+              for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? vs.l(c, q, k, kl) : 0.0;
+              const double rk = vs.res(c, k, kl);
+              int idx[3];
+              grid_index<NDIM>(a, k, idx);
+              double hr = apply_h_nd<NDIM>(a, rc, k, 1.0, idx);
+              if (a.dm) hr -= __ldg(a.dm + k) * efs * rk;
+              const double xk = ld_state(x + k);
+              h_out = hr;
+              acc[0] += rk * hr;
+              acc[1] += rk * xk;
+#pragma unroll
+              for (int q = 0; q < 15; ++q) {
+                if (q < it) {
+                  acc[2 + q] += hr * lq[q];
+                  acc[17 + q] += rk * lq[q];
+                }
+              }
+            };
+            int k0 = r.lo + t;
+            for (; k0 + kSilThreads < r.hi; k0 += 2 * kSilThreads) {
+              double h0, h1;
+              point(k0, h0);
+              point(k0 + kSilThreads, h1);
+              vs.set_w(c, k0, k0 - r.lo, h0);
+              vs.set_w(c, k0 + kSilThreads, k0 + kSilThreads - r.lo, h1);
+            }
+            for (; k0 < r.hi; k0 += kSilThreads) {
+              double h0;
+              point(k0, h0);
+              vs.set_w(c, k0, k0 - r.lo, h0);
+            }
+          }
+          const double v = warp_scatter<32>(acc);
+          const int i = t & 31;
+          int slot = -1;
+          if (i < 2) slot = slot_of(c, it, i);
+          else if (i < 17) slot = i - 2 < it ? slot_of(c, it, 3 + i - 2) : -1;
+          else slot = i - 17 < it ? slot_of(c, it, 3 + it + i - 17) : -1;
+          if (slot >= 0) ws[(t >> 5) * kSilNQ + slot] = v;
+        }
       }
       __syncthreads();
-      const int nq = 2 * (3 + 2 * it);
+      const int nq = 2 * nslots(it);
       for (int q = t; q < nq; q += kSilThreads) {
         double sum = 0.0;
         for (int w = 0; w < NW; ++w) sum += ws[w * kSilNQ + q];
@@ -465,63 +702,70 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
       if (!grid_reduce(a, sp, st, nq, s_flag, s_red, phase)) return;
       if (t < 2) {
         const int c = t, b0 = slot_of(c, it, 0);
-        const double al = st[b0];
-        s_al[c][it] = al;
-        s_proj[c][it] = st[b0 + 1];
-        // reort.f against the it+1 stored vectors: r_q = <w - al vi, L_q>
-        for (int q = 0; q < it; ++q) s_r[c][q] = st[b0 + 3 + q] - al * st[b0 + 3 + it + q];
-        s_r[c][it] = al - al * st[b0 + 2];
-      }
-      __syncthreads();
-      if (it == m - 1) break;  // the last residual is not needed (BT(M) unused)
-      // both chains at each point: their loads are in flight together
-      double nn[2] = {0.0, 0.0};
-      for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-        double res[2];
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          const double al = s_al[c][it];
-          const double* Lc = a.L + (long)c * m * n;
-          double lq[kSilMaxM + 1];
-#pragma unroll
-          for (int q = 0; q <= kSilMaxM; ++q) lq[q] = q <= it ? ld_state(Lc + (long)q * n + k) : 0.0;
-          double acc = ld_state(a.wbuf + c * n + k);
-          double vi = 0.0;
-#pragma unroll
-          for (int q = 0; q <= kSilMaxM; ++q)
-            if (q == it) vi = lq[q];
-          acc -= al * vi;
-#pragma unroll
-          for (int q = 0; q <= kSilMaxM; ++q)
-            if (q <= it) acc -= s_r[c][q] * lq[q];
-          res[c] = acc;
+        if (!s_active[c]) {
+          s_al[c][it] = s_proj[c][it] = 0.0;
+          if (it > 0) s_bt[c][it - 1] = 0.0;
+          for (int q = 0; q <= it; ++q) s_r[c][q] = 0.0;
+        } else if (it == 0) {
+          const double al = st[b0];
+          s_al[c][0] = al;
+          s_proj[c][0] = st[b0 + 1];
+          s_r[c][0] = al - al * st[b0 + 2];  // reort.f against vi itself
+        } else {
+          // bt = |res| of iteration it-1 (lnz.f:113); vi = res/bt and
+          // w = H res/bt - bt vi_{it-1}, so al = <res,H res>/bt^2 -
+          // <res,vi_{it-1}>, <w,L_q> = <H res,L_q>/bt - bt <vi_{it-1},L_q>,
+          // <vi,L_q> = <res,L_q>/bt
+          const double bt = sqrt(st[b0 + 2]);
+          const double rb = 1.0 / bt;
+          s_bt[c][it - 1] = bt;
+          s_rbt[c][it - 1] = rb;
+          const double al = st[b0] * rb * rb - st[b0 + 3 + it + (it - 1)];
+          s_al[c][it] = al;
+          s_proj[c][it] = st[b0 + 1] * rb;
+          for (int q = 0; q < it; ++q) {
+            const double wl = st[b0 + 3 + q] * rb - bt * st[b0 + 3 + 2 * it + q];
+            s_r[c][q] = wl - al * (st[b0 + 3 + it + q] * rb);
+          }
+          s_r[c][it] = al - al * (st[b0 + 2] * rb * rb);
         }
-#pragma unroll
-        for (int c = 0; c < 2; ++c) {
-          a.work[c * n + k] = res[c];
-          nn[c] += res[c] * res[c];
-        }
-      }
-      block_sum<2>(nn, sp, scratch);
-      if (!grid_reduce(a, sp, st, 2, s_flag, s_red, phase)) return;
-      if (t < 2) {
-        s_bt[t][it] = sqrt(st[t]);
-        s_bt0[t] = s_bt[t][it];
       }
       __syncthreads();
     }
     // ---- Krylov exponential and the new state
     krylov_coeffs(m, a.cst, a.quirk, s_al, s_bt, s_proj, s_active, ks, s_coef);
-    const double* Lu = a.L;
-    const double* Lv = a.L + (long)m * n;
+    // the last Lanczos vector is formed here: vi_{m-1} = res * (1/bt) from the
+    // residual of iteration m-2 (an inactive chain's residual is zero), and
+    // stored with the others (the drop-ins return the step's basis)
+    const int ms = m >= 2 ? m - 1 : m;  // vectors stored by the iterations
+    const double rbu = (m >= 2 && s_active[0]) ? s_rbt[0][m - 2] : 0.0;
+    const double rbv = (m >= 2 && s_active[1]) ? s_rbt[1][m - 2] : 0.0;
 #pragma unroll
     for (int i = 0; i < 6; ++i) qn[i] = 0.0;
+    // the launch's last step leaves its basis in global memory
+    const bool basis_out = kS && s == a.nsteps - 1;
     for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
+      const int kl = k - r.lo;
       double lu[kSilMaxM], lv[kSilMaxM];
 #pragma unroll
       for (int j = 0; j < kSilMaxM; ++j) {
-        lu[j] = j < m ? ld_state(Lu + (long)j * n + k) : 0.0;
-        lv[j] = j < m ? ld_state(Lv + (long)j * n + k) : 0.0;
+        lu[j] = j < ms ? vs.l(0, j, k, kl) : (j < m ? vs.res(0, k, kl) * rbu : 0.0);
+        lv[j] = j < ms ? vs.l(1, j, k, kl) : (j < m ? vs.res(1, k, kl) * rbv : 0.0);
+      }
+      if (basis_out) {
+#pragma unroll
+        for (int j = 0; j < kSilMaxM; ++j)
+          if (j < m) {
+            a.L[(long)j * n + k] = lu[j];
+            a.L[(long)(m + j) * n + k] = lv[j];
+          }
+      } else if (!kS && ms < m) {
+#pragma unroll
+        for (int j = 0; j < kSilMaxM; ++j)
+          if (j == ms) {
+            a.L[(long)j * n + k] = lu[j];
+            a.L[(long)(m + j) * n + k] = lv[j];
+          }
       }
       double ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
 #pragma unroll
@@ -857,6 +1101,7 @@ static SilArgs sil_args(const espec_grid_plan* p) {
   a.wbuf = p->d_wbuf;
   a.part = p->d_part;
   a.bar = p->d_bar;
+  a.nflag = p->d_bar + 2;
   a.err = p->d_err;
   a.spin_limit = g_wait_limit.load();
   a.c_out = p->d_c;
@@ -919,9 +1164,9 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
       psod ? (ndim == 1   ? (const void*)psod_kernel<1>
               : ndim == 2 ? (const void*)psod_kernel<2>
                           : (const void*)psod_kernel<3>)
-           : (ndim == 1   ? (const void*)sil_kernel<1>
-              : ndim == 2 ? (const void*)sil_kernel<2>
-                          : (const void*)sil_kernel<3>);
+           : (ndim == 1   ? (const void*)sil_kernel<1, false>
+              : ndim == 2 ? (const void*)sil_kernel<2, false>
+                          : (const void*)sil_kernel<3, false>);
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSilThreads, 0);
@@ -967,9 +1212,12 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
     return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_epart, sizeof(double) * 2 * 1024), "cudaMalloc"))) return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_eout, sizeof(double) * 2), "cudaMalloc"))) return fail(rc);
-  if ((rc = ck(cudaMalloc(&p->d_bar, sizeof(unsigned) * 2), "cudaMalloc"))) return fail(rc);
+  // the 64-bit arrival count, then one handshake flag per CTA
+  if ((rc = ck(cudaMalloc(&p->d_bar, sizeof(unsigned) * (2 + p->nblocks_max)), "cudaMalloc")))
+    return fail(rc);
   if ((rc = ck(cudaMalloc(&p->d_err, sizeof(int)), "cudaMalloc"))) return fail(rc);
-  if ((rc = ck(cudaMemset(p->d_bar, 0, sizeof(unsigned) * 2), "cudaMemset"))) return fail(rc);
+  if ((rc = ck(cudaMemset(p->d_bar, 0, sizeof(unsigned) * (2 + p->nblocks_max)), "cudaMemset")))
+    return fail(rc);
   if ((rc = ck(cudaMemset(p->d_err, 0, sizeof(int)), "cudaMemset"))) return fail(rc);
   *out = p;
   return ESPEC_OK;
@@ -1015,6 +1263,7 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
   // first barrier's G arrivals, modulo 2^64) for a self-test launch
   const bool short_start = g_short_arrivals.load() > 0 && g_short_arrivals.fetch_sub(1) > 0;
   GRID_CK(cudaMemsetAsync(p->d_bar, short_start ? 0xFF : 0, sizeof(unsigned) * 2, st));
+  GRID_CK(cudaMemsetAsync(p->d_bar + 2, 0, sizeof(unsigned) * p->nblocks, st));
   GRID_CK(cudaMemsetAsync(p->d_err, 0, sizeof(int), st));
   SilArgs a = sil_args(p);
   a.nsteps = nsteps;
@@ -1050,11 +1299,25 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
   if (p->d_dm && a.slot0 + nsteps >= p->n_ef)
     return set_error(ESPEC_EINVAL, "the pulse field table ends before the run does");
   void* args[] = {&a};
-  const void* kern = p->ndim == 1   ? (const void*)sil_kernel<1>
-                     : p->ndim == 2 ? (const void*)sil_kernel<2>
-                                    : (const void*)sil_kernel<3>;
-  GRID_CK(cudaLaunchCooperativeKernel(kern, dim3(p->nblocks), dim3(kSilThreads),
-                                      args, 0, st));
+  // the CTAs' own Lanczos vectors in shared memory when they fit
+  const long chunk = (p->n + p->nblocks - 1) / p->nblocks;
+  const size_t dyn = sil_vec_smem(p->m, chunk);
+  const void* ks = p->ndim == 1   ? (const void*)sil_kernel<1, true>
+                   : p->ndim == 2 ? (const void*)sil_kernel<2, true>
+                                  : (const void*)sil_kernel<3, true>;
+  const void* kg = p->ndim == 1   ? (const void*)sil_kernel<1, false>
+                   : p->ndim == 2 ? (const void*)sil_kernel<2, false>
+                                  : (const void*)sil_kernel<3, false>;
+  int dev = 0, optin = 0;
+  cudaFuncAttributes fa{};
+  GRID_CK(cudaGetDevice(&dev));
+  GRID_CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  GRID_CK(cudaFuncGetAttributes(&fa, ks));
+  const bool in_smem = fa.sharedSizeBytes + dyn <= (size_t)optin;
+  if (in_smem)
+    GRID_CK(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn));
+  GRID_CK(cudaLaunchCooperativeKernel(in_smem ? ks : kg, dim3(p->nblocks), dim3(kSilThreads),
+                                      args, in_smem ? dyn : 0, st));
   p->slot = a.slot0 + nsteps;
   return ESPEC_OK;
 }

@@ -13,15 +13,20 @@
 //   against all stored vectors) ; bt = |work|
 // with H the 4th-order finite-difference Hamiltonian.  The two dot-product
 // rounds of an iteration are merged into one (<w - al vi, L_q> = <w,L_q> -
-// al <vi,L_q>), so an iteration costs two grid barriers.  Each barrier is
-// also the reduction: after it every CTA sums the per-CTA partials itself in
-// one fixed order, so all CTAs hold the same (deterministic) totals.
+// al <vi,L_q>), and the residual's norm joins the next iteration's dot
+// products: the residual is formed pointwise, H is applied to it
+// unnormalised (H is linear) after a handshake with the neighbouring CTAs
+// only, and the one reduction yields bt = |res| together with the next
+// iteration's products, rescaled by 1/bt.  An iteration costs one grid
+// barrier.  Each barrier is also the reduction: after it every CTA sums the
+// per-CTA partials itself in one fixed order, so all CTAs hold the same
+// (deterministic) totals.
 //
 // The Krylov exponential e^{-i cst T} of the m x m tridiagonal T is formed by
 // every CTA (same inputs, same result) by Taylor series with scaling and
 // squaring in FP64 -- the same matrix function the reference forms through
 // the eigenvectors of T (DSTEVX) -- and the new state is the combination of
-// the stored Lanczos vectors.
+// the Lanczos vectors (the last one formed from the residual in that pass).
 #pragma once
 #include <cuda_runtime.h>
 
@@ -29,7 +34,7 @@ namespace espec {
 
 constexpr int kSilMaxM = 16;      // Lanczos order limit
 constexpr int kSilThreads = 256;  // threads per CTA
-constexpr int kSilNQ = 80;        // partial sums per CTA and barrier (>= 2 (3 + 2 (m-1)))
+constexpr int kSilNQ = 96;        // partial sums per CTA and barrier (>= 2 (3 + 3 (m-1)))
 
 struct SilArgs {
   int ndim, nx, ny, nz;
@@ -48,6 +53,7 @@ struct SilArgs {
   double* wbuf;  // [2][n]
   double* part;  // [2][gridDim.x][kSilNQ]: partial sums, by barrier parity
   unsigned* bar;  // [0..1]: one 64-bit count of the grid barrier arrivals of the launch
+  unsigned* nflag;  // [gridDim.x]: neighbour handshake epoch of each CTA (zeroed per launch)
   int* err;       // set when a barrier wait gave up
   long spin_limit;  // polls before a barrier wait gives up
   double2* c_out;  // C(t) of every step: slot s for step s (slot 0 only if write_c0)
