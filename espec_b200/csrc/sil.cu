@@ -49,6 +49,7 @@ __device__ __forceinline__ double ld_state(const double* p) { return *p; }
 // every thread of every CTA): a CTA runs at most one barrier ahead of the
 // slowest, which can still be reading the other buffer.  false = a wait
 // gave up.
+template <int kInFlight = 16>
 __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int nq,
                             int* s_flag, double* s_red /* kSilThreads doubles */,
                             unsigned& phase) {
@@ -85,27 +86,23 @@ __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int 
   __syncthreads();
   if (!s_flag[1]) return false;
   // R threads per quantity, each summing every R-th CTA in CTA order with up
-  // to 16 loads in flight, then the R partial sums in order
+  // to kInFlight loads in flight (48: one round of L2 latency for 128 CTAs
+  // and up to 96 quantities), then the R partial sums in order
   double* red = s_red;
   const int R = nq > 0 ? min(kSilThreads / nq, 32) : 1;
   if (t < R * nq) {
     const int q = t % nq, r = t / nq;
-    double acc[16];
+    double s = 0.0;
+    for (int i0 = r; i0 < G; i0 += kInFlight * R) {
+      double x[kInFlight];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-    for (int i0 = r; i0 < G; i0 += 16 * R) {
-      double x[16];
-#pragma unroll
-      for (int j = 0; j < 16; ++j) {
+      for (int j = 0; j < kInFlight; ++j) {
         const int i = i0 + j * R;
         x[j] = i < G ? __ldcg(part + (long)i * kSilNQ + q) : 0.0;
       }
 #pragma unroll
-      for (int j = 0; j < 16; ++j) acc[j] += x[j];
+      for (int j = 0; j < kInFlight; ++j) s += x[j];
     }
-    double s = 0.0;
-#pragma unroll
-    for (int j = 0; j < 16; ++j) s += acc[j];
     red[r * nq + q] = s;
   }
   __syncthreads();
@@ -238,13 +235,14 @@ __device__ double2 expm_tridiag_apply(int m, double tau, const double* al, const
     const int K = min((int)(1.5 * zp) + 25, kChebMax);
     const double sgn = tau < 0.0 ? -1.0 : 1.0;       // J_k(-z) = (-1)^k J_k(z)
     if (lane == 0) {
-      // Miller: J_{j-1} = (2j/z) J_j - J_{j+1} downward from a start well
-      // above K, normalised by J_0 + 2 sum_k J_2k = 1
-      const int nstart = 2 * ((K + 30 + (int)sqrt(40.0 * K)) / 2);
+      // Miller: J_{j-1} = (2j/z) J_j - J_{j+1} downward from a start 20
+      // orders above K (J_K is already below 1e-17 of J_0 there), normalised
+      // by J_0 + 2 sum_k J_2k = 1
+      const int nstart = 2 * ((K + 21) / 2);
       const double tz = 2.0 / zp;
-      double bjp = 0.0, bj = 1e-280, sum = 0.0;
-      for (int j = nstart; j > 0; --j) {
-        const double bjm = j * tz * bj - bjp;
+      double bjp = 0.0, bj = 1e-280, sum = 0.0, jd = nstart;
+      for (int j = nstart; j > 0; --j, jd -= 1.0) {
+        const double bjm = fma(jd * tz, bj, -bjp);
         bjp = bj;
         bj = bjm;
         if (fabs(bj) > 1e200) {
@@ -510,7 +508,7 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         for (int i = 0; i < 6; ++i) q[i] = qn[i];
       }
       block_sum<6>(q, sp, scratch);
-      if (!grid_reduce(a, sp, st, 6, s_flag, s_red, phase)) return;
+      if (!grid_reduce<48>(a, sp, st, 6, s_flag, s_red, phase)) return;
       if (t == 0 && blockIdx.x == 0 && (s > 0 || a.write_c0))
         a.c_out[s] = make_double2(st[2] + st[3], st[4] - st[5]);
       if (s == a.nsteps) break;
@@ -585,46 +583,63 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         for (int c = 0; c < 2; ++c)
 #pragma unroll
           for (int i = 0; i < 16; ++i) acc1[c][i] = 0.0;
-        for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
-          const int kl = k - r.lo;
+        // two points x two chains per thread at a time, the Gram-Schmidt
+        // sum of each as its own chain of operations (q outermost), so that
+        // the four interleave
+        for (int k0 = r.lo + t; k0 < r.hi; k0 += 2 * kSilThreads) {
+          const int kk[2] = {k0, k0 + kSilThreads};
+          bool on[2][2];
+          double vi[2][2], res[2][2];
 #pragma unroll
-          for (int c = 0; c < 2; ++c) {
-            if (!s_active[c]) {
-              if (p >= 1) vs.set_l(c, p, k, kl, 0.0);
-              vs.set_res(c, k, kl, 0.0);
-              continue;
+          for (int pt = 0; pt < 2; ++pt)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int k = kk[pt], kl = k - r.lo;
+              on[pt][c] = k < r.hi && s_active[c];
+              vi[pt][c] = res[pt][c] = 0.0;
+              if (on[pt][c]) {
+                double w;
+                if (p == 0) {
+                  vi[pt][c] = vs.l(c, 0, k, kl);
+                  w = vs.w(c, k, kl);
+                } else {
+                  const double bp = s_bt[c][p - 1], rbp = s_rbt[c][p - 1];
+                  vi[pt][c] = vs.res(c, k, kl) * rbp;
+                  w = vs.w(c, k, kl) * rbp - bp * vs.l(c, p - 1, k, kl);
+                }
+                res[pt][c] = w - s_al[c][p] * vi[pt][c];
+              }
             }
-            double lq[kSilMaxM];
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < p ? vs.l(c, q, k, kl) : 0.0;
-            double vi, w;
-            if (p == 0) {
-              vi = vs.l(c, 0, k, kl);
-              w = vs.w(c, k, kl);
-            } else {
-              const double bp = s_bt[c][p - 1];
-              const double rbp = s_rbt[c][p - 1];
-              double vprev = 0.0;
+          for (int q = 0; q < 15; ++q) {
+            if (q < p) {
 #pragma unroll
-              for (int q = 0; q < kSilMaxM; ++q)
-                if (q == p - 1) vprev = lq[q];
-              vi = vs.res(c, k, kl) * rbp;
-              w = vs.w(c, k, kl) * rbp - bp * vprev;
-              vs.set_l(c, p, k, kl, vi);
-            }
-            double res = w - s_al[c][p] * vi;
+              for (int pt = 0; pt < 2; ++pt)
 #pragma unroll
-            for (int q = 0; q < kSilMaxM; ++q)
-              if (q < p) res -= s_r[c][q] * lq[q];
-            res -= s_r[c][p] * vi;
-            vs.set_res(c, k, kl, res);
-            acc1[c][0] += res * res;
-#pragma unroll
-            for (int q = 0; q < 15; ++q) {
-              if (q < p) acc1[c][1 + q] += vi * lq[q];
-              if (q == p) acc1[c][1 + q] += vi * vi;
+                for (int c = 0; c < 2; ++c)
+                  if (on[pt][c]) {
+                    const double lq = vs.l(c, q, kk[pt], kk[pt] - r.lo);
+                    res[pt][c] -= s_r[c][q] * lq;
+                    acc1[c][1 + q] += vi[pt][c] * lq;
+                  }
             }
           }
+#pragma unroll
+          for (int pt = 0; pt < 2; ++pt)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int k = kk[pt], kl = k - r.lo;
+              if (k >= r.hi) continue;
+              if (on[pt][c]) {
+                res[pt][c] -= s_r[c][p] * vi[pt][c];
+                acc1[c][0] += res[pt][c] * res[pt][c];
+#pragma unroll
+                for (int q = 0; q < 15; ++q)
+                  if (q == p) acc1[c][1 + q] += vi[pt][c] * vi[pt][c];
+              }
+              if (p >= 1) vs.set_l(c, p, k, kl, vi[pt][c]);
+              vs.set_res(c, k, kl, res[pt][c]);
+            }
         }
 #pragma unroll
         for (int c = 0; c < 2; ++c) {
@@ -636,50 +651,62 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         // the residual at the points this CTA's stencil reaches is written
         if (!halo_sync(a, r, reach, ++hep)) return;
         // pass 2: H res at the CTA's points and the unnormalised dot products
-        // of iteration it: <res,H res>, <res,x>, <H res,L_q>, <res,L_q>
+        // of iteration it: <res,H res>, <res,x>, <H res,L_q>, <res,L_q>.
+        // First the stencils (global loads of the neighbours' residual) of
+        // two points x two chains together, H res kept with the CTA's
+        // vectors; then the products against the vectors.
+        double dd[2][2] = {{0.0, 0.0}, {0.0, 0.0}};  // [c]: <res,H res>, <res,x>
+        for (int k0 = r.lo + t; k0 < r.hi; k0 += 2 * kSilThreads) {
+          const int kk[2] = {k0, k0 + kSilThreads};
+          double hr[2][2], rk[2][2], xk[2][2];
+#pragma unroll
+          for (int pt = 0; pt < 2; ++pt)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int k = kk[pt];
+              hr[pt][c] = rk[pt][c] = xk[pt][c] = 0.0;
+              if (k < r.hi && s_active[c]) {
+                const double* rc = a.work + (long)c * n;
+                int idx[3];
+                grid_index<NDIM>(a, k, idx);
+                rk[pt][c] = vs.res(c, k, k - r.lo);
+                hr[pt][c] = apply_h_nd<NDIM>(a, rc, k, 1.0, idx);
+                if (a.dm) hr[pt][c] -= __ldg(a.dm + k) * efs * rk[pt][c];
+                xk[pt][c] = ld_state((c ? a.v : a.u) + k);
+              }
+            }
+#pragma unroll
+          for (int pt = 0; pt < 2; ++pt)
+#pragma unroll
+            for (int c = 0; c < 2; ++c) {
+              const int k = kk[pt];
+              if (k < r.hi && s_active[c]) {
+                vs.set_w(c, k, k - r.lo, hr[pt][c]);
+                dd[c][0] += rk[pt][c] * hr[pt][c];
+                dd[c][1] += rk[pt][c] * xk[pt][c];
+              }
+            }
+        }
         for (int c = 0; c < 2; ++c) {
-          const double* x = c ? a.v : a.u;
-          const double* rc = a.work + (long)c * n;
           // [0] <res,H res>, [1] <res,x>, [2 + q] <H res,L_q>, [17 + q] <res,L_q>
           // (q < it <= 15)
           double acc[32];
 #pragma unroll
           for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+          acc[0] = dd[c][0];
+          acc[1] = dd[c][1];
           if (s_active[c]) {
-            auto point = [&](int k, double& h_out) __attribute__((always_inline)) {
+            for (int k = r.lo + t; k < r.hi; k += kSilThreads) {
               const int kl = k - r.lo;
-              double lq[kSilMaxM];
-#pragma unroll
-              for (int q = 0; q < kSilMaxM; ++q) lq[q] = q < it ? vs.l(c, q, k, kl) : 0.0;
-              const double rk = vs.res(c, k, kl);
-              int idx[3];
-              grid_index<NDIM>(a, k, idx);
-              double hr = apply_h_nd<NDIM>(a, rc, k, 1.0, idx);
-              if (a.dm) hr -= __ldg(a.dm + k) * efs * rk;
-              const double xk = ld_state(x + k);
-              h_out = hr;
-              acc[0] += rk * hr;
-              acc[1] += rk * xk;
+              const double hk = vs.w(c, k, kl), rq = vs.res(c, k, kl);
 #pragma unroll
               for (int q = 0; q < 15; ++q) {
                 if (q < it) {
-                  acc[2 + q] += hr * lq[q];
-                  acc[17 + q] += rk * lq[q];
+                  const double lq = vs.l(c, q, k, kl);
+                  acc[2 + q] += hk * lq;
+                  acc[17 + q] += rq * lq;
                 }
               }
-            };
-            int k0 = r.lo + t;
-            for (; k0 + kSilThreads < r.hi; k0 += 2 * kSilThreads) {
-              double h0, h1;
-              point(k0, h0);
-              point(k0 + kSilThreads, h1);
-              vs.set_w(c, k0, k0 - r.lo, h0);
-              vs.set_w(c, k0 + kSilThreads, k0 + kSilThreads - r.lo, h1);
-            }
-            for (; k0 < r.hi; k0 += kSilThreads) {
-              double h0;
-              point(k0, h0);
-              vs.set_w(c, k0, k0 - r.lo, h0);
             }
           }
           const double v = warp_scatter<32>(acc);
@@ -699,13 +726,17 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
         sp[q] = sum;
       }
       __syncthreads();
-      if (!grid_reduce(a, sp, st, nq, s_flag, s_red, phase)) return;
-      if (t < 2) {
-        const int c = t, b0 = slot_of(c, it, 0);
+      if (!grid_reduce<48>(a, sp, st, nq, s_flag, s_red, phase)) return;
+      // the iteration's coefficients: thread (c, q) of the first two warps
+      // forms r_q of chain c; every one of them forms bt and al alike
+      if (t < 64 && (t & 31) <= it) {
+        const int c = t >> 5, q = t & 31, b0 = slot_of(c, it, 0);
         if (!s_active[c]) {
-          s_al[c][it] = s_proj[c][it] = 0.0;
-          if (it > 0) s_bt[c][it - 1] = 0.0;
-          for (int q = 0; q <= it; ++q) s_r[c][q] = 0.0;
+          s_r[c][q] = 0.0;
+          if (q == 0) {
+            s_al[c][it] = s_proj[c][it] = 0.0;
+            if (it > 0) s_bt[c][it - 1] = s_rbt[c][it - 1] = 0.0;
+          }
         } else if (it == 0) {
           const double al = st[b0];
           s_al[c][0] = al;
@@ -718,16 +749,17 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
           // <vi,L_q> = <res,L_q>/bt
           const double bt = sqrt(st[b0 + 2]);
           const double rb = 1.0 / bt;
-          s_bt[c][it - 1] = bt;
-          s_rbt[c][it - 1] = rb;
           const double al = st[b0] * rb * rb - st[b0 + 3 + it + (it - 1)];
-          s_al[c][it] = al;
-          s_proj[c][it] = st[b0 + 1] * rb;
-          for (int q = 0; q < it; ++q) {
+          if (q < it) {
             const double wl = st[b0 + 3 + q] * rb - bt * st[b0 + 3 + 2 * it + q];
             s_r[c][q] = wl - al * (st[b0 + 3 + it + q] * rb);
+          } else {
+            s_r[c][it] = al - al * (st[b0 + 2] * rb * rb);
+            s_bt[c][it - 1] = bt;
+            s_rbt[c][it - 1] = rb;
+            s_al[c][it] = al;
+            s_proj[c][it] = st[b0 + 1] * rb;
           }
-          s_r[c][it] = al - al * (st[b0 + 2] * rb * rb);
         }
       }
       __syncthreads();
