@@ -22,7 +22,7 @@ Q_DIGT_ND = 16
 Q_PSOD_COPY = 32
 PULSE_NONE, PULSE_GAUS, PULSE_GGAUS, PULSE_SIN2 = 0, 1, 2, 3
 SPO, SOD, SIL, PSOD = 0, 1, 2, 3
-MEM_HOST, MEM_DEVICE = 0, 1
+MEM_HOST, MEM_DEVICE, MEM_HOST_ASYNC = 0, 1, 2
 LAUNCH_CLASSES, LAUNCH_PERSISTENT = 0, 1
 VARIANT_TC = 5
 SHFS = 2.4188843243e-2

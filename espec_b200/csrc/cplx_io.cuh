@@ -58,10 +58,13 @@ inline int stage_reserve(HostStage& s, size_t bytes) {
 }
 
 // dst (device, n complex) <- (re, im) at `where`; im may be null (zero)
+// a user pointer in host memory (synchronous or in-flight copies)
+inline bool on_host(int where) { return where == ESPEC_MEM_HOST || where == ESPEC_MEM_HOST_ASYNC; }
+
 inline int put_complex(HostStage& s, double2* dst, const double* re, const double* im, size_t n,
                        int where, cudaStream_t st) {
   if (n == 0) return ESPEC_OK;
-  if (where == ESPEC_MEM_HOST) {
+  if (on_host(where)) {
     const int rc = stage_reserve(s, 16 * n);
     if (rc) return rc;
     IO_CK(cudaMemcpyAsync(s.d, re, 8 * n, cudaMemcpyHostToDevice, st));
@@ -78,7 +81,7 @@ inline int put_complex(HostStage& s, double2* dst, const double* re, const doubl
 inline int get_complex(HostStage& s, const double2* src, double* re, double* im, size_t n,
                        int where, cudaStream_t st) {
   if ((!re && !im) || n == 0) return ESPEC_OK;
-  if (where != ESPEC_MEM_HOST) {
+  if (!on_host(where)) {
     deinterleave_kernel<<<io_blocks(n), 256, 0, st>>>(src, re, im, n);
     IO_CK(cudaGetLastError());
     return ESPEC_OK;

@@ -677,7 +677,7 @@ extern "C" int espec_spo_load(espec_spo_plan* p, const double* vpot, const doubl
   if (p->absorb != ESPEC_ABS_NONE && !vabc) return set_error(ESPEC_EINVAL, "absorber table missing");
   cudaStream_t st = (cudaStream_t)stream;
   const size_t np = p->npts;
-  const cudaMemcpyKind kind = where == ESPEC_MEM_HOST ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+  const cudaMemcpyKind kind = on_host(where) ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
   ESPEC_CK(cudaMemcpyAsync(p->d_vpot, vpot, np * 8, kind, st));
   if (vabc) ESPEC_CK(cudaMemcpyAsync(p->d_vabc, vabc, np * 8, kind, st));
   int rc = put_complex(p->stage, p->d_psi0, psi_re, psi_im, np, where, st);

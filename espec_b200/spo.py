@@ -53,16 +53,18 @@ class SpoBatch:
         N.check(N.load().espec_spo_set_variant(self._h, int(npts), int(variant)),
                 "espec_spo_set_variant")
 
-    def load(self, vpot, psi, vabc=None, stream=None):
+    def load(self, vpot, psi, vabc=None, stream=None, asynchronous=False):
         """vpot, psi (complex or real), vabc: host numpy arrays (concatenated),
-        or device tensors (torch float64) with psi given as (re, im)."""
+        or device tensors (torch float64) with psi given as (re, im).  With
+        asynchronous=True, host (re, im) arrays must be page-locked float64
+        arrays that stay untouched until the stream has passed the copies."""
         lib = N.load()
         if isinstance(psi, tuple) and isinstance(psi[0], np.ndarray):  # host (re, im)
             self._keep = [N.f64(vpot), N.f64(psi[0]), N.f64(psi[1]),
                           None if vabc is None else N.f64(vabc)]
             v, re, im, ab = self._keep
             rc = lib.espec_spo_load(self._h, N.ptr(v), N.ptr(ab), N.ptr(re), N.ptr(im),
-                                    N.MEM_HOST, stream)
+                                    N.MEM_HOST_ASYNC if asynchronous else N.MEM_HOST, stream)
         elif isinstance(psi, tuple):  # device (re, im)
             re, im = psi
             rc = lib.espec_spo_load(self._h, N.ptr(vpot), N.ptr(vabc), N.ptr(re), N.ptr(im),
@@ -108,12 +110,15 @@ class SpoBatch:
         N.check(rc, "espec_spo_results")
         return (cr + 1j * ci).reshape(self.npk, ns + 1), pr + 1j * pi
 
-    def results_into(self, c_re, c_im, psi_re, psi_im, stream=None):
+    def results_into(self, c_re, c_im, psi_re, psi_im, stream=None, asynchronous=False):
         """Copy C(t) ([npk * (nsteps+1)], packet-major) and psi(TF) as separate
         real and imaginary float64 host arrays into the caller's buffers (any
-        may be None); returns when the copies are done."""
+        may be None); returns when the copies are done, or at once with
+        asynchronous=True (page-locked buffers; synchronise the stream before
+        reading them)."""
+        where = N.MEM_HOST_ASYNC if asynchronous else N.MEM_HOST
         N.check(N.load().espec_spo_results(self._h, N.ptr(c_re), N.ptr(c_im), N.ptr(psi_re),
-                                           N.ptr(psi_im), N.MEM_HOST, stream),
+                                           N.ptr(psi_im), where, stream),
                 "espec_spo_results")
 
     def nonfinite(self, stream=None):

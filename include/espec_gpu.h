@@ -83,6 +83,10 @@ extern "C" {
 /* memory space of user pointers */
 #define ESPEC_MEM_HOST 0
 #define ESPEC_MEM_DEVICE 1
+/* host memory (page-locked) with the copies left in flight on the stream:
+ * espec_spo_load and espec_spo_results return at once, the caller
+ * synchronises the stream before it reads or reuses the buffers */
+#define ESPEC_MEM_HOST_ASYNC 2
 
 /* launch shape of a batched split-operator run (espec_spo_set_launch) */
 #define ESPEC_LAUNCH_CLASSES 0     /* one kernel per packet size, concurrent streams */

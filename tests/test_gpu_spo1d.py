@@ -167,3 +167,38 @@ def test_every_variant_matches_oracle(oracle, variant):
         err = np.max(np.abs(c - c_ref), axis=1)
         assert np.all(err <= tol), (prec, dict(zip(n.tolist(), err.tolist())))
         assert np.max(np.abs(p - p_ref)) <= (1e-10 if prec == "fp64" else 1e-5)
+
+
+def test_async_host_copies_match_synchronous():
+    """ESPEC_MEM_HOST_ASYNC: load and results with page-locked buffers left in
+    flight on a stream give the synchronous path's results, also with two
+    plans taking alternate runs on two streams."""
+    import torch
+
+    w = W.morse_scan(npk=40, nsteps=60, seed=31)
+    npts, nc = int(w["off"][-1]), 40 * 61
+
+    def pinned(n):
+        return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+
+    vh, rh, ih = pinned(npts), pinned(npts), pinned(npts)
+    vh[:], rh[:], ih[:] = w["vpot"], w["psi"].real, w["psi"].imag
+    b = E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision="fp64")
+    b.load(vh, (rh, ih))
+    b.run(60)
+    c_ref, p_ref = b.results()
+    plans = [b, E.SpoBatch(w["n"], w["sh"], w["sm"], w["dt_fs"], precision="fp64")]
+    strs = [torch.cuda.Stream(), torch.cuda.Stream()]
+    outs = [[pinned(nc), pinned(nc), pinned(npts), pinned(npts)] for _ in range(2)]
+    for i in range(4):
+        j = i % 2
+        plans[j].load(vh, (rh, ih), stream=strs[j].cuda_stream, asynchronous=True)
+        plans[j].run(60, stream=strs[j].cuda_stream)
+        plans[j].results_into(*outs[j], stream=strs[j].cuda_stream, asynchronous=True)
+    torch.cuda.synchronize()
+    for j in range(2):
+        c = (outs[j][0] + 1j * outs[j][1]).reshape(40, 61)
+        assert np.array_equal(c, c_ref)
+        assert np.array_equal(outs[j][2] + 1j * outs[j][3], p_ref)
+    for pl in plans:
+        pl.close()
