@@ -839,10 +839,124 @@ __device__ __forceinline__ void psod_points(const SilArgs& a, Range r, const dou
                                             const double* vn, double* um, double* vm, double c,
                                             double e, double (&q)[4]);
 
+// PSOD on a 2D grid by column strips: CTA b owns columns [256 s, 256 s + 256)
+// (s = b mod nstrips) of a band of rows; each thread walks its column down the
+// band with the y-stencil's five rows of psi_n in registers, so psi_n is read
+// from memory once per band (plus two halo rows at each end), the x
+// neighbours come from the row the warp has just loaded (L1), and every other
+// array is one streaming read or write per point.
+constexpr int kBandMinRows = 16;
+
+struct Band {
+  int col, r0, r1;
+};
+
+__device__ __forceinline__ Band my_band(const SilArgs& a) {
+  const int ns = a.nstrips, nb = gridDim.x / ns;
+  const int s = blockIdx.x % ns, band = blockIdx.x / ns;
+  const int rows = (a.ny + nb - 1) / nb;
+  Band B;
+  B.col = s * kSilThreads + threadIdx.x;
+  B.r0 = min(band * rows, a.ny);
+  B.r1 = min(B.r0 + rows, a.ny);
+  return B;
+}
+
+template <int KABS, bool DM>
+__device__ __forceinline__ void psod2d_band(const SilArgs& a, const Band& B, const double* un,
+                                            const double* vn, double* um, double* vm, double c,
+                                            double e, double (&q)[4]) {
+  const int nx = a.nx, ny = a.ny, col = B.col;
+  if (col >= nx || B.r0 >= B.r1) return;
+  const double hx = a.shm[0], hy = a.shm[1];
+  // rows r-2 .. r+2 of psi_n at this column (zero off the grid)
+  double wu[5], wv[5];
+#pragma unroll
+  for (int j = 0; j < 5; ++j) {
+    const int row = B.r0 - 2 + j;
+    const bool in = row >= 0 && row < ny;
+    wu[j] = in ? ld_state(un + (long)row * nx + col) : 0.0;
+    wv[j] = in ? ld_state(vn + (long)row * nx + col) : 0.0;
+  }
+#pragma unroll 2
+  for (int r = B.r0; r < B.r1; ++r) {
+    const long k = (long)r * nx + col;
+    // x neighbours of row r, issued unconditionally (from k when off the grid)
+    const long xm2 = col >= 2 ? k - 2 : k, xm1 = col >= 1 ? k - 1 : k;
+    const long xp1 = col + 1 < nx ? k + 1 : k, xp2 = col + 2 < nx ? k + 2 : k;
+    const double um2 = ld_state(un + xm2), um1 = ld_state(un + xm1);
+    const double up1 = ld_state(un + xp1), up2 = ld_state(un + xp2);
+    const double vm2 = ld_state(vn + xm2), vm1 = ld_state(vn + xm1);
+    const double vp1 = ld_state(vn + xp1), vp2 = ld_state(vn + xp2);
+    const double vk = __ldg(a.vpot + k);
+    const double umk = um[k], vmk = vm[k];
+    const double u0k = __ldg(a.u0 + k), v0k = __ldg(a.v0 + k);
+    // the next window row
+    const int rn = r + 3;
+    const bool inn = rn < ny;
+    const double nu3 = inn ? ld_state(un + (long)rn * nx + col) : 0.0;
+    const double nv3 = inn ? ld_state(vn + (long)rn * nx + col) : 0.0;
+    // H psi_n at (col, r): au2di.f's terms in apply_h_nd's order
+    double hu = (a.sht30 + vk) * wu[2], hv = (a.sht30 + vk) * wv[2];
+    if (col >= 2) { hu += hx * um2; hv += hx * vm2; }
+    if (col >= 1) { hu += -16.0 * hx * um1; hv += -16.0 * hx * vm1; }
+    if (col + 1 < nx) { hu += -16.0 * hx * up1; hv += -16.0 * hx * vp1; }
+    if (col + 2 < nx) { hu += hx * up2; hv += hx * vp2; }
+    if (r >= 2) { hu += hy * wu[0]; hv += hy * wv[0]; }
+    if (r >= 1) { hu += -16.0 * hy * wu[1]; hv += -16.0 * hy * wv[1]; }
+    if (r + 1 < ny) { hu += -16.0 * hy * wu[3]; hv += -16.0 * hy * wv[3]; }
+    if (r + 2 < ny) { hu += hy * wu[4]; hv += hy * wv[4]; }
+    const double uk = wu[2], vkk = wv[2];
+    if (DM) {
+      const double de = __ldg(a.dm + k) * e;
+      hv -= de * vkk;
+      hu -= de * uk;
+    }
+    double nu, nv;
+    if (KABS == 1) {
+      const double w = a.vabc[k];
+      nu = umk + c * hv - c * w * uk;
+      nv = vmk - c * hu - c * w * vkk;
+    } else if (KABS == 2) {
+      const double w = a.vabc[k];
+      nu = w * (umk + c * hv);
+      nv = w * (vmk - c * hu);
+    } else {
+      nu = umk + c * hv;
+      nv = vmk - c * hu;
+    }
+    um[k] = nu;
+    vm[k] = nv;
+    q[0] += u0k * nu;
+    q[1] += v0k * nv;
+    q[2] += u0k * nv;
+    q[3] += v0k * nu;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      wu[j] = wu[j + 1];
+      wv[j] = wv[j + 1];
+    }
+    wu[4] = nu3;
+    wv[4] = nv3;
+  }
+}
+
 template <int NDIM>
 __device__ __forceinline__ void psod_dispatch(const SilArgs& a, Range r, const double* un,
                                               const double* vn, double* um, double* vm, double c,
                                               double e, double (&q)[4]) {
+  if (NDIM == 2 && a.nstrips > 0) {
+    const Band B = my_band(a);
+    switch (a.kabs + (a.dm ? 3 : 0)) {
+      case 0: psod2d_band<0, false>(a, B, un, vn, um, vm, c, e, q); break;
+      case 1: psod2d_band<1, false>(a, B, un, vn, um, vm, c, e, q); break;
+      case 2: psod2d_band<2, false>(a, B, un, vn, um, vm, c, e, q); break;
+      case 3: psod2d_band<0, true>(a, B, un, vn, um, vm, c, e, q); break;
+      case 4: psod2d_band<1, true>(a, B, un, vn, um, vm, c, e, q); break;
+      default: psod2d_band<2, true>(a, B, un, vn, um, vm, c, e, q); break;
+    }
+    return;
+  }
   switch (a.kabs + (a.dm ? 3 : 0)) {
     case 0: psod_points<0, false, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
     case 1: psod_points<1, false, NDIM>(a, r, un, vn, um, vm, c, e, q); break;
@@ -981,9 +1095,17 @@ __global__ void __launch_bounds__(kSilThreads, 2) psod_kernel(SilArgs a) {
   if (a.start && a.nsteps >= 1) {
     if (!step(0.25 * a.cst, -1, 0)) return;  // psod.f:120-121
     if (!step(0.5 * a.cst, 1, 1)) return;    // psod.f:123-124
-    for (int k = r.lo + t; k < r.hi; k += kSilThreads) {  // psod.f:136-141
+    // psod.f:136-141, over the points this CTA's steps write
+    auto copy_back = [&](long k) {
       um[k] = __ldg(a.u0 + k);
       vm[k] = (a.copy_quirk && (k & 1)) ? __ldg(a.v0 + k - 1) : __ldg(a.v0 + k);
+    };
+    if (NDIM == 2 && a.nstrips > 0) {
+      const Band B = my_band(a);
+      if (B.col < a.nx)
+        for (int row = B.r0; row < B.r1; ++row) copy_back((long)row * a.nx + B.col);
+    } else {
+      for (int k = r.lo + t; k < r.hi; k += kSilThreads) copy_back(k);
     }
     __syncthreads();
     s0 = 2;
@@ -1108,6 +1230,17 @@ static void grid_free(espec_grid_plan* p) {
 static std::atomic<long> g_wait_limit{kSpinLimit};
 static std::atomic<int> g_short_arrivals{0};
 
+// column strips of the PSOD pass on a 2D grid (0: contiguous point ranges):
+// used when the CTA count is a multiple of the strip count and every band
+// holds at least kBandMinRows rows
+static int band_strips(const espec_grid_plan* p) {
+  if (p->method != ESPEC_PSOD || p->ndim != 2) return 0;
+  const int ns = (p->np[0] + kSilThreads - 1) / kSilThreads;
+  if (p->nblocks % ns != 0) return 0;
+  const int nb = p->nblocks / ns;
+  return p->np[1] / nb >= kBandMinRows ? ns : 0;
+}
+
 static SilArgs sil_args(const espec_grid_plan* p) {
   SilArgs a{};
   a.ndim = p->ndim;
@@ -1151,6 +1284,7 @@ static SilArgs sil_args(const espec_grid_plan* p) {
   }
   a.dm = p->d_dm;
   a.ef = p->d_dm ? p->d_ef : nullptr;
+  a.nstrips = band_strips(p);
   return a;
 }
 
@@ -1219,6 +1353,12 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   if (want > cap) {
     const long per = (want + cap - 1) / cap;
     want = (want + per - 1) / per;
+  }
+  // a PSOD pass over a large 2D grid runs by column strips: every co-resident
+  // CTA, a multiple of the strip count, each band at least kBandMinRows rows
+  if (psod && ndim == 2) {
+    const long ns = (np[0] + kSilThreads - 1) / kSilThreads, nb = cap / ns;
+    if (nb >= 1 && np[1] / nb >= kBandMinRows) want = ns * nb;
   }
   p->nblocks = (int)(want > 0 ? want : 1);
   p->nblocks_max = p->nblocks;

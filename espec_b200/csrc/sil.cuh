@@ -42,6 +42,7 @@ struct SilArgs {
   double shm[3];  // 1/(24 m_a h_a^2) per axis
   double sht30;   // 30 * (shm[0] + shm[1] + shm[2])
   double inv_nx, inv_ny;  // 1/nx, 1/ny: grid indices by multiplication
+  int nstrips;  // PSOD on a 2D grid: column strips of kSilThreads (0: point ranges)
   const double* vpot;
   const double* mask;  // .SMOOTHW mask or null
   double* u;           // state (in / out)

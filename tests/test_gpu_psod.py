@@ -13,8 +13,10 @@ import golden_cases as G
 pytestmark = pytest.mark.gpu
 
 
-def gpu_psod(np_, shm, dt, v, psi, nsteps, absorb=0, vabc=None, quirks=0):
+def gpu_psod(np_, shm, dt, v, psi, nsteps, absorb=0, vabc=None, quirks=0, ctas=None):
     g = E.PsodGrid(np_, shm, dt, absorb=absorb, quirks=quirks)
+    if ctas:
+        g.set_ctas(ctas)
     g.load(v, psi, vabc=vabc)
     g.run(nsteps)
     c, out = g.results()
@@ -80,6 +82,7 @@ def test_psod_random_grids(oracle, np_, absorb, quirk):
 
 
 @pytest.mark.parametrize("np_,dt_au,absorb", [([1024, 640], 2e-4, 0), ([1024, 640], 2e-4, 1),
+                                               ([2048, 600], 2e-4, 2),
                                                ([700000], 5e-10, 2), ([100, 96, 64], 0.01, 1)])
 def test_psod_large_grids(oracle, np_, dt_au, absorb):
     """Grids of 16 or more points per thread, where the plan takes every
@@ -127,3 +130,31 @@ def test_psod_continue_and_energies(oracle):
     ref_e1 = oracle.eigenerg(np_, shm, v, p2.real) + oracle.eigenerg(np_, shm, v, p2.imag)
     assert abs(e1 - ref_e1) <= 1e-12 * abs(ref_e1)
     assert abs(n1 - np.sum(np.abs(p2) ** 2)) <= 1e-12
+
+
+@pytest.mark.parametrize("np_,ctas,absorb,quirk", [
+    ([300, 70], 4, 0, True), ([300, 70], 4, 1, False), ([512, 80], 4, 2, True),
+    ([260, 100], 6, 0, False)])
+def test_psod_column_strips(oracle, np_, ctas, absorb, quirk):
+    """The column-strip pass of 2D grids (CTA count a multiple of the strip
+    count, 16 or more rows per band), forced on small grids by the CTA count,
+    ragged last strip included: the oracle's results, the restart-copy
+    defect and the absorbers as on the point-range pass."""
+    v, psi, sh, grids = packet(np_, 17 + absorb)
+    sm = [1000.0, 1400.0]
+    shm = [G.shm_of(m, h) for m, h in zip(sm, sh)]
+    vabc = None
+    if absorb == NAT.ABS_VOPTIC:
+        vabc = -0.05 * np.clip(grids[0] - 0.3, 0, None).ravel(order="F") ** 2
+    elif absorb == NAT.ABS_SMOOTHW:
+        vabc = np.where(grids[0] > 0.35, 0.97, 1.0).ravel(order="F")
+    dt = 0.0005 * NAT.SHFS
+    q_o = oracle.Q_PSOD_COPY if quirk else 0
+    p = oracle.make_prop(np_, dt, 0.0, 40 * dt, sh, sm, lc=1, absorb=absorb, quirks=q_o,
+                         shm=shm)
+    ref = oracle.psod(p, v, np.real(psi), np.imag(psi), vabc=vabc)
+    c, out, prev = gpu_psod(np_, shm, dt, v, psi, ref["nc"] - 1, absorb=absorb, vabc=vabc,
+                            quirks=NAT.Q_PSOD_COPY if quirk else 0, ctas=ctas)
+    assert np.max(np.abs(c - ref["c"])) <= 1e-10, np.max(np.abs(c - ref["c"]))
+    assert np.max(np.abs(out - (ref["u"] + 1j * ref["v"]))) <= 1e-10
+    assert np.max(np.abs(prev - (ref["u_prev"] + 1j * ref["v_prev"]))) <= 1e-10
