@@ -15,7 +15,7 @@ state cannot hold 1e-6 over 8000 steps of this scan
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--precision fp64|mixed] [--npk 4096] [--nsteps 8000]
     python bench.py --leg c1|c2|c3|mixed|sil_2d|sil_ctas|psod_2d|grid_sweep|eig|tc256
-    python bench.py --case eig|spond2d|spond3d|spectrum|sil|gemm|tc256   (profiling)
+    python bench.py --case eig|spond2d|spond3d|spectrum|sil|gemm|tc256|psod2048   (profiling)
 
 Multi-GPU (torchrun): packets are independent, each rank propagates its own
 batch (seed + rank) with no collective on the data path -> weak scaling.
@@ -68,7 +68,8 @@ def parse():
                              "grid_sweep", "eig", "tc256"],
                     help="run one leg alone and print its JSON")
     ap.add_argument("--case", default=None,
-                    choices=["eig", "spond2d", "spond3d", "spectrum", "sil", "gemm", "tc256"],
+                    choices=["eig", "spond2d", "spond3d", "spectrum", "sil", "gemm", "tc256",
+                             "psod2048"],
                     help="small self-checking workload for profiling one kernel")
     ap.add_argument("--leg-steps", type=int, default=100)
     ap.add_argument("--eig-train", type=int, default=50000)
@@ -850,6 +851,21 @@ def profile_case(name, dev):
         psi /= np.sqrt(np.sum(np.abs(psi) ** 2))
         h = x[1] - x[0]
         g = E.SilGrid([n, n], [1 / (24 * 918 * h * h), 1 / (24 * 1500 * h * h)], SHFS, 12)
+        g.load(v.ravel(order="F"), psi.ravel(order="F"))
+        g.run(20)
+        c, _ = g.results()
+        g.close()
+        return float(np.abs(c[-1]))
+    if name == "psod2048":  # psod_kernel<2>, column strips: 2048 x 2048 coupled Morse, 20 steps
+        n = 2048
+        x = np.linspace(0.5, 8.0, n)
+        X, Y = np.meshgrid(x, x, indexing="ij")
+        v = 0.17 * (1 - np.exp(-(X - 1.4))) ** 2 + 0.12 * (1 - np.exp(-1.2 * (Y - 1.8))) ** 2
+        psi = np.exp(-((X - 1.6) ** 2 + (Y - 2.0) ** 2) / 0.045).astype(complex)
+        psi /= np.sqrt(np.sum(np.abs(psi) ** 2))
+        h = x[1] - x[0]
+        g = E.PsodGrid([n, n], [1.0 / (24.0 * 918.0 * h * h), 1.0 / (24.0 * 1500.0 * h * h)],
+                       0.002 * SHFS)
         g.load(v.ravel(order="F"), psi.ravel(order="F"))
         g.run(20)
         c, _ = g.results()

@@ -862,10 +862,14 @@ __device__ __forceinline__ Band my_band(const SilArgs& a) {
   return B;
 }
 
+// (psi_n and psi_{n-1} are distinct buffers within a step: the loads of later
+// rows may move ahead of this row's stores)
 template <int KABS, bool DM>
-__device__ __forceinline__ void psod2d_band(const SilArgs& a, const Band& B, const double* un,
-                                            const double* vn, double* um, double* vm, double c,
-                                            double e, double (&q)[4]) {
+__device__ __forceinline__ void psod2d_band(const SilArgs& a, const Band& B,
+                                            const double* __restrict__ un,
+                                            const double* __restrict__ vn,
+                                            double* __restrict__ um, double* __restrict__ vm,
+                                            double c, double e, double (&q)[4]) {
   const int nx = a.nx, ny = a.ny, col = B.col;
   if (col >= nx || B.r0 >= B.r1) return;
   const double hx = a.shm[0], hy = a.shm[1];
@@ -878,7 +882,7 @@ __device__ __forceinline__ void psod2d_band(const SilArgs& a, const Band& B, con
     wu[j] = in ? ld_state(un + (long)row * nx + col) : 0.0;
     wv[j] = in ? ld_state(vn + (long)row * nx + col) : 0.0;
   }
-#pragma unroll 2
+#pragma unroll 4
   for (int r = B.r0; r < B.r1; ++r) {
     const long k = (long)r * nx + col;
     // x neighbours of row r, issued unconditionally (from k when off the grid)
