@@ -526,6 +526,17 @@ def leg_c2(dev, nsteps=10000):
                                                    "of its passes and m + 1 grid-wide "
                                                    "reductions")}
     out["sil_vs_spo_fp64_dC_max"] = float(np.max(np.abs(c_sil - cs["fp64"])))
+    # the mixed SIL form (FP32 Lanczos vectors and H psi, FP64 dot products,
+    # coefficients, Krylov exponential and state) over the same steps
+    g = E.SilGrid([n, n], shm, dt, m, absorb=N.ABS_SMOOTHW, precision="mixed")
+    g.load(v, psi, vabc=np.exp(-wv * dt_au))
+    g.run(5)
+    ms = timed(lambda: g.run(nsteps), 1, dev)
+    c_sm, _ = g.results()
+    g.close()
+    out["sil12_mixed"] = {"value": n * n * nsteps / (ms * 1e-3) / 1e6,
+                          "us_per_step": ms * 1e3 / nsteps,
+                          "dC_vs_sil12_fp64_max": float(np.max(np.abs(c_sm - c_sil)))}
     return out
 
 

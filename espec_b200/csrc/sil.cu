@@ -162,27 +162,27 @@ __device__ __forceinline__ void grid_index(const SilArgs& a, int k, int (&idx)[3
 // grid_index.  Every neighbour load is issued unconditionally (from x_k where
 // the neighbour is off the grid) so that no branch separates a point's loads
 // from the next point's; the sums skip the off-grid terms.
-template <int NDIM>
-__device__ __forceinline__ double apply_h_nd(const SilArgs& a, const double* x, int k, double d,
-                                             const int (&idx)[3]) {
+template <int NDIM, typename T = double>
+__device__ __forceinline__ T apply_h_nd(const SilArgs& a, const T* x, int k, T d,
+                                        const int (&idx)[3]) {
   const int len[3] = {a.nx, a.ny, a.nz}, str[3] = {1, a.nx, a.nx * a.ny};
-  double xm2[NDIM], xm1[NDIM], xp1[NDIM], xp2[NDIM];
+  T xm2[NDIM], xm1[NDIM], xp1[NDIM], xp2[NDIM];
 #pragma unroll
   for (int ax = 0; ax < NDIM; ++ax) {
     const int i = idx[ax], st = str[ax], L = len[ax];
-    xm2[ax] = ld_state(x + (i >= 2 ? k - 2 * st : k));
-    xm1[ax] = ld_state(x + (i >= 1 ? k - st : k));
-    xp1[ax] = ld_state(x + (i + 1 < L ? k + st : k));
-    xp2[ax] = ld_state(x + (i + 2 < L ? k + 2 * st : k));
+    xm2[ax] = x[i >= 2 ? k - 2 * st : k];
+    xm1[ax] = x[i >= 1 ? k - st : k];
+    xp1[ax] = x[i + 1 < L ? k + st : k];
+    xp2[ax] = x[i + 2 < L ? k + 2 * st : k];
   }
-  double s = (a.sht30 + __ldg(a.vpot + k)) * (ld_state(x + k) * d);
+  T s = ((T)a.sht30 + (T)__ldg(a.vpot + k)) * (x[k] * d);
 #pragma unroll
   for (int ax = 0; ax < NDIM; ++ax) {
-    const double h = a.shm[ax];
+    const T h = (T)a.shm[ax];
     const int i = idx[ax], L = len[ax];
     if (i >= 2) s += h * (xm2[ax] * d);
-    if (i >= 1) s += -16.0 * h * (xm1[ax] * d);
-    if (i + 1 < L) s += -16.0 * h * (xp1[ax] * d);
+    if (i >= 1) s += (T)-16.0 * h * (xm1[ax] * d);
+    if (i + 1 < L) s += (T)-16.0 * h * (xp1[ax] * d);
     if (i + 2 < L) s += h * (xp2[ax] * d);
   }
   return s;
@@ -414,48 +414,53 @@ __device__ bool halo_sync(const SilArgs& a, Range r, long reach, unsigned ep) {
 // the vectors reach global memory in the launch's last step only (the
 // drop-ins return that basis).  The residual is also written to global
 // memory: the neighbouring CTAs' stencils read it there.
-template <bool kS>
+template <bool kS, typename S>
 struct SilVecs {
-  double* L;   // global [2][m][n]
-  double* wb;  // global [2][n]
-  double* wk;  // global [2][n]
-  double* sm;  // shared (kS)
+  S* L;   // global [2][m][n]
+  S* wb;  // global [2][n]
+  S* wk;  // global [2][n]
+  S* sm;  // shared (kS)
   long n;
   int m, chunk;
   __device__ __forceinline__ double l(int c, int q, int k, int kl) const {
-    if constexpr (kS) return sm[((long)c * m + q) * chunk + kl];
-    else return ld_state(L + ((long)c * m + q) * n + k);
+    if constexpr (kS) return (double)sm[((long)c * m + q) * chunk + kl];
+    else return (double)L[((long)c * m + q) * n + k];
   }
   __device__ __forceinline__ void set_l(int c, int q, int k, int kl, double v) const {
-    if constexpr (kS) sm[((long)c * m + q) * chunk + kl] = v;
-    else L[((long)c * m + q) * n + k] = v;
+    if constexpr (kS) sm[((long)c * m + q) * chunk + kl] = (S)v;
+    else L[((long)c * m + q) * n + k] = (S)v;
   }
   __device__ __forceinline__ double w(int c, int k, int kl) const {
-    if constexpr (kS) return sm[(long)(2 * m + c) * chunk + kl];
-    else return ld_state(wb + (long)c * n + k);
+    if constexpr (kS) return (double)sm[(long)(2 * m + c) * chunk + kl];
+    else return (double)wb[(long)c * n + k];
   }
   __device__ __forceinline__ void set_w(int c, int k, int kl, double v) const {
-    if constexpr (kS) sm[(long)(2 * m + c) * chunk + kl] = v;
-    else wb[(long)c * n + k] = v;
+    if constexpr (kS) sm[(long)(2 * m + c) * chunk + kl] = (S)v;
+    else wb[(long)c * n + k] = (S)v;
   }
   __device__ __forceinline__ double res(int c, int k, int kl) const {
-    if constexpr (kS) return sm[(long)(2 * m + 2 + c) * chunk + kl];
-    else return ld_state(wk + (long)c * n + k);
+    if constexpr (kS) return (double)sm[(long)(2 * m + 2 + c) * chunk + kl];
+    else return (double)wk[(long)c * n + k];
   }
   __device__ __forceinline__ void set_res(int c, int k, int kl, double v) const {
-    if constexpr (kS) sm[(long)(2 * m + 2 + c) * chunk + kl] = v;
-    wk[(long)c * n + k] = v;
+    if constexpr (kS) sm[(long)(2 * m + 2 + c) * chunk + kl] = (S)v;
+    wk[(long)c * n + k] = (S)v;
   }
 };
 
-// dynamic shared memory of the kS form for m vectors and chunk points per CTA
-__host__ __device__ constexpr size_t sil_vec_smem(int m, long chunk) {
-  return (size_t)(2 * m + 4) * (size_t)chunk * sizeof(double);
+// dynamic shared memory of the kS form for m vectors and chunk points per
+// CTA, vectors of `bytes` bytes per value
+__host__ __device__ constexpr size_t sil_vec_smem(int m, long chunk, int bytes) {
+  return (size_t)(2 * m + 4) * (size_t)chunk * (size_t)bytes;
 }
 
-template <int NDIM, bool kS>
+// S: the storage (and stencil arithmetic) of the Lanczos vectors, the
+// residual and H times the residual -- double, or float in the mixed form
+// (dot products, coefficients, Krylov exponential and state in FP64 both ways)
+template <int NDIM, bool kS, typename S>
 __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
-  extern __shared__ double sil_dyn[];
+  extern __shared__ __align__(16) unsigned char sil_dyn_raw[];
+  S* sil_dyn = reinterpret_cast<S*>(sil_dyn_raw);
   __shared__ double sp[kSilNQ], st[kSilNQ], scratch[(kSilThreads / 32) * 8];
   __shared__ double ws[(kSilThreads / 32) * kSilNQ];
   __shared__ double s_red[kSilThreads];
@@ -470,10 +475,10 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
   const int t = threadIdx.x;
   const long n = a.n;
   const int m = a.m;
-  SilVecs<kS> vs;
-  vs.L = a.L;
-  vs.wb = a.wbuf;
-  vs.wk = a.work;
+  SilVecs<kS, S> vs;
+  vs.L = reinterpret_cast<S*>(a.L);
+  vs.wb = reinterpret_cast<S*>(a.wbuf);
+  vs.wk = reinterpret_cast<S*>(a.work);
   vs.sm = sil_dyn;
   vs.n = n;
   vs.m = m;
@@ -666,11 +671,11 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
               const int k = kk[pt];
               hr[pt][c] = rk[pt][c] = xk[pt][c] = 0.0;
               if (k < r.hi && s_active[c]) {
-                const double* rc = a.work + (long)c * n;
+                const S* rc = vs.wk + (long)c * n;
                 int idx[3];
                 grid_index<NDIM>(a, k, idx);
                 rk[pt][c] = vs.res(c, k, k - r.lo);
-                hr[pt][c] = apply_h_nd<NDIM>(a, rc, k, 1.0, idx);
+                hr[pt][c] = (double)apply_h_nd<NDIM, S>(a, rc, k, (S)1, idx);
                 if (a.dm) hr[pt][c] -= __ldg(a.dm + k) * efs * rk[pt][c];
                 xk[pt][c] = ld_state((c ? a.v : a.u) + k);
               }
@@ -788,15 +793,15 @@ __global__ void __launch_bounds__(kSilThreads, 1) sil_kernel(SilArgs a) {
 #pragma unroll
         for (int j = 0; j < kSilMaxM; ++j)
           if (j < m) {
-            a.L[(long)j * n + k] = lu[j];
-            a.L[(long)(m + j) * n + k] = lv[j];
+            vs.L[(long)j * n + k] = (S)lu[j];
+            vs.L[(long)(m + j) * n + k] = (S)lv[j];
           }
       } else if (!kS && ms < m) {
 #pragma unroll
         for (int j = 0; j < kSilMaxM; ++j)
           if (j == ms) {
-            a.L[(long)j * n + k] = lu[j];
-            a.L[(long)(m + j) * n + k] = lv[j];
+            vs.L[(long)j * n + k] = (S)lu[j];
+            vs.L[(long)(m + j) * n + k] = (S)lv[j];
           }
       }
       double ur = 0.0, ui = 0.0, vr = 0.0, vi = 0.0;
@@ -1197,6 +1202,7 @@ struct espec_grid_plan {
   double shm[3] = {0, 0, 0};
   double dt_fs = 0.0;
   int m = 0, absorb = 0, quirks = 0;
+  int precision = ESPEC_FP64;  // ESPEC_MIXED (SIL): FP32 Lanczos vectors and H psi
   int nblocks = 0, nblocks_max = 0;  // CTAs of the cooperative launches (<= co-resident)
   bool loaded = false, has_state = false;
   double *d_vpot = nullptr, *d_mask = nullptr, *d_u = nullptr, *d_v = nullptr;
@@ -1298,7 +1304,13 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   if (!out || !np || !shm) return set_error(ESPEC_EINVAL, "null argument");
   if (method != ESPEC_SIL && method != ESPEC_PSOD)
     return set_error(ESPEC_EINVAL, "grid plans run ESPEC_SIL or ESPEC_PSOD");
-  if (precision != ESPEC_FP64) return set_error(ESPEC_EINVAL, "grid plans run in FP64");
+  if (precision != ESPEC_FP64 && !(precision == ESPEC_MIXED && method == ESPEC_SIL))
+    return set_error(ESPEC_EINVAL, "grid plans run in FP64 (SIL also in ESPEC_MIXED)");
+  // the reference-defect form (sil.f:145-148) is not unitary and grows the
+  // state, amplifying FP32 rounding: it is kept for the FP64 form, which
+  // reproduces the executable's output
+  if (precision == ESPEC_MIXED && (quirks & ESPEC_Q_SIL_INPLACE))
+    return set_error(ESPEC_EINVAL, "the SIL defect form runs in FP64 only");
   if (ndim < 1 || ndim > 3) return set_error(ESPEC_EINVAL, "ndim must be 1, 2 or 3");
   const bool psod = method == ESPEC_PSOD;
   if (psod) mp = 0;
@@ -1328,15 +1340,16 @@ extern "C" int espec_grid_create(espec_grid_plan** out, int method, int ndim, co
   p->m = mp;
   p->absorb = absorb;
   p->quirks = quirks;
+  p->precision = precision;
   // co-resident CTAs for the cooperative launch
   int dev = 0, nsm = 0, occ = 0;
   const void* kern =
       psod ? (ndim == 1   ? (const void*)psod_kernel<1>
               : ndim == 2 ? (const void*)psod_kernel<2>
                           : (const void*)psod_kernel<3>)
-           : (ndim == 1   ? (const void*)sil_kernel<1, false>
-              : ndim == 2 ? (const void*)sil_kernel<2, false>
-                          : (const void*)sil_kernel<3, false>);
+           : (ndim == 1   ? (const void*)sil_kernel<1, false, double>
+              : ndim == 2 ? (const void*)sil_kernel<2, false, double>
+                          : (const void*)sil_kernel<3, false, double>);
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
   if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, kSilThreads, 0);
@@ -1477,13 +1490,20 @@ static int grid_launch(espec_grid_plan* p, int nsteps, bool from_start, cudaStre
   void* args[] = {&a};
   // the CTAs' own Lanczos vectors in shared memory when they fit
   const long chunk = (p->n + p->nblocks - 1) / p->nblocks;
-  const size_t dyn = sil_vec_smem(p->m, chunk);
-  const void* ks = p->ndim == 1   ? (const void*)sil_kernel<1, true>
-                   : p->ndim == 2 ? (const void*)sil_kernel<2, true>
-                                  : (const void*)sil_kernel<3, true>;
-  const void* kg = p->ndim == 1   ? (const void*)sil_kernel<1, false>
-                   : p->ndim == 2 ? (const void*)sil_kernel<2, false>
-                                  : (const void*)sil_kernel<3, false>;
+  const bool mixed = p->precision == ESPEC_MIXED;
+  const size_t dyn = sil_vec_smem(p->m, chunk, mixed ? 4 : 8);
+  const void* ks = mixed ? (p->ndim == 1   ? (const void*)sil_kernel<1, true, float>
+                            : p->ndim == 2 ? (const void*)sil_kernel<2, true, float>
+                                           : (const void*)sil_kernel<3, true, float>)
+                         : (p->ndim == 1   ? (const void*)sil_kernel<1, true, double>
+                            : p->ndim == 2 ? (const void*)sil_kernel<2, true, double>
+                                           : (const void*)sil_kernel<3, true, double>);
+  const void* kg = mixed ? (p->ndim == 1   ? (const void*)sil_kernel<1, false, float>
+                            : p->ndim == 2 ? (const void*)sil_kernel<2, false, float>
+                                           : (const void*)sil_kernel<3, false, float>)
+                         : (p->ndim == 1   ? (const void*)sil_kernel<1, false, double>
+                            : p->ndim == 2 ? (const void*)sil_kernel<2, false, double>
+                                           : (const void*)sil_kernel<3, false, double>);
   int dev = 0, optin = 0;
   cudaFuncAttributes fa{};
   GRID_CK(cudaGetDevice(&dev));
@@ -1643,6 +1663,8 @@ extern "C" int espec_grid_basis(espec_grid_plan* p, int chain, double* dst, int 
   if (!p || !dst || chain < 0 || chain > 1) return set_error(ESPEC_EINVAL, "bad argument");
   if (p->c_cap < 0) return set_error(ESPEC_EINVAL, "no basis: run the plan first");
   if (ld < p->n) return set_error(ESPEC_EINVAL, "leading dimension below the grid size");
+  if (p->precision != ESPEC_FP64)
+    return set_error(ESPEC_EINVAL, "a mixed plan keeps its Lanczos basis in FP32");
   cudaStream_t st = (cudaStream_t)stream;
   const cudaMemcpyKind kind =
       where == ESPEC_MEM_HOST ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice;

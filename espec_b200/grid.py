@@ -16,11 +16,13 @@ from . import _native as N
 
 class SilGrid:
     """Short-iterative-Lanczos propagation (PLNZ, plnz.f:71-151) of one packet
-    on a 1D/2D/3D grid with the finite-difference Hamiltonian, FP64."""
+    on a 1D/2D/3D grid with the finite-difference Hamiltonian, FP64; with
+    precision="mixed" the Lanczos vectors and H psi are FP32 (dot products,
+    coefficients, Krylov exponential and state FP64)."""
 
     method = N.SIL
 
-    def __init__(self, np_, shm, dt_fs, mp, absorb=N.ABS_NONE, quirks=0):
+    def __init__(self, np_, shm, dt_fs, mp, absorb=N.ABS_NONE, quirks=0, precision="fp64"):
         lib = N.load()
         self.np = [int(x) for x in np_]
         self.ndim = len(self.np)
@@ -31,7 +33,8 @@ class SilGrid:
         rc = lib.espec_grid_create(C.byref(self._h), self.method, self.ndim,
                                    npa.ctypes.data_as(C.POINTER(C.c_int)),
                                    shma.ctypes.data_as(C.POINTER(C.c_double)), float(dt_fs),
-                                   int(mp), N.FP64, absorb, quirks)
+                                   int(mp), {"fp64": N.FP64, "mixed": N.MIXED}[precision],
+                                   absorb, quirks)
         N.check(rc, "espec_grid_create")
         self.nsteps = None
 
