@@ -24,8 +24,9 @@ import numpy as np
 from . import _native as N
 from . import eig as EG
 
-# C2-family parameter box (BASELINE's 2D coupled Morse, De/a varied by about
-# +-6 % and +-4 %, coupling +-0.01 Eh/bohr^2); inside it the four lowest states
+# parameter box around the 2D coupled Morse of the 256 x 256 workload (De =
+# 0.17 / 0.12 Eh, a = 1.0 / 1.2 bohr^-1, varied by about +-6 % and +-4 %,
+# coupling +-0.01 Eh/bohr^2); inside it the four lowest states
 # keep their order (no crossings), so each state is a smooth function of q
 PARAM_LO = np.array([0.16, 0.95, 0.11, 1.15, -0.01])
 PARAM_HI = np.array([0.18, 1.05, 0.13, 1.25, 0.01])
