@@ -328,7 +328,9 @@ void espec_spo_destroy(espec_spo_plan* plan);
  * No absorber; C(t) every step, same arithmetic as variant 0 of the plans.
  * Calls share the array: calls whose GPU work overlaps race; serialise them.
  * The first call on each device resolves the array's address; make it
- * before any stream capture.  That address is cached for the life of the
+ * before any stream capture.  A call is not itself capturable into a graph:
+ * it copies its packet descriptors from host memory that is gone by the time
+ * a graph would replay.  The array's address is cached for the life of the
  * process (one primary context per device; do not call again on a device
  * after cudaDeviceReset).  Sizes beyond the limits return ESPEC_EINVAL.
  * ---------------------------------------------------------------------- */
