@@ -262,12 +262,12 @@ static bool variant_fits(int n, int v, int precision) {
 static int default_variant(int n, int precision) {
   if (precision == ESPEC_MIXED) {
     switch (n) {
-      case 256: return 2;
+      case 256: return 1;
       case 384: return 2;
       case 512: return 3;
       case 768: return 2;
       case 1024: return 1;
-      case 1536: return 3;
+      case 1536: return 2;
       case 2048: return 0;
       case 4096: return 2;
       default: return 0;
@@ -275,6 +275,7 @@ static int default_variant(int n, int precision) {
   }
   switch (n) {
     case 256: case 384: case 512: case 768: case 4096: return 2;
+    case 2048: return 1;
     default: return 0;
   }
 }
