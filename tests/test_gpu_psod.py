@@ -134,12 +134,13 @@ def test_psod_continue_and_energies(oracle):
 
 @pytest.mark.parametrize("np_,ctas,absorb,quirk", [
     ([300, 70], 4, 0, True), ([300, 70], 4, 1, False), ([512, 80], 4, 2, True),
-    ([260, 100], 6, 0, False)])
+    ([260, 100], 6, 0, False), ([301, 70], 4, 1, True), ([257, 64], 2, 2, False)])
 def test_psod_column_strips(oracle, np_, ctas, absorb, quirk):
     """The column-strip pass of 2D grids (CTA count a multiple of the strip
     count, 16 or more rows per band), forced on small grids by the CTA count,
     ragged last strip included: the oracle's results, the restart-copy
-    defect and the absorbers as on the point-range pass."""
+    defect and the absorbers as on the point-range pass, for even and odd
+    nx and one or several bands."""
     v, psi, sh, grids = packet(np_, 17 + absorb)
     sm = [1000.0, 1400.0]
     shm = [G.shm_of(m, h) for m, h in zip(sm, sh)]
