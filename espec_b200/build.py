@@ -13,7 +13,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libespecgpu.so")
 SOURCES = ["spo1d.cu", "capi.cu", "spo1d_inst_f32_pow2.cu", "spo1d_inst_f32_r3.cu",
-           "spo1d_inst_f64_pow2.cu", "spo1d_inst_f64_r3.cu", "spo1d_persist.cu", "spo_tc.cu", "spo1d_static.cu", "sod1d_inst.cu",
+           "spo1d_inst_f64_pow2.cu", "spo1d_inst_f64_r3.cu", "spo1d_persist.cu", "spo1d_any.cu", "spo_tc.cu", "spo1d_static.cu", "sod1d_inst.cu",
            "diag1d.cu", "dropin.cu", "sil.cu",
            "spectrum.cu", "potential.cu", "eig.cu", "mlp.cu", "mlp_tc.cu",
            "spond.cu", "deck.cpp", "pulse.cpp"]

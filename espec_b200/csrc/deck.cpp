@@ -1,27 +1,34 @@
 // deck.cpp -- eSPec input decks run through the GPU propagators: the part of
 // the driver (espec.f) from the input deck (rdinput.f) to the spectrum, for
-// time-dependent runs of one packet with a tabulated potential.
+// time-dependent runs of one packet, with a tabulated potential and its
+// eigenvector or with an analytic .1D potential and a computed eigenstate.
 //
-// Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL .FILE, *MASS,
-// *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION), *INIEIGVC .GETR,
-// *CHANGE, *SHIFT_POTENTIAL, *PRTCRL, *MASS_FACTOR, *DONOTSTOP; **TD *PROPAG
-// (.PFSPO, .PFSOD, .PSIL, .PSOD, .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE 0, *TPTRANS .ONE,
-// *PRPTOL, *ABSORBING, *PULSE_AND_DIPOLE (.GAUS, .GGAUS, .SIN2, .NONE with
-// the dipoles .CONST, .EXP, .NONE, .NULL), *NPROJECTIONS (projections on
-// LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.
-// Print and output-file switches (*PRTPOT, *PRTEIGVC, ...) are accepted and
-// ignored: no files are written.  Anything else -- analytic potentials,
-// computed initial states (the TI part), several states, dipoles read from a
-// file -- is refused with a message: there is no CPU path.
+// Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL (.FILE; the analytic
+// .1D forms of MAKECST with their initial and final constant records),
+// *GRID_RANGES, *MASS, *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION),
+// *INIEIGVC (.GETR; .CALC on .1D grids), *CHANGE, *SHIFT_POTENTIAL, *PRTCRL,
+// *MASS_FACTOR, *DONOTSTOP; **TI *TPDIAG (.MTRXDIAG, .LANCZS, .LANCZSG), *NIST,
+// *ABSTOL and an initial potential of its own; **TD *PROPAG (.PFSPO, .PFSOD,
+// .PSIL, .PSOD, .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE, *TPTRANS .ONE, *PRPTOL,
+// *ABSORBING, *PULSE_AND_DIPOLE (.GAUS, .GGAUS, .SIN2, .NONE with the dipoles
+// .CONST, .EXP, .NONE, .NULL), *NPROJECTIONS (on the computed states; with
+// .GETR on LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER,
+// *WINDOWING, *HWHM.  Print and output-file switches (*PRTPOT, *PRTEIGVC, ...)
+// are accepted and ignored: no files are written.  Anything else -- 2D/3D
+// computed states, the TI formalism, several transitions, dipoles read from
+// a file -- is refused with a message: there is no CPU path.
 //
 // The run follows espec.f: the .FILE reads of RDPTE / RDPT (rdpte.f, rdpt.f:
 // eigenvector block, then potential block, optionally shifted to its
-// minimum), SH = (XF - XI)/(NP - 1) and SHM = 1/(24 m SH^2) per axis, the C(t)
+// minimum) or, for .CALC, the potentials of GVPOT and the eigenstates of the
+// initial one (initial_state below),
+// SH = (XF - XI)/(NP - 1) and SHM = 1/(24 m SH^2) per axis, the C(t)
 // stride NC and the final time of espec.f:1328-1353, the absorber table of
 // ABSORBINGBC (absorb.f:62-205), the propagator drop-in (which prints the
 // partial auto-correlation table), the total correlation of espec.f:1545-1576
 // printed as FORMAT 1041/1042, and HWHM / SPECTRUMTD (espec.f:1596-1606).
 #include <algorithm>
+#include <cctype>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -40,6 +47,7 @@
 namespace {
 
 const double kAmu = 1.836152667539e3;  // espec.f:614
+const double kA0A = 5.291772083e-1;    // angstrom per bohr (espec.f:67)
 
 struct DeckError {
   std::string what;
@@ -80,6 +88,9 @@ bool starts(const std::string& s, const char* p) { return s.compare(0, std::strl
 // removed, blank lines skipped).
 struct Deck {
   std::map<std::string, std::map<std::string, std::vector<std::string>>> sec;
+  // the keyword lines themselves (rdinput.f tests columns past the keyword,
+  // e.g. '*GRID_RANGES au')
+  std::map<std::string, std::map<std::string, std::string>> head;
   const std::vector<std::string>* get(const char* s, const char* k) const {
     auto a = sec.find(s);
     if (a == sec.end()) return nullptr;
@@ -97,13 +108,15 @@ Deck parse_deck(const std::string& text) {
     if (bang != std::string::npos) line = line.substr(0, bang);
     const std::string t = trim(line);
     if (t.empty()) continue;
-    if (starts(t, "**")) {
+    if (starts(t, "**") && t.size() > 2 && std::isalpha((unsigned char)t[2])) {
       section = upper(t.substr(0, t.find_first_of(" \t")));
+      d.sec[section];
       key.clear();
     } else if (t[0] == '*') {
-      if (section.empty()) continue;  // the title lines before **MAIN
+      if (section.empty() || starts(t, "**")) continue;  // title lines
       key = upper(t.substr(0, t.find_first_of(" \t")));
       d.sec[section][key];
+      d.head[section][key] = t;
     } else if (!section.empty() && !key.empty()) {
       d.sec[section][key].push_back(t);
     }
@@ -244,9 +257,110 @@ std::string list_real(double x) {
   return " " + std::string(s.size() < 18 ? 18 - s.size() : 0, ' ') + s + "     ";
 }
 
+// Fortran Ew.d: 0.ddd...E+xx right-justified in w (the leading 0 dropped
+// when the sign leaves no room for it)
+std::string fort_e(double x, int w, int d) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%.*E", d - 1, x);  // one digit before the point
+  std::string s(buf);
+  const bool neg = s[0] == '-';
+  if (neg) s = s.substr(1);
+  const size_t e = s.find('E');
+  const int ex = x == 0.0 ? 0 : std::atoi(s.c_str() + e + 1) + 1;
+  std::string digits = s.substr(0, 1) + s.substr(2, e - 2);
+  char eb[16];
+  std::snprintf(eb, sizeof eb, "E%c%02d", ex < 0 ? '-' : '+', std::abs(ex));
+  std::string out = "0." + digits + eb;
+  if (neg) out = "-" + out;
+  if ((int)out.size() > w && neg) out = "-" + out.substr(2);
+  if ((int)out.size() > w) return std::string(w, '*');
+  return std::string(w - out.size(), ' ') + out;
+}
+
+// MAKECST (makecst.f:82-175) for a .1D deck: the constants of an analytic
+// potential to atomic units, the first prefix that matches deciding, with its
+// FORMAT 1020/1031/1041/1051/1061 lines.  sm1: the mass in electron masses.
+void makecst_1d(const std::string& potch, double sm1, std::vector<double>& c) {
+  const double ffreq = 4.556335252750e-6, ccgs = 2.99792458e10, eev = 27.211383411;
+  const double tau = 2.4188843243e-17, twopi = 6.2831853071795864769252867663;
+  c.resize(14, 0.0);
+  auto is = [&](const char* p) { return starts(potch, p); };
+  auto l1031 = [&](int i, double a, double b) {
+    std::printf(" Re_%d/a.u. = %s; K_%d/a.u. = %s;\n", i, fort_e(a, 12, 6).c_str(), i,
+                fort_e(b, 12, 6).c_str());
+  };
+  auto l1041 = [&](int i, double a, double b, double d) {
+    std::printf(" Re_%d/a.u. = %s; alpha_%d/a.u. = %s; D_%d/a.u. = %s\n", i,
+                fort_e(a, 12, 6).c_str(), i, fort_e(b, 12, 6).c_str(), i,
+                fort_e(d, 12, 6).c_str());
+  };
+  auto l1051 = [&]() {
+    std::printf(" R(min)_1/a.u. = %s; R(max)_1/a.u. = %s; Const_1/a.u. = %s\n",
+                fort_e(c[0], 12, 6).c_str(), fort_e(c[1], 12, 6).c_str(),
+                fort_e(c[2], 12, 6).c_str());
+  };
+  auto l1061 = [&]() { std::printf(" Const_1/a.u. = %s\n", fort_e(c[0], 12, 6).c_str()); };
+  const char* au = " These parameters were already inputed in a.u.\n";
+  auto sq = [](double x) { return x * x; };
+  if (is(".OHS")) {
+    const double fk1 = sq(((c[1] * ccgs) * tau) * twopi) * sm1;
+    c[0] = c[0] / kA0A;
+    c[1] = fk1;
+    l1031(1, c[0], c[1]);
+  } else if (is(".DOHS")) {
+    const double fk1 = sq(c[1] * ffreq) * sm1;
+    const double fk2 = sq(((c[4] * ccgs) * tau) * twopi) * sm1 / sq(kA0A * 1.0e-10);
+    const double re1 = c[0] / kA0A, re2 = c[2] / kA0A, re3 = c[3] / kA0A;
+    c[0] = re1;
+    c[1] = fk1;
+    c[2] = re2;
+    c[3] = re3;
+    c[4] = fk2;
+    l1031(1, c[0], c[1]);
+    l1031(2, c[2], c[3]);
+  } else if (is(".MORSE_Dalpha_au") || is(".ANTI-MORSE_Dalpha_au") || is(".MORSEM_Dalpha_au") ||
+             is(".ANTI-MORSEM_Dalpha_au") || is(".MOD-MORSE_Dalpha_au")) {
+    std::printf("%s", au);
+    l1041(1, c[0], c[1], c[2]);
+  } else if (is(".MORSE_Dalpha") || is(".ANTI-MORSE_Dalpha") || is(".MORSEM_Dalpha") ||
+             is(".ANTI-MORSEM_Dalpha") || is(".MOD-MORSE_Dalpha")) {
+    c[0] = c[0] / kA0A;
+    c[1] = c[1] * kA0A;
+    c[2] = c[2] / eev;
+    l1041(1, c[0], c[1], c[2]);
+  } else if (is(".MORSE") || is(".ANTI-MORSE") || is(".MORSEM") || is(".ANTI-MORSEM") ||
+             is(".MOD-MORSE")) {  // the _CM^1 names share these prefixes
+    const double re1 = c[0] / kA0A;
+    const double fk1 = sq(((c[1] * ccgs) * tau) * twopi) * sm1;
+    const double d1 = (((twopi * ccgs) * tau) * sq(c[1])) / (4.0 * c[2]);
+    const double al1 = std::sqrt(fk1 / (2.0 * d1));
+    c[0] = re1;
+    c[1] = al1;
+    c[2] = d1;
+    l1041(1, c[0], c[1], c[2]);
+  } else if (is(".BARRIER_au") || is(".WELL_au")) {
+    std::printf("%s", au);
+    l1051();
+  } else if (is(".CONST_au")) {
+    std::printf("%s", au);
+    l1061();
+  } else if (is(".BARRIER") || is(".WELL")) {
+    c[0] = c[0] / kA0A;
+    c[1] = c[1] / kA0A;
+    c[2] = c[2] / eev;
+    l1051();
+  } else if (is(".CONST") || is(".FREE")) {
+    c[0] = c[0] / eev;
+    l1061();
+  } else {
+    std::printf("<<<>>> Potential parameter converting error <<<>>>\n");
+    throw DeckError{"potential " + potch + ": no unit conversion for .1D (makecst.f:170-174)"};
+  }
+}
+
 struct Run {
   int nd = 1, np[3] = {1, 1, 1};
-  std::string dim = ".1D", potch = ".NULL", potfile, tpclc = ".SPECTRUM", tdi = ".NC";
+  std::string dim = ".1D", potch = ".NULL", potchf = ".NULL", potfile, tpclc = ".SPECTRUM", tdi = ".NC";
   std::string inieigvc = ".CALC", prtcrl = ".NO", tppropg = ".NULL", tptrans = ".ONE";
   std::string tpabsor, tpwind = ".NONE";
   bool change = false, shiftp = true, absorb = false, fstop = true, lhwhm = false;
@@ -260,6 +374,16 @@ struct Run {
   double e0 = 0.0, tp = 0.0, omg = 0.0, t0 = 0.0, td = 0.0, sni = 0.0;
   int kl = 0, npr = 1, kp = 1;
   std::vector<double> cstdm;
+  // analytic potential (rdinput.f:193-205: CSTI then CSTF records) and
+  // *GRID_RANGES in angstrom (rdinput.f:206-214)
+  std::vector<double> csti, cstf;
+  double gxi[3] = {0, 0, 0}, gxf[3] = {0, 0, 0};
+  // **TI (rdinput.f:370-381; defaults espec.f:129, 141-157): NIS states from
+  // the IIL-th, counted from 0 as in the deck
+  std::string tpdiag = ".MTRXDIAG";
+  int nis = 1, iil = 0;
+  double abstol = 1e-6;
+  bool calc() const { return starts(inieigvc, ".CALC"); }
 };
 
 const std::string& rec(const std::vector<std::string>* r, size_t i, const char* key) {
@@ -282,9 +406,9 @@ Run read_run(const Deck& d) {
   };
   for (const auto& s : d.sec) {
     const std::string& sname = s.first;
-    if (sname != "**MAIN" && sname != "**TD" && sname != "**SPECTRUM" && sname != "**END")
-      throw DeckError{"section " + sname + " is not covered (time-independent and "
-                      "eigenstate runs are not)"};
+    if (sname != "**MAIN" && sname != "**TI" && sname != "**TD" && sname != "**SPECTRUM" &&
+        sname != "**END")
+      throw DeckError{"section " + sname + " is not covered (collision runs are not)"};
     for (const auto& kv : s.second) {
       const std::string& k = kv.first;
       const std::vector<std::string>* v = &kv.second;
@@ -300,10 +424,22 @@ Run read_run(const Deck& d) {
           if ((int)n.size() < r.nd) throw DeckError{"*DIMENSION: grid sizes missing"};
           for (int a = 0; a < r.nd; ++a) r.np[a] = (int)n[a];
         } else if (k == "*POTENTIAL") {
-          r.potch = upper(rec(v, 0, "*POTENTIAL"));
-          if (!starts(r.potch, ".FILE"))
-            throw DeckError{"*POTENTIAL " + r.potch + ": only .FILE potentials are covered"};
-          r.potfile = rec(v, 1, "*POTENTIAL");
+          r.potch = r.potchf = upper(rec(v, 0, "*POTENTIAL"));
+          if (starts(r.potch, ".FILE")) {
+            r.potfile = rec(v, 1, "*POTENTIAL");
+          } else {
+            r.csti = numbers(rec(v, 1, "*POTENTIAL"));
+            r.cstf = numbers(rec(v, 2, "*POTENTIAL"));
+          }
+        } else if (k == "*GRID_RANGES") {
+          const std::vector<double> x = numbers(rec(v, 0, "*GRID_RANGES"));
+          // rdinput.f:206-214: columns 14-15 'au' give bohr
+          const std::string& h = d.head.at(sname).at(k);
+          const bool au = h.size() >= 15 && h.compare(13, 2, "au") == 0;
+          for (size_t a = 0; a < 3 && 2 * a + 1 < x.size(); ++a) {
+            r.gxi[a] = au ? x[2 * a] * kA0A : x[2 * a];
+            r.gxf[a] = au ? x[2 * a + 1] * kA0A : x[2 * a + 1];
+          }
         } else if (k == "*MASS") {
           const std::vector<double> m = numbers(rec(v, 0, "*MASS"));
           for (size_t a = 0; a < m.size() && a < 3; ++a) r.sm[a] = m[a];
@@ -331,19 +467,46 @@ Run read_run(const Deck& d) {
         } else {
           throw DeckError{"keyword " + k + " of **MAIN is not covered"};
         }
+      } else if (sname == "**TI") {
+        // rdinput.f:355-381: an initial potential of its own, the
+        // diagonalisation and the states it keeps
+        if (k == "*INITIAL_POTENTIAL" || k == "*INITIAL_CONDITION" || k == "*INITIAL_WP" ||
+            k == "*INITIAL_WF" || k == "*INITIAL_WAVE_FUNCTION" || k == "*WAVE_FUNCTION" ||
+            k == "*WAVE_PACKET" || k == "*POTENTIAL") {
+          r.potch = upper(rec(v, 0, k.c_str()));
+          if (starts(r.potch, ".FILE")) r.potfile = rec(v, 1, k.c_str());
+          else r.csti = numbers(rec(v, 1, k.c_str()));
+        } else if (k == "*TPDIAG") {
+          r.tpdiag = upper(rec(v, 0, "*TPDIAG"));
+        } else if (k == "*NIST") {
+          const std::vector<double> x = numbers(rec(v, 0, "*NIST"));
+          if (x.size() < 2) throw DeckError{"*NIST: NIS IIL"};
+          r.nis = (int)x[0];
+          r.iil = (int)x[1];
+        } else if (k == "*ABSTOL") {
+          r.abstol = numbers(rec(v, 0, "*ABSTOL")).at(0);
+        } else if (k == "*NFST" || k == "*SEED" || k == "*MAXINT") {
+          continue;  // final states (the TI formalism); the seed and length of LANCZSG
+        } else {
+          throw DeckError{"keyword " + k + " of **TI is not covered"};
+        }
       } else if (sname == "**TD") {
         if (k == "*PROPAG") {
           r.tppropg = upper(rec(v, 0, "*PROPAG"));
-          const std::vector<double> x = numbers(rec(v, 1, "*PROPAG"));
+          const std::string& line = rec(v, 1, "*PROPAG");
+          const std::vector<double> x = numbers(line);
           const bool sil = starts(r.tppropg, ".PSIL") || starts(r.tppropg, ".PPSIL") ||
                            starts(r.tppropg, ".PPLNZ");  // rdinput.f:439-444
-          if (x.size() < (sil ? 4u : 3u)) throw DeckError{"*PROPAG: TI TF DT" + std::string(sil ? " MP" : "")};
+          // a '/' ends the list early and leaves MP at its default
+          const bool slash = line.find('/') != std::string::npos;
+          if (x.size() < (sil && !slash ? 4u : 3u))
+            throw DeckError{"*PROPAG: TI TF DT" + std::string(sil ? " MP" : "")};
           r.ti = x[0];
           r.tf = x[1];
           r.dt = x[2];
           if (!(r.dt > 0.0) || !((r.tf - r.ti) / r.dt < 1.0e9))
             throw DeckError{"*PROPAG: DT must be positive and (TF - TI)/DT below 1e9"};
-          if (sil) r.mp = (int)x[3];
+          if (sil && x.size() >= 4) r.mp = (int)x[3];
         } else if (k == "*PRPGSTATE") {
           r.prpgstate = (int)numbers(rec(v, 0, "*PRPGSTATE")).at(0);
         } else if (k == "*TPTRANS") {
@@ -424,11 +587,38 @@ Run read_run(const Deck& d) {
       }
     }
   }
-  if (!starts(r.inieigvc, ".GETR") && !starts(r.inieigvc, ".READR"))
-    throw DeckError{"*INIEIGVC " + r.inieigvc + ": only .GETR (the eigenvector of the .FILE) is "
-                    "covered"};
-  if (!starts(r.tptrans, ".ONE") || r.prpgstate != 0)
-    throw DeckError{"one propagated state (*TPTRANS .ONE, *PRPGSTATE 0) is covered"};
+  const bool file_i = starts(r.potch, ".FILE"), file_f = starts(r.potchf, ".FILE");
+  if (starts(r.potch, ".NULL") || starts(r.potchf, ".NULL"))
+    throw DeckError{"*POTENTIAL is missing"};
+  // espec.f:410-413: an analytic potential always has its state computed
+  if (!file_i && !r.calc()) {
+    std::printf(" -> Warning! Replacing *INIEIGVC to .CALC\n");
+    r.inieigvc = ".CALC";
+  }
+  if (file_i != file_f)
+    throw DeckError{"an initial potential from a .FILE with an analytic final one (or the "
+                    "reverse) is not covered"};
+  if (file_i && !starts(r.inieigvc, ".GETR") && !starts(r.inieigvc, ".READR"))
+    throw DeckError{"*INIEIGVC " + r.inieigvc + ": a .FILE potential is covered with .GETR (the "
+                    "eigenvector of the .FILE)"};
+  if (!starts(r.tptrans, ".ONE"))
+    throw DeckError{"one propagated state (*TPTRANS .ONE) is covered"};
+  if (r.calc()) {
+    if (r.nd != 1)
+      throw DeckError{"computed initial states (.CALC) are covered on .1D grids"};
+    if (!(r.gxf[0] > r.gxi[0])) throw DeckError{"*GRID_RANGES: XI < XF is needed"};
+    // espec.f:1083: the propagated state is column NISPG - IIL + 1 of the NIS
+    // computed ones (IIL, NISPG counted from 1 there)
+    if (r.nis < 1 || r.iil < 0 || r.prpgstate < r.iil || r.prpgstate >= r.iil + r.nis)
+      throw DeckError{"*PRPGSTATE must be one of the states *NIST computes"};
+    if (r.iil + r.nis > 16 || r.prpgstate >= 16)
+      throw DeckError{"*NIST: the GPU eigensolver computes the 16 lowest states at most"};
+    if (!starts(r.tpdiag, ".MTRXDIAG") && !starts(r.tpdiag, ".LANCZS"))
+      throw DeckError{"*TPDIAG " + r.tpdiag + ": initial eigenvalue(s) and eigenvector(s) "
+                      "error (espec.f:920-925)"};
+  } else if (r.prpgstate != 0) {
+    throw DeckError{".GETR gives one state: *PRPGSTATE 0"};
+  }
   if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD"))
     throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": only .TD is covered"};
   if (!starts(r.tppropg, ".PFSPO") && !starts(r.tppropg, ".PFSOD") &&
@@ -436,18 +626,21 @@ Run read_run(const Deck& d) {
       !starts(r.tppropg, ".PPSIL") && !starts(r.tppropg, ".PPLNZ"))
     throw DeckError{"propagator " + r.tppropg + " is not covered (.PFSPO, .PFSOD, .PSIL, .PSOD, "
                     ".PPSOD, .PPSIL, .PPLNZ)"};
-  // rdinput.f:650-660 with NIS = 1 (.GETR).  The populations PPSOD prints are
-  // on LNZVC(., KP+1..KP+NPR), PPLNZ's on LNZVC(., KP+1..KP+NPR-1): the deck's
-  // eigenvector matrix, of which the executable holds column 1 at zero at the
-  // call; columns past it would be computed eigenstates (the TI branch)
-  if (r.npr + r.kp > 1) r.npr -= 1;
+  // rdinput.f:650-660 with NIS = 1 for .GETR.  The populations PPSOD prints
+  // are on LNZVC(., KP+1..KP+NPR), PPLNZ's on LNZVC(., KP+1..KP+NPR-1): the
+  // eigenvector matrix, which holds the NIS computed states for .CALC; for
+  // .GETR the executable holds its column 1 at zero at the call
+  const int nis = r.calc() ? r.nis : 1;
+  if (r.npr + r.kp > nis) r.npr -= nis;
   if (r.npr > 6) r.npr = 6;
   const int printed_w = starts(r.tppropg, ".PPSOD") ? r.npr
                         : (starts(r.tppropg, ".PPSIL") || starts(r.tppropg, ".PPLNZ")) ? r.npr - 1
                                                                                         : 0;
-  if (printed_w > 0 && (r.kp != 0 || printed_w > 1))
-    throw DeckError{"*NPROJECTIONS: projections on computed eigenstates are not covered "
-                    "(.GETR gives one state; KP = 0 with one printed projection is)"};
+  if (printed_w > 0 && !r.calc() && (r.kp != 0 || printed_w > 1))
+    throw DeckError{"*NPROJECTIONS: projections on computed eigenstates need .CALC (.GETR "
+                    "gives one state; KP = 0 with one printed projection is covered)"};
+  if (printed_w > 0 && r.calc() && (r.kp < 0 || r.kp + printed_w > r.nis))
+    throw DeckError{"*NPROJECTIONS: the projections reach past the states *NIST computes"};
   return r;
 }
 
@@ -513,6 +706,158 @@ std::string correlation_table(int mc, double tf, const std::vector<double>& cu,
   return out;
 }
 
+// Device buffers of one deck run, freed on every exit
+struct DevBufs {
+  std::vector<void*> p;
+  double* alloc(size_t count) {
+    void* q = nullptr;
+    if (cudaMalloc(&q, sizeof(double) * (count ? count : 1)) != cudaSuccess)
+      throw DeckError{"device memory for the initial state"};
+    p.push_back(q);
+    return (double*)q;
+  }
+  ~DevBufs() {
+    for (void* q : p) cudaFree(q);
+  }
+};
+
+// The time-independent part of espec.f for an analytic .1D potential: the
+// grid of *GRID_RANGES in bohr (espec.f:345, 618-641), MAKECST of both constant
+// records (espec.f:683-690), GVPOT of the initial potential (espec.f:865-869),
+// its eigenstates IIL..IIU (espec.f:872-927) and GVPOT of the final potential
+// (espec.f:985-990), both potentials on the GPU.  MTRXDIAG (DSPEVX of the
+// packed AP1D matrix) and LANCZS both diagonalise the finite-difference
+// Hamiltonian of AP1D / AU1D; here the GPU eigensolver does, its states
+// converged to a residual of 1e-12 ||H|| (the reference's ABSTOL = 1e-6 bounds
+// only the bisection of its eigenvalues).  Returns the propagated state
+// (EIGVC(., K), espec.f:1262-1265) and the final potential; eigvc: the NIS
+// states, n each; r.e1i = E1I (espec.f:927).
+FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<double>& eigvc) {
+  const int n = r.np[0];
+  FileData fd;
+  sm[0] = kAmu * r.sm[0];
+  sh[0] = ((r.gxf[0] - r.gxi[0]) / (n - 1.0)) / kA0A;
+  fd.xi[0] = r.gxi[0] / kA0A;
+  fd.xf[0] = r.gxf[0] / kA0A;
+  shm[0] = 1.0 / ((((24.0 * sm[0]) * r.smf[0]) * sh[0]) * sh[0]);  // espec.f:630
+  std::printf(" Initial potential:\n");
+  makecst_1d(r.potch, sm[0], r.csti);
+  std::printf(" Final potential:\n");
+  makecst_1d(r.potchf, sm[0], r.cstf);
+  std::printf(" \n Units converted.\n");
+  const int ki = espec_pot_kind(r.potch.c_str(), r.potch.size(), 1);
+  const int kf = espec_pot_kind(r.potchf.c_str(), r.potchf.size(), 1);
+  if (!ki || !kf)
+    throw DeckError{"potential " + (ki ? r.potchf : r.potch) + " is not a .1D form (pot1d)"};
+  // espec.f:879-905: *CHANGE on a grid above 3e4 points switches to LANCZSG,
+  // which keeps the ground state only
+  std::string tpdiag = r.tpdiag;
+  int iil = r.iil, nis = r.nis;
+  if (r.change && n > 30000) {
+    tpdiag = ".LANCZSG";
+    std::printf(" -> Type of diagonalization changed to: LANCZSG\n");
+  }
+  if (r.change && starts(tpdiag, ".LANCZSG")) {
+    std::printf(" -> .LANCZSG allows only the ground state eigenvectors calculation\n");
+    iil = 0;
+    nis = 1;
+    std::printf(" -> Total number of eigenvectors changed to %11d\n", 1);
+    if (r.prpgstate != 0) throw DeckError{".LANCZSG keeps the ground state: *PRPGSTATE 0"};
+  }
+  const int nst = std::max(iil + nis, r.prpgstate + 1);  // states 0 .. nst-1
+  const int m = std::min(40, n);
+  if (m < 2) throw DeckError{"the grid needs two points at least"};
+  DevBufs dev;
+  double* d_vi = dev.alloc(n);
+  double* d_vf = dev.alloc(n);
+  double* d_start = dev.alloc((size_t)nst * n);
+  double* d_vec = dev.alloc((size_t)nst * n);
+  double* d_eval = dev.alloc(nst);
+  double* d_resid = dev.alloc(nst);
+  int* d_mv = (int*)dev.alloc(nst);
+  double* d_L = dev.alloc((size_t)m * n);
+  double* d_w = dev.alloc(n);
+  double xmin = 0.0, xminb = 0.0;
+  msg1003("Generating initial potential...");
+  if (espec_gvpot_1d(1, &n, fd.xi, sh, ki, r.csti.data(), r.shiftp ? 1 : 0, d_vi, &xmin,
+                     nullptr))
+    throw DeckError{std::string("GVPOT: ") + espec_last_error()};
+  std::printf(" Initial potential generated.\n");
+  msg1003("Calculating eigenvalue(s) and eigenvector(s)");
+  std::printf("   %68s\n", "for the initial state...");
+  std::printf(" %s\n", starts(tpdiag, ".MTRXDIAG")   ? "Using complete matrix diagonalization procedure,"
+                       : starts(tpdiag, ".LANCZSG") ? "Using interative lanczos tri-diagonalization procedure,"
+                                                    : "Using lanczos tri-diagonalization procedure,");
+  std::fflush(stdout);
+  std::vector<double> vi(n);
+  if (cudaMemcpy(vi.data(), d_vi, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    throw DeckError{"copy of the initial potential"};
+  double vmax = 0.0;
+  for (double x : vi) vmax = std::max(vmax, std::fabs(x));
+  const double tol = 1e-12 * std::max(1.0, 64.0 * shm[0] + vmax);
+  const int npp[2] = {n, 1};
+  const double shmp[2] = {shm[0], 0.0};
+  std::vector<double> eval(nst), resid(nst);
+  eigvc.assign((size_t)nst * n, 0.0);
+  if (espec_eig_lcg_start(d_start, n, nst, nullptr) ||
+      espec_eig_solve_dev(1, npp, shmp, d_vi, d_start, nst, m, tol, 20000, d_vec, d_eval,
+                          d_resid, d_mv, d_L, d_w, nullptr) ||
+      cudaMemcpy(eval.data(), d_eval, sizeof(double) * nst, cudaMemcpyDeviceToHost) !=
+          cudaSuccess ||
+      cudaMemcpy(resid.data(), d_resid, sizeof(double) * nst, cudaMemcpyDeviceToHost) !=
+          cudaSuccess ||
+      cudaMemcpy(eigvc.data(), d_vec, sizeof(double) * nst * n, cudaMemcpyDeviceToHost) !=
+          cudaSuccess)
+    throw DeckError{std::string("initial eigenstates: ") + espec_last_error()};
+  bool ok = true;
+  for (int j = 0; j < nst; ++j) ok = ok && resid[j] <= tol;
+  if (ok) {
+    std::printf(" \n Eigenvalues:\n \"\"\"\"\"\"\"\"\"\"\"\"\n");
+    std::printf(" ---------------------------------\n");
+    std::printf(" |  Eigenstate  |  Eigenvalues   |\n =================================\n");
+    for (int j = iil; j < iil + nis; ++j)  // FORMAT 1015, 1014
+      std::printf(" |   %3d        |  %s  |\n ---------------------------------\n", j,
+                  fort_e(eval[j], 12, 6).c_str());
+  } else {
+    std::printf(" <<<>>> It wasn`t possible obtain eignvalues and eignvectors correctly <<<>>>\n"
+                " Exiting.\n");
+    if (r.fstop) throw DeckError{"the initial eigenstates did not converge"};
+  }
+  r.e1i = eval[r.prpgstate] * 27.2113834;
+  std::printf(" \n");
+  msg1003("   Generating final potential...");
+  fd.vpot.resize(n);
+  if (espec_gvpot_1d(1, &n, fd.xi, sh, kf, r.cstf.data(), r.shiftp ? 1 : 0, d_vf, &xminb,
+                     nullptr) ||
+      cudaMemcpy(fd.vpot.data(), d_vf, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+    throw DeckError{std::string("GVPOT: ") + espec_last_error()};
+  if (std::fabs(xminb - xmin) < 1e-6)
+    std::printf(" -> Warning: The initial and final potential have the same minimum possition.\n");
+  std::printf(" Final potential generated.\n");
+  // FORMAT 1031 and the list-directed 'state started' line (espec.f:1083-1108)
+  const int k = r.prpgstate - iil;
+  const char* th = k == 1 ? "st" : k == 2 ? "nd" : k == 3 ? "rd" : "th";
+  std::printf("\n%33sStarting %s%s state to be propagated...\n%12d %s state started.\n", "",
+              k < 10 ? std::to_string(k).c_str() : "*", th, k, th);
+  fd.psi.assign(eigvc.begin() + (size_t)r.prpgstate * n,
+                eigvc.begin() + (size_t)(r.prpgstate + 1) * n);
+  eigvc.erase(eigvc.begin(), eigvc.begin() + (size_t)iil * n);
+  eigvc.resize((size_t)nis * n);
+  return fd;
+}
+
+// espec.f:631-641, 818-830: the grid step in bohr; above 4e-2 the run stops
+void check_step(const Run& r, const double* sh) {
+  for (int a = 0; a < r.nd; ++a) {
+    if (sh[a] > 4.0e-2) {
+      std::printf(" <<<>>> Step bigger than%s  a.u. <<<>>>\n", list_real(4.0e-2).c_str());
+      if (r.fstop) throw DeckError{"the grid step is above 4e-2 bohr"};
+    } else if (sh[a] > 1.0e-2) {
+      std::printf(" -> Warning step bigger than%s  a.u. !\n", list_real(1.0e-2).c_str());
+    }
+  }
+}
+
 int run_deck(const std::string& deck_path) {
   Run r = load_run(deck_path);
   const size_t slash = deck_path.find_last_of('/');
@@ -520,23 +865,43 @@ int run_deck(const std::string& deck_path) {
   const std::string file = !r.potfile.empty() && r.potfile[0] == '/' ? r.potfile : dir + r.potfile;
   int n = 1;
   for (int a = 0; a < r.nd; ++a) n *= r.np[a];
-  FileData fd = read_file(file, n, r.nd, r.shiftp);
   double sh[3] = {1, 1, 1}, shm[3] = {0, 0, 0}, sm[3] = {1, 1, 1};
-  for (int a = 0; a < r.nd; ++a) {
-    sm[a] = kAmu * r.sm[a];  // espec.f:614
-    sh[a] = (fd.xf[a] - fd.xi[a]) / (r.np[a] - 1.0);
-    shm[a] = 1.0 / ((((24.0 * sm[a]) * r.smf[a]) * sh[a]) * sh[a]);  // espec.f:819
+  FileData fd;
+  std::vector<double> eigvc;  // the computed states IIL..IIU (.CALC)
+  if (r.calc()) {
+    // espec.f:646-664: absorber bounds in angstrom unless the form is in bohr
+    if (r.absorb && !starts(r.tpabsor, ".SMOOTHW_au") && !starts(r.tpabsor, ".SMRS_au") &&
+        !starts(r.tpabsor, ".VOPTIC"))
+      for (int a = 0; a < r.nd; ++a) {
+        r.al[a] = r.al[a] / kA0A;
+        r.ar[a] = r.ar[a] / kA0A;
+      }
+    sh[0] = ((r.gxf[0] - r.gxi[0]) / (n - 1.0)) / kA0A;
+    check_step(r, sh);
+    fd = initial_state(r, sh, shm, sm, eigvc);
+  } else {
+    fd = read_file(file, n, r.nd, r.shiftp);
+    for (int a = 0; a < r.nd; ++a) {
+      sm[a] = kAmu * r.sm[a];  // espec.f:614
+      sh[a] = (fd.xf[a] - fd.xi[a]) / (r.np[a] - 1.0);
+      shm[a] = 1.0 / ((((24.0 * sm[a]) * r.smf[a]) * sh[a]) * sh[a]);  // espec.f:819
+    }
+    check_step(r, sh);
   }
   const int nc = c_stride(r);
   std::vector<double> vabc(n, 0.0);
   if (r.absorb)
     vabc = absorber_table(r.nd, r.np, r.tpabsor, r.al, r.ar, sh, fd.xi, fd.xf, r.voi);
-  // propagation: the reference's LNZVC holds the Lanczos basis in columns
-  // 1..MP and C(t) in MP+1, MP+2 (espec.f:1357-1359)
+  // propagation: the reference's LNZVC (its EIGVC) holds the computed states
+  // in columns 1..NIS, the Lanczos basis in columns 1..MP and C(t) in MP+1,
+  // MP+2 (espec.f:1357-1359)
   const int steps = (int)std::lround((r.tf - r.ti) / r.dt) + 4;
   const int mxdct = std::max(n, steps / nc + 4);
   const int mpr = r.mp + 1, mpi = r.mp + 2;
-  std::vector<double> lnzvc((size_t)mxdct * (r.mp + 2), 0.0);
+  const int ncol = std::max({r.mp + 2, r.nis, r.kp + r.npr + 1});
+  std::vector<double> lnzvc((size_t)mxdct * ncol, 0.0);
+  for (size_t j = 0; j < eigvc.size() / (n ? n : 1); ++j)
+    std::copy(eigvc.begin() + j * n, eigvc.begin() + (j + 1) * n, lnzvc.begin() + j * mxdct);
   std::vector<double> u1 = fd.psi, v1(n, 0.0), u2(n, 0.0), v2(n, 0.0), tc(n, 0.0), wrk(n, 0.0);
   const int absorb = r.absorb ? 1 : 0, lmt = 10, change = r.change ? 1 : 0;
   double abstol = 1e-6;
@@ -657,6 +1022,7 @@ int run_scan(const std::string& deck_path, int njobs, const char* const* files,
              const std::string& prefix) {
   Run r = load_run(deck_path);
   if (r.nd != 1) throw DeckError{"scans run 1D decks (the batched plans are 1D)"};
+  if (r.calc()) throw DeckError{"scans read their states from .FILE inputs (.GETR)"};
   const bool spo = starts(r.tppropg, ".PFSPO");
   if (!spo && !starts(r.tppropg, ".PFSOD"))
     throw DeckError{"scans run .PFSPO or .PFSOD (the batched plans)"};

@@ -17,9 +17,9 @@
 // The arithmetic is the reference's, defects included: the in-place kinetic
 // multiply of spofft.f:150-153 and the never-applied .SMOOTHW mask of
 // sodfft.f:108, and PLNZ's cos-before-sin of sil.f:145-148.  Cases the GPU
-// path does not cover (PSPOFFT: 1D sizes other than 256..4096 of the form 2^k
-// or 3*2^k, 2D/3D axes other than 32..512 powers of two; PSODFFT: 1D sizes
-// above 2048; PLNZ: order above 16) and
+// path does not cover (PSPOFFT: odd 1D sizes and sizes above 7252 points,
+// 2D/3D axes other than 32..512 powers of two; PSODFFT: odd 1D sizes and
+// sizes above 3626; PLNZ: order above 16) and
 // device errors set INFO = 2 and write the reason to standard error; nothing
 // is computed on the CPU.
 #include <cuda_runtime.h>

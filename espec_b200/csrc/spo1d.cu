@@ -16,6 +16,7 @@
 #include "cplx_io.cuh"
 #include "diag1d.cuh"
 #include "sod1d.cuh"
+#include "spo1d_any.cuh"
 #include "spo1d_launch.cuh"
 #include "spo1d_persist.cuh"
 
@@ -233,7 +234,11 @@ static void plan_info(int n, int v, std::vector<int>& kap, int& n3) {
     case 1536: plan_info_n<1536>(v, kap, n3); break;
     case 2048: plan_info_n<2048>(v, kap, n3); break;
     case 4096: plan_info_n<4096>(v, kap, n3); break;
-    default: break;
+    default:  // the any-size kernels: natural order
+      kap.resize(n);
+      for (int j = 0; j < n; ++j) kap[j] = j;
+      n3 = 0;
+      break;
   }
 }
 
@@ -301,6 +306,9 @@ struct espec_spo_plan {
     int variant;
     SpoPacket* d_pkd;  // diagnostics: c_off = packet index
     int* d_kfreq;      // FFT index at each final position of the diagnostic FFT
+    bool any;          // a size outside the register plans (spo1d_any.cu)
+    AnyPlan ap;
+    double2* d_tw;     // its twiddle table
   };
   bool index_dirty = true;
   std::vector<Class> classes;
@@ -350,6 +358,7 @@ static void plan_free(espec_spo_plan* p) {
     cudaFree(c.d_pk);
     if (c.d_pkd) cudaFree(c.d_pkd);
     if (c.d_kfreq) cudaFree(c.d_kfreq);
+    if (c.d_tw) cudaFree(c.d_tw);
   }
   for (auto s : p->streams) cudaStreamDestroy(s);
   for (auto e : p->events) cudaEventDestroy(e);
@@ -443,15 +452,20 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
   p->sm.assign(sm, sm + npk);
   p->off.resize(npk + 1);
   p->off[0] = 0;
+  // sizes outside the register plans run the any-size kernels (FP64)
+  auto native = [&](int n) {
+    return size_supported(n) && (method != ESPEC_SOD || sod_size_supported(n));
+  };
   for (int i = 0; i < npk; ++i) {
-    if (!size_supported(p->n[i])) {
+    AnyPlan ap;
+    if (!native(p->n[i]) && (precision != ESPEC_FP64 || !any_plan(p->n[i], ap) ||
+                             any_smem_bytes(p->n[i], method) > kMaxSmem)) {
       delete p;
-      return set_error(ESPEC_EINVAL, "unsupported packet size (supported: 256, 384, 512, 768, "
-                                     "1024, 1536, 2048, 4096)");
-    }
-    if (method == ESPEC_SOD && !sod_size_supported(p->n[i])) {
-      delete p;
-      return set_error(ESPEC_EINVAL, "unsupported packet size for SOD (supported: 256 to 2048)");
+      return set_error(ESPEC_EINVAL, precision != ESPEC_FP64
+                                         ? "unsupported packet size for the mixed form (256, 384, "
+                                           "512, 768, 1024, 1536, 2048, 4096)"
+                                         : "unsupported packet size (FP64: even sizes from 4 to "
+                                           "7252 points, 3626 for SOD)");
     }
     if ((long long)p->off[i] + p->n[i] > INT_MAX) {
       delete p;
@@ -472,13 +486,22 @@ extern "C" int espec_prop_create(espec_spo_plan** out, int npk, const int* npts,
   for (auto& kv : cls) {
     espec_spo_plan::Class c{kv.first, (int)kv.second.size(), nullptr,
                             method == ESPEC_SOD ? 0 : default_variant(kv.first, precision),
-                            nullptr, nullptr};
+                            nullptr, nullptr, !native(kv.first), AnyPlan{}, nullptr};
     p->classes.push_back(c);  // owned by the plan from here on (freed by plan_free)
     auto& cc = p->classes.back();
     if ((rc = ck(cudaMalloc(&cc.d_pk, sizeof(SpoPacket) * cc.count), "cudaMalloc"))) return fail(rc);
     if ((rc = ck(cudaMalloc(&cc.d_pkd, sizeof(SpoPacket) * cc.count), "cudaMalloc")))
       return fail(rc);
     if ((rc = ck(cudaMalloc(&cc.d_kfreq, sizeof(int) * cc.n), "cudaMalloc"))) return fail(rc);
+    if (cc.any) {
+      any_plan(cc.n, cc.ap);
+      std::vector<double2> tw(cc.n);
+      any_twiddles(cc.n, tw.data());
+      if ((rc = ck(cudaMalloc(&cc.d_tw, sizeof(double2) * cc.n), "cudaMalloc"))) return fail(rc);
+      if ((rc = ck(cudaMemcpy(cc.d_tw, tw.data(), sizeof(double2) * cc.n, cudaMemcpyHostToDevice),
+                   "H2D")))
+        return fail(rc);
+    }
     {
       std::vector<SpoPacket> pkd;
       for (int i = 0; i < npk; ++i)
@@ -585,6 +608,7 @@ extern "C" int espec_spo_set_variant(espec_spo_plan* p, int npts, int variant) {
   bool found = false;
   for (auto& c : p->classes)
     if (c.n == npts) {
+      if (c.any) return set_error(ESPEC_EINVAL, "packets of this size have one kernel (any size)");
       c.variant = variant;
       found = true;
     }
@@ -824,7 +848,8 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
       a.nsteps = nsteps;
       int kabs = p->absorb == ESPEC_ABS_VOPTIC ? 1 : (p->absorb == ESPEC_ABS_SMOOTHW ? 2 : 0);
       if (kabs == 2 && (p->quirks & ESPEC_Q_SOD_SMOOTHW)) kabs = 0;  // sodfft.f:108
-      e = sod_launch(c.n, kabs, a, c.count, cs);
+      e = c.any ? sod_any_launch(a, c.ap, c.d_tw, kabs, c.count, cs)
+                : sod_launch(c.n, kabs, a, c.count, cs);
     } else if (p->precision == ESPEC_FP64) {
       SpoArgs<double> a{};
       a.tab = p->t64;
@@ -838,7 +863,8 @@ static int prop_launch(espec_spo_plan* p, int nsteps, bool resume, cudaStream_t 
       a.kq_scale = 1.0 / c.n;
       a.nsteps = nsteps;
       a.nonfinite = p->d_nonfinite;
-      e = launch_n<double>(c.n, c.variant, a, c.count, quirk, cs);
+      e = c.any ? spo_any_launch(a, c.ap, c.d_tw, quirk, c.count, cs)
+                : launch_n<double>(c.n, c.variant, a, c.count, quirk, cs);
     } else {
       SpoArgs<float> a{};
       a.tab = p->t32;
@@ -880,7 +906,8 @@ extern "C" int espec_prop_energies(espec_spo_plan* p, double* e, double* norm, v
   cudaStream_t st = (cudaStream_t)stream;
   for (auto& c : p->classes) {
     DiagArgs a{p->d_psi, p->d_vpot, p->d_tc, c.d_kfreq, c.d_pkd, p->d_diag};
-    cudaError_t err = diag_launch(c.n, a, c.count, st);
+    cudaError_t err = c.any ? diag_any_launch(a, c.ap, c.d_tw, c.count, st)
+                            : diag_launch(c.n, a, c.count, st);
     if (err != cudaSuccess) return set_cuda_error("diag1d_kernel launch", err);
   }
   std::vector<double2> h(p->npk);

@@ -26,7 +26,15 @@ Cases:
   deck_*      whole decks for the deck driver (input.spc, wf_pot.inp and the
               executable's output from the propagation on); --decks-only
               [name ...] generates only these (or the named ones).
+  reftest*    the reference's own test decks ttests/input.test<i> with an
+              analytic .1D potential and a computed initial state (.CALC):
+              the deck as input.spc and the executable's output from the
+              propagation on, gzipped, as expected.txt.gz; --reftests-only
+              [i ...] generates only these.  Tests 1 and 5 are left out: the
+              executable stops in their .LANCZS diagonalisation (DSTEIN is
+              called with an illegal argument); test 2 runs with .MTRXDIAG.
 """
+import gzip
 import json
 import os
 import re
@@ -451,6 +459,31 @@ def case_deck(name):
         f.write("\n".join(lines[i - 1:]) + "\n")
 
 
+# test 2 runs with .MTRXDIAG in place of its .LANCZS: on its 560-point grid
+# the executable's LANCZS returns ghost eigenvalues (0.0132557 and 0.0190582
+# twice each) and propagates a vector of norm^2 1.94 as "state 2"
+REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag"]
+
+
+def case_reftest(i):
+    """The reference's test deck i under tests/golden/reftest<i>/."""
+    num = int(str(i).split("_")[0])
+    with open(os.path.join(REF, "ttests", f"input.test{num}")) as f:
+        deck = f.read()
+    if str(i).endswith("_mtrxdiag"):
+        assert ".LANCZS" in deck
+        deck = deck.replace("*TPDIAG\n.LANCZS", "*TPDIAG\n.MTRXDIAG")
+    d = os.path.join(OUT, f"reftest{i}")
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "input.spc"), "w") as f:
+        f.write(deck)
+    out = run_deck(deck, {}, timeout=3600)
+    lines = out.splitlines()
+    k = max(j for j, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
+    with gzip.open(os.path.join(d, "expected.txt.gz"), "wt") as f:
+        f.write("\n".join(lines[k - 1:]) + "\n")
+
+
 def psod_cases():
     vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
     smeta = dict(absorb="SMOOTHW", voi=[0.05, 1.0], al=1.55, ar=2.3)
@@ -472,6 +505,12 @@ def save(cases, manifest):
 def main():
     if not os.path.exists(BIN):
         sys.exit("eSPec executable not found at " + BIN)
+    if "--reftests-only" in sys.argv:
+        picked = [a for a in sys.argv[1:] if a in map(str, REFTESTS)] or REFTESTS
+        from concurrent.futures import ThreadPoolExecutor
+        with ThreadPoolExecutor(4) as ex:
+            list(ex.map(case_reftest, picked))
+        return
     if "--decks-only" in sys.argv:
         names = [a for a in sys.argv[1:] if a in DECK_CASES] or list(DECK_CASES)
         for name in names:
@@ -511,6 +550,8 @@ def main():
     save(cases, {})
     for name in DECK_CASES:
         case_deck(name)
+    for i in REFTESTS:
+        case_reftest(i)
 
 
 if __name__ == "__main__":

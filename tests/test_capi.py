@@ -36,6 +36,23 @@ def test_errors_are_reported_without_a_device_call():
     assert b"null" in lib.espec_last_error()
 
 
+def test_packet_sizes_refused_without_a_device_call():
+    """Sizes outside the register FFT plans run FP64 only, even and up to the
+    shared memory of one CTA (7252 points; 3626 for SOD); what is refused is
+    refused before any CUDA call."""
+    lib = N.load()
+    cases = [(250, N.MIXED, N.SPO, b"mixed form"), (251, N.FP64, N.SPO, b"even sizes"),
+             (8000, N.FP64, N.SPO, b"even sizes"), (4096, N.FP64, N.SOD, b"even sizes")]
+    for n, prec, method, why in cases:
+        h = C.c_void_p()
+        npts = (C.c_int * 1)(n)
+        sh, sm = (C.c_double * 1)(0.01), (C.c_double * 1)(1000.0)
+        rc = lib.espec_prop_create(C.byref(h), 1, npts, sh, sm, C.c_double(0.1), method, prec,
+                                   0, 0)
+        assert rc == N.EINVAL, (n, prec, method)
+        assert why in lib.espec_last_error(), (n, lib.espec_last_error())
+
+
 def test_fortran_shim_binds_exported_drop_ins():
     """include/espec_gpu.f90 binds (bind(C)) only symbols the library exports,
     one per reference routine it replaces, with three hidden lengths each."""

@@ -1,6 +1,8 @@
 """The deck driver's reading of eSPec input decks (espec_b200/csrc/deck.cpp),
 on the CPU: what it does not cover is refused with the reason before any
-device work, and a .FILE that is missing or short is reported."""
+device work, a .FILE that is missing or short is reported, and the unit
+conversion of analytic potentials (MAKECST) prints the executable's
+constants."""
 import os
 
 import pytest
@@ -23,13 +25,16 @@ def refused(tmp_path, text, files=None):
 
 
 @pytest.mark.parametrize("old,new,why", [
-    (".FILE\nwf_pot.inp", ".MORSE\n1.1 1943.8 13.7 1.0/\n1.2 1629.2 17.7 1.0/", ".FILE"),
+    # an analytic potential turns *INIEIGVC into .CALC; the deck has no grid
+    (".FILE\nwf_pot.inp", ".MORSE\n1.1 1943.8 13.7 1.0/\n1.2 1629.2 17.7 1.0/", "*GRID_RANGES"),
     (".GETR", ".CALC", ".GETR"),
     (".PFSPO", ".P2PABM", "propagator"),
     (" 0.0  0.3096171935104  0.00120944216215/", " 0.0  0.3096171935104  0.0/", "DT must be"),
     (".1D\n 256/", ".2DC\n 16 16/", "*DIMENSION"),
     ("*TPTRANS\n.ONE", "*TPTRANS\n.ALL", "one propagated state"),
-    ("**TD", "**TI\n*TPDIAG\n.LANCZS\n**TD", "section **TI"),
+    ("*PRPGSTATE\n 0/", "*PRPGSTATE\n 1/", "*PRPGSTATE 0"),
+    ("**TD", "**COLLISION\n**TD", "section **COLLISION"),
+    ("**TD", "**TI\n*COLLISION_ENERGY\n 1.0/\n**TD", "keyword *COLLISION_ENERGY"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n*PRPTOL", "*PULSE_AND_DIPOLE"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.LASER\n 1 2 3 4 5/\n.NULL\n*PRPTOL", "pulse is not known"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.READ\ndm.inp\n*PRPTOL", "dipole .READ"),
@@ -123,3 +128,129 @@ def test_final_time_warning_text(tmp_path, capfd):
         pass  # no device here: the propagation itself fails after the warning
     out = capfd.readouterr().out.split("\n")
     assert " -> Warning! Final time changed to  0.309617193510400     " in out
+
+
+# the reference's test deck 6 (ttests/input.test6) with MF lowered, and the
+# constants its executable prints for it (espec_v07.x, "Initial potential:" /
+# "Final potential:" lines)
+CALC = """*** eSPec input file ***
+**MAIN
+*DIMENSION
+.1D
+ 256/
+*POTENTIAL
+.MORSE
+ 1.14600  1943.79  13.71  1.0/
+ 1.21100  1629.23  17.74  1.0/
+*GRID_RANGES
+ 0.5  2.8/
+*MASS
+ 7.49D0/
+*TPCALC
+.SPECTRUM
+.TD
+*INIEIGVC
+.CALC
+*CHANGE
+.YES
+**TI
+*TPDIAG
+.LANCZS
+*NIST
+ 1  0/
+*ABSTOL
+ 1D-6/
+**TD
+*PROPAG
+.PFSPO
+ 0.0  0.0512  2D-4/
+*PRPGSTATE
+ 0/
+*TPTRANS
+.ONE
+**SPECTRUM
+*FOURIER
+ 8/
+*WINDOWING
+.SG
+ 1D-5/
+**END
+"""
+CALC_CONSTANTS = [
+    " Re_1/a.u. = 0.216563E+01; alpha_1/a.u. = 0.131080E+01; D_1/a.u. = 0.313919E+00",
+    " Re_1/a.u. = 0.228846E+01; alpha_1/a.u. = 0.149106E+01; D_1/a.u. = 0.170438E+00"]
+
+
+def run_calc(tmp_path, text):
+    """Runs a .CALC deck; without a GPU it stops at the first device buffer,
+    after the unit conversion.  Returns the error message or None."""
+    p = tmp_path / "input.spc"
+    p.write_text(text)
+    try:
+        D.run(p)
+    except N.EspecError as e:
+        return str(e)
+    return None
+
+
+def test_calc_morse_constants(tmp_path, capfd):
+    """MAKECST of .MORSE (makecst.f:134-157): Re / A0A, alpha and D from the
+    frequency and the anharmonic constant; the two lines the executable
+    prints for the reference's test deck 6."""
+    msg = run_calc(tmp_path, CALC)
+    assert msg is None or "device memory" in msg, msg
+    out = capfd.readouterr().out.split("\n")
+    i = out.index(" Initial potential:")
+    assert out[i + 1] == CALC_CONSTANTS[0]
+    assert out[i + 2] == " Final potential:"
+    assert out[i + 3] == CALC_CONSTANTS[1]
+    assert " -> Warning step bigger than  1.000000000000000E-002  a.u. !" in out
+
+
+def test_calc_ohs_constants(tmp_path, capfd):
+    """.OHS (makecst.f:83-88): the constants the executable prints for the
+    reference's test decks 9-14."""
+    text = CALC.replace(".MORSE\n 1.14600  1943.79  13.71  1.0/\n 1.21100  1629.23  17.74  1.0/",
+                        ".OHS\n 1.14600  1943.79/\n 1.21100  1629.23/")
+    msg = run_calc(tmp_path, text)
+    assert msg is None or "device memory" in msg, msg
+    out = capfd.readouterr().out.split("\n")
+    assert " Re_1/a.u. = 0.216563E+01; K_1/a.u. = 0.107875E+01;" in out
+    assert " Re_1/a.u. = 0.228846E+01; K_1/a.u. = 0.757856E+00;" in out
+
+
+@pytest.mark.parametrize("old,new,why", [
+    (".1D\n 256/", ".2D\n 64 64/", ".1D grids"),
+    ("*NIST\n 1  0/", "*NIST\n 3  1/", "*PRPGSTATE must be one of"),
+    ("*NIST\n 1  0/", "*NIST\n 17  0/", "16 lowest states"),
+    (".LANCZS\n", ".JACOBI\n", "eigenvalue(s) and eigenvector(s)"),
+    (".MORSE\n", ".DMORSE\n", "no unit conversion"),
+    (".MORSE\n", ".WELL\n", "not a .1D form"),
+    (" 0.5  2.8/", " 2.8  0.5/", "XI < XF"),
+    (" 1.21100  1629.23  17.74  1.0/\n", "", "missing record of *POTENTIAL"),
+    (" 256/", " 20/", "grid step is above 4e-2"),
+])
+def test_calc_refusals(tmp_path, old, new, why):
+    """What the .CALC path does not cover, or where the executable stops, is
+    refused before any device work."""
+    assert old in CALC
+    msg = run_calc(tmp_path, CALC.replace(old, new))
+    assert msg is not None and why in msg, msg
+
+
+def test_calc_projections_on_computed_states(tmp_path):
+    """rdinput.f:659-660 with NIS computed states: the populations PPSOD
+    prints are on states KP+1..KP+NPR, which *NIST must provide."""
+    text = CALC.replace(".PFSPO\n 0.0  0.0512  2D-4/", ".PPSOD\n 0.0  0.0512  2D-4/")
+    text = text.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.PROPAGATION")
+    # NPR + KP > NIS lowers NPR by NIS: 3 1 with NIS = 3 leaves none; 6 1
+    # leaves 3 on states 2..4, one past the computed ones
+    for nist, proj, ok in (("7  0", "6 1", True), ("3  0", "3 1", True), ("3  0", "2 1", True),
+                           ("3  0", "6 1", False)):
+        t = text.replace("*NIST\n 1  0/", f"*NIST\n {nist}/")
+        t = t.replace("*TPTRANS", f"*NPROJECTIONS\n {proj}/\n*TPTRANS")
+        msg = run_calc(tmp_path, t)
+        if ok:
+            assert msg is None or "device memory" in msg, (nist, proj, msg)
+        else:
+            assert msg is not None and "*NPROJECTIONS" in msg, (nist, proj, msg)

@@ -10,6 +10,7 @@ For .PSIL the executable's total correlation is corrupted (it stores C(t)
 in LNZVC columns MP+1, MP+2 past the LMTREORT columns of its array, where
 scratch data overwrite samples); there the driver's table is checked against
 the mirror assembly of the C samples in its own partial table instead."""
+import gzip
 import os
 import re
 
@@ -60,37 +61,91 @@ def compare(have, want, slack=0.0):
     return exact
 
 
-@pytest.mark.parametrize("name", DECKS)
-def test_deck_matches_executable(capfd, name):
-    d = os.path.join(G.GOLDEN, name)
+def run_and_read(capfd, d):
+    """The driver's output for the deck in directory d, from the line before
+    the last 'Propagating eigenvector...', and the executable's."""
     capfd.readouterr()
     D.run(os.path.join(d, "input.spc"))
     out, err = capfd.readouterr()
     assert err == ""
     lines = out.split("\n")
     i = max(k for k, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
-    have = lines[i - 1:]
-    with open(os.path.join(d, "expected.txt")) as f:
-        want = f.read().split("\n")
+    if os.path.exists(os.path.join(d, "expected.txt")):
+        with open(os.path.join(d, "expected.txt")) as f:
+            want = f.read().split("\n")
+    else:
+        with gzip.open(os.path.join(d, "expected.txt.gz"), "rt") as f:
+            want = f.read().split("\n")
+    return lines[i - 1:], want
+
+
+@pytest.mark.parametrize("name", DECKS)
+def test_deck_matches_executable(capfd, name):
+    have, want = run_and_read(capfd, os.path.join(G.GOLDEN, name))
     if "_sil" not in name:
         exact = compare(have, want, slack=4e-7 if "ppsil" in name else 0.0)
         assert exact >= 0.9 * len(want), (exact, len(want))
         return
+    check_sil(have, want, 4e-7)
+
+
+# The reference's own test decks (ttests/input.test<i>): an analytic .1D
+# potential, the initial state computed (.CALC) and propagated on the final
+# potential for 125 thousand to 3 million steps.  Allowances beyond one unit
+# of the last printed digit, measured:
+#   .PFSPO, .PFSOD (tests 6, 12, 10): the executable's C(t) drifts from the
+#     oracle's restatements of spofft.f / sodfft.f (which the GPU matches to
+#     print precision) by a phase growing linearly with t: 3e-7 (.PFSPO) and
+#     6.3e-6 (.PFSOD, N = 250) after 2.5 million steps.  fft3d.f assigns its
+#     constants RAD, C72, S72, S120 from default-REAL (single precision)
+#     literals, so the executable's transforms differ from a DFT by a
+#     relative 3e-8;
+#   .PSIL, .PPSIL (tests 13, 14): the executable bisects the eigenvalues of
+#     its Krylov matrices to ABSTOL = 1e-6 only, so its norm falls by 3e-6
+#     over the 125 thousand steps and C(t) moves by up to 4.5e-6; its total
+#     correlation is corrupted (samples overwritten, see check_sil).
+# .PSOD and .PPSOD (tests 9, 11) need none, nor test 2 (.PPSOD,
+# six populations on computed states, HWHM shifted by the computed E1I), run
+# with .MTRXDIAG: its own .LANCZS gives the executable ghost eigenvalues.
+REFTESTS = {"reftest9": 0.0, "reftest10": 8e-6, "reftest11": 0.0, "reftest12": 4e-7,
+            "reftest6": 4e-7, "reftest13": 5e-6, "reftest14": 5e-6, "reftest2_mtrxdiag": 0.0}
+
+
+@pytest.mark.parametrize("name", sorted(REFTESTS))
+def test_reference_test_deck(capfd, name):
+    have, want = run_and_read(capfd, os.path.join(G.GOLDEN, name))
+    if name in ("reftest13", "reftest14"):
+        check_sil(have, want, REFTESTS[name])
+    else:
+        compare(have, want, slack=REFTESTS[name])
+
+
+def check_sil(have, want, slack):
+    """Partial table within slack; the executable's total correlation and
+    spectrum are not comparable (LNZVC columns overwritten), so the driver's
+    total correlation is checked against the mirror assembly of its own
+    partial table, and the text lines of the rest against the executable's."""
     k = have.index(" Correlation Function:")
     assert want.index(" Correlation Function:") == k and len(have) == len(want)
-    compare(have[:k], want[:k], slack=4e-7)  # last digits of |C|^2 often differ
+    compare(have[:k], want[:k], slack=slack)
     for h, w in zip(have[k:], want[k:]):  # the text lines of the rest
         if not (w.split() and all(NUM.match(t) or set(t) == {"*"} for t in w.split())):
             assert h == w, (h, w)
     # total correlation: C(-t) = C(t)*, 2^MF samples from the partial table
-    j = have.index(" Partial auto-correlation function:")
-    part = np.array([[float(x) for x in l.split()] for l in have[j + 3:k] if is_row(l, 6)])
+    # (PPLNZ's 1D table, "Auto-correlation function:", prints Cr, Ci in
+    # columns 4, 5 with five decimals; PLNZ's in columns 3, 4 with seven)
+    j = [i for i, l in enumerate(have) if l.strip() in ("Partial auto-correlation function:",
+                                                        "Auto-correlation function:")][0]
+    pulse = have[j].strip() == "Auto-correlation function:"
+    ncol = max(len(l.split()) for l in have[j + 3:k])
+    part = np.array([[float(x) for x in l.split()] for l in have[j + 3:k] if is_row(l, ncol)])
     corr = np.array([[float(x) for x in l.split()] for l in have[k + 3:] if is_row(l, 3)])
     mc = len(corr) // 2
-    c = part[:mc, 2] + 1j * part[:mc, 3]
+    c = part[:mc, 3] + 1j * part[:mc, 4] if pulse else part[:mc, 2] + 1j * part[:mc, 3]
+    tol = 0.51e-5 + 0.51e-7 if pulse else 1.01e-7
     full = np.concatenate([[np.conj(c[mc - 1])], np.conj(c[1:mc][::-1]), c])
-    assert np.max(np.abs(corr[:, 1] - full.real)) <= 1.01e-7
-    assert np.max(np.abs(corr[:, 2] - full.imag)) <= 1.01e-7
+    assert np.max(np.abs(corr[:, 1] - full.real)) <= tol
+    assert np.max(np.abs(corr[:, 2] - full.imag)) <= tol
 
 
 def test_scan_equals_one_run_per_file(tmp_path, capfd):
