@@ -10,13 +10,15 @@
 // *MASS_FACTOR, *DONOTSTOP; **TI *TPDIAG (.MTRXDIAG, .LANCZS, .LANCZSG), *NIST,
 // *ABSTOL and an initial potential of its own; **TD *PROPAG (.PFSPO, .PFSOD,
 // .PSIL, .PSOD, .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE, *TPTRANS .ONE, *PRPTOL,
-// *ABSORBING, *PULSE_AND_DIPOLE (.GAUS, .GGAUS, .SIN2, .NONE with the dipoles
-// .CONST, .EXP, .NONE, .NULL), *NPROJECTIONS (on the computed states; with
-// .GETR on LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER,
-// *WINDOWING, *HWHM.  Print and output-file switches (*PRTPOT, *PRTEIGVC, ...)
-// are accepted and ignored: no files are written.  Anything else -- 2D/3D
-// computed states, the TI formalism, several transitions, dipoles read from
-// a file -- is refused with a message: there is no CPU path.
+// *ABSORBING, *PULSE_AND_DIPOLE (pulses .GAUS, .GGAUS, .SIN2, .NONE; dipoles
+// .CONST, .EXP, .EXP+ (analytic decks), .READ (a file as RDPTE reads it),
+// .NONE, .NULL), *NPROJECTIONS (on the computed states; with .GETR on
+// LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING,
+// *HWHM.  Print and output-file switches
+// (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored: no files are written
+// (nor the unit-21 table .EXP+ writes).  Anything else -- 2D/3D computed
+// states, the TI formalism, several transitions -- is refused with a
+// message: there is no CPU path.
 //
 // The run follows espec.f: the .FILE reads of RDPTE / RDPT (rdpte.f, rdpt.f:
 // eigenvector block, then potential block, optionally shifted to its
@@ -131,28 +133,31 @@ struct FileData {
   double xi[3] = {0, 0, 0}, xf[3] = {0, 0, 0};
 };
 
+// one block of RDPTE / RDPT: a title record, then nt records of nd
+// coordinates (last axis first) and a value; XI, XF from the first and last
+void read_block(std::ifstream& f, const std::string& path, int nt, int nd, std::vector<double>& out,
+                double* xi, double* xf) {
+  std::string line;
+  out.resize(nt);
+  if (!std::getline(f, line)) throw DeckError{"reading file error: " + path};
+  for (int j = 0; j < nt; ++j) {
+    if (!std::getline(f, line)) throw DeckError{"reading file error: " + path};
+    const std::vector<double> v = numbers(line);
+    if ((int)v.size() < nd + 1) throw DeckError{"reading file error: " + path};
+    out[j] = v[nd];
+    if (j == 0)
+      for (int a = 0; a < nd; ++a) xi[a] = v[nd - 1 - a];
+    if (j == nt - 1)
+      for (int a = 0; a < nd; ++a) xf[a] = v[nd - 1 - a];
+  }
+}
+
 FileData read_file(const std::string& path, int nt, int nd, bool shiftp) {
   std::ifstream f(path);
   if (!f) throw DeckError{"potential input file \"" + path + "\" cannot be opened"};
   FileData r;
-  r.psi.resize(nt);
-  r.vpot.resize(nt);
-  std::string line;
-  auto block = [&](std::vector<double>& out, bool coords) {
-    if (!std::getline(f, line)) throw DeckError{"reading file error: " + path};
-    for (int j = 0; j < nt; ++j) {
-      if (!std::getline(f, line)) throw DeckError{"reading file error: " + path};
-      const std::vector<double> v = numbers(line);
-      if ((int)v.size() < nd + 1) throw DeckError{"reading file error: " + path};
-      out[j] = v[nd];
-      if (coords && j == 0)
-        for (int a = 0; a < nd; ++a) r.xi[a] = v[nd - 1 - a];
-      if (coords && j == nt - 1)
-        for (int a = 0; a < nd; ++a) r.xf[a] = v[nd - 1 - a];
-    }
-  };
-  block(r.psi, true);
-  block(r.vpot, true);  // RDPT sets XI, XF again from the potential block
+  read_block(f, path, nt, nd, r.psi, r.xi, r.xf);
+  read_block(f, path, nt, nd, r.vpot, r.xi, r.xf);  // RDPT sets XI, XF again
   if (shiftp) {
     double vmin = r.vpot[0];
     for (double x : r.vpot) vmin = x < vmin ? x : vmin;
@@ -370,7 +375,7 @@ struct Run {
   double voi[3] = {0, 0, 0}, al[3] = {0, 0, 0}, ar[3] = {0, 0, 0};
   int mf = 13, mp = 10, prpgstate = 0;
   // *PULSE_AND_DIPOLE (rdinput.f:549-578; defaults espec.f:124-177)
-  std::string efc = ".NONE", tpdipl = ".NULL";
+  std::string efc = ".NONE", tpdipl = ".NULL", dmfile;
   double e0 = 0.0, tp = 0.0, omg = 0.0, t0 = 0.0, td = 0.0, sni = 0.0;
   int kl = 0, npr = 1, kp = 1;
   std::vector<double> cstdm;
@@ -540,9 +545,11 @@ Run read_run(const Deck& d) {
             if (ggaus) r.kl = (int)x[5];
           }
           r.tpdipl = upper(rec(v, i++, "*PULSE_AND_DIPOLE"));
-          if (starts(r.tpdipl, ".READ") || starts(r.tpdipl, ".GET") || starts(r.tpdipl, ".EXP+"))
-            throw DeckError{"dipole " + r.tpdipl + " is not covered (.CONST, .EXP, .NONE, .NULL)"};
-          if (!starts(r.tpdipl, ".NULL")) {
+          if (starts(r.tpdipl, ".READ") || starts(r.tpdipl, ".GET")) {
+            r.dmfile = rec(v, i++, "*PULSE_AND_DIPOLE");  // rdinput.f:571-572
+            if (starts(r.tpdipl, ".GET"))
+              throw DeckError{"desired dipole moment .GET wasn't found (dipl.f:86-89)"};
+          } else if (!starts(r.tpdipl, ".NULL")) {
             if (!starts(r.tpdipl, ".CONST") && !starts(r.tpdipl, ".EXP") &&
                 !starts(r.tpdipl, ".NONE"))
               throw DeckError{"desired dipole moment " + r.tpdipl + " wasn't found (dipl.f:86-89)"};
@@ -619,6 +626,9 @@ Run read_run(const Deck& d) {
   } else if (r.prpgstate != 0) {
     throw DeckError{".GETR gives one state: *PRPGSTATE 0"};
   }
+  if (starts(r.tpdipl, ".EXP+") && !r.calc())
+    throw DeckError{"dipole .EXP+ is normalised at the final potential's Re (CSTF(1), dipl.f), "
+                    "which a .FILE potential leaves at zero"};
   if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD"))
     throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": only .TD is covered"};
   if (!starts(r.tppropg, ".PFSPO") && !starts(r.tppropg, ".PFSOD") &&
@@ -946,12 +956,27 @@ int run_deck(const std::string& deck_path) {
           std::strlen(pr), std::strlen(ta));
   } else if (starts(r.tppropg, ".PPSOD") || starts(r.tppropg, ".PPSIL") ||
              starts(r.tppropg, ".PPLNZ")) {
-    // DIPLMMT (dipl.f:61-85): R = XI(1) + (I - 1) SH(1) for every I of the grid
+    // DIPLMMT (dipl.f:61-95): R = XI(1) + (I - 1) SH(1) for every I of the
+    // grid, or the values of a file read as RDPTE reads (which sets XI, XF
+    // again from its coordinates)
     std::vector<double> dmv(n, 0.0);
-    for (int i = 0; i < n; ++i) {
+    if (starts(r.tpdipl, ".READ")) {
+      const std::string dmf = !r.dmfile.empty() && r.dmfile[0] == '/' ? r.dmfile : dir + r.dmfile;
+      std::ifstream f(dmf);
+      if (!f) throw DeckError{"dipole file \"" + dmf + "\" cannot be opened"};
+      read_block(f, dmf, n, r.nd, dmv, fd.xi, fd.xf);
+    }
+    for (int i = 0; i < n && !starts(r.tpdipl, ".READ"); ++i) {
       const double rab = fd.xi[0] + i * sh[0];
-      if (starts(r.tpdipl, ".CONST")) dmv[i] = r.cstdm[0] / rab;
-      else if (starts(r.tpdipl, ".EXP")) dmv[i] = r.cstdm[0] * rab * std::exp(-r.cstdm[1] * rab);
+      if (starts(r.tpdipl, ".CONST")) {
+        dmv[i] = r.cstdm[0] / rab;
+      } else if (starts(r.tpdipl, ".EXP+")) {  // normalised at the final surface's Re
+        const double c = r.cstdm[1], re = r.cstf[0];
+        dmv[i] = r.cstdm[0] * (std::exp(-c * rab) - std::exp(-3.0 * c * rab)) /
+                 (std::exp(-c * re) - std::exp(-3.0 * c * re));
+      } else if (starts(r.tpdipl, ".EXP")) {
+        dmv[i] = r.cstdm[0] * rab * std::exp(-r.cstdm[1] * rab);
+      }
     }
     const int off = 0, nshot = 10, nispg = r.prpgstate + 1;  // espec.f:240
     const char* ef = r.efc.c_str();

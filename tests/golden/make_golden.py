@@ -32,7 +32,7 @@ Cases:
               propagation on, gzipped, as expected.txt.gz; --reftests-only
               [i ...] generates only these.  Tests 1 and 5 are left out: the
               executable stops in their .LANCZS diagonalisation (DSTEIN is
-              called with an illegal argument); test 2 runs with .MTRXDIAG.
+              called with an illegal argument); tests 2 and 3 run edited (REFTEST_EDITS).
 """
 import gzip
 import json
@@ -459,10 +459,22 @@ def case_deck(name):
         f.write("\n".join(lines[i - 1:]) + "\n")
 
 
-# test 2 runs with .MTRXDIAG in place of its .LANCZS: on its 560-point grid
-# the executable's LANCZS returns ghost eigenvalues (0.0132557 and 0.0190582
-# twice each) and propagates a vector of norm^2 1.94 as "state 2"
-REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag"]
+# Edited decks.  Test 2 runs with .MTRXDIAG in place of its .LANCZS: on its
+# 560-point grid the executable's LANCZS returns ghost eigenvalues (0.0132557
+# and 0.0190582 twice each) and propagates a vector of norm^2 1.94 as "state
+# 2".  Test 3 (.PPSOD with the dipole file dipol2.inp and populations of six
+# computed states) runs 40 fs instead of 2000 with its .GGAUS pulse moved into
+# that window (TP 10 fs, T0 20 fs), and with .MTRXDIAG: its LANCZS states above
+# the ground state include a ghost as well (test 9's table: 0.0275652).
+LANCZS_TO_MTRXDIAG = ("*TPDIAG\n.LANCZS", "*TPDIAG\n.MTRXDIAG")
+REFTEST_EDITS = {
+    "2_mtrxdiag": [LANCZS_TO_MTRXDIAG],
+    "3_short": [LANCZS_TO_MTRXDIAG, (" 0.0  2000.0  5D-5  10/", " 0.0  40.0  5D-5  10/"),
+                (" 1.5D+12  100.0  0.241  700.0  4.7124   1.0/",
+                 " 1.5D+12  10.0  0.241  20.0  4.7124   1.0/")],
+}
+REFTEST_FILES = {"3_short": ["dipol2.inp"]}
+REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag", "3_short"]
 
 
 def case_reftest(i):
@@ -470,14 +482,19 @@ def case_reftest(i):
     num = int(str(i).split("_")[0])
     with open(os.path.join(REF, "ttests", f"input.test{num}")) as f:
         deck = f.read()
-    if str(i).endswith("_mtrxdiag"):
-        assert ".LANCZS" in deck
-        deck = deck.replace("*TPDIAG\n.LANCZS", "*TPDIAG\n.MTRXDIAG")
+    for old, new in REFTEST_EDITS.get(str(i), []):
+        assert old in deck, (i, old)
+        deck = deck.replace(old, new)
     d = os.path.join(OUT, f"reftest{i}")
     os.makedirs(d, exist_ok=True)
     with open(os.path.join(d, "input.spc"), "w") as f:
         f.write(deck)
-    out = run_deck(deck, {}, timeout=3600)
+    files = {}
+    for name in REFTEST_FILES.get(str(i), []):
+        src = os.path.join(REF, "ttests", name)
+        shutil.copyfile(src, os.path.join(d, name))
+        files[name] = src
+    out = run_deck(deck, files, timeout=3600)
     lines = out.splitlines()
     k = max(j for j, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
     with gzip.open(os.path.join(d, "expected.txt.gz"), "wt") as f:

@@ -37,7 +37,7 @@ def refused(tmp_path, text, files=None):
     ("**TD", "**TI\n*COLLISION_ENERGY\n 1.0/\n**TD", "keyword *COLLISION_ENERGY"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n*PRPTOL", "*PULSE_AND_DIPOLE"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.LASER\n 1 2 3 4 5/\n.NULL\n*PRPTOL", "pulse is not known"),
-    ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.READ\ndm.inp\n*PRPTOL", "dipole .READ"),
+    ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.GET\ndm.inp\n*PRPTOL", "dipole moment .GET"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.EXP\n 0.5/\n*PRPTOL", "constants"),
 ])
 def test_uncovered_decks_are_refused(tmp_path, old, new, why):
@@ -254,3 +254,18 @@ def test_calc_projections_on_computed_states(tmp_path):
             assert msg is None or "device memory" in msg, (nist, proj, msg)
         else:
             assert msg is not None and "*NPROJECTIONS" in msg, (nist, proj, msg)
+
+
+def test_dipole_file_is_read(tmp_path):
+    """*PULSE_AND_DIPOLE .READ (rdinput.f:571-572, dipl.f:81-82): the dipole
+    file's name is the record after .READ, relative to the deck; a missing
+    file is reported after the deck's own .FILE is read, before any device
+    work."""
+    src = os.path.join(HERE, "golden", "deck_ppsod")
+    text = open(os.path.join(src, "input.spc")).read()
+    i = text.index("*PULSE_AND_DIPOLE")
+    j = text.index("*", i + 1)
+    pulse = "*PULSE_AND_DIPOLE\n.GAUS\n 5.0D7  0.1  2.5  0.15  0.0/\n.READ\nmu.inp\n"
+    files = {"wf_pot.inp": open(os.path.join(src, "wf_pot.inp")).read()}
+    msg = refused(tmp_path, text[:i] + pulse + text[j:], files)
+    assert "dipole file" in msg and "mu.inp" in msg, msg

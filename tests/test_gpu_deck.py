@@ -104,11 +104,14 @@ def test_deck_matches_executable(capfd, name):
 #     its Krylov matrices to ABSTOL = 1e-6 only, so its norm falls by 3e-6
 #     over the 125 thousand steps and C(t) moves by up to 4.5e-6; its total
 #     correlation is corrupted (samples overwritten, see check_sil).
-# .PSOD and .PPSOD (tests 9, 11) need none, nor test 2 (.PPSOD,
-# six populations on computed states, HWHM shifted by the computed E1I), run
-# with .MTRXDIAG: its own .LANCZS gives the executable ghost eigenvalues.
+# .PSOD and .PPSOD (tests 9, 11) need none, nor test 2 (.PPSOD, six
+# populations on computed states, HWHM shifted by the computed E1I) and test
+# 3 (.PPSOD, a .GGAUS pulse on the dipole file dipol2.inp, six populations;
+# 40 fs of its 2000), both run with .MTRXDIAG: their own .LANCZS gives the
+# executable ghost eigenvalues.
 REFTESTS = {"reftest9": 0.0, "reftest10": 8e-6, "reftest11": 0.0, "reftest12": 4e-7,
-            "reftest6": 4e-7, "reftest13": 5e-6, "reftest14": 5e-6, "reftest2_mtrxdiag": 0.0}
+            "reftest6": 4e-7, "reftest13": 5e-6, "reftest14": 5e-6, "reftest2_mtrxdiag": 0.0,
+            "reftest3_short": 0.0}
 
 
 @pytest.mark.parametrize("name", sorted(REFTESTS))
