@@ -282,12 +282,15 @@ std::string fort_e(double x, int w, int d) {
   return std::string(w - out.size(), ' ') + out;
 }
 
-// MAKECST (makecst.f:82-175) for a .1D deck: the constants of an analytic
-// potential to atomic units, the first prefix that matches deciding, with its
-// FORMAT 1020/1031/1041/1051/1061 lines.  sm1: the mass in electron masses.
-void makecst_1d(const std::string& potch, double sm1, std::vector<double>& c) {
+// MAKECST (makecst.f:82-340) for a .1D or .2D deck: the constants of an
+// analytic potential to atomic units, the first prefix that matches deciding,
+// with its FORMAT 1020/1031/1041/1051/1061/1071 lines.  sm: the masses in
+// electron masses.
+void makecst(int nd, const std::string& potch, const double* sm, std::vector<double>& c) {
   const double ffreq = 4.556335252750e-6, ccgs = 2.99792458e10, eev = 27.211383411;
   const double tau = 2.4188843243e-17, twopi = 6.2831853071795864769252867663;
+  const double ecm = 2.19474631371017e5, pi = 3.14159265358979323846;
+  const double sm1 = sm[0];
   c.resize(14, 0.0);
   auto is = [&](const char* p) { return starts(potch, p); };
   auto l1031 = [&](int i, double a, double b) {
@@ -299,14 +302,119 @@ void makecst_1d(const std::string& potch, double sm1, std::vector<double>& c) {
                 fort_e(a, 12, 6).c_str(), i, fort_e(b, 12, 6).c_str(), i,
                 fort_e(d, 12, 6).c_str());
   };
-  auto l1051 = [&]() {
-    std::printf(" R(min)_1/a.u. = %s; R(max)_1/a.u. = %s; Const_1/a.u. = %s\n",
-                fort_e(c[0], 12, 6).c_str(), fort_e(c[1], 12, 6).c_str(),
-                fort_e(c[2], 12, 6).c_str());
+  auto l1051i = [&](int i, double a, double b, double d) {
+    std::printf(" R(min)_%d/a.u. = %s; R(max)_%d/a.u. = %s; Const_%d/a.u. = %s\n", i,
+                fort_e(a, 12, 6).c_str(), i, fort_e(b, 12, 6).c_str(), i,
+                fort_e(d, 12, 6).c_str());
   };
+  auto l1051 = [&]() { l1051i(1, c[0], c[1], c[2]); };
   auto l1061 = [&]() { std::printf(" Const_1/a.u. = %s\n", fort_e(c[0], 12, 6).c_str()); };
   const char* au = " These parameters were already inputed in a.u.\n";
+  const char* bad = "<<<>>> Potential parameter converting error <<<>>>\n";
   auto sq = [](double x) { return x * x; };
+  if (nd == 2) {
+    if (is(".OHS")) {
+      const double fk1 = sq(((c[1] * ccgs) * tau) * twopi) * sm[0];
+      const double fk2 = sq(((c[3] * ccgs) * tau) * twopi) * sm[1];
+      c[0] = c[0] / kA0A;
+      c[2] = c[2] / kA0A;
+      c[1] = fk1;
+      c[3] = fk2;
+      l1031(1, c[0], c[1]);
+      l1031(2, c[2], c[3]);
+    } else if (is(".LSM_au")) {
+      std::printf("%s", au);
+      l1041(1, c[0], c[1], c[2]);
+      l1041(2, c[0], c[3], c[4]);
+      l1041(3, c[5], c[6], c[7]);
+    } else if (is(".LSM")) {
+      c[0] = c[0] / kA0A;
+      c[5] = c[5] / kA0A;
+      c[1] = c[1] * kA0A;
+      c[3] = c[3] * kA0A;
+      c[6] = c[6] * kA0A;
+      c[2] = c[2] / ecm;
+      c[4] = c[4] / ecm;
+      c[7] = c[7] / ecm;
+      l1041(1, c[0], c[1], c[2]);
+      l1041(2, c[0], c[3], c[4]);
+      l1041(3, c[5], c[6], c[7]);
+    } else if (is(".LS_au")) {
+      std::printf("%s", au);
+      l1041(1, c[0], c[1], c[2]);
+      l1041(2, c[0], c[3], c[4]);
+    } else if (is(".LS")) {
+      c[0] = c[0] / kA0A;
+      c[1] = c[1] * kA0A;
+      c[3] = c[3] * kA0A;
+      c[2] = c[2] / ecm;
+      c[4] = c[4] / ecm;
+      l1041(1, c[0], c[1], c[2]);
+      l1041(2, c[0], c[3], c[4]);
+    } else if (is(".LBH")) {  // .LBH and .LBH_CC
+      std::printf(" Not implemented!\n");
+      throw DeckError{"potential " + potch + ": MAKECST stops (not implemented, makecst.f)"};
+    } else if (is(".LEPS_CC_Dalpha_au") || is(".LEPS_Dalpha_au")) {
+      std::printf("%s", au);
+      l1041(1, c[0], c[1], c[2]);
+      l1041(2, c[3], c[4], c[5]);
+      l1041(3, c[6], c[7], c[8]);
+      std::printf(" a = %s; b = %s; c = %s\n", fort_e(c[9], 10, 4).c_str(),
+                  fort_e(c[10], 10, 4).c_str(), fort_e(c[11], 10, 4).c_str());
+      c[12] = pi * c[12] / 1.8e2;
+      std::printf(" Angle (rad) =%s\n", list_real(c[12]).c_str());
+    } else if (is(".LEPS_CC_Dalpha") || is(".LEPS_Dalpha")) {
+      for (int k = 0; k < 9; k += 3) {
+        c[k] = c[k] / kA0A;
+        c[k + 1] = c[k + 1] * kA0A;
+        c[k + 2] = c[k + 2] / eev;
+      }
+      l1041(1, c[0], c[1], c[2]);
+      l1041(2, c[3], c[4], c[5]);
+      l1041(3, c[6], c[7], c[8]);
+      std::printf(" a = %s; b = %s; c = %s\n", fort_e(c[9], 10, 4).c_str(),
+                  fort_e(c[10], 10, 4).c_str(), fort_e(c[11], 10, 4).c_str());
+    } else if (is(".BARRIERXY_au") || is(".WELLXY_au")) {
+      std::printf("%s", au);
+      l1051i(1, c[0], c[1], c[2]);
+      l1051i(2, c[3], c[4], c[5]);
+    } else if (is(".BARRIERX_au") || is(".BARRIERY_au") || is(".WELLX_au") || is(".WELLY_au")) {
+      std::printf("%s", au);
+      l1051i(is(".BARRIERX") || is(".WELLX") ? 1 : 2, c[0], c[1], c[2]);
+    } else if (is(".BARRIER_au") || is(".WELL_au")) {
+      std::printf("%s", au);
+      l1051i(1, c[0], c[1], c[4]);
+      l1051i(2, c[2], c[3], c[4]);
+    } else if (is(".CONST_au")) {
+      std::printf("%s", au);
+      l1061();
+    } else if (is(".BARRIERXY") || is(".WELLXY")) {
+      for (int k = 0; k < 6; k += 3) {
+        c[k] = c[k] / kA0A;
+        c[k + 1] = c[k + 1] / kA0A;
+        c[k + 2] = c[k + 2] / eev;
+      }
+      l1051i(1, c[0], c[1], c[2]);
+      l1051i(2, c[3], c[4], c[5]);
+    } else if (is(".BARRIERX") || is(".BARRIERY") || is(".WELLX") || is(".WELLY")) {
+      c[0] = c[0] / kA0A;
+      c[1] = c[1] / kA0A;
+      c[2] = c[2] / eev;
+      l1051i(is(".BARRIERX") || is(".WELLX") ? 1 : 2, c[0], c[1], c[2]);
+    } else if (is(".BARRIER") || is(".WELL")) {
+      for (int k = 0; k < 4; ++k) c[k] = c[k] / kA0A;
+      c[4] = c[4] / eev;
+      l1051i(1, c[0], c[1], c[4]);
+      l1051i(2, c[2], c[3], c[4]);
+    } else if (is(".CONST") || is(".FREE")) {
+      c[0] = c[0] / eev;
+      l1061();
+    } else {
+      // makecst.f:337-339: the message, and the constants stay as read
+      std::printf("%s", bad);
+    }
+    return;
+  }
   if (is(".OHS")) {
     const double fk1 = sq(((c[1] * ccgs) * tau) * twopi) * sm1;
     c[0] = c[0] / kA0A;
@@ -358,7 +466,7 @@ void makecst_1d(const std::string& potch, double sm1, std::vector<double>& c) {
     c[0] = c[0] / eev;
     l1061();
   } else {
-    std::printf("<<<>>> Potential parameter converting error <<<>>>\n");
+    std::printf("%s", bad);
     throw DeckError{"potential " + potch + ": no unit conversion for .1D (makecst.f:170-174)"};
   }
 }
@@ -429,7 +537,8 @@ Run read_run(const Deck& d) {
           if ((int)n.size() < r.nd) throw DeckError{"*DIMENSION: grid sizes missing"};
           for (int a = 0; a < r.nd; ++a) r.np[a] = (int)n[a];
         } else if (k == "*POTENTIAL") {
-          r.potch = r.potchf = upper(rec(v, 0, "*POTENTIAL"));
+          // the names are compared as written (makecst.f: '.MORSE_Dalpha_au', ...)
+          r.potch = r.potchf = rec(v, 0, "*POTENTIAL");
           if (starts(r.potch, ".FILE")) {
             r.potfile = rec(v, 1, "*POTENTIAL");
           } else {
@@ -478,7 +587,7 @@ Run read_run(const Deck& d) {
         if (k == "*INITIAL_POTENTIAL" || k == "*INITIAL_CONDITION" || k == "*INITIAL_WP" ||
             k == "*INITIAL_WF" || k == "*INITIAL_WAVE_FUNCTION" || k == "*WAVE_FUNCTION" ||
             k == "*WAVE_PACKET" || k == "*POTENTIAL") {
-          r.potch = upper(rec(v, 0, k.c_str()));
+          r.potch = rec(v, 0, k.c_str());
           if (starts(r.potch, ".FILE")) r.potfile = rec(v, 1, k.c_str());
           else r.csti = numbers(rec(v, 1, k.c_str()));
         } else if (k == "*TPDIAG") {
@@ -558,7 +667,7 @@ Run read_run(const Deck& d) {
               throw DeckError{"*PULSE_AND_DIPOLE: dipole constants missing"};
           }
         } else if (k == "*ABSORBING") {
-          r.tpabsor = upper(rec(v, 0, "*ABSORBING"));
+          r.tpabsor = rec(v, 0, "*ABSORBING");  // '.SMOOTHW_au' as written
           if (starts(r.tpabsor, ".NULL")) continue;
           if (!starts(r.tpabsor, ".SMOOTHW") && !starts(r.tpabsor, ".SMRS") &&
               !starts(r.tpabsor, ".VOPTIC"))
@@ -611,9 +720,11 @@ Run read_run(const Deck& d) {
   if (!starts(r.tptrans, ".ONE"))
     throw DeckError{"one propagated state (*TPTRANS .ONE) is covered"};
   if (r.calc()) {
-    if (r.nd != 1)
-      throw DeckError{"computed initial states (.CALC) are covered on .1D grids"};
-    if (!(r.gxf[0] > r.gxi[0])) throw DeckError{"*GRID_RANGES: XI < XF is needed"};
+    if (r.nd > 2)
+      throw DeckError{"computed initial states (.CALC) are covered on .1D and .2D grids (the "
+                      "GPU eigensolver's)"};
+    for (int a = 0; a < r.nd; ++a)
+      if (!(r.gxf[a] > r.gxi[a])) throw DeckError{"*GRID_RANGES: XI < XF is needed"};
     // espec.f:1083: the propagated state is column NISPG - IIL + 1 of the NIS
     // computed ones (IIL, NISPG counted from 1 there)
     if (r.nis < 1 || r.iil < 0 || r.prpgstate < r.iil || r.prpgstate >= r.iil + r.nis)
@@ -743,22 +854,31 @@ struct DevBufs {
 // (EIGVC(., K), espec.f:1262-1265) and the final potential; eigvc: the NIS
 // states, n each; r.e1i = E1I (espec.f:927).
 FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<double>& eigvc) {
-  const int n = r.np[0];
+  const int nd = r.nd;
+  int n = 1;
   FileData fd;
-  sm[0] = kAmu * r.sm[0];
-  sh[0] = ((r.gxf[0] - r.gxi[0]) / (n - 1.0)) / kA0A;
-  fd.xi[0] = r.gxi[0] / kA0A;
-  fd.xf[0] = r.gxf[0] / kA0A;
-  shm[0] = 1.0 / ((((24.0 * sm[0]) * r.smf[0]) * sh[0]) * sh[0]);  // espec.f:630
+  for (int a = 0; a < nd; ++a) {
+    n *= r.np[a];
+    sm[a] = kAmu * r.sm[a];
+    sh[a] = ((r.gxf[a] - r.gxi[a]) / (r.np[a] - 1.0)) / kA0A;
+    fd.xi[a] = r.gxi[a] / kA0A;
+    fd.xf[a] = r.gxf[a] / kA0A;
+    shm[a] = 1.0 / ((((24.0 * sm[a]) * r.smf[a]) * sh[a]) * sh[a]);  // espec.f:630
+  }
+  // espec.f:252-258, 613-616: a third mass (in atomic units) for the
+  // mass-scaled coordinates of .LEPS_CC on a .2D grid
+  const bool cc = nd == 2 && (starts(r.potch, ".LEPS_CC") || starts(r.potchf, ".LEPS_CC"));
+  sm[2] = cc ? kAmu * r.sm[2] : r.sm[2];
   std::printf(" Initial potential:\n");
-  makecst_1d(r.potch, sm[0], r.csti);
+  makecst(nd, r.potch, sm, r.csti);
   std::printf(" Final potential:\n");
-  makecst_1d(r.potchf, sm[0], r.cstf);
+  makecst(nd, r.potchf, sm, r.cstf);
   std::printf(" \n Units converted.\n");
-  const int ki = espec_pot_kind(r.potch.c_str(), r.potch.size(), 1);
-  const int kf = espec_pot_kind(r.potchf.c_str(), r.potchf.size(), 1);
+  const int ki = espec_pot_kind(r.potch.c_str(), r.potch.size(), nd);
+  const int kf = espec_pot_kind(r.potchf.c_str(), r.potchf.size(), nd);
   if (!ki || !kf)
-    throw DeckError{"potential " + (ki ? r.potchf : r.potch) + " is not a .1D form (pot1d)"};
+    throw DeckError{"potential " + (ki ? r.potchf : r.potch) + " is not a form of " + r.dim +
+                    " grids (potfuncs.f)"};
   // espec.f:879-905: *CHANGE on a grid above 3e4 points switches to LANCZSG,
   // which keeps the ground state only
   std::string tpdiag = r.tpdiag;
@@ -788,9 +908,15 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   double* d_L = dev.alloc((size_t)m * n);
   double* d_w = dev.alloc(n);
   double xmin = 0.0, xminb = 0.0;
+  // GVPOT (gvpot.f:21-64): XMIN is set for .1D grids only
+  auto gvpot = [&](int kind, const double* cst, double* d_v, double* xm) {
+    return nd == 1 ? espec_gvpot_1d(1, &n, fd.xi, sh, kind, cst, r.shiftp ? 1 : 0, d_v, xm,
+                                    nullptr)
+                   : espec_gvpot_nd(nd, r.np, fd.xi, sh, sm, kind, cst, r.shiftp ? 1 : 0, 0,
+                                    d_v, nullptr);
+  };
   msg1003("Generating initial potential...");
-  if (espec_gvpot_1d(1, &n, fd.xi, sh, ki, r.csti.data(), r.shiftp ? 1 : 0, d_vi, &xmin,
-                     nullptr))
+  if (gvpot(ki, r.csti.data(), d_vi, &xmin))
     throw DeckError{std::string("GVPOT: ") + espec_last_error()};
   std::printf(" Initial potential generated.\n");
   msg1003("Calculating eigenvalue(s) and eigenvector(s)");
@@ -804,9 +930,9 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
     throw DeckError{"copy of the initial potential"};
   double vmax = 0.0;
   for (double x : vi) vmax = std::max(vmax, std::fabs(x));
-  const double tol = 1e-12 * std::max(1.0, 64.0 * shm[0] + vmax);
-  const int npp[2] = {n, 1};
-  const double shmp[2] = {shm[0], 0.0};
+  const double tol = 1e-12 * std::max(1.0, 64.0 * (shm[0] + shm[1]) + vmax);
+  const int npp[2] = {r.np[0], nd == 2 ? r.np[1] : 1};
+  const double shmp[2] = {shm[0], nd == 2 ? shm[1] : 0.0};
   std::vector<double> eval(nst), resid(nst);
   eigvc.assign((size_t)nst * n, 0.0);
   if (espec_eig_lcg_start(d_start, n, nst, nullptr) ||
@@ -837,8 +963,7 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   std::printf(" \n");
   msg1003("   Generating final potential...");
   fd.vpot.resize(n);
-  if (espec_gvpot_1d(1, &n, fd.xi, sh, kf, r.cstf.data(), r.shiftp ? 1 : 0, d_vf, &xminb,
-                     nullptr) ||
+  if (gvpot(kf, r.cstf.data(), d_vf, &xminb) ||
       cudaMemcpy(fd.vpot.data(), d_vf, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
     throw DeckError{std::string("GVPOT: ") + espec_last_error()};
   if (std::fabs(xminb - xmin) < 1e-6)
@@ -886,7 +1011,7 @@ int run_deck(const std::string& deck_path) {
         r.al[a] = r.al[a] / kA0A;
         r.ar[a] = r.ar[a] / kA0A;
       }
-    sh[0] = ((r.gxf[0] - r.gxi[0]) / (n - 1.0)) / kA0A;
+    for (int a = 0; a < r.nd; ++a) sh[a] = ((r.gxf[a] - r.gxi[a]) / (r.np[a] - 1.0)) / kA0A;
     check_step(r, sh);
     fd = initial_state(r, sh, shm, sm, eigvc);
   } else {

@@ -26,6 +26,9 @@ Cases:
   deck_*      whole decks for the deck driver (input.spc, wf_pot.inp and the
               executable's output from the propagation on); --decks-only
               [name ...] generates only these (or the named ones).
+  calc2d_*    2D decks with computed initial states (.CALC, .MTRXDIAG) and the
+              executable's output, with its MAKECST lines (constants.txt);
+              --calc2d-only generates only these.
   reftest*    the reference's own test decks ttests/input.test<i> with an
               analytic .1D potential and a computed initial state (.CALC):
               the deck as input.spc and the executable's output from the
@@ -65,8 +68,8 @@ def run_deck(deck, files, timeout=600):
             else:
                 with open(dst, "w") as f:
                     f.write(src)
-        r = subprocess.run([BIN], cwd=d, capture_output=True, text=True, timeout=timeout)
-        return r.stdout
+        r = subprocess.run([BIN], cwd=d, capture_output=True, timeout=timeout)
+        return r.stdout.decode("utf-8", errors="replace")
     finally:
         shutil.rmtree(d, ignore_errors=True)
 
@@ -501,6 +504,126 @@ def case_reftest(i):
         f.write("\n".join(lines[k - 1:]) + "\n")
 
 
+# 2D decks with computed initial states (.CALC with .MTRXDIAG on a 32 x 32
+# grid): the harmonic .OHS surfaces in cm^-1 and angstrom, propagated on the
+# final surface from its second state with .PSIL; and a .MORSE pair whose
+# constants MAKECST leaves as written (it has no 2D .MORSE branch: the
+# message, then the constants in atomic units), grid ranges in bohr
+# ('*GRID_RANGES au'), with .PSOD.  (The executable's 2D .PFSPO diverges
+# from the first step on such a deck: its 2D kinetic table fills TC(1..NP1)
+# only.)
+CALC2D = {
+    "calc2d_ohs_psil": """*** eSPec input file ***
+**MAIN
+*TITLE
+ 2D harmonic surfaces, computed state 1, .PSIL
+*DIMENSION
+.2D
+ 32 32/
+*POTENTIAL
+.OHS
+ 1.14600  1943.79  1.14600  1700.00/
+ 1.21100  1629.23  1.18000  1800.00/
+*GRID_RANGES
+ 0.85  1.45  0.90  1.50/
+*MASS
+ 7.49D0  9.0D0/
+*TPCALC
+.SPECTRUM
+.TD
+*INIEIGVC
+.CALC
+*CHANGE
+.YES
+*PRTCRL
+.PARTIAL
+**TI
+*TPDIAG
+.MTRXDIAG
+*NIST
+ 3  0/
+**TD
+*PROPAG
+.PSIL
+ 0.0  4.0  2D-3  10/
+*PRPGSTATE
+ 1/
+*TPTRANS
+.ONE
+**SPECTRUM
+*FOURIER
+ 8/
+*WINDOWING
+.SG
+ 1D-3/
+**END
+""",
+    "calc2d_morse_psod": """*** eSPec input file ***
+**MAIN
+*TITLE
+ 2D Morse surfaces in atomic units, computed ground state, .PSOD
+*DIMENSION
+.2D
+ 32 32/
+*POTENTIAL
+.MORSE
+ 2.0  1.0  0.17  2.3  0.9  0.15/
+ 2.1  1.0  0.17  2.4  0.9  0.14/
+*GRID_RANGES au
+ 1.45  2.65  1.75  2.95/
+*MASS
+ 1.0D0  1.5D0/
+*TPCALC
+.SPECTRUM
+.TD
+*INIEIGVC
+.CALC
+*CHANGE
+.YES
+*PRTCRL
+.PARTIAL
+**TI
+*TPDIAG
+.MTRXDIAG
+*NIST
+ 1  0/
+**TD
+*PROPAG
+.PSOD
+ 0.0  5.0  2.5D-3/
+*PRPGSTATE
+ 0/
+*TPTRANS
+.ONE
+**SPECTRUM
+*FOURIER
+ 9/
+*WINDOWING
+.SG
+ 1D-3/
+**END
+""",
+}
+
+
+def case_calc2d(name):
+    deck = CALC2D[name]
+    d = os.path.join(OUT, name)
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "input.spc"), "w") as f:
+        f.write(deck)
+    out = run_deck(deck, {})
+    lines = out.splitlines()
+    k = max(j for j, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
+    with gzip.open(os.path.join(d, "expected.txt.gz"), "wt") as f:
+        f.write("\n".join(lines[k - 1:]) + "\n")
+    # MAKECST's lines, for the CPU test of the unit conversion
+    with open(os.path.join(d, "constants.txt"), "w") as f:
+        i = lines.index(" Initial potential:")
+        j = lines.index(" Units converted.")
+        f.write("\n".join(lines[i:j - 1]) + "\n")
+
+
 def psod_cases():
     vmeta = dict(absorb="VOPTIC_POLIN", voi=[-0.02, 2.0], al=1.6, ar=2.2)
     smeta = dict(absorb="SMOOTHW", voi=[0.05, 1.0], al=1.55, ar=2.3)
@@ -522,6 +645,10 @@ def save(cases, manifest):
 def main():
     if not os.path.exists(BIN):
         sys.exit("eSPec executable not found at " + BIN)
+    if "--calc2d-only" in sys.argv:
+        for name in CALC2D:
+            case_calc2d(name)
+        return
     if "--reftests-only" in sys.argv:
         picked = [a for a in sys.argv[1:] if a in map(str, REFTESTS)] or REFTESTS
         from concurrent.futures import ThreadPoolExecutor
@@ -569,6 +696,8 @@ def main():
         case_deck(name)
     for i in REFTESTS:
         case_reftest(i)
+    for name in CALC2D:
+        case_calc2d(name)
 
 
 if __name__ == "__main__":

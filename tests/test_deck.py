@@ -220,12 +220,13 @@ def test_calc_ohs_constants(tmp_path, capfd):
 
 
 @pytest.mark.parametrize("old,new,why", [
-    (".1D\n 256/", ".2D\n 64 64/", ".1D grids"),
+    (".1D\n 256/", ".3D\n 16 16 16/", ".2D grids"),
+    (".1D\n 256/", ".2D\n 64 64/", "XI < XF"),
     ("*NIST\n 1  0/", "*NIST\n 3  1/", "*PRPGSTATE must be one of"),
     ("*NIST\n 1  0/", "*NIST\n 17  0/", "16 lowest states"),
     (".LANCZS\n", ".JACOBI\n", "eigenvalue(s) and eigenvector(s)"),
     (".MORSE\n", ".DMORSE\n", "no unit conversion"),
-    (".MORSE\n", ".WELL\n", "not a .1D form"),
+    (".MORSE\n", ".WELL\n", "not a form of .1D grids"),
     (" 0.5  2.8/", " 2.8  0.5/", "XI < XF"),
     (" 1.21100  1629.23  17.74  1.0/\n", "", "missing record of *POTENTIAL"),
     (" 256/", " 20/", "grid step is above 4e-2"),
@@ -269,3 +270,18 @@ def test_dipole_file_is_read(tmp_path):
     files = {"wf_pot.inp": open(os.path.join(src, "wf_pot.inp")).read()}
     msg = refused(tmp_path, text[:i] + pulse + text[j:], files)
     assert "dipole file" in msg and "mu.inp" in msg, msg
+
+
+@pytest.mark.parametrize("name", ["calc2d_ohs_psil", "calc2d_morse_psod"])
+def test_calc_2d_constants(tmp_path, capfd, name):
+    """MAKECST's 2D branch (makecst.f:176-340): the lines the executable
+    prints for the two 2D .CALC decks -- .OHS in cm^-1 with two masses, and a
+    .MORSE pair, for which MAKECST has no 2D branch (the message; the
+    constants stay in atomic units)."""
+    d = os.path.join(HERE, "golden", name)
+    msg = run_calc(tmp_path, open(os.path.join(d, "input.spc")).read())
+    assert msg is None or "device memory" in msg, msg
+    out = capfd.readouterr().out.split("\n")
+    want = open(os.path.join(d, "constants.txt")).read().rstrip("\n").split("\n")
+    i = out.index(" Initial potential:")
+    assert out[i:i + len(want)] == want
