@@ -1,12 +1,12 @@
 // deck.cpp -- eSPec input decks run through the GPU propagators: the part of
 // the driver (espec.f) from the input deck (rdinput.f) to the spectrum, for
 // time-dependent runs of one packet, with a tabulated potential and its
-// eigenvector or with an analytic .1D potential and a computed eigenstate.
+// eigenvector or with an analytic .1D/.2D potential and a computed eigenstate.
 //
 // Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL (.FILE; the analytic
-// .1D forms of MAKECST with their initial and final constant records),
+// .1D/.2D forms of MAKECST with their initial and final constant records),
 // *GRID_RANGES, *MASS, *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION),
-// *INIEIGVC (.GETR; .CALC on .1D grids), *CHANGE, *SHIFT_POTENTIAL, *PRTCRL,
+// *INIEIGVC (.GETR; .CALC on .1D and .2D grids), *CHANGE, *SHIFT_POTENTIAL, *PRTCRL,
 // *MASS_FACTOR, *DONOTSTOP; **TI *TPDIAG (.MTRXDIAG, .LANCZS, .LANCZSG), *NIST,
 // *ABSTOL and an initial potential of its own; **TD *PROPAG (.PFSPO, .PFSOD,
 // .PSIL, .PSOD, .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE, *TPTRANS .ONE, *PRPTOL,
@@ -16,7 +16,7 @@
 // LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING,
 // *HWHM.  Print and output-file switches
 // (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored: no files are written
-// (nor the unit-21 table .EXP+ writes).  Anything else -- 2D/3D computed
+// (nor the unit-21 table .EXP+ writes).  Anything else -- 3D computed
 // states, the TI formalism, several transitions -- is refused with a
 // message: there is no CPU path.
 //
@@ -842,7 +842,7 @@ struct DevBufs {
   }
 };
 
-// The time-independent part of espec.f for an analytic .1D potential: the
+// The time-independent part of espec.f for an analytic .1D or .2D potential: the
 // grid of *GRID_RANGES in bohr (espec.f:345, 618-641), MAKECST of both constant
 // records (espec.f:683-690), GVPOT of the initial potential (espec.f:865-869),
 // its eigenstates IIL..IIU (espec.f:872-927) and GVPOT of the final potential
