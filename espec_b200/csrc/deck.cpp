@@ -494,9 +494,13 @@ struct Run {
   // **TI (rdinput.f:370-381; defaults espec.f:129, 141-157): NIS states from
   // the IIL-th, counted from 0 as in the deck
   std::string tpdiag = ".MTRXDIAG";
-  int nis = 1, iil = 0;
+  int nis = 1, iil = 0, nfs = 0, ifl = 0;  // *NIST; *NFST (the final states of .TI)
   double abstol = 1e-6;
+  std::string fileaux;  // .ONLYSPEC: the output file holding a correlation function
   bool calc() const { return starts(inieigvc, ".CALC"); }
+  bool onlyspec() const { return starts(tpclc, ".ONLYSPEC"); }
+  bool energy() const { return starts(tpclc, ".ENERGY"); }
+  bool ti_form() const { return starts(tdi, ".TI"); }  // .ENERGY or .SPECTRUM .TI
 };
 
 const std::string& rec(const std::vector<std::string>* r, size_t i, const char* key) {
@@ -564,6 +568,8 @@ Run read_run(const Deck& d) {
           r.tpclc = upper(rec(v, 0, "*TPCALC"));
           if (starts(r.tpclc, ".SPECTRUM")) r.tdi = upper(rec(v, 1, "*TPCALC"));
           else if (starts(r.tpclc, ".PROPAGATION") || starts(r.tpclc, ".CORRELATION")) r.tdi = ".TD";
+          else if (starts(r.tpclc, ".ONLYSPEC")) r.fileaux = rec(v, 1, "*TPCALC");  // TDI .NC
+          else if (starts(r.tpclc, ".ENERGY")) r.tdi = ".TI";
           else throw DeckError{"*TPCALC " + r.tpclc + " is not covered"};
         } else if (k == "*INIEIGVC") {
           r.inieigvc = upper(rec(v, 0, "*INIEIGVC"));
@@ -599,8 +605,13 @@ Run read_run(const Deck& d) {
           r.iil = (int)x[1];
         } else if (k == "*ABSTOL") {
           r.abstol = numbers(rec(v, 0, "*ABSTOL")).at(0);
-        } else if (k == "*NFST" || k == "*SEED" || k == "*MAXINT") {
-          continue;  // final states (the TI formalism); the seed and length of LANCZSG
+        } else if (k == "*NFST") {
+          const std::vector<double> x = numbers(rec(v, 0, "*NFST"));
+          if (x.size() < 2) throw DeckError{"*NFST: NFS IFL"};
+          r.nfs = (int)x[0];
+          r.ifl = (int)x[1];
+        } else if (k == "*SEED" || k == "*MAXINT") {
+          continue;  // the seed and the length of LANCZSG's iterations
         } else {
           throw DeckError{"keyword " + k + " of **TI is not covered"};
         }
@@ -703,6 +714,7 @@ Run read_run(const Deck& d) {
       }
     }
   }
+  if (r.onlyspec()) return r;  // no grid, potential or propagation (espec.f:602)
   const bool file_i = starts(r.potch, ".FILE"), file_f = starts(r.potchf, ".FILE");
   if (starts(r.potch, ".NULL") || starts(r.potchf, ".NULL"))
     throw DeckError{"*POTENTIAL is missing"};
@@ -727,10 +739,13 @@ Run read_run(const Deck& d) {
       if (!(r.gxf[a] > r.gxi[a])) throw DeckError{"*GRID_RANGES: XI < XF is needed"};
     // espec.f:1083: the propagated state is column NISPG - IIL + 1 of the NIS
     // computed ones (IIL, NISPG counted from 1 there)
-    if (r.nis < 1 || r.iil < 0 || r.prpgstate < r.iil || r.prpgstate >= r.iil + r.nis)
+    if (r.nis < 1 || r.iil < 0 ||
+        (!r.ti_form() && (r.prpgstate < r.iil || r.prpgstate >= r.iil + r.nis)))
       throw DeckError{"*PRPGSTATE must be one of the states *NIST computes"};
-    if (r.iil + r.nis > 16 || r.prpgstate >= 16)
-      throw DeckError{"*NIST: the GPU eigensolver computes the 16 lowest states at most"};
+    if (r.iil + r.nis > 16 || r.prpgstate >= 16 || r.ifl + r.nfs > 16)
+      throw DeckError{"*NIST, *NFST: the GPU eigensolver computes the 16 lowest states at most"};
+    if (r.ti_form() && !r.energy() && (r.nfs < 1 || r.ifl < 0))
+      throw DeckError{"*NFST: the .TI spectrum needs final states"};
     if (!starts(r.tpdiag, ".MTRXDIAG") && !starts(r.tpdiag, ".LANCZS"))
       throw DeckError{"*TPDIAG " + r.tpdiag + ": initial eigenvalue(s) and eigenvector(s) "
                       "error (espec.f:920-925)"};
@@ -740,8 +755,12 @@ Run read_run(const Deck& d) {
   if (starts(r.tpdipl, ".EXP+") && !r.calc())
     throw DeckError{"dipole .EXP+ is normalised at the final potential's Re (CSTF(1), dipl.f), "
                     "which a .FILE potential leaves at zero"};
-  if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD"))
-    throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": only .TD is covered"};
+  if (starts(r.tpclc, ".SPECTRUM") && !starts(r.tdi, ".TD") && !starts(r.tdi, ".TI"))
+    throw DeckError{"*TPCALC .SPECTRUM " + r.tdi + ": .TD and .TI are covered"};
+  if (r.ti_form()) {
+    if (!r.calc()) throw DeckError{"the .TI formalism computes the states: *INIEIGVC .CALC"};
+    return r;  // no propagation
+  }
   if (!starts(r.tppropg, ".PFSPO") && !starts(r.tppropg, ".PFSOD") &&
       !starts(r.tppropg, ".PSIL") && !starts(r.tppropg, ".PSOD") && !starts(r.tppropg, ".PPSOD") &&
       !starts(r.tppropg, ".PPSIL") && !starts(r.tppropg, ".PPLNZ"))
@@ -814,10 +833,10 @@ void total_correlation(int mc, const double* cr, const double* ci, std::vector<d
 
 // the "Correlation Function:" block (FORMAT 1041 / 1042)
 std::string correlation_table(int mc, double tf, const std::vector<double>& cu,
-                              const std::vector<double>& cv) {
+                              const std::vector<double>& cv, double dtf = 0.0) {
   std::string out = " \n Correlation Function:\n \"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\n";
   out += "       *t/fs*       *C(t)r*       *C(t)i*\n";
-  const double dtf = tf / mc;
+  if (dtf == 0.0) dtf = tf / mc;  // espec.f:1548 (GETCORR's DTF for .ONLYSPEC)
   char buf[128];
   for (int i = 1; i <= 2 * mc; ++i) {
     const double t = -tf + (i - 1.0) * dtf;
@@ -894,17 +913,19 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
     std::printf(" -> Total number of eigenvectors changed to %11d\n", 1);
     if (r.prpgstate != 0) throw DeckError{".LANCZSG keeps the ground state: *PRPGSTATE 0"};
   }
-  const int nst = std::max(iil + nis, r.prpgstate + 1);  // states 0 .. nst-1
+  const int nst = std::max(iil + nis, r.ti_form() ? 1 : r.prpgstate + 1);  // states 0 .. nst-1
+  const int nstf = r.ti_form() ? r.ifl + r.nfs : 0;  // final states of .TI
+  const int nbuf = std::max(nst, nstf);
   const int m = std::min(40, n);
   if (m < 2) throw DeckError{"the grid needs two points at least"};
   DevBufs dev;
   double* d_vi = dev.alloc(n);
   double* d_vf = dev.alloc(n);
-  double* d_start = dev.alloc((size_t)nst * n);
-  double* d_vec = dev.alloc((size_t)nst * n);
-  double* d_eval = dev.alloc(nst);
-  double* d_resid = dev.alloc(nst);
-  int* d_mv = (int*)dev.alloc(nst);
+  double* d_start = dev.alloc((size_t)nbuf * n);
+  double* d_vec = dev.alloc((size_t)nbuf * n);
+  double* d_eval = dev.alloc(nbuf);
+  double* d_resid = dev.alloc(nbuf);
+  int* d_mv = (int*)dev.alloc(nbuf);
   double* d_L = dev.alloc((size_t)m * n);
   double* d_w = dev.alloc(n);
   double xmin = 0.0, xminb = 0.0;
@@ -914,6 +935,39 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
                                     nullptr)
                    : espec_gvpot_nd(nd, r.np, fd.xi, sh, sm, kind, cst, r.shiftp ? 1 : 0, 0,
                                     d_v, nullptr);
+  };
+  // the lowest ns states of the potential on the device, to a residual of
+  // 1e-12 ||H||; false if one did not converge
+  const int npp[2] = {r.np[0], nd == 2 ? r.np[1] : 1};
+  const double shmp[2] = {shm[0], nd == 2 ? shm[1] : 0.0};
+  auto solve = [&](const double* d_v, int ns, std::vector<double>& ev, std::vector<double>& vec) {
+    std::vector<double> v(n), resid(ns);
+    if (cudaMemcpy(v.data(), d_v, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw DeckError{"copy of a potential"};
+    double vmax = 0.0;
+    for (double x : v) vmax = std::max(vmax, std::fabs(x));
+    const double tol = 1e-12 * std::max(1.0, 64.0 * (shm[0] + shm[1]) + vmax);
+    ev.assign(ns, 0.0);
+    vec.assign((size_t)ns * n, 0.0);
+    if (espec_eig_lcg_start(d_start, n, ns, nullptr) ||
+        espec_eig_solve_dev(1, npp, shmp, d_v, d_start, ns, m, tol, 20000, d_vec, d_eval,
+                            d_resid, d_mv, d_L, d_w, nullptr) ||
+        cudaMemcpy(ev.data(), d_eval, sizeof(double) * ns, cudaMemcpyDeviceToHost) !=
+            cudaSuccess ||
+        cudaMemcpy(resid.data(), d_resid, sizeof(double) * ns, cudaMemcpyDeviceToHost) !=
+            cudaSuccess ||
+        cudaMemcpy(vec.data(), d_vec, sizeof(double) * ns * n, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+      throw DeckError{std::string("eigenstates: ") + espec_last_error()};
+    bool ok = true;
+    for (int j = 0; j < ns; ++j) ok = ok && resid[j] <= tol;
+    return ok;
+  };
+  // FORMAT 1014/1015 rows of states j0 .. j0+cnt-1
+  auto table = [&](const std::vector<double>& ev, int j0, int cnt) {
+    for (int j = j0; j < j0 + cnt; ++j)
+      std::printf(" |   %3d        |  %s  |\n ---------------------------------\n", j,
+                  fort_e(ev[j], 12, 6).c_str());
   };
   msg1003("Generating initial potential...");
   if (gvpot(ki, r.csti.data(), d_vi, &xmin))
@@ -925,41 +979,22 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
                        : starts(tpdiag, ".LANCZSG") ? "Using interative lanczos tri-diagonalization procedure,"
                                                     : "Using lanczos tri-diagonalization procedure,");
   std::fflush(stdout);
-  std::vector<double> vi(n);
-  if (cudaMemcpy(vi.data(), d_vi, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
-    throw DeckError{"copy of the initial potential"};
-  double vmax = 0.0;
-  for (double x : vi) vmax = std::max(vmax, std::fabs(x));
-  const double tol = 1e-12 * std::max(1.0, 64.0 * (shm[0] + shm[1]) + vmax);
-  const int npp[2] = {r.np[0], nd == 2 ? r.np[1] : 1};
-  const double shmp[2] = {shm[0], nd == 2 ? shm[1] : 0.0};
-  std::vector<double> eval(nst), resid(nst);
-  eigvc.assign((size_t)nst * n, 0.0);
-  if (espec_eig_lcg_start(d_start, n, nst, nullptr) ||
-      espec_eig_solve_dev(1, npp, shmp, d_vi, d_start, nst, m, tol, 20000, d_vec, d_eval,
-                          d_resid, d_mv, d_L, d_w, nullptr) ||
-      cudaMemcpy(eval.data(), d_eval, sizeof(double) * nst, cudaMemcpyDeviceToHost) !=
-          cudaSuccess ||
-      cudaMemcpy(resid.data(), d_resid, sizeof(double) * nst, cudaMemcpyDeviceToHost) !=
-          cudaSuccess ||
-      cudaMemcpy(eigvc.data(), d_vec, sizeof(double) * nst * n, cudaMemcpyDeviceToHost) !=
-          cudaSuccess)
-    throw DeckError{std::string("initial eigenstates: ") + espec_last_error()};
-  bool ok = true;
-  for (int j = 0; j < nst; ++j) ok = ok && resid[j] <= tol;
-  if (ok) {
+  std::vector<double> eval;
+  if (solve(d_vi, nst, eval, eigvc)) {
     std::printf(" \n Eigenvalues:\n \"\"\"\"\"\"\"\"\"\"\"\"\n");
     std::printf(" ---------------------------------\n");
     std::printf(" |  Eigenstate  |  Eigenvalues   |\n =================================\n");
-    for (int j = iil; j < iil + nis; ++j)  // FORMAT 1015, 1014
-      std::printf(" |   %3d        |  %s  |\n ---------------------------------\n", j,
-                  fort_e(eval[j], 12, 6).c_str());
+    table(eval, iil, nis);
   } else {
     std::printf(" <<<>>> It wasn`t possible obtain eignvalues and eignvectors correctly <<<>>>\n"
                 " Exiting.\n");
     if (r.fstop) throw DeckError{"the initial eigenstates did not converge"};
   }
-  r.e1i = eval[r.prpgstate] * 27.2113834;
+  if (!r.ti_form()) r.e1i = eval[r.prpgstate] * 27.2113834;
+  if (r.energy()) {  // espec.f:954: the eigenvalues only
+    eigvc.clear();
+    return fd;
+  }
   std::printf(" \n");
   msg1003("   Generating final potential...");
   fd.vpot.resize(n);
@@ -969,6 +1004,46 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   if (std::fabs(xminb - xmin) < 1e-6)
     std::printf(" -> Warning: The initial and final potential have the same minimum possition.\n");
   std::printf(" Final potential generated.\n");
+  if (r.ti_form()) {
+    // espec.f:1015-1078: the final surface's states IFL..IFU and SPECTRUMTI
+    msg1003("   Calculating eigenvalue(s) and eigenvector(s)");
+    std::printf("   %68s\n", "      from final state...");
+    std::printf(" %s\n", starts(tpdiag, ".MTRXDIAG")
+                             ? "Using complete matrix diagonalization procedure."
+                             : "Using lanczos tri-diagonalization procedure.");
+    std::fflush(stdout);
+    std::vector<double> evf, vecf;
+    if (solve(d_vf, nstf, evf, vecf)) {
+      std::printf(" \n Eigenvalues:\n \"\"\"\"\"\"\"\"\"\"\"\"\n");
+      std::printf(" ---------------------------------\n");
+      std::printf(" |  Eigenstate  |   Eigenvalues   |\n ==================================\n");
+      table(evf, r.ifl, r.nfs);
+    } else {
+      std::printf(" <<<>>> It wasn`t able obtain eignvalues and eignvectors correctly <<<>>>\n"
+                  " EXIT\n");
+      if (r.fstop) throw DeckError{"the final eigenstates did not converge"};
+    }
+    // SPECTRUMTI (spectrumti.f:52-94): the initial states come back from the
+    // file initial_spc.aux, written as E20.12 (12 significant digits)
+    auto e20 = [](double x) {
+      char b[40];
+      std::snprintf(b, sizeof b, "%.11E", x);
+      return std::strtod(b, nullptr);
+    };
+    std::printf(" \n Spectrum:\n =========\n");
+    std::printf("     *E/a.u.*        *AMPT*           *FC*              *I->F*\n");
+    for (int k = iil; k < iil + nis; ++k) {
+      const double ei = e20(eval[k]);
+      for (int j = r.ifl; j < r.ifl + r.nfs; ++j) {
+        double w = 0.0;
+        for (int i = 0; i < n; ++i) w += vecf[(size_t)j * n + i] * e20(eigvc[(size_t)k * n + i]);
+        std::printf(" %12.7f    %12.7f    %12.7f          %2d ->%2d\n", evf[j] - ei, w, w * w,
+                    k, j);
+      }
+    }
+    eigvc.clear();
+    return fd;
+  }
   // FORMAT 1031 and the list-directed 'state started' line (espec.f:1083-1108)
   const int k = r.prpgstate - iil;
   const char* th = k == 1 ? "st" : k == 2 ? "nd" : k == 3 ? "rd" : "th";
@@ -993,10 +1068,72 @@ void check_step(const Run& r, const double* sh) {
   }
 }
 
+// .ONLYSPEC (espec.f:1596-1626): the correlation function of an earlier run's
+// output (GETCORR, getcorr.f: the 2^MF rows after its " Correlation
+// Function:" line, DTF from the first two times and TF = last time + DTF),
+// printed again with *PRTCRL, then HWHM and SPECTRUMTD
+int only_spectrum(Run& r, const std::string& dir) {
+  const std::string path = !r.fileaux.empty() && r.fileaux[0] == '/' ? r.fileaux : dir + r.fileaux;
+  const int n2 = 1 << r.mf, mc = n2 / 2;
+  msg1003("   Getting correlation function...");
+  std::ifstream f(path);
+  if (!f) {
+    std::printf(" <<<>>> File %s cannot be open <<<>>>\n Please check and resubimit \n",
+                r.fileaux.c_str());
+    throw DeckError{"correlation file \"" + path + "\" cannot be opened"};
+  }
+  std::string line;
+  bool found = false;
+  while (std::getline(f, line))
+    if (line.compare(0, 22, " Correlation Function:") == 0) {
+      found = true;
+      break;
+    }
+  if (!found) {
+    std::printf(" <<<>>> Correlation function wasn`t found <<<>>>\n");
+    throw DeckError{"no correlation function in " + path};
+  }
+  std::getline(f, line);
+  std::getline(f, line);
+  std::vector<double> t(n2), cu(n2), cv(n2);
+  for (int i = 0; i < n2; ++i) {
+    std::vector<double> x;
+    if (!std::getline(f, line) || (x = numbers(line)).size() < 3) {
+      std::printf(" <<<>>> Error reading correlation function <<<>>>\n");
+      throw DeckError{"the correlation function in " + path + " has fewer than 2^MF rows"};
+    }
+    t[i] = x[0];
+    cu[i] = x[1];
+    cv[i] = x[2];
+  }
+  double dtf = t[1] - t[0];
+  const double tf = t[n2 - 1] + dtf;
+  std::printf(" Correlation function got.\n");
+  if (starts(r.prtcrl, ".YES") || starts(r.prtcrl, ".PARTIAL"))
+    std::printf("%s", correlation_table(mc, tf, cu, cv, dtf).c_str());
+  double tff = tf;
+  if (r.lhwhm) {
+    double dde = r.de - r.e1i;
+    msg1003("Appling the half-width at half-maximum...");
+    std::fflush(stdout);
+    hwhm_(&r.mf, &dtf, &tff, &r.chwhm, &dde, cu.data(), cv.data());
+    std::printf(" Half-width at half-maximum applied.\n");
+  }
+  msg1003("   Processing spectrum...");
+  std::fflush(stdout);
+  double ade = r.ade;
+  spectrumtd_(r.tpwind.c_str(), &r.mf, &dtf, &tff, &r.wp, &ade, cu.data(), cv.data(),
+              r.tpwind.size());
+  std::printf(" Spectrum done.\n \n The eSPec program finished successfully!\n");
+  std::fflush(stdout);
+  return ESPEC_OK;
+}
+
 int run_deck(const std::string& deck_path) {
   Run r = load_run(deck_path);
   const size_t slash = deck_path.find_last_of('/');
   const std::string dir = slash == std::string::npos ? std::string() : deck_path.substr(0, slash + 1);
+  if (r.onlyspec()) return only_spectrum(r, dir);
   const std::string file = !r.potfile.empty() && r.potfile[0] == '/' ? r.potfile : dir + r.potfile;
   int n = 1;
   for (int a = 0; a < r.nd; ++a) n *= r.np[a];
@@ -1014,6 +1151,11 @@ int run_deck(const std::string& deck_path) {
     for (int a = 0; a < r.nd; ++a) sh[a] = ((r.gxf[a] - r.gxi[a]) / (r.np[a] - 1.0)) / kA0A;
     check_step(r, sh);
     fd = initial_state(r, sh, shm, sm, eigvc);
+    if (r.ti_form()) {  // .ENERGY, .SPECTRUM .TI: no propagation (espec.f:954, 1015-1080)
+      std::printf(" \n The eSPec program finished successfully!\n");
+      std::fflush(stdout);
+      return ESPEC_OK;
+    }
   } else {
     fd = read_file(file, n, r.nd, r.shiftp);
     for (int a = 0; a < r.nd; ++a) {

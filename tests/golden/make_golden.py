@@ -29,6 +29,10 @@ Cases:
   calc2d_*    2D decks with computed initial states (.CALC, .MTRXDIAG) and the
               executable's output, with its MAKECST lines (constants.txt);
               --calc2d-only generates only these.
+  ti_*        the time-independent formalism (.ENERGY, .SPECTRUM .TI) on the
+              surfaces of reference test 12 and of calc2d_ohs_psil; the
+              executable's output from its first "Calculating eigenvalue(s)"
+              line; --ti-only generates only these.
   reftest*    the reference's own test decks ttests/input.test<i> with an
               analytic .1D potential and a computed initial state (.CALC):
               the deck as input.spc and the executable's output from the
@@ -477,7 +481,11 @@ REFTEST_EDITS = {
                  " 1.5D+12  10.0  0.241  20.0  4.7124   1.0/")],
 }
 REFTEST_FILES = {"3_short": ["dipol2.inp"]}
-REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag", "3_short"]
+# test 8 (.ONLYSPEC) reads the correlation function of an old output file;
+# its table (the lines from " Correlation Function:" on) is kept, gzipped
+REFTEST_GZ_FILES = {"8": ["correl8.inp"]}
+REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag", "3_short", 8]
+MARKS = ("Propagating eigenvector...", "Getting correlation function...")
 
 
 def case_reftest(i):
@@ -497,9 +505,17 @@ def case_reftest(i):
         src = os.path.join(REF, "ttests", name)
         shutil.copyfile(src, os.path.join(d, name))
         files[name] = src
+    for name in REFTEST_GZ_FILES.get(str(i), []):
+        with open(os.path.join(REF, "ttests", name), "rb") as f:
+            raw = f.read().decode("latin-1").split("\n")
+        k = next(j for j, l in enumerate(raw) if l.startswith(" Correlation Function:"))
+        text = "\n".join(raw[k:]) + "\n"
+        with gzip.open(os.path.join(d, name + ".gz"), "wt") as f:
+            f.write(text)
+        files[name] = text
     out = run_deck(deck, files, timeout=3600)
     lines = out.splitlines()
-    k = max(j for j, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
+    k = max(j for j, l in enumerate(lines) if l.strip() in MARKS)
     with gzip.open(os.path.join(d, "expected.txt.gz"), "wt") as f:
         f.write("\n".join(lines[k - 1:]) + "\n")
 
@@ -606,6 +622,35 @@ CALC2D = {
 }
 
 
+# The time-independent formalism: eigenvalues only (.ENERGY) and the
+# Franck-Condon spectrum of SPECTRUMTI (.SPECTRUM .TI) between the initial
+# and final surfaces of reference test 12, and of the 2D .OHS deck above
+def ti_decks():
+    with open(os.path.join(REF, "ttests", "input.test12")) as f:
+        t12 = f.read()
+    energy = t12.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.ENERGY")
+    ti = t12.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.SPECTRUM\n.TI")
+    ti = ti.replace("*NIST\n 7  0/", "*NIST\n 2  0/\n*NFST\n 6  0/")
+    ti2d = CALC2D["calc2d_ohs_psil"].replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.SPECTRUM\n.TI")
+    ti2d = ti2d.replace("*NIST\n 3  0/", "*NIST\n 2  0/\n*NFST\n 5  0/")
+    for d in (energy, ti, ti2d):
+        assert d.count(".ENERGY") + d.count(".TI\n") == 1
+    return {"ti_energy_ohs": energy, "ti_spectrum_ohs": ti, "ti_spectrum_2d_ohs": ti2d}
+
+
+def case_ti(name, deck):
+    d = os.path.join(OUT, name)
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "input.spc"), "w") as f:
+        f.write(deck)
+    out = run_deck(deck, {})
+    lines = out.splitlines()
+    k = min(j for j, l in enumerate(lines)
+            if l.strip() == "Calculating eigenvalue(s) and eigenvector(s)")
+    with open(os.path.join(d, "expected.txt"), "w") as f:
+        f.write("\n".join(lines[k - 1:]) + "\n")
+
+
 def case_calc2d(name):
     deck = CALC2D[name]
     d = os.path.join(OUT, name)
@@ -648,6 +693,10 @@ def main():
     if "--calc2d-only" in sys.argv:
         for name in CALC2D:
             case_calc2d(name)
+        return
+    if "--ti-only" in sys.argv:
+        for name, deck in ti_decks().items():
+            case_ti(name, deck)
         return
     if "--reftests-only" in sys.argv:
         picked = [a for a in sys.argv[1:] if a in map(str, REFTESTS)] or REFTESTS
@@ -698,6 +747,8 @@ def main():
         case_reftest(i)
     for name in CALC2D:
         case_calc2d(name)
+    for name, deck in ti_decks().items():
+        case_ti(name, deck)
 
 
 if __name__ == "__main__":

@@ -285,3 +285,42 @@ def test_calc_2d_constants(tmp_path, capfd, name):
     want = open(os.path.join(d, "constants.txt")).read().rstrip("\n").split("\n")
     i = out.index(" Initial potential:")
     assert out[i:i + len(want)] == want
+
+
+def test_onlyspec_reads_and_prints_the_correlation(tmp_path, capfd):
+    """.ONLYSPEC (espec.f:1596-1626, getcorr.f): the reference's test deck 8
+    reads the 2^MF rows after " Correlation Function:" of an old output and
+    prints them again as the executable does (DTF from the first two times,
+    TF = last time + DTF); the HWHM and spectrum that follow run on the GPU
+    (tests/test_gpu_deck.py)."""
+    import gzip
+    d = os.path.join(HERE, "golden", "reftest8")
+    (tmp_path / "input.spc").write_text(open(os.path.join(d, "input.spc")).read())
+    with gzip.open(os.path.join(d, "correl8.inp.gz"), "rt") as f:
+        (tmp_path / "correl8.inp").write_text(f.read())
+    try:
+        D.run(tmp_path / "input.spc")
+    except N.EspecError:
+        pass
+    out = capfd.readouterr().out.split("\n")
+    with gzip.open(os.path.join(d, "expected.txt.gz"), "rt") as f:
+        want = f.read().split("\n")
+    i, j = out.index(" Correlation function got."), want.index(" Correlation function got.")
+    k = want.index(" Half-width at half-maximum applied.") - 2  # the HWHM message
+    assert out[i:i + (k - j)] == want[j:k]
+
+
+def test_time_independent_decks_are_read(tmp_path):
+    """.ENERGY and .SPECTRUM .TI (rdinput.f:139-149, *NFST of rdinput.f:375-377):
+    no propagator is needed; the .TI spectrum needs final states and computed
+    ones; a deck that reads through stops at the first device buffer."""
+    energy = CALC.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.ENERGY")
+    msg = run_calc(tmp_path, energy.replace(".PFSPO\n", ".NULL\n"))
+    assert msg is None or "device memory" in msg, msg
+    ti = CALC.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.SPECTRUM\n.TI")
+    msg = run_calc(tmp_path, ti)
+    assert msg is not None and "*NFST" in msg, msg
+    msg = run_calc(tmp_path, ti.replace("*NIST\n 1  0/", "*NIST\n 1  0/\n*NFST\n 4  0/"))
+    assert msg is None or "device memory" in msg, msg
+    msg = run_calc(tmp_path, CALC.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.SPECTRUM\n.XX"))
+    assert msg is not None and ".TD and .TI" in msg, msg

@@ -61,15 +61,29 @@ def compare(have, want, slack=0.0):
     return exact
 
 
-def run_and_read(capfd, d):
+MARKS = ("Propagating eigenvector...", "Getting correlation function...")
+
+
+def run_and_read(capfd, d, tmp=None):
     """The driver's output for the deck in directory d, from the line before
-    the last 'Propagating eigenvector...', and the executable's."""
+    the last 'Propagating eigenvector...' (or, for .ONLYSPEC, 'Getting
+    correlation function...'), and the executable's.  Gzipped input files
+    beside the deck are unpacked with it into tmp."""
+    deck = os.path.join(d, "input.spc")
+    packed = [f for f in os.listdir(d) if f.endswith(".gz") and f != "expected.txt.gz"]
+    if packed:
+        with open(deck) as f:
+            (tmp / "input.spc").write_text(f.read())
+        for name in packed:
+            with gzip.open(os.path.join(d, name), "rt") as f:
+                (tmp / name[:-3]).write_text(f.read())
+        deck = str(tmp / "input.spc")
     capfd.readouterr()
-    D.run(os.path.join(d, "input.spc"))
+    D.run(deck)
     out, err = capfd.readouterr()
     assert err == ""
     lines = out.split("\n")
-    i = max(k for k, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
+    i = max(k for k, l in enumerate(lines) if l.strip() in MARKS)
     if os.path.exists(os.path.join(d, "expected.txt")):
         with open(os.path.join(d, "expected.txt")) as f:
             want = f.read().split("\n")
@@ -116,13 +130,16 @@ REFTESTS = {"reftest9": 0.0, "reftest10": 8e-6, "reftest11": 0.0, "reftest12": 4
             # of a 32 x 32 grid, 1920 .PSIL steps (the ABSTOL bisection again, on
             # Krylov spectra ten times wider: 7e-7 in C(t), 1e-6 in the norm) and
             # 1920 .PSOD steps
-            "calc2d_ohs_psil": 1.5e-6, "calc2d_morse_psod": 0.0}
+            "calc2d_ohs_psil": 1.5e-6, "calc2d_morse_psod": 0.0,
+            # test 8: .ONLYSPEC on the correlation function of an old output
+            # (ttests/correl8.inp), HWHM and the spectrum
+            "reftest8": 0.0}
 SIL_DECKS = ("reftest13", "reftest14", "calc2d_ohs_psil")
 
 
 @pytest.mark.parametrize("name", sorted(REFTESTS))
-def test_reference_test_deck(capfd, name):
-    have, want = run_and_read(capfd, os.path.join(G.GOLDEN, name))
+def test_reference_test_deck(capfd, tmp_path, name):
+    have, want = run_and_read(capfd, os.path.join(G.GOLDEN, name), tmp_path)
     if name in SIL_DECKS:
         check_sil(have, want, REFTESTS[name])
     else:
@@ -191,3 +208,42 @@ def test_scan_equals_one_run_per_file(tmp_path, capfd):
         assert out[i:].startswith(crl)
         assert spc == out[j:j + len(spc)]
         assert out[j + len(spc):].startswith(" Spectrum done.")
+
+
+# The time-independent formalism (tests/golden/ti_*): .ENERGY and .SPECTRUM
+# .TI (SPECTRUMTI's Franck-Condon table) on the surfaces of reference test 12
+# and on a 2D pair.  The executable's eigenvalues are DSPEVX bisections to
+# ABSTOL = 1e-6 (the same state prints 0.440579E-02 or 0.440584E-02 with
+# different *NIST ranges; the converged value is 0.440574E-02), so eigenvalues
+# and the transition energies E get 1.1e-6; the amplitudes are compared in
+# magnitude (an eigenvector's sign is arbitrary) and, with the Franck-Condon
+# factors, to one unit of the last printed digit.
+TI_DECKS = ["ti_energy_ohs", "ti_spectrum_ohs", "ti_spectrum_2d_ohs"]
+
+
+@pytest.mark.parametrize("name", TI_DECKS)
+def test_time_independent_deck(capfd, name):
+    d = os.path.join(G.GOLDEN, name)
+    capfd.readouterr()
+    D.run(os.path.join(d, "input.spc"))
+    out, err = capfd.readouterr()
+    assert err == ""
+    lines = out.split("\n")
+    i = min(k for k, l in enumerate(lines)
+            if l.strip() == "Calculating eigenvalue(s) and eigenvector(s)")
+    have = lines[i - 1:]
+    with open(os.path.join(d, "expected.txt")) as f:
+        want = f.read().split("\n")
+
+    def unsign_amplitudes(rows):
+        out, spec = [], False
+        for l in rows:
+            t = l.split()
+            if l.strip() == "Spectrum:":
+                spec = True
+            if spec and len(t) == 6 and t[4] == "->":
+                l = l.replace(t[1], t[1].lstrip("-"), 1)
+            out.append(l)
+        return out
+
+    compare(unsign_amplitudes(have), unsign_amplitudes(want), slack=1.1e-6)
