@@ -1,24 +1,25 @@
-// deck.cpp -- eSPec input decks run through the GPU propagators: the part of
-// the driver (espec.f) from the input deck (rdinput.f) to the spectrum, for
-// time-dependent runs of one packet, with a tabulated potential and its
-// eigenvector or with an analytic .1D/.2D potential and a computed eigenstate.
+// deck.cpp -- eSPec input decks run through the GPU: the driver (espec.f)
+// from the input deck (rdinput.f) to the spectrum, for one packet with a
+// tabulated potential and its eigenvector, or with an analytic .1D/.2D
+// potential and computed eigenstates (time-dependent or time-independent
+// formalism), or for a spectrum of a correlation function read back.
 //
 // Covered: **MAIN *DIMENSION (.1D/.2D/.3D), *POTENTIAL (.FILE; the analytic
 // .1D/.2D forms of MAKECST with their initial and final constant records),
-// *GRID_RANGES, *MASS, *TPCALC (.SPECTRUM .TD, .PROPAGATION, .CORRELATION),
-// *INIEIGVC (.GETR; .CALC on .1D and .2D grids), *CHANGE, *SHIFT_POTENTIAL, *PRTCRL,
-// *MASS_FACTOR, *DONOTSTOP; **TI *TPDIAG (.MTRXDIAG, .LANCZS, .LANCZSG), *NIST,
-// *ABSTOL and an initial potential of its own; **TD *PROPAG (.PFSPO, .PFSOD,
-// .PSIL, .PSOD, .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE, *TPTRANS .ONE, *PRPTOL,
-// *ABSORBING, *PULSE_AND_DIPOLE (pulses .GAUS, .GGAUS, .SIN2, .NONE; dipoles
-// .CONST, .EXP, .EXP+ (analytic decks), .READ (a file as RDPTE reads it),
-// .NONE, .NULL), *NPROJECTIONS (on the computed states; with .GETR on
-// LNZVC(., 1) only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING,
-// *HWHM.  Print and output-file switches
-// (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored: no files are written
-// (nor the unit-21 table .EXP+ writes).  Anything else -- 3D computed
-// states, the TI formalism, several transitions -- is refused with a
-// message: there is no CPU path.
+// *GRID_RANGES, *MASS, *TPCALC (.SPECTRUM .TD or .TI, .PROPAGATION,
+// .CORRELATION, .ENERGY, .ONLYSPEC), *INIEIGVC (.GETR; .CALC on .1D and .2D
+// grids), *CHANGE, *SHIFT_POTENTIAL, *PRTCRL, *MASS_FACTOR, *DONOTSTOP;
+// **TI *TPDIAG (.MTRXDIAG, .LANCZS, .LANCZSG), *NIST, *NFST, *ABSTOL and an
+// initial potential of its own; **TD *PROPAG (.PFSPO, .PFSOD, .PSIL, .PSOD,
+// .PPSOD, .PPSIL/.PPLNZ), *PRPGSTATE, *TPTRANS .ONE, *PRPTOL, *ABSORBING,
+// *PULSE_AND_DIPOLE (pulses .GAUS, .GGAUS, .SIN2, .NONE; dipoles .CONST,
+// .EXP, .EXP+ (analytic decks), .READ (a file as RDPTE reads it), .NONE,
+// .NULL), *NPROJECTIONS (on the computed states; with .GETR on LNZVC(., 1)
+// only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.  Print and
+// output-file switches (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored:
+// no files are written (nor initial_spc.aux or the unit-21 table of .EXP+).
+// Anything else -- 3D computed states, several transitions, collisions,
+// .2DC operators -- is refused with a message: there is no CPU path.
 //
 // The run follows espec.f: the .FILE reads of RDPTE / RDPT (rdpte.f, rdpt.f:
 // eigenvector block, then potential block, optionally shifted to its
