@@ -102,6 +102,33 @@ struct Deck {
   }
 };
 
+// rdinput.f tests keyword lines by prefix, in this order per section (so
+// '*MASSES' is *MASS, '*MASS_FACTORS' *MASS_FACTOR, '*GRID_RANGES_au'
+// *GRID_RANGES); a line no prefix matches keeps its own name
+std::string canon_key(const std::string& section, const std::string& key) {
+  static const std::map<std::string, std::vector<std::string>> kOrder = {
+      {"**MAIN",
+       {"*TITLE", "*TPCALC", "*DIMENSION", "*GRID_CUT", "*TPTRANS", "*NREORT",
+        "*INITIAL_POTENTIAL", "*FINAL_POTENTIAL", "*POTENTIAL", "*GRID_RANGES", "*INIEIGVC",
+        "*MASS_FACTOR", "*MASS", "*SCALING_FA", "*CROSS_TERM", "*SEED", "*NSHOT", "*CHANGE",
+        "*SHIFT_POTENTIAL", "*PRTEIGVC2", "*PRTREGION", "*PRTONLYREIM", "*PRTEIGVC", "*PRTPOT",
+        "*PRTVEFF", "*PRTPULSE", "*PRTDIPOLE", "*DONOTSTOP", "*PRTCRL"}},
+      {"**TI",
+       {"*INITIAL_POTENTIAL", "*INITIAL_CONDITION", "*INITIAL_WP", "*INITIAL_WF",
+        "*INITIAL_WAVE_FUNCTION", "*WAVE_FUNCTION", "*WAVE_PACKET", "*POTENTIAL", "*TPDIAG",
+        "*NIST", "*ABSTOL", "*SEED", "*MAXINT", "*COLLISION_ENERGY", "*GRID_RANGES",
+        "*INIT_POSSITION", "*SIZE_OF_GAUSSIAN"}},
+      {"**TD",
+       {"*PROPAG", "*FINAL_POTENTIAL", "*GRID_RANGES", "*ABSORBING", "*PULSE_AND_DIPOLE",
+        "*PRPGSTATE", "*TPTRANS", "*PRPTOL", "*NSHOT", "*NPROJECTIONS", "*FOURIER"}},
+      {"**SPECTRUM", {"*FOURIER", "*WINDOWING", "*HWHM"}}};
+  auto it = kOrder.find(section);
+  if (it == kOrder.end()) return key;
+  for (const std::string& p : it->second)
+    if (starts(key, p.c_str())) return p;
+  return key;
+}
+
 Deck parse_deck(const std::string& text) {
   Deck d;
   std::istringstream in(text);
@@ -117,7 +144,7 @@ Deck parse_deck(const std::string& text) {
       key.clear();
     } else if (t[0] == '*') {
       if (section.empty() || starts(t, "**")) continue;  // title lines
-      key = upper(t.substr(0, t.find_first_of(" \t")));
+      key = canon_key(section, upper(t.substr(0, t.find_first_of(" \t"))));
       d.sec[section][key];
       d.head[section][key] = t;
     } else if (!section.empty() && !key.empty()) {
@@ -501,6 +528,8 @@ struct Run {
   bool calc() const { return starts(inieigvc, ".CALC"); }
   bool onlyspec() const { return starts(tpclc, ".ONLYSPEC"); }
   bool energy() const { return starts(tpclc, ".ENERGY"); }
+  bool pes() const { return starts(tpclc, ".PES") || starts(tpclc, ".POTENTIAL"); }
+  bool prtpot = false;
   bool ti_form() const { return starts(tdi, ".TI"); }  // .ENERGY or .SPECTRUM .TI
 };
 
@@ -515,7 +544,7 @@ bool yes_opt(const std::string& o) { return !(starts(o, ".NO") || starts(o, ".OF
 // are accepted and not acted on
 Run read_run(const Deck& d) {
   Run r;
-  static const char* kIgnored[] = {"*TITLE", "*PRTPOT", "*PRTEIGVC", "*PRTVEFF", "*PRTEIGVC2",
+  static const char* kIgnored[] = {"*TITLE", "*PRTEIGVC", "*PRTVEFF", "*PRTEIGVC2",
                                    "*PRTPULSE", "*PRTDIPOLE", "*PRTREGION", "*PRTONLYREIM"};
   auto ignored = [&](const std::string& k) {
     for (const char* x : kIgnored)
@@ -550,6 +579,13 @@ Run read_run(const Deck& d) {
             r.csti = numbers(rec(v, 1, "*POTENTIAL"));
             r.cstf = numbers(rec(v, 2, "*POTENTIAL"));
           }
+        } else if (k == "*INITIAL_POTENTIAL" || k == "*FINAL_POTENTIAL") {
+          // rdinput.f:177-191: one surface with its one constant record
+          const bool ini = k == "*INITIAL_POTENTIAL";
+          (ini ? r.potch : r.potchf) = rec(v, 0, k.c_str());
+          if (starts(ini ? r.potch : r.potchf, ".FILE"))
+            throw DeckError{k + " .FILE: a .FILE potential is read with *POTENTIAL"};
+          (ini ? r.csti : r.cstf) = numbers(rec(v, 1, k.c_str()));
         } else if (k == "*GRID_RANGES") {
           const std::vector<double> x = numbers(rec(v, 0, "*GRID_RANGES"));
           // rdinput.f:206-214: columns 14-15 'au' give bohr
@@ -571,6 +607,7 @@ Run read_run(const Deck& d) {
           else if (starts(r.tpclc, ".PROPAGATION") || starts(r.tpclc, ".CORRELATION")) r.tdi = ".TD";
           else if (starts(r.tpclc, ".ONLYSPEC")) r.fileaux = rec(v, 1, "*TPCALC");  // TDI .NC
           else if (starts(r.tpclc, ".ENERGY")) r.tdi = ".TI";
+          else if (starts(r.tpclc, ".PES") || starts(r.tpclc, ".POTENTIAL")) r.tdi = ".NC";
           else throw DeckError{"*TPCALC " + r.tpclc + " is not covered"};
         } else if (k == "*INIEIGVC") {
           r.inieigvc = upper(rec(v, 0, "*INIEIGVC"));
@@ -578,6 +615,9 @@ Run read_run(const Deck& d) {
           r.change = yes_opt(upper(rec(v, 0, "*CHANGE")));
         } else if (k == "*SHIFT_POTENTIAL") {
           r.shiftp = yes_opt(upper(rec(v, 0, "*SHIFT_POTENTIAL")));
+        } else if (k == "*PRTPOT") {  // rdinput.f:289-296
+          const std::string o = upper(rec(v, 0, "*PRTPOT"));
+          r.prtpot = starts(o, ".YES") || starts(o, ".ON");
         } else if (k == "*DONOTSTOP") {
           r.fstop = !yes_opt(upper(rec(v, 0, "*DONOTSTOP")));
         } else if (k == "*PRTCRL") {
@@ -716,6 +756,14 @@ Run read_run(const Deck& d) {
     }
   }
   if (r.onlyspec()) return r;  // no grid, potential or propagation (espec.f:602)
+  if (r.pes()) {  // espec.f:860-881: the initial potential only
+    if (starts(r.potch, ".FILE") || starts(r.potch, ".NULL"))
+      throw DeckError{"*TPCALC .PES: an analytic initial potential is covered"};
+    if (r.nd > 2) throw DeckError{"*TPCALC .PES: .1D and .2D grids are covered"};
+    for (int a = 0; a < r.nd; ++a)
+      if (!(r.gxf[a] > r.gxi[a])) throw DeckError{"*GRID_RANGES: XI < XF is needed"};
+    return r;
+  }
   const bool file_i = starts(r.potch, ".FILE"), file_f = starts(r.potchf, ".FILE");
   if (starts(r.potch, ".NULL") || starts(r.potchf, ".NULL"))
     throw DeckError{"*POTENTIAL is missing"};
@@ -847,6 +895,26 @@ std::string correlation_table(int mc, double tf, const std::vector<double>& cu,
   return out;
 }
 
+// PRTPT (prtpot.f:1-47) on standard output: the FORMAT 1011 header and one
+// FORMAT 1012 row per grid point (coordinates last axis first, |V| < 1e-99
+// printed as zero); gfortran ends each record at its last item
+void prtpt(int nd, const int* np, const double* xi, const double* sh, const double* v) {
+  std::string out = "    ";
+  for (int a = nd; a >= 1; --a) out += " *R" + std::to_string(a) + "*" + std::string(10, ' ');
+  out += " *V0*\n";
+  const int n1 = np[0], n2 = nd > 1 ? np[1] : 1, n3 = nd > 2 ? np[2] : 1;
+  for (int l = 0; l < n3; ++l)
+    for (int k = 0; k < n2; ++k)
+      for (int j = 0; j < n1; ++j) {
+        const double xp[3] = {xi[0] + j * sh[0], xi[1] + k * sh[1], xi[2] + l * sh[2]};
+        const double w = v[j + (size_t)n1 * (k + (size_t)n2 * l)];
+        out += " ";
+        for (int a = nd - 1; a >= 0; --a) out += fort_e(xp[a], 12, 6) + "   ";
+        out += fort_e(std::fabs(w) < 1e-99 ? 0.0 : w, 12, 6) + "\n";
+      }
+  std::fwrite(out.data(), 1, out.size(), stdout);
+}
+
 // Device buffers of one deck run, freed on every exit
 struct DevBufs {
   std::vector<void*> p;
@@ -889,13 +957,17 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   // mass-scaled coordinates of .LEPS_CC on a .2D grid
   const bool cc = nd == 2 && (starts(r.potch, ".LEPS_CC") || starts(r.potchf, ".LEPS_CC"));
   sm[2] = cc ? kAmu * r.sm[2] : r.sm[2];
+  // espec.f:683-690: a surface named .NULL (a .PES deck's final one) is not converted
+  const bool final_surface = !starts(r.potchf, ".NULL");
   std::printf(" Initial potential:\n");
   makecst(nd, r.potch, sm, r.csti);
-  std::printf(" Final potential:\n");
-  makecst(nd, r.potchf, sm, r.cstf);
+  if (final_surface) {
+    std::printf(" Final potential:\n");
+    makecst(nd, r.potchf, sm, r.cstf);
+  }
   std::printf(" \n Units converted.\n");
   const int ki = espec_pot_kind(r.potch.c_str(), r.potch.size(), nd);
-  const int kf = espec_pot_kind(r.potchf.c_str(), r.potchf.size(), nd);
+  const int kf = final_surface ? espec_pot_kind(r.potchf.c_str(), r.potchf.size(), nd) : -1;
   if (!ki || !kf)
     throw DeckError{"potential " + (ki ? r.potchf : r.potch) + " is not a form of " + r.dim +
                     " grids (potfuncs.f)"};
@@ -903,16 +975,14 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   // which keeps the ground state only
   std::string tpdiag = r.tpdiag;
   int iil = r.iil, nis = r.nis;
-  if (r.change && n > 30000) {
-    tpdiag = ".LANCZSG";
-    std::printf(" -> Type of diagonalization changed to: LANCZSG\n");
-  }
-  if (r.change && starts(tpdiag, ".LANCZSG")) {
-    std::printf(" -> .LANCZSG allows only the ground state eigenvectors calculation\n");
+  const bool to_lanczsg = r.change && n > 30000;
+  if (to_lanczsg) tpdiag = ".LANCZSG";
+  const bool lanczsg = r.change && starts(tpdiag, ".LANCZSG");
+  if (lanczsg) {
     iil = 0;
     nis = 1;
-    std::printf(" -> Total number of eigenvectors changed to %11d\n", 1);
-    if (r.prpgstate != 0) throw DeckError{".LANCZSG keeps the ground state: *PRPGSTATE 0"};
+    if (r.prpgstate != 0 && !r.pes())
+      throw DeckError{".LANCZSG keeps the ground state: *PRPGSTATE 0"};
   }
   const int nst = std::max(iil + nis, r.ti_form() ? 1 : r.prpgstate + 1);  // states 0 .. nst-1
   const int nstf = r.ti_form() ? r.ifl + r.nfs : 0;  // final states of .TI
@@ -974,8 +1044,26 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   if (gvpot(ki, r.csti.data(), d_vi, &xmin))
     throw DeckError{std::string("GVPOT: ") + espec_last_error()};
   std::printf(" Initial potential generated.\n");
+  if (r.prtpot || r.pes()) {
+    std::vector<double> v(n);
+    if (cudaMemcpy(v.data(), d_vi, sizeof(double) * n, cudaMemcpyDeviceToHost) != cudaSuccess)
+      throw DeckError{"copy of the initial potential"};
+    if (r.prtpot) {  // espec.f:871-876
+      std::printf(" \n Initial potential points:\n \"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\n");
+      prtpt(nd, r.np, fd.xi, sh, v.data());
+    }
+    if (r.pes()) {  // espec.f:880-881
+      fd.vpot = v;
+      eigvc.clear();
+      return fd;
+    }
+  }
   msg1003("Calculating eigenvalue(s) and eigenvector(s)");
   std::printf("   %68s\n", "for the initial state...");
+  if (to_lanczsg) std::printf(" -> Type of diagonalization changed to: LANCZSG\n");
+  if (lanczsg)
+    std::printf(" -> .LANCZSG allows only the ground state eigenvectors calculation\n"
+                " -> Total number of eigenvectors changed to %11d\n", 1);
   std::printf(" %s\n", starts(tpdiag, ".MTRXDIAG")   ? "Using complete matrix diagonalization procedure,"
                        : starts(tpdiag, ".LANCZSG") ? "Using interative lanczos tri-diagonalization procedure,"
                                                     : "Using lanczos tri-diagonalization procedure,");
@@ -1005,6 +1093,10 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   if (std::fabs(xminb - xmin) < 1e-6)
     std::printf(" -> Warning: The initial and final potential have the same minimum possition.\n");
   std::printf(" Final potential generated.\n");
+  if (r.prtpot) {  // espec.f:994-1010
+    std::printf(" \n Final potential values:\n \"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\"\n");
+    prtpt(nd, r.np, fd.xi, sh, fd.vpot.data());
+  }
   if (r.ti_form()) {
     // espec.f:1015-1078: the final surface's states IFL..IFU and SPECTRUMTI
     msg1003("   Calculating eigenvalue(s) and eigenvector(s)");
@@ -1141,7 +1233,7 @@ int run_deck(const std::string& deck_path) {
   double sh[3] = {1, 1, 1}, shm[3] = {0, 0, 0}, sm[3] = {1, 1, 1};
   FileData fd;
   std::vector<double> eigvc;  // the computed states IIL..IIU (.CALC)
-  if (r.calc()) {
+  if (r.calc() || r.pes()) {
     // espec.f:646-664: absorber bounds in angstrom unless the form is in bohr
     if (r.absorb && !starts(r.tpabsor, ".SMOOTHW_au") && !starts(r.tpabsor, ".SMRS_au") &&
         !starts(r.tpabsor, ".VOPTIC"))
@@ -1152,7 +1244,7 @@ int run_deck(const std::string& deck_path) {
     for (int a = 0; a < r.nd; ++a) sh[a] = ((r.gxf[a] - r.gxi[a]) / (r.np[a] - 1.0)) / kA0A;
     check_step(r, sh);
     fd = initial_state(r, sh, shm, sm, eigvc);
-    if (r.ti_form()) {  // .ENERGY, .SPECTRUM .TI: no propagation (espec.f:954, 1015-1080)
+    if (r.ti_form() || r.pes()) {  // no propagation (espec.f:881, 954, 1015-1080)
       std::printf(" \n The eSPec program finished successfully!\n");
       std::fflush(stdout);
       return ESPEC_OK;

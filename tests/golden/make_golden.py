@@ -33,8 +33,8 @@ Cases:
               surfaces of reference test 12 and of calc2d_ohs_psil; the
               executable's output from its first "Calculating eigenvalue(s)"
               line; --ti-only generates only these.
-  reftest*    the reference's own test decks ttests/input.test<i> with an
-              analytic .1D potential and a computed initial state (.CALC):
+  reftest*    the reference's own test decks ttests/input.test<i> (most with
+              an analytic potential and a computed initial state, .CALC):
               the deck as input.spc and the executable's output from the
               propagation on, gzipped, as expected.txt.gz; --reftests-only
               [i ...] generates only these.  Tests 1 and 5 are left out: the
@@ -480,12 +480,15 @@ REFTEST_EDITS = {
                 (" 1.5D+12  100.0  0.241  700.0  4.7124   1.0/",
                  " 1.5D+12  10.0  0.241  20.0  4.7124   1.0/")],
 }
-REFTEST_FILES = {"3_short": ["dipol2.inp"]}
+REFTEST_FILES = {"3_short": ["dipol2.inp"], "4": ["eigpot_test3.inp"]}
 # test 8 (.ONLYSPEC) reads the correlation function of an old output file;
 # its table (the lines from " Correlation Function:" on) is kept, gzipped
 REFTEST_GZ_FILES = {"8": ["correl8.inp"]}
-REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag", "3_short", 8]
-MARKS = ("Propagating eigenvector...", "Getting correlation function...")
+# test 4: .PSIL from the .FILE eigpot_test3.inp; test 15: .PES, the 2D
+# .LEPS_CC potential (200 x 180 points) printed
+REFTESTS = [6, 9, 10, 11, 12, 13, 14, "2_mtrxdiag", "3_short", 8, 4, 15]
+MARKS = ("Propagating eigenvector...", "Getting correlation function...",
+         "Generating initial potential...")
 
 
 def case_reftest(i):

@@ -324,3 +324,22 @@ def test_time_independent_decks_are_read(tmp_path):
     assert msg is None or "device memory" in msg, msg
     msg = run_calc(tmp_path, CALC.replace("*TPCALC\n.SPECTRUM\n.TD", "*TPCALC\n.SPECTRUM\n.XX"))
     assert msg is not None and ".TD and .TI" in msg, msg
+
+
+def test_keywords_match_by_prefix(tmp_path, capfd):
+    """rdinput.f tests keyword lines by prefix: the reference's test deck 15
+    writes *MASSES, *MASS_FACTORS and *GRID_RANGES_au (ranges in bohr).  It
+    reads through (.PES, the 2D .LEPS_CC_Dalpha_au potential) to the first
+    device buffer, printing MAKECST's lines as the executable does."""
+    d = os.path.join(HERE, "golden", "reftest15")
+    msg = run_calc(tmp_path, open(os.path.join(d, "input.spc")).read())
+    assert msg is None or "device memory" in msg, msg
+    out = capfd.readouterr().out.split("\n")
+    i = out.index(" Initial potential:")
+    assert out[i + 1:i + 7] == [
+        " These parameters were already inputed in a.u.",
+        " Re_1/a.u. = 0.140200E+01; alpha_1/a.u. = 0.102700E+01; D_1/a.u. = 0.174430E+00",
+        " Re_2/a.u. = 0.140200E+01; alpha_2/a.u. = 0.102700E+01; D_2/a.u. = 0.174430E+00",
+        " Re_3/a.u. = 0.140200E+01; alpha_3/a.u. = 0.102700E+01; D_3/a.u. = 0.174430E+00",
+        " a = 0.3000E+00; b = 0.5000E-01; c = 0.5000E-01",
+        " Angle (rad) =   3.14159265358979     "]

@@ -61,13 +61,15 @@ def compare(have, want, slack=0.0):
     return exact
 
 
-MARKS = ("Propagating eigenvector...", "Getting correlation function...")
+MARKS = ("Propagating eigenvector...", "Getting correlation function...",
+         "Generating initial potential...")
 
 
 def run_and_read(capfd, d, tmp=None):
     """The driver's output for the deck in directory d, from the line before
-    the last 'Propagating eigenvector...' (or, for .ONLYSPEC, 'Getting
-    correlation function...'), and the executable's.  Gzipped input files
+    the last 'Propagating eigenvector...' (for .ONLYSPEC 'Getting correlation
+    function...', for .PES 'Generating initial potential...'), and the
+    executable's.  Gzipped input files
     beside the deck are unpacked with it into tmp."""
     deck = os.path.join(d, "input.spc")
     packed = [f for f in os.listdir(d) if f.endswith(".gz") and f != "expected.txt.gz"]
@@ -132,9 +134,11 @@ REFTESTS = {"reftest9": 0.0, "reftest10": 8e-6, "reftest11": 0.0, "reftest12": 4
             # 1920 .PSOD steps
             "calc2d_ohs_psil": 1.5e-6, "calc2d_morse_psod": 0.0,
             # test 8: .ONLYSPEC on the correlation function of an old output
-            # (ttests/correl8.inp), HWHM and the spectrum
-            "reftest8": 0.0}
-SIL_DECKS = ("reftest13", "reftest14", "calc2d_ohs_psil")
+            # (ttests/correl8.inp), HWHM and the spectrum; test 4: .PSIL from a
+            # .FILE (the allowance of test 13); test 15: .PES, the 2D .LEPS_CC
+            # potential printed on 200 x 180 points
+            "reftest8": 0.0, "reftest4": 5e-6, "reftest15": 0.0}
+SIL_DECKS = ("reftest13", "reftest14", "calc2d_ohs_psil", "reftest4")
 
 
 @pytest.mark.parametrize("name", sorted(REFTESTS))
