@@ -3,11 +3,13 @@
     python -m espec_b200.deck path/to/input.spc
     python -m espec_b200.deck path/to/input.spc data1.inp data2.inp ... out_prefix
 
-covers the time-dependent part of espec.f for one packet with a .FILE
-potential and its .GETR eigenvector (.PFSPO, .PFSOD, .PSIL, .PSOD, and .PPSOD /
-.PPSIL with a laser pulse; absorbers, total correlation, HWHM, spectrum) and
-prints what espec.x prints from
-"Propagating eigenvector..." on; other decks are refused with the reason.
+runs espec.f's driver for one packet: a .FILE potential with its .GETR
+eigenvector, or analytic 1D/2D potentials with the initial states computed
+(.CALC) on the GPU; the time-dependent propagators (.PFSPO, .PFSOD, .PSIL,
+.PSOD, and .PPSOD / .PPSIL with a laser pulse; absorbers, total correlation,
+HWHM, spectrum), the time-independent formalism (.ENERGY, .SPECTRUM .TI),
+.PES and .ONLYSPEC, printing what espec.x prints; other decks are refused with
+the reason.
 """
 import sys
 
