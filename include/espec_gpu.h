@@ -234,8 +234,11 @@ int espec_device_ok(void);
  *
  * Replaces the time loop of PSPOFFT (pspofft.f:110-145) with PSPOFFTAUX
  * (spofft.f:3-203) for many independent 1D packets at once.  Packet k has
- * npts[k] points (256, 384, 512, 768, 1024, 1536, 2048 or 4096), grid step
- * sh[k] (bohr) and mass sm[k] (electron masses); all packets share dt_fs.
+ * npts[k] points, grid step sh[k] (bohr) and mass sm[k] (electron masses);
+ * all packets share dt_fs.  Sizes 256, 384, 512, 768, 1024, 1536, 2048 and
+ * 4096 run the register FFT plans (FP64 or mixed); any other even size from 4
+ * to 7252 runs, in FP64, one CTA per packet with a shared-memory mixed-radix
+ * FFT (any N, as the reference's fft3d.f).
  * Arrays passed to espec_spo_load are concatenated over packets in order.
  * C(t) = <psi(0)|psi(t)> is produced for every step: nsteps+1 complex
  * samples per packet, packet-major.
@@ -246,7 +249,8 @@ int espec_spo_create(espec_spo_plan** plan, int npk, const int* npts,
                      const double* sh, const double* sm, double dt_fs,
                      int precision, int absorb, int quirks);
 /* Same plan for another method: ESPEC_SOD replaces the time loop of PSODFFT
- * (psodfft.f:77-206, sodfft.f:64-126), FP64 only, sizes 256..2048; its first
+ * (psodfft.f:77-206, sodfft.f:64-126), FP64 only, register plans for sizes
+ * 256..2048 and any other even size up to 3626 in shared memory; its first
  * step is the reference's two-half-step start-up and C(t) again has nsteps+1
  * samples.  espec_spo_create(...) = espec_prop_create(..., ESPEC_SPO, ...). */
 int espec_prop_create(espec_spo_plan** plan, int npk, const int* npts,
