@@ -4,11 +4,11 @@
 // eSPec's FFT (fft3d.f, Singleton's mixed-radix transform) takes any N, so
 // its .PFSPO / .PFSOD runs do too.  Here one CTA owns one packet and keeps it
 // in shared memory; the transform is a mixed-radix Stockham FFT (radices 4
-// and 2, then every odd prime factor), natural order in and out, in which
-// each output of a radix-r stage is the direct sum of its r inputs times
-// twiddles from a per-size table w[e] = e^{+2 pi i e / N}.  A stage costs N r
-// complex multiply-adds, so a size with a large prime factor is slow but
-// exact to FP64 rounding.  The step, the tables (x order, and the kinetic
+// and 2, then every odd prime factor), natural order in and out: each thread
+// takes one butterfly of a stage into registers, twiddles it from a per-size
+// table w[e] = e^{+2 pi i e / N} and writes its r outputs (radix 2, 3, 4 and 5
+// written out, other radices up to 16 as a direct sum in registers, larger
+// primes output by output: N r complex multiply-adds for such a stage).  The step, the tables (x order, and the kinetic
 // table in natural FFT order) and the C(t) samples are those of the register
 // kernels: spo_packet (spo1d.cuh) and sod1d_kernel (sod1d.cuh).
 #include <cuda_runtime.h>
@@ -52,40 +52,144 @@ size_t any_smem_bytes(int n, int method) {
 
 namespace {
 
+// x * w, w given as (cos, sin) and conjugated for the inverse
+__device__ __forceinline__ cpx<double> twid(cpx<double> x, double2 w, bool inv) {
+  const double wi = inv ? -w.y : w.y;
+  return mk(fma(x.x, w.x, -x.y * wi), fma(x.x, wi, x.y * w.x));
+}
+// i * x (forward) or -i * x (inverse)
+__device__ __forceinline__ cpx<double> rot90(cpx<double> x, bool inv) {
+  return inv ? mk(x.y, -x.x) : mk(-x.y, x.x);
+}
+
+// y_k = sum_q x_q w_R^{qk}, w_R = e^{+2 pi i/R} (conjugated for the
+// inverse), in registers: the radix-2, 3, 4 and 5 butterflies written out,
+// other radices up to kAnyRegRadix as the direct sum with the table's w_R
+constexpr int kAnyRegRadix = 16;
+template <int R>
+__device__ __forceinline__ void dft_small(cpx<double>* x, const double2* __restrict__ tw, int n,
+                                          bool inv) {
+  if constexpr (R == 2) {
+    const cpx<double> a = x[0], b = x[1];
+    x[0] = mk(a.x + b.x, a.y + b.y);
+    x[1] = mk(a.x - b.x, a.y - b.y);
+  } else if constexpr (R == 4) {
+    const cpx<double> a = mk(x[0].x + x[2].x, x[0].y + x[2].y);
+    const cpx<double> b = mk(x[0].x - x[2].x, x[0].y - x[2].y);
+    const cpx<double> c = mk(x[1].x + x[3].x, x[1].y + x[3].y);
+    const cpx<double> d = rot90(mk(x[1].x - x[3].x, x[1].y - x[3].y), inv);
+    x[0] = mk(a.x + c.x, a.y + c.y);
+    x[2] = mk(a.x - c.x, a.y - c.y);
+    x[1] = mk(b.x + d.x, b.y + d.y);
+    x[3] = mk(b.x - d.x, b.y - d.y);
+  } else if constexpr (R == 3) {
+    const double2 w = __ldg(tw + n / 3);  // (cos 2pi/3, sin 2pi/3)
+    const cpx<double> a = mk(x[1].x + x[2].x, x[1].y + x[2].y);
+    const cpx<double> b = mk(x[1].x - x[2].x, x[1].y - x[2].y);
+    const cpx<double> c = mk(fma(w.x, a.x, x[0].x), fma(w.x, a.y, x[0].y));
+    const cpx<double> u = rot90(mk(w.y * b.x, w.y * b.y), inv);
+    x[0] = mk(x[0].x + a.x, x[0].y + a.y);
+    x[1] = mk(c.x + u.x, c.y + u.y);
+    x[2] = mk(c.x - u.x, c.y - u.y);
+  } else if constexpr (R == 5) {
+    const double2 w1 = __ldg(tw + n / 5), w2 = __ldg(tw + 2 * (n / 5));
+    const cpx<double> a1 = mk(x[1].x + x[4].x, x[1].y + x[4].y);
+    const cpx<double> b1 = mk(x[1].x - x[4].x, x[1].y - x[4].y);
+    const cpx<double> a2 = mk(x[2].x + x[3].x, x[2].y + x[3].y);
+    const cpx<double> b2 = mk(x[2].x - x[3].x, x[2].y - x[3].y);
+    const cpx<double> c1 = mk(x[0].x + w1.x * a1.x + w2.x * a2.x, x[0].y + w1.x * a1.y + w2.x * a2.y);
+    const cpx<double> c2 = mk(x[0].x + w2.x * a1.x + w1.x * a2.x, x[0].y + w2.x * a1.y + w1.x * a2.y);
+    const cpx<double> s1 = rot90(mk(w1.y * b1.x + w2.y * b2.x, w1.y * b1.y + w2.y * b2.y), inv);
+    const cpx<double> s2 = rot90(mk(w2.y * b1.x - w1.y * b2.x, w2.y * b1.y - w1.y * b2.y), inv);
+    x[0] = mk(x[0].x + a1.x + a2.x, x[0].y + a1.y + a2.y);
+    x[1] = mk(c1.x + s1.x, c1.y + s1.y);
+    x[4] = mk(c1.x - s1.x, c1.y - s1.y);
+    x[2] = mk(c2.x + s2.x, c2.y + s2.y);
+    x[3] = mk(c2.x - s2.x, c2.y - s2.y);
+  }
+}
+
+// one Stockham stage of radix R (compile time) or r (run time): butterfly j
+// takes x_q = src[j + q m], q < r, twiddles them by w_N^{(j % ns) q N/span},
+// and writes its r-point DFT to dst[(j / ns) span + k ns + j % ns]
+template <int R>
+__device__ __forceinline__ void any_stage(const double2* __restrict__ tw, const cpx<double>* src,
+                                          cpx<double>* dst, int n, int r, int ns, bool inv) {
+  const int T = blockDim.x, t = threadIdx.x;
+  const int m = n / r, span = ns * r, tws = n / span;
+  for (int j = t; j < m; j += T) {
+    const int jm = j % ns, base = (j / ns) * span + jm;
+    if (R > 0 || r <= kAnyRegRadix) {
+      constexpr int RR = R > 0 ? R : kAnyRegRadix;
+      cpx<double> x[RR];
+      const int e1 = jm * tws;  // < n / r
+      int e = 0;
+#pragma unroll
+      for (int q = 0; q < RR; ++q) {
+        if (R == 0 && q >= r) break;
+        x[q] = src[j + q * m];
+        if (q > 0) x[q] = twid(x[q], __ldg(tw + e), inv);
+        e += e1;  // q e1 < n: no wrap
+      }
+      if constexpr (R > 0) {
+        dft_small<R>(x, tw, n, inv);
+#pragma unroll
+        for (int k = 0; k < R; ++k) dst[base + k * ns] = x[k];
+      } else {
+        for (int k = 0; k < r; ++k) {  // direct sum with w_r^{qk} = w_N^{qk m}
+          double sr = 0.0, si = 0.0;
+          int f = 0;
+          for (int q = 0; q < r; ++q) {
+            const cpx<double> y = twid(x[q], __ldg(tw + f), inv);
+            sr += y.x;
+            si += y.y;
+            f += k * m;
+            if (f >= n) f -= n;
+          }
+          dst[base + k * ns] = mk(sr, si);
+        }
+      }
+    } else {
+      // a prime radix above kAnyRegRadix: each output from the r inputs
+      for (int k = 0; k < r; ++k) {
+        int e1 = jm * tws + k * m;
+        if (e1 >= n) e1 -= n;
+        double sr = 0.0, si = 0.0;
+        int e = 0;
+        for (int q = 0; q < r; ++q) {
+          const cpx<double> y = twid(src[j + q * m], __ldg(tw + e), inv);
+          sr += y.x;
+          si += y.y;
+          e += e1;
+          if (e >= n) e -= n;
+        }
+        dst[base + k * ns] = mk(sr, si);
+      }
+    }
+  }
+}
+
 // out = src transformed (forward: e^{+2 pi i jk/N}, inverse: conjugate, no
 // scaling); src and dst are the two N-point buffers, the result lands in one
 // of them (returned).  Ends with a CTA barrier.
 __device__ cpx<double>* any_fft(const AnyPlan& pl, const double2* __restrict__ tw,
                                 cpx<double>* src, cpx<double>* dst, bool inv) {
-  const int n = pl.n, T = blockDim.x, t = threadIdx.x;
+  const int n = pl.n;
   int ns = 1;  // size of the sub-transforms done so far
   for (int s = 0; s < pl.ns; ++s) {
-    const int r = pl.r[s], m = n / r, span = ns * r, tws = n / span;
-    for (int o = t; o < n; o += T) {
-      // output o = (j / ns) span + k ns + j % ns of input group j, digit k
-      const int blk = o / span, rem = o - blk * span;
-      const int k = rem / ns, jm = rem - k * ns;
-      const int j = blk * ns + jm;
-      int e1 = jm * tws + k * m;
-      if (e1 >= n) e1 -= n;
-      double sr = 0.0, si = 0.0;
-      int e = 0;
-      for (int q = 0; q < r; ++q) {
-        const cpx<double> x = src[j + q * m];
-        const double2 w = __ldg(tw + e);
-        const double wi = inv ? -w.y : w.y;
-        sr = fma(x.x, w.x, fma(-x.y, wi, sr));
-        si = fma(x.x, wi, fma(x.y, w.x, si));
-        e += e1;
-        if (e >= n) e -= n;
-      }
-      dst[o] = mk(sr, si);
+    const int r = pl.r[s];
+    switch (r) {
+      case 2: any_stage<2>(tw, src, dst, n, r, ns, inv); break;
+      case 3: any_stage<3>(tw, src, dst, n, r, ns, inv); break;
+      case 4: any_stage<4>(tw, src, dst, n, r, ns, inv); break;
+      case 5: any_stage<5>(tw, src, dst, n, r, ns, inv); break;
+      default: any_stage<0>(tw, src, dst, n, r, ns, inv); break;
     }
     __syncthreads();
     cpx<double>* tmp = src;
     src = dst;
     dst = tmp;
-    ns = span;
+    ns *= r;
   }
   return src;
 }
