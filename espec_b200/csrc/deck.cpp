@@ -158,6 +158,7 @@ Deck parse_deck(const std::string& text) {
 // (rdpte.f:39-58, rdpt.f:40-62), coordinates listed last axis first
 struct FileData {
   std::vector<double> psi, vpot;
+  std::vector<double> psi_im;  // a complex initial state (.COLLISION); empty: real
   double xi[3] = {0, 0, 0}, xf[3] = {0, 0, 0};
 };
 
@@ -529,6 +530,8 @@ struct Run {
   bool onlyspec() const { return starts(tpclc, ".ONLYSPEC"); }
   bool energy() const { return starts(tpclc, ".ENERGY"); }
   bool pes() const { return starts(tpclc, ".PES") || starts(tpclc, ".POTENTIAL"); }
+  bool collision() const { return starts(tpclc, ".COLLISION"); }
+  double rk[3] = {0, 0, 0}, ra[3] = {0, 0, 0}, x0[3] = {0, 0, 0};  // .COLLISION wave packet
   bool prtpot = false;
   bool ti_form() const { return starts(tdi, ".TI"); }  // .ENERGY or .SPECTRUM .TI
 };
@@ -604,7 +607,9 @@ Run read_run(const Deck& d) {
         } else if (k == "*TPCALC") {
           r.tpclc = upper(rec(v, 0, "*TPCALC"));
           if (starts(r.tpclc, ".SPECTRUM")) r.tdi = upper(rec(v, 1, "*TPCALC"));
-          else if (starts(r.tpclc, ".PROPAGATION") || starts(r.tpclc, ".CORRELATION")) r.tdi = ".TD";
+          else if (starts(r.tpclc, ".PROPAGATION") || starts(r.tpclc, ".CORRELATION") ||
+                   starts(r.tpclc, ".COLLISION"))
+            r.tdi = ".TD";
           else if (starts(r.tpclc, ".ONLYSPEC")) r.fileaux = rec(v, 1, "*TPCALC");  // TDI .NC
           else if (starts(r.tpclc, ".ENERGY")) r.tdi = ".TI";
           else if (starts(r.tpclc, ".PES") || starts(r.tpclc, ".POTENTIAL")) r.tdi = ".NC";
@@ -651,6 +656,19 @@ Run read_run(const Deck& d) {
           if (x.size() < 2) throw DeckError{"*NFST: NFS IFL"};
           r.nfs = (int)x[0];
           r.ifl = (int)x[1];
+        } else if (k == "*COLLISION_ENERGY" || k == "*SIZE_OF_GAUSSIAN" ||
+                   k == "*INIT_POSSITION") {
+          // rdinput.f:384-419: per axis; the energy in eV unless columns 19-20
+          // read 'au', the size multiplied by A0A when they do, the position
+          // as written
+          const std::vector<double> x = numbers(rec(v, 0, k.c_str()));
+          const std::string& h = d.head.at(sname).at(k);
+          const bool au = h.size() >= 20 && h.compare(18, 2, "au") == 0;
+          for (size_t a = 0; a < 3 && a < x.size(); ++a) {
+            if (k == "*COLLISION_ENERGY") r.rk[a] = au ? x[a] : x[a] / 27.2113834;
+            else if (k == "*SIZE_OF_GAUSSIAN") r.ra[a] = au ? x[a] * kA0A : x[a];
+            else r.x0[a] = x[a];
+          }
         } else if (k == "*SEED" || k == "*MAXINT") {
           continue;  // the seed and the length of LANCZSG's iterations
         } else {
@@ -780,7 +798,16 @@ Run read_run(const Deck& d) {
                     "eigenvector of the .FILE)"};
   if (!starts(r.tptrans, ".ONE"))
     throw DeckError{"one propagated state (*TPTRANS .ONE) is covered"};
-  if (r.calc()) {
+  if (r.collision()) {
+    // espec.f:849-864 with init_cond.f:18-38: a Gaussian wave packet with a
+    // momentum on an analytic .1D potential (the .2D forms build on a .FILE
+    // eigenvector, .GETR2/.GETC*)
+    if (r.nd != 1 || file_i || !r.calc())
+      throw DeckError{".COLLISION: the .1D wave packet of an analytic potential is covered "
+                      "(*INIEIGVC .CALC)"};
+    if (!(r.gxf[0] > r.gxi[0])) throw DeckError{"*GRID_RANGES: XI < XF is needed"};
+    if (!(r.ra[0] > 0.0)) throw DeckError{"*SIZE_OF_GAUSSIAN must be positive"};
+  } else if (r.calc()) {
     if (r.nd > 2)
       throw DeckError{"computed initial states (.CALC) are covered on .1D and .2D grids (the "
                       "GPU eigensolver's)"};
@@ -971,6 +998,49 @@ FileData initial_state(Run& r, double* sh, double* shm, double* sm, std::vector<
   if (!ki || !kf)
     throw DeckError{"potential " + (ki ? r.potchf : r.potch) + " is not a form of " + r.dim +
                     " grids (potfuncs.f)"};
+  if (r.collision()) {
+    // espec.f:849-864: the wave packet instead of eigenstates, then the
+    // final surface; INIT_COND (init_cond.f:18-38) and GET_GAUSS (gauss.f:20):
+    // psi = N exp(-ln2 ((x - X0)/A)^2) e^{i k (x - X0)}, k = +-sqrt(2 m |E|)
+    msg1003("Computing the initial wave packet...");
+    double rk = r.rk[0];
+    rk = rk < 0.0 ? -std::sqrt(-(((2.0 * sm[0]) * r.smf[0]) * rk))
+                  : std::sqrt(((2.0 * sm[0]) * r.smf[0]) * rk);
+    const double ln2 = 0.69314718;  // gauss.f's constant as written
+    auto gauss = [&](double coord, double norm) {
+      const double q = coord / r.ra[0];
+      return norm * std::exp(-ln2 * (q * q));
+    };
+    double nrm = 0.0;
+    for (int i = 0; i < n; ++i) {
+      const double g = gauss(fd.xi[0] + i * sh[0] - r.x0[0], 1.0);
+      nrm = nrm + g * g;
+    }
+    nrm = 1.0 / std::sqrt(nrm);
+    fd.psi.resize(n);
+    fd.psi_im.resize(n);
+    for (int i = 0; i < n; ++i) {
+      const double coord = fd.xi[0] + i * sh[0] - r.x0[0];
+      const double g = gauss(coord, nrm);
+      fd.psi[i] = std::cos(rk * coord) * g;
+      fd.psi_im[i] = std::sin(rk * coord) * g;
+    }
+    std::printf(" Initial wave packet computed.\n \n");
+    DevBufs dev;
+    double* d_vf = dev.alloc(n);
+    double xmin = 0.0;
+    msg1003("   Generating final potential...");
+    fd.vpot.resize(n);
+    if (espec_gvpot_1d(1, &n, fd.xi, sh, kf, r.cstf.data(), r.shiftp ? 1 : 0, d_vf, &xmin,
+                       nullptr) ||
+        cudaMemcpy(fd.vpot.data(), d_vf, sizeof(double) * n, cudaMemcpyDeviceToHost) !=
+            cudaSuccess)
+      throw DeckError{std::string("GVPOT: ") + espec_last_error()};
+    std::printf(" Final potential generated.\n");
+    std::printf("\n%33sStarting 0th state to be propagated...\n%12d th state started.\n", "", 0);
+    eigvc.clear();
+    return fd;
+  }
   // espec.f:879-905: *CHANGE on a grid above 3e4 points switches to LANCZSG,
   // which keeps the ground state only
   std::string tpdiag = r.tpdiag;
@@ -1272,7 +1342,8 @@ int run_deck(const std::string& deck_path) {
   std::vector<double> lnzvc((size_t)mxdct * ncol, 0.0);
   for (size_t j = 0; j < eigvc.size() / (n ? n : 1); ++j)
     std::copy(eigvc.begin() + j * n, eigvc.begin() + (j + 1) * n, lnzvc.begin() + j * mxdct);
-  std::vector<double> u1 = fd.psi, v1(n, 0.0), u2(n, 0.0), v2(n, 0.0), tc(n, 0.0), wrk(n, 0.0);
+  std::vector<double> u1 = fd.psi, v1 = fd.psi_im, u2(n, 0.0), v2(n, 0.0), tc(n, 0.0), wrk(n, 0.0);
+  v1.resize(n, 0.0);
   const int absorb = r.absorb ? 1 : 0, lmt = 10, change = r.change ? 1 : 0;
   double abstol = 1e-6;
   std::vector<int> iwork(64, 0);
@@ -1365,7 +1436,7 @@ int run_deck(const std::string& deck_path) {
     if (r.fstop) throw DeckError{"propagation operator error (INFO = 1)"};
   }
   std::printf(" Eigenvector propagated.\n");
-  if (starts(r.tpclc, ".PROPAGATION")) {
+  if (starts(r.tpclc, ".PROPAGATION") || r.collision()) {  // espec.f:1541-1542
     std::printf(" \n The eSPec program finished successfully!\n");
     return ESPEC_OK;
   }

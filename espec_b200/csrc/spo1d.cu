@@ -388,8 +388,12 @@ static int spo_index_tables(espec_spo_plan* p) {
   std::vector<int> kperm(np), pk_of(np);
   std::map<int, int> var_of;
   const bool persist = p->launch == ESPEC_LAUNCH_PERSISTENT;
+  // the reference-defect form always runs DefaultPlan<N> (launch_variant),
+  // so its tables take that plan's final layout whatever the class's variant
+  const bool quirk = p->method == ESPEC_SPO && (p->quirks & ESPEC_Q_SPO_INPLACE);
   for (auto& c : p->classes)
-    var_of[c.n] = persist ? persist_variant(c.n, p->precision == ESPEC_FP64) : c.variant;
+    var_of[c.n] = persist ? persist_variant(c.n, p->precision == ESPEC_FP64)
+                          : (quirk ? 0 : c.variant);
   std::map<int, std::pair<std::vector<int>, int>> kap_cache;
   for (int i = 0; i < npk; ++i) {
     const int n = p->n[i];

@@ -29,6 +29,8 @@ Cases:
   calc2d_*    2D decks with computed initial states (.CALC, .MTRXDIAG) and the
               executable's output, with its MAKECST lines (constants.txt);
               --calc2d-only generates only these.
+  collision_* a Gaussian wave packet with momentum (.COLLISION) in a 1D well,
+              .PSOD and .PFSPO; --collision-only generates only these.
   ti_*        the time-independent formalism (.ENERGY, .SPECTRUM .TI) on the
               surfaces of reference test 12 and of calc2d_ohs_psil; the
               executable's output from its first "Calculating eigenvalue(s)"
@@ -654,6 +656,64 @@ def case_ti(name, deck):
         f.write("\n".join(lines[k - 1:]) + "\n")
 
 
+# .COLLISION: a Gaussian wave packet with momentum (init_cond.f) in a 1D
+# harmonic well, propagated with .PSOD and with .PFSPO.  The complex initial
+# state meets PSOD's restart copy (psod.f:136-141, V1(I+1) = V0(I)): its norm
+# and energy drift until INFO = 1, and *DONOTSTOP lets the run end normally.
+COLLISION = """*** eSPec input file ***
+**MAIN
+*TITLE
+ a Gaussian wave packet with momentum in a harmonic well
+*DIMENSION
+.1D
+ 512/
+*POTENTIAL
+.OHS
+ 1.14600  1943.79/
+ 1.14600  1943.79/
+*GRID_RANGES
+ 0.6  1.8/
+*MASS
+ 7.49D0/
+*TPCALC
+.COLLISION
+*INIEIGVC
+.CALC
+*CHANGE
+.YES
+*PRTCRL
+.PARTIAL
+*DONOTSTOP
+.ON
+**TI
+*COLLISION_ENERGY
+ 0.05/
+*INIT_POSSITION
+ 2.0/
+*SIZE_OF_GAUSSIAN
+ 0.1/
+**TD
+*PROPAG
+{prop}
+**END
+"""
+COLLISION_DECKS = {"collision_psod": ".PSOD\n 0.0  20.0  2D-4/",
+                   "collision_pfspo": ".PFSPO\n 0.0  20.0  2D-4/"}
+
+
+def case_collision(name):
+    deck = COLLISION.format(prop=COLLISION_DECKS[name])
+    d = os.path.join(OUT, name)
+    os.makedirs(d, exist_ok=True)
+    with open(os.path.join(d, "input.spc"), "w") as f:
+        f.write(deck)
+    out = run_deck(deck, {})
+    lines = out.splitlines()
+    k = max(j for j, l in enumerate(lines) if l.strip() == "Propagating eigenvector...")
+    with gzip.open(os.path.join(d, "expected.txt.gz"), "wt") as f:
+        f.write("\n".join(lines[k - 1:]) + "\n")
+
+
 def case_calc2d(name):
     deck = CALC2D[name]
     d = os.path.join(OUT, name)
@@ -696,6 +756,10 @@ def main():
     if "--calc2d-only" in sys.argv:
         for name in CALC2D:
             case_calc2d(name)
+        return
+    if "--collision-only" in sys.argv:
+        for name in COLLISION_DECKS:
+            case_collision(name)
         return
     if "--ti-only" in sys.argv:
         for name, deck in ti_decks().items():
@@ -752,6 +816,8 @@ def main():
         case_calc2d(name)
     for name, deck in ti_decks().items():
         case_ti(name, deck)
+    for name in COLLISION_DECKS:
+        case_collision(name)
 
 
 if __name__ == "__main__":

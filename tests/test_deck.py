@@ -34,7 +34,7 @@ def refused(tmp_path, text, files=None):
     ("*TPTRANS\n.ONE", "*TPTRANS\n.ALL", "one propagated state"),
     ("*PRPGSTATE\n 0/", "*PRPGSTATE\n 1/", "*PRPGSTATE 0"),
     ("**TD", "**COLLISION\n**TD", "section **COLLISION"),
-    ("**TD", "**TI\n*COLLISION_ENERGY\n 1.0/\n**TD", "keyword *COLLISION_ENERGY"),
+    ("**TD", "**TI\n*QUANTUM_FOO\n 1.0/\n**TD", "keyword *QUANTUM_FOO"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n*PRPTOL", "*PULSE_AND_DIPOLE"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.LASER\n 1 2 3 4 5/\n.NULL\n*PRPTOL", "pulse is not known"),
     ("*PRPTOL", "*PULSE_AND_DIPOLE\n.GAUS\n 1 2 3 4 5/\n.GET\ndm.inp\n*PRPTOL", "dipole moment .GET"),
@@ -343,3 +343,17 @@ def test_keywords_match_by_prefix(tmp_path, capfd):
         " Re_3/a.u. = 0.140200E+01; alpha_3/a.u. = 0.102700E+01; D_3/a.u. = 0.174430E+00",
         " a = 0.3000E+00; b = 0.5000E-01; c = 0.5000E-01",
         " Angle (rad) =   3.14159265358979     "]
+
+
+def test_collision_decks_are_read(tmp_path):
+    """.COLLISION (rdinput.f:141-143, 384-419; espec.f:849-864): a 1D wave
+    packet on an analytic potential reads through to the first device buffer;
+    other forms are refused."""
+    d = os.path.join(HERE, "golden", "collision_psod")
+    text = open(os.path.join(d, "input.spc")).read()
+    msg = run_calc(tmp_path, text)
+    assert msg is None or "device memory" in msg, msg
+    msg = run_calc(tmp_path, text.replace(" 0.1/\n", " 0.0/\n"))
+    assert msg is not None and "*SIZE_OF_GAUSSIAN" in msg, msg
+    msg = run_calc(tmp_path, text.replace(".1D\n 512/", ".2D\n 64 64/"))
+    assert msg is not None and ".COLLISION" in msg, msg

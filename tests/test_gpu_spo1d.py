@@ -72,9 +72,14 @@ def test_fp64_morse1d_full_length(oracle):
 
 
 def test_fp64_reference_defect_mode(oracle):
-    """spofft.f:150-153 in-place kinetic multiply, reproduced on request."""
-    n, off, sh, sm, v, psi = random_packets([1024, 2048, 384])
-    dt = 0.005 * W.SHFS
+    """spofft.f:150-153 in-place kinetic multiply, reproduced on request, for
+    every size: the defect form runs one plan per size (DefaultPlan), and its
+    tables must follow that plan's layout whatever variant the size's class
+    defaults to."""
+    n, off, sh, sm, v, psi = random_packets(SIZES)
+    # dt T_max below ~2 for every size (the defect's map grows without bound
+    # beyond that, spofft.f:150-153)
+    dt = 0.001 * W.SHFS
     c_ref, p_ref = oracle_batch(oracle, n, off, sh, sm, v, psi, dt, 400, quirks=oracle.Q_SPO_INPLACE)
     c, p = gpu_batch(n, sh, sm, v, psi, dt, 400, "fp64", quirks=NAT.Q_SPO_INPLACE)
     assert np.max(np.abs(c - c_ref)) <= 1e-10
