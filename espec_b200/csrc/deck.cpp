@@ -18,7 +18,9 @@
 // only, KP = 0), *NSHOT; **SPECTRUM *FOURIER, *WINDOWING, *HWHM.  Print and
 // output-file switches (*PRTPOT, *PRTEIGVC, ...) are accepted and ignored:
 // no files are written (nor initial_spc.aux or the unit-21 table of .EXP+).
-// Anything else -- 3D computed states, several transitions, collisions,
+// *TPCALC .COLLISION starts a .1D run from a Gaussian wave packet with a
+// momentum (**TI *COLLISION_ENERGY, *SIZE_OF_GAUSSIAN, *INIT_POSSITION).
+// Anything else -- 3D computed states, several transitions, 2D collisions,
 // .2DC operators -- is refused with a message: there is no CPU path.
 //
 // The run follows espec.f: the .FILE reads of RDPTE / RDPT (rdpte.f, rdpt.f:
