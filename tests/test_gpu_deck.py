@@ -112,10 +112,8 @@ def test_deck_matches_executable(capfd, name):
 #   .PFSPO, .PFSOD (tests 6, 12, 10): the executable's C(t) drifts from the
 #     oracle's restatements of spofft.f / sodfft.f (which the GPU matches to
 #     print precision) by a phase growing linearly with t: 3e-7 (.PFSPO) and
-#     6.3e-6 (.PFSOD, N = 250) after 2.5 million steps.  fft3d.f assigns its
-#     constants RAD, C72, S72, S120 from default-REAL (single precision)
-#     literals, so the executable's transforms differ from a DFT by a
-#     relative 3e-8;
+#     6.3e-6 (.PFSOD, N = 250) after 2.5 million steps; the cause is not
+#     pinned (fft3d.f's single-precision constants are a candidate);
 #   .PSIL, .PPSIL (tests 13, 14): the executable bisects the eigenvalues of
 #     its Krylov matrices to ABSTOL = 1e-6 only, so its norm falls by 3e-6
 #     over the 125 thousand steps and C(t) moves by up to 4.5e-6; its total
