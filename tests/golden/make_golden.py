@@ -29,6 +29,8 @@ Cases:
   calc2d_*    2D decks with computed initial states (.CALC, .MTRXDIAG) and the
               executable's output, with its MAKECST lines (constants.txt);
               --calc2d-only generates only these.
+  makecst_lines.json  MAKECST's printed constants for every named 1D/2D form
+              (a .PES deck each); --makecst-only generates only these.
   collision_* a Gaussian wave packet with momentum (.COLLISION) in a 1D well,
               .PSOD and .PFSPO; --collision-only generates only these.
   ti_*        the time-independent formalism (.ENERGY, .SPECTRUM .TI) on the
@@ -714,6 +716,57 @@ def case_collision(name):
         f.write("\n".join(lines[k - 1:]) + "\n")
 
 
+# MAKECST's unit conversion (makecst.f:82-340) for every named form: a
+# .PES deck per form with two constant records, and the lines the executable
+# prints from " Initial potential:" to " Units converted."
+MAKECST_FORMS = [
+    (".1D", ".OHS", "1.146 1943.79", "1.211 1629.23"),
+    (".1D", ".DOHS", "1.146 1943.79 1.2 1.3 1629.23", "1.211 1629.23 1.25 1.35 1500.0"),
+    (".1D", ".MORSE", "1.146 1943.79 13.71", "1.211 1629.23 17.74"),
+    (".1D", ".MORSE_CM^1", "1.146 1943.79 13.71", "1.211 1629.23 17.74"),
+    (".1D", ".MORSE_Dalpha", "1.146 1.9 4.6", "1.211 2.1 3.1"),
+    (".1D", ".MORSE_Dalpha_au", "2.17 1.0 0.17", "2.29 1.1 0.12"),
+    (".1D", ".ANTI-MORSE", "1.146 1943.79 13.71", "1.211 1629.23 17.74"),
+    (".1D", ".MORSEM", "1.146 1943.79 13.71", "1.211 1629.23 17.74"),
+    (".1D", ".MOD-MORSE", "1.146 1943.79 13.71", "1.211 1629.23 17.74"),
+    (".1D", ".BARRIER", "1.0 1.3 0.5", "1.1 1.4 0.6"),
+    (".1D", ".BARRIER_au", "2.0 2.5 0.02", "2.1 2.6 0.03"),
+    (".1D", ".CONST", "0.5", "0.7"),
+    (".1D", ".FREE", "0.0", "0.0"),
+    (".2D", ".OHS", "1.146 1943.79 1.146 1700.0", "1.211 1629.23 1.18 1800.0"),
+    (".2D", ".LSM", "1.1 1.9 30000 2.1 25000 1.2 1.8 20000",
+     "1.15 1.8 31000 2.0 24000 1.25 1.7 21000"),
+    (".2D", ".LS", "1.1 1.9 30000 2.1 25000", "1.15 1.8 31000 2.0 24000"),
+    (".2D", ".LEPS_Dalpha", "0.74 1.94 4.75 0.74 1.94 4.75 0.74 1.94 4.75 0.3 0.05 0.05 180",
+     "0.74 1.94 4.75 0.74 1.94 4.75 0.74 1.94 4.75 0.3 0.05 0.05 180"),
+    (".2D", ".BARRIERXY", "1.0 1.3 0.5 1.1 1.4 0.6", "1.0 1.3 0.5 1.1 1.4 0.6"),
+    (".2D", ".WELLY", "1.0 1.3 0.5", "1.1 1.4 0.6"),
+    (".2D", ".BARRIER", "1.0 1.3 1.1 1.4 0.5", "1.0 1.3 1.1 1.4 0.6"),
+    (".2D", ".CONST", "0.5", "0.7"),
+    (".2D", ".MORSE", "2.0 1.0 0.17 2.3 0.9 0.15", "2.1 1.0 0.17 2.4 0.9 0.14"),
+]
+
+
+def makecst_deck(dim, form, c1, c2):
+    npt, ranges, mass = (" 64/", " 0.9  1.5/", " 7.49D0/") if dim == ".1D" else \
+        (" 32 32/", " 0.9  1.5  0.9  1.5/", " 7.49D0  9.0D0/")
+    return (f"*** eSPec input file ***\n**MAIN\n*TITLE\n MAKECST {form}\n*DIMENSION\n{dim}\n"
+            f"{npt}\n*POTENTIAL\n{form}\n {c1}/\n {c2}/\n*GRID_RANGES\n{ranges}\n*MASS\n"
+            f"{mass}\n*TPCALC\n.PES\n*INIEIGVC\n.CALC\n*CHANGE\n.YES\n**END\n")
+
+
+def case_makecst():
+    out = {}
+    for dim, form, c1, c2 in MAKECST_FORMS:
+        deck = makecst_deck(dim, form, c1, c2)
+        lines = run_deck(deck, {}).splitlines()
+        i = lines.index(" Initial potential:")
+        j = lines.index(" Units converted.")
+        out[f"{dim}{form}"] = {"deck": deck, "lines": lines[i:j - 1]}
+    with open(os.path.join(OUT, "makecst_lines.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def case_calc2d(name):
     deck = CALC2D[name]
     d = os.path.join(OUT, name)
@@ -756,6 +809,9 @@ def main():
     if "--calc2d-only" in sys.argv:
         for name in CALC2D:
             case_calc2d(name)
+        return
+    if "--makecst-only" in sys.argv:
+        case_makecst()
         return
     if "--collision-only" in sys.argv:
         for name in COLLISION_DECKS:
@@ -818,6 +874,7 @@ def main():
         case_ti(name, deck)
     for name in COLLISION_DECKS:
         case_collision(name)
+    case_makecst()
 
 
 if __name__ == "__main__":

@@ -357,3 +357,20 @@ def test_collision_decks_are_read(tmp_path):
     assert msg is not None and "*SIZE_OF_GAUSSIAN" in msg, msg
     msg = run_calc(tmp_path, text.replace(".1D\n 512/", ".2D\n 64 64/"))
     assert msg is not None and ".COLLISION" in msg, msg
+
+
+def test_makecst_every_form(tmp_path, capfd):
+    """MAKECST (makecst.f:82-340) for every named 1D and 2D form: the lines
+    the executable prints for a .PES deck per form (tests/golden/
+    makecst_lines.json), compared with the driver's, printed before any
+    device work."""
+    import json
+    with open(os.path.join(HERE, "golden", "makecst_lines.json")) as f:
+        cases = json.load(f)
+    assert len(cases) >= 20
+    for name, case in cases.items():
+        capfd.readouterr()
+        msg = run_calc(tmp_path, case["deck"])
+        out = capfd.readouterr().out.split("\n")
+        i = out.index(" Initial potential:")
+        assert out[i:i + len(case["lines"])] == case["lines"], (name, msg)
