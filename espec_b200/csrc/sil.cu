@@ -54,6 +54,13 @@ __device__ bool grid_reduce(const SilArgs& a, const double* sp, double* st, int 
                             int* s_flag, double* s_red /* kSilThreads doubles */,
                             unsigned& phase) {
   const int b = blockIdx.x, G = gridDim.x, t = threadIdx.x;
+  if (G == 1) {  // one CTA: its partials are the totals (the same bits: 0 + x)
+    ++phase;
+    __syncthreads();
+    for (int q = t; q < nq; q += blockDim.x) st[q] = 0.0 + sp[q];
+    __syncthreads();
+    return true;
+  }
   double* part = a.part + (size_t)(phase & 1u) * G * kSilNQ;
   // a.bar counts the arrivals of the launch (zeroed before it): barrier k is
   // passed once it reaches (k + 1) G
